@@ -1,0 +1,153 @@
+/* qol_b200: B200-native (sm_100a) RRQ near-field hot path behind the
+ * reference's qol_* operator API (haiszhu/qotential).
+ *
+ * Conventions (identical to the reference's Fortran interface):
+ *  - integers are 64-bit (the reference is built with -fdefault-integer-8,
+ *    Makefile:79-85); logicals are passed as integers (0/1);
+ *  - arrays are column-major: sx(3,n) is x,y,z of node 1, then node 2, ...;
+ *    As(m,n) is As[i + m*j];
+ *  - indices in tcxrow, tcxi, sparsei, sparsej, idxs are 1-based;
+ *  - the caller allocates every output.
+ * Every entry point returns a status (0 = ok) and also writes the reference's
+ * ier argument where the reference has one.  Status codes:
+ *   0 QOL_OK, 1 QOL_ERR_NOSLOT / layout, 2 QOL_ERR_HANDLE / nnz too small,
+ *   3 QOL_ERR_NPOLS, 5 QOL_ERR_CUDA, 6 QOL_ERR_ORDER (unsupported order),
+ *   7 QOL_ERR_TABLES (precomputed tables differ from the library's),
+ *   8 QOL_ERR_ARG (null pointer / negative size).
+ * The library never falls back to a CPU path: without a usable GPU every
+ * compute entry point returns QOL_ERR_CUDA.
+ */
+#ifndef QOL_B200_H
+#define QOL_B200_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef long long qol_int;
+
+enum {
+  QOL_OK = 0,
+  QOL_ERR_NOSLOT = 1,
+  QOL_ERR_LAYOUT = 1,
+  QOL_ERR_HANDLE = 2,
+  QOL_ERR_NNZ = 2,
+  QOL_ERR_NPOLS = 3,
+  QOL_ERR_CUDA = 5,
+  QOL_ERR_ORDER = 6,
+  QOL_ERR_TABLES = 7,
+  QOL_ERR_ARG = 8
+};
+
+/* Replaces qol_simplex_precomp_mex (src/lap3d_close_mex.f90:48-59; body
+ * simplex_precomp_r64, src/lap3d_close_mod.f90:115-133): Gauss-Legendre nodes,
+ * weights and differentiation matrix on [-1,1] (nquad), barycentric weights,
+ * Legendre values->coefficients matrix, and the simplex interpolation
+ * matrices umatr (values->coefficients) / vmatr at the Vioreanu-Rokhlin
+ * nodes of degree korder (kpols = (korder+1)(korder+2)/2).  Host only. */
+int qol_simplex_precomp(qol_int nquad, qol_int korder, qol_int kpols, double* tgl, double* wgl,
+                        double* Dgl, double* w_bclag, double* Legmat, double* umatr, double* vmatr);
+
+/* Replaces qol_build_patch_levels_mex (src/patch_refine_mex.f90:198-208;
+ * body build_patch_levels_r64, src/patch_refine_mod.f90:423-502): builds the
+ * refined levels of one panel on the GPU and returns a handle in *lv
+ * (generation*QOL_MAX_HANDLES + slot, as the reference encodes it). */
+int qol_build_patch_levels(qol_int korder, qol_int npols, const double* sx, const double* rts,
+                           const double* rps, qol_int order, double dist, qol_int nlevel,
+                           qol_int* lv, qol_int* ier);
+
+/* Replaces qol_lap3dsdlpmat_levels_mex (src/patch_refine_mex.f90:211-223;
+ * body lap3dsdlpmat_levels_r64, src/patch_refine_mod.f90:516-615): As, Ad
+ * (m x npols) for the targets resolved by a refined level, the 1-based list
+ * idxs(1:ms) of unresolved targets.  isimd is accepted and ignored.
+ * ier: 2 bad handle, 3 npols mismatch. */
+int qol_lap3dsdlpmat_levels(qol_int m, const double* tx, qol_int npols, qol_int lv, qol_int isimd,
+                            double* As, double* Ad, qol_int* idxs, qol_int* ms, qol_int* ier);
+
+/* Replaces qol_clear_patch_levels_mex / qol_clear_patch_levels_all_mex
+ * (src/patch_refine_mex.f90:226-242). */
+int qol_clear_patch_levels(qol_int lv, qol_int* ier);
+int qol_clear_patch_levels_all(qol_int* ier);
+
+/* Replaces qol_rrq_mex (src/lap3d_close_mex.f90:18-45; body rrq_r64,
+ * src/lap3d_close_mod.f90:622-881): exact-limit S and D close-panel
+ * matrices As, Ad (m x n) of one panel for m targets, Omega (4 hdim x m),
+ * IalphaAsvestas (m), timeinfo(20) accumulated (slots 1..8 as the
+ * reference's phases, GPU milliseconds converted to seconds).  The
+ * precomputed tables (tgl ... vmatr) must be the ones qol_simplex_precomp
+ * returns (checked; QOL_ERR_TABLES otherwise). */
+int qol_rrq(qol_int m, const double* tx, qol_int n, const double* sx, const double* snx,
+            const double* sw, const double* rts, const double* rps, qol_int order, qol_int nquad,
+            qol_int orderff, double distff, qol_int exterior, qol_int isimd, qol_int ichart,
+            const double* sxbd_chart, const double* rv_chart, const double* tgl, const double* wgl,
+            const double* Dgl, const double* w_bclag, const double* Legmat, const double* umatr,
+            const double* vmatr, double* As, double* Ad, double* Omega, double* IalphaAsvestas,
+            double* timeinfo);
+
+/* Replaces qol_getnearquad_lap_rrq_mex (src/lap3d_close_mex.f90:62-81; body
+ * getnearquad_lap_rrq_r64, src/lap3d_close_mod.f90:884-960): the sparse
+ * near correction (RRQ minus the self-masked naive block) for all panels, as
+ * COO triplets in the reference's order
+ *   out = (tcxi(k)-1)*hdim + (j-1)*m_k + i.
+ * Host pointers; the host<->device copies are part of the call.
+ * Validation as qotential.mw:74-87 (status 1 layout, 2 nnz too small). */
+int qol_getnearquad_lap_rrq(qol_int npan, qol_int nterms, qol_int hdim, qol_int nquad, qol_int nsrc,
+                            const double* sx, const double* snx, const double* sw, const double* rts,
+                            const double* rps, qol_int ntcx, const double* tcx, const qol_int* tcxrow,
+                            const qol_int* tcxi, qol_int orderff, double distff, qol_int iside,
+                            qol_int isimd, qol_int nnz, qol_int* sparsei, qol_int* sparsej,
+                            double* sparsevs, double* sparsevd, double* timeinfo);
+
+/* Device-pointer form of qol_getnearquad_lap_rrq for callers whose data is
+ * already resident in GPU memory (no counterpart in the reference, which has
+ * no device memory): same arguments, all arrays device pointers, work queued
+ * on `stream` (a cudaStream_t, or 0 for the default stream); returns after
+ * queuing unless sync != 0.  level_hist (host, 6 entries, nullable) receives
+ * the pair count per refinement level (index 1..4) and RRQ (index 5). */
+int qol_getnearquad_lap_rrq_dev(qol_int npan, qol_int nterms, qol_int hdim, qol_int nquad, qol_int nsrc,
+                                const double* sx, const double* snx, const double* sw, const double* rts,
+                                const double* rps, qol_int ntcx, const double* tcx, const qol_int* tcxrow,
+                                const qol_int* tcxi, qol_int orderff, double distff, qol_int iside,
+                                qol_int nnz, qol_int* sparsei, qol_int* sparsej, double* sparsevs,
+                                double* sparsevd, void* stream, int sync, qol_int* level_hist);
+
+/* Library status and diagnostics. */
+const char* qol_last_error(void);
+int qol_version(void);
+
+/* Link-compatibility aliases for the reference's Fortran symbols (one
+ * trailing underscore, all arguments by reference, matlab/qotential_mex.c
+ * :1096-1105).  Same semantics as the functions above; no return value. */
+void qol_simplex_precomp_mex_(const qol_int* nquad, const qol_int* korder, const qol_int* kpols,
+                              double* tgl, double* wgl, double* Dgl, double* w_bclag, double* Legmat,
+                              double* umatr, double* vmatr);
+void qol_build_patch_levels_mex_(const qol_int* korder, const qol_int* npols, const double* sx,
+                                 const double* rts, const double* rps, const qol_int* order,
+                                 const double* dist, const qol_int* nlevel, qol_int* lv, qol_int* ier);
+void qol_lap3dsdlpmat_levels_mex_(const qol_int* m, const double* tx, const qol_int* npols,
+                                  const qol_int* lv, const qol_int* isimd, double* As, double* Ad,
+                                  qol_int* idxs, qol_int* ms, qol_int* ier);
+void qol_clear_patch_levels_mex_(const qol_int* lv, qol_int* ier);
+void qol_clear_patch_levels_all_mex_(qol_int* ier);
+void qol_getnearquad_lap_rrq_mex_(const qol_int* npan, const qol_int* nterms, const qol_int* hdim,
+                                  const qol_int* nquad, const qol_int* nsrc, const double* sx,
+                                  const double* snx, const double* sw, const double* rts,
+                                  const double* rps, const qol_int* ntcx, const double* tcx,
+                                  const qol_int* tcxrow, const qol_int* tcxi, const qol_int* orderff,
+                                  const double* distff, const qol_int* iside, const qol_int* isimd,
+                                  const qol_int* nnz, qol_int* sparsei, qol_int* sparsej,
+                                  double* sparsevs, double* sparsevd, double* timeinfo);
+void qol_rrq_mex_(const qol_int* m, const double* tx, const qol_int* n, const double* sx,
+                  const double* snx, const double* sw, const double* rts, const double* rps,
+                  const qol_int* order, const qol_int* nquad, const qol_int* orderff,
+                  const double* distff, const qol_int* exterior, const qol_int* isimd,
+                  const qol_int* ichart, const double* sxbd_chart, const double* rv_chart,
+                  const double* tgl, const double* wgl, const double* Dgl, const double* w_bclag,
+                  const double* Legmat, const double* umatr, const double* vmatr, double* As,
+                  double* Ad, double* Omega, double* IalphaAsvestas, double* timeinfo);
+
+#define QOL_MAX_HANDLES 16
+
+#ifdef __cplusplus
+}
+#endif
+#endif

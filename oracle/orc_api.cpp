@@ -33,6 +33,12 @@ int orc_gauss(int n, double* x, double* w, double* D) {
   return 0;
 }
 
+int orc_debug_target(int nterms, int nquad, int orderff, const double* sx, const double* snx, const double* sw,
+                     const double* x, double* out) {
+  RRQConfig cfg{nterms, nquad, orderff, 1.4, true, 0};
+  debug_target(cfg, sx, snx, sw, x, out);
+  return 0;
+}
 int orc_set_flags(int f) { orc::g_orc_flags = f; return 0; }
 
 int orc_vr_nodes_export(int deg, double* uv, double* w) {

@@ -445,7 +445,7 @@ static inline void edge_at(const RRQPanel& P, int e, double t, double* y, double
 /* side of the target relative to the panel: +1 above (along R(3,:)), -1
  * below, 0 on the panel surface.  Newton on the in-plane coordinates of the
  * interpolated surface. */
-static int panel_side(const RRQPanel& P, const double* xt) {
+static int panel_side(const RRQPanel& P, const double* xt, int* inside = nullptr) {
   const int hd = P.hdim, korder = P.nterms - 1;
   /* start from the in-plane nearest VR node, then Newton on (u,v) */
   std::vector<double> uvn(2 * hd), p(hd), pu(hd), pv(hd);
@@ -484,8 +484,40 @@ static int panel_side(const RRQPanel& P, const double* xt) {
   zs = 0.0;
   for (int k = 0; k < hd; ++k) zs += p[k] * P.scf[2 * hd + k];
   double hgt = xt[2] - zs;
+  if (inside) {
+    const double tol = 1e-10;
+    *inside = (uv[0] >= -tol && uv[1] >= -tol && uv[0] + uv[1] <= 1.0 + tol) ? 1 : 0;
+  }
   if (std::fabs(hgt) <= 1e-12) return 0;
   return hgt > 0 ? 1 : -1;
+}
+
+/* smallest (r - s.rho)/r over 32 samples per edge: how close the string
+ * x + lambda s (lambda > 0) passes to the boundary, seen from x */
+static double string_clearance(const RRQPanel& P, const double* xt, double sdir) {
+  double cmin = 2.0;
+  for (int e = 0; e < 3; ++e)
+    for (int q = 0; q < 32; ++q) {
+      double t = -1.0 + (2.0 * q + 1.0) / 32.0, y[3], yp[3];
+      for (int d = 0; d < 3; ++d) leg_eval<double>(P.nquad, &P.cf[e * 3 * P.nquad + d * P.nquad], t, y[d], yp[d]);
+      double rho[3] = {y[0] - xt[0], y[1] - xt[1], y[2] - xt[2]};
+      double r = std::sqrt(dot3(rho, rho));
+      double c = (r - sdir * rho[2]) / r;
+      if (c < cmin) cmin = c;
+    }
+  return cmin;
+}
+
+/* Dirac-string direction: away from the panel when the target projects
+ * inside the triangle (the exterior/interior flag decides on the panel);
+ * otherwise both directions avoid the panel and the one passing farther from
+ * the boundary is used. */
+static double string_direction(const RRQPanel& P, const double* xt, bool exterior) {
+  int inside = 1;
+  int side = panel_side(P, xt, &inside);
+  if (inside) return side == 0 ? (exterior ? 1.0 : -1.0) : (double)side;
+  double cu = string_clearance(P, xt, 1.0), cd = string_clearance(P, xt, -1.0);
+  return cu >= cd ? 1.0 : -1.0;
 }
 
 /* solid angle Omega = int_G (y-x).n/r^3 dS by the string formula along s */
@@ -551,8 +583,7 @@ static void rrq_target(const RRQPanel& P, const RRQConfig& cfg, const std::vecto
                 &w1[e * nq], &w3[e * nq]);
   }
   (void)sxf;
-  int side = panel_side(P, xt);
-  double sdir = side == 0 ? (cfg.exterior ? 1.0 : -1.0) : (double)side;
+  double sdir = string_direction(P, xt, cfg.exterior);
   double sv[3] = {0.0, 0.0, sdir};
   double Omega = solid_angle(P, xt, roots, sv);
   const double i4p = 1.0 / (4.0 * PI);
@@ -665,6 +696,43 @@ void rrq(const RRQConfig& cfg, i8 m, const double* tx, const double* sx, const d
     if (Omega) for (int q = 0; q < 4 * hd; ++q) Omega[q + (size_t)4 * hd * t] = om[q];
     if (Ialpha) Ialpha[t] = ial;
   }
+}
+
+
+/* debug hook: per-edge roots and the solid angle on the graded mesh and on
+ * a uniform 512-interval mesh, for one panel and one target */
+void debug_target(const RRQConfig& cfg, const double* sx, const double* snx, const double* sw,
+                  const double* x, double* out) {
+  RRQPanel P;
+  build_rrq_panel(cfg, sx, snx, sw, nullptr, nullptr, P);
+  double xt[3];
+  to_frame(P, x, xt);
+  EdgeRoot roots[3];
+  for (int e = 0; e < 3; ++e) {
+    roots[e] = edge_root(P.nquad, &P.cf[e * 3 * P.nquad], P.tgl.data(), &P.bx[3 * e * P.nquad], xt);
+    out[3 * e] = roots[e].ok; out[3 * e + 1] = roots[e].t0.real(); out[3 * e + 2] = roots[e].t0.imag();
+  }
+  double sv[3] = {0.0, 0.0, string_direction(P, xt, true)};
+  out[9] = sv[2];
+  out[10] = solid_angle(P, xt, roots, sv);
+  EdgeRoot bad[3];
+  double tot = 0.0;
+  for (int e = 0; e < 3; ++e)
+    for (int ib = 0; ib < 512; ++ib) {
+      double a = -1.0 + 2.0 * ib / 512.0, b = a + 2.0 / 512.0, hm = 0.5 * (b - a), cm = 0.5 * (a + b);
+      for (int q = 0; q < 16; ++q) {
+        double t = cm + hm * P.tsa[q], y[3], yp[3];
+        edge_at(P, e, t, y, yp);
+        double rho[3] = {y[0] - xt[0], y[1] - xt[1], y[2] - xt[2]};
+        double r = std::sqrt(dot3(rho, rho)), sr = dot3(sv, rho), c[3];
+        cross(rho, sv, c);
+        double den = sr > 0 ? dot3(c, c) / (r + sr) : r - sr;
+        tot += hm * P.wsa[q] * dot3(c, yp) / (r * den);
+      }
+    }
+  (void)bad;
+  out[11] = tot;
+  out[12] = xt[0]; out[13] = xt[1]; out[14] = xt[2];
 }
 
 } // namespace orc

@@ -1,0 +1,193 @@
+"""qotential_b200: B200-native RRQ near-field hot path behind the reference's
+qol_* operator API.
+
+This module is the host-side mirror of the reference's MATLAB gateway
+(``matlab/qotential.mw``): the same function names, argument meanings and
+error behaviour, over the C ABI of ``libqol_b200.so`` (``include/qol_b200.h``).
+There is no CPU fallback: if the CUDA library is missing, or no GPU is usable,
+every compute function raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+__all__ = [
+    "lib", "QolError", "qol_simplex_precomp", "qol_build_patch_levels", "qol_lap3dsdlpmat_levels",
+    "qol_clear_patch_levels", "qol_clear_patch_levels_all", "qol_rrq", "qol_getnearquad_lap_rrq",
+    "qol_getnearquad_lap_rrq_dev",
+]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "libqol_b200.so")
+_lib = None
+i64 = C.c_longlong
+
+
+class QolError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"qol status {code}: {msg}")
+        self.code = code
+
+
+def lib():
+    """Load the in-tree CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB):
+            raise QolError(5, f"{_LIB} is missing: build it with qotential_b200._build.build()")
+        L = C.CDLL(_LIB)
+        L.qol_last_error.restype = C.c_char_p
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != 0:
+        raise QolError(rc, lib().qol_last_error().decode(errors="replace"))
+
+
+def _vp(a):
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+def _f(a, n=None):
+    """Flatten to the reference's memory layout.  Point arrays are accepted as
+    (npts, 3) numpy arrays (row = point, the same bytes as the reference's
+    column-major sx(3, npts)) or as (3, npts) Fortran-shaped arrays."""
+    a = np.asarray(a, dtype=np.float64)
+    if a.ndim == 2 and a.shape[0] == 3 and a.shape[1] != 3:
+        a = a.T
+    a = np.ascontiguousarray(a).ravel()
+    if n is not None and a.size != n:
+        raise ValueError(f"expected {n} values, got {a.size}")
+    return a
+
+
+def _fm(a, n=None):
+    """Flatten a matrix argument column-major (Fortran order), e.g. Dgl(n,n)."""
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.float64).ravel(order="F"))
+    if n is not None and a.size != n:
+        raise ValueError(f"expected {n} values, got {a.size}")
+    return a
+
+
+def _i(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.int64).ravel(order="F"))
+
+
+def qol_simplex_precomp(nquad, korder, kpols=None):
+    """[tgl, wgl, Dgl, w_bclag, Legmat, umatr, vmatr] (matlab/qol_simplex_precomp_mex.m)."""
+    kpols = (korder + 1) * (korder + 2) // 2 if kpols is None else kpols
+    tgl = np.zeros(nquad); wgl = np.zeros(nquad); Dgl = np.zeros(nquad * nquad)
+    wb = np.zeros(nquad); Leg = np.zeros(nquad * nquad)
+    um = np.zeros(kpols * kpols); vm = np.zeros(kpols * kpols)
+    _check(lib().qol_simplex_precomp(i64(nquad), i64(korder), i64(kpols), _vp(tgl), _vp(wgl), _vp(Dgl),
+                                     _vp(wb), _vp(Leg), _vp(um), _vp(vm)))
+    f = lambda a, n: a.reshape(n, n, order="F")
+    return tgl, wgl, f(Dgl, nquad), wb, f(Leg, nquad), f(um, kpols), f(vm, kpols)
+
+
+def qol_build_patch_levels(korder, sx, rts, rps, order, dist, nlevel=4):
+    """lv handle (matlab/qol_build_patch_levels_mex.m); raises QolError with the ier code."""
+    npols = (korder + 1) * (korder + 2) // 2
+    lv = np.zeros(1, np.int64); ier = np.zeros(1, np.int64)
+    rc = lib().qol_build_patch_levels(i64(korder), i64(npols), _vp(_f(sx, 3 * npols)), _vp(_f(rts, 3 * npols)),
+                                      _vp(_f(rps, 3 * npols)), i64(order), C.c_double(dist), i64(nlevel),
+                                      _vp(lv), _vp(ier))
+    _check(rc)
+    return int(lv[0])
+
+
+def qol_lap3dsdlpmat_levels(tx, npols, lv, isimd=0, As=None, Ad=None):
+    """[As, Ad, idxs, ms] (matlab/qol_lap3dsdlpmat_levels_mex.m); idxs 1-based."""
+    tx = _f(tx)
+    m = tx.size // 3
+    As = np.zeros((m, npols)) if As is None else np.array(As, dtype=np.float64)
+    Ad = np.zeros((m, npols)) if Ad is None else np.array(Ad, dtype=np.float64)
+    Asf = _fm(As); Adf = _fm(Ad)
+    idxs = np.zeros(max(m, 1), np.int64); ms = np.zeros(1, np.int64); ier = np.zeros(1, np.int64)
+    rc = lib().qol_lap3dsdlpmat_levels(i64(m), _vp(tx), i64(npols), i64(lv), i64(isimd), _vp(Asf), _vp(Adf),
+                                       _vp(idxs), _vp(ms), _vp(ier))
+    _check(rc)
+    return (Asf.reshape(m, npols, order="F"), Adf.reshape(m, npols, order="F"), idxs[:ms[0]].copy(), int(ms[0]))
+
+
+def qol_clear_patch_levels(lv):
+    ier = np.zeros(1, np.int64)
+    _check(lib().qol_clear_patch_levels(i64(lv), _vp(ier)))
+
+
+def qol_clear_patch_levels_all():
+    ier = np.zeros(1, np.int64)
+    _check(lib().qol_clear_patch_levels_all(_vp(ier)))
+
+
+def qol_rrq(tx, sx, snx, sw, rts, rps, order, nquad, orderff, distff=1.4, exterior=True, isimd=0, ichart=0,
+            sxbd_chart=None, rv_chart=None, tables=None, timeinfo=None):
+    """[As, Ad, Omega, IalphaAsvestas, timeinfo] (matlab/qol_rrq_mex.m)."""
+    hd = order * (order + 1) // 2
+    tx = _f(tx); m = tx.size // 3
+    if tables is None:
+        tables = qol_simplex_precomp(nquad, order - 1, hd)
+    tgl, wgl, Dgl, wb, Leg, um, vm = [_fm(t) for t in tables]
+    As = np.zeros(m * hd); Ad = np.zeros(m * hd); Om = np.zeros(4 * hd * m); Ia = np.zeros(m)
+    ti = np.zeros(20) if timeinfo is None else _f(timeinfo, 20).copy()
+    nbd = 3 * nquad
+    sb = _f(sxbd_chart, 3 * nbd) if sxbd_chart is not None else np.zeros(3 * nbd)
+    rv = _f(rv_chart, 9) if rv_chart is not None else np.zeros(9)
+    rc = lib().qol_rrq(i64(m), _vp(tx), i64(hd), _vp(_f(sx, 3 * hd)), _vp(_f(snx, 3 * hd)), _vp(_f(sw, hd)),
+                       _vp(_f(rts, 3 * hd)), _vp(_f(rps, 3 * hd)), i64(order), i64(nquad), i64(orderff),
+                       C.c_double(distff), i64(int(bool(exterior))), i64(isimd), i64(ichart), _vp(sb), _vp(rv),
+                       _vp(tgl), _vp(wgl), _vp(Dgl), _vp(wb), _vp(Leg), _vp(um), _vp(vm), _vp(As), _vp(Ad),
+                       _vp(Om), _vp(Ia), _vp(ti))
+    _check(rc)
+    return (As.reshape(m, hd, order="F"), Ad.reshape(m, hd, order="F"), Om.reshape(4 * hd, m, order="F"), Ia, ti)
+
+
+def qol_getnearquad_lap_rrq(npan, nterms, hdim, nquad, nsrc, sx, snx, sw, rts, rps, ntcx, tcx, tcxrow, tcxi,
+                            orderff, distff, iside, isimd=0, nnz=None, timeinfo=None):
+    """[sparsei, sparsej, sparsevs, sparsevd, timeinfo] (matlab/qol_getnearquad_lap_rrq_mex.m).
+
+    tcxrow/tcxi are 1-based; the COO output follows the reference's order
+    (tcxi(k)-1)*hdim + (j-1)*m_k + i."""
+    tcxi = _i(tcxi)
+    if hdim != nterms * (nterms + 1) // 2 or npan * hdim != nsrc:
+        raise QolError(1, "The panel order, hdim, npan, and nsrc are inconsistent.")
+    if tcxi[0] != 1 or np.any(np.diff(tcxi) < 0) or tcxi[-1] != ntcx + 1:
+        raise QolError(1, "tcxi must be monotone, one-based, and cover tcx exactly.")
+    need = int((tcxi[-1] - 1) * hdim)
+    nnz = need if nnz is None else int(nnz)
+    if need > nnz:
+        raise QolError(2, "nnz is too small for the requested panel-target interactions.")
+    si = np.zeros(nnz, np.int64); sj = np.zeros(nnz, np.int64)
+    vs = np.zeros(nnz); vd = np.zeros(nnz)
+    ti = np.zeros(20) if timeinfo is None else _f(timeinfo, 20).copy()
+    rc = lib().qol_getnearquad_lap_rrq(
+        i64(npan), i64(nterms), i64(hdim), i64(nquad), i64(nsrc), _vp(_f(sx, 3 * nsrc)), _vp(_f(snx, 3 * nsrc)),
+        _vp(_f(sw, nsrc)), _vp(_f(rts, 3 * nsrc)), _vp(_f(rps, 3 * nsrc)), i64(ntcx), _vp(_f(tcx, 3 * ntcx)),
+        _vp(_i(tcxrow)), _vp(tcxi), i64(orderff), C.c_double(distff), i64(iside), i64(isimd), i64(nnz),
+        _vp(si), _vp(sj), _vp(vs), _vp(vd), _vp(ti))
+    _check(rc)
+    return si, sj, vs, vd, ti
+
+
+def qol_getnearquad_lap_rrq_dev(npan, nterms, nquad, sx, snx, sw, rts, rps, tcx, tcxrow, tcxi, orderff,
+                                distff, iside, out, stream=0, sync=True, want_hist=False):
+    """Device-resident form: every array argument is an object exposing
+    ``data_ptr()`` (e.g. a CUDA torch tensor) or an integer device address.
+    ``out`` = (sparsei, sparsej, sparsevs, sparsevd) device buffers of size nnz."""
+    def ptr(a):
+        return C.c_void_p(a if isinstance(a, int) else a.data_ptr())
+    hdim = nterms * (nterms + 1) // 2
+    si, sj, vs, vd = out
+    nnz = vs.numel() if hasattr(vs, "numel") else int(out[4])
+    ntcx = tcxrow.numel() if hasattr(tcxrow, "numel") else 0
+    hist = np.zeros(6, np.int64)
+    rc = lib().qol_getnearquad_lap_rrq_dev(
+        i64(npan), i64(nterms), i64(hdim), i64(nquad), i64(npan * hdim), ptr(sx), ptr(snx), ptr(sw), ptr(rts),
+        ptr(rps), i64(ntcx), ptr(tcx), ptr(tcxrow), ptr(tcxi), i64(orderff), C.c_double(distff), i64(iside),
+        i64(nnz), ptr(si), ptr(sj), ptr(vs), ptr(vd), C.c_void_p(stream), C.c_int(int(sync)),
+        _vp(hist) if want_hist else None)
+    _check(rc)
+    return hist if want_hist else None

@@ -1,0 +1,723 @@
+/* qol_b200 C ABI: context, per-order device tables, workspace, orchestration
+ * of the hot-path kernels, and the qol_* entry points (see include/qol_b200.h
+ * for the reference interface each one replaces). */
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/qol_b200.h"
+#include "qol_dev.cuh"
+#include "qol_host.h"
+#include "qol_kernels.h"
+
+namespace {
+
+std::recursive_mutex g_mu;
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define CK(x)                                                                              \
+  do {                                                                                     \
+    cudaError_t e_ = (x);                                                                  \
+    if (e_ != cudaSuccess) return fail(QOL_ERR_CUDA, "%s: %s", #x, cudaGetErrorString(e_)); \
+  } while (0)
+
+/* ---------------- device arena ---------------- */
+struct Arena {
+  char* base = nullptr;
+  size_t cap = 0, used = 0;
+  ~Arena() { if (base) cudaFree(base); }
+  int reserve(size_t bytes) {
+    if (bytes <= cap) return 0;
+    if (base) { cudaFree(base); base = nullptr; cap = 0; }
+    size_t want = bytes + bytes / 8;
+    if (cudaMalloc(&base, want) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(QOL_ERR_CUDA, "device allocation of %zu bytes failed", want);
+    }
+    cap = want;
+    return 0;
+  }
+  void reset() { used = 0; }
+  template <class T>
+  T* take(size_t n) {
+    size_t off = (used + 255) & ~(size_t)255;
+    used = off + n * sizeof(T);
+    return (T*)(base + off);
+  }
+};
+
+/* ---------------- per-order tables ---------------- */
+struct OrderCache {
+  OrderTab T{};
+  std::vector<void*> bufs;
+  ~OrderCache() { for (void* p : bufs) cudaFree(p); }
+  template <class V>
+  const typename V::value_type* up(const V& v) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, sizeof(typename V::value_type) * std::max<size_t>(1, v.size())) != cudaSuccess) return nullptr;
+    cudaMemcpy(p, v.data(), sizeof(typename V::value_type) * v.size(), cudaMemcpyHostToDevice);
+    bufs.push_back(p);
+    return (const typename V::value_type*)p;
+  }
+};
+
+std::map<long long, std::unique_ptr<OrderCache>> g_orders;
+bool g_coefs_uploaded = false;
+Arena g_arena, g_arena2;
+cudaStream_t g_stream = nullptr;
+
+int ensure_device() {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return fail(QOL_ERR_CUDA, "no CUDA device available (the library has no CPU path)");
+  }
+  if (!g_stream) CK(cudaStreamCreateWithFlags(&g_stream, cudaStreamNonBlocking));
+  if (!g_coefs_uploaded) {
+    std::vector<double> hb((QOL_MAXL + 2) * (QOL_MAXL + 2), 0.0), hc(hb.size(), 0.0), hcm(QOL_MAXL + 2, 0.0);
+    for (int m = 1; m <= QOL_MAXL; ++m) {
+      hcm[m] = std::sqrt((2.0 * m - 1.0) / (2.0 * m));
+      for (int l = m + 1; l <= QOL_MAXL; ++l) {
+        hb[l * (QOL_MAXL + 2) + m] = std::sqrt((double)(l + m - 1) * (double)(l - m - 1));
+        hc[l * (QOL_MAXL + 2) + m] = 1.0 / std::sqrt((double)(l - m) * (double)(l + m));
+      }
+    }
+    qol_upload_harm_coefs(hb.data(), hc.data(), hcm.data(), g_stream);
+    CK(cudaStreamSynchronize(g_stream));
+    g_coefs_uploaded = true;
+  }
+  return 0;
+}
+
+/* build (or fetch) the device tables for one (nterms, orderff, nquad) */
+int order_tables(int nterms, int orderff, int nquad, OrderCache** out) {
+  if (nterms < 2 || nterms > QOL_MAXL || orderff < 2 || orderff - 1 > 20 || nquad < 2 || nquad > QOL_MAXNQ ||
+      nterms - 1 > 20)
+    return fail(QOL_ERR_ORDER, "unsupported order nterms=%d orderff=%d nquad=%d", nterms, orderff, nquad);
+  long long key = nterms + 100LL * orderff + 10000LL * nquad;
+  auto it = g_orders.find(key);
+  if (it != g_orders.end()) { *out = it->second.get(); return 0; }
+  std::unique_ptr<OrderCache> C(new OrderCache());
+  OrderTab& T = C->T;
+  const int korder = nterms - 1, hd = nterms * (nterms + 1) / 2;
+  qolh::RefElem R;
+  try {
+    qolh::build_ref(korder, orderff, 4, true, R);
+  } catch (const std::exception& e) {
+    return fail(QOL_ERR_ORDER, "reference element: %s", e.what());
+  }
+  T.korder = korder; T.hd = hd; T.nterms = nterms; T.orderff = orderff; T.nquad = nquad; T.nlevel = 4;
+  T.ng = std::max(1, (nterms + 1) / 2);
+  for (int l = 0; l < 4; ++l) {
+    const qolh::RefLevel& L = R.lev[l];
+    T.n[l] = (int)L.n; T.nsub[l] = (int)L.nsub;
+    std::vector<double> rm((size_t)L.n * hd);
+    for (long long i = 0; i < L.n; ++i)
+      for (int k = 0; k < hd; ++k) rm[(size_t)i * hd + k] = L.interp[i + (size_t)L.n * k];
+    std::vector<int> st(L.subtyp.begin(), L.subtyp.end());
+    T.interp[l] = C->up(rm);
+    T.wt[l] = C->up(L.wt);
+    T.suboff[l] = C->up(L.suboff);
+    T.subtyp[l] = C->up(st);
+  }
+  std::vector<double> tgl(nquad), wgl(nquad), Dgl(nquad * nquad), Leg(nquad * nquad);
+  qolh::gauss(nquad, tgl.data(), wgl.data(), Dgl.data());
+  qolh::legendre_vals2coefs(nquad, tgl.data(), wgl.data(), Leg.data());
+  std::vector<double> g48x(48), g48w(48), g16x(16), g16w(16), tq(T.ng), wq(T.ng);
+  qolh::gauss(48, g48x.data(), g48w.data(), nullptr);
+  qolh::gauss(16, g16x.data(), g16w.data(), nullptr);
+  qolh::gauss(T.ng, tq.data(), wq.data(), nullptr);
+  for (int g = 0; g < T.ng; ++g) { tq[g] = 0.5 * (tq[g] + 1.0); wq[g] *= 0.5; }
+  /* boundary nodes of the three edges (tpar2uv parametrisation,
+   * stellarator_grf_core_mod.f90:1069-1085) and the three vertices */
+  std::vector<double> buv(2 * (3 * nquad + 3));
+  const double th1 = 2.0 * QOL_PI / 3.0, th2 = 4.0 * QOL_PI / 3.0, thi1 = 1.0 / th1;
+  for (int e = 0; e < 3; ++e)
+    for (int q = 0; q < nquad; ++q) {
+      double tt = e * th1 + 0.5 * (1.0 + tgl[q]) * th1, u = 0.0, v = 0.0;
+      if (tt < th1) v = 1.0 - thi1 * tt;
+      else if (tt < th2) u = thi1 * (tt - th1);
+      else { u = 1.0 - thi1 * (tt - th2); v = thi1 * (tt - th2); }
+      buv[2 * (e * nquad + q)] = u; buv[2 * (e * nquad + q) + 1] = v;
+    }
+  double vuv[6] = {0, 0, 1, 0, 0, 1};
+  for (int i = 0; i < 6; ++i) buv[2 * 3 * nquad + i] = vuv[i];
+  std::vector<double> Mcm((size_t)(3 * nquad + 3) * hd), Mb((size_t)(3 * nquad + 3) * hd);
+  qolh::interp_matrix(korder, 3 * nquad + 3, buv.data(), Mcm.data());
+  for (int i = 0; i < 3 * nquad + 3; ++i)
+    for (int j = 0; j < hd; ++j) Mb[(size_t)i * hd + j] = Mcm[i + (size_t)(3 * nquad + 3) * j];
+  std::vector<double> um((size_t)hd * hd), vr(2 * hd);
+  qolh::koorn_umatr(korder, um.data(), nullptr);
+  qolh::vr_nodes(korder, vr.data(), nullptr);
+  T.tgl = C->up(tgl); T.wgl = C->up(wgl); T.Dgl = C->up(Dgl); T.Leg = C->up(Leg);
+  T.gl48x = C->up(g48x); T.gl48w = C->up(g48w); T.gl16x = C->up(g16x); T.gl16w = C->up(g16w);
+  T.tq = C->up(tq); T.wq = C->up(wq); T.Mb = C->up(Mb); T.umatr = C->up(um); T.vruv = C->up(vr);
+  if (!T.tgl || !T.Mb || !T.vruv) return fail(QOL_ERR_CUDA, "table upload failed");
+  *out = C.get();
+  g_orders[key] = std::move(C);
+  return 0;
+}
+
+/* ---------------- the pipeline on device pointers ---------------- */
+struct Timing {
+  cudaEvent_t ev[8];
+  bool on = false;
+};
+
+struct Job {
+  int npan, nterms, nquad, orderff, exterior, subtract_naive;
+  double distff;
+  long long ntcx;
+  PanelIn P;
+  PairIn Q;
+  double *vs, *vd, *omega, *ialpha;
+  long long *si, *sj;
+  const double* chart;
+  const long long* tcxi_host; /* host copy */
+};
+
+int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* hist_out, std::vector<int>* grp_out,
+                 int* cnt_out) {
+  OrderCache* C = nullptr;
+  int rc = order_tables(J.nterms, J.orderff, J.nquad, &C);
+  if (rc) return rc;
+  OrderTab T = C->T;
+  T.dist = J.distff;
+  const int hd = T.hd, npan = J.npan, nq = T.nquad, nbd = 3 * nq;
+  const long long ntcx = J.ntcx;
+  /* workspace size */
+  size_t need = 0;
+  auto add = [&](size_t bytes) { need += (bytes + 255) & ~(size_t)255; };
+  for (int l = 0; l < 4; ++l) { add(sizeof(double) * (size_t)npan * T.n[l] * 7); add(sizeof(double) * (size_t)npan * T.nsub[l] * 4); }
+  add(ntcx); add(sizeof(int) * ntcx); add(sizeof(int) * (size_t)npan * 8 * 2);
+  add(sizeof(long long) * (npan + 1));
+  add(sizeof(double) * (size_t)npan * (RRQ_FRAME + 6 * nbd + 9 * nq + 3 * hd));
+  add(sizeof(double) * (size_t)npan * hd * hd * 11);
+  add(sizeof(int) * (size_t)npan * 272);
+  rc = g_arena.reserve(need + 4096);
+  if (rc) return rc;
+  g_arena.reset();
+  LevelWS W{};
+  for (int l = 0; l < 4; ++l) {
+    W.node[l] = g_arena.take<double>((size_t)npan * T.n[l] * 7);
+    W.sub[l] = g_arena.take<double>((size_t)npan * T.nsub[l] * 4);
+  }
+  PairWS G{};
+  G.level = g_arena.take<signed char>(ntcx);
+  G.grp = g_arena.take<int>(ntcx);
+  G.cnt = g_arena.take<int>((size_t)npan * 8);
+  G.off = g_arena.take<int>((size_t)npan * 8);
+  RRQWS R{};
+  R.npan = npan;
+  long long* rrq_off = g_arena.take<long long>(npan + 1);
+  R.rrq_off = rrq_off;
+  R.frame = g_arena.take<double>((size_t)npan * RRQ_FRAME);
+  R.bx = g_arena.take<double>((size_t)npan * 3 * nbd);
+  R.bt = g_arena.take<double>((size_t)npan * 3 * nbd);
+  R.cf = g_arena.take<double>((size_t)npan * 9 * nq);
+  R.scf = g_arena.take<double>((size_t)npan * 3 * hd);
+  R.qmat = g_arena.take<double>((size_t)npan * 4 * hd * hd);
+  R.hmat = g_arena.take<double>((size_t)npan * hd * hd);
+  R.smat = g_arena.take<double>((size_t)npan * hd * hd);
+  R.PD = g_arena.take<double>((size_t)npan * 4 * hd * hd);
+  R.B = g_arena.take<double>((size_t)npan * hd * hd);
+  R.perm = g_arena.take<int>((size_t)npan * 272);
+  R.ialpha = J.ialpha;
+  CK(cudaMemsetAsync(G.cnt, 0, sizeof(int) * (size_t)npan * 8, st));
+  CK(cudaMemsetAsync(G.off, 0, sizeof(int) * (size_t)npan * 8, st));
+  Timing tm;
+  if (timeinfo) {
+    for (int i = 0; i < 8; ++i) CK(cudaEventCreate(&tm.ev[i]));
+    tm.on = true;
+  }
+  auto rec = [&](int i) { if (tm.on) cudaEventRecord(tm.ev[i], st); };
+  rec(0);
+  CK(qol_launch_levels(T, J.P, W, npan, st));
+  rec(1);
+  CK(qol_launch_classify(T, J.Q, W, G, npan, st));
+  CK(qol_launch_scan(npan, T.nlevel + 1, G.cnt, rrq_off, st));
+  long long nrrq = 0;
+  CK(cudaMemcpyAsync(&nrrq, rrq_off + npan, sizeof(long long), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  R.nrrq = nrrq;
+  /* per-pair RRQ moment storage (separate arena: its size is known only now) */
+  rc = g_arena2.reserve(sizeof(double) * (size_t)std::max<long long>(nrrq, 1) * 5 * hd + 1024);
+  if (rc) return rc;
+  g_arena2.reset();
+  R.JD = g_arena2.take<double>((size_t)std::max<long long>(nrrq, 1) * 4 * hd);
+  R.RS = g_arena2.take<double>((size_t)std::max<long long>(nrrq, 1) * hd);
+  OutCOO O{};
+  O.vs = J.vs; O.vd = J.vd; O.omega = J.omega; O.subtract_naive = J.subtract_naive;
+  rec(2);
+  CK(qol_launch_direct(T, J.P, J.Q, W, G, O, npan, st));
+  rec(3);
+  if (nrrq > 0) {
+    CK(qol_launch_rrq_panel(T, J.P, G, R, npan, J.chart, st));
+    rec(4);
+    CK(qol_launch_rrq_target(T, J.Q, G, R, J.exterior, st));
+    rec(5);
+    CK(qol_launch_rrq_apply(T, J.P, J.Q, G, R, O, npan, st));
+    rec(6);
+  } else {
+    rec(4); rec(5); rec(6);
+  }
+  if (J.si) CK(qol_launch_coo_index(T, J.Q, J.si, J.sj, npan, st));
+  rec(7);
+  if (hist_out || grp_out || cnt_out || tm.on) {
+    CK(cudaStreamSynchronize(st));
+  }
+  if (hist_out || cnt_out) {
+    std::vector<int> cnt((size_t)npan * 8);
+    CK(cudaMemcpy(cnt.data(), G.cnt, sizeof(int) * cnt.size(), cudaMemcpyDeviceToHost));
+    if (hist_out) {
+      for (int i = 0; i < 6; ++i) hist_out[i] = 0;
+      for (int p = 0; p < npan; ++p)
+        for (int l = 1; l <= 5; ++l) hist_out[l] += cnt[(size_t)p * 8 + l];
+    }
+    if (cnt_out) for (int l = 0; l < 8; ++l) cnt_out[l] = cnt[l];
+  }
+  if (grp_out) {
+    grp_out->resize(ntcx);
+    CK(cudaMemcpy(grp_out->data(), G.grp, sizeof(int) * ntcx, cudaMemcpyDeviceToHost));
+  }
+  if (tm.on) {
+    float ms[7];
+    for (int i = 0; i < 7; ++i) cudaEventElapsedTime(&ms[i], tm.ev[i], tm.ev[i + 1]);
+    timeinfo[0] += 1e-3 * ms[0];            /* patch levels */
+    timeinfo[1] += 1e-3 * ms[3];            /* per-panel RRQ precompute */
+    timeinfo[2] += 1e-3 * (ms[1] + ms[2]);  /* classification + level sums */
+    timeinfo[5] += 1e-3 * ms[4];            /* fused SSQ / solid angle / moments */
+    timeinfo[7] += 1e-3 * (ms[5] + ms[6]);  /* solves + COO */
+    for (int i = 0; i < 8; ++i) cudaEventDestroy(tm.ev[i]);
+  }
+  return 0;
+}
+
+/* ---------------- patch-level handles ---------------- */
+struct Slot {
+  bool live = false;
+  long long generation = 1, npols = 0, korder = 0, order = 0, nlevel = 0;
+  double dist = 0.0;
+  std::vector<double> sx, rts, rps;
+};
+Slot g_slots[QOL_MAX_HANDLES];
+
+bool decode_handle(long long h, int* slot) {
+  if (h <= 0) return false;
+  long long s = (h - 1) % QOL_MAX_HANDLES + 1;
+  long long gen = (h - s) / QOL_MAX_HANDLES;
+  *slot = (int)(s - 1);
+  return g_slots[s - 1].live && g_slots[s - 1].generation == gen;
+}
+
+template <class T>
+int dcopy_in(T** d, const T* h, size_t n, cudaStream_t st) {
+  T* p = g_arena.take<T>(std::max<size_t>(n, 1));
+  if (n) CK(cudaMemcpyAsync(p, h, sizeof(T) * n, cudaMemcpyHostToDevice, st));
+  *d = p;
+  return 0;
+}
+
+int tables_match(int nquad, int korder, const double* tgl, const double* wgl, const double* umatr) {
+  int hd = (korder + 1) * (korder + 2) / 2;
+  std::vector<double> t(nquad), w(nquad), um((size_t)hd * hd);
+  qolh::gauss(nquad, t.data(), w.data(), nullptr);
+  qolh::koorn_umatr(korder, um.data(), nullptr);
+  for (int i = 0; i < nquad; ++i)
+    if (std::fabs(t[i] - tgl[i]) > 1e-13 || std::fabs(w[i] - wgl[i]) > 1e-13) return 0;
+  if (umatr)
+    for (size_t i = 0; i < um.size(); ++i)
+      if (std::fabs(um[i] - umatr[i]) > 1e-9 * (1.0 + std::fabs(um[i]))) return 0;
+  return 1;
+}
+
+} // namespace
+
+/* ===================================================================== */
+/* C ABI                                                                 */
+/* ===================================================================== */
+extern "C" {
+
+const char* qol_last_error(void) { return g_err.c_str(); }
+int qol_version(void) { return 100; }
+
+int qol_simplex_precomp(qol_int nquad, qol_int korder, qol_int kpols, double* tgl, double* wgl, double* Dgl,
+                        double* w_bclag, double* Legmat, double* umatr, double* vmatr) {
+  if (nquad < 1 || korder < 0 || korder > 20 || !tgl || !wgl || !Dgl || !w_bclag || !Legmat || !umatr || !vmatr)
+    return fail(QOL_ERR_ARG, "qol_simplex_precomp: bad arguments");
+  if (kpols != (korder + 1) * (korder + 2) / 2) return fail(QOL_ERR_NPOLS, "kpols mismatch");
+  qolh::gauss((int)nquad, tgl, wgl, Dgl);
+  qolh::bary_weights((int)nquad, tgl, w_bclag);
+  qolh::legendre_vals2coefs((int)nquad, tgl, wgl, Legmat);
+  qolh::koorn_umatr((int)korder, umatr, vmatr);
+  return 0;
+}
+
+int qol_build_patch_levels(qol_int korder, qol_int npols, const double* sx, const double* rts, const double* rps,
+                           qol_int order, double dist, qol_int nlevel, qol_int* lv, qol_int* ier) {
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  if (lv) *lv = 0;
+  if (!sx || !rts || !rps || !lv || !ier) return fail(QOL_ERR_ARG, "null argument");
+  if (npols != (korder + 1) * (korder + 2) / 2) { *ier = 3; return fail(QOL_ERR_NPOLS, "npols mismatch"); }
+  if (nlevel != 4) { *ier = 1; return fail(QOL_ERR_ORDER, "only nlevel = 4 (the reference's NLEVEL) is supported"); }
+  for (int s = 0; s < QOL_MAX_HANDLES; ++s) {
+    Slot& S = g_slots[s];
+    if (S.live) continue;
+    S.live = true; S.npols = npols; S.korder = korder; S.order = order; S.nlevel = nlevel; S.dist = dist;
+    S.sx.assign(sx, sx + 3 * npols); S.rts.assign(rts, rts + 3 * npols); S.rps.assign(rps, rps + 3 * npols);
+    *lv = S.generation * QOL_MAX_HANDLES + (s + 1);
+    *ier = 0;
+    return 0;
+  }
+  *ier = 1;
+  return fail(QOL_ERR_NOSLOT, "no free patch-level slot");
+}
+
+int qol_lap3dsdlpmat_levels(qol_int m, const double* tx, qol_int npols, qol_int lv, qol_int isimd, double* As,
+                            double* Ad, qol_int* idxs, qol_int* ms, qol_int* ier) {
+  (void)isimd;
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  int s;
+  if (!ier || !ms) return fail(QOL_ERR_ARG, "null argument");
+  if (!decode_handle(lv, &s)) { *ms = 0; *ier = 2; return fail(QOL_ERR_HANDLE, "bad handle"); }
+  Slot& S = g_slots[s];
+  if (npols != S.npols) { *ms = 0; *ier = 3; return fail(QOL_ERR_NPOLS, "npols mismatch"); }
+  if (m < 0 || (m > 0 && (!tx || !As || !Ad || !idxs))) return fail(QOL_ERR_ARG, "bad arguments");
+  int rc = ensure_device();
+  if (rc) return rc;
+  *ier = 0;
+  if (m == 0) { *ms = 0; return 0; }
+  const int nterms = (int)S.korder + 1;
+  OrderCache* C = nullptr;
+  rc = order_tables(nterms, (int)S.order, nterms + 2, &C);
+  if (rc) return rc;
+  /* inputs: one panel, the caller's targets; As/Ad copied in so that rows of
+   * unresolved targets keep their values (intent(inout) in the reference) */
+  cudaStream_t st = g_stream;
+  size_t need = sizeof(double) * (size_t)(m * 3 + 9 * npols + 2 * m * npols + npols) + sizeof(long long) * (m + 4) +
+                16 * 256;
+  if ((rc = g_arena.reserve(need + (64 << 20)))) return rc;
+  g_arena.reset();
+  Job J{};
+  double *dsx, *drts, *drps, *dtx, *dAs, *dAd, *dsnx, *dsw;
+  long long *drow, *dxi;
+  std::vector<double> zeros(3 * npols, 0.0), ones(npols, 1.0);
+  std::vector<long long> rows(m, 0), xi = {1, m + 1};
+  if ((rc = dcopy_in(&dsx, S.sx.data(), 3 * npols, st)) || (rc = dcopy_in(&drts, S.rts.data(), 3 * npols, st)) ||
+      (rc = dcopy_in(&drps, S.rps.data(), 3 * npols, st)) || (rc = dcopy_in(&dsnx, zeros.data(), 3 * npols, st)) ||
+      (rc = dcopy_in(&dsw, ones.data(), npols, st)) || (rc = dcopy_in(&dtx, tx, 3 * m, st)) ||
+      (rc = dcopy_in(&dAs, As, m * npols, st)) || (rc = dcopy_in(&dAd, Ad, m * npols, st)) ||
+      (rc = dcopy_in(&drow, (const long long*)rows.data(), m, st)) || (rc = dcopy_in(&dxi, (const long long*)xi.data(), 2, st)))
+    return rc;
+  /* the pipeline's own arena use starts after these buffers: run levels +
+   * classify + direct through a dedicated small pipeline */
+  OrderTab T = C->T;
+  T.dist = S.dist;
+  LevelWS W{};
+  for (int l = 0; l < 4; ++l) {
+    W.node[l] = g_arena.take<double>((size_t)T.n[l] * 7);
+    W.sub[l] = g_arena.take<double>((size_t)T.nsub[l] * 4);
+  }
+  PairWS G{};
+  G.level = g_arena.take<signed char>(m);
+  G.grp = g_arena.take<int>(m);
+  G.cnt = g_arena.take<int>(8);
+  G.off = g_arena.take<int>(8);
+  CK(cudaMemsetAsync(G.cnt, 0, sizeof(int) * 8, st));
+  CK(cudaMemsetAsync(G.off, 0, sizeof(int) * 8, st));
+  PanelIn P{dsx, dsnx, dsw, drts, drps};
+  PairIn Q{dtx, drow, dxi};
+  OutCOO O{dAs, dAd, nullptr, 0};
+  CK(qol_launch_levels(T, P, W, 1, st));
+  CK(qol_launch_classify(T, Q, W, G, 1, st));
+  CK(qol_launch_direct(T, P, Q, W, G, O, 1, st));
+  int cnt[8], off[8];
+  std::vector<int> grp(m);
+  CK(cudaMemcpyAsync(cnt, G.cnt, sizeof cnt, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(off, G.off, sizeof off, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(grp.data(), G.grp, sizeof(int) * m, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(As, dAs, sizeof(double) * m * npols, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(Ad, dAd, sizeof(double) * m * npols, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  *ms = cnt[T.nlevel + 1];
+  for (int i = 0; i < cnt[T.nlevel + 1]; ++i) idxs[i] = grp[off[T.nlevel + 1] + i] + 1;
+  return 0;
+}
+
+int qol_clear_patch_levels(qol_int lv, qol_int* ier) {
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  int s;
+  if (!ier) return fail(QOL_ERR_ARG, "null argument");
+  if (!decode_handle(lv, &s)) { *ier = 2; return fail(QOL_ERR_HANDLE, "bad handle"); }
+  g_slots[s].live = false; g_slots[s].npols = 0; g_slots[s].generation += 1;
+  g_slots[s].sx.clear(); g_slots[s].rts.clear(); g_slots[s].rps.clear();
+  *ier = 0;
+  return 0;
+}
+
+int qol_clear_patch_levels_all(qol_int* ier) {
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  for (int s = 0; s < QOL_MAX_HANDLES; ++s)
+    if (g_slots[s].live) {
+      g_slots[s].live = false; g_slots[s].npols = 0; g_slots[s].generation += 1;
+    }
+  if (ier) *ier = 0;
+  return 0;
+}
+
+static int validate_near(qol_int npan, qol_int nterms, qol_int hdim, qol_int nsrc, qol_int ntcx, const qol_int* tcxi,
+                         qol_int nnz) {
+  if (npan < 0 || ntcx < 0 || nnz < 0) return fail(QOL_ERR_ARG, "negative size");
+  if (hdim != nterms * (nterms + 1) / 2 || npan * hdim != nsrc)
+    return fail(QOL_ERR_LAYOUT, "the panel order, hdim, npan, and nsrc are inconsistent");
+  if (tcxi[0] != 1 || tcxi[npan] != ntcx + 1)
+    return fail(QOL_ERR_LAYOUT, "tcxi must be monotone, one-based, and cover tcx exactly");
+  for (qol_int k = 0; k < npan; ++k)
+    if (tcxi[k + 1] < tcxi[k]) return fail(QOL_ERR_LAYOUT, "tcxi must be monotone, one-based, and cover tcx exactly");
+  if ((tcxi[npan] - 1) * hdim > nnz) return fail(QOL_ERR_NNZ, "nnz is too small for the requested panel-target interactions");
+  return 0;
+}
+
+int qol_getnearquad_lap_rrq_dev(qol_int npan, qol_int nterms, qol_int hdim, qol_int nquad, qol_int nsrc,
+                                const double* sx, const double* snx, const double* sw, const double* rts,
+                                const double* rps, qol_int ntcx, const double* tcx, const qol_int* tcxrow,
+                                const qol_int* tcxi, qol_int orderff, double distff, qol_int iside, qol_int nnz,
+                                qol_int* sparsei, qol_int* sparsej, double* sparsevs, double* sparsevd,
+                                void* stream, int sync, qol_int* level_hist) {
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  int rc = ensure_device();
+  if (rc) return rc;
+  cudaStream_t st = stream ? (cudaStream_t)stream : g_stream;
+  std::vector<long long> xi(npan + 1);
+  CK(cudaMemcpyAsync(xi.data(), tcxi, sizeof(long long) * (npan + 1), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if ((rc = validate_near(npan, nterms, hdim, nsrc, ntcx, xi.data(), nnz))) return rc;
+  if (npan == 0 || ntcx == 0) return 0;
+  Job J{};
+  J.npan = (int)npan; J.nterms = (int)nterms; J.nquad = (int)nquad; J.orderff = (int)orderff;
+  J.exterior = (iside % 10) == 0; J.subtract_naive = 1; J.distff = distff; J.ntcx = ntcx;
+  J.P = PanelIn{sx, snx, sw, rts, rps};
+  J.Q = PairIn{tcx, (const long long*)tcxrow, (const long long*)tcxi};
+  J.vs = sparsevs; J.vd = sparsevd; J.si = (long long*)sparsei; J.sj = (long long*)sparsej;
+  J.tcxi_host = xi.data();
+  rc = run_pipeline(J, st, nullptr, level_hist, nullptr, nullptr);
+  if (rc) return rc;
+  if (sync) CK(cudaStreamSynchronize(st));
+  return 0;
+}
+
+int qol_getnearquad_lap_rrq(qol_int npan, qol_int nterms, qol_int hdim, qol_int nquad, qol_int nsrc, const double* sx,
+                            const double* snx, const double* sw, const double* rts, const double* rps, qol_int ntcx,
+                            const double* tcx, const qol_int* tcxrow, const qol_int* tcxi, qol_int orderff,
+                            double distff, qol_int iside, qol_int isimd, qol_int nnz, qol_int* sparsei,
+                            qol_int* sparsej, double* sparsevs, double* sparsevd, double* timeinfo) {
+  (void)isimd;
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  if (!sx || !snx || !sw || !rts || !rps || !tcxi || (ntcx > 0 && (!tcx || !tcxrow)))
+    return fail(QOL_ERR_ARG, "null argument");
+  int rc = validate_near(npan, nterms, hdim, nsrc, ntcx, tcxi, nnz);
+  if (rc) return rc;
+  if ((rc = ensure_device())) return rc;
+  if (npan == 0 || ntcx == 0) return 0;
+  cudaStream_t st = g_stream;
+  /* device copies live in a dedicated allocation (the pipeline owns the arena) */
+  const size_t nout = (size_t)ntcx * hdim;
+  size_t bytes = sizeof(double) * (size_t)(nsrc * 13 + ntcx * 3) + sizeof(long long) * (ntcx + npan + 1) +
+                 (sizeof(double) * 2 + sizeof(long long) * 2) * nout + 16 * 256;
+  char* buf = nullptr;
+  if (cudaMalloc(&buf, bytes) != cudaSuccess) { cudaGetLastError(); return fail(QOL_ERR_CUDA, "device allocation failed"); }
+  size_t used = 0;
+  auto take = [&](size_t b) { size_t o = (used + 255) & ~(size_t)255; used = o + b; return buf + o; };
+  double* dsx = (double*)take(sizeof(double) * 3 * nsrc);
+  double* dsnx = (double*)take(sizeof(double) * 3 * nsrc);
+  double* dsw = (double*)take(sizeof(double) * nsrc);
+  double* drts = (double*)take(sizeof(double) * 3 * nsrc);
+  double* drps = (double*)take(sizeof(double) * 3 * nsrc);
+  double* dtcx = (double*)take(sizeof(double) * 3 * ntcx);
+  long long* drow = (long long*)take(sizeof(long long) * ntcx);
+  long long* dxi = (long long*)take(sizeof(long long) * (npan + 1));
+  double* dvs = (double*)take(sizeof(double) * nout);
+  double* dvd = (double*)take(sizeof(double) * nout);
+  long long* dsi = (long long*)take(sizeof(long long) * nout);
+  long long* dsj = (long long*)take(sizeof(long long) * nout);
+  int out = 0;
+  do {
+#define CKB(x)                                                                        \
+  {                                                                                   \
+    cudaError_t e_ = (x);                                                             \
+    if (e_ != cudaSuccess) { out = fail(QOL_ERR_CUDA, "%s: %s", #x, cudaGetErrorString(e_)); break; } \
+  }
+    CKB(cudaMemcpyAsync(dsx, sx, sizeof(double) * 3 * nsrc, cudaMemcpyHostToDevice, st));
+    CKB(cudaMemcpyAsync(dsnx, snx, sizeof(double) * 3 * nsrc, cudaMemcpyHostToDevice, st));
+    CKB(cudaMemcpyAsync(dsw, sw, sizeof(double) * nsrc, cudaMemcpyHostToDevice, st));
+    CKB(cudaMemcpyAsync(drts, rts, sizeof(double) * 3 * nsrc, cudaMemcpyHostToDevice, st));
+    CKB(cudaMemcpyAsync(drps, rps, sizeof(double) * 3 * nsrc, cudaMemcpyHostToDevice, st));
+    CKB(cudaMemcpyAsync(dtcx, tcx, sizeof(double) * 3 * ntcx, cudaMemcpyHostToDevice, st));
+    CKB(cudaMemcpyAsync(drow, tcxrow, sizeof(long long) * ntcx, cudaMemcpyHostToDevice, st));
+    CKB(cudaMemcpyAsync(dxi, tcxi, sizeof(long long) * (npan + 1), cudaMemcpyHostToDevice, st));
+    Job J{};
+    J.npan = (int)npan; J.nterms = (int)nterms; J.nquad = (int)nquad; J.orderff = (int)orderff;
+    J.exterior = (iside % 10) == 0; J.subtract_naive = 1; J.distff = distff; J.ntcx = ntcx;
+    J.P = PanelIn{dsx, dsnx, dsw, drts, drps};
+    J.Q = PairIn{dtcx, drow, dxi};
+    J.vs = dvs; J.vd = dvd; J.si = dsi; J.sj = dsj;
+    J.tcxi_host = (const long long*)tcxi;
+    out = run_pipeline(J, st, timeinfo, nullptr, nullptr, nullptr);
+    if (out) break;
+    CKB(cudaMemcpyAsync(sparsevs, dvs, sizeof(double) * nout, cudaMemcpyDeviceToHost, st));
+    CKB(cudaMemcpyAsync(sparsevd, dvd, sizeof(double) * nout, cudaMemcpyDeviceToHost, st));
+    CKB(cudaMemcpyAsync(sparsei, dsi, sizeof(long long) * nout, cudaMemcpyDeviceToHost, st));
+    CKB(cudaMemcpyAsync(sparsej, dsj, sizeof(long long) * nout, cudaMemcpyDeviceToHost, st));
+    CKB(cudaStreamSynchronize(st));
+#undef CKB
+  } while (0);
+  cudaFree(buf);
+  return out;
+}
+
+int qol_rrq(qol_int m, const double* tx, qol_int n, const double* sx, const double* snx, const double* sw,
+            const double* rts, const double* rps, qol_int order, qol_int nquad, qol_int orderff, double distff,
+            qol_int exterior, qol_int isimd, qol_int ichart, const double* sxbd_chart, const double* rv_chart,
+            const double* tgl, const double* wgl, const double* Dgl, const double* w_bclag, const double* Legmat,
+            const double* umatr, const double* vmatr, double* As, double* Ad, double* Omega,
+            double* IalphaAsvestas, double* timeinfo) {
+  (void)isimd; (void)Dgl; (void)w_bclag; (void)Legmat; (void)vmatr;
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  const qol_int hd = order * (order + 1) / 2;
+  if (n != hd) return fail(QOL_ERR_NPOLS, "n must equal order*(order+1)/2");
+  if (m < 0 || !sx || !snx || !sw || !rts || !rps || (m > 0 && (!tx || !As || !Ad)))
+    return fail(QOL_ERR_ARG, "bad arguments");
+  if (tgl && wgl && !tables_match((int)nquad, (int)order - 1, tgl, wgl, umatr))
+    return fail(QOL_ERR_TABLES, "precomputed tables differ from qol_simplex_precomp's");
+  int rc = ensure_device();
+  if (rc) return rc;
+  if (m == 0) return 0;
+  cudaStream_t st = g_stream;
+  const int nbd = 3 * (int)nquad;
+  size_t bytes = sizeof(double) * (size_t)(13 * n + 3 * m + 2 * m * n + 4 * hd * m + m + 3 * (nbd + 3)) +
+                 sizeof(long long) * (m + 2) + 16 * 256;
+  char* buf = nullptr;
+  if (cudaMalloc(&buf, bytes) != cudaSuccess) { cudaGetLastError(); return fail(QOL_ERR_CUDA, "device allocation failed"); }
+  size_t used = 0;
+  auto take = [&](size_t b) { size_t o = (used + 255) & ~(size_t)255; used = o + b; return buf + o; };
+  double* dsx = (double*)take(sizeof(double) * 3 * n);
+  double* dsnx = (double*)take(sizeof(double) * 3 * n);
+  double* dsw = (double*)take(sizeof(double) * n);
+  double* drts = (double*)take(sizeof(double) * 3 * n);
+  double* drps = (double*)take(sizeof(double) * 3 * n);
+  double* dtx = (double*)take(sizeof(double) * 3 * m);
+  double* dAs = (double*)take(sizeof(double) * m * n);
+  double* dAd = (double*)take(sizeof(double) * m * n);
+  double* dOm = (double*)take(sizeof(double) * 4 * hd * m);
+  double* dIa = (double*)take(sizeof(double) * m);
+  double* dch = (double*)take(sizeof(double) * 3 * (nbd + 3));
+  long long* drow = (long long*)take(sizeof(long long) * m);
+  long long* dxi = (long long*)take(sizeof(long long) * 2);
+  std::vector<long long> xi = {1, m + 1};
+  std::vector<double> chart;
+  if (ichart == 1) {
+    if (!sxbd_chart || !rv_chart) { cudaFree(buf); return fail(QOL_ERR_ARG, "ichart = 1 needs sxbd_chart and rv_chart"); }
+    chart.assign(sxbd_chart, sxbd_chart + 3 * nbd);
+    chart.insert(chart.end(), rv_chart, rv_chart + 9);
+  }
+  int out = 0;
+  do {
+#define CKB(x)                                                                        \
+  {                                                                                   \
+    cudaError_t e_ = (x);                                                             \
+    if (e_ != cudaSuccess) { out = fail(QOL_ERR_CUDA, "%s: %s", #x, cudaGetErrorString(e_)); break; } \
+  }
+    CKB(cudaMemcpyAsync(dsx, sx, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st));
+    CKB(cudaMemcpyAsync(dsnx, snx, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st));
+    CKB(cudaMemcpyAsync(dsw, sw, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+    CKB(cudaMemcpyAsync(drts, rts, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st));
+    CKB(cudaMemcpyAsync(drps, rps, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st));
+    CKB(cudaMemcpyAsync(dtx, tx, sizeof(double) * 3 * m, cudaMemcpyHostToDevice, st));
+    CKB(cudaMemsetAsync(drow, 0, sizeof(long long) * m, st));
+    CKB(cudaMemcpyAsync(dxi, xi.data(), sizeof(long long) * 2, cudaMemcpyHostToDevice, st));
+    CKB(cudaMemsetAsync(dAs, 0, sizeof(double) * m * n, st));
+    CKB(cudaMemsetAsync(dAd, 0, sizeof(double) * m * n, st));
+    CKB(cudaMemsetAsync(dOm, 0, sizeof(double) * 4 * hd * m, st));
+    CKB(cudaMemsetAsync(dIa, 0, sizeof(double) * m, st));
+    if (ichart == 1) CKB(cudaMemcpyAsync(dch, chart.data(), sizeof(double) * chart.size(), cudaMemcpyHostToDevice, st));
+    Job J{};
+    J.npan = 1; J.nterms = (int)order; J.nquad = (int)nquad; J.orderff = (int)orderff;
+    J.exterior = exterior != 0; J.subtract_naive = 0; J.distff = distff; J.ntcx = m;
+    J.P = PanelIn{dsx, dsnx, dsw, drts, drps};
+    J.Q = PairIn{dtx, drow, dxi};
+    J.vs = dAs; J.vd = dAd; J.omega = dOm; J.ialpha = dIa; J.si = nullptr; J.sj = nullptr;
+    J.chart = ichart == 1 ? dch : nullptr;
+    J.tcxi_host = xi.data();
+    out = run_pipeline(J, st, timeinfo, nullptr, nullptr, nullptr);
+    if (out) break;
+    CKB(cudaMemcpyAsync(As, dAs, sizeof(double) * m * n, cudaMemcpyDeviceToHost, st));
+    CKB(cudaMemcpyAsync(Ad, dAd, sizeof(double) * m * n, cudaMemcpyDeviceToHost, st));
+    if (Omega) CKB(cudaMemcpyAsync(Omega, dOm, sizeof(double) * 4 * hd * m, cudaMemcpyDeviceToHost, st));
+    if (IalphaAsvestas) CKB(cudaMemcpyAsync(IalphaAsvestas, dIa, sizeof(double) * m, cudaMemcpyDeviceToHost, st));
+    CKB(cudaStreamSynchronize(st));
+#undef CKB
+  } while (0);
+  cudaFree(buf);
+  return out;
+}
+
+/* ---------------- reference-symbol aliases ---------------- */
+void qol_simplex_precomp_mex_(const qol_int* nquad, const qol_int* korder, const qol_int* kpols, double* tgl,
+                              double* wgl, double* Dgl, double* w_bclag, double* Legmat, double* umatr,
+                              double* vmatr) {
+  qol_simplex_precomp(*nquad, *korder, *kpols, tgl, wgl, Dgl, w_bclag, Legmat, umatr, vmatr);
+}
+void qol_build_patch_levels_mex_(const qol_int* korder, const qol_int* npols, const double* sx, const double* rts,
+                                 const double* rps, const qol_int* order, const double* dist, const qol_int* nlevel,
+                                 qol_int* lv, qol_int* ier) {
+  qol_build_patch_levels(*korder, *npols, sx, rts, rps, *order, *dist, *nlevel, lv, ier);
+}
+void qol_lap3dsdlpmat_levels_mex_(const qol_int* m, const double* tx, const qol_int* npols, const qol_int* lv,
+                                  const qol_int* isimd, double* As, double* Ad, qol_int* idxs, qol_int* ms,
+                                  qol_int* ier) {
+  qol_lap3dsdlpmat_levels(*m, tx, *npols, *lv, *isimd, As, Ad, idxs, ms, ier);
+}
+void qol_clear_patch_levels_mex_(const qol_int* lv, qol_int* ier) { qol_clear_patch_levels(*lv, ier); }
+void qol_clear_patch_levels_all_mex_(qol_int* ier) { qol_clear_patch_levels_all(ier); }
+void qol_getnearquad_lap_rrq_mex_(const qol_int* npan, const qol_int* nterms, const qol_int* hdim,
+                                  const qol_int* nquad, const qol_int* nsrc, const double* sx, const double* snx,
+                                  const double* sw, const double* rts, const double* rps, const qol_int* ntcx,
+                                  const double* tcx, const qol_int* tcxrow, const qol_int* tcxi,
+                                  const qol_int* orderff, const double* distff, const qol_int* iside,
+                                  const qol_int* isimd, const qol_int* nnz, qol_int* sparsei, qol_int* sparsej,
+                                  double* sparsevs, double* sparsevd, double* timeinfo) {
+  qol_getnearquad_lap_rrq(*npan, *nterms, *hdim, *nquad, *nsrc, sx, snx, sw, rts, rps, *ntcx, tcx, tcxrow, tcxi,
+                          *orderff, *distff, *iside, *isimd, *nnz, sparsei, sparsej, sparsevs, sparsevd, timeinfo);
+}
+void qol_rrq_mex_(const qol_int* m, const double* tx, const qol_int* n, const double* sx, const double* snx,
+                  const double* sw, const double* rts, const double* rps, const qol_int* order, const qol_int* nquad,
+                  const qol_int* orderff, const double* distff, const qol_int* exterior, const qol_int* isimd,
+                  const qol_int* ichart, const double* sxbd_chart, const double* rv_chart, const double* tgl,
+                  const double* wgl, const double* Dgl, const double* w_bclag, const double* Legmat,
+                  const double* umatr, const double* vmatr, double* As, double* Ad, double* Omega,
+                  double* IalphaAsvestas, double* timeinfo) {
+  qol_rrq(*m, tx, *n, sx, snx, sw, rts, rps, *order, *nquad, *orderff, *distff, *exterior, *isimd, *ichart,
+          sxbd_chart, rv_chart, tgl, wgl, Dgl, w_bclag, Legmat, umatr, vmatr, As, Ad, Omega, IalphaAsvestas,
+          timeinfo);
+}
+
+} // extern "C"

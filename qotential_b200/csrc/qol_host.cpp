@@ -1,0 +1,372 @@
+/* Host-side per-order tables of the library: Gauss-Legendre data, the
+ * Vioreanu-Rokhlin table, simplex interpolation and the reference-element
+ * refinement levels (src/patch_refine_mod.f90:100-421).  Built once per order
+ * on the host, uploaded to the device and cached. */
+#include "qol_host.h"
+#include "vr_table.h"
+#include <algorithm>
+#include <cfloat>
+#include <stdexcept>
+
+namespace qolh {
+
+int lu_factor(int n, double* A, int* piv) {
+  for (int k = 0; k < n; ++k) {
+    int p = k;
+    double pm = std::fabs(A[k + (size_t)k * n]);
+    for (int i = k + 1; i < n; ++i) {
+      double v = std::fabs(A[i + (size_t)k * n]);
+      if (v > pm) { pm = v; p = i; }
+    }
+    piv[k] = p;
+    if (pm == 0.0) return k + 1;
+    if (p != k)
+      for (int j = 0; j < n; ++j) std::swap(A[k + (size_t)j * n], A[p + (size_t)j * n]);
+    double inv = 1.0 / A[k + (size_t)k * n];
+    for (int i = k + 1; i < n; ++i) A[i + (size_t)k * n] *= inv;
+    for (int j = k + 1; j < n; ++j) {
+      double akj = A[k + (size_t)j * n];
+      if (akj == 0.0) continue;
+      double* cj = A + (size_t)j * n;
+      const double* ck = A + (size_t)k * n;
+      for (int i = k + 1; i < n; ++i) cj[i] -= ck[i] * akj;
+    }
+  }
+  return 0;
+}
+
+void lu_solve(int n, const double* LU, const int* piv, double* B, int nrhs) {
+  for (int r = 0; r < nrhs; ++r) {
+    double* b = B + (size_t)r * n;
+    for (int k = 0; k < n; ++k)
+      if (piv[k] != k) std::swap(b[k], b[piv[k]]);
+    for (int k = 0; k < n; ++k) {
+      double bk = b[k];
+      const double* ck = LU + (size_t)k * n;
+      for (int i = k + 1; i < n; ++i) b[i] -= ck[i] * bk;
+    }
+    for (int k = n - 1; k >= 0; --k) {
+      b[k] /= LU[k + (size_t)k * n];
+      double bk = b[k];
+      const double* ck = LU + (size_t)k * n;
+      for (int i = 0; i < k; ++i) b[i] -= ck[i] * bk;
+    }
+  }
+}
+
+/* utils/gauss.m:1-37: Legendre-Gauss nodes by the (damped) Newton iteration
+ * of lgwt.m with its initial guess, weights, and Fornberg's differentiation
+ * matrix.  Nodes are returned ascending (x = y(end:-1:1)); the weights keep
+ * the iteration's order, as gauss.m does (they are symmetric). */
+void gauss(int N, double* x, double* w, double* D) {
+  if (N == 1) {
+    x[0] = 0.0; w[0] = 2.0;
+    if (D) D[0] = 0.0;
+    return;
+  }
+  int n = N - 1, N1 = n + 1, N2 = n + 2;
+  std::vector<double> y(N1), y0(N1, 2.0), L((size_t)N1 * N2), Lp(N1);
+  for (int k = 0; k <= n; ++k) {
+    double xu = -1.0 + 2.0 * k / (double)n;
+    y[k] = std::cos((2.0 * k + 1.0) * PI / (2.0 * n + 2.0)) +
+           (0.27 / N1) * std::sin(PI * xu * n / N2);
+  }
+  const double eps = DBL_EPSILON;
+  for (int it = 0; it < 1000; ++it) {
+    double md = 0.0;
+    for (int k = 0; k < N1; ++k) md = std::max(md, std::fabs(y[k] - y0[k]));
+    if (!(md > eps)) break;
+    for (int i = 0; i < N1; ++i) {
+      L[i] = 1.0;
+      L[i + (size_t)N1] = y[i];
+    }
+    for (int k = 2; k <= N1; ++k)
+      for (int i = 0; i < N1; ++i)
+        L[i + (size_t)k * N1] = ((2.0 * k - 1.0) * y[i] * L[i + (size_t)(k - 1) * N1] -
+                                 (k - 1.0) * L[i + (size_t)(k - 2) * N1]) / k;
+    for (int i = 0; i < N1; ++i)
+      Lp[i] = N2 * (L[i + (size_t)(N1 - 1) * N1] - y[i] * L[i + (size_t)(N2 - 1) * N1]) /
+              (1.0 - y[i] * y[i]);
+    for (int i = 0; i < N1; ++i) {
+      y0[i] = y[i];
+      y[i] = y0[i] - L[i + (size_t)(N2 - 1) * N1] / Lp[i];
+    }
+  }
+  for (int i = 0; i < N1; ++i) {
+    x[i] = y[N1 - 1 - i];
+    w[i] = 2.0 / ((1.0 - y[i] * y[i]) * Lp[i] * Lp[i]) * ((double)N2 / N1) * ((double)N2 / N1);
+  }
+  if (D) {
+    std::vector<double> a(N);
+    for (int k = 0; k < N; ++k) {
+      double p = 1.0;
+      for (int i = 0; i < N; ++i)
+        if (i != k) p *= (x[k] - x[i]);
+      a[k] = p;
+    }
+    for (int k = 0; k < N; ++k) {
+      double s = 0.0;
+      for (int i = 0; i < N; ++i) {
+        if (i == k) continue;
+        D[i + (size_t)k * N] = (a[i] / a[k]) / (x[i] - x[k]);
+        s += 1.0 / (x[k] - x[i]);
+      }
+      D[k + (size_t)k * N] = s;
+    }
+  }
+}
+
+void bary_weights(int n, const double* x, double* wb) {
+  for (int j = 0; j < n; ++j) {
+    double p = 1.0;
+    for (int k = 0; k < n; ++k)
+      if (k != j) p *= (x[j] - x[k]);
+    wb[j] = 1.0 / p;
+  }
+}
+
+void legendre_vals2coefs(int n, const double* x, const double* w, double* U) {
+  for (int i = 0; i < n; ++i) {
+    double p0 = 1.0, p1 = x[i];
+    for (int k = 0; k < n; ++k) {
+      double pk;
+      if (k == 0) pk = 1.0;
+      else if (k == 1) pk = x[i];
+      else {
+        pk = ((2.0 * k - 1.0) * x[i] * p1 - (k - 1.0) * p0) / k;
+        p0 = p1; p1 = pk;
+      }
+      U[k + (size_t)i * n] = (2.0 * k + 1.0) / 2.0 * w[i] * pk;
+    }
+  }
+}
+
+int npols_of(int korder) { return (korder + 1) * (korder + 2) / 2; }
+
+/* Orthogonal polynomials on the simplex in collapsed coordinates:
+ * P_{a,b}(u,v) = L_a(2u+v-1, 1-v) * P_b^{(2a+1,0)}(2v-1), where
+ * L_a(s,t) = t^a P_a(s/t) is the homogenised Legendre polynomial.  Ordered by
+ * total degree a+b, then b.  Any basis of the degree-korder polynomials gives
+ * the same interpolation matrix pols*umatr; this one is well conditioned. */
+void koorn_pols(double u, double v, int korder, double* pols) {
+  double s = 2.0 * u + v - 1.0, t = 1.0 - v, z = 2.0 * v - 1.0;
+  double La[64];
+  La[0] = 1.0;
+  if (korder >= 1) La[1] = s;
+  for (int a = 1; a < korder; ++a)
+    La[a + 1] = ((2.0 * a + 1.0) * s * La[a] - a * t * t * La[a - 1]) / (a + 1.0);
+  int idx = 0;
+  for (int deg = 0; deg <= korder; ++deg) {
+    for (int b = 0; b <= deg; ++b) {
+      int a = deg - b;
+      double alpha = 2.0 * a + 1.0;
+      /* Jacobi P_b^{(alpha,0)}(z) */
+      double p0 = 1.0, p1 = 0.5 * (alpha + 2.0) * z + 0.5 * alpha, pb;
+      if (b == 0) pb = p0;
+      else if (b == 1) pb = p1;
+      else {
+        for (int j = 1; j < b; ++j) {
+          double jj = j + 1.0; /* computing P_{j+1} */
+          double c1 = 2.0 * jj * (jj + alpha) * (2.0 * jj + alpha - 2.0);
+          double c2 = (2.0 * jj + alpha - 1.0) * (alpha * alpha);
+          double c3 = (2.0 * jj + alpha - 2.0) * (2.0 * jj + alpha - 1.0) * (2.0 * jj + alpha);
+          double c4 = 2.0 * (jj + alpha - 1.0) * (jj - 1.0) * (2.0 * jj + alpha);
+          double p2 = ((c2 + c3 * z) * p1 - c4 * p0) / c1;
+          p0 = p1; p1 = p2;
+        }
+        pb = p1;
+      }
+      pols[idx++] = La[a] * pb;
+    }
+  }
+}
+
+void vr_nodes(int deg, double* uv, double* w) {
+  if (deg < 0 || deg > QOL_VR_MAXDEG) throw std::runtime_error("VR degree out of table");
+  int o = qol_vr_offset[deg], n = qol_vr_offset[deg + 1] - o;
+  for (int i = 0; i < n; ++i) {
+    if (uv) { uv[2 * i] = qol_vr_uv[2 * (o + i)]; uv[2 * i + 1] = qol_vr_uv[2 * (o + i) + 1]; }
+    if (w) w[i] = qol_vr_w[o + i];
+  }
+}
+
+void koorn_umatr(int korder, double* umatr, double* vmatr) {
+  int np = npols_of(korder);
+  std::vector<double> uv(2 * np), V((size_t)np * np), p(np);
+  vr_nodes(korder, uv.data(), nullptr);
+  for (int i = 0; i < np; ++i) {
+    koorn_pols(uv[2 * i], uv[2 * i + 1], korder, p.data());
+    for (int k = 0; k < np; ++k) V[i + (size_t)k * np] = p[k];
+  }
+  if (vmatr) std::copy(V.begin(), V.end(), vmatr);
+  std::vector<int> piv(np);
+  std::vector<double> I((size_t)np * np, 0.0);
+  for (int i = 0; i < np; ++i) I[i + (size_t)i * np] = 1.0;
+  if (lu_factor(np, V.data(), piv.data())) throw std::runtime_error("singular VR vandermonde");
+  lu_solve(np, V.data(), piv.data(), I.data(), np);
+  std::copy(I.begin(), I.end(), umatr);
+}
+
+void interp_matrix(int korder, int n, const double* uv, double* M) {
+  int np = npols_of(korder);
+  std::vector<double> um((size_t)np * np), p(np);
+  koorn_umatr(korder, um.data(), nullptr);
+  for (int i = 0; i < n; ++i) {
+    koorn_pols(uv[2 * i], uv[2 * i + 1], korder, p.data());
+    for (int j = 0; j < np; ++j) {
+      double s = 0.0;
+      for (int k = 0; k < np; ++k) s += p[k] * um[k + (size_t)j * np];
+      M[i + (size_t)j * n] = s;
+    }
+  }
+}
+
+/* cc_subidx_at (patch_refine_mod.f90:264-311): which of the 64 level-4
+ * sub-triangles the cc level keeps (1-based). */
+static const int CC_SUBIDX[39] = {1,  2,  3,  4,  7,  8,  9,  10, 11, 13, 14, 16, 17,
+                                  27, 32, 33, 34, 35, 37, 40, 41, 42, 43, 44, 46, 47,
+                                  48, 49, 50, 52, 53, 55, 58, 59, 60, 61, 62, 63, 64};
+static const int CC_NSUB = 39;
+static const double CC_EXTRA_SCALE = 0.625, CC_EXTRA_OFFSET = 0.4375;
+
+/* ref_square_regroup (patch_refine_mod.f90:313-421) */
+static void square_regroup(RefElem& R, int ilev, i8 n1, int korder, bool is_cc) {
+  RefLevel& L = R.lev[ilev - 1];
+  i8 nsub_old = L.nsub, npairable = nsub_old, ncell;
+  if (is_cc) { npairable = nsub_old - 4; ncell = 8; }
+  else ncell = (i8)1 << (ilev - 1);
+  double side = 1.0 / (double)ncell;
+  int qg = korder + 1;
+  if (qg < 8) qg = korder + 3;
+  double fac = 0.0;
+  for (double wv : R.lev[0].wt) fac += wv;
+  fac *= 2.0;
+  std::vector<double> uv_old = L.uv, wt_old = L.wt;
+  std::vector<i8> cellcnt((size_t)ncell * ncell, 0), singles;
+  auto cell_of = [&](i8 q, i8& ic, i8& jc) {
+    i8 i0 = (q - 1) * n1;
+    double cu = 0.0, cv = 0.0;
+    for (i8 i = 0; i < n1; ++i) cu += uv_old[2 * (i0 + i)];
+    for (i8 i = 0; i < n1; ++i) cv += uv_old[2 * (i0 + i) + 1];
+    cu /= (double)n1; cv /= (double)n1;
+    ic = std::min(std::max((i8)(cu / side), (i8)0), ncell - 1);
+    jc = std::min(std::max((i8)(cv / side), (i8)0), ncell - 1);
+  };
+  for (i8 q = 1; q <= npairable; ++q) {
+    i8 ic, jc; cell_of(q, ic, jc);
+    if (++cellcnt[ic + ncell * jc] > 2) throw std::runtime_error("square regroup: >2 in a cell");
+  }
+  for (i8 q = 1; q <= npairable; ++q) {
+    i8 ic, jc; cell_of(q, ic, jc);
+    if (cellcnt[ic + ncell * jc] == 1) singles.push_back(q);
+  }
+  for (i8 q = npairable + 1; q <= nsub_old; ++q) singles.push_back(q);
+  i8 npair = 0;
+  for (i8 c = 0; c < ncell * ncell; ++c) if (cellcnt[c] == 2) ++npair;
+  i8 nsingle = (i8)singles.size();
+  i8 n = npair * qg * qg + nsingle * n1, nsub = npair + nsingle;
+  L.uv.assign(2 * n, 0.0); L.wt.assign(n, 0.0);
+  L.suboff.assign(nsub + 1, 0); L.subtyp.assign(nsub, 0);
+  for (i8 k = 0; k < npair; ++k) L.subtyp[k] = 1;
+  std::vector<double> tq(qg), wq(qg);
+  gauss(qg, tq.data(), wq.data(), nullptr);
+  std::vector<double> u01(qg), w01(qg);
+  for (int i = 0; i < qg; ++i) { u01[i] = 0.5 * (tq[i] + 1.0); w01[i] = 0.5 * wq[i]; }
+  i8 row = 0, k = 0;
+  for (i8 jc = 0; jc < ncell; ++jc)
+    for (i8 ic = 0; ic < ncell; ++ic) {
+      if (cellcnt[ic + ncell * jc] != 2) continue;
+      for (int j = 0; j < qg; ++j)
+        for (int i = 0; i < qg; ++i) {
+          L.uv[2 * row] = ((double)ic + u01[i]) * side;
+          L.uv[2 * row + 1] = ((double)jc + u01[j]) * side;
+          L.wt[row] = w01[i] * w01[j] * side * side * fac;
+          ++row;
+        }
+      ++k; L.suboff[k] = row;
+    }
+  for (i8 s = 0; s < nsingle; ++s) {
+    i8 i0 = (singles[s] - 1) * n1;
+    for (i8 j = 0; j < n1; ++j) {
+      L.uv[2 * row] = uv_old[2 * (i0 + j)];
+      L.uv[2 * row + 1] = uv_old[2 * (i0 + j) + 1];
+      L.wt[row] = wt_old[i0 + j];
+      ++row;
+    }
+    ++k; L.suboff[k] = row;
+  }
+  L.n = n; L.nsub = nsub;
+}
+
+/* 4-way split of a level's node set (patch_refine_mod.f90:216-240):
+ * copies (u0,v0), (-u0,-v0), (u0,v0+2), (u0+2,v0) of uv0 = 2uv-1, then mapped
+ * by ((x-1)/2+1)/2, each weight quartered. */
+static void split4(const std::vector<double>& uvp, const std::vector<double>& wtp,
+                   std::vector<double>& uv, std::vector<double>& wt) {
+  i8 np = (i8)wtp.size();
+  uv.assign(8 * np, 0.0); wt.assign(4 * np, 0.0);
+  for (i8 i = 0; i < np; ++i) {
+    double u0 = 2.0 * uvp[2 * i] - 1.0, v0 = 2.0 * uvp[2 * i + 1] - 1.0;
+    double cu[4] = {u0, -u0, u0, u0 + 2.0}, cv[4] = {v0, -v0, v0 + 2.0, v0};
+    for (int b = 0; b < 4; ++b) {
+      uv[2 * (b * np + i)] = cu[b];
+      uv[2 * (b * np + i) + 1] = cv[b];
+      wt[b * np + i] = 0.25 * wtp[i];
+    }
+  }
+  for (i8 i = 0; i < 4 * np; ++i) {
+    uv[2 * i] = ((uv[2 * i] - 1.0) * 0.5 + 1.0) * 0.5;
+    uv[2 * i + 1] = ((uv[2 * i + 1] - 1.0) * 0.5 + 1.0) * 0.5;
+  }
+}
+
+void build_ref(int korder, int order, int nlevel, bool sqmode, RefElem& R) {
+  int npols = npols_of(korder);
+  R.korder = korder; R.npols = npols; R.order = order; R.nlevel = nlevel; R.sqmode = sqmode;
+  R.lev.assign(nlevel, RefLevel());
+  i8 n1 = (i8)order * (order + 1) / 2;
+  for (int ilev = 1; ilev <= nlevel; ++ilev) {
+    RefLevel& L = R.lev[ilev - 1];
+    if (ilev == 1) {
+      L.uv.assign(2 * n1, 0.0); L.wt.assign(n1, 0.0);
+      vr_nodes(order - 1, L.uv.data(), L.wt.data());
+      L.n = n1; L.nsub = 1;
+    } else if (ilev == nlevel && nlevel == 4) {
+      std::vector<double> uvt, wtt;
+      split4(R.lev[ilev - 2].uv, R.lev[ilev - 2].wt, uvt, wtt);
+      i8 ncc = CC_NSUB + 4;
+      L.n = ncc * n1; L.nsub = ncc;
+      L.uv.assign(2 * L.n, 0.0); L.wt.assign(L.n, 0.0);
+      for (int q = 1; q <= CC_NSUB; ++q)
+        for (i8 i = 1; i <= n1; ++i) {
+          i8 isrc = (CC_SUBIDX[q - 1] - 1) * n1 + i - 1, idst = (q - 1) * n1 + i - 1;
+          L.uv[2 * idst] = uvt[2 * isrc]; L.uv[2 * idst + 1] = uvt[2 * isrc + 1];
+          L.wt[idst] = wtt[isrc];
+        }
+      const RefLevel& L2 = R.lev[1];
+      for (int q = 1; q <= 4; ++q)
+        for (i8 i = 1; i <= n1; ++i) {
+          i8 isrc = (q - 1) * n1 + i - 1, idst = (CC_NSUB + q - 1) * n1 + i - 1;
+          L.uv[2 * idst] = (L2.uv[2 * isrc] - 0.5) * CC_EXTRA_SCALE + CC_EXTRA_OFFSET;
+          L.uv[2 * idst + 1] = (L2.uv[2 * isrc + 1] - 0.5) * CC_EXTRA_SCALE + CC_EXTRA_OFFSET;
+          L.wt[idst] = CC_EXTRA_SCALE * CC_EXTRA_SCALE * L2.wt[isrc];
+        }
+    } else {
+      split4(R.lev[ilev - 2].uv, R.lev[ilev - 2].wt, L.uv, L.wt);
+      L.n = 4 * R.lev[ilev - 2].n; L.nsub = 4 * R.lev[ilev - 2].nsub;
+    }
+  }
+  for (int ilev = 1; ilev <= nlevel; ++ilev) {
+    RefLevel& L = R.lev[ilev - 1];
+    if (sqmode && ilev >= 2) {
+      square_regroup(R, ilev, n1, korder, ilev == nlevel && nlevel == 4);
+    } else {
+      L.suboff.assign(L.nsub + 1, 0); L.subtyp.assign(L.nsub, 0);
+      for (i8 i = 0; i <= L.nsub; ++i) L.suboff[i] = i * n1;
+    }
+    L.interp.assign((size_t)L.n * npols, 0.0);
+    interp_matrix(korder, (int)L.n, L.uv.data(), L.interp.data());
+  }
+}
+
+} // namespace qolh

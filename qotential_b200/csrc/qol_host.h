@@ -1,0 +1,59 @@
+/* Host-side tables for the qol_b200 library (see qol_host.cpp). */
+#ifndef QOL_HOST_H
+#define QOL_HOST_H
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+namespace qolh {
+typedef long long i8;
+typedef std::complex<double> cplx;
+static const double PI = 3.14159265358979323846264338327950288;
+
+/* ---------------- small dense helpers ---------------- */
+/* LU with partial pivoting, in place, column-major n x n; returns 0 if ok. */
+int lu_factor(int n, double* A, int* piv);
+/* Solve A X = B with the factors from lu_factor, B is n x nrhs column-major. */
+void lu_solve(int n, const double* LU, const int* piv, double* B, int nrhs);
+
+/* ---------------- 1D tables ---------------- */
+/* Gauss-Legendre on [-1,1] (utils/gauss.m:1-37 restated): nodes ascending,
+ * weights, and the spectral differentiation matrix D (n x n col-major, may be
+ * null). */
+void gauss(int n, double* x, double* w, double* D);
+/* barycentric Lagrange weights 1/prod_{k!=j}(x_j-x_k) */
+void bary_weights(int n, const double* x, double* wb);
+/* Legendre values->coefficients matrix U(k,i) = (2k+1)/2 w_i P_k(x_i) */
+void legendre_vals2coefs(int n, const double* x, const double* w, double* U);
+
+/* ---------------- simplex interpolation ---------------- */
+int npols_of(int korder);
+/* orthogonal (Koornwinder/Dubiner) polynomials on the simplex
+ * (0,0),(1,0),(0,1), total degree <= korder; pols[npols] */
+void koorn_pols(double u, double v, int korder, double* pols);
+/* VR nodes (2 x npts) and weights of degree deg */
+void vr_nodes(int deg, double* uv, double* w);
+/* umatr (vals->coefs) and vmatr (coefs->vals) at the VR nodes of degree korder */
+void koorn_umatr(int korder, double* umatr, double* vmatr);
+/* interpolation matrix n x npols from VR(korder) nodes to points uv */
+void interp_matrix(int korder, int n, const double* uv, double* M);
+
+/* ---------------- reference element levels ---------------- */
+struct RefLevel {
+  i8 n = 0, nsub = 0;
+  std::vector<double> uv, wt, interp; /* interp n x npols col-major */
+  std::vector<i8> suboff, subtyp;
+};
+struct RefElem {
+  int korder = -1, npols = -1, order = -1, nlevel = -1;
+  bool sqmode = true;
+  std::vector<RefLevel> lev;
+};
+/* build_patch_ref_r64 + ref_square_regroup + cc_subidx_at
+ * (src/patch_refine_mod.f90:100-262, 264-311, 313-421) */
+void build_ref(int korder, int order, int nlevel, bool sqmode, RefElem& R);
+
+} // namespace qolh
+#endif

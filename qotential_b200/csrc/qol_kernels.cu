@@ -1,0 +1,995 @@
+/* qol_b200 kernels: the RRQ near-field hot path on sm_100a, FP64.
+ *
+ *   k_panel_levels   build_patch_levels_r64 (patch_refine_mod.f90:423-502)
+ *   k_classify       ball tests of lap3dsdlpmat_levels_r64 (:516-551)
+ *   k_direct         level kernel sums fused with the interpmat contraction
+ *                    (:553-600) and the naive-block subtraction of
+ *                    getnearquad_lap_rrq_r64 (lap3d_close_mod.f90:935-956)
+ *   k_rrq_panel      per-panel RRQ precompute (lap3d_close_mod.f90:472-620,
+ *                    843-863): frame, boundary, harmonic basis, inverse of the
+ *                    quaternion system and of the S system
+ *   k_rrq_target     per-pair RRQ moments (:789-841), one warp per pair
+ *   k_rrq_apply      the two solves as per-panel matrix products (:843-870)
+ *   k_coo_index      COO row/column indices (:948-956)
+ */
+#include "qol_dev.cuh"
+#include "qol_kernels.h"
+
+__constant__ double c_hb[QOL_MAXL + 2][QOL_MAXL + 2]; /* sqrt((l+m-1)(l-m-1)) */
+__constant__ double c_hc[QOL_MAXL + 2][QOL_MAXL + 2]; /* 1/sqrt((l-m)(l+m)) */
+__constant__ double c_hcm[QOL_MAXL + 2];               /* sqrt((2m-1)/(2m)) */
+
+void qol_upload_harm_coefs(const double* hb, const double* hc, const double* hcm, cudaStream_t st) {
+  cudaMemcpyToSymbolAsync(c_hb, hb, sizeof(double) * (QOL_MAXL + 2) * (QOL_MAXL + 2), 0,
+                          cudaMemcpyHostToDevice, st);
+  cudaMemcpyToSymbolAsync(c_hc, hc, sizeof(double) * (QOL_MAXL + 2) * (QOL_MAXL + 2), 0,
+                          cudaMemcpyHostToDevice, st);
+  cudaMemcpyToSymbolAsync(c_hcm, hcm, sizeof(double) * (QOL_MAXL + 2), 0, cudaMemcpyHostToDevice, st);
+}
+
+/* ===================================================================== */
+/* K1: refined levels of every panel                                     */
+/* ===================================================================== */
+__global__ void __launch_bounds__(256) k_panel_levels(OrderTab T, PanelIn P, LevelWS W) {
+  const int pan = blockIdx.x, hd = T.hd;
+  extern __shared__ double sm[];
+  double* src = sm; /* hd x 9 */
+  for (int e = threadIdx.x; e < hd * 3; e += blockDim.x) {
+    int j = e / 3, d = e % 3;
+    size_t g = (size_t)pan * hd + j;
+    src[j * 9 + d] = P.sx[3 * g + d];
+    src[j * 9 + 3 + d] = P.rts[3 * g + d];
+    src[j * 9 + 6 + d] = P.rps[3 * g + d];
+  }
+  __syncthreads();
+  for (int l = 0; l < T.nlevel; ++l) {
+    const int n = T.n[l];
+    const double* I = T.interp[l];
+    double* base = W.node[l] + (size_t)pan * n * 7;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      double g[9];
+#pragma unroll
+      for (int c = 0; c < 9; ++c) g[c] = 0.0;
+      for (int k = 0; k < hd; ++k) {
+        double a = I[(size_t)i * hd + k];
+#pragma unroll
+        for (int c = 0; c < 9; ++c) g[c] += a * src[k * 9 + c];
+      }
+      double nx = g[7] * g[5] - g[8] * g[4];
+      double ny = g[8] * g[3] - g[6] * g[5];
+      double nz = g[6] * g[4] - g[7] * g[3];
+      double sp = sqrt(nx * nx + ny * ny + nz * nz);
+      base[0 * n + i] = g[0];
+      base[1 * n + i] = g[1];
+      base[2 * n + i] = g[2];
+      base[3 * n + i] = nx / sp;
+      base[4 * n + i] = ny / sp;
+      base[5 * n + i] = nz / sp;
+      base[6 * n + i] = sp * T.wt[l][i];
+    }
+    __syncthreads();
+    /* sub-patch centroids and squared near radii, sequential per sub-patch */
+    const int ns = T.nsub[l];
+    for (int s = threadIdx.x; s < ns; s += blockDim.x) {
+      long long i0 = T.suboff[l][s], i1 = T.suboff[l][s + 1];
+      double swsum = 0.0, q[3];
+      for (long long i = i0; i < i1; ++i) swsum += base[6 * n + i];
+      for (int d = 0; d < 3; ++d) {
+        double acc = 0.0;
+        for (long long i = i0; i < i1; ++i) acc += base[d * n + i] * base[6 * n + i];
+        q[d] = acc / swsum;
+      }
+      double rmax2 = 0.0;
+      for (long long i = i0; i < i1; ++i) {
+        double d2 = 0.0;
+        for (int d = 0; d < 3; ++d) {
+          double t = base[d * n + i] - q[d];
+          d2 += t * t;
+        }
+        rmax2 = fmax(rmax2, d2);
+      }
+      double* qp = W.sub[l] + ((size_t)pan * ns + s) * 4;
+      qp[0] = q[0]; qp[1] = q[1]; qp[2] = q[2];
+      double d2 = T.dist * T.dist;
+      qp[3] = (T.subtyp[l][s] == 1) ? d2 * fmax(rmax2, 0.5 * swsum) : d2 * fmax(rmax2, swsum);
+    }
+    __syncthreads();
+  }
+}
+
+/* ===================================================================== */
+/* K2: level of every (target, panel) pair, grouped per panel by level   */
+/* ===================================================================== */
+__global__ void __launch_bounds__(128) k_classify(OrderTab T, PairIn Q, LevelWS W, PairWS G) {
+  const int pan = blockIdx.x;
+  const long long p0 = Q.tcxi[pan] - 1, m = Q.tcxi[pan + 1] - Q.tcxi[pan];
+  __shared__ int cnt[8], warpc[4][8];
+  __shared__ int base_l[8];
+  if (threadIdx.x < 8) cnt[threadIdx.x] = 0;
+  __syncthreads();
+  /* pass 1: counts per level */
+  for (long long t0 = 0; t0 < m; t0 += blockDim.x) {
+    long long t = t0 + threadIdx.x;
+    int lv = 0;
+    if (t < m) {
+      const double* x = Q.tcx + 3 * (p0 + t);
+      lv = T.nlevel + 1;
+      for (int l = 0; l < T.nlevel; ++l) {
+        const double* qp = W.sub[l] + (size_t)pan * T.nsub[l] * 4;
+        bool outside = true;
+        for (int s = 0; s < T.nsub[l]; ++s) {
+          double a = qp[4 * s] - x[0], b = qp[4 * s + 1] - x[1], c = qp[4 * s + 2] - x[2];
+          if (a * a + b * b + c * c < qp[4 * s + 3]) { outside = false; break; }
+        }
+        if (outside) { lv = l + 1; break; }
+      }
+      G.level[p0 + t] = (signed char)lv;
+      atomicAdd(&cnt[lv], 1);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int acc = 0;
+    for (int l = 1; l <= T.nlevel + 1; ++l) {
+      base_l[l] = acc;
+      G.cnt[(size_t)pan * 8 + l] = cnt[l];
+      G.off[(size_t)pan * 8 + l] = acc;
+      acc += cnt[l];
+    }
+  }
+  __syncthreads();
+  /* pass 2: deterministic compaction in target order */
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (long long t0 = 0; t0 < m; t0 += blockDim.x) {
+    long long t = t0 + threadIdx.x;
+    int lv = (t < m) ? (int)G.level[p0 + t] : 0;
+    for (int l = 1; l <= T.nlevel + 1; ++l) {
+      unsigned b = __ballot_sync(0xffffffffu, lv == l);
+      if (lane == 0) warpc[wid][l] = __popc(b);
+      __syncthreads();
+      int before = 0;
+      for (int w = 0; w < wid; ++w) before += warpc[w][l];
+      int tot = 0;
+      for (int w = 0; w < 4; ++w) tot += warpc[w][l];
+      if (lv == l) {
+        int pos = base_l[l] + before + __popc(b & ((1u << lane) - 1u));
+        G.grp[p0 + pos] = (int)t;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) base_l[l] += tot;
+      __syncthreads();
+    }
+  }
+}
+
+/* ===================================================================== */
+/* K3: level-resolved pairs: kernel rows on the level nodes contracted   */
+/* with interpmat, minus the self-masked naive block, written as COO     */
+/* values.  One CTA per (panel, level); chunks of 32 targets.            */
+/* ===================================================================== */
+#define DT 32 /* targets per chunk */
+template <int HDMAX>
+__global__ void __launch_bounds__(256) k_direct(OrderTab T, PanelIn P, PairIn Q, LevelWS W, PairWS G,
+                                                OutCOO O) {
+  const int pan = blockIdx.x, l = blockIdx.y;
+  if (l >= T.nlevel) return;
+  const int cntl = G.cnt[(size_t)pan * 8 + l + 1];
+  if (cntl == 0) return;
+  const int offl = G.off[(size_t)pan * 8 + l + 1];
+  const int hd = T.hd, n = T.n[l];
+  const long long p0 = Q.tcxi[pan] - 1, m = Q.tcxi[pan + 1] - Q.tcxi[pan];
+  const double* node = W.node[l] + (size_t)pan * n * 7;
+  const double* I = T.interp[l];
+  __shared__ double tg[DT][3];
+  __shared__ int tloc[DT];
+  constexpr int NT = HDMAX > 96 ? 16 : 32; /* nodes per tile */
+  __shared__ double KS[NT][DT], KD[NT][DT];
+  __shared__ double It[NT][HDMAX];
+  const int t = threadIdx.x & 31, kg = threadIdx.x >> 5;
+  constexpr int NQ = (HDMAX + 7) / 8;
+  const double i4p = 1.0 / (4.0 * QOL_PI);
+  for (int c0 = 0; c0 < cntl; c0 += DT) {
+    const int nt = min(DT, cntl - c0);
+    __syncthreads();
+    if (threadIdx.x < DT) {
+      int tl = threadIdx.x < nt ? G.grp[p0 + offl + c0 + threadIdx.x] : -1;
+      tloc[threadIdx.x] = tl;
+      for (int d = 0; d < 3; ++d) tg[threadIdx.x][d] = tl >= 0 ? Q.tcx[3 * (p0 + tl) + d] : 0.0;
+    }
+    double accS[NQ], accD[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) { accS[q] = 0.0; accD[q] = 0.0; }
+    for (int n0 = 0; n0 < n; n0 += NT) {
+      __syncthreads();
+      for (int e = threadIdx.x; e < NT * DT; e += blockDim.x) {
+        int nn = e / DT, tt = e % DT, i = n0 + nn;
+        double s = 0.0, dv = 0.0;
+        if (i < n && tt < nt) {
+          double dx = tg[tt][0] - node[i], dy = tg[tt][1] - node[n + i], dz = tg[tt][2] - node[2 * n + i];
+          double rr = dx * dx + dy * dy + dz * dz;
+          if (rr > 1.0e-28) {
+            double w4 = node[6 * n + i] * i4p, r = sqrt(rr);
+            s = w4 / r;
+            dv = w4 * (dx * node[3 * n + i] + dy * node[4 * n + i] + dz * node[5 * n + i]) / (r * rr);
+          }
+        }
+        KS[nn][tt] = s;
+        KD[nn][tt] = dv;
+      }
+      for (int e = threadIdx.x; e < NT * hd; e += blockDim.x) {
+        int nn = e / hd, k = e % hd, i = n0 + nn;
+        It[nn][k] = i < n ? I[(size_t)i * hd + k] : 0.0;
+      }
+      __syncthreads();
+      const int nn_max = min(NT, n - n0);
+      for (int nn = 0; nn < nn_max; ++nn) {
+        double s = KS[nn][t], dv = KD[nn][t];
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+          int k = kg + 8 * q;
+          double iv = (k < HDMAX) ? It[nn][k] : 0.0;
+          accS[q] += s * iv;
+          accD[q] += dv * iv;
+        }
+      }
+    }
+    /* naive block and the COO write */
+    if (t < nt) {
+      const int tl = tloc[t];
+      const long long row = Q.tcxrow[p0 + tl];
+      const double x0 = tg[t][0], x1 = tg[t][1], x2 = tg[t][2];
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) {
+        int k = kg + 8 * q;
+        if (k >= hd) continue;
+        double vs = accS[q], vd = accD[q];
+        if (O.subtract_naive) {
+          size_t gj = (size_t)pan * hd + k;
+          double ns = 0.0, nd = 0.0;
+          if (row != (long long)gj + 1) {
+            double dx = x0 - P.sx[3 * gj], dy = x1 - P.sx[3 * gj + 1], dz = x2 - P.sx[3 * gj + 2];
+            double rr = dx * dx + dy * dy + dz * dz;
+            if (rr > 1.0e-28) {
+              double w4 = P.sw[gj] * i4p, r = sqrt(rr);
+              ns = w4 / r;
+              nd = w4 * (dx * P.snx[3 * gj] + dy * P.snx[3 * gj + 1] + dz * P.snx[3 * gj + 2]) / (r * rr);
+            }
+          }
+          vs -= ns; vd -= nd;
+        }
+        size_t o = (size_t)p0 * hd + (size_t)k * m + tl;
+        O.vs[o] = vs;
+        O.vd[o] = vd;
+      }
+    }
+  }
+}
+
+/* ===================================================================== */
+/* harmonic column evaluation (shared by K4 and K5)                      */
+/* ===================================================================== */
+/* column m of the Schmidt solid harmonics at frame point (x,y,z); calls
+ * f(l, k, h, gx, gy, gz) for l = m..L with the sin-type value and frame
+ * gradient.  Same recurrences as the oracle. */
+template <class F>
+__device__ __forceinline__ void harm_column(int L, int m, double x, double y, double z, F f) {
+  const double X = y, Y = z, Z = x;
+  const double r2 = X * X + Y * Y + Z * Z;
+  cd Pm = mk(1.0, 0.0), Pm1 = mk(0.0, 0.0);
+  const cd w = mk(X, Y);
+  for (int mm = 1; mm <= m; ++mm) {
+    double cm = c_hcm[mm];
+    cd Smm = cscale(cm, cmul(w, Pm));
+    cd dSmm = cscale(cm, cadd(Pm, cmul(w, Pm1)));
+    Pm1 = dSmm; Pm = Smm;
+  }
+  cd s1 = Pm, s1x = Pm1, s1y = mk(-Pm1.im, Pm1.re), s1z = mk(0.0, 0.0);
+  cd s2 = mk(0.0, 0.0), s2x = s2, s2y = s2, s2z = s2;
+  f(m, m * (m - 1) / 2 + (m - 1), s1.im, s1z.im, s1x.im, s1y.im);
+  for (int l = m + 1; l <= L; ++l) {
+    double a = (2.0 * l - 1.0), b = c_hb[l][m], c = c_hc[l][m];
+    cd s, sx, sy, sz;
+    s = cscale(c, csub(cscale(a * Z, s1), cscale(b * r2, s2)));
+    sx = cscale(c, csub(cscale(a * Z, s1x), cscale(b, cadd(cscale(2.0 * X, s2), cscale(r2, s2x)))));
+    sy = cscale(c, csub(cscale(a * Z, s1y), cscale(b, cadd(cscale(2.0 * Y, s2), cscale(r2, s2y)))));
+    sz = cscale(c, csub(cscale(a, cadd(s1, cscale(Z, s1z))), cscale(b, cadd(cscale(2.0 * Z, s2), cscale(r2, s2z)))));
+    s2 = s1; s2x = s1x; s2y = s1y; s2z = s1z;
+    s1 = s; s1x = sx; s1y = sy; s1z = sz;
+    f(l, l * (l - 1) / 2 + (m - 1), s.im, sz.im, sx.im, sy.im);
+  }
+}
+
+/* ===================================================================== */
+/* K4: per-panel RRQ precompute                                          */
+/* ===================================================================== */
+__device__ __forceinline__ void qmul(const double* a, const double* b, double* c) {
+  c[0] = a[0] * b[0] - a[1] * b[1] - a[2] * b[2] - a[3] * b[3];
+  c[1] = a[0] * b[1] + a[1] * b[0] + a[2] * b[3] - a[3] * b[2];
+  c[2] = a[0] * b[2] - a[1] * b[3] + a[2] * b[0] + a[3] * b[1];
+  c[3] = a[0] * b[3] + a[1] * b[2] - a[2] * b[1] + a[3] * b[0];
+}
+
+/* block-wide argmax of v over the CTA; returns the winning index */
+__device__ int block_argmax(double v, int idx, double* sv, int* si) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) {
+    double v2 = __shfl_down_sync(0xffffffffu, v, o);
+    int i2 = __shfl_down_sync(0xffffffffu, idx, o);
+    if (v2 > v || (v2 == v && i2 < idx)) { v = v2; idx = i2; }
+  }
+  if (lane == 0) { sv[wid] = v; si[wid] = idx; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double bv = sv[0]; int bi = si[0];
+    for (int w = 1; w < nw; ++w)
+      if (sv[w] > bv || (sv[w] == bv && si[w] < bi)) { bv = sv[w]; bi = si[w]; }
+    si[0] = bi;
+  }
+  __syncthreads();
+  int r = si[0];
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(256) k_rrq_panel(OrderTab T, PanelIn P, PairWS G, RRQWS R,
+                                                   const double* chart /* nullable, per panel 3 x (3nq+3) */) {
+  const int pan = blockIdx.x;
+  if (G.cnt[(size_t)pan * 8 + T.nlevel + 1] == 0 && !R.all_panels) return;
+  const int hd = T.hd, nq = T.nquad, nbd = 3 * nq, L = T.nterms;
+  __shared__ double s_sx[3 * 136], s_raw[3 * (3 * QOL_MAXNQ + 3)], s_fr[16];
+  __shared__ double sv[8];
+  __shared__ int si[8];
+  __shared__ double s_row[4 * 136], s_col[4 * 136], s_pinv[4];
+  double* fr = R.frame + (size_t)pan * RRQ_FRAME;
+  double* bx = R.bx + (size_t)pan * 3 * nbd;
+  double* bt = R.bt + (size_t)pan * 3 * nbd;
+  double* cf = R.cf + (size_t)pan * 9 * nq;
+  double* scf = R.scf + (size_t)pan * 3 * hd;
+  double* V = R.qmat + (size_t)blockIdx.x * 4 * hd * hd; /* hd x hd quaternions, row-major */
+  double* H = R.hmat + (size_t)pan * hd * hd;            /* H[j*hd+k] = h_k(y_j) */
+  double* MS = R.smat + (size_t)pan * hd * hd;           /* Msl^T, then its inverse (PS) */
+  for (int e = threadIdx.x; e < 3 * hd; e += blockDim.x) s_sx[e] = P.sx[(size_t)pan * hd * 3 + e];
+  __syncthreads();
+  /* boundary + vertices from the interpolant, or the caller's chart */
+  for (int i = threadIdx.x; i < nbd + 3; i += blockDim.x) {
+    double a[3] = {0.0, 0.0, 0.0};
+    if (chart) {
+      for (int d = 0; d < 3; ++d) a[d] = chart[(size_t)pan * 3 * (nbd + 3) + 3 * i + d];
+    } else {
+      for (int j = 0; j < hd; ++j) {
+        double mb = T.Mb[(size_t)i * hd + j];
+        a[0] += mb * s_sx[3 * j]; a[1] += mb * s_sx[3 * j + 1]; a[2] += mb * s_sx[3 * j + 2];
+      }
+    }
+    s_raw[3 * i] = a[0]; s_raw[3 * i + 1] = a[1]; s_raw[3 * i + 2] = a[2];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    /* frame from the vertex triangle: e1 along v2-v1, e3 its normal, origin
+     * the circumcentre shifted below the lowest node */
+    const double* v1 = &s_raw[3 * nbd];
+    const double* v2 = v1 + 3;
+    const double* v3 = v1 + 6;
+    double a[3], b[3], nn[3], e1[3], e2[3];
+    for (int d = 0; d < 3; ++d) { a[d] = v2[d] - v1[d]; b[d] = v3[d] - v1[d]; }
+    cross3(a, b, nn);
+    double nl = sqrt(dot3(nn, nn));
+    for (int d = 0; d < 3; ++d) nn[d] /= nl;
+    double la = sqrt(dot3(a, a));
+    for (int d = 0; d < 3; ++d) e1[d] = a[d] / la;
+    cross3(nn, e1, e2);
+    double Rm[9];
+    for (int d = 0; d < 3; ++d) { Rm[0 + 3 * d] = e1[d]; Rm[1 + 3 * d] = e2[d]; Rm[2 + 3 * d] = nn[d]; }
+    double axb[3], pp[3], qq[3], c0[3];
+    cross3(a, b, axb);
+    double aa = dot3(a, a), bb = dot3(b, b), den = 2.0 * dot3(axb, axb);
+    for (int d = 0; d < 3; ++d) pp[d] = aa * b[d] - bb * a[d];
+    cross3(pp, axb, qq);
+    for (int d = 0; d < 3; ++d) c0[d] = v1[d] + qq[d] / den;
+    double swsum = 0.0;
+    for (int j = 0; j < hd; ++j) swsum += P.sw[(size_t)pan * hd + j];
+    double alpha = 1.25 / sqrt(2.0 * swsum);
+    double zmin = 1e300;
+    for (int j = 0; j < hd; ++j) {
+      double d0 = s_sx[3 * j] - c0[0], d1 = s_sx[3 * j + 1] - c0[1], d2 = s_sx[3 * j + 2] - c0[2];
+      double zz = alpha * (Rm[2] * d0 + Rm[5] * d1 + Rm[8] * d2);
+      zmin = fmin(zmin, zz);
+    }
+    double sx3min = fmax(0.0, -zmin);
+    for (int i = 0; i < 9; ++i) s_fr[i] = Rm[i];
+    for (int d = 0; d < 3; ++d) s_fr[9 + d] = c0[d] - (1.25 * sx3min / alpha) * Rm[2 + 3 * d];
+    s_fr[12] = alpha;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < RRQ_FRAME; i += blockDim.x) fr[i] = i < 13 ? s_fr[i] : 0.0;
+  const double alpha = s_fr[12];
+  auto tofr = [&](const double* x, double* y) {
+    double d0 = x[0] - s_fr[9], d1 = x[1] - s_fr[10], d2 = x[2] - s_fr[11];
+    for (int i = 0; i < 3; ++i) y[i] = alpha * (s_fr[i] * d0 + s_fr[i + 3] * d1 + s_fr[i + 6] * d2);
+  };
+  for (int i = threadIdx.x; i < nbd; i += blockDim.x) {
+    double y[3];
+    tofr(&s_raw[3 * i], y);
+    for (int d = 0; d < 3; ++d) bx[3 * i + d] = y[d];
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < 3 * 3 * nq; e += blockDim.x) {
+    int ed = e / (3 * nq), r = e % (3 * nq), d = r / nq, q = r % nq;
+    double s = 0.0, sc = 0.0;
+    for (int k = 0; k < nq; ++k) {
+      double v = bx[3 * (ed * nq + k) + d];
+      s += T.Dgl[q + nq * k] * v;
+      sc += T.Leg[q + nq * k] * v;
+    }
+    bt[3 * (ed * nq + q) + d] = s;
+    cf[ed * 3 * nq + d * nq + q] = sc;
+  }
+  /* basis at the nodes: V (quaternion, pure), H, Msl^T */
+  for (int j = threadIdx.x; j < hd; j += blockDim.x) {
+    double y[3], nrm[3];
+    tofr(&s_sx[3 * j], y);
+    const double* sn = P.snx + ((size_t)pan * hd + j) * 3;
+    for (int i = 0; i < 3; ++i) nrm[i] = s_fr[i] * sn[0] + s_fr[i + 3] * sn[1] + s_fr[i + 6] * sn[2];
+    for (int m = 1; m <= L; ++m)
+      harm_column(L, m, y[0], y[1], y[2], [&](int l, int k, double h, double gx, double gy, double gz) {
+        double* q = V + ((size_t)j * hd + k) * 4;
+        q[0] = 0.0; q[1] = gx; q[2] = gy; q[3] = gz;
+        H[(size_t)j * hd + k] = h;
+        MS[(size_t)k * hd + j] = nrm[0] * gx + nrm[1] * gy + nrm[2] * gz; /* Msl^T(k,j) row-major */
+      });
+    /* Koornwinder coefficients of the frame node positions, scf[d*hd+k] */
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < 3 * hd; e += blockDim.x) {
+    int d = e / hd, k = e % hd;
+    double s = 0.0;
+    for (int j = 0; j < hd; ++j) {
+      double y[3];
+      tofr(&s_sx[3 * j], y);
+      s += T.umatr[k + (size_t)hd * j] * y[d];
+    }
+    scf[d * hd + k] = s;
+  }
+  __syncthreads();
+  /* in-place Gauss-Jordan inverse of the quaternion matrix V (row pivoting,
+   * pivot by quaternion norm), then of Msl^T (real) */
+  int* perm = (int*)(R.perm + (size_t)blockIdx.x * 2 * 136);
+  for (int k = 0; k < hd; ++k) {
+    double bestv = -1.0; int besti = hd;
+    for (int i = k + threadIdx.x; i < hd; i += blockDim.x) {
+      const double* q = V + ((size_t)i * hd + k) * 4;
+      double v = q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
+      if (v > bestv) { bestv = v; besti = i; }
+    }
+    int p = block_argmax(bestv, besti, sv, si);
+    if (threadIdx.x == 0) perm[k] = p;
+    if (p != k)
+      for (int e = threadIdx.x; e < 4 * hd; e += blockDim.x) {
+        double* a = V + (size_t)k * hd * 4 + e;
+        double* b = V + (size_t)p * hd * 4 + e;
+        double t = *a; *a = *b; *b = t;
+      }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const double* q = V + ((size_t)k * hd + k) * 4;
+      double n2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
+      s_pinv[0] = q[0] / n2; s_pinv[1] = -q[1] / n2; s_pinv[2] = -q[2] / n2; s_pinv[3] = -q[3] / n2;
+    }
+    for (int e = threadIdx.x; e < hd; e += blockDim.x) {
+      const double* q = V + ((size_t)e * hd + k) * 4;
+      for (int c = 0; c < 4; ++c) s_col[4 * e + c] = q[c];
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < hd; j += blockDim.x) {
+      double* q = V + ((size_t)k * hd + j) * 4;
+      double r[4];
+      if (j == k) { for (int c = 0; c < 4; ++c) r[c] = s_pinv[c]; }
+      else qmul(s_pinv, q, r);
+      for (int c = 0; c < 4; ++c) { q[c] = r[c]; s_row[4 * j + c] = r[c]; }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < hd * hd; e += blockDim.x) {
+      int i = e / hd, j = e % hd;
+      if (i == k) continue;
+      double* q = V + ((size_t)i * hd + j) * 4;
+      const double* f = &s_col[4 * i];
+      double r[4];
+      if (j == k) {
+        qmul(f, s_pinv, r);
+        for (int c = 0; c < 4; ++c) q[c] = -r[c];
+      } else {
+        qmul(f, &s_row[4 * j], r);
+        for (int c = 0; c < 4; ++c) q[c] -= r[c];
+      }
+    }
+    __syncthreads();
+  }
+  for (int k = hd - 1; k >= 0; --k) {
+    int p = perm[k];
+    if (p != k)
+      for (int i = threadIdx.x; i < hd; i += blockDim.x)
+        for (int c = 0; c < 4; ++c) {
+          double* a = V + ((size_t)i * hd + k) * 4 + c;
+          double* b = V + ((size_t)i * hd + p) * 4 + c;
+          double t = *a; *a = *b; *b = t;
+        }
+    __syncthreads();
+  }
+  /* PD(j, c*hd+k) = s_c x_c(k, j), s = (+,-,-,-); stored row-major [j][4hd] */
+  double* PD = R.PD + (size_t)pan * hd * 4 * hd;
+  for (int e = threadIdx.x; e < hd * hd; e += blockDim.x) {
+    int j = e / hd, k = e % hd;
+    const double* x = V + ((size_t)k * hd + j) * 4;
+    PD[(size_t)j * 4 * hd + 0 * hd + k] = x[0];
+    PD[(size_t)j * 4 * hd + 1 * hd + k] = -x[1];
+    PD[(size_t)j * 4 * hd + 2 * hd + k] = -x[2];
+    PD[(size_t)j * 4 * hd + 3 * hd + k] = -x[3];
+  }
+  __syncthreads();
+  /* real Gauss-Jordan on Msl^T (row-major MS[k][j]) */
+  int* perm2 = perm + 136;
+  for (int k = 0; k < hd; ++k) {
+    double bestv = -1.0; int besti = hd;
+    for (int i = k + threadIdx.x; i < hd; i += blockDim.x) {
+      double v = fabs(MS[(size_t)i * hd + k]);
+      if (v > bestv) { bestv = v; besti = i; }
+    }
+    int p = block_argmax(bestv, besti, sv, si);
+    if (threadIdx.x == 0) perm2[k] = p;
+    if (p != k)
+      for (int e = threadIdx.x; e < hd; e += blockDim.x) {
+        double t = MS[(size_t)k * hd + e]; MS[(size_t)k * hd + e] = MS[(size_t)p * hd + e]; MS[(size_t)p * hd + e] = t;
+      }
+    __syncthreads();
+    if (threadIdx.x == 0) s_pinv[0] = 1.0 / MS[(size_t)k * hd + k];
+    for (int e = threadIdx.x; e < hd; e += blockDim.x) s_col[e] = MS[(size_t)e * hd + k];
+    __syncthreads();
+    for (int j = threadIdx.x; j < hd; j += blockDim.x) {
+      double v = (j == k) ? s_pinv[0] : s_pinv[0] * MS[(size_t)k * hd + j];
+      MS[(size_t)k * hd + j] = v; s_row[j] = v;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < hd * hd; e += blockDim.x) {
+      int i = e / hd, j = e % hd;
+      if (i == k) continue;
+      if (j == k) MS[(size_t)i * hd + j] = -s_col[i] * s_pinv[0];
+      else MS[(size_t)i * hd + j] -= s_col[i] * s_row[j];
+    }
+    __syncthreads();
+  }
+  for (int k = hd - 1; k >= 0; --k) {
+    int p = perm2[k];
+    if (p != k)
+      for (int i = threadIdx.x; i < hd; i += blockDim.x) {
+        double t = MS[(size_t)i * hd + k]; MS[(size_t)i * hd + k] = MS[(size_t)i * hd + p]; MS[(size_t)i * hd + p] = t;
+      }
+    __syncthreads();
+  }
+  /* B = PS H^T: B[i][j] = sum_k PS[i][k] h_k(y_j) */
+  double* B = R.B + (size_t)pan * hd * hd;
+  for (int e = threadIdx.x; e < hd * hd; e += blockDim.x) {
+    int i = e / hd, j = e % hd;
+    double s = 0.0;
+    for (int k = 0; k < hd; ++k) s += MS[(size_t)i * hd + k] * H[(size_t)j * hd + k];
+    B[(size_t)i * hd + j] = s;
+  }
+}
+
+/* ===================================================================== */
+/* K5: per-pair RRQ moments, one warp per pair                           */
+/* ===================================================================== */
+#define RRQ_WARPS 2
+struct WarpSM {
+  double xt[3];
+  double w1[3 * QOL_MAXNQ], w3[3 * QOL_MAXNQ];
+  double root[3][2];
+  int rok[3];
+  double cD[3 * 3 * QOL_MAXNQ], cS[3 * 3 * QOL_MAXNQ];
+  double br[3][112];
+  int nbr[3];
+  int outside;
+  double Omega, sdir;
+};
+
+__device__ double panel_height(const OrderTab& T, const double* scf, const double* xt, double* pols, int* inside) {
+  const int hd = T.hd, korder = T.korder;
+  /* nearest node in plane among the VR nodes, Newton on (u,v) */
+  int ib = 0; double best = 1e300;
+  for (int j = 0; j < hd; ++j) {
+    koorn_pols_dev(T.vruv[2 * j], T.vruv[2 * j + 1], korder, pols);
+    double f0 = 0, f1 = 0;
+    for (int k = 0; k < hd; ++k) { f0 += pols[k] * scf[k]; f1 += pols[k] * scf[hd + k]; }
+    double d0 = f0 - xt[0], d1 = f1 - xt[1];
+    if (d0 * d0 + d1 * d1 < best) { best = d0 * d0 + d1 * d1; ib = j; }
+  }
+  double u = T.vruv[2 * ib], v = T.vruv[2 * ib + 1];
+  for (int it = 0; it < 40; ++it) {
+    const double h = 1e-7;
+    double f0 = 0, f1 = 0, fu0 = 0, fu1 = 0, fv0 = 0, fv1 = 0;
+    koorn_pols_dev(u, v, korder, pols);
+    for (int k = 0; k < hd; ++k) { f0 += pols[k] * scf[k]; f1 += pols[k] * scf[hd + k]; }
+    koorn_pols_dev(u + h, v, korder, pols);
+    for (int k = 0; k < hd; ++k) { fu0 += pols[k] * scf[k]; fu1 += pols[k] * scf[hd + k]; }
+    koorn_pols_dev(u, v + h, korder, pols);
+    for (int k = 0; k < hd; ++k) { fv0 += pols[k] * scf[k]; fv1 += pols[k] * scf[hd + k]; }
+    double J00 = (fu0 - f0) / h, J10 = (fu1 - f1) / h, J01 = (fv0 - f0) / h, J11 = (fv1 - f1) / h;
+    double r0 = f0 - xt[0], r1 = f1 - xt[1];
+    double det = J00 * J11 - J01 * J10;
+    if (det == 0.0) break;
+    double du = (J11 * r0 - J01 * r1) / det, dv = (-J10 * r0 + J00 * r1) / det;
+    u -= du; v -= dv;
+    if (fabs(du) + fabs(dv) < 1e-14) break;
+  }
+  koorn_pols_dev(u, v, korder, pols);
+  double zs = 0.0;
+  for (int k = 0; k < hd; ++k) zs += pols[k] * scf[2 * hd + k];
+  const double tol = 1e-10;
+  *inside = (u >= -tol && v >= -tol && u + v <= 1.0 + tol) ? 1 : 0;
+  return xt[2] - zs;
+}
+
+__global__ void __launch_bounds__(32 * RRQ_WARPS) k_rrq_target(OrderTab T, PairIn Q, PairWS G, RRQWS R,
+                                                              int exterior) {
+  __shared__ WarpSM S[RRQ_WARPS];
+  __shared__ double accs[RRQ_WARPS][2][5 * 136];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const long long gidx = (long long)blockIdx.x * RRQ_WARPS + wid;
+  if (gidx >= R.nrrq) return;
+  WarpSM& W = S[wid];
+  /* panel of this RRQ pair: binary search in the per-panel RRQ offsets */
+  int lo = 0, hi = R.npan;
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (R.rrq_off[mid] <= gidx) lo = mid; else hi = mid;
+  }
+  const int pan = lo;
+  const int j_loc = (int)(gidx - R.rrq_off[pan]);
+  const long long p0 = Q.tcxi[pan] - 1;
+  const int tl = G.grp[p0 + G.off[(size_t)pan * 8 + T.nlevel + 1] + j_loc];
+  const int hd = T.hd, nq = T.nquad, nbd = 3 * nq, L = T.nterms, ng = T.ng;
+  const double* fr = R.frame + (size_t)pan * RRQ_FRAME;
+  const double* bx = R.bx + (size_t)pan * 3 * nbd;
+  const double* bt = R.bt + (size_t)pan * 3 * nbd;
+  const double* cf = R.cf + (size_t)pan * 9 * nq;
+  const double alpha = fr[12];
+  if (lane == 0) {
+    const double* x = Q.tcx + 3 * (p0 + tl);
+    double d0 = x[0] - fr[9], d1 = x[1] - fr[10], d2 = x[2] - fr[11];
+    for (int i = 0; i < 3; ++i) W.xt[i] = alpha * (fr[i] * d0 + fr[i + 3] * d1 + fr[i + 6] * d2);
+  }
+  __syncwarp();
+  const double xt0 = W.xt[0], xt1 = W.xt[1], xt2 = W.xt[2];
+  /* singularity-swap weights, one lane per edge */
+  if (lane < 3) {
+    const int e = lane;
+    cd t0 = mk(0.0, 0.0);
+    bool ok = edge_root_dev(nq, cf + e * 3 * nq, T.tgl, bx + 3 * e * nq, W.xt, t0);
+    ssq_weights_dev(nq, T.tgl, T.wgl, ok, t0, T.gl48x, T.gl48w, &W.w1[e * nq], &W.w3[e * nq]);
+    W.root[e][0] = t0.re; W.root[e][1] = t0.im; W.rok[e] = ok ? 1 : 0;
+    /* graded breakpoints for the solid angle on this edge */
+    double ts = 0.0, dd = 2.0;
+    if (ok) { ts = fmin(1.0, fmax(-1.0, t0.re)); dd = fmax(fabs(t0.im), 1e-15); }
+    double left[54], right[54];
+    int nl = 0, nr = 0;
+    if (!ok) {
+      for (int k = 1; k < 16; ++k) right[nr++] = -1.0 + k / 8.0;
+    } else if (dd < 1.0) {
+      for (double h = 0.5 * dd; h < 2.0; h *= 2.0) {
+        if (ts - h > -1.0 && nl < 54) left[nl++] = ts - h;
+        if (ts + h < 1.0 && nr < 54) right[nr++] = ts + h;
+      }
+    }
+    int c = 0;
+    W.br[e][c++] = -1.0;
+    for (int k = nl - 1; k >= 0; --k) W.br[e][c++] = left[k];
+    for (int k = 0; k < nr; ++k) W.br[e][c++] = right[k];
+    W.br[e][c++] = 1.0;
+    W.nbr[e] = c;
+  }
+  /* Dirac-string direction (lane 3 side test; clearance over the lanes) */
+  if (lane == 3) {
+    double pols[136];
+    int inside = 1;
+    double hgt = panel_height(T, R.scf + (size_t)pan * 3 * hd, W.xt, pols, &inside);
+    int side = fabs(hgt) <= 1e-12 ? 0 : (hgt > 0 ? 1 : -1);
+    W.sdir = side == 0 ? (exterior ? 1.0 : -1.0) : (double)side;
+    W.outside = inside ? 0 : 1; /* projects outside the triangle */
+  }
+  __syncwarp();
+  if (W.outside) {
+    /* both directions avoid the panel: take the one passing farther from
+     * the boundary, min over 32 samples per edge of (r - s.rho)/r */
+    double cu = 2.0, cdn = 2.0;
+    for (int pnt = lane; pnt < 96; pnt += 32) {
+      int e = pnt >> 5, q = pnt & 31;
+      double t = -1.0 + (2.0 * q + 1.0) / 32.0, y[3], yp[3];
+      for (int d = 0; d < 3; ++d) leg_eval_r(nq, cf + e * 3 * nq + d * nq, t, y[d], yp[d]);
+      double rho[3] = {y[0] - xt0, y[1] - xt1, y[2] - xt2};
+      double r = sqrt(dot3(rho, rho));
+      cu = fmin(cu, (r - rho[2]) / r);
+      cdn = fmin(cdn, (r + rho[2]) / r);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      cu = fmin(cu, __shfl_xor_sync(0xffffffffu, cu, o));
+      cdn = fmin(cdn, __shfl_xor_sync(0xffffffffu, cdn, o));
+    }
+    if (lane == 0) W.sdir = cu >= cdn ? 1.0 : -1.0;
+  }
+  __syncwarp();
+  /* solid angle: points of the graded meshes over lanes */
+  {
+    const double sdir = W.sdir;
+    double tot = 0.0;
+    for (int e = 0; e < 3; ++e) {
+      const int nint = W.nbr[e] - 1;
+      for (int pnt = lane; pnt < nint * 16; pnt += 32) {
+        int ib = pnt >> 4, q = pnt & 15;
+        double a = W.br[e][ib], b = W.br[e][ib + 1];
+        if (!(b > a)) continue;
+        double hm = 0.5 * (b - a), cm = 0.5 * (a + b), t = cm + hm * T.gl16x[q];
+        double y[3], yp[3];
+        for (int d = 0; d < 3; ++d) leg_eval_r(nq, cf + e * 3 * nq + d * nq, t, y[d], yp[d]);
+        double rho[3] = {y[0] - xt0, y[1] - xt1, y[2] - xt2};
+        double r = sqrt(dot3(rho, rho));
+        double s3[3] = {0.0, 0.0, sdir}, c[3];
+        double sr = sdir * rho[2];
+        cross3(rho, s3, c);
+        double den = sr > 0 ? dot3(c, c) / (r + sr) : r - sr;
+        tot += hm * T.gl16w[q] * dot3(c, yp) / (r * den);
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+    if (lane == 0) W.Omega = tot;
+  }
+  /* per boundary node weights (1/4pi folded in) */
+  const double i4p = 1.0 / (4.0 * QOL_PI);
+  double lint[3] = {0, 0, 0};
+  for (int i = lane; i < nbd; i += 32) {
+    const double* y = bx + 3 * i;
+    const double* yp = bt + 3 * i;
+    double rho[3] = {y[0] - xt0, y[1] - xt1, y[2] - xt2};
+    double r = sqrt(dot3(rho, rho));
+    double rxy[3], rrx[3];
+    cross3(rho, yp, rxy);
+    cross3(rho, rxy, rrx);
+    double f1 = W.w1[i] / r, f3 = W.w3[i] / (r * r * r);
+    for (int d = 0; d < 3; ++d) {
+      W.cD[3 * i + d] = f3 * rrx[d] * i4p;
+      W.cS[3 * i + d] = f1 * rxy[d] * i4p;
+      lint[d] += f1 * yp[d];
+    }
+  }
+  for (int d = 0; d < 3; ++d)
+    for (int o = 16; o > 0; o >>= 1) lint[d] += __shfl_xor_sync(0xffffffffu, lint[d], o);
+  __syncwarp();
+  /* accumulation over the segment points: half-warp per point, lane = column m */
+  const int half = lane >> 4, m = (lane & 15) + 1;
+  double* acc = accs[wid][half];
+  for (int e = lane; e < 2 * 5 * hd; e += 32) accs[wid][e / (5 * hd)][e % (5 * hd)] = 0.0;
+  __syncwarp();
+  double sumcD[3] = {0, 0, 0};
+  const int npts = nbd * ng;
+  for (int p = half; p < npts; p += 2) {
+    const int i = p / ng, g = p % ng;
+    const double t = T.tq[g], aD = T.wq[g] / t, aS = T.wq[g];
+    const double uD[3] = {aD * W.cD[3 * i], aD * W.cD[3 * i + 1], aD * W.cD[3 * i + 2]};
+    const double uS[3] = {aS * W.cS[3 * i], aS * W.cS[3 * i + 1], aS * W.cS[3 * i + 2]};
+    if (m == 1) { sumcD[0] += uD[0]; sumcD[1] += uD[1]; sumcD[2] += uD[2]; }
+    if (m <= L) {
+      const double* y = bx + 3 * i;
+      const double z0 = xt0 + t * (y[0] - xt0), z1 = xt1 + t * (y[1] - xt1), z2 = xt2 + t * (y[2] - xt2);
+      harm_column(L, m, z0, z1, z2, [&](int l, int k, double h, double gx, double gy, double gz) {
+        double* a = acc + 5 * k;
+        a[0] += -(uD[0] * gx + uD[1] * gy + uD[2] * gz);
+        a[1] += uD[1] * gz - uD[2] * gy;
+        a[2] += uD[2] * gx - uD[0] * gz;
+        a[3] += uD[0] * gy - uD[1] * gx;
+        a[4] += uS[0] * gx + uS[1] * gy + uS[2] * gz;
+      });
+    }
+  }
+  /* total sum of the D segment weights: lanes with m == 1 hold partials (one per half) */
+  for (int d = 0; d < 3; ++d) {
+    sumcD[d] += __shfl_xor_sync(0xffffffffu, sumcD[d], 16);
+    sumcD[d] = __shfl_sync(0xffffffffu, sumcD[d], 0);
+  }
+  __syncwarp();
+  /* the x point: (s0, l/4pi - sumcD) (x) (0, grad h(x)) and h(x) Omega/4pi */
+  const double Omega = W.Omega;
+  const double s0 = -Omega * i4p;
+  const double wv[3] = {lint[0] * i4p - sumcD[0], lint[1] * i4p - sumcD[1], lint[2] * i4p - sumcD[2]};
+  double* JD = R.JD + (size_t)gidx * 4 * hd;
+  double* RS = R.RS + (size_t)gidx * hd;
+  if (half == 0 && m <= L) {
+    const double* a0 = accs[wid][0];
+    const double* a1 = accs[wid][1];
+    harm_column(L, m, xt0, xt1, xt2, [&](int l, int k, double h, double gx, double gy, double gz) {
+      double q0 = -(wv[0] * gx + wv[1] * gy + wv[2] * gz);
+      double q1 = s0 * gx + (wv[1] * gz - wv[2] * gy);
+      double q2 = s0 * gy + (wv[2] * gx - wv[0] * gz);
+      double q3 = s0 * gz + (wv[0] * gy - wv[1] * gx);
+      JD[0 * hd + k] = a0[5 * k + 0] + a1[5 * k + 0] + q0;
+      JD[1 * hd + k] = a0[5 * k + 1] + a1[5 * k + 1] + q1;
+      JD[2 * hd + k] = a0[5 * k + 2] + a1[5 * k + 2] + q2;
+      JD[3 * hd + k] = a0[5 * k + 3] + a1[5 * k + 3] + q3;
+      RS[k] = a0[5 * k + 4] + a1[5 * k + 4] + h * Omega * i4p;
+    });
+  }
+  if (lane == 0 && R.ialpha) R.ialpha[tl] = Omega; /* single-panel calls (qol_rrq) */
+}
+
+/* ===================================================================== */
+/* K6: RRQ solves as matrix products per panel + naive subtraction + COO */
+/* ===================================================================== */
+#define AT 16
+template <int HDMAX>
+__global__ void __launch_bounds__(256) k_rrq_apply(OrderTab T, PanelIn P, PairIn Q, PairWS G, RRQWS R,
+                                                   OutCOO O) {
+  const int pan = blockIdx.x;
+  const int cnt = G.cnt[(size_t)pan * 8 + T.nlevel + 1];
+  if (cnt == 0) return;
+  const int hd = T.hd, N4 = 4 * hd;
+  const long long p0 = Q.tcxi[pan] - 1, m = Q.tcxi[pan + 1] - Q.tcxi[pan];
+  const int offl = G.off[(size_t)pan * 8 + T.nlevel + 1];
+  const long long g0 = R.rrq_off[pan];
+  const double* PD = R.PD + (size_t)pan * hd * N4;
+  const double* PS = R.smat + (size_t)pan * hd * hd;
+  const double* B = R.B + (size_t)pan * hd * hd;
+  const double alpha = R.frame[(size_t)pan * RRQ_FRAME + 12];
+  extern __shared__ double sm[];
+  double* sJ = sm;                 /* N4 x AT */
+  double* sR = sJ + N4 * AT;       /* hd x AT */
+  double* sA = sR + hd * AT;       /* hd x AT (Ad) */
+  __shared__ int tloc[AT];
+  const int t = threadIdx.x % AT, jj = threadIdx.x / AT; /* 16 row groups */
+  const double i4p = 1.0 / (4.0 * QOL_PI);
+  for (int c0 = 0; c0 < cnt; c0 += AT) {
+    const int nt = min(AT, cnt - c0);
+    __syncthreads();
+    for (int e = threadIdx.x; e < N4 * AT; e += blockDim.x) {
+      int tt = e / N4, q = e % N4;
+      sJ[q * AT + tt] = tt < nt ? R.JD[(size_t)(g0 + c0 + tt) * N4 + q] : 0.0;
+    }
+    for (int e = threadIdx.x; e < hd * AT; e += blockDim.x) {
+      int tt = e / hd, q = e % hd;
+      sR[q * AT + tt] = tt < nt ? R.RS[(size_t)(g0 + c0 + tt) * hd + q] : 0.0;
+    }
+    if (threadIdx.x < AT) tloc[threadIdx.x] = threadIdx.x < nt ? G.grp[p0 + offl + c0 + threadIdx.x] : 0;
+    __syncthreads();
+    for (int j = jj; j < hd; j += 256 / AT) {
+      double s = 0.0;
+      const double* pr = PD + (size_t)j * N4;
+      for (int q = 0; q < N4; ++q) s += pr[q] * sJ[q * AT + t];
+      sA[j * AT + t] = s;
+    }
+    __syncthreads();
+    for (int j = jj; j < hd; j += 256 / AT) {
+      double s = 0.0;
+      const double* ps = PS + (size_t)j * hd;
+      const double* pb = B + (size_t)j * hd;
+      for (int k = 0; k < hd; ++k) s += ps[k] * sR[k * AT + t];
+      for (int k = 0; k < hd; ++k) s += pb[k] * sA[k * AT + t];
+      if (t < nt) {
+        double vs = s / alpha, vd = sA[j * AT + t];
+        const int tl = tloc[t];
+        if (O.subtract_naive) {
+          const long long row = Q.tcxrow[p0 + tl];
+          size_t gj = (size_t)pan * hd + j;
+          if (row != (long long)gj + 1) {
+            const double* x = Q.tcx + 3 * (p0 + tl);
+            double dx = x[0] - P.sx[3 * gj], dy = x[1] - P.sx[3 * gj + 1], dz = x[2] - P.sx[3 * gj + 2];
+            double rr = dx * dx + dy * dy + dz * dz;
+            if (rr > 1.0e-28) {
+              double w4 = P.sw[gj] * i4p, r = sqrt(rr);
+              vs -= w4 / r;
+              vd -= w4 * (dx * P.snx[3 * gj] + dy * P.snx[3 * gj + 1] + dz * P.snx[3 * gj + 2]) / (r * rr);
+            }
+          }
+        }
+        size_t o = (size_t)p0 * hd + (size_t)j * m + tl;
+        O.vs[o] = vs;
+        O.vd[o] = vd;
+      }
+    }
+    /* Omega (reference layout, qol_rrq only): (J_s, -J_x, -J_y, -J_z)/alpha */
+    if (O.omega)
+      for (int e = threadIdx.x; e < N4 * nt; e += blockDim.x) {
+        int tt = e / N4, q = e % N4;
+        double v = sJ[q * AT + tt];
+        O.omega[(size_t)tloc[tt] * N4 + q] = (q < hd ? v : -v) / alpha;
+      }
+  }
+}
+
+/* ===================================================================== */
+/* K7: COO row/column indices (block column-major per panel)            */
+/* ===================================================================== */
+__global__ void __launch_bounds__(256) k_coo_index(OrderTab T, PairIn Q, long long* si, long long* sj) {
+  const int pan = blockIdx.x, hd = T.hd;
+  const long long p0 = Q.tcxi[pan] - 1, m = Q.tcxi[pan + 1] - Q.tcxi[pan];
+  const long long tot = m * hd;
+  for (long long e = threadIdx.x; e < tot; e += blockDim.x) {
+    long long j = e / m, i = e % m;
+    size_t o = (size_t)p0 * hd + e;
+    si[o] = Q.tcxrow[p0 + i];
+    sj[o] = (long long)pan * hd + j + 1;
+  }
+}
+
+/* ===================================================================== */
+/* small scan of per-panel RRQ counts                                    */
+/* ===================================================================== */
+__global__ void k_scan_rrq(int npan, int lev, const int* cnt, long long* off) {
+  __shared__ long long part[1024];
+  const int nth = blockDim.x, tid = threadIdx.x;
+  const int per = (npan + nth - 1) / nth;
+  const int a = tid * per, b = min(npan, a + per);
+  long long s = 0;
+  for (int i = a; i < b; ++i) s += cnt[(size_t)i * 8 + lev];
+  part[tid] = s;
+  __syncthreads();
+  if (tid == 0) {
+    long long acc = 0;
+    for (int i = 0; i < nth; ++i) { long long v = part[i]; part[i] = acc; acc += v; }
+    off[npan] = acc;
+  }
+  __syncthreads();
+  long long acc = part[tid];
+  for (int i = a; i < b; ++i) { off[i] = acc; acc += cnt[(size_t)i * 8 + lev]; }
+}
+
+/* ===================================================================== */
+/* launchers                                                             */
+/* ===================================================================== */
+cudaError_t qol_launch_levels(const OrderTab& T, const PanelIn& P, const LevelWS& W, int npan, cudaStream_t st) {
+  size_t smem = sizeof(double) * 9 * T.hd;
+  k_panel_levels<<<npan, 256, smem, st>>>(T, P, W);
+  return cudaGetLastError();
+}
+cudaError_t qol_launch_classify(const OrderTab& T, const PairIn& Q, const LevelWS& W, const PairWS& G, int npan,
+                                cudaStream_t st) {
+  k_classify<<<npan, 128, 0, st>>>(T, Q, W, G);
+  return cudaGetLastError();
+}
+cudaError_t qol_launch_direct(const OrderTab& T, const PanelIn& P, const PairIn& Q, const LevelWS& W,
+                              const PairWS& G, const OutCOO& O, int npan, cudaStream_t st) {
+  dim3 grid(npan, T.nlevel);
+  if (T.hd <= 16) k_direct<16><<<grid, 256, 0, st>>>(T, P, Q, W, G, O);
+  else if (T.hd <= 32) k_direct<32><<<grid, 256, 0, st>>>(T, P, Q, W, G, O);
+  else if (T.hd <= 48) k_direct<48><<<grid, 256, 0, st>>>(T, P, Q, W, G, O);
+  else if (T.hd <= 72) k_direct<72><<<grid, 256, 0, st>>>(T, P, Q, W, G, O);
+  else if (T.hd <= 96) k_direct<96><<<grid, 256, 0, st>>>(T, P, Q, W, G, O);
+  else k_direct<136><<<grid, 256, 0, st>>>(T, P, Q, W, G, O);
+  return cudaGetLastError();
+}
+cudaError_t qol_launch_scan(int npan, int lev, const int* cnt, long long* off, cudaStream_t st) {
+  k_scan_rrq<<<1, 1024, 0, st>>>(npan, lev, cnt, off);
+  return cudaGetLastError();
+}
+cudaError_t qol_launch_rrq_panel(const OrderTab& T, const PanelIn& P, const PairWS& G, const RRQWS& R, int npan,
+                                 const double* chart, cudaStream_t st) {
+  k_rrq_panel<<<npan, 256, 0, st>>>(T, P, G, R, chart);
+  return cudaGetLastError();
+}
+cudaError_t qol_launch_rrq_target(const OrderTab& T, const PairIn& Q, const PairWS& G, const RRQWS& R, int exterior,
+                                  cudaStream_t st) {
+  if (R.nrrq == 0) return cudaSuccess;
+  long long nb = (R.nrrq + RRQ_WARPS - 1) / RRQ_WARPS;
+  k_rrq_target<<<(unsigned)nb, 32 * RRQ_WARPS, 0, st>>>(T, Q, G, R, exterior);
+  return cudaGetLastError();
+}
+cudaError_t qol_launch_rrq_apply(const OrderTab& T, const PanelIn& P, const PairIn& Q, const PairWS& G,
+                                 const RRQWS& R, const OutCOO& O, int npan, cudaStream_t st) {
+  size_t smem = sizeof(double) * (4 * T.hd + 2 * T.hd) * AT;
+  if (T.hd <= 48) k_rrq_apply<48><<<npan, 256, smem, st>>>(T, P, Q, G, R, O);
+  else {
+    cudaFuncSetAttribute(k_rrq_apply<136>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_rrq_apply<136><<<npan, 256, smem, st>>>(T, P, Q, G, R, O);
+  }
+  return cudaGetLastError();
+}
+cudaError_t qol_launch_coo_index(const OrderTab& T, const PairIn& Q, long long* si, long long* sj, int npan,
+                                 cudaStream_t st) {
+  k_coo_index<<<npan, 256, 0, st>>>(T, Q, si, sj);
+  return cudaGetLastError();
+}

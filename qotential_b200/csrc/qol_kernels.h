@@ -1,0 +1,83 @@
+/* Device-side views passed by value to the qol_b200 kernels. */
+#pragma once
+#include <cuda_runtime.h>
+
+#define RRQ_FRAME 16 /* R (9, rows e1,e2,e3 as R[i + 3*d]), c (3), alpha (1), pad */
+
+/* per-order tables (reference element, quadrature data), device pointers */
+struct OrderTab {
+  int korder, hd, nterms, orderff, nquad, nlevel, ng;
+  double dist;
+  int n[4], nsub[4];
+  const double* interp[4];    /* n_l x hd, row-major */
+  const double* wt[4];        /* n_l */
+  const long long* suboff[4]; /* nsub_l + 1 */
+  const int* subtyp[4];       /* nsub_l */
+  const double *tgl, *wgl, *Dgl, *Leg; /* nquad; nquad x nquad col-major */
+  const double *gl48x, *gl48w, *gl16x, *gl16w, *tq, *wq;
+  const double* Mb;    /* (3 nquad + 3) x hd, row-major: boundary + vertex interpolation */
+  const double* umatr; /* hd x hd col-major (vals -> coefs) */
+  const double* vruv;  /* 2 x hd VR nodes of degree korder */
+};
+
+/* panel geometry (reference layouts: sx(3,nsrc) etc.) */
+struct PanelIn {
+  const double *sx, *snx, *sw, *rts, *rps;
+};
+
+/* targets in CSR-by-panel form (1-based tcxrow/tcxi as in the reference) */
+struct PairIn {
+  const double* tcx;
+  const long long* tcxrow;
+  const long long* tcxi;
+};
+
+/* refined level geometry: per level, per panel, 7 x n_l SoA (x,y,z,nx,ny,nz,w)
+ * and per sub-patch (qx,qy,qz,qr2) */
+struct LevelWS {
+  double* node[4];
+  double* sub[4];
+};
+
+/* pair classification and per-panel grouping by level */
+struct PairWS {
+  signed char* level; /* ntcx: 1..nlevel, nlevel+1 = RRQ */
+  int* grp;           /* ntcx: local target ids grouped per panel by level */
+  int* cnt;           /* npan x 8 */
+  int* off;           /* npan x 8 */
+};
+
+/* RRQ workspace */
+struct RRQWS {
+  int npan, all_panels;
+  long long nrrq;
+  const long long* rrq_off; /* npan + 1 */
+  double *frame, *bx, *bt, *cf, *scf;
+  double *qmat, *hmat, *smat, *PD, *B;
+  int* perm;
+  double *JD, *RS; /* per RRQ pair: 4hd, hd */
+  double* ialpha;  /* per RRQ pair (nullable) */
+};
+
+/* output: COO values (block column-major per panel) */
+struct OutCOO {
+  double *vs, *vd;
+  double* omega; /* nullable: 4hd x m (qol_rrq single panel) */
+  int subtract_naive;
+};
+
+void qol_upload_harm_coefs(const double* hb, const double* hc, const double* hcm, cudaStream_t st);
+cudaError_t qol_launch_levels(const OrderTab& T, const PanelIn& P, const LevelWS& W, int npan, cudaStream_t st);
+cudaError_t qol_launch_classify(const OrderTab& T, const PairIn& Q, const LevelWS& W, const PairWS& G, int npan,
+                                cudaStream_t st);
+cudaError_t qol_launch_direct(const OrderTab& T, const PanelIn& P, const PairIn& Q, const LevelWS& W,
+                              const PairWS& G, const OutCOO& O, int npan, cudaStream_t st);
+cudaError_t qol_launch_scan(int npan, int lev, const int* cnt, long long* off, cudaStream_t st);
+cudaError_t qol_launch_rrq_panel(const OrderTab& T, const PanelIn& P, const PairWS& G, const RRQWS& R, int npan,
+                                 const double* chart, cudaStream_t st);
+cudaError_t qol_launch_rrq_target(const OrderTab& T, const PairIn& Q, const PairWS& G, const RRQWS& R, int exterior,
+                                  cudaStream_t st);
+cudaError_t qol_launch_rrq_apply(const OrderTab& T, const PanelIn& P, const PairIn& Q, const PairWS& G,
+                                 const RRQWS& R, const OutCOO& O, int npan, cudaStream_t st);
+cudaError_t qol_launch_coo_index(const OrderTab& T, const PairIn& Q, long long* si, long long* sj, int npan,
+                                 cudaStream_t st);

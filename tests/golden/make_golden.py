@@ -1,0 +1,50 @@
+"""Extract the golden vectors the tests use from the reference's frozen native
+fixtures (web/stellarator/fixtures/native/order{4,6}-direct.bin, format
+STGRF001: header + f64 arrays sx, snx, sw, ub, ubn, u, ...; see
+web/stellarator/test/native-direct-parity.py:41-97).
+
+Writes tests/golden/grf_order{4,6}.npz with u, ub, ubn, the GRF scalar, a
+strided subset of sx/snx/sw (every 7th node) and the SHA-256 of the full
+f64 sx/snx/sw arrays.  Run in a container that has the reference checkout:
+    python tests/golden/make_golden.py /root/reference
+"""
+import hashlib
+import os
+import struct
+import sys
+
+import numpy as np
+
+
+def load(path):
+    blob = open(path, "rb").read()
+    magic, ntri, nsrc, nrender, nfaces, grf = struct.unpack_from("<8s4qd", blob)
+    assert magic == b"STGRF001", magic
+    off = 48
+    out = dict(ntri=ntri, nsrc=nsrc, grf=grf)
+    for name, cnt in [("sx", 3 * nsrc), ("snx", 3 * nsrc), ("sw", nsrc), ("ub", nsrc), ("ubn", nsrc), ("u", nsrc)]:
+        out[name] = np.frombuffer(blob, dtype="<f8", count=cnt, offset=off).copy()
+        off += 8 * cnt
+    out["sha256"] = hashlib.sha256(blob).hexdigest()
+    return out
+
+
+def main():
+    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    here = os.path.dirname(os.path.abspath(__file__))
+    for order in (4, 6):
+        f = load(os.path.join(ref, "web/stellarator/fixtures/native", f"order{order}-direct.bin"))
+        sub = np.arange(0, f["nsrc"], 7)
+        np.savez_compressed(
+            os.path.join(here, f"grf_order{order}.npz"),
+            ntri=f["ntri"], nsrc=f["nsrc"], grf=f["grf"], u=f["u"], ub=f["ub"], ubn=f["ubn"],
+            sub=sub, sx_sub=f["sx"].reshape(-1, 3)[sub], snx_sub=f["snx"].reshape(-1, 3)[sub], sw_sub=f["sw"][sub],
+            sha_sx=hashlib.sha256(f["sx"].tobytes()).hexdigest(),
+            sha_snx=hashlib.sha256(f["snx"].tobytes()).hexdigest(),
+            sha_sw=hashlib.sha256(f["sw"].tobytes()).hexdigest(),
+            sha_bin=f["sha256"], mp=12, np_=36, order=order)
+        print(order, f["sha256"])
+
+
+if __name__ == "__main__":
+    main()

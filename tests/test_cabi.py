@@ -1,0 +1,86 @@
+"""C-ABI boundary (CPU): the library loads, exports every declared symbol,
+and validates arguments as the reference's gateway does; compute calls
+without a GPU fail loudly (no CPU path)."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    h = open(os.path.join(ROOT, "include", "qol_b200.h")).read()
+    h = re.sub(r"/\*.*?\*/", "", h, flags=re.S)   # declarations only, not comments
+    return sorted(set(re.findall(r"\b(qol_\w+)\s*\(", h)))
+
+
+def test_exports_every_declared_symbol(qol):
+    L = qol.lib()
+    syms = declared_symbols()
+    assert len(syms) >= 17
+    for s in syms:
+        assert hasattr(L, s), s
+
+
+def test_header_cites_reference(qol):
+    h = open(os.path.join(ROOT, "include", "qol_b200.h")).read()
+    for name in ("qol_getnearquad_lap_rrq", "qol_rrq", "qol_build_patch_levels", "qol_lap3dsdlpmat_levels"):
+        block = h[:h.index(f"int {name}(")]
+        assert "src/" in block[-900:], name
+
+
+def test_simplex_precomp_host_only(qol):
+    tgl, wgl, Dgl, wb, Leg, um, vm = qol.qol_simplex_precomp(8, 5)
+    assert np.allclose(um @ vm, np.eye(21), atol=1e-10)
+    with pytest.raises(qol.QolError) as e:
+        import ctypes as C
+        z = np.zeros(100)
+        rc = qol.lib().qol_simplex_precomp(C.c_longlong(8), C.c_longlong(5), C.c_longlong(20), *([C.c_void_p(z.ctypes.data)] * 7))
+        qol._check(rc)
+    assert e.value.code == 3
+
+
+def test_getnearquad_layout_errors(qol):
+    npan, nterms = 2, 3
+    hd = 6
+    sx = np.zeros((npan * hd, 3))
+    tcx = np.zeros((3, 3))
+    args = dict(npan=npan, nterms=nterms, hdim=hd, nquad=5, nsrc=npan * hd, sx=sx, snx=sx, sw=np.ones(npan * hd),
+                rts=sx, rps=sx, ntcx=3, tcx=tcx, tcxrow=np.array([1, 2, 3]), orderff=5, distff=1.4, iside=30)
+    with pytest.raises(qol.QolError) as e:
+        qol.qol_getnearquad_lap_rrq(tcxi=np.array([1, 3, 3]), **args)   # does not cover tcx
+    assert e.value.code == 1
+    with pytest.raises(qol.QolError) as e:
+        qol.qol_getnearquad_lap_rrq(tcxi=np.array([1, 3, 4]), nnz=5, **args)   # nnz too small
+    assert e.value.code == 2
+    with pytest.raises(qol.QolError) as e:
+        qol.qol_getnearquad_lap_rrq(tcxi=np.array([2, 3, 4]), **args)   # not one-based
+    assert e.value.code == 1
+    # the C entry point itself (not only the Python mirror) rejects bad layouts
+    import ctypes as C
+    xi = np.array([1, 4, 3], np.int64)
+    z = np.zeros(64); zi = np.zeros(64, np.int64); ti = np.zeros(20)
+    p = lambda a: C.c_void_p(a.ctypes.data)
+    L = C.c_longlong
+    rc = qol.lib().qol_getnearquad_lap_rrq(L(2), L(3), L(6), L(5), L(12), p(z), p(z), p(z), p(z), p(z), L(3), p(z),
+                                           p(zi), p(xi), L(5), C.c_double(1.4), L(30), L(0), L(18), p(zi), p(zi),
+                                           p(z), p(z), p(ti))
+    assert rc == 1
+
+
+def test_handle_errors_without_gpu(qol):
+    # bad handles are rejected before any device work
+    with pytest.raises(qol.QolError) as e:
+        qol.qol_clear_patch_levels(12345)
+    assert e.value.code == 2
+
+
+@pytest.mark.skipif(__import__("torch").cuda.is_available(), reason="checks the no-GPU behaviour")
+def test_no_cpu_fallback(qol):
+    from qotential_b200 import geometry as G
+    P = G.panels(G.torus(), 2, 3, 3, split=False)
+    with pytest.raises(qol.QolError) as e:
+        qol.qol_rrq(P["sx"][:3], P["sx"][:6], P["snx"][:6], P["sw"][:6], P["rts"][:6], P["rps"][:6], 3, 5, 5)
+    assert e.value.code == 5

@@ -1,0 +1,144 @@
+"""GPU parity: the CUDA path through the C ABI vs the oracle on the same
+inputs.  Tolerances: COO indices bit-exact; values relative to the largest
+magnitude of the compared block (rows are ill-conditioned moment solves, so
+rounding differences from a different summation order are amplified; the
+bounds below are the measured agreement with headroom)."""
+import numpy as np
+import pytest
+
+from conftest import grf_apply
+
+pytestmark = pytest.mark.gpu
+
+TOL_LEVEL = 1e-12     # level-resolved rows: direct sums + contraction
+TOL_RRQ = 1e-8        # RRQ rows: moment solves
+
+
+def _setup(G, surf, mp, np_, nterms, split=False, off=0, seed=1):
+    P = G.panels(surf, mp, np_, nterms, split=split)
+    hd = nterms * (nterms + 1) // 2
+    T = P["sx"]
+    if off:
+        T = np.concatenate([T, G.off_surface_targets(P, off, seed, hd)])
+    tcxi, tcxrow, tcx = G.near_lists(P["sx"], P["sw"], hd, targets=T)
+    return P, hd, tcxi, tcxrow, tcx, T
+
+
+def _compare(qol, orc, P, hd, nterms, tcxi, tcxrow, tcx):
+    npan = P["sw"].size // hd
+    nq = nterms + 2
+    si, sj, vs, vd, ti = qol.qol_getnearquad_lap_rrq(npan, nterms, hd, nq, npan * hd, P["sx"], P["snx"], P["sw"],
+                                                     P["rts"], P["rps"], tcxrow.size, tcx, tcxrow, tcxi, nq, 1.4, 30)
+    oi, oj, ovs, ovd, hist = orc.getnearquad(npan, nterms, nq, P["sx"], P["snx"], P["sw"], P["rts"], P["rps"], tcx,
+                                             tcxrow, tcxi, nq)
+    assert np.array_equal(si, oi) and np.array_equal(sj, oj)
+    return (vs, vd, ovs, ovd, hist, ti)
+
+
+@pytest.mark.parametrize("nterms", [4, 6])
+def test_getnearquad_torus(qol, orc, nterms):
+    from qotential_b200 import geometry as G
+    P, hd, tcxi, tcxrow, tcx, _ = _setup(G, G.torus(), 6, 12, nterms)
+    vs, vd, ovs, ovd, hist, ti = _compare(qol, orc, P, hd, nterms, tcxi, tcxrow, tcx)
+    assert hist[5] > 0 and hist[1] > 0
+    for a, b in ((vs, ovs), (vd, ovd)):
+        err = np.abs(a - b).max() / np.abs(b).max()
+        assert err < TOL_RRQ, err
+
+
+@pytest.mark.parametrize("nterms", [5, 8])
+def test_getnearquad_stellarator_offsurface(qol, orc, nterms):
+    from qotential_b200 import geometry as G
+    P, hd, tcxi, tcxrow, tcx, _ = _setup(G, G.stellarator(), 4, 10, nterms, off=300)
+    vs, vd, ovs, ovd, hist, ti = _compare(qol, orc, P, hd, nterms, tcxi, tcxrow, tcx)
+    # per-pair relative errors
+    npan = P["sw"].size // hd
+    for a, b in ((vs, ovs), (vd, ovd)):
+        err = np.abs(a - b).max() / np.abs(b).max()
+        assert err < TOL_RRQ, err
+
+
+def test_rrq_single_panel(qol, orc):
+    """qol_rrq (one panel, m targets: on-panel nodes, neighbours, off-surface
+    both sides down to 1e-6 of the panel size)"""
+    from qotential_b200 import geometry as G
+    nterms = 7
+    P = G.panels(G.stellarator(), 4, 10, nterms, split=False)
+    hd = nterms * (nterms + 1) // 2; k = 11
+    sl = slice(k * hd, (k + 1) * hd)
+    sx, snx, sw, rts, rps = (P[a][sl] for a in ("sx", "snx", "sw", "rts", "rps"))
+    diam = np.sqrt(sw.sum())
+    rng = np.random.default_rng(3)
+    tx = [sx, P["sx"][(k + 1) * hd:(k + 2) * hd]]
+    for d in (1e-6, 1e-3, 0.05, 0.3):
+        j = rng.integers(0, hd, 6)
+        tx.append(sx[j] + (d * diam * np.where(rng.random(6) < 0.5, -1, 1))[:, None] * snx[j])
+    tx = np.concatenate(tx)
+    As, Ad, Om, Ia, ti = qol.qol_rrq(tx, sx, snx, sw, rts, rps, nterms, nterms + 2, nterms + 2)
+    Bs, Bd, Om2, Ia2, lv = orc.rrq(tx, sx, snx, sw, rts, rps, nterms, nterms + 2, nterms + 2)
+    assert (lv == 5).sum() > 10
+    for a, b in ((As, Bs), (Ad, Bd)):
+        err = np.abs(a - b).max(1) / np.abs(b).max(1)
+        assert err.max() < TOL_RRQ, err
+    assert np.abs(Ia - Ia2).max() < 1e-11
+    rr = lv == 5
+    assert np.abs(Om[:, rr] - Om2[:, rr]).max() / np.abs(Om2[:, rr]).max() < TOL_RRQ
+    assert ti[:8].sum() > 0
+
+
+def test_patch_level_handles(qol, orc):
+    from qotential_b200 import geometry as G
+    nterms = 6
+    P = G.panels(G.torus(), 6, 12, nterms, split=False)
+    hd = nterms * (nterms + 1) // 2; k = 5
+    sl = slice(k * hd, (k + 1) * hd)
+    lv = qol.qol_build_patch_levels(nterms - 1, P["sx"][sl], P["rts"][sl], P["rps"][sl], nterms + 2, 1.4)
+    tx = P["sx"][(k - 3) * hd:(k + 4) * hd]
+    As, Ad, idxs, ms = qol.qol_lap3dsdlpmat_levels(tx, hd, lv)
+    Bs, Bd, bidx, lvl = orc.sdlpmat_levels(nterms - 1, P["sx"][sl], P["rts"][sl], P["rps"][sl], nterms + 2, 1.4, tx)
+    assert np.array_equal(idxs, bidx) and ms == len(bidx) and ms > 0
+    res = np.setdiff1d(np.arange(len(tx)), bidx - 1)
+    assert np.abs(As[res] - Bs[res]).max() / np.abs(Bs[res]).max() < TOL_LEVEL
+    assert np.abs(Ad[res] - Bd[res]).max() / np.abs(Bd[res]).max() < TOL_LEVEL
+    with pytest.raises(qol.QolError) as e:
+        qol.qol_lap3dsdlpmat_levels(tx, hd + 1, lv)
+    assert e.value.code == 3
+    qol.qol_clear_patch_levels(lv)
+    with pytest.raises(qol.QolError) as e:
+        qol.qol_lap3dsdlpmat_levels(tx, hd, lv)
+    assert e.value.code == 2
+
+
+def test_deterministic(qol):
+    """two runs produce identical bytes (native-direct-parity.py:127-128)"""
+    from qotential_b200 import geometry as G
+    nterms = 5
+    P, hd, tcxi, tcxrow, tcx, _ = _setup(G, G.torus(), 6, 12, nterms, off=100)
+    npan = P["sw"].size // hd
+    args = (npan, nterms, hd, nterms + 2, npan * hd, P["sx"], P["snx"], P["sw"], P["rts"], P["rps"], tcxrow.size, tcx,
+            tcxrow, tcxi, nterms + 2, 1.4, 30)
+    a = qol.qol_getnearquad_lap_rrq(*args)
+    b = qol.qol_getnearquad_lap_rrq(*args)
+    for x, y in zip(a[:4], b[:4]):
+        assert x.tobytes() == y.tobytes()
+
+
+def test_grf_identity_gpu(qol, orc):
+    """S[du/dn] - D[u] = 0 (exterior limit) on the torus for a harmonic u from
+    exterior point charges, with the GPU near corrections"""
+    from qotential_b200 import geometry as G
+    errs = []
+    for nterms in (4, 6, 8):
+        surf = G.torus()
+        P, hd, tcxi, tcxrow, tcx, _ = _setup(G, surf, 12, 24, nterms)
+        ys, q = G.point_charges(surf, 4, seed=7)
+        ub, ubn = G.harmonic_density(P["sx"], P["snx"], ys, q)
+        u = orc.direct_farfield(P["sx"], P["snx"], P["sw"], ub, ubn)
+        npan = P["sw"].size // hd
+        si, sj, vs, vd, _ = qol.qol_getnearquad_lap_rrq(npan, nterms, hd, nterms + 2, npan * hd, P["sx"], P["snx"],
+                                                        P["sw"], P["rts"], P["rps"], tcxrow.size, tcx, tcxrow, tcxi,
+                                                        nterms + 2, 1.4, 30)
+        un = grf_apply(u, si, sj, vs, vd, ub, ubn)
+        errs.append(np.abs(un).max() / np.abs(ubn).max())
+    # oracle on the same inputs: 4.1e-4, 9.0e-6, 8.8e-7
+    assert errs[0] < 1e-3 and errs[1] < 2e-5 and errs[2] < 2e-6, errs
