@@ -1,0 +1,320 @@
+"""Benchmark: near-pair evaluations/s of the RRQ near-field correction
+(qol_getnearquad_lap_rrq) on the order-12 stellarator.
+
+Workload (plain FP64 drop-in): stellarator R = 5 + cos p + 0.25 cos(p - 5t),
+Z = sin p - 0.25 sin(p - 5t), 16 x 80 quads -> 2560 triangles, order 12
+(Vioreanu-Rokhlin degree 12: nterms 13, hdim 91, nquad = orderff = 15);
+targets = all 232,960 surface nodes + 20,000 seeded off-surface points
+(normal offsets log-uniform in [1e-6, 1e-1] x local panel diameter); the near
+lists come from the reference driver's ball test (1.75 sqrt(panel area)).
+One step = one qol_getnearquad_lap_rrq over all panels.  Synthetic inputs,
+seeded.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+ORDER = 12
+MP, NP = 16, 80
+NOFF = 20000
+SEED = 2026
+
+
+def workload(rank=0, world=1):
+    from qotential_b200 import geometry as G
+    nterms = ORDER + 1
+    hd = nterms * (nterms + 1) // 2
+    P = G.panels(G.stellarator(), MP, NP, nterms, split=False)
+    off = G.off_surface_targets(P, NOFF, SEED, hd)
+    T = np.concatenate([P["sx"], off])
+    tcxi, tcxrow, tcx = G.near_lists(P["sx"], P["sw"], hd, targets=T)
+    npan = P["sw"].size // hd
+    a, b = (rank * npan) // world, ((rank + 1) * npan) // world
+    sl = slice(a * hd, b * hd)
+    lo, hi = tcxi[a] - 1, tcxi[b] - 1
+    W = dict(nterms=nterms, hd=hd, nquad=nterms + 2, npan=b - a, npan_total=npan,
+             sx=np.ascontiguousarray(P["sx"][sl]), snx=np.ascontiguousarray(P["snx"][sl]),
+             sw=np.ascontiguousarray(P["sw"][sl]), rts=np.ascontiguousarray(P["rts"][sl]),
+             rps=np.ascontiguousarray(P["rps"][sl]), tcx=np.ascontiguousarray(tcx[lo:hi]),
+             tcxrow=np.ascontiguousarray(tcxrow[lo:hi]), tcxi=np.ascontiguousarray(tcxi[a:b + 1] - lo),
+             pairs_total=int(tcxrow.size))
+    W["pairs"] = int(W["tcxrow"].size)
+    return W
+
+
+def config_dict(W, world):
+    return {"workload": f"stellarator {MP}x{NP} quads ({W['npan_total']} triangles), order {ORDER} "
+                        f"(nterms {W['nterms']}, hdim {W['hd']}, nquad=orderff {W['nquad']}), "
+                        f"{W['npan_total'] * W['hd']} surface-node + {NOFF} off-surface targets",
+            "near_pairs": W["pairs_total"], "seed": SEED, "form": "plain FP64 drop-in",
+            "l2": "no flush: per-step inputs+workspace+outputs (> 8 GB) exceed the 126 MB L2",
+            "parallelism": f"panel shards x{world}" if world > 1 else "1 GPU"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+    FIELDS = ["clocks.sm", "clocks.max.sm", "clocks_event_reasons.hw_slowdown",
+              "clocks_event_reasons.hw_thermal_slowdown", "clocks_event_reasons.sw_thermal_slowdown",
+              "clocks_event_reasons.sw_power_cap"]
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + ",".join(self.FIELDS),
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 6:
+                continue
+            try:
+                sm.append(float(f[0])); mx.append(float(f[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[2:6]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_sample(W, budget_s=15.0, nthreads=0):
+    """The oracle (CPU restatement, OpenMP over panels) on a bounded sample of
+    the same workload: leading panels until about budget_s of work."""
+    import oracle
+    if not os.path.exists(os.path.join(ROOT, "oracle", "liborc.so")):
+        oracle.build()
+    hd = W["hd"]
+    tot_pairs, tot_t, k0, chunk = 0, 0.0, 0, 4
+    while tot_t < budget_s and k0 < W["npan"]:
+        k1 = min(W["npan"], k0 + chunk)
+        lo, hi = W["tcxi"][k0] - 1, W["tcxi"][k1] - 1
+        xi = W["tcxi"][k0:k1 + 1] - lo
+        sl = slice(k0 * hd, k1 * hd)
+        t0 = time.perf_counter()
+        oracle.getnearquad(k1 - k0, W["nterms"], W["nquad"], W["sx"][sl], W["snx"][sl], W["sw"][sl], W["rts"][sl],
+                           W["rps"][sl], W["tcx"][lo:hi], W["tcxrow"][lo:hi], xi, W["nquad"], nthreads=nthreads)
+        tot_t += time.perf_counter() - t0
+        tot_pairs += int(hi - lo)
+        k0 = k1
+        chunk *= 2
+    return tot_pairs, tot_t, k0
+
+
+def run_reference(args):
+    """--impl reference: the reference's algorithm on the host cores (the
+    oracle port; the Fortran reference cannot be built here)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    W = workload(0, 1)
+    nthr = os.cpu_count() or 1
+    per_step = []
+    pairs_step = None
+    for s in range(args.warmup + args.steps):
+        p, t, k = cpu_sample(W, budget_s=6.0, nthreads=nthr)
+        if s >= args.warmup:
+            per_step.append((p, t))
+            pairs_step = p
+    pairs = sum(p for p, _ in per_step)
+    t = sum(t for _, t in per_step)
+    v = pairs / t
+    line = {"metric": "near-pair evals/s", "value": v, "unit": "pairs/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t / max(1, args.steps), "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": config_dict(W, 1),
+            "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": nthr, "kind": "port",
+                             "sample": f"{pairs_step} near pairs (leading panels, ~6 s of CPU work) per step, "
+                                       f"OpenMP over panels on {nthr} threads"},
+            "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--kernels-only", action="store_true",
+                    help="only the warm-up and timed steps (for profiler launch lists)")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import qotential_b200 as qol
+    from qotential_b200 import _build
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    _build.build()
+    L = qol.lib()
+    W = workload(rank, world)
+    dev = torch.device("cuda", local)
+    t = lambda a, dt=torch.float64: torch.as_tensor(a, dtype=dt).to(dev)
+    D = {k: t(W[k]) for k in ("sx", "snx", "sw", "rts", "rps", "tcx")}
+    D["tcxrow"] = t(W["tcxrow"], torch.int64)
+    D["tcxi"] = t(W["tcxi"], torch.int64)
+    nnz = W["pairs"] * W["hd"]
+    out = (torch.empty(nnz, dtype=torch.int64, device=dev), torch.empty(nnz, dtype=torch.int64, device=dev),
+           torch.empty(nnz, dtype=torch.float64, device=dev), torch.empty(nnz, dtype=torch.float64, device=dev))
+    stream = torch.cuda.Stream(dev)   # an explicit stream: the events and the library share it
+    torch.cuda.set_stream(stream)
+
+    def step(hist=False):
+        return qol.qol_getnearquad_lap_rrq_dev(W["npan"], W["nterms"], W["nquad"], D["sx"], D["snx"], D["sw"],
+                                               D["rts"], D["rps"], D["tcx"], D["tcxrow"], D["tcxi"], W["nquad"], 1.4,
+                                               30, out, stream=stream.cuda_stream, sync=False, want_hist=hist)
+
+    hist = step(hist=True)
+    for _ in range(max(0, args.warmup - 1)):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    if dist:
+        tt = torch.tensor([ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+        dist.barrier()
+    pairs_total = W["pairs_total"]
+    value = pairs_total / (ms * 1e-3)
+    if args.kernels_only:
+        if rank == 0:
+            print(json.dumps({"metric": "near-pair evals/s", "value": value, "ms_per_step": ms,
+                              "steps": args.steps, "note": "kernels-only run"}))
+        if dist:
+            dist.destroy_process_group()
+        return 0
+
+    # per-kernel device times of one more (untimed) step, for the roofline
+    import ctypes as C
+    ms7 = np.zeros(7); calls = np.zeros(1, np.int64)
+    L.qol_kernel_times(C.c_int(1), None, None)
+    step()
+    torch.cuda.synchronize()
+    L.qol_kernel_times(C.c_int(-1), C.c_void_p(ms7.ctypes.data), C.c_void_p(calls.ctypes.data))
+    L.qol_kernel_times(C.c_int(0), None, None)
+    names = ["levels", "classify", "direct", "rrq_panel", "rrq_target", "rrq_apply", "coo_index"]
+    peak = C.c_double(0.0)
+    L.qol_probe_fp64_peak(C.byref(peak))
+    hd, nq = W["hd"], W["nquad"]
+    n4 = np.zeros(4, np.int64); s4 = np.zeros(4, np.int64)
+    L.qol_level_sizes(C.c_longlong(W["nterms"]), C.c_longlong(W["nquad"]), C.c_void_p(n4.ctypes.data),
+                      C.c_void_p(s4.ctypes.data))
+    nl = [int(x) for x in n4]
+    flops_direct = sum(int(hist[l + 1]) * nl[l] * (20 + 4 * hd) for l in range(4))
+    nbd, ncoeff = 3 * nq, (W["nterms"] + 1) * (W["nterms"] + 2) // 2
+    flops_rrq_alg = int(hist[5]) * (48 * nbd * ncoeff + 2 * (4 * hd) ** 2 + 4 * hd * hd)
+    k_share = {n: float(v) for n, v in zip(names, ms7)}
+    dom = max(k_share, key=k_share.get)
+    if dom == "direct":
+        ach = flops_direct / (k_share["direct"] * 1e-3) / 1e12
+        rl_note = "k_direct: sum over level-resolved pairs of (20 + 4 hdim) x n_level FLOPs"
+    else:
+        ach = flops_rrq_alg / ((k_share["rrq_target"] + k_share["rrq_apply"]) * 1e-3) / 1e12
+        rl_note = ("RRQ kernels (moments + solves): per RRQ pair 48 nbd ncoeff + 2 (4 hdim)^2 + 4 hdim^2 FLOPs "
+                   "(the reference's a8 + a10 counts)")
+    roofline = {"bound": "fp64", "achieved": ach, "peak": peak.value, "unit": "TFLOP/s",
+                "frac": ach / peak.value if peak.value else None, "traffic": None, "kernel": dom,
+                "peak_source": "measured: in-library FP64 FMA probe (MEASURED_PEAKS.json has no FP64 figure)",
+                "flops": rl_note,
+                "kernel_ms": k_share, "level_hist": [int(x) for x in hist[1:6]]}
+
+    # end to end through the public host-pointer API
+    e2e = None
+    if rank == 0:
+        h_in = (W["sx"], W["snx"], W["sw"], W["rts"], W["rps"], W["tcx"], W["tcxrow"], W["tcxi"])
+        h2d = sum(a.nbytes for a in h_in)
+        d2h = nnz * 32
+        reps = min(2, args.steps)
+        times = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            r = qol.qol_getnearquad_lap_rrq(W["npan"], W["nterms"], hd, nq, W["npan"] * hd, W["sx"], W["snx"],
+                                            W["sw"], W["rts"], W["rps"], W["pairs"], W["tcx"], W["tcxrow"],
+                                            W["tcxi"], nq, 1.4, 30)
+            times.append(time.perf_counter() - t0)
+            del r
+        e2e = {"value": W["pairs"] / min(times), "unit": "pairs/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "note": "qol_getnearquad_lap_rrq with host (numpy) buffers, "
+                                                        "including the COO output copy to the host"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        nthr = os.cpu_count() or 1
+        p, tcpu, kk = cpu_sample(W, budget_s=15.0, nthreads=nthr)
+        cpu = {"value": p / tcpu, "unit": "pairs/s", "cores": nthr, "kind": "port",
+               "sample": f"{p} near pairs of the leading {kk} panels of the same workload, oracle (C++ restatement, "
+                         f"OpenMP over panels) on {nthr} threads, {tcpu:.1f} s"}
+    if rank == 0:
+        line = {"metric": "near-pair evals/s", "value": value, "unit": "pairs/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": config_dict(W, world), "clocks": clocks, "e2e": e2e,
+                "gpu_launches": 8 * args.steps, "roofline": roofline, "cpu_baseline": cpu}
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -110,9 +110,24 @@ int qol_getnearquad_lap_rrq_dev(qol_int npan, qol_int nterms, qol_int hdim, qol_
                                 qol_int nnz, qol_int* sparsei, qol_int* sparsej, double* sparsevs,
                                 double* sparsevd, void* stream, int sync, qol_int* level_hist);
 
-/* Library status and diagnostics. */
+/* Library status and diagnostics.  qol_kernel_times: when enabled, every
+ * pipeline call records CUDA events on its stream around its phases and
+ * accumulates the device milliseconds: [0] refined levels, [1] classification,
+ * [2] level sums, [3] per-panel RRQ precompute, [4] per-pair RRQ moments,
+ * [5] RRQ solves + COO values, [6] COO indices.  Returns the sums and the
+ * call count; enable >= 0 resets them and sets the switch (-1: read only).
+ * (No counterpart in the reference; its timeinfo is the host-side analogue.) */
 const char* qol_last_error(void);
+int qol_kernel_times(int enable, double* ms7, qol_int* calls);
 int qol_version(void);
+/* FP64 FMA throughput of this GPU in TFLOP/s (best of 5 timed launches of
+ * independent FMA chains on every SM); the roofline denominator for the FP64
+ * kernels.  No counterpart in the reference. */
+int qol_probe_fp64_peak(double* tflops);
+/* Node and sub-patch counts of the four refined levels for one order
+ * (build_patch_ref_r64, src/patch_refine_mod.f90:100-262, square regroup on).
+ * Host only. */
+int qol_level_sizes(qol_int nterms, qol_int orderff, qol_int* n4, qol_int* nsub4);
 
 /* Link-compatibility aliases for the reference's Fortran symbols (one
  * trailing underscore, all arguments by reference, matlab/qotential_mex.c

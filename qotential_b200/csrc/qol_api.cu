@@ -83,6 +83,10 @@ struct OrderCache {
 std::map<long long, std::unique_ptr<OrderCache>> g_orders;
 bool g_coefs_uploaded = false;
 Arena g_arena, g_arena2;
+/* per-phase device milliseconds of the pipeline (diagnostics) */
+int g_ktime_on = 0;
+double g_ktime[7] = {0, 0, 0, 0, 0, 0, 0};
+long long g_kcalls = 0;
 cudaStream_t g_stream = nullptr;
 
 int ensure_device() {
@@ -245,7 +249,7 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
   CK(cudaMemsetAsync(G.cnt, 0, sizeof(int) * (size_t)npan * 8, st));
   CK(cudaMemsetAsync(G.off, 0, sizeof(int) * (size_t)npan * 8, st));
   Timing tm;
-  if (timeinfo) {
+  if (timeinfo || g_ktime_on) {
     for (int i = 0; i < 8; ++i) CK(cudaEventCreate(&tm.ev[i]));
     tm.on = true;
   }
@@ -302,11 +306,15 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
   if (tm.on) {
     float ms[7];
     for (int i = 0; i < 7; ++i) cudaEventElapsedTime(&ms[i], tm.ev[i], tm.ev[i + 1]);
-    timeinfo[0] += 1e-3 * ms[0];            /* patch levels */
-    timeinfo[1] += 1e-3 * ms[3];            /* per-panel RRQ precompute */
-    timeinfo[2] += 1e-3 * (ms[1] + ms[2]);  /* classification + level sums */
-    timeinfo[5] += 1e-3 * ms[4];            /* fused SSQ / solid angle / moments */
-    timeinfo[7] += 1e-3 * (ms[5] + ms[6]);  /* solves + COO */
+    if (timeinfo) {
+      timeinfo[0] += 1e-3 * ms[0];            /* patch levels */
+      timeinfo[1] += 1e-3 * ms[3];            /* per-panel RRQ precompute */
+      timeinfo[2] += 1e-3 * (ms[1] + ms[2]);  /* classification + level sums */
+      timeinfo[5] += 1e-3 * ms[4];            /* fused SSQ / solid angle / moments */
+      timeinfo[7] += 1e-3 * (ms[5] + ms[6]);  /* solves + COO */
+    }
+    for (int i = 0; i < 7; ++i) g_ktime[i] += ms[i];
+    g_kcalls += 1;
     for (int i = 0; i < 8; ++i) cudaEventDestroy(tm.ev[i]);
   }
   return 0;
@@ -358,7 +366,59 @@ int tables_match(int nquad, int korder, const double* tgl, const double* wgl, co
 extern "C" {
 
 const char* qol_last_error(void) { return g_err.c_str(); }
+
+int qol_kernel_times(int enable, double* ms7, qol_int* calls) {
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  if (ms7) for (int i = 0; i < 7; ++i) ms7[i] = g_ktime[i];
+  if (calls) *calls = g_kcalls;
+  if (enable >= 0) {
+    g_ktime_on = enable;
+    for (int i = 0; i < 7; ++i) g_ktime[i] = 0.0;
+    g_kcalls = 0;
+  }
+  return 0;
+}
 int qol_version(void) { return 100; }
+
+int qol_level_sizes(qol_int nterms, qol_int orderff, qol_int* n4, qol_int* nsub4) {
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  qolh::RefElem R;
+  try {
+    qolh::build_ref((int)nterms - 1, (int)orderff, 4, true, R);
+  } catch (const std::exception& e) {
+    return fail(QOL_ERR_ORDER, "reference element: %s", e.what());
+  }
+  for (int l = 0; l < 4; ++l) { n4[l] = R.lev[l].n; nsub4[l] = R.lev[l].nsub; }
+  return 0;
+}
+
+int qol_probe_fp64_peak(double* tflops) {
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  int rc = ensure_device();
+  if (rc) return rc;
+  int dev = 0, nsm = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  double* out = nullptr;
+  const int blocks = nsm * 8, iters = 1 << 16;
+  CK(cudaMalloc(&out, sizeof(double) * blocks));
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a)); CK(cudaEventCreate(&b));
+  double best = 0.0;
+  for (int rep = 0; rep < 6; ++rep) {
+    CK(cudaEventRecord(a, g_stream));
+    CK(qol_launch_fp64_peak(out, blocks, iters, g_stream));
+    CK(cudaEventRecord(b, g_stream));
+    CK(cudaEventSynchronize(b));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, a, b));
+    double fl = 2.0 * 8.0 * (double)iters * blocks * 256.0;
+    if (rep > 0) best = std::max(best, fl / (ms * 1e-3) / 1e12);
+  }
+  cudaEventDestroy(a); cudaEventDestroy(b); cudaFree(out);
+  *tflops = best;
+  return 0;
+}
 
 int qol_simplex_precomp(qol_int nquad, qol_int korder, qol_int kpols, double* tgl, double* wgl, double* Dgl,
                         double* w_bclag, double* Legmat, double* umatr, double* vmatr) {
@@ -506,7 +566,7 @@ int qol_getnearquad_lap_rrq_dev(qol_int npan, qol_int nterms, qol_int hdim, qol_
   std::lock_guard<std::recursive_mutex> g(g_mu);
   int rc = ensure_device();
   if (rc) return rc;
-  cudaStream_t st = stream ? (cudaStream_t)stream : g_stream;
+  cudaStream_t st = (cudaStream_t)stream; /* 0 = the legacy default stream */
   std::vector<long long> xi(npan + 1);
   CK(cudaMemcpyAsync(xi.data(), tcxi, sizeof(long long) * (npan + 1), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));

@@ -993,3 +993,22 @@ cudaError_t qol_launch_coo_index(const OrderTab& T, const PairIn& Q, long long* 
   k_coo_index<<<npan, 256, 0, st>>>(T, Q, si, sj);
   return cudaGetLastError();
 }
+
+/* ===================================================================== */
+/* FP64 FMA throughput probe (roofline denominator for the FP64 kernels)  */
+/* ===================================================================== */
+__global__ void __launch_bounds__(256) k_fp64_peak(double* out, int iters, double a, double b) {
+  double x0 = threadIdx.x * 1e-3, x1 = x0 + 1.0, x2 = x0 + 2.0, x3 = x0 + 3.0;
+  double x4 = x0 + 4.0, x5 = x0 + 5.0, x6 = x0 + 6.0, x7 = x0 + 7.0;
+  for (int i = 0; i < iters; ++i) {
+    x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b); x3 = fma(x3, a, b);
+    x4 = fma(x4, a, b); x5 = fma(x5, a, b); x6 = fma(x6, a, b); x7 = fma(x7, a, b);
+  }
+  double s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+  if (s == 12345.678) out[blockIdx.x] = s; /* keep the chains alive */
+}
+
+cudaError_t qol_launch_fp64_peak(double* out, int blocks, int iters, cudaStream_t st) {
+  k_fp64_peak<<<blocks, 256, 0, st>>>(out, iters, 0.999999999, 1e-9);
+  return cudaGetLastError();
+}

@@ -81,3 +81,4 @@ cudaError_t qol_launch_rrq_apply(const OrderTab& T, const PanelIn& P, const Pair
                                  const RRQWS& R, const OutCOO& O, int npan, cudaStream_t st);
 cudaError_t qol_launch_coo_index(const OrderTab& T, const PairIn& Q, long long* si, long long* sj, int npan,
                                  cudaStream_t st);
+cudaError_t qol_launch_fp64_peak(double* out, int blocks, int iters, cudaStream_t st);
