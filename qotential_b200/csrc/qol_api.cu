@@ -214,7 +214,7 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
   for (int l = 0; l < 4; ++l) { add(sizeof(double) * (size_t)npan * T.n[l] * 7); add(sizeof(double) * (size_t)npan * T.nsub[l] * 4); }
   add(ntcx); add(sizeof(int) * ntcx); add(sizeof(int) * (size_t)npan * 8 * 2);
   add(sizeof(long long) * (npan + 1));
-  add(sizeof(double) * (size_t)npan * (RRQ_FRAME + 6 * nbd + 9 * nq + 3 * hd));
+  add(sizeof(double) * (size_t)npan * (RRQ_FRAME + 6 * nbd + 9 * nq + 6 * hd));
   add(sizeof(double) * (size_t)npan * hd * hd * 11);
   add(sizeof(int) * (size_t)npan * 272);
   rc = g_arena.reserve(need + 4096);
@@ -239,6 +239,7 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
   R.bt = g_arena.take<double>((size_t)npan * 3 * nbd);
   R.cf = g_arena.take<double>((size_t)npan * 9 * nq);
   R.scf = g_arena.take<double>((size_t)npan * 3 * hd);
+  R.sxf = g_arena.take<double>((size_t)npan * 3 * hd);
   R.qmat = g_arena.take<double>((size_t)npan * 4 * hd * hd);
   R.hmat = g_arena.take<double>((size_t)npan * hd * hd);
   R.smat = g_arena.take<double>((size_t)npan * hd * hd);

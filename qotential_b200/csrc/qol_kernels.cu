@@ -450,6 +450,11 @@ __global__ void __launch_bounds__(256) k_rrq_panel(OrderTab T, PanelIn P, PairWS
     }
     scf[d * hd + k] = s;
   }
+  for (int j = threadIdx.x; j < hd; j += blockDim.x) {
+    double y[3];
+    tofr(&s_sx[3 * j], y);
+    for (int d = 0; d < 3; ++d) R.sxf[(size_t)pan * 3 * hd + 3 * j + d] = y[d];
+  }
   __syncthreads();
   /* in-place Gauss-Jordan inverse of the quaternion matrix V (row pivoting,
    * pivot by quaternion norm), then of Msl^T (real) */
@@ -578,65 +583,157 @@ __global__ void __launch_bounds__(256) k_rrq_panel(OrderTab T, PanelIn P, PairWS
 /* ===================================================================== */
 /* K5: per-pair RRQ moments, one warp per pair                           */
 /* ===================================================================== */
-#define RRQ_WARPS 2
+#define RRQ_WARPS 4
 struct WarpSM {
-  double xt[3];
   double w1[3 * QOL_MAXNQ], w3[3 * QOL_MAXNQ];
-  double root[3][2];
-  int rok[3];
   double cD[3 * 3 * QOL_MAXNQ], cS[3 * 3 * QOL_MAXNQ];
   double br[3][112];
   int nbr[3];
-  int outside;
-  double Omega, sdir;
 };
 
-__device__ double panel_height(const OrderTab& T, const double* scf, const double* xt, double* pols, int* inside) {
-  const int hd = T.hd, korder = T.korder;
-  /* nearest node in plane among the VR nodes, Newton on (u,v) */
-  int ib = 0; double best = 1e300;
-  for (int j = 0; j < hd; ++j) {
-    koorn_pols_dev(T.vruv[2 * j], T.vruv[2 * j + 1], korder, pols);
-    double f0 = 0, f1 = 0;
-    for (int k = 0; k < hd; ++k) { f0 += pols[k] * scf[k]; f1 += pols[k] * scf[hd + k]; }
-    double d0 = f0 - xt[0], d1 = f1 - xt[1];
-    if (d0 * d0 + d1 * d1 < best) { best = d0 * d0 + d1 * d1; ib = j; }
+/* warp-cooperative surface evaluation for the side test: f[c*3+p] = sum_k
+ * pols_k(point p) scf[c*hd+k] for the coordinates c = x,y,z and the points
+ * (u,v), (u+h,v), (u,v+h).  Lane a evaluates the polynomials (a, b),
+ * b = 0..korder-a, i.e. L_a(s,t) P_b^{(2a+1,0)}(z) (the host basis). */
+__device__ void koorn_eval3_warp(int korder, int hd, const double* scf, double u, double v, double h,
+                                 double* f /* 9 */) {
+  const int lane = threadIdx.x & 31;
+  double acc[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) acc[i] = 0.0;
+  if (lane <= korder) {
+    const int a = lane;
+    const double us[3] = {u, u + h, u}, vs[3] = {v, v, v + h};
+#pragma unroll
+    for (int p = 0; p < 3; ++p) {
+      double s = 2.0 * us[p] + vs[p] - 1.0, t = 1.0 - vs[p], z = 2.0 * vs[p] - 1.0;
+      double L0 = 1.0, L1 = s, La = 1.0;
+      if (a >= 1) La = s;
+      for (int q = 1; q < a; ++q) {
+        double L2 = ((2.0 * q + 1.0) * s * L1 - q * t * t * L0) / (q + 1.0);
+        L0 = L1; L1 = L2; La = L2;
+      }
+      double alpha = 2.0 * a + 1.0;
+      double p0 = 1.0, p1 = 0.5 * (alpha + 2.0) * z + 0.5 * alpha;
+      for (int b = 0; b <= korder - a; ++b) {
+        double pb;
+        if (b == 0) pb = p0;
+        else if (b == 1) pb = p1;
+        else {
+          double jj = b;
+          double c1 = 2.0 * jj * (jj + alpha) * (2.0 * jj + alpha - 2.0);
+          double c2 = (2.0 * jj + alpha - 1.0) * (alpha * alpha);
+          double c3 = (2.0 * jj + alpha - 2.0) * (2.0 * jj + alpha - 1.0) * (2.0 * jj + alpha);
+          double c4 = 2.0 * (jj + alpha - 1.0) * (jj - 1.0) * (2.0 * jj + alpha);
+          double p2 = ((c2 + c3 * z) * p1 - c4 * p0) / c1;
+          p0 = p1; p1 = p2; pb = p2;
+        }
+        int deg = a + b, idx = deg * (deg + 1) / 2 + b;
+        double val = La * pb;
+        acc[0 * 3 + p] += val * scf[idx];
+        acc[1 * 3 + p] += val * scf[hd + idx];
+        acc[2 * 3 + p] += val * scf[2 * hd + idx];
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    double x = acc[i];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    f[i] = x;
+  }
+}
+
+/* height of the target above the panel surface at its in-plane position and
+ * whether that position lies inside the triangle (warp-cooperative) */
+__device__ double panel_height_warp(const OrderTab& T, const double* scf, const double* sxf, const double* xt,
+                                    int* inside) {
+  const int hd = T.hd, lane = threadIdx.x & 31;
+  double best = 1e300;
+  int ib = hd;
+  for (int j = lane; j < hd; j += 32) {
+    double d0 = sxf[3 * j] - xt[0], d1 = sxf[3 * j + 1] - xt[1], d2 = d0 * d0 + d1 * d1;
+    if (d2 < best) { best = d2; ib = j; }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    double b2 = __shfl_xor_sync(0xffffffffu, best, o);
+    int i2 = __shfl_xor_sync(0xffffffffu, ib, o);
+    if (b2 < best || (b2 == best && i2 < ib)) { best = b2; ib = i2; }
   }
   double u = T.vruv[2 * ib], v = T.vruv[2 * ib + 1];
+  double f[9];
+  const double h = 1e-7;
   for (int it = 0; it < 40; ++it) {
-    const double h = 1e-7;
-    double f0 = 0, f1 = 0, fu0 = 0, fu1 = 0, fv0 = 0, fv1 = 0;
-    koorn_pols_dev(u, v, korder, pols);
-    for (int k = 0; k < hd; ++k) { f0 += pols[k] * scf[k]; f1 += pols[k] * scf[hd + k]; }
-    koorn_pols_dev(u + h, v, korder, pols);
-    for (int k = 0; k < hd; ++k) { fu0 += pols[k] * scf[k]; fu1 += pols[k] * scf[hd + k]; }
-    koorn_pols_dev(u, v + h, korder, pols);
-    for (int k = 0; k < hd; ++k) { fv0 += pols[k] * scf[k]; fv1 += pols[k] * scf[hd + k]; }
-    double J00 = (fu0 - f0) / h, J10 = (fu1 - f1) / h, J01 = (fv0 - f0) / h, J11 = (fv1 - f1) / h;
-    double r0 = f0 - xt[0], r1 = f1 - xt[1];
+    koorn_eval3_warp(T.korder, hd, scf, u, v, h, f);
+    double J00 = (f[1] - f[0]) / h, J10 = (f[4] - f[3]) / h, J01 = (f[2] - f[0]) / h, J11 = (f[5] - f[3]) / h;
+    double r0 = f[0] - xt[0], r1 = f[3] - xt[1];
     double det = J00 * J11 - J01 * J10;
     if (det == 0.0) break;
     double du = (J11 * r0 - J01 * r1) / det, dv = (-J10 * r0 + J00 * r1) / det;
     u -= du; v -= dv;
     if (fabs(du) + fabs(dv) < 1e-14) break;
   }
-  koorn_pols_dev(u, v, korder, pols);
-  double zs = 0.0;
-  for (int k = 0; k < hd; ++k) zs += pols[k] * scf[2 * hd + k];
+  koorn_eval3_warp(T.korder, hd, scf, u, v, 0.0, f);
   const double tol = 1e-10;
   *inside = (u >= -tol && v >= -tol && u + v <= 1.0 + tol) ? 1 : 0;
-  return xt[2] - zs;
+  return xt[2] - f[6];
 }
 
-__global__ void __launch_bounds__(32 * RRQ_WARPS) k_rrq_target(OrderTab T, PairIn Q, PairWS G, RRQWS R,
+/* column m of the sin-type solid harmonics, real recurrences on the
+ * imaginary parts (the column recurrence has real coefficients), calling
+ * f(j, h, gx, gy, gz) for l = m + j, j = 0..L-m.  hb/hc: recurrence
+ * coefficients in shared memory (lanes index different m). */
+template <int LB, class F>
+__device__ __forceinline__ void harm_column_re(int L, int m, double x, double y, double z, const double* hb,
+                                               const double* hc, F f) {
+  const double X = y, Y = z, Z = x;
+  const double r2 = X * X + Y * Y + Z * Z;
+  /* diagonal S_m^m = C_m (X+iY)^m and its derivative in w = X+iY */
+  double pr = 1.0, pi = 0.0, dr = 0.0, di = 0.0;
+  for (int mm = 1; mm <= m; ++mm) {
+    double cm = hc[(QOL_MAXL + 2) * (QOL_MAXL + 2) + mm];
+    double nr = cm * (X * pr - Y * pi), ni = cm * (X * pi + Y * pr);
+    double ndr = cm * (pr + (X * dr - Y * di)), ndi = cm * (pi + (X * di + Y * dr));
+    pr = nr; pi = ni; dr = ndr; di = ndi;
+  }
+  /* Im parts: value, d/dX = Im dS, d/dY = Im(i dS) = Re dS, d/dZ = 0 */
+  double s1 = pi, s1x = di, s1y = dr, s1z = 0.0;
+  double s2 = 0.0, s2x = 0.0, s2y = 0.0, s2z = 0.0;
+  f(0, s1, s1z, s1x, s1y);
+#pragma unroll
+  for (int j = 1; j < LB; ++j) {
+    const int l = m + j;
+    if (l <= L) {
+      const double a = 2.0 * l - 1.0, b = hb[l * (QOL_MAXL + 2) + m], c = hc[l * (QOL_MAXL + 2) + m];
+      const double aZ = a * Z, br2 = b * r2;
+      double s = (aZ * s1 - br2 * s2) * c;
+      double sx = (aZ * s1x - b * (2.0 * X * s2 + r2 * s2x)) * c;
+      double sy = (aZ * s1y - b * (2.0 * Y * s2 + r2 * s2y)) * c;
+      double sz = (a * (s1 + Z * s1z) - b * (2.0 * Z * s2 + r2 * s2z)) * c;
+      s2 = s1; s2x = s1x; s2y = s1y; s2z = s1z;
+      s1 = s; s1x = sx; s1y = sy; s1z = sz;
+      f(j, s, sz, sx, sy);
+    }
+  }
+}
+
+template <int LB>
+__global__ void __launch_bounds__(32 * RRQ_WARPS, 2) k_rrq_target(OrderTab T, PairIn Q, PairWS G, RRQWS R,
                                                               int exterior) {
   __shared__ WarpSM S[RRQ_WARPS];
-  __shared__ double accs[RRQ_WARPS][2][5 * 136];
+  __shared__ double s_h[2 * (QOL_MAXL + 2) * (QOL_MAXL + 2) + (QOL_MAXL + 2)];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int e = threadIdx.x; e < (QOL_MAXL + 2) * (QOL_MAXL + 2); e += blockDim.x) {
+    s_h[e] = c_hb[e / (QOL_MAXL + 2)][e % (QOL_MAXL + 2)];
+    s_h[(QOL_MAXL + 2) * (QOL_MAXL + 2) + e] = c_hc[e / (QOL_MAXL + 2)][e % (QOL_MAXL + 2)];
+  }
+  for (int e = threadIdx.x; e < QOL_MAXL + 2; e += blockDim.x) s_h[2 * (QOL_MAXL + 2) * (QOL_MAXL + 2) + e] = c_hcm[e];
+  __syncthreads();
+  const double* hb = s_h;
+  const double* hc = s_h + (QOL_MAXL + 2) * (QOL_MAXL + 2); /* hc[(QOL_MAXL+2)^2 + m] is c_m */
   const long long gidx = (long long)blockIdx.x * RRQ_WARPS + wid;
   if (gidx >= R.nrrq) return;
   WarpSM& W = S[wid];
-  /* panel of this RRQ pair: binary search in the per-panel RRQ offsets */
   int lo = 0, hi = R.npan;
   while (hi - lo > 1) {
     int mid = (lo + hi) >> 1;
@@ -652,21 +749,19 @@ __global__ void __launch_bounds__(32 * RRQ_WARPS) k_rrq_target(OrderTab T, PairI
   const double* bt = R.bt + (size_t)pan * 3 * nbd;
   const double* cf = R.cf + (size_t)pan * 9 * nq;
   const double alpha = fr[12];
-  if (lane == 0) {
+  double xt[3];
+  {
     const double* x = Q.tcx + 3 * (p0 + tl);
     double d0 = x[0] - fr[9], d1 = x[1] - fr[10], d2 = x[2] - fr[11];
-    for (int i = 0; i < 3; ++i) W.xt[i] = alpha * (fr[i] * d0 + fr[i + 3] * d1 + fr[i + 6] * d2);
+    for (int i = 0; i < 3; ++i) xt[i] = alpha * (fr[i] * d0 + fr[i + 3] * d1 + fr[i + 6] * d2);
   }
-  __syncwarp();
-  const double xt0 = W.xt[0], xt1 = W.xt[1], xt2 = W.xt[2];
-  /* singularity-swap weights, one lane per edge */
+  const double xt0 = xt[0], xt1 = xt[1], xt2 = xt[2];
+  /* singularity-swap weights and graded breakpoints, one lane per edge */
   if (lane < 3) {
     const int e = lane;
     cd t0 = mk(0.0, 0.0);
-    bool ok = edge_root_dev(nq, cf + e * 3 * nq, T.tgl, bx + 3 * e * nq, W.xt, t0);
+    bool ok = edge_root_dev(nq, cf + e * 3 * nq, T.tgl, bx + 3 * e * nq, xt, t0);
     ssq_weights_dev(nq, T.tgl, T.wgl, ok, t0, T.gl48x, T.gl48w, &W.w1[e * nq], &W.w3[e * nq]);
-    W.root[e][0] = t0.re; W.root[e][1] = t0.im; W.rok[e] = ok ? 1 : 0;
-    /* graded breakpoints for the solid angle on this edge */
     double ts = 0.0, dd = 2.0;
     if (ok) { ts = fmin(1.0, fmax(-1.0, t0.re)); dd = fmax(fabs(t0.im), 1e-15); }
     double left[54], right[54];
@@ -686,39 +781,36 @@ __global__ void __launch_bounds__(32 * RRQ_WARPS) k_rrq_target(OrderTab T, PairI
     W.br[e][c++] = 1.0;
     W.nbr[e] = c;
   }
-  /* Dirac-string direction (lane 3 side test; clearance over the lanes) */
-  if (lane == 3) {
-    double pols[136];
-    int inside = 1;
-    double hgt = panel_height(T, R.scf + (size_t)pan * 3 * hd, W.xt, pols, &inside);
-    int side = fabs(hgt) <= 1e-12 ? 0 : (hgt > 0 ? 1 : -1);
-    W.sdir = side == 0 ? (exterior ? 1.0 : -1.0) : (double)side;
-    W.outside = inside ? 0 : 1; /* projects outside the triangle */
-  }
-  __syncwarp();
-  if (W.outside) {
-    /* both directions avoid the panel: take the one passing farther from
-     * the boundary, min over 32 samples per edge of (r - s.rho)/r */
-    double cu = 2.0, cdn = 2.0;
-    for (int pnt = lane; pnt < 96; pnt += 32) {
-      int e = pnt >> 5, q = pnt & 31;
-      double t = -1.0 + (2.0 * q + 1.0) / 32.0, y[3], yp[3];
-      for (int d = 0; d < 3; ++d) leg_eval_r(nq, cf + e * 3 * nq + d * nq, t, y[d], yp[d]);
-      double rho[3] = {y[0] - xt0, y[1] - xt1, y[2] - xt2};
-      double r = sqrt(dot3(rho, rho));
-      cu = fmin(cu, (r - rho[2]) / r);
-      cdn = fmin(cdn, (r + rho[2]) / r);
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-      cu = fmin(cu, __shfl_xor_sync(0xffffffffu, cu, o));
-      cdn = fmin(cdn, __shfl_xor_sync(0xffffffffu, cdn, o));
-    }
-    if (lane == 0) W.sdir = cu >= cdn ? 1.0 : -1.0;
-  }
-  __syncwarp();
-  /* solid angle: points of the graded meshes over lanes */
+  /* Dirac-string direction: away from the panel when the target projects
+   * inside the triangle; otherwise the one passing farther from the boundary */
+  double sdir;
   {
-    const double sdir = W.sdir;
+    int inside = 1;
+    double hgt = panel_height_warp(T, R.scf + (size_t)pan * 3 * hd, R.sxf + (size_t)pan * 3 * hd, xt, &inside);
+    int side = fabs(hgt) <= 1e-12 ? 0 : (hgt > 0 ? 1 : -1);
+    sdir = side == 0 ? (exterior ? 1.0 : -1.0) : (double)side;
+    if (!inside) {
+      double cu = 2.0, cdn = 2.0;
+      for (int pnt = lane; pnt < 96; pnt += 32) {
+        int e = pnt >> 5, q = pnt & 31;
+        double t = -1.0 + (2.0 * q + 1.0) / 32.0, y[3], yp[3];
+        for (int d = 0; d < 3; ++d) leg_eval_r(nq, cf + e * 3 * nq + d * nq, t, y[d], yp[d]);
+        double rho[3] = {y[0] - xt0, y[1] - xt1, y[2] - xt2};
+        double r = sqrt(dot3(rho, rho));
+        cu = fmin(cu, (r - rho[2]) / r);
+        cdn = fmin(cdn, (r + rho[2]) / r);
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        cu = fmin(cu, __shfl_xor_sync(0xffffffffu, cu, o));
+        cdn = fmin(cdn, __shfl_xor_sync(0xffffffffu, cdn, o));
+      }
+      sdir = cu >= cdn ? 1.0 : -1.0;
+    }
+  }
+  __syncwarp();
+  /* solid angle: points of the graded meshes over the lanes */
+  double Omega;
+  {
     double tot = 0.0;
     for (int e = 0; e < 3; ++e) {
       const int nint = W.nbr[e] - 1;
@@ -739,7 +831,7 @@ __global__ void __launch_bounds__(32 * RRQ_WARPS) k_rrq_target(OrderTab T, PairI
       }
     }
     for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
-    if (lane == 0) W.Omega = tot;
+    Omega = tot;
   }
   /* per boundary node weights (1/4pi folded in) */
   const double i4p = 1.0 / (4.0 * QOL_PI);
@@ -762,57 +854,56 @@ __global__ void __launch_bounds__(32 * RRQ_WARPS) k_rrq_target(OrderTab T, PairI
   for (int d = 0; d < 3; ++d)
     for (int o = 16; o > 0; o >>= 1) lint[d] += __shfl_xor_sync(0xffffffffu, lint[d], o);
   __syncwarp();
-  /* accumulation over the segment points: half-warp per point, lane = column m */
+  /* segment points: half-warp per point, lane = column m, accumulators in
+   * registers (entry l = m + j of column m in acc[j]) */
   const int half = lane >> 4, m = (lane & 15) + 1;
-  double* acc = accs[wid][half];
-  for (int e = lane; e < 2 * 5 * hd; e += 32) accs[wid][e / (5 * hd)][e % (5 * hd)] = 0.0;
-  __syncwarp();
+  double acc[LB][5];
+#pragma unroll
+  for (int j = 0; j < LB; ++j)
+#pragma unroll
+    for (int c = 0; c < 5; ++c) acc[j][c] = 0.0;
   double sumcD[3] = {0, 0, 0};
   const int npts = nbd * ng;
   for (int p = half; p < npts; p += 2) {
     const int i = p / ng, g = p % ng;
     const double t = T.tq[g], aD = T.wq[g] / t, aS = T.wq[g];
-    const double uD[3] = {aD * W.cD[3 * i], aD * W.cD[3 * i + 1], aD * W.cD[3 * i + 2]};
-    const double uS[3] = {aS * W.cS[3 * i], aS * W.cS[3 * i + 1], aS * W.cS[3 * i + 2]};
-    if (m == 1) { sumcD[0] += uD[0]; sumcD[1] += uD[1]; sumcD[2] += uD[2]; }
+    const double uD0 = aD * W.cD[3 * i], uD1 = aD * W.cD[3 * i + 1], uD2 = aD * W.cD[3 * i + 2];
+    const double uS0 = aS * W.cS[3 * i], uS1 = aS * W.cS[3 * i + 1], uS2 = aS * W.cS[3 * i + 2];
+    if (m == 1) { sumcD[0] += uD0; sumcD[1] += uD1; sumcD[2] += uD2; }
     if (m <= L) {
       const double* y = bx + 3 * i;
       const double z0 = xt0 + t * (y[0] - xt0), z1 = xt1 + t * (y[1] - xt1), z2 = xt2 + t * (y[2] - xt2);
-      harm_column(L, m, z0, z1, z2, [&](int l, int k, double h, double gx, double gy, double gz) {
-        double* a = acc + 5 * k;
-        a[0] += -(uD[0] * gx + uD[1] * gy + uD[2] * gz);
-        a[1] += uD[1] * gz - uD[2] * gy;
-        a[2] += uD[2] * gx - uD[0] * gz;
-        a[3] += uD[0] * gy - uD[1] * gx;
-        a[4] += uS[0] * gx + uS[1] * gy + uS[2] * gz;
+      harm_column_re<LB>(L, m, z0, z1, z2, hb, hc, [&](int j, double h, double gx, double gy, double gz) {
+        acc[j][0] -= uD0 * gx + uD1 * gy + uD2 * gz;
+        acc[j][1] += uD1 * gz - uD2 * gy;
+        acc[j][2] += uD2 * gx - uD0 * gz;
+        acc[j][3] += uD0 * gy - uD1 * gx;
+        acc[j][4] += uS0 * gx + uS1 * gy + uS2 * gz;
       });
     }
   }
-  /* total sum of the D segment weights: lanes with m == 1 hold partials (one per half) */
+  /* combine the two half-warps (same column m, different points) */
+#pragma unroll
+  for (int j = 0; j < LB; ++j)
+#pragma unroll
+    for (int c = 0; c < 5; ++c) acc[j][c] += __shfl_xor_sync(0xffffffffu, acc[j][c], 16);
   for (int d = 0; d < 3; ++d) {
     sumcD[d] += __shfl_xor_sync(0xffffffffu, sumcD[d], 16);
     sumcD[d] = __shfl_sync(0xffffffffu, sumcD[d], 0);
   }
-  __syncwarp();
   /* the x point: (s0, l/4pi - sumcD) (x) (0, grad h(x)) and h(x) Omega/4pi */
-  const double Omega = W.Omega;
   const double s0 = -Omega * i4p;
-  const double wv[3] = {lint[0] * i4p - sumcD[0], lint[1] * i4p - sumcD[1], lint[2] * i4p - sumcD[2]};
+  const double wv0 = lint[0] * i4p - sumcD[0], wv1 = lint[1] * i4p - sumcD[1], wv2 = lint[2] * i4p - sumcD[2];
   double* JD = R.JD + (size_t)gidx * 4 * hd;
   double* RS = R.RS + (size_t)gidx * hd;
   if (half == 0 && m <= L) {
-    const double* a0 = accs[wid][0];
-    const double* a1 = accs[wid][1];
-    harm_column(L, m, xt0, xt1, xt2, [&](int l, int k, double h, double gx, double gy, double gz) {
-      double q0 = -(wv[0] * gx + wv[1] * gy + wv[2] * gz);
-      double q1 = s0 * gx + (wv[1] * gz - wv[2] * gy);
-      double q2 = s0 * gy + (wv[2] * gx - wv[0] * gz);
-      double q3 = s0 * gz + (wv[0] * gy - wv[1] * gx);
-      JD[0 * hd + k] = a0[5 * k + 0] + a1[5 * k + 0] + q0;
-      JD[1 * hd + k] = a0[5 * k + 1] + a1[5 * k + 1] + q1;
-      JD[2 * hd + k] = a0[5 * k + 2] + a1[5 * k + 2] + q2;
-      JD[3 * hd + k] = a0[5 * k + 3] + a1[5 * k + 3] + q3;
-      RS[k] = a0[5 * k + 4] + a1[5 * k + 4] + h * Omega * i4p;
+    harm_column_re<LB>(L, m, xt0, xt1, xt2, hb, hc, [&](int j, double h, double gx, double gy, double gz) {
+      const int l = m + j, k = l * (l - 1) / 2 + (m - 1);
+      JD[0 * hd + k] = acc[j][0] - (wv0 * gx + wv1 * gy + wv2 * gz);
+      JD[1 * hd + k] = acc[j][1] + s0 * gx + (wv1 * gz - wv2 * gy);
+      JD[2 * hd + k] = acc[j][2] + s0 * gy + (wv2 * gx - wv0 * gz);
+      JD[3 * hd + k] = acc[j][3] + s0 * gz + (wv0 * gy - wv1 * gx);
+      RS[k] = acc[j][4] + h * Omega * i4p;
     });
   }
   if (lane == 0 && R.ialpha) R.ialpha[tl] = Omega; /* single-panel calls (qol_rrq) */
@@ -975,7 +1066,12 @@ cudaError_t qol_launch_rrq_target(const OrderTab& T, const PairIn& Q, const Pair
                                   cudaStream_t st) {
   if (R.nrrq == 0) return cudaSuccess;
   long long nb = (R.nrrq + RRQ_WARPS - 1) / RRQ_WARPS;
-  k_rrq_target<<<(unsigned)nb, 32 * RRQ_WARPS, 0, st>>>(T, Q, G, R, exterior);
+  if (T.nterms <= 4) k_rrq_target<4><<<(unsigned)nb, 32 * RRQ_WARPS, 0, st>>>(T, Q, G, R, exterior);
+  else if (T.nterms <= 6) k_rrq_target<6><<<(unsigned)nb, 32 * RRQ_WARPS, 0, st>>>(T, Q, G, R, exterior);
+  else if (T.nterms <= 8) k_rrq_target<8><<<(unsigned)nb, 32 * RRQ_WARPS, 0, st>>>(T, Q, G, R, exterior);
+  else if (T.nterms <= 10) k_rrq_target<10><<<(unsigned)nb, 32 * RRQ_WARPS, 0, st>>>(T, Q, G, R, exterior);
+  else if (T.nterms <= 13) k_rrq_target<13><<<(unsigned)nb, 32 * RRQ_WARPS, 0, st>>>(T, Q, G, R, exterior);
+  else k_rrq_target<16><<<(unsigned)nb, 32 * RRQ_WARPS, 0, st>>>(T, Q, G, R, exterior);
   return cudaGetLastError();
 }
 cudaError_t qol_launch_rrq_apply(const OrderTab& T, const PanelIn& P, const PairIn& Q, const PairWS& G,

@@ -52,7 +52,7 @@ struct RRQWS {
   int npan, all_panels;
   long long nrrq;
   const long long* rrq_off; /* npan + 1 */
-  double *frame, *bx, *bt, *cf, *scf;
+  double *frame, *bx, *bt, *cf, *scf, *sxf;
   double *qmat, *hmat, *smat, *PD, *B;
   int* perm;
   double *JD, *RS; /* per RRQ pair: 4hd, hd */
