@@ -32,7 +32,7 @@ NOFF = 20000
 SEED = 2026
 
 
-def workload(rank=0, world=1):
+def workload(rank=0, world=1, panels=0):
     from qotential_b200 import geometry as G
     nterms = ORDER + 1
     hd = nterms * (nterms + 1) // 2
@@ -41,6 +41,9 @@ def workload(rank=0, world=1):
     T = np.concatenate([P["sx"], off])
     tcxi, tcxrow, tcx = G.near_lists(P["sx"], P["sw"], hd, targets=T)
     npan = P["sw"].size // hd
+    if panels:  # a leading slice of the same workload (profiling captures)
+        npan = min(npan, panels)
+        tcxrow = tcxrow[:tcxi[npan] - 1]
     a, b = (rank * npan) // world, ((rank + 1) * npan) // world
     sl = slice(a * hd, b * hd)
     lo, hi = tcxi[a] - 1, tcxi[b] - 1
@@ -173,6 +176,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--panels", type=int, default=0, help="use only the leading N panels (profiling)")
     ap.add_argument("--kernels-only", action="store_true",
                     help="only the warm-up and timed steps (for profiler launch lists)")
     args = ap.parse_args()
@@ -193,7 +197,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     _build.build()
     L = qol.lib()
-    W = workload(rank, world)
+    W = workload(rank, world, args.panels)
     dev = torch.device("cuda", local)
     t = lambda a, dt=torch.float64: torch.as_tensor(a, dtype=dt).to(dev)
     D = {k: t(W[k]) for k in ("sx", "snx", "sw", "rts", "rps", "tcx")}
