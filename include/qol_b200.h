@@ -35,7 +35,8 @@ enum {
   QOL_ERR_CUDA = 5,
   QOL_ERR_ORDER = 6,
   QOL_ERR_TABLES = 7,
-  QOL_ERR_ARG = 8
+  QOL_ERR_ARG = 8,
+  QOL_ERR_LIMIT = 9
 };
 
 /* Replaces qol_simplex_precomp_mex (src/lap3d_close_mex.f90:48-59; body
@@ -109,6 +110,30 @@ int qol_getnearquad_lap_rrq_dev(qol_int npan, qol_int nterms, qol_int hdim, qol_
                                 const qol_int* tcxi, qol_int orderff, double distff, qol_int iside,
                                 qol_int nnz, qol_int* sparsei, qol_int* sparsej, double* sparsevs,
                                 double* sparsevd, void* stream, int sync, qol_int* level_hist);
+
+/* No counterpart in the reference.  The work of qol_rrq for one panel (As, Ad;
+ * no Omega/IalphaAsvestas/timeinfo) for callers that cannot allocate GPU
+ * memory: codes inside a host application that owns all GPU memory through its
+ * own pool (a cudaMalloc there fails under the pool's cap or fragments it) and
+ * codes on a latency-critical path where cudaMalloc's implicit device-wide
+ * synchronisation is not allowed.  Allocates no GPU memory: all workspace and
+ * the per-order tables live in one static device array of 16 MiB, held by
+ * every GPU that loads the library until exit.  Every array argument is a
+ * device pointer; work is queued on `stream` (0 = the legacy default stream)
+ * with one host synchronisation inside.
+ *  - The first call on a device sets up (takes the array's device address with
+ *    cudaGetSymbolAddress, uploads constants); make that first call before
+ *    any stream capture.  A call with a new (order, orderff, nquad) re-uploads
+ *    the tables into the array.
+ *  - Calls share the array: calls that overlap on the GPU (other streams, other
+ *    host threads' work still running) race.  Serialize them.
+ *  - Limit: the tables plus 5*hdim doubles per target must fit in 16 MiB
+ *    (order 12, orderff 15: about 2,500 targets per call); larger requests
+ *    return QOL_ERR_LIMIT (9) with a message from qol_noalloc_last_error(). */
+int qol_rrq_noalloc(qol_int m, const double* tx, qol_int n, const double* sx, const double* snx,
+                    const double* sw, const double* rts, const double* rps, qol_int order, qol_int nquad,
+                    qol_int orderff, double distff, qol_int exterior, double* As, double* Ad, void* stream);
+const char* qol_noalloc_last_error(void);
 
 /* Library status and diagnostics.  qol_kernel_times: when enabled, every
  * pipeline call records CUDA events on its stream around its phases and
