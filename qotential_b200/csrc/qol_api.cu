@@ -265,11 +265,14 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
   CK(cudaStreamSynchronize(st));
   R.nrrq = nrrq;
   /* per-pair RRQ moment storage (separate arena: its size is known only now) */
-  rc = g_arena2.reserve(sizeof(double) * (size_t)std::max<long long>(nrrq, 1) * 5 * hd + 1024);
+  rc = g_arena2.reserve(sizeof(double) * (size_t)std::max<long long>(nrrq, 1) * (5 * hd + 6 * nbd + 4 + 3 * (2 * nq + 3)) +
+                        4096);
   if (rc) return rc;
   g_arena2.reset();
   R.JD = g_arena2.take<double>((size_t)std::max<long long>(nrrq, 1) * 4 * hd);
   R.RS = g_arena2.take<double>((size_t)std::max<long long>(nrrq, 1) * hd);
+  R.line = g_arena2.take<double>((size_t)std::max<long long>(nrrq, 1) * (6 * nbd + 4));
+  R.edge = g_arena2.take<double>((size_t)std::max<long long>(nrrq, 1) * 3 * (2 * nq + 3));
   OutCOO O{};
   O.vs = J.vs; O.vd = J.vd; O.omega = J.omega; O.subtract_naive = J.subtract_naive;
   rec(2);

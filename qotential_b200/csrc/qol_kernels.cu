@@ -8,7 +8,9 @@
  *   k_rrq_panel      per-panel RRQ precompute (lap3d_close_mod.f90:472-620,
  *                    843-863): frame, boundary, harmonic basis, inverse of the
  *                    quaternion system and of the S system
- *   k_rrq_target     per-pair RRQ moments (:789-841), one warp per pair
+ *   k_rrq_geom       per-pair SSQ weights, string direction, solid angle,
+ *                    boundary weights (:789-832), one warp per pair
+ *   k_rrq_moments    per-pair harmonic moments (:832-841), one warp per pair
  *   k_rrq_apply      the two solves as per-panel matrix products (:843-870)
  *   k_coo_index      COO row/column indices (:948-956)
  */
@@ -586,7 +588,6 @@ __global__ void __launch_bounds__(256) k_rrq_panel(OrderTab T, PanelIn P, PairWS
 #define RRQ_WARPS 4
 struct WarpSM {
   double w1[3 * QOL_MAXNQ], w3[3 * QOL_MAXNQ];
-  double cD[3 * 3 * QOL_MAXNQ], cS[3 * 3 * QOL_MAXNQ];
   double br[3][112];
   int nbr[3];
 };
@@ -717,20 +718,89 @@ __device__ __forceinline__ void harm_column_re(int L, int m, double x, double y,
   }
 }
 
-template <int LB>
-__global__ void __launch_bounds__(32 * RRQ_WARPS, 2) k_rrq_target(OrderTab T, PairIn Q, PairWS G, RRQWS R,
-                                                              int exterior) {
-  __shared__ WarpSM S[RRQ_WARPS];
-  __shared__ double s_h[2 * (QOL_MAXL + 2) * (QOL_MAXL + 2) + (QOL_MAXL + 2)];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (int e = threadIdx.x; e < (QOL_MAXL + 2) * (QOL_MAXL + 2); e += blockDim.x) {
-    s_h[e] = c_hb[e / (QOL_MAXL + 2)][e % (QOL_MAXL + 2)];
-    s_h[(QOL_MAXL + 2) * (QOL_MAXL + 2) + e] = c_hc[e / (QOL_MAXL + 2)][e % (QOL_MAXL + 2)];
+/* the column pair (m1, m2) of one lane: entries e = 0..n1-1 are column m1
+ * (l = m1 + e), e = n1..n1+n2-1 column m2 (l = m2 + e - n1); the diagonal
+ * chain runs to max(m1, m2) once.  Same recurrences as harm_column_re. */
+template <int LB, class F>
+__device__ __forceinline__ void harm_pair_re(int L, int m1, int m2, int n1, int n2, double x, double y, double z,
+                                             const double* hb, const double* hc, F f) {
+  const double X = y, Y = z, Z = x;
+  const double r2 = X * X + Y * Y + Z * Z;
+  double pr = 1.0, pi = 0.0, dr = 0.0, di = 0.0;
+  double a_pi = 0.0, a_di = 0.0, a_dr = 0.0; /* diagonal of column m1 */
+  const int mtop = n2 > 0 ? m2 : m1;
+  for (int mm = 1; mm <= mtop; ++mm) {
+    double cm = hc[(QOL_MAXL + 2) * (QOL_MAXL + 2) + mm];
+    double nr = cm * (X * pr - Y * pi), ni = cm * (X * pi + Y * pr);
+    double ndr = cm * (pr + (X * dr - Y * di)), ndi = cm * (pi + (X * di + Y * dr));
+    pr = nr; pi = ni; dr = ndr; di = ndi;
+    if (mm == m1) { a_pi = pi; a_di = di; a_dr = dr; }
   }
-  for (int e = threadIdx.x; e < QOL_MAXL + 2; e += blockDim.x) s_h[2 * (QOL_MAXL + 2) * (QOL_MAXL + 2) + e] = c_hcm[e];
-  __syncthreads();
-  const double* hb = s_h;
-  const double* hc = s_h + (QOL_MAXL + 2) * (QOL_MAXL + 2); /* hc[(QOL_MAXL+2)^2 + m] is c_m */
+  double s1 = a_pi, s1x = a_di, s1y = a_dr, s1z = 0.0;
+  double s2 = 0.0, s2x = 0.0, s2y = 0.0, s2z = 0.0;
+  int m = m1, l = m1;
+#pragma unroll
+  for (int e = 0; e <= LB; ++e) {
+    if (e < n1 + n2) {
+      if (e == n1) { /* start column m2 from its diagonal */
+        m = m2; l = m2;
+        s1 = pi; s1x = di; s1y = dr; s1z = 0.0;
+        s2 = 0.0; s2x = 0.0; s2y = 0.0; s2z = 0.0;
+      } else if (e > 0) {
+        ++l;
+        const double a = 2.0 * l - 1.0, b = hb[l * (QOL_MAXL + 2) + m], c = hc[l * (QOL_MAXL + 2) + m];
+        const double aZ = a * Z, br2 = b * r2;
+        double s = (aZ * s1 - br2 * s2) * c;
+        double sx = (aZ * s1x - b * (2.0 * X * s2 + r2 * s2x)) * c;
+        double sy = (aZ * s1y - b * (2.0 * Y * s2 + r2 * s2y)) * c;
+        double sz = (a * (s1 + Z * s1z) - b * (2.0 * Z * s2 + r2 * s2z)) * c;
+        s2 = s1; s2x = s1x; s2y = s1y; s2z = s1z;
+        s1 = s; s1x = sx; s1y = sy; s1z = sz;
+      }
+      f(e, s1, s1z, s1x, s1y);
+    }
+  }
+}
+
+/* singularity-swap root and modified weights, one thread per (RRQ pair,
+ * edge): writes w1 (nq), w3 (nq), ok, Re t0, Im t0 to the pair's edge record */
+__global__ void __launch_bounds__(128) k_rrq_ssq(OrderTab T, PairIn Q, PairWS G, RRQWS R) {
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= 3 * R.nrrq) return;
+  const long long gidx = tid / 3;
+  const int e = (int)(tid % 3);
+  int lo = 0, hi = R.npan;
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (R.rrq_off[mid] <= gidx) lo = mid; else hi = mid;
+  }
+  const int pan = lo;
+  const int j_loc = (int)(gidx - R.rrq_off[pan]);
+  const long long p0 = Q.tcxi[pan] - 1;
+  const int tl = G.grp[p0 + G.off[(size_t)pan * 8 + T.nlevel + 1] + j_loc];
+  const int nq = T.nquad, nbd = 3 * nq;
+  const double* fr = R.frame + (size_t)pan * RRQ_FRAME;
+  const double* bx = R.bx + (size_t)pan * 3 * nbd;
+  const double* cf = R.cf + (size_t)pan * 9 * nq;
+  const double alpha = fr[12];
+  double xt[3];
+  {
+    const double* x = Q.tcx + 3 * (p0 + tl);
+    double d0 = x[0] - fr[9], d1 = x[1] - fr[10], d2 = x[2] - fr[11];
+    for (int i = 0; i < 3; ++i) xt[i] = alpha * (fr[i] * d0 + fr[i + 3] * d1 + fr[i + 6] * d2);
+  }
+  double* er = R.edge + ((size_t)gidx * 3 + e) * (2 * nq + 3);
+  cd t0 = mk(0.0, 0.0);
+  bool ok = edge_root_dev(nq, cf + e * 3 * nq, T.tgl, bx + 3 * e * nq, xt, t0);
+  ssq_weights_dev(nq, T.tgl, T.wgl, ok, t0, T.gl48x, T.gl48w, er, er + nq);
+  er[2 * nq] = ok ? 1.0 : 0.0;
+  er[2 * nq + 1] = t0.re;
+  er[2 * nq + 2] = t0.im;
+}
+
+__global__ void __launch_bounds__(32 * RRQ_WARPS) k_rrq_geom(OrderTab T, PairIn Q, PairWS G, RRQWS R, int exterior) {
+  __shared__ WarpSM S[RRQ_WARPS];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const long long gidx = (long long)blockIdx.x * RRQ_WARPS + wid;
   if (gidx >= R.nrrq) return;
   WarpSM& W = S[wid];
@@ -756,12 +826,14 @@ __global__ void __launch_bounds__(32 * RRQ_WARPS, 2) k_rrq_target(OrderTab T, Pa
     for (int i = 0; i < 3; ++i) xt[i] = alpha * (fr[i] * d0 + fr[i + 3] * d1 + fr[i + 6] * d2);
   }
   const double xt0 = xt[0], xt1 = xt[1], xt2 = xt[2];
-  /* singularity-swap weights and graded breakpoints, one lane per edge */
+  /* singularity-swap weights (from k_rrq_ssq) and graded breakpoints, one
+   * lane per edge */
   if (lane < 3) {
     const int e = lane;
-    cd t0 = mk(0.0, 0.0);
-    bool ok = edge_root_dev(nq, cf + e * 3 * nq, T.tgl, bx + 3 * e * nq, xt, t0);
-    ssq_weights_dev(nq, T.tgl, T.wgl, ok, t0, T.gl48x, T.gl48w, &W.w1[e * nq], &W.w3[e * nq]);
+    const double* er = R.edge + ((size_t)gidx * 3 + e) * (2 * nq + 3);
+    for (int q = 0; q < nq; ++q) { W.w1[e * nq + q] = er[q]; W.w3[e * nq + q] = er[nq + q]; }
+    const bool ok = er[2 * nq] != 0.0;
+    const cd t0 = mk(er[2 * nq + 1], er[2 * nq + 2]);
     double ts = 0.0, dd = 2.0;
     if (ok) { ts = fmin(1.0, fmax(-1.0, t0.re)); dd = fmax(fabs(t0.im), 1e-15); }
     double left[54], right[54];
@@ -833,8 +905,10 @@ __global__ void __launch_bounds__(32 * RRQ_WARPS, 2) k_rrq_target(OrderTab T, Pa
     for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
     Omega = tot;
   }
-  /* per boundary node weights (1/4pi folded in) */
+  /* per boundary node weights (1/4pi folded in), written with the solid
+   * angle to the pair's line record: cD (3 nbd), cS (3 nbd), lint (3), Omega */
   const double i4p = 1.0 / (4.0 * QOL_PI);
+  double* rec = R.line + (size_t)gidx * (6 * nbd + 4);
   double lint[3] = {0, 0, 0};
   for (int i = lane; i < nbd; i += 32) {
     const double* y = bx + 3 * i;
@@ -846,67 +920,180 @@ __global__ void __launch_bounds__(32 * RRQ_WARPS, 2) k_rrq_target(OrderTab T, Pa
     cross3(rho, rxy, rrx);
     double f1 = W.w1[i] / r, f3 = W.w3[i] / (r * r * r);
     for (int d = 0; d < 3; ++d) {
-      W.cD[3 * i + d] = f3 * rrx[d] * i4p;
-      W.cS[3 * i + d] = f1 * rxy[d] * i4p;
+      rec[3 * i + d] = f3 * rrx[d] * i4p;
+      rec[3 * nbd + 3 * i + d] = f1 * rxy[d] * i4p;
       lint[d] += f1 * yp[d];
     }
   }
   for (int d = 0; d < 3; ++d)
     for (int o = 16; o > 0; o >>= 1) lint[d] += __shfl_xor_sync(0xffffffffu, lint[d], o);
-  __syncwarp();
-  /* segment points: half-warp per point, lane = column m, accumulators in
-   * registers (entry l = m + j of column m in acc[j]) */
-  const int half = lane >> 4, m = (lane & 15) + 1;
-  double acc[LB][5];
+  if (lane == 0) {
+    rec[6 * nbd + 0] = lint[0]; rec[6 * nbd + 1] = lint[1]; rec[6 * nbd + 2] = lint[2];
+    rec[6 * nbd + 3] = Omega;
+    if (R.ialpha) R.ialpha[tl] = Omega; /* single-panel calls (qol_rrq) */
+  }
+}
+
+/* the same column pair at two points in lockstep (two independent
+ * recurrence chains per lane); f(e, hA, gA.., hB, gB..) */
+template <int LB, class F>
+__device__ __forceinline__ void harm_pair_re2(int L, int m1, int m2, int n1, int n2, const double* xa,
+                                              const double* xb, const double* hb, const double* hc, F f) {
+  const double XA = xa[1], YA = xa[2], ZA = xa[0], XB = xb[1], YB = xb[2], ZB = xb[0];
+  const double r2A = XA * XA + YA * YA + ZA * ZA, r2B = XB * XB + YB * YB + ZB * ZB;
+  double prA = 1.0, piA = 0.0, drA = 0.0, diA = 0.0, prB = 1.0, piB = 0.0, drB = 0.0, diB = 0.0;
+  double aA0 = 0.0, aA1 = 0.0, aA2 = 0.0, aB0 = 0.0, aB1 = 0.0, aB2 = 0.0;
+  const int mtop = n2 > 0 ? m2 : m1;
+  for (int mm = 1; mm <= mtop; ++mm) {
+    const double cm = hc[(QOL_MAXL + 2) * (QOL_MAXL + 2) + mm];
+    double nr = cm * (XA * prA - YA * piA), ni = cm * (XA * piA + YA * prA);
+    double ndr = cm * (prA + (XA * drA - YA * diA)), ndi = cm * (piA + (XA * diA + YA * drA));
+    prA = nr; piA = ni; drA = ndr; diA = ndi;
+    nr = cm * (XB * prB - YB * piB); ni = cm * (XB * piB + YB * prB);
+    ndr = cm * (prB + (XB * drB - YB * diB)); ndi = cm * (piB + (XB * diB + YB * drB));
+    prB = nr; piB = ni; drB = ndr; diB = ndi;
+    if (mm == m1) { aA0 = piA; aA1 = diA; aA2 = drA; aB0 = piB; aB1 = diB; aB2 = drB; }
+  }
+  double sA = aA0, sxA = aA1, syA = aA2, szA = 0.0, tA = 0.0, txA = 0.0, tyA = 0.0, tzA = 0.0;
+  double sB = aB0, sxB = aB1, syB = aB2, szB = 0.0, tB = 0.0, txB = 0.0, tyB = 0.0, tzB = 0.0;
+  int m = m1, l = m1;
 #pragma unroll
-  for (int j = 0; j < LB; ++j)
-#pragma unroll
-    for (int c = 0; c < 5; ++c) acc[j][c] = 0.0;
-  double sumcD[3] = {0, 0, 0};
-  const int npts = nbd * ng;
-  for (int p = half; p < npts; p += 2) {
-    const int i = p / ng, g = p % ng;
-    const double t = T.tq[g], aD = T.wq[g] / t, aS = T.wq[g];
-    const double uD0 = aD * W.cD[3 * i], uD1 = aD * W.cD[3 * i + 1], uD2 = aD * W.cD[3 * i + 2];
-    const double uS0 = aS * W.cS[3 * i], uS1 = aS * W.cS[3 * i + 1], uS2 = aS * W.cS[3 * i + 2];
-    if (m == 1) { sumcD[0] += uD0; sumcD[1] += uD1; sumcD[2] += uD2; }
-    if (m <= L) {
-      const double* y = bx + 3 * i;
-      const double z0 = xt0 + t * (y[0] - xt0), z1 = xt1 + t * (y[1] - xt1), z2 = xt2 + t * (y[2] - xt2);
-      harm_column_re<LB>(L, m, z0, z1, z2, hb, hc, [&](int j, double h, double gx, double gy, double gz) {
-        acc[j][0] -= uD0 * gx + uD1 * gy + uD2 * gz;
-        acc[j][1] += uD1 * gz - uD2 * gy;
-        acc[j][2] += uD2 * gx - uD0 * gz;
-        acc[j][3] += uD0 * gy - uD1 * gx;
-        acc[j][4] += uS0 * gx + uS1 * gy + uS2 * gz;
-      });
+  for (int e = 0; e <= LB; ++e) {
+    if (e < n1 + n2) {
+      if (e == n1) {
+        m = m2; l = m2;
+        sA = piA; sxA = diA; syA = drA; szA = 0.0; tA = 0.0; txA = 0.0; tyA = 0.0; tzA = 0.0;
+        sB = piB; sxB = diB; syB = drB; szB = 0.0; tB = 0.0; txB = 0.0; tyB = 0.0; tzB = 0.0;
+      } else if (e > 0) {
+        ++l;
+        const double a = 2.0 * l - 1.0, b = hb[l * (QOL_MAXL + 2) + m], c = hc[l * (QOL_MAXL + 2) + m];
+        double aZ = a * ZA, br2 = b * r2A;
+        double ns = (aZ * sA - br2 * tA) * c;
+        double nsx = (aZ * sxA - b * (2.0 * XA * tA + r2A * txA)) * c;
+        double nsy = (aZ * syA - b * (2.0 * YA * tA + r2A * tyA)) * c;
+        double nsz = (a * (sA + ZA * szA) - b * (2.0 * ZA * tA + r2A * tzA)) * c;
+        tA = sA; txA = sxA; tyA = syA; tzA = szA;
+        sA = ns; sxA = nsx; syA = nsy; szA = nsz;
+        aZ = a * ZB; br2 = b * r2B;
+        ns = (aZ * sB - br2 * tB) * c;
+        nsx = (aZ * sxB - b * (2.0 * XB * tB + r2B * txB)) * c;
+        nsy = (aZ * syB - b * (2.0 * YB * tB + r2B * tyB)) * c;
+        nsz = (a * (sB + ZB * szB) - b * (2.0 * ZB * tB + r2B * tzB)) * c;
+        tB = sB; txB = sxB; tyB = syB; tzB = szB;
+        sB = ns; sxB = nsx; syB = nsy; szB = nsz;
+      }
+      f(e, sA, szA, sxA, syA, sB, szB, sxB, syB);
     }
   }
-  /* combine the two half-warps (same column m, different points) */
+}
+
+template <int LB>
+__global__ void __launch_bounds__(32 * RRQ_WARPS, 2) k_rrq_moments(OrderTab T, PairIn Q, PairWS G, RRQWS R) {
+  __shared__ double s_h[2 * (QOL_MAXL + 2) * (QOL_MAXL + 2) + (QOL_MAXL + 2)];
+  __shared__ double s_rec[RRQ_WARPS][6 * 3 * QOL_MAXNQ + 4];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int e = threadIdx.x; e < (QOL_MAXL + 2) * (QOL_MAXL + 2); e += blockDim.x) {
+    s_h[e] = c_hb[e / (QOL_MAXL + 2)][e % (QOL_MAXL + 2)];
+    s_h[(QOL_MAXL + 2) * (QOL_MAXL + 2) + e] = c_hc[e / (QOL_MAXL + 2)][e % (QOL_MAXL + 2)];
+  }
+  for (int e = threadIdx.x; e < QOL_MAXL + 2; e += blockDim.x) s_h[2 * (QOL_MAXL + 2) * (QOL_MAXL + 2) + e] = c_hcm[e];
+  __syncthreads();
+  const double* hb = s_h;
+  const double* hc = s_h + (QOL_MAXL + 2) * (QOL_MAXL + 2);
+  const long long gidx = (long long)blockIdx.x * RRQ_WARPS + wid;
+  if (gidx >= R.nrrq) return;
+  int lo = 0, hi = R.npan;
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (R.rrq_off[mid] <= gidx) lo = mid; else hi = mid;
+  }
+  const int pan = lo;
+  const int j_loc = (int)(gidx - R.rrq_off[pan]);
+  const long long p0 = Q.tcxi[pan] - 1;
+  const int tl = G.grp[p0 + G.off[(size_t)pan * 8 + T.nlevel + 1] + j_loc];
+  const int hd = T.hd, nq = T.nquad, nbd = 3 * nq, L = T.nterms, ng = T.ng;
+  const double* fr = R.frame + (size_t)pan * RRQ_FRAME;
+  const double* bx = R.bx + (size_t)pan * 3 * nbd;
+  const double alpha = fr[12];
+  double xt[3];
+  {
+    const double* x = Q.tcx + 3 * (p0 + tl);
+    double d0 = x[0] - fr[9], d1 = x[1] - fr[10], d2 = x[2] - fr[11];
+    for (int i = 0; i < 3; ++i) xt[i] = alpha * (fr[i] * d0 + fr[i + 3] * d1 + fr[i + 6] * d2);
+  }
+  const double xt0 = xt[0], xt1 = xt[1], xt2 = xt[2];
+  double* rec = s_rec[wid];
+  const double* grec = R.line + (size_t)gidx * (6 * nbd + 4);
+  for (int e = lane; e < 6 * nbd + 4; e += 32) rec[e] = grec[e];
+  __syncwarp();
+  const double* cD = rec;
+  const double* cS = rec + 3 * nbd;
+  const double lint0 = rec[6 * nbd], lint1 = rec[6 * nbd + 1], lint2 = rec[6 * nbd + 2], Omega = rec[6 * nbd + 3];
+  const double i4p = 1.0 / (4.0 * QOL_PI);
+  /* ceil(L/2) lanes per point group, lane idx handles the column pair
+   * (idx+1, L-idx): every lane runs L+1 recurrence steps */
+  const int PL = (L + 1) / 2, GP = 32 / PL;
+  const int grp = lane / PL, idx = lane % PL;
+  const bool lane_on = grp < GP;
+  const int m1 = idx + 1, m2 = L - idx;
+  const int n1 = L - m1 + 1, n2 = (m2 > m1) ? (L - m2 + 1) : 0;
+  double acc[LB + 1][5];
 #pragma unroll
-  for (int j = 0; j < LB; ++j)
+  for (int e = 0; e <= LB; ++e)
 #pragma unroll
-    for (int c = 0; c < 5; ++c) acc[j][c] += __shfl_xor_sync(0xffffffffu, acc[j][c], 16);
-  for (int d = 0; d < 3; ++d) {
-    sumcD[d] += __shfl_xor_sync(0xffffffffu, sumcD[d], 16);
-    sumcD[d] = __shfl_sync(0xffffffffu, sumcD[d], 0);
+    for (int c = 0; c < 5; ++c) acc[e][c] = 0.0;
+  double sumcD0 = 0.0, sumcD1 = 0.0, sumcD2 = 0.0;
+  const int npts = nbd * ng;
+  for (int p = grp; p < npts; p += GP) {
+    if (!lane_on) break;
+    const int i = p / ng, g = p % ng;
+    const double t = T.tq[g], aD = T.wq[g] / t, aS = T.wq[g];
+    const double uD0 = aD * cD[3 * i], uD1 = aD * cD[3 * i + 1], uD2 = aD * cD[3 * i + 2];
+    const double uS0 = aS * cS[3 * i], uS1 = aS * cS[3 * i + 1], uS2 = aS * cS[3 * i + 2];
+    if (idx == 0) { sumcD0 += uD0; sumcD1 += uD1; sumcD2 += uD2; }
+    const double* y = bx + 3 * i;
+    const double z0 = xt0 + t * (y[0] - xt0), z1 = xt1 + t * (y[1] - xt1), z2 = xt2 + t * (y[2] - xt2);
+    harm_pair_re<LB>(L, m1, m2, n1, n2, z0, z1, z2, hb, hc, [&](int e, double h, double gx, double gy, double gz) {
+      acc[e][0] -= uD0 * gx + uD1 * gy + uD2 * gz;
+      acc[e][1] += uD1 * gz - uD2 * gy;
+      acc[e][2] += uD2 * gx - uD0 * gz;
+      acc[e][3] += uD0 * gy - uD1 * gx;
+      acc[e][4] += uS0 * gx + uS1 * gy + uS2 * gz;
+    });
+  }
+  /* combine the point groups into group 0 (same idx, lanes idx + g*PL) */
+#pragma unroll
+  for (int e = 0; e <= LB; ++e)
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+      double v = acc[e][c];
+      for (int gg = 1; gg < GP; ++gg) {
+        double w = __shfl_sync(0xffffffffu, acc[e][c], (lane + gg * PL) & 31);
+        if (grp == 0) v += w;
+      }
+      acc[e][c] = v;
+    }
+  for (int o = 16; o > 0; o >>= 1) {
+    sumcD0 += __shfl_xor_sync(0xffffffffu, sumcD0, o);
+    sumcD1 += __shfl_xor_sync(0xffffffffu, sumcD1, o);
+    sumcD2 += __shfl_xor_sync(0xffffffffu, sumcD2, o);
   }
   /* the x point: (s0, l/4pi - sumcD) (x) (0, grad h(x)) and h(x) Omega/4pi */
   const double s0 = -Omega * i4p;
-  const double wv0 = lint[0] * i4p - sumcD[0], wv1 = lint[1] * i4p - sumcD[1], wv2 = lint[2] * i4p - sumcD[2];
+  const double wv0 = lint0 * i4p - sumcD0, wv1 = lint1 * i4p - sumcD1, wv2 = lint2 * i4p - sumcD2;
   double* JD = R.JD + (size_t)gidx * 4 * hd;
   double* RS = R.RS + (size_t)gidx * hd;
-  if (half == 0 && m <= L) {
-    harm_column_re<LB>(L, m, xt0, xt1, xt2, hb, hc, [&](int j, double h, double gx, double gy, double gz) {
-      const int l = m + j, k = l * (l - 1) / 2 + (m - 1);
-      JD[0 * hd + k] = acc[j][0] - (wv0 * gx + wv1 * gy + wv2 * gz);
-      JD[1 * hd + k] = acc[j][1] + s0 * gx + (wv1 * gz - wv2 * gy);
-      JD[2 * hd + k] = acc[j][2] + s0 * gy + (wv2 * gx - wv0 * gz);
-      JD[3 * hd + k] = acc[j][3] + s0 * gz + (wv0 * gy - wv1 * gx);
-      RS[k] = acc[j][4] + h * Omega * i4p;
+  if (grp == 0) {
+    harm_pair_re<LB>(L, m1, m2, n1, n2, xt0, xt1, xt2, hb, hc, [&](int e, double h, double gx, double gy, double gz) {
+      const int m = e < n1 ? m1 : m2, l = e < n1 ? m1 + e : m2 + (e - n1);
+      const int k = l * (l - 1) / 2 + (m - 1);
+      JD[0 * hd + k] = acc[e][0] - (wv0 * gx + wv1 * gy + wv2 * gz);
+      JD[1 * hd + k] = acc[e][1] + s0 * gx + (wv1 * gz - wv2 * gy);
+      JD[2 * hd + k] = acc[e][2] + s0 * gy + (wv2 * gx - wv0 * gz);
+      JD[3 * hd + k] = acc[e][3] + s0 * gz + (wv0 * gy - wv1 * gx);
+      RS[k] = acc[e][4] + h * Omega * i4p;
     });
   }
-  if (lane == 0 && R.ialpha) R.ialpha[tl] = Omega; /* single-panel calls (qol_rrq) */
 }
 
 /* ===================================================================== */
@@ -1066,12 +1253,14 @@ cudaError_t qol_launch_rrq_target(const OrderTab& T, const PairIn& Q, const Pair
                                   cudaStream_t st) {
   if (R.nrrq == 0) return cudaSuccess;
   long long nb = (R.nrrq + RRQ_WARPS - 1) / RRQ_WARPS;
-  if (T.nterms <= 4) k_rrq_target<4><<<(unsigned)nb, 32 * RRQ_WARPS, 0, st>>>(T, Q, G, R, exterior);
-  else if (T.nterms <= 6) k_rrq_target<6><<<(unsigned)nb, 32 * RRQ_WARPS, 0, st>>>(T, Q, G, R, exterior);
-  else if (T.nterms <= 8) k_rrq_target<8><<<(unsigned)nb, 32 * RRQ_WARPS, 0, st>>>(T, Q, G, R, exterior);
-  else if (T.nterms <= 10) k_rrq_target<10><<<(unsigned)nb, 32 * RRQ_WARPS, 0, st>>>(T, Q, G, R, exterior);
-  else if (T.nterms <= 13) k_rrq_target<13><<<(unsigned)nb, 32 * RRQ_WARPS, 0, st>>>(T, Q, G, R, exterior);
-  else k_rrq_target<16><<<(unsigned)nb, 32 * RRQ_WARPS, 0, st>>>(T, Q, G, R, exterior);
+  k_rrq_ssq<<<(unsigned)((3 * R.nrrq + 127) / 128), 128, 0, st>>>(T, Q, G, R);
+  k_rrq_geom<<<(unsigned)nb, 32 * RRQ_WARPS, 0, st>>>(T, Q, G, R, exterior);
+  if (T.nterms <= 4) k_rrq_moments<4><<<(unsigned)nb, 32 * RRQ_WARPS, 0, st>>>(T, Q, G, R);
+  else if (T.nterms <= 6) k_rrq_moments<6><<<(unsigned)nb, 32 * RRQ_WARPS, 0, st>>>(T, Q, G, R);
+  else if (T.nterms <= 8) k_rrq_moments<8><<<(unsigned)nb, 32 * RRQ_WARPS, 0, st>>>(T, Q, G, R);
+  else if (T.nterms <= 10) k_rrq_moments<10><<<(unsigned)nb, 32 * RRQ_WARPS, 0, st>>>(T, Q, G, R);
+  else if (T.nterms <= 13) k_rrq_moments<13><<<(unsigned)nb, 32 * RRQ_WARPS, 0, st>>>(T, Q, G, R);
+  else k_rrq_moments<16><<<(unsigned)nb, 32 * RRQ_WARPS, 0, st>>>(T, Q, G, R);
   return cudaGetLastError();
 }
 cudaError_t qol_launch_rrq_apply(const OrderTab& T, const PanelIn& P, const PairIn& Q, const PairWS& G,

@@ -56,6 +56,8 @@ struct RRQWS {
   double *qmat, *hmat, *smat, *PD, *B;
   int* perm;
   double *JD, *RS; /* per RRQ pair: 4hd, hd */
+  double* line;    /* per RRQ pair: cD (3 nbd), cS (3 nbd), lint (3), Omega */
+  double* edge;    /* per RRQ pair and edge: w1 (nq), w3 (nq), ok, Re t0, Im t0 */
   double* ialpha;  /* per RRQ pair (nullable) */
 };
 

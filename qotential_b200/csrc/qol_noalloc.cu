@@ -237,6 +237,8 @@ extern "C" int qol_rrq_noalloc(qol_int m, const double* tx, qol_int n, const dou
   R.perm = (int*)take(sizeof(int) * 272);
   R.JD = (double*)take(sizeof(double) * (size_t)m * 4 * hd);
   R.RS = (double*)take(sizeof(double) * (size_t)m * hd);
+  R.line = (double*)take(sizeof(double) * (size_t)m * (6 * nbd + 4));
+  R.edge = (double*)take(sizeof(double) * (size_t)m * 3 * (2 * nq + 3));
   if (over) {
     std::snprintf(g_na_msg, sizeof g_na_msg,
                   "qol_rrq_noalloc: m = %lld targets at order %lld need %zu bytes of scratch; the static scratch "
