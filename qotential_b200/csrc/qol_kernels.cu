@@ -1099,10 +1099,44 @@ __global__ void __launch_bounds__(32 * RRQ_WARPS, 2) k_rrq_moments(OrderTab T, P
 /* ===================================================================== */
 /* K6: RRQ solves as matrix products per panel + naive subtraction + COO */
 /* ===================================================================== */
-#define AT 16
-template <int HDMAX>
-__global__ void __launch_bounds__(256) k_rrq_apply(OrderTab T, PanelIn P, PairIn Q, PairWS G, RRQWS R,
-                                                   OutCOO O) {
+#define AT 64 /* RRQ targets per chunk */
+#define AQ 32 /* inner-dimension tile */
+/* Out[t][j] (+)= sum_q M[j][q] In[t][q] for AT targets and hd rows j, with
+ * the q range tiled through shared memory; thread (tx, ty) holds targets
+ * tx + 16a (a < 4) and rows ty + 16b (b < NB). */
+template <int NB>
+__device__ __forceinline__ void apply_tile_gemm(const double* __restrict__ M, int ldm, const double* In, int ldin,
+                                                int hd, int nq, int nt, double (&acc)[4][NB], double* sM,
+                                                double* sI) {
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  for (int q0 = 0; q0 < nq; q0 += AQ) {
+    __syncthreads();
+    for (int e = threadIdx.x; e < hd * AQ; e += blockDim.x) {
+      int j = e / AQ, q = e % AQ;
+      sM[q * (16 * NB) + j] = (q0 + q < nq) ? M[(size_t)j * ldm + q0 + q] : 0.0;
+    }
+    for (int e = threadIdx.x; e < AT * AQ; e += blockDim.x) {
+      int tt = e / AQ, q = e % AQ;
+      sI[q * AT + tt] = (tt < nt && q0 + q < nq) ? In[(size_t)tt * ldin + q0 + q] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int q = 0; q < AQ; ++q) {
+      double iv[4], mv[NB];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) iv[a] = sI[q * AT + tx + 16 * a];
+#pragma unroll
+      for (int b = 0; b < NB; ++b) mv[b] = sM[q * (16 * NB) + ty + 16 * b];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < NB; ++b) acc[a][b] += mv[b] * iv[a];
+    }
+  }
+}
+
+template <int NB>
+__global__ void __launch_bounds__(256) k_rrq_apply(OrderTab T, PanelIn P, PairIn Q, PairWS G, RRQWS R, OutCOO O) {
   const int pan = blockIdx.x;
   const int cnt = G.cnt[(size_t)pan * 8 + T.nlevel + 1];
   if (cnt == 0) return;
@@ -1115,46 +1149,51 @@ __global__ void __launch_bounds__(256) k_rrq_apply(OrderTab T, PanelIn P, PairIn
   const double* B = R.B + (size_t)pan * hd * hd;
   const double alpha = R.frame[(size_t)pan * RRQ_FRAME + 12];
   extern __shared__ double sm[];
-  double* sJ = sm;                 /* N4 x AT */
-  double* sR = sJ + N4 * AT;       /* hd x AT */
-  double* sA = sR + hd * AT;       /* hd x AT (Ad) */
+  double* sM = sm;                   /* AQ x 16NB */
+  double* sI = sM + AQ * 16 * NB;    /* AQ x AT */
+  double* sA = sI + AQ * AT;         /* AT x hd: Ad of the chunk, row-major per target */
   __shared__ int tloc[AT];
-  const int t = threadIdx.x % AT, jj = threadIdx.x / AT; /* 16 row groups */
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   const double i4p = 1.0 / (4.0 * QOL_PI);
   for (int c0 = 0; c0 < cnt; c0 += AT) {
     const int nt = min(AT, cnt - c0);
     __syncthreads();
-    for (int e = threadIdx.x; e < N4 * AT; e += blockDim.x) {
-      int tt = e / N4, q = e % N4;
-      sJ[q * AT + tt] = tt < nt ? R.JD[(size_t)(g0 + c0 + tt) * N4 + q] : 0.0;
-    }
-    for (int e = threadIdx.x; e < hd * AT; e += blockDim.x) {
-      int tt = e / hd, q = e % hd;
-      sR[q * AT + tt] = tt < nt ? R.RS[(size_t)(g0 + c0 + tt) * hd + q] : 0.0;
-    }
     if (threadIdx.x < AT) tloc[threadIdx.x] = threadIdx.x < nt ? G.grp[p0 + offl + c0 + threadIdx.x] : 0;
+    double acc[4][NB];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < NB; ++b) acc[a][b] = 0.0;
+    /* Ad = PD JD */
+    apply_tile_gemm<NB>(PD, N4, R.JD + (size_t)(g0 + c0) * N4, N4, hd, N4, nt, acc, sM, sI);
     __syncthreads();
-    for (int j = jj; j < hd; j += 256 / AT) {
-      double s = 0.0;
-      const double* pr = PD + (size_t)j * N4;
-      for (int q = 0; q < N4; ++q) s += pr[q] * sJ[q * AT + t];
-      sA[j * AT + t] = s;
-    }
-    __syncthreads();
-    for (int j = jj; j < hd; j += 256 / AT) {
-      double s = 0.0;
-      const double* ps = PS + (size_t)j * hd;
-      const double* pb = B + (size_t)j * hd;
-      for (int k = 0; k < hd; ++k) s += ps[k] * sR[k * AT + t];
-      for (int k = 0; k < hd; ++k) s += pb[k] * sA[k * AT + t];
-      if (t < nt) {
-        double vs = s / alpha, vd = sA[j * AT + t];
-        const int tl = tloc[t];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+        int t = tx + 16 * a, j = ty + 16 * b;
+        if (j < hd) sA[t * hd + j] = acc[a][b];
+        acc[a][b] = 0.0;
+      }
+    /* As = (PS RS + B Ad) / alpha */
+    apply_tile_gemm<NB>(PS, hd, R.RS + (size_t)(g0 + c0) * hd, hd, hd, hd, nt, acc, sM, sI);
+    apply_tile_gemm<NB>(B, hd, sA, hd, hd, hd, nt, acc, sM, sI);
+    /* naive block, COO values, Omega */
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const int t = tx + 16 * a;
+      if (t >= nt) continue;
+      const int tl = tloc[t];
+      const long long row = Q.tcxrow[p0 + tl];
+      const double* x = Q.tcx + 3 * (p0 + tl);
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+        const int j = ty + 16 * b;
+        if (j >= hd) continue;
+        double vs = acc[a][b] / alpha, vd = sA[t * hd + j];
         if (O.subtract_naive) {
-          const long long row = Q.tcxrow[p0 + tl];
           size_t gj = (size_t)pan * hd + j;
           if (row != (long long)gj + 1) {
-            const double* x = Q.tcx + 3 * (p0 + tl);
             double dx = x[0] - P.sx[3 * gj], dy = x[1] - P.sx[3 * gj + 1], dz = x[2] - P.sx[3 * gj + 2];
             double rr = dx * dx + dy * dy + dz * dz;
             if (rr > 1.0e-28) {
@@ -1173,7 +1212,7 @@ __global__ void __launch_bounds__(256) k_rrq_apply(OrderTab T, PanelIn P, PairIn
     if (O.omega)
       for (int e = threadIdx.x; e < N4 * nt; e += blockDim.x) {
         int tt = e / N4, q = e % N4;
-        double v = sJ[q * AT + tt];
+        double v = R.JD[(size_t)(g0 + c0 + tt) * N4 + q];
         O.omega[(size_t)tloc[tt] * N4 + q] = (q < hd ? v : -v) / alpha;
       }
   }
@@ -1265,12 +1304,17 @@ cudaError_t qol_launch_rrq_target(const OrderTab& T, const PairIn& Q, const Pair
 }
 cudaError_t qol_launch_rrq_apply(const OrderTab& T, const PanelIn& P, const PairIn& Q, const PairWS& G,
                                  const RRQWS& R, const OutCOO& O, int npan, cudaStream_t st) {
-  size_t smem = sizeof(double) * (4 * T.hd + 2 * T.hd) * AT;
-  if (T.hd <= 48) k_rrq_apply<48><<<npan, 256, smem, st>>>(T, P, Q, G, R, O);
-  else {
-    cudaFuncSetAttribute(k_rrq_apply<136>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_rrq_apply<136><<<npan, 256, smem, st>>>(T, P, Q, G, R, O);
-  }
+  const int NBn = (T.hd + 15) / 16;
+  auto go = [&](auto kern, int nb) {
+    size_t smem = sizeof(double) * ((size_t)AQ * 16 * nb + AQ * AT + (size_t)AT * T.hd);
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    kern<<<npan, 256, smem, st>>>(T, P, Q, G, R, O);
+  };
+  if (NBn <= 2) go(k_rrq_apply<2>, 2);
+  else if (NBn <= 3) go(k_rrq_apply<3>, 3);
+  else if (NBn <= 4) go(k_rrq_apply<4>, 4);
+  else if (NBn <= 6) go(k_rrq_apply<6>, 6);
+  else go(k_rrq_apply<9>, 9);
   return cudaGetLastError();
 }
 cudaError_t qol_launch_coo_index(const OrderTab& T, const PairIn& Q, long long* si, long long* sj, int npan,
