@@ -57,6 +57,62 @@ def workload(rank=0, world=1, panels=0):
     return W
 
 
+# kernels of one qol_getnearquad_lap_rrq call: levels, classify, scan, direct,
+# rrq_panel, rrq_ssq, rrq_geom, rrq_moments, rrq_apply, coo_index
+LAUNCHES_PER_STEP = 10
+
+
+def xlate_terms(L):
+    """terms of the solid-harmonic translation T_n^k = sum M_lam^mu R_{n-lam}^{k-mu}(x),
+    0 <= k <= n <= L-1 (the work list of k_rrq_moments)"""
+    t = 0
+    for n in range(L):
+        for k in range(n + 1):
+            for lam in range(n + 1):
+                nu = n - lam
+                t += min(lam, k + nu) - max(-lam, k - nu) + 1
+    return t
+
+
+def kernel_flops(W, hist):
+    """algorithmic FP64 FLOPs of one step, per kernel with a closed form"""
+    import ctypes as C
+    from qotential_b200 import lib
+    hd, nq, L = W["hd"], W["nquad"], W["nterms"]
+    nbd = 3 * nq
+    n4 = np.zeros(4, np.int64); s4 = np.zeros(4, np.int64)
+    lib().qol_level_sizes(C.c_longlong(L), C.c_longlong(nq), C.c_void_p(n4.ctypes.data), C.c_void_p(s4.ctypes.data))
+    nrrq = int(hist[5])
+    ne = L * (L + 1) // 2  # complex entries R_lam^mu, lam <= L-1, mu >= 0
+    return {
+        # kernel sum over level nodes fused with the interpolation contraction
+        "direct": sum(int(hist[l + 1]) * int(n4[l]) * (20 + 4 * hd) for l in range(4)),
+        # R(rho_i) recurrences (8 per complex entry), 6-weight contraction (2 x 6 per real row),
+        # translation (6 complex multiply-adds = 48 per term)
+        "rrq_moments": nrrq * (8 * ne * nbd + 24 * ne * nbd + 48 * xlate_terms(L)),
+        # Ad = PD JD (hd x 4hd), As = PS RS + B Ad (2 hd x hd)
+        "rrq_apply": nrrq * (2 * hd * 4 * hd + 4 * hd * hd),
+    }
+
+
+def roofline_line(W, hist, k_ms, peak):
+    fl = kernel_flops(W, hist)
+    dom = max(k_ms, key=k_ms.get)
+    rl_kernel = dom if dom in fl else max(fl, key=lambda k: k_ms[k])
+    ach = fl[rl_kernel] / (k_ms[rl_kernel] * 1e-3) / 1e12
+    notes = {"direct": "k_direct: sum over level-resolved pairs of (20 + 4 hdim) x n_level FLOPs",
+             "rrq_moments": "k_rrq_moments: per RRQ pair 8 ne nbd + 24 ne nbd + 48 x (translation terms), "
+                            "ne = L(L+1)/2",
+             "rrq_apply": "k_rrq_apply: per RRQ pair 12 hdim^2"}
+    return {"bound": "fp64", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
+            "frac": ach / peak if peak else None, "traffic": None, "kernel": rl_kernel,
+            "dominant_kernel": dom,
+            "peak_source": "measured: in-library FP64 FMA probe (MEASURED_PEAKS.json has no FP64 figure)",
+            "flops": notes[rl_kernel], "kernel_ms": k_ms,
+            "kernel_tflops": {k: fl[k] / (k_ms[k] * 1e-3) / 1e12 for k in fl if k_ms[k] > 0},
+            "level_hist": [int(x) for x in hist[1:6]]}
+
+
 def config_dict(W, world):
     return {"workload": f"stellarator {MP}x{NP} quads ({W['npan_total']} triangles), order {ORDER} "
                         f"(nterms {W['nterms']}, hdim {W['hd']}, nquad=orderff {W['nquad']}), "
@@ -240,47 +296,29 @@ def main():
         dist.barrier()
     pairs_total = W["pairs_total"]
     value = pairs_total / (ms * 1e-3)
-    if args.kernels_only:
-        if rank == 0:
-            print(json.dumps({"metric": "near-pair evals/s", "value": value, "ms_per_step": ms,
-                              "steps": args.steps, "note": "kernels-only run"}))
-        if dist:
-            dist.destroy_process_group()
-        return 0
-
     # per-kernel device times of one more (untimed) step, for the roofline
     import ctypes as C
-    ms7 = np.zeros(7); calls = np.zeros(1, np.int64)
+    NPH = 9
+    ms_ph = np.zeros(NPH); calls = np.zeros(1, np.int64)
     L.qol_kernel_times(C.c_int(1), None, None)
     step()
     torch.cuda.synchronize()
-    L.qol_kernel_times(C.c_int(-1), C.c_void_p(ms7.ctypes.data), C.c_void_p(calls.ctypes.data))
+    L.qol_kernel_times(C.c_int(-1), C.c_void_p(ms_ph.ctypes.data), C.c_void_p(calls.ctypes.data))
     L.qol_kernel_times(C.c_int(0), None, None)
-    names = ["levels", "classify", "direct", "rrq_panel", "rrq_target", "rrq_apply", "coo_index"]
+    names = ["levels", "classify", "direct", "rrq_panel", "rrq_ssq", "rrq_geom", "rrq_moments", "rrq_apply",
+             "coo_index"]
     peak = C.c_double(0.0)
     L.qol_probe_fp64_peak(C.byref(peak))
-    hd, nq = W["hd"], W["nquad"]
-    n4 = np.zeros(4, np.int64); s4 = np.zeros(4, np.int64)
-    L.qol_level_sizes(C.c_longlong(W["nterms"]), C.c_longlong(W["nquad"]), C.c_void_p(n4.ctypes.data),
-                      C.c_void_p(s4.ctypes.data))
-    nl = [int(x) for x in n4]
-    flops_direct = sum(int(hist[l + 1]) * nl[l] * (20 + 4 * hd) for l in range(4))
-    nbd, ncoeff = 3 * nq, (W["nterms"] + 1) * (W["nterms"] + 2) // 2
-    flops_rrq_alg = int(hist[5]) * (48 * nbd * ncoeff + 2 * (4 * hd) ** 2 + 4 * hd * hd)
-    k_share = {n: float(v) for n, v in zip(names, ms7)}
-    dom = max(k_share, key=k_share.get)
-    if dom == "direct":
-        ach = flops_direct / (k_share["direct"] * 1e-3) / 1e12
-        rl_note = "k_direct: sum over level-resolved pairs of (20 + 4 hdim) x n_level FLOPs"
-    else:
-        ach = flops_rrq_alg / ((k_share["rrq_target"] + k_share["rrq_apply"]) * 1e-3) / 1e12
-        rl_note = ("RRQ kernels (moments + solves): per RRQ pair 48 nbd ncoeff + 2 (4 hdim)^2 + 4 hdim^2 FLOPs "
-                   "(the reference's a8 + a10 counts)")
-    roofline = {"bound": "fp64", "achieved": ach, "peak": peak.value, "unit": "TFLOP/s",
-                "frac": ach / peak.value if peak.value else None, "traffic": None, "kernel": dom,
-                "peak_source": "measured: in-library FP64 FMA probe (MEASURED_PEAKS.json has no FP64 figure)",
-                "flops": rl_note,
-                "kernel_ms": k_share, "level_hist": [int(x) for x in hist[1:6]]}
+    roofline = roofline_line(W, hist, dict(zip(names, (float(v) for v in ms_ph))), peak.value)
+
+    if args.kernels_only:
+        if rank == 0:
+            print(json.dumps({"metric": "near-pair evals/s", "value": value, "ms_per_step": ms,
+                              "steps": args.steps, "note": "kernels-only run", "kernel_ms": roofline["kernel_ms"],
+                              "kernel_tflops": roofline["kernel_tflops"]}))
+        if dist:
+            dist.destroy_process_group()
+        return 0
 
     # end to end through the public host-pointer API
     e2e = None
@@ -312,7 +350,7 @@ def main():
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
                 "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": config_dict(W, world), "clocks": clocks, "e2e": e2e,
-                "gpu_launches": 8 * args.steps, "roofline": roofline, "cpu_baseline": cpu}
+                "gpu_launches": LAUNCHES_PER_STEP * args.steps, "roofline": roofline, "cpu_baseline": cpu}
         print(json.dumps(line))
     if dist:
         dist.barrier()

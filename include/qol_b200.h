@@ -137,13 +137,17 @@ const char* qol_noalloc_last_error(void);
 
 /* Library status and diagnostics.  qol_kernel_times: when enabled, every
  * pipeline call records CUDA events on its stream around its phases and
- * accumulates the device milliseconds: [0] refined levels, [1] classification,
- * [2] level sums, [3] per-panel RRQ precompute, [4] per-pair RRQ moments,
- * [5] RRQ solves + COO values, [6] COO indices.  Returns the sums and the
- * call count; enable >= 0 resets them and sets the switch (-1: read only).
- * (No counterpart in the reference; its timeinfo is the host-side analogue.) */
+ * accumulates the device milliseconds of its QOL_NPHASE phases: [0] refined
+ * levels, [1] classification (with the host read of the RRQ pair count),
+ * [2] level sums, [3] per-panel RRQ precompute, [4] singularity-swap roots and
+ * weights, [5] string direction, solid angle and boundary weights, [6]
+ * harmonic moments, [7] RRQ solves + COO values, [8] COO indices.  Returns the
+ * sums (ms[QOL_NPHASE]) and the call count; enable >= 0 resets them and sets
+ * the switch (-1: read only).  (No counterpart in the reference; its timeinfo
+ * is the host-side analogue.) */
+#define QOL_NPHASE 9
 const char* qol_last_error(void);
-int qol_kernel_times(int enable, double* ms7, qol_int* calls);
+int qol_kernel_times(int enable, double* ms, qol_int* calls);
 int qol_version(void);
 /* FP64 FMA throughput of this GPU in TFLOP/s (best of 5 timed launches of
  * independent FMA chains on every SM); the roofline denominator for the FP64

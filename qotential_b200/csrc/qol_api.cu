@@ -85,7 +85,7 @@ bool g_coefs_uploaded = false;
 Arena g_arena, g_arena2;
 /* per-phase device milliseconds of the pipeline (diagnostics) */
 int g_ktime_on = 0;
-double g_ktime[7] = {0, 0, 0, 0, 0, 0, 0};
+double g_ktime[QOL_NPHASE] = {};
 long long g_kcalls = 0;
 cudaStream_t g_stream = nullptr;
 
@@ -175,7 +175,10 @@ int order_tables(int nterms, int orderff, int nquad, OrderCache** out) {
   T.tgl = C->up(tgl); T.wgl = C->up(wgl); T.Dgl = C->up(Dgl); T.Leg = C->up(Leg);
   T.gl48x = C->up(g48x); T.gl48w = C->up(g48w); T.gl16x = C->up(g16x); T.gl16w = C->up(g16w);
   T.tq = C->up(tq); T.wq = C->up(wq); T.Mb = C->up(Mb); T.umatr = C->up(um); T.vruv = C->up(vr);
-  if (!T.tgl || !T.Mb || !T.vruv) return fail(QOL_ERR_CUDA, "table upload failed");
+  std::vector<uint32_t> xs;
+  qolh::xlate_schedule(nterms, xs, T.xsteps);
+  T.xsched = C->up(xs);
+  if (!T.tgl || !T.Mb || !T.vruv || !T.xsched) return fail(QOL_ERR_CUDA, "table upload failed");
   *out = C.get();
   g_orders[key] = std::move(C);
   return 0;
@@ -183,7 +186,7 @@ int order_tables(int nterms, int orderff, int nquad, OrderCache** out) {
 
 /* ---------------- the pipeline on device pointers ---------------- */
 struct Timing {
-  cudaEvent_t ev[8];
+  cudaEvent_t ev[QOL_NPHASE + 1];
   bool on = false;
 };
 
@@ -251,7 +254,7 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
   CK(cudaMemsetAsync(G.off, 0, sizeof(int) * (size_t)npan * 8, st));
   Timing tm;
   if (timeinfo || g_ktime_on) {
-    for (int i = 0; i < 8; ++i) CK(cudaEventCreate(&tm.ev[i]));
+    for (int i = 0; i <= QOL_NPHASE; ++i) CK(cudaEventCreate(&tm.ev[i]));
     tm.on = true;
   }
   auto rec = [&](int i) { if (tm.on) cudaEventRecord(tm.ev[i], st); };
@@ -281,15 +284,19 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
   if (nrrq > 0) {
     CK(qol_launch_rrq_panel(T, J.P, G, R, npan, J.chart, st));
     rec(4);
-    CK(qol_launch_rrq_target(T, J.Q, G, R, J.exterior, st));
+    CK(qol_launch_rrq_ssq(T, J.Q, G, R, st));
     rec(5);
-    CK(qol_launch_rrq_apply(T, J.P, J.Q, G, R, O, npan, st));
+    CK(qol_launch_rrq_geom(T, J.Q, G, R, J.exterior, st));
     rec(6);
+    CK(qol_launch_rrq_moments(T, J.Q, G, R, st));
+    rec(7);
+    CK(qol_launch_rrq_apply(T, J.P, J.Q, G, R, O, npan, st));
+    rec(8);
   } else {
-    rec(4); rec(5); rec(6);
+    for (int i = 4; i <= 8; ++i) rec(i);
   }
   if (J.si) CK(qol_launch_coo_index(T, J.Q, J.si, J.sj, npan, st));
-  rec(7);
+  rec(9);
   if (hist_out || grp_out || cnt_out || tm.on) {
     CK(cudaStreamSynchronize(st));
   }
@@ -308,18 +315,18 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
     CK(cudaMemcpy(grp_out->data(), G.grp, sizeof(int) * ntcx, cudaMemcpyDeviceToHost));
   }
   if (tm.on) {
-    float ms[7];
-    for (int i = 0; i < 7; ++i) cudaEventElapsedTime(&ms[i], tm.ev[i], tm.ev[i + 1]);
+    float ms[QOL_NPHASE];
+    for (int i = 0; i < QOL_NPHASE; ++i) cudaEventElapsedTime(&ms[i], tm.ev[i], tm.ev[i + 1]);
     if (timeinfo) {
-      timeinfo[0] += 1e-3 * ms[0];            /* patch levels */
-      timeinfo[1] += 1e-3 * ms[3];            /* per-panel RRQ precompute */
-      timeinfo[2] += 1e-3 * (ms[1] + ms[2]);  /* classification + level sums */
-      timeinfo[5] += 1e-3 * ms[4];            /* fused SSQ / solid angle / moments */
-      timeinfo[7] += 1e-3 * (ms[5] + ms[6]);  /* solves + COO */
+      timeinfo[0] += 1e-3 * ms[0];                   /* patch levels */
+      timeinfo[1] += 1e-3 * ms[3];                   /* per-panel RRQ precompute */
+      timeinfo[2] += 1e-3 * (ms[1] + ms[2]);         /* classification + level sums */
+      timeinfo[5] += 1e-3 * (ms[4] + ms[5] + ms[6]); /* SSQ / solid angle / moments */
+      timeinfo[7] += 1e-3 * (ms[7] + ms[8]);         /* solves + COO */
     }
-    for (int i = 0; i < 7; ++i) g_ktime[i] += ms[i];
+    for (int i = 0; i < QOL_NPHASE; ++i) g_ktime[i] += ms[i];
     g_kcalls += 1;
-    for (int i = 0; i < 8; ++i) cudaEventDestroy(tm.ev[i]);
+    for (int i = 0; i <= QOL_NPHASE; ++i) cudaEventDestroy(tm.ev[i]);
   }
   return 0;
 }
@@ -371,13 +378,13 @@ extern "C" {
 
 const char* qol_last_error(void) { return g_err.c_str(); }
 
-int qol_kernel_times(int enable, double* ms7, qol_int* calls) {
+int qol_kernel_times(int enable, double* ms, qol_int* calls) {
   std::lock_guard<std::recursive_mutex> g(g_mu);
-  if (ms7) for (int i = 0; i < 7; ++i) ms7[i] = g_ktime[i];
+  if (ms) for (int i = 0; i < QOL_NPHASE; ++i) ms[i] = g_ktime[i];
   if (calls) *calls = g_kcalls;
   if (enable >= 0) {
     g_ktime_on = enable;
-    for (int i = 0; i < 7; ++i) g_ktime[i] = 0.0;
+    for (int i = 0; i < QOL_NPHASE; ++i) g_ktime[i] = 0.0;
     g_kcalls = 0;
   }
   return 0;

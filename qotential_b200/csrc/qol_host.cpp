@@ -6,6 +6,7 @@
 #include "vr_table.h"
 #include <algorithm>
 #include <cfloat>
+#include <cstdlib>
 #include <stdexcept>
 
 namespace qolh {
@@ -367,6 +368,47 @@ void build_ref(int korder, int order, int nlevel, bool sqmode, RefElem& R) {
     L.interp.assign((size_t)L.n * npols, 0.0);
     interp_matrix(korder, (int)L.n, L.uv.data(), L.interp.data());
   }
+}
+
+void xlate_schedule(int L, std::vector<uint32_t>& tab, int& steps) {
+  struct Out { int idx, cost; std::vector<uint32_t> terms; };
+  std::vector<Out> outs;
+  for (int n = 0; n < L; ++n)
+    for (int k = 0; k <= n; ++k) {
+      Out o;
+      o.idx = n * (n + 1) / 2 + k;
+      for (int lam = 0; lam <= n; ++lam) {
+        const int nu = n - lam;
+        for (int mu = std::max(-lam, k - nu); mu <= std::min(lam, k + nu); ++mu) {
+          const int kr = k - mu, am = std::abs(mu), ar = std::abs(kr);
+          const int neg = ((mu < 0 && (am & 1)) ? 1 : 0) ^ ((kr < 0 && (ar & 1)) ? 1 : 0);
+          uint32_t w = (uint32_t)(lam * (lam + 1) / 2 + am) | ((uint32_t)(nu * (nu + 1) / 2 + ar) << 8) |
+                       ((uint32_t)o.idx << 16) | ((uint32_t)(mu < 0) << 24) | ((uint32_t)(kr < 0) << 25) |
+                       ((uint32_t)neg << 26) | (1u << 27);
+          o.terms.push_back(w);
+        }
+      }
+      o.cost = (int)o.terms.size();
+      outs.push_back(std::move(o));
+    }
+  /* longest first; ties by output index, lanes by load then index */
+  std::vector<int> ord(outs.size());
+  for (size_t i = 0; i < ord.size(); ++i) ord[i] = (int)i;
+  std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return outs[a].cost > outs[b].cost; });
+  std::vector<std::vector<uint32_t>> lane(32);
+  std::vector<int> load(32, 0);
+  for (int oi : ord) {
+    int best = 0;
+    for (int q = 1; q < 32; ++q)
+      if (load[q] < load[best]) best = q;
+    load[best] += outs[oi].cost;
+    lane[best].insert(lane[best].end(), outs[oi].terms.begin(), outs[oi].terms.end());
+  }
+  steps = 0;
+  for (int q = 0; q < 32; ++q) steps = std::max(steps, load[q]);
+  tab.assign((size_t)steps * 32, 0u);
+  for (int q = 0; q < 32; ++q)
+    for (size_t s = 0; s < lane[q].size(); ++s) tab[s * 32 + q] = lane[q][s];
 }
 
 } // namespace qolh

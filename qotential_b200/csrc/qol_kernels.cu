@@ -10,16 +10,23 @@
  *                    quaternion system and of the S system
  *   k_rrq_geom       per-pair SSQ weights, string direction, solid angle,
  *                    boundary weights (:789-832), one warp per pair
- *   k_rrq_moments    per-pair harmonic moments (:832-841), one warp per pair
+ *   k_rrq_moments    per-pair harmonic moments (:832-841) by solid-harmonic
+ *                    translation, one warp per pair
  *   k_rrq_apply      the two solves as per-panel matrix products (:843-870)
  *   k_coo_index      COO row/column indices (:948-956)
  */
 #include "qol_dev.cuh"
 #include "qol_kernels.h"
+#include <cmath>
 
 __constant__ double c_hb[QOL_MAXL + 2][QOL_MAXL + 2]; /* sqrt((l+m-1)(l-m-1)) */
 __constant__ double c_hc[QOL_MAXL + 2][QOL_MAXL + 2]; /* 1/sqrt((l-m)(l+m)) */
 __constant__ double c_hcm[QOL_MAXL + 2];               /* sqrt((2m-1)/(2m)) */
+/* regular solid harmonics R_l^m (k_rrq_moments) */
+__constant__ double c_rq[QOL_MAXL + 2][QOL_MAXL + 2]; /* 1/((l+m)(l-m)), l > m */
+__constant__ double c_rn[QOL_MAXL + 2][QOL_MAXL + 2]; /* sqrt((l-m)!(l+m)!) */
+__constant__ double c_rd[QOL_MAXL + 2];               /* 1/(2m) */
+__constant__ double c_rinv[QOL_MAXL + 2];             /* 1/l, 0 at l = 0 */
 
 void qol_upload_harm_coefs(const double* hb, const double* hc, const double* hcm, cudaStream_t st) {
   cudaMemcpyToSymbolAsync(c_hb, hb, sizeof(double) * (QOL_MAXL + 2) * (QOL_MAXL + 2), 0,
@@ -27,6 +34,23 @@ void qol_upload_harm_coefs(const double* hb, const double* hc, const double* hcm
   cudaMemcpyToSymbolAsync(c_hc, hc, sizeof(double) * (QOL_MAXL + 2) * (QOL_MAXL + 2), 0,
                           cudaMemcpyHostToDevice, st);
   cudaMemcpyToSymbolAsync(c_hcm, hcm, sizeof(double) * (QOL_MAXL + 2), 0, cudaMemcpyHostToDevice, st);
+  const int M = QOL_MAXL + 2;
+  double rq[M][M] = {}, rn[M][M] = {}, rd[M] = {}, rinv[M] = {};
+  double fact[2 * M];
+  fact[0] = 1.0;
+  for (int i = 1; i < 2 * M; ++i) fact[i] = fact[i - 1] * i;
+  for (int l = 0; l < M; ++l) {
+    if (l > 0) { rd[l] = 1.0 / (2.0 * l); rinv[l] = 1.0 / l; }
+    for (int m = 0; m <= l; ++m) {
+      if (l > m) rq[l][m] = 1.0 / ((double)(l + m) * (double)(l - m));
+      rn[l][m] = std::sqrt(fact[l - m] * fact[l + m]);
+    }
+  }
+  cudaMemcpyToSymbolAsync(c_rq, rq, sizeof(rq), 0, cudaMemcpyHostToDevice, st);
+  cudaMemcpyToSymbolAsync(c_rn, rn, sizeof(rn), 0, cudaMemcpyHostToDevice, st);
+  cudaMemcpyToSymbolAsync(c_rd, rd, sizeof(rd), 0, cudaMemcpyHostToDevice, st);
+  cudaMemcpyToSymbolAsync(c_rinv, rinv, sizeof(rinv), 0, cudaMemcpyHostToDevice, st);
+  cudaStreamSynchronize(st); /* the host tables above are locals */
 }
 
 /* ===================================================================== */
@@ -680,88 +704,6 @@ __device__ double panel_height_warp(const OrderTab& T, const double* scf, const 
   return xt[2] - f[6];
 }
 
-/* column m of the sin-type solid harmonics, real recurrences on the
- * imaginary parts (the column recurrence has real coefficients), calling
- * f(j, h, gx, gy, gz) for l = m + j, j = 0..L-m.  hb/hc: recurrence
- * coefficients in shared memory (lanes index different m). */
-template <int LB, class F>
-__device__ __forceinline__ void harm_column_re(int L, int m, double x, double y, double z, const double* hb,
-                                               const double* hc, F f) {
-  const double X = y, Y = z, Z = x;
-  const double r2 = X * X + Y * Y + Z * Z;
-  /* diagonal S_m^m = C_m (X+iY)^m and its derivative in w = X+iY */
-  double pr = 1.0, pi = 0.0, dr = 0.0, di = 0.0;
-  for (int mm = 1; mm <= m; ++mm) {
-    double cm = hc[(QOL_MAXL + 2) * (QOL_MAXL + 2) + mm];
-    double nr = cm * (X * pr - Y * pi), ni = cm * (X * pi + Y * pr);
-    double ndr = cm * (pr + (X * dr - Y * di)), ndi = cm * (pi + (X * di + Y * dr));
-    pr = nr; pi = ni; dr = ndr; di = ndi;
-  }
-  /* Im parts: value, d/dX = Im dS, d/dY = Im(i dS) = Re dS, d/dZ = 0 */
-  double s1 = pi, s1x = di, s1y = dr, s1z = 0.0;
-  double s2 = 0.0, s2x = 0.0, s2y = 0.0, s2z = 0.0;
-  f(0, s1, s1z, s1x, s1y);
-#pragma unroll
-  for (int j = 1; j < LB; ++j) {
-    const int l = m + j;
-    if (l <= L) {
-      const double a = 2.0 * l - 1.0, b = hb[l * (QOL_MAXL + 2) + m], c = hc[l * (QOL_MAXL + 2) + m];
-      const double aZ = a * Z, br2 = b * r2;
-      double s = (aZ * s1 - br2 * s2) * c;
-      double sx = (aZ * s1x - b * (2.0 * X * s2 + r2 * s2x)) * c;
-      double sy = (aZ * s1y - b * (2.0 * Y * s2 + r2 * s2y)) * c;
-      double sz = (a * (s1 + Z * s1z) - b * (2.0 * Z * s2 + r2 * s2z)) * c;
-      s2 = s1; s2x = s1x; s2y = s1y; s2z = s1z;
-      s1 = s; s1x = sx; s1y = sy; s1z = sz;
-      f(j, s, sz, sx, sy);
-    }
-  }
-}
-
-/* the column pair (m1, m2) of one lane: entries e = 0..n1-1 are column m1
- * (l = m1 + e), e = n1..n1+n2-1 column m2 (l = m2 + e - n1); the diagonal
- * chain runs to max(m1, m2) once.  Same recurrences as harm_column_re. */
-template <int LB, class F>
-__device__ __forceinline__ void harm_pair_re(int L, int m1, int m2, int n1, int n2, double x, double y, double z,
-                                             const double* hb, const double* hc, F f) {
-  const double X = y, Y = z, Z = x;
-  const double r2 = X * X + Y * Y + Z * Z;
-  double pr = 1.0, pi = 0.0, dr = 0.0, di = 0.0;
-  double a_pi = 0.0, a_di = 0.0, a_dr = 0.0; /* diagonal of column m1 */
-  const int mtop = n2 > 0 ? m2 : m1;
-  for (int mm = 1; mm <= mtop; ++mm) {
-    double cm = hc[(QOL_MAXL + 2) * (QOL_MAXL + 2) + mm];
-    double nr = cm * (X * pr - Y * pi), ni = cm * (X * pi + Y * pr);
-    double ndr = cm * (pr + (X * dr - Y * di)), ndi = cm * (pi + (X * di + Y * dr));
-    pr = nr; pi = ni; dr = ndr; di = ndi;
-    if (mm == m1) { a_pi = pi; a_di = di; a_dr = dr; }
-  }
-  double s1 = a_pi, s1x = a_di, s1y = a_dr, s1z = 0.0;
-  double s2 = 0.0, s2x = 0.0, s2y = 0.0, s2z = 0.0;
-  int m = m1, l = m1;
-#pragma unroll
-  for (int e = 0; e <= LB; ++e) {
-    if (e < n1 + n2) {
-      if (e == n1) { /* start column m2 from its diagonal */
-        m = m2; l = m2;
-        s1 = pi; s1x = di; s1y = dr; s1z = 0.0;
-        s2 = 0.0; s2x = 0.0; s2y = 0.0; s2z = 0.0;
-      } else if (e > 0) {
-        ++l;
-        const double a = 2.0 * l - 1.0, b = hb[l * (QOL_MAXL + 2) + m], c = hc[l * (QOL_MAXL + 2) + m];
-        const double aZ = a * Z, br2 = b * r2;
-        double s = (aZ * s1 - br2 * s2) * c;
-        double sx = (aZ * s1x - b * (2.0 * X * s2 + r2 * s2x)) * c;
-        double sy = (aZ * s1y - b * (2.0 * Y * s2 + r2 * s2y)) * c;
-        double sz = (a * (s1 + Z * s1z) - b * (2.0 * Z * s2 + r2 * s2z)) * c;
-        s2 = s1; s2x = s1x; s2y = s1y; s2z = s1z;
-        s1 = s; s1x = sx; s1y = sy; s1z = sz;
-      }
-      f(e, s1, s1z, s1x, s1y);
-    }
-  }
-}
-
 /* singularity-swap root and modified weights, one thread per (RRQ pair,
  * edge): writes w1 (nq), w3 (nq), ok, Re t0, Im t0 to the pair's edge record */
 __global__ void __launch_bounds__(128) k_rrq_ssq(OrderTab T, PairIn Q, PairWS G, RRQWS R) {
@@ -934,73 +876,61 @@ __global__ void __launch_bounds__(32 * RRQ_WARPS) k_rrq_geom(OrderTab T, PairIn 
   }
 }
 
-/* the same column pair at two points in lockstep (two independent
- * recurrence chains per lane); f(e, hA, gA.., hB, gB..) */
-template <int LB, class F>
-__device__ __forceinline__ void harm_pair_re2(int L, int m1, int m2, int n1, int n2, const double* xa,
-                                              const double* xb, const double* hb, const double* hc, F f) {
-  const double XA = xa[1], YA = xa[2], ZA = xa[0], XB = xb[1], YB = xb[2], ZB = xb[0];
-  const double r2A = XA * XA + YA * YA + ZA * ZA, r2B = XB * XB + YB * YB + ZB * ZB;
-  double prA = 1.0, piA = 0.0, drA = 0.0, diA = 0.0, prB = 1.0, piB = 0.0, drB = 0.0, diB = 0.0;
-  double aA0 = 0.0, aA1 = 0.0, aA2 = 0.0, aB0 = 0.0, aB1 = 0.0, aB2 = 0.0;
-  const int mtop = n2 > 0 ? m2 : m1;
-  for (int mm = 1; mm <= mtop; ++mm) {
-    const double cm = hc[(QOL_MAXL + 2) * (QOL_MAXL + 2) + mm];
-    double nr = cm * (XA * prA - YA * piA), ni = cm * (XA * piA + YA * prA);
-    double ndr = cm * (prA + (XA * drA - YA * diA)), ndi = cm * (piA + (XA * diA + YA * drA));
-    prA = nr; piA = ni; drA = ndr; diA = ndi;
-    nr = cm * (XB * prB - YB * piB); ni = cm * (XB * piB + YB * prB);
-    ndr = cm * (prB + (XB * drB - YB * diB)); ndi = cm * (piB + (XB * diB + YB * drB));
-    prB = nr; piB = ni; drB = ndr; diB = ndi;
-    if (mm == m1) { aA0 = piA; aA1 = diA; aA2 = drA; aB0 = piB; aB1 = diB; aB2 = drB; }
-  }
-  double sA = aA0, sxA = aA1, syA = aA2, szA = 0.0, tA = 0.0, txA = 0.0, tyA = 0.0, tzA = 0.0;
-  double sB = aB0, sxB = aB1, syB = aB2, szB = 0.0, tB = 0.0, txB = 0.0, tyB = 0.0, tzB = 0.0;
-  int m = m1, l = m1;
-#pragma unroll
-  for (int e = 0; e <= LB; ++e) {
-    if (e < n1 + n2) {
-      if (e == n1) {
-        m = m2; l = m2;
-        sA = piA; sxA = diA; syA = drA; szA = 0.0; tA = 0.0; txA = 0.0; tyA = 0.0; tzA = 0.0;
-        sB = piB; sxB = diB; syB = drB; szB = 0.0; tB = 0.0; txB = 0.0; tyB = 0.0; tzB = 0.0;
-      } else if (e > 0) {
-        ++l;
-        const double a = 2.0 * l - 1.0, b = hb[l * (QOL_MAXL + 2) + m], c = hc[l * (QOL_MAXL + 2) + m];
-        double aZ = a * ZA, br2 = b * r2A;
-        double ns = (aZ * sA - br2 * tA) * c;
-        double nsx = (aZ * sxA - b * (2.0 * XA * tA + r2A * txA)) * c;
-        double nsy = (aZ * syA - b * (2.0 * YA * tA + r2A * tyA)) * c;
-        double nsz = (a * (sA + ZA * szA) - b * (2.0 * ZA * tA + r2A * tzA)) * c;
-        tA = sA; txA = sxA; tyA = syA; tzA = szA;
-        sA = ns; sxA = nsx; syA = nsy; szA = nsz;
-        aZ = a * ZB; br2 = b * r2B;
-        ns = (aZ * sB - br2 * tB) * c;
-        nsx = (aZ * sxB - b * (2.0 * XB * tB + r2B * txB)) * c;
-        nsy = (aZ * syB - b * (2.0 * YB * tB + r2B * tyB)) * c;
-        nsz = (a * (sB + ZB * szB) - b * (2.0 * ZB * tB + r2B * tzB)) * c;
-        tB = sB; txB = sxB; tyB = syB; tzB = szB;
-        sB = ns; sxB = nsx; syB = nsy; szB = nsz;
-      }
-      f(e, sA, szA, sxA, syA, sB, szB, sxB, syB);
-    }
-  }
+/* ---------------------------------------------------------------------
+ * Harmonic moments by translation.
+ *
+ * Regular solid harmonics R_l^m = r^l P_l^m(cos th) e^{i m phi} / (l+m)!
+ * (no Condon-Shortley phase) in the harmonic coordinates (X,Y,Z) = (p1,p2,p0)
+ * of a frame point p.  The sin-type basis of the RRQ systems is
+ * h_{l,m} = N_lm Im R_l^m, N_lm = sqrt((l-m)!(l+m)!), and
+ *   R_m^m = R_{m-1}^{m-1} (X+iY)/(2m),
+ *   R_l^m = ((2l-1) Z R_{l-1}^m - r^2 R_{l-2}^m) / ((l+m)(l-m)),
+ *   d_Z R_l^m = R_{l-1}^m,  d_X R_l^m = (R_{l-1}^{m-1} - R_{l-1}^{m+1})/2,
+ *   d_Y R_l^m = i (R_{l-1}^{m-1} + R_{l-1}^{m+1})/2,
+ *   R_l^m(x+rho) = sum_{lam,mu} R_lam^mu(rho) R_{l-lam}^{m-mu}(x)  (addition
+ *   theorem), R_l^{-m} = (-1)^m conj(R_l^m).
+ * The reference's moments (lap3d_close_mod.f90:832-841) integrate grad h_k
+ * along the segments x -> y_i to the boundary nodes:
+ *   Phi_k(y) = int_0^1 [grad h_k(x+t rho) - grad h_k(x)]/t dt,
+ *   Psi_k(y) = int_0^1 grad h_k(x+t rho) dt.
+ * The degree-lam part of grad h_k(x+rho) in rho integrates to 1/lam (Phi) and
+ * 1/(lam+1) (Psi), so with the node sums
+ *   M_lam^mu[d] = sum_i c_i[d] R_lam^mu(rho_i) / lam   (D weights cD)
+ *                                            / (lam+1) (S weights cS)
+ * every moment is a translation T_n^k = sum M_lam^mu R_{n-lam}^{k-mu}(x) of
+ * degree n = l-1 and the three derivative rules above.  Same quadrature as
+ * the point-wise segment rule (that rule is exact for these polynomials),
+ * a fraction of the arithmetic.
+ * --------------------------------------------------------------------- */
+
+#define MOM_WARPS 2
+#define MOM_NC 8 /* boundary nodes per chunk */
+#define MOM_CS (MOM_NC + 1)
+
+__host__ __device__ constexpr int mom_rows(int L) { return L * (L + 1); }
+/* doubles of shared memory per warp: line record (rounded to 2), then the
+ * node chunk, later reused for M (6 rows), R(x) and T (6 rows) */
+__host__ __device__ constexpr int mom_region(int L) {
+  return mom_rows(L) * MOM_CS > 12 * mom_rows(L) + (L + 1) * (L + 2) ? mom_rows(L) * MOM_CS
+                                                                      : 12 * mom_rows(L) + (L + 1) * (L + 2);
 }
+__host__ __device__ constexpr int mom_warp_doubles(int L, int nbd) { return ((6 * nbd + 4 + 1) & ~1) + mom_region(L); }
 
 template <int LB>
-__global__ void __launch_bounds__(32 * RRQ_WARPS, 2) k_rrq_moments(OrderTab T, PairIn Q, PairWS G, RRQWS R) {
-  __shared__ double s_h[2 * (QOL_MAXL + 2) * (QOL_MAXL + 2) + (QOL_MAXL + 2)];
-  __shared__ double s_rec[RRQ_WARPS][6 * 3 * QOL_MAXNQ + 4];
+__global__ void __launch_bounds__(32 * MOM_WARPS) k_rrq_moments(OrderTab T, PairIn Q, PairWS G, RRQWS R) {
+  constexpr int RPL = (LB * (LB + 1) + 31) / 32; /* real rows of M per lane */
+  extern __shared__ __align__(16) double mom_sm[];
+  __shared__ double s_rq[(QOL_MAXL + 2) * (QOL_MAXL + 2)];
+  __shared__ double s_rn[(QOL_MAXL + 2) * (QOL_MAXL + 2)];
+  __shared__ double s_rd[QOL_MAXL + 2], s_ri[QOL_MAXL + 2];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   for (int e = threadIdx.x; e < (QOL_MAXL + 2) * (QOL_MAXL + 2); e += blockDim.x) {
-    s_h[e] = c_hb[e / (QOL_MAXL + 2)][e % (QOL_MAXL + 2)];
-    s_h[(QOL_MAXL + 2) * (QOL_MAXL + 2) + e] = c_hc[e / (QOL_MAXL + 2)][e % (QOL_MAXL + 2)];
+    s_rq[e] = c_rq[e / (QOL_MAXL + 2)][e % (QOL_MAXL + 2)];
+    s_rn[e] = c_rn[e / (QOL_MAXL + 2)][e % (QOL_MAXL + 2)];
   }
-  for (int e = threadIdx.x; e < QOL_MAXL + 2; e += blockDim.x) s_h[2 * (QOL_MAXL + 2) * (QOL_MAXL + 2) + e] = c_hcm[e];
+  for (int e = threadIdx.x; e < QOL_MAXL + 2; e += blockDim.x) { s_rd[e] = c_rd[e]; s_ri[e] = c_rinv[e]; }
   __syncthreads();
-  const double* hb = s_h;
-  const double* hc = s_h + (QOL_MAXL + 2) * (QOL_MAXL + 2);
-  const long long gidx = (long long)blockIdx.x * RRQ_WARPS + wid;
+  const long long gidx = (long long)blockIdx.x * MOM_WARPS + wid;
   if (gidx >= R.nrrq) return;
   int lo = 0, hi = R.npan;
   while (hi - lo > 1) {
@@ -1011,88 +941,226 @@ __global__ void __launch_bounds__(32 * RRQ_WARPS, 2) k_rrq_moments(OrderTab T, P
   const int j_loc = (int)(gidx - R.rrq_off[pan]);
   const long long p0 = Q.tcxi[pan] - 1;
   const int tl = G.grp[p0 + G.off[(size_t)pan * 8 + T.nlevel + 1] + j_loc];
-  const int hd = T.hd, nq = T.nquad, nbd = 3 * nq, L = T.nterms, ng = T.ng;
+  const int hd = T.hd, nq = T.nquad, nbd = 3 * nq, L = T.nterms;
   const double* fr = R.frame + (size_t)pan * RRQ_FRAME;
   const double* bx = R.bx + (size_t)pan * 3 * nbd;
   const double alpha = fr[12];
-  double xt[3];
+  double xt0, xt1, xt2;
   {
     const double* x = Q.tcx + 3 * (p0 + tl);
     double d0 = x[0] - fr[9], d1 = x[1] - fr[10], d2 = x[2] - fr[11];
-    for (int i = 0; i < 3; ++i) xt[i] = alpha * (fr[i] * d0 + fr[i + 3] * d1 + fr[i + 6] * d2);
+    xt0 = alpha * (fr[0] * d0 + fr[3] * d1 + fr[6] * d2);
+    xt1 = alpha * (fr[1] * d0 + fr[4] * d1 + fr[7] * d2);
+    xt2 = alpha * (fr[2] * d0 + fr[5] * d1 + fr[8] * d2);
   }
-  const double xt0 = xt[0], xt1 = xt[1], xt2 = xt[2];
-  double* rec = s_rec[wid];
-  const double* grec = R.line + (size_t)gidx * (6 * nbd + 4);
-  for (int e = lane; e < 6 * nbd + 4; e += 32) rec[e] = grec[e];
+  double* rec = mom_sm + (size_t)wid * mom_warp_doubles(L, nbd);
+  double* ch = rec + ((6 * nbd + 4 + 1) & ~1);
+  {
+    const double* grec = R.line + (size_t)gidx * (6 * nbd + 4);
+    for (int e = lane; e < 6 * nbd + 4; e += 32) rec[e] = grec[e];
+  }
   __syncwarp();
   const double* cD = rec;
   const double* cS = rec + 3 * nbd;
-  const double lint0 = rec[6 * nbd], lint1 = rec[6 * nbd + 1], lint2 = rec[6 * nbd + 2], Omega = rec[6 * nbd + 3];
-  const double i4p = 1.0 / (4.0 * QOL_PI);
-  /* ceil(L/2) lanes per point group, lane idx handles the column pair
-   * (idx+1, L-idx): every lane runs L+1 recurrence steps */
-  const int PL = (L + 1) / 2, GP = 32 / PL;
-  const int grp = lane / PL, idx = lane % PL;
-  const bool lane_on = grp < GP;
-  const int m1 = idx + 1, m2 = L - idx;
-  const int n1 = L - m1 + 1, n2 = (m2 > m1) ? (L - m2 + 1) : 0;
-  double acc[LB + 1][5];
+  const int NE = mom_rows(L);
+  /* (A) R_lam^mu(rho_i), lam <= L-1, mu >= 0, chunks of MOM_NC nodes: lane
+   * (g, j) evaluates node c0+j over the column pairs (p, L-1-p), p = g and
+   * g+4 (L <= 16: at most 8 pairs), the two columns of a pair as two
+   * recurrence chains in flight, into ch[row][j], row = 2 entry(lam,mu) + re/im.
+   * (B) each lane contracts its rows e = lane + 32 r with the 6 weights. */
+  double acc[RPL][6];
 #pragma unroll
-  for (int e = 0; e <= LB; ++e)
+  for (int r = 0; r < RPL; ++r)
 #pragma unroll
-    for (int c = 0; c < 5; ++c) acc[e][c] = 0.0;
-  double sumcD0 = 0.0, sumcD1 = 0.0, sumcD2 = 0.0;
-  const int npts = nbd * ng;
-  for (int p = grp; p < npts; p += GP) {
-    if (!lane_on) break;
-    const int i = p / ng, g = p % ng;
-    const double t = T.tq[g], aD = T.wq[g] / t, aS = T.wq[g];
-    const double uD0 = aD * cD[3 * i], uD1 = aD * cD[3 * i + 1], uD2 = aD * cD[3 * i + 2];
-    const double uS0 = aS * cS[3 * i], uS1 = aS * cS[3 * i + 1], uS2 = aS * cS[3 * i + 2];
-    if (idx == 0) { sumcD0 += uD0; sumcD1 += uD1; sumcD2 += uD2; }
-    const double* y = bx + 3 * i;
-    const double z0 = xt0 + t * (y[0] - xt0), z1 = xt1 + t * (y[1] - xt1), z2 = xt2 + t * (y[2] - xt2);
-    harm_pair_re<LB>(L, m1, m2, n1, n2, z0, z1, z2, hb, hc, [&](int e, double h, double gx, double gy, double gz) {
-      acc[e][0] -= uD0 * gx + uD1 * gy + uD2 * gz;
-      acc[e][1] += uD1 * gz - uD2 * gy;
-      acc[e][2] += uD2 * gx - uD0 * gz;
-      acc[e][3] += uD0 * gy - uD1 * gx;
-      acc[e][4] += uS0 * gx + uS1 * gy + uS2 * gz;
-    });
-  }
-  /* combine the point groups into group 0 (same idx, lanes idx + g*PL) */
+    for (int c = 0; c < 6; ++c) acc[r][c] = 0.0;
+  int erow[RPL];
 #pragma unroll
-  for (int e = 0; e <= LB; ++e)
-#pragma unroll
-    for (int c = 0; c < 5; ++c) {
-      double v = acc[e][c];
-      for (int gg = 1; gg < GP; ++gg) {
-        double w = __shfl_sync(0xffffffffu, acc[e][c], (lane + gg * PL) & 31);
-        if (grp == 0) v += w;
+  for (int r = 0; r < RPL; ++r) erow[r] = min(lane + 32 * r, NE - 1) * MOM_CS;
+  const int np = (L + 1) / 2, g4 = lane >> 3, jn = lane & 7;
+  const int pa = g4, pb = g4 + 4, qa = L - 1 - pa, qb = L - 1 - pb;
+  for (int c0 = 0; c0 < nbd; c0 += MOM_NC) {
+    if (pa < np) {
+      const int i = min(c0 + jn, nbd - 1);
+      const double Z = bx[3 * i] - xt0, X = bx[3 * i + 1] - xt1, Y = bx[3 * i + 2] - xt2;
+      const double r2 = X * X + Y * Y + Z * Z;
+      /* diagonal R_m^m up to column qa, keeping columns pa, pb, qb, qa */
+      double dr = 1.0, di = 0.0;
+      double a1r = 1.0, a1i = 0.0, b1r = 1.0, b1i = 0.0, b2r = 1.0, b2i = 0.0;
+      for (int mm = 1; mm <= qa; ++mm) {
+        const double t = dr * X - di * Y;
+        di = (dr * Y + di * X) * s_rd[mm];
+        dr = t * s_rd[mm];
+        if (mm == pa) { a1r = dr; a1i = di; }
+        if (mm == pb) { b1r = dr; b1i = di; }
+        if (mm == qb) { b2r = dr; b2i = di; }
       }
-      acc[e][c] = v;
+      auto pair = [&](int c1, double d1r, double d1i, int c2, double d2r, double d2i) {
+        const int n1 = L - c1, n2 = c2 > c1 ? L - c2 : 0;
+        double ur = d1r, ui = d1i, vr = 0.0, vi = 0.0; /* column c1: R_{l}, R_{l-1} */
+        double sr = d2r, si = d2i, tr = 0.0, ti = 0.0; /* column c2 */
+        for (int e = 0; e < n1; ++e) {
+          if (e > 0) {
+            const int l = c1 + e;
+            const double q = s_rq[l * (QOL_MAXL + 2) + c1], a = (2.0 * l - 1.0) * Z;
+            const double nr = (a * ur - r2 * vr) * q, ni = (a * ui - r2 * vi) * q;
+            vr = ur; vi = ui; ur = nr; ui = ni;
+          }
+          const int row = (c1 + e) * (c1 + e + 1) + 2 * c1;
+          ch[row * MOM_CS + jn] = ur;
+          ch[(row + 1) * MOM_CS + jn] = ui;
+          if (e < n2) {
+            if (e > 0) {
+              const int l = c2 + e;
+              const double q = s_rq[l * (QOL_MAXL + 2) + c2], a = (2.0 * l - 1.0) * Z;
+              const double nr = (a * sr - r2 * tr) * q, ni = (a * si - r2 * ti) * q;
+              tr = sr; ti = si; sr = nr; si = ni;
+            }
+            const int row2 = (c2 + e) * (c2 + e + 1) + 2 * c2;
+            ch[row2 * MOM_CS + jn] = sr;
+            ch[(row2 + 1) * MOM_CS + jn] = si;
+          }
+        }
+      };
+      pair(pa, a1r, a1i, qa, dr, di);
+      if (pb < np) pair(pb, b1r, b1i, qb, b2r, b2i);
     }
-  for (int o = 16; o > 0; o >>= 1) {
-    sumcD0 += __shfl_xor_sync(0xffffffffu, sumcD0, o);
-    sumcD1 += __shfl_xor_sync(0xffffffffu, sumcD1, o);
-    sumcD2 += __shfl_xor_sync(0xffffffffu, sumcD2, o);
+    __syncwarp();
+    const int nj = min(MOM_NC, nbd - c0);
+    for (int jj = 0; jj < nj; ++jj) {
+      const int ii = c0 + jj;
+      const double w0 = cD[3 * ii], w1 = cD[3 * ii + 1], w2 = cD[3 * ii + 2];
+      const double w3 = cS[3 * ii], w4 = cS[3 * ii + 1], w5 = cS[3 * ii + 2];
+#pragma unroll
+      for (int r = 0; r < RPL; ++r) {
+        const double v = ch[erow[r] + jj];
+        acc[r][0] += v * w0; acc[r][1] += v * w1; acc[r][2] += v * w2;
+        acc[r][3] += v * w3; acc[r][4] += v * w4; acc[r][5] += v * w5;
+      }
+    }
+    __syncwarp();
   }
-  /* the x point: (s0, l/4pi - sumcD) (x) (0, grad h(x)) and h(x) Omega/4pi */
+  /* M[entry][6 components][re,im] with the 1/lam (D) and 1/(lam+1) (S)
+   * segment weights; then R(x) up to degree L; then T */
+  double* Mt = ch;
+  double* Rx = ch + 6 * NE;
+  double* Tt = Rx + (L + 1) * (L + 2);
+#pragma unroll
+  for (int r = 0; r < RPL; ++r) {
+    const int e = lane + 32 * r;
+    if (e < NE) {
+      const int ent = e >> 1, ri = e & 1;
+      int lam = 0;
+      while ((lam + 1) * (lam + 2) / 2 <= ent) ++lam;
+      const double wD = s_ri[lam], wS = s_ri[lam + 1];
+      double* dst = Mt + ent * 12 + ri;
+      dst[0] = acc[r][0] * wD; dst[2] = acc[r][1] * wD; dst[4] = acc[r][2] * wD;
+      dst[6] = acc[r][3] * wS; dst[8] = acc[r][4] * wS; dst[10] = acc[r][5] * wS;
+    }
+  }
+  if (lane <= L) { /* column m = lane of R(x) */
+    const int m = lane;
+    const double Z = xt0, X = xt1, Y = xt2, r2 = X * X + Y * Y + Z * Z;
+    double dr = 1.0, di = 0.0;
+    for (int mm = 1; mm <= m; ++mm) {
+      const double t = dr * X - di * Y;
+      di = (dr * Y + di * X) * s_rd[mm];
+      dr = t * s_rd[mm];
+    }
+    double ar = dr, ai = di, br = 0.0, bi = 0.0;
+    for (int l = m; l <= L; ++l) {
+      if (l > m) {
+        const double q = s_rq[l * (QOL_MAXL + 2) + m], a = (2.0 * l - 1.0) * Z;
+        const double nr = (a * ar - r2 * br) * q, ni = (a * ai - r2 * bi) * q;
+        br = ar; bi = ai; ar = nr; ai = ni;
+      }
+      const int ent = l * (l + 1) / 2 + m;
+      Rx[2 * ent] = ar; Rx[2 * ent + 1] = ai;
+    }
+  }
+  __syncwarp();
+  /* (D) translation: this lane's terms of the schedule, its outputs one
+   * after the other (each output belongs to one lane) */
+  {
+    double a[12];
+#pragma unroll
+    for (int c = 0; c < 12; ++c) a[c] = 0.0;
+    int cur = -1;
+    const unsigned* tab = T.xsched + lane;
+    const int nst = T.xsteps;
+    unsigned wn = nst > 0 ? __ldg(tab) : 0u;
+    for (int s = 0; s < nst; ++s) {
+      const unsigned w = wn;
+      if (s + 1 < nst) wn = __ldg(tab + 32 * (s + 1));
+      if (!(w & (1u << 27))) break; /* a lane's terms are contiguous from step 0 */
+      const int em = w & 255, ex = (w >> 8) & 255, out = (w >> 16) & 255;
+      if (out != cur) {
+        if (cur >= 0) {
+#pragma unroll
+          for (int c = 0; c < 12; ++c) { Tt[cur * 12 + c] = a[c]; a[c] = 0.0; }
+        }
+        cur = out;
+      }
+      const double2 rv = *reinterpret_cast<const double2*>(Rx + 2 * ex);
+      double c = rv.x, d = rv.y;
+      if (w & (1u << 26)) { c = -c; d = -d; }
+      if (w & (1u << 25)) d = -d;
+      double p = d, q = c;
+      if (w & (1u << 24)) { p = -d; q = -c; }
+      const double2* mv = reinterpret_cast<const double2*>(Mt + em * 12);
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        const double2 v = mv[k];
+        a[2 * k] += v.x * c - v.y * p;
+        a[2 * k + 1] += v.y * q + v.x * d;
+      }
+    }
+    if (cur >= 0) {
+#pragma unroll
+      for (int c = 0; c < 12; ++c) Tt[cur * 12 + c] = a[c];
+    }
+  }
+  __syncwarp();
+  /* (E) the moments of h_{l,m}: T of degree l-1 at orders m-1, m, m+1, and
+   * the x point: (s0, lint/4pi) (x) (0, grad h(x)) and h(x) Omega/4pi */
+  const double i4p = 1.0 / (4.0 * QOL_PI);
+  const double lint0 = rec[6 * nbd], lint1 = rec[6 * nbd + 1], lint2 = rec[6 * nbd + 2], Omega = rec[6 * nbd + 3];
   const double s0 = -Omega * i4p;
-  const double wv0 = lint0 * i4p - sumcD0, wv1 = lint1 * i4p - sumcD1, wv2 = lint2 * i4p - sumcD2;
+  const double wv0 = lint0 * i4p, wv1 = lint1 * i4p, wv2 = lint2 * i4p;
   double* JD = R.JD + (size_t)gidx * 4 * hd;
   double* RS = R.RS + (size_t)gidx * hd;
-  if (grp == 0) {
-    harm_pair_re<LB>(L, m1, m2, n1, n2, xt0, xt1, xt2, hb, hc, [&](int e, double h, double gx, double gy, double gz) {
-      const int m = e < n1 ? m1 : m2, l = e < n1 ? m1 + e : m2 + (e - n1);
-      const int k = l * (l - 1) / 2 + (m - 1);
-      JD[0 * hd + k] = acc[e][0] - (wv0 * gx + wv1 * gy + wv2 * gz);
-      JD[1 * hd + k] = acc[e][1] + s0 * gx + (wv1 * gz - wv2 * gy);
-      JD[2 * hd + k] = acc[e][2] + s0 * gy + (wv2 * gx - wv0 * gz);
-      JD[3 * hd + k] = acc[e][3] + s0 * gz + (wv0 * gy - wv1 * gx);
-      RS[k] = acc[e][4] + h * Omega * i4p;
-    });
+  for (int k = lane; k < hd; k += 32) {
+    int l = 1;
+    while ((l + 1) * l / 2 <= k) ++l;
+    const int m = k - l * (l - 1) / 2 + 1, n = l - 1;
+    const double Nf = s_rn[l * (QOL_MAXL + 2) + m];
+    /* P[d][c]: component c (x,y,z frame) of the d-weighted moment */
+    double PD[3][3], PS[3][3];
+    const double* t0 = Tt + (n * (n + 1) / 2 + (m - 1)) * 12; /* order m-1 (always <= n) */
+    const bool h1 = m <= n, h2 = m + 1 <= n;
+    const double* t1 = Tt + (n * (n + 1) / 2 + m) * 12;
+    const double* t2 = Tt + (n * (n + 1) / 2 + m + 1) * 12;
+#pragma unroll
+    for (int d = 0; d < 6; ++d) {
+      const double ar = t0[2 * d], ai = t0[2 * d + 1];
+      const double zi = h1 ? t1[2 * d + 1] : 0.0;
+      const double br = h2 ? t2[2 * d] : 0.0, bi = h2 ? t2[2 * d + 1] : 0.0;
+      double* P = d < 3 ? PD[d] : PS[d - 3];
+      P[0] = Nf * zi;
+      P[1] = 0.5 * Nf * (ai - bi);
+      P[2] = 0.5 * Nf * (ar + br);
+    }
+    /* h(x) and grad h(x) */
+    const double hx = Nf * Rx[2 * (l * (l + 1) / 2 + m) + 1];
+    const double* q0 = Rx + 2 * (n * (n + 1) / 2 + (m - 1));
+    const double gzi = h1 ? Rx[2 * (n * (n + 1) / 2 + m) + 1] : 0.0;
+    const double q2r = h2 ? Rx[2 * (n * (n + 1) / 2 + m + 1)] : 0.0;
+    const double q2i = h2 ? Rx[2 * (n * (n + 1) / 2 + m + 1) + 1] : 0.0;
+    const double gx = Nf * gzi, gy = 0.5 * Nf * (q0[1] - q2i), gz = 0.5 * Nf * (q0[0] + q2r);
+    JD[0 * hd + k] = -(PD[0][0] + PD[1][1] + PD[2][2]) - (wv0 * gx + wv1 * gy + wv2 * gz);
+    JD[1 * hd + k] = (PD[1][2] - PD[2][1]) + s0 * gx + (wv1 * gz - wv2 * gy);
+    JD[2 * hd + k] = (PD[2][0] - PD[0][2]) + s0 * gy + (wv2 * gx - wv0 * gz);
+    JD[3 * hd + k] = (PD[0][1] - PD[1][0]) + s0 * gz + (wv0 * gy - wv1 * gx);
+    RS[k] = (PS[0][0] + PS[1][1] + PS[2][2]) + hx * Omega * i4p;
   }
 }
 
@@ -1288,18 +1356,41 @@ cudaError_t qol_launch_rrq_panel(const OrderTab& T, const PanelIn& P, const Pair
   k_rrq_panel<<<npan, 256, 0, st>>>(T, P, G, R, chart);
   return cudaGetLastError();
 }
-cudaError_t qol_launch_rrq_target(const OrderTab& T, const PairIn& Q, const PairWS& G, const RRQWS& R, int exterior,
-                                  cudaStream_t st) {
+cudaError_t qol_launch_rrq_ssq(const OrderTab& T, const PairIn& Q, const PairWS& G, const RRQWS& R, cudaStream_t st) {
+  if (R.nrrq == 0) return cudaSuccess;
+  k_rrq_ssq<<<(unsigned)((3 * R.nrrq + 127) / 128), 128, 0, st>>>(T, Q, G, R);
+  return cudaGetLastError();
+}
+cudaError_t qol_launch_rrq_geom(const OrderTab& T, const PairIn& Q, const PairWS& G, const RRQWS& R, int exterior,
+                                cudaStream_t st) {
   if (R.nrrq == 0) return cudaSuccess;
   long long nb = (R.nrrq + RRQ_WARPS - 1) / RRQ_WARPS;
-  k_rrq_ssq<<<(unsigned)((3 * R.nrrq + 127) / 128), 128, 0, st>>>(T, Q, G, R);
   k_rrq_geom<<<(unsigned)nb, 32 * RRQ_WARPS, 0, st>>>(T, Q, G, R, exterior);
-  if (T.nterms <= 4) k_rrq_moments<4><<<(unsigned)nb, 32 * RRQ_WARPS, 0, st>>>(T, Q, G, R);
-  else if (T.nterms <= 6) k_rrq_moments<6><<<(unsigned)nb, 32 * RRQ_WARPS, 0, st>>>(T, Q, G, R);
-  else if (T.nterms <= 8) k_rrq_moments<8><<<(unsigned)nb, 32 * RRQ_WARPS, 0, st>>>(T, Q, G, R);
-  else if (T.nterms <= 10) k_rrq_moments<10><<<(unsigned)nb, 32 * RRQ_WARPS, 0, st>>>(T, Q, G, R);
-  else if (T.nterms <= 13) k_rrq_moments<13><<<(unsigned)nb, 32 * RRQ_WARPS, 0, st>>>(T, Q, G, R);
-  else k_rrq_moments<16><<<(unsigned)nb, 32 * RRQ_WARPS, 0, st>>>(T, Q, G, R);
+  return cudaGetLastError();
+}
+cudaError_t qol_launch_rrq_target(const OrderTab& T, const PairIn& Q, const PairWS& G, const RRQWS& R, int exterior,
+                                  cudaStream_t st) {
+  cudaError_t e = qol_launch_rrq_ssq(T, Q, G, R, st);
+  if (e == cudaSuccess) e = qol_launch_rrq_geom(T, Q, G, R, exterior, st);
+  if (e == cudaSuccess) e = qol_launch_rrq_moments(T, Q, G, R, st);
+  return e;
+}
+cudaError_t qol_launch_rrq_moments(const OrderTab& T, const PairIn& Q, const PairWS& G, const RRQWS& R,
+                                   cudaStream_t st) {
+  if (R.nrrq == 0) return cudaSuccess;
+  const unsigned nbm = (unsigned)((R.nrrq + MOM_WARPS - 1) / MOM_WARPS);
+  const size_t smem = sizeof(double) * MOM_WARPS * mom_warp_doubles(T.nterms, 3 * T.nquad);
+  auto go = [&](auto kern) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    kern<<<nbm, 32 * MOM_WARPS, smem, st>>>(T, Q, G, R);
+  };
+  if (T.nterms <= 4) go(k_rrq_moments<4>);
+  else if (T.nterms <= 6) go(k_rrq_moments<6>);
+  else if (T.nterms <= 8) go(k_rrq_moments<8>);
+  else if (T.nterms <= 10) go(k_rrq_moments<10>);
+  else if (T.nterms <= 12) go(k_rrq_moments<12>);
+  else if (T.nterms <= 14) go(k_rrq_moments<14>);
+  else go(k_rrq_moments<16>);
   return cudaGetLastError();
 }
 cudaError_t qol_launch_rrq_apply(const OrderTab& T, const PanelIn& P, const PairIn& Q, const PairWS& G,

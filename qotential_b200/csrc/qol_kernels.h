@@ -18,6 +18,8 @@ struct OrderTab {
   const double* Mb;    /* (3 nquad + 3) x hd, row-major: boundary + vertex interpolation */
   const double* umatr; /* hd x hd col-major (vals -> coefs) */
   const double* vruv;  /* 2 x hd VR nodes of degree korder */
+  const unsigned* xsched; /* xsteps x 32 translation terms (qolh::xlate_schedule) */
+  int xsteps;
 };
 
 /* panel geometry (reference layouts: sx(3,nsrc) etc.) */
@@ -77,6 +79,12 @@ cudaError_t qol_launch_direct(const OrderTab& T, const PanelIn& P, const PairIn&
 cudaError_t qol_launch_scan(int npan, int lev, const int* cnt, long long* off, cudaStream_t st);
 cudaError_t qol_launch_rrq_panel(const OrderTab& T, const PanelIn& P, const PairWS& G, const RRQWS& R, int npan,
                                  const double* chart, cudaStream_t st);
+cudaError_t qol_launch_rrq_ssq(const OrderTab& T, const PairIn& Q, const PairWS& G, const RRQWS& R, cudaStream_t st);
+cudaError_t qol_launch_rrq_geom(const OrderTab& T, const PairIn& Q, const PairWS& G, const RRQWS& R, int exterior,
+                                cudaStream_t st);
+cudaError_t qol_launch_rrq_moments(const OrderTab& T, const PairIn& Q, const PairWS& G, const RRQWS& R,
+                                   cudaStream_t st);
+/* ssq + geom + moments */
 cudaError_t qol_launch_rrq_target(const OrderTab& T, const PairIn& Q, const PairWS& G, const RRQWS& R, int exterior,
                                   cudaStream_t st);
 cudaError_t qol_launch_rrq_apply(const OrderTab& T, const PanelIn& P, const PairIn& Q, const PairWS& G,

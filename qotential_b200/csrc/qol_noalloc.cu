@@ -147,6 +147,9 @@ int na_tables(NoAllocDev& D, int nterms, int orderff, int nquad, cudaStream_t st
   size_t o_tq = put(tq.data(), 8 * tq.size()), o_wq = put(wq.data(), 8 * wq.size());
   size_t o_Mb = put(Mb.data(), 8 * Mb.size()), o_um = put(um.data(), 8 * um.size());
   size_t o_vr = put(vr.data(), 8 * vr.size());
+  std::vector<uint32_t> xs;
+  qolh::xlate_schedule(nterms, xs, T.xsteps);
+  size_t o_xs = put(xs.data(), sizeof(uint32_t) * xs.size());
   size_t bytes = (stage.size() + 255) & ~(size_t)255;
   if (bytes > QOL_NOALLOC_SCRATCH_BYTES / 2)
     return na_fail(QOL_ERR_LIMIT, "qol_rrq_noalloc: tables of this order exceed half of the 16 MiB scratch");
@@ -165,6 +168,7 @@ int na_tables(NoAllocDev& D, int nterms, int orderff, int nquad, cudaStream_t st
   T.gl16x = (const double*)dp(o_16x); T.gl16w = (const double*)dp(o_16w);
   T.tq = (const double*)dp(o_tq); T.wq = (const double*)dp(o_wq);
   T.Mb = (const double*)dp(o_Mb); T.umatr = (const double*)dp(o_um); T.vruv = (const double*)dp(o_vr);
+  T.xsched = (const unsigned*)dp(o_xs);
   D.T = T;
   D.table_bytes = bytes;
   D.key = key;
