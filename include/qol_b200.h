@@ -146,6 +146,12 @@ const char* qol_noalloc_last_error(void);
  * the switch (-1: read only).  (No counterpart in the reference; its timeinfo
  * is the host-side analogue.) */
 #define QOL_NPHASE 9
+/* Wall-clock milestones (ms from the start) of the last
+ * qol_getnearquad_lap_rrq call: [0] inputs queued, [1] all panel chunks
+ * queued, [2] all value copies queued, [3] values landed in pinned staging,
+ * [4] every host task done (indices filled, values in the caller's arrays),
+ * [5] return, [6] COO indices filled.  No counterpart in the reference. */
+int qol_last_host_times(double* ms7);
 const char* qol_last_error(void);
 int qol_kernel_times(int enable, double* ms, qol_int* calls);
 int qol_version(void);

@@ -4,6 +4,14 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <functional>
+#include <thread>
+#include <sys/mman.h>
+#include <unistd.h>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -82,7 +90,7 @@ struct OrderCache {
 
 std::map<long long, std::unique_ptr<OrderCache>> g_orders;
 bool g_coefs_uploaded = false;
-Arena g_arena, g_arena2;
+Arena g_arena, g_arena2, g_arena_io; /* pipeline, per-pair RRQ storage, host-entry buffers */
 /* per-phase device milliseconds of the pipeline (diagnostics) */
 int g_ktime_on = 0;
 double g_ktime[QOL_NPHASE] = {};
@@ -185,10 +193,37 @@ int order_tables(int nterms, int orderff, int nquad, OrderCache** out) {
 }
 
 /* ---------------- the pipeline on device pointers ---------------- */
+/* events recorded in stream order; the interval from ev[k] to ev[k+1]
+ * belongs to phase ph[k] (-1: none) */
 struct Timing {
-  cudaEvent_t ev[QOL_NPHASE + 1];
+  std::vector<cudaEvent_t> ev;
+  std::vector<int> ph;
   bool on = false;
 };
+
+/* after the stream passed every event: accumulate into timeinfo (the
+ * reference's slots) and the per-phase totals, release the events */
+void finish_timing(Timing& tm, double* timeinfo) {
+  if (!tm.on) return;
+  double ms[QOL_NPHASE] = {};
+  for (size_t k = 0; k + 1 < tm.ev.size(); ++k) {
+    float t = 0.f;
+    if (tm.ph[k] >= 0 && cudaEventElapsedTime(&t, tm.ev[k], tm.ev[k + 1]) == cudaSuccess) ms[tm.ph[k]] += t;
+  }
+  if (timeinfo) {
+    timeinfo[0] += 1e-3 * ms[0];                   /* patch levels */
+    timeinfo[1] += 1e-3 * ms[3];                   /* per-panel RRQ precompute */
+    timeinfo[2] += 1e-3 * (ms[1] + ms[2]);         /* classification + level sums */
+    timeinfo[5] += 1e-3 * (ms[4] + ms[5] + ms[6]); /* SSQ / solid angle / moments */
+    timeinfo[7] += 1e-3 * (ms[7] + ms[8]);         /* solves + COO */
+  }
+  for (int i = 0; i < QOL_NPHASE; ++i) g_ktime[i] += ms[i];
+  g_kcalls += 1;
+  for (cudaEvent_t e : tm.ev) cudaEventDestroy(e);
+  tm.ev.clear();
+  tm.ph.clear();
+  tm.on = false;
+}
 
 struct Job {
   int npan, nterms, nquad, orderff, exterior, subtract_naive;
@@ -199,7 +234,10 @@ struct Job {
   double *vs, *vd, *omega, *ialpha;
   long long *si, *sj;
   const double* chart;
-  const long long* tcxi_host; /* host copy */
+  /* optional: the per-pair phase over these panel chunks (boundaries, first 0,
+   * last npan), after_chunk(c) once chunk c's values are queued */
+  const std::vector<long long>* chunk_pan;
+  std::function<void(int)> after_chunk;
 };
 
 int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* hist_out, std::vector<int>* grp_out,
@@ -253,19 +291,26 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
   CK(cudaMemsetAsync(G.cnt, 0, sizeof(int) * (size_t)npan * 8, st));
   CK(cudaMemsetAsync(G.off, 0, sizeof(int) * (size_t)npan * 8, st));
   Timing tm;
-  if (timeinfo || g_ktime_on) {
-    for (int i = 0; i <= QOL_NPHASE; ++i) CK(cudaEventCreate(&tm.ev[i]));
-    tm.on = true;
-  }
-  auto rec = [&](int i) { if (tm.on) cudaEventRecord(tm.ev[i], st); };
+  tm.on = timeinfo || g_ktime_on;
+  auto rec = [&](int phase) {
+    if (!tm.on) return;
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return;
+    cudaEventRecord(e, st);
+    tm.ev.push_back(e);
+    tm.ph.push_back(phase);
+  };
   rec(0);
   CK(qol_launch_levels(T, J.P, W, npan, st));
   rec(1);
   CK(qol_launch_classify(T, J.Q, W, G, npan, st));
   CK(qol_launch_scan(npan, T.nlevel + 1, G.cnt, rrq_off, st));
-  long long nrrq = 0;
-  CK(cudaMemcpyAsync(&nrrq, rrq_off + npan, sizeof(long long), cudaMemcpyDeviceToHost, st));
+  /* RRQ pair offsets per panel (all of them when the per-pair phase is chunked) */
+  std::vector<long long> off_h(J.chunk_pan ? npan + 1 : 1);
+  CK(cudaMemcpyAsync(off_h.data(), J.chunk_pan ? rrq_off : rrq_off + npan, sizeof(long long) * off_h.size(),
+                     cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
+  const long long nrrq = off_h.back();
   R.nrrq = nrrq;
   /* per-pair RRQ moment storage (separate arena: its size is known only now) */
   rc = g_arena2.reserve(sizeof(double) * (size_t)std::max<long long>(nrrq, 1) * (5 * hd + 6 * nbd + 4 + 3 * (2 * nq + 3)) +
@@ -281,22 +326,31 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
   rec(2);
   CK(qol_launch_direct(T, J.P, J.Q, W, G, O, npan, st));
   rec(3);
-  if (nrrq > 0) {
-    CK(qol_launch_rrq_panel(T, J.P, G, R, npan, J.chart, st));
-    rec(4);
-    CK(qol_launch_rrq_ssq(T, J.Q, G, R, st));
-    rec(5);
-    CK(qol_launch_rrq_geom(T, J.Q, G, R, J.exterior, st));
-    rec(6);
-    CK(qol_launch_rrq_moments(T, J.Q, G, R, st));
-    rec(7);
-    CK(qol_launch_rrq_apply(T, J.P, J.Q, G, R, O, npan, st));
-    rec(8);
-  } else {
-    for (int i = 4; i <= 8; ++i) rec(i);
+  if (nrrq > 0) CK(qol_launch_rrq_panel(T, J.P, G, R, npan, J.chart, st));
+  const int nch = J.chunk_pan ? (int)J.chunk_pan->size() - 1 : 1;
+  for (int c = 0; c < nch; ++c) {
+    const long long a = J.chunk_pan ? (*J.chunk_pan)[c] : 0, b = J.chunk_pan ? (*J.chunk_pan)[c + 1] : npan;
+    R.plo = (int)a; R.phi = (int)b;
+    R.glo = J.chunk_pan ? off_h[a] : 0;
+    R.ghi = J.chunk_pan ? off_h[b] : nrrq;
+    if (R.ghi > R.glo) {
+      rec(4);
+      CK(qol_launch_rrq_ssq(T, J.Q, G, R, st));
+      rec(5);
+      CK(qol_launch_rrq_geom(T, J.Q, G, R, J.exterior, st));
+      rec(6);
+      CK(qol_launch_rrq_moments(T, J.Q, G, R, st));
+      rec(7);
+      CK(qol_launch_rrq_apply(T, J.P, J.Q, G, R, O, st));
+    }
+    if (J.after_chunk) {
+      rec(-1);
+      J.after_chunk(c);
+    }
   }
+  rec(8);
   if (J.si) CK(qol_launch_coo_index(T, J.Q, J.si, J.sj, npan, st));
-  rec(9);
+  rec(-1);
   if (hist_out || grp_out || cnt_out || tm.on) {
     CK(cudaStreamSynchronize(st));
   }
@@ -314,20 +368,7 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
     grp_out->resize(ntcx);
     CK(cudaMemcpy(grp_out->data(), G.grp, sizeof(int) * ntcx, cudaMemcpyDeviceToHost));
   }
-  if (tm.on) {
-    float ms[QOL_NPHASE];
-    for (int i = 0; i < QOL_NPHASE; ++i) cudaEventElapsedTime(&ms[i], tm.ev[i], tm.ev[i + 1]);
-    if (timeinfo) {
-      timeinfo[0] += 1e-3 * ms[0];                   /* patch levels */
-      timeinfo[1] += 1e-3 * ms[3];                   /* per-panel RRQ precompute */
-      timeinfo[2] += 1e-3 * (ms[1] + ms[2]);         /* classification + level sums */
-      timeinfo[5] += 1e-3 * (ms[4] + ms[5] + ms[6]); /* SSQ / solid angle / moments */
-      timeinfo[7] += 1e-3 * (ms[7] + ms[8]);         /* solves + COO */
-    }
-    for (int i = 0; i < QOL_NPHASE; ++i) g_ktime[i] += ms[i];
-    g_kcalls += 1;
-    for (int i = 0; i <= QOL_NPHASE; ++i) cudaEventDestroy(tm.ev[i]);
-  }
+  finish_timing(tm, timeinfo);
   return 0;
 }
 
@@ -367,6 +408,170 @@ int tables_match(int nquad, int korder, const double* tgl, const double* wgl, co
     for (size_t i = 0; i < um.size(); ++i)
       if (std::fabs(um[i] - umatr[i]) > 1e-9 * (1.0 + std::fabs(um[i]))) return 0;
   return 1;
+}
+
+/* ---------------- host-buffer output: staged, overlapped copies ---------------- */
+/* The host-pointer entry point runs the pipeline over panel chunks; each
+ * chunk's COO values leave the GPU on a copy stream while the next chunk
+ * computes, through a ring of pinned staging buffers that host threads empty
+ * into the caller's arrays.  The COO indices are a layout function of
+ * tcxrow/tcxi (k_coo_index computes the same), so that entry point fills them
+ * on host threads while the GPU works instead of moving them over the link. */
+constexpr size_t kStageBytes = (size_t)16 << 20;
+/* wall-clock milestones of the last host-pointer call, ms from its start:
+ * inputs queued, all chunks queued, value copies queued, values landed,
+ * every host task done, end, indices filled */
+double g_host_ms[7] = {0, 0, 0, 0, 0, 0, 0};
+inline double ms_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+constexpr int kNStage = 16;
+
+struct StageRing {
+  void* buf[kNStage] = {};
+  cudaEvent_t ev[kNStage] = {};
+  cudaStream_t cs = nullptr;
+  bool ok = false;
+  int init() {
+    if (ok) return 0;
+    for (int b = 0; b < kNStage; ++b) {
+      CK(cudaMallocHost(&buf[b], kStageBytes));
+      CK(cudaEventCreateWithFlags(&ev[b], cudaEventDisableTiming));
+    }
+    CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    ok = true;
+    return 0;
+  }
+} g_ring;
+
+/* host threads draining a task queue in order (the index fills are queued
+ * first and run while the GPU computes, the staging copies follow);
+ * finish() runs what is queued and joins */
+class Workers {
+ public:
+  explicit Workers(int n) {
+    for (int i = 0; i < n; ++i) th_.emplace_back([this] { loop(); });
+  }
+  ~Workers() { finish(); }
+  void submit(std::function<void()> f) {
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      q_.push_back(std::move(f));
+    }
+    cv_.notify_one();
+  }
+  void finish() {
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      if (closed_) return;
+      closed_ = true;
+    }
+    cv_.notify_all();
+    for (auto& t : th_) t.join();
+  }
+
+ private:
+  void loop() {
+    for (;;) {
+      std::function<void()> f;
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&] { return closed_ || !q_.empty(); });
+        if (q_.empty()) return;
+        f = std::move(q_.front());
+        q_.pop_front();
+      }
+      f();
+    }
+  }
+  std::vector<std::thread> th_;
+  std::mutex mu_;
+  std::condition_variable cv_;
+  std::deque<std::function<void()>> q_;
+  bool closed_ = false;
+};
+
+/* staging buffers free for a new device-to-host copy */
+class FreeList {
+ public:
+  FreeList() { for (int b = 0; b < kNStage; ++b) free_.push_back(b); }
+  int take() {
+    std::unique_lock<std::mutex> lk(mu_);
+    cv_.wait(lk, [&] { return !free_.empty(); });
+    int b = free_.back();
+    free_.pop_back();
+    return b;
+  }
+  void give(int b) {
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      free_.push_back(b);
+    }
+    cv_.notify_one();
+  }
+
+ private:
+  std::mutex mu_;
+  std::condition_variable cv_;
+  std::vector<int> free_;
+};
+
+/* chunks recorded on the compute stream so far (the copy side waits on it
+ * before it waits on a chunk's event, which must already be recorded) */
+class Progress {
+ public:
+  void set(int n) {
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      n_ = n;
+    }
+    cv_.notify_all();
+  }
+  void abort() {
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      abort_ = true;
+    }
+    cv_.notify_all();
+  }
+  bool wait(int c) { /* false when aborted first */
+    std::unique_lock<std::mutex> lk(mu_);
+    cv_.wait(lk, [&] { return abort_ || n_ > c; });
+    return n_ > c;
+  }
+
+ private:
+  std::mutex mu_;
+  std::condition_variable cv_;
+  int n_ = 0;
+  bool abort_ = false;
+};
+
+/* map the pages of [p, p+n) writable before the values arrive (the kernel
+ * zeroes fresh pages on first write; done here it overlaps the GPU work).
+ * Advisory: contents are unchanged and a kernel without it is skipped. */
+#ifndef MADV_POPULATE_WRITE
+#define MADV_POPULATE_WRITE 23
+#endif
+void prefault(void* p, size_t n) {
+  static const size_t pg = (size_t)sysconf(_SC_PAGESIZE);
+  const size_t a = ((size_t)p + pg - 1) & ~(pg - 1), b = ((size_t)p + n) & ~(pg - 1);
+  if (b > a) madvise((void*)a, b - a, MADV_POPULATE_WRITE);
+}
+
+/* COO indices of panels [k0, k1) (reference order (tcxi(k)-1) hd + (j-1) m + i) */
+void fill_indices(long long k0, long long k1, int hd, const long long* tcxi, const long long* tcxrow, long long* si,
+                  long long* sj) {
+  for (long long k = k0; k < k1; ++k) {
+    const long long p0 = tcxi[k] - 1, m = tcxi[k + 1] - tcxi[k];
+    long long* oi = si + (size_t)p0 * hd;
+    long long* oj = sj + (size_t)p0 * hd;
+    const long long* row = tcxrow + p0;
+    for (int j = 0; j < hd; ++j) {
+      const long long col = k * hd + j + 1;
+      for (long long i = 0; i < m; ++i) { oi[(size_t)j * m + i] = row[i]; oj[(size_t)j * m + i] = col; }
+    }
+  }
 }
 
 } // namespace
@@ -488,7 +693,6 @@ int qol_lap3dsdlpmat_levels(qol_int m, const double* tx, qol_int npols, qol_int 
                 16 * 256;
   if ((rc = g_arena.reserve(need + (64 << 20)))) return rc;
   g_arena.reset();
-  Job J{};
   double *dsx, *drts, *drps, *dtx, *dAs, *dAd, *dsnx, *dsw;
   long long *drow, *dxi;
   std::vector<double> zeros(3 * npols, 0.0), ones(npols, 1.0);
@@ -589,7 +793,6 @@ int qol_getnearquad_lap_rrq_dev(qol_int npan, qol_int nterms, qol_int hdim, qol_
   J.P = PanelIn{sx, snx, sw, rts, rps};
   J.Q = PairIn{tcx, (const long long*)tcxrow, (const long long*)tcxi};
   J.vs = sparsevs; J.vd = sparsevd; J.si = (long long*)sparsei; J.sj = (long long*)sparsej;
-  J.tcxi_host = xi.data();
   rc = run_pipeline(J, st, nullptr, level_hist, nullptr, nullptr);
   if (rc) return rc;
   if (sync) CK(cudaStreamSynchronize(st));
@@ -609,60 +812,153 @@ int qol_getnearquad_lap_rrq(qol_int npan, qol_int nterms, qol_int hdim, qol_int 
   if (rc) return rc;
   if ((rc = ensure_device())) return rc;
   if (npan == 0 || ntcx == 0) return 0;
+  if ((rc = g_ring.init())) return rc;
+  const auto tstart = std::chrono::steady_clock::now();
   cudaStream_t st = g_stream;
-  /* device copies live in a dedicated allocation (the pipeline owns the arena) */
+  const int hd = (int)hdim;
   const size_t nout = (size_t)ntcx * hdim;
-  size_t bytes = sizeof(double) * (size_t)(nsrc * 13 + ntcx * 3) + sizeof(long long) * (ntcx + npan + 1) +
-                 (sizeof(double) * 2 + sizeof(long long) * 2) * nout + 16 * 256;
-  char* buf = nullptr;
-  if (cudaMalloc(&buf, bytes) != cudaSuccess) { cudaGetLastError(); return fail(QOL_ERR_CUDA, "device allocation failed"); }
-  size_t used = 0;
-  auto take = [&](size_t b) { size_t o = (used + 255) & ~(size_t)255; used = o + b; return buf + o; };
-  double* dsx = (double*)take(sizeof(double) * 3 * nsrc);
-  double* dsnx = (double*)take(sizeof(double) * 3 * nsrc);
-  double* dsw = (double*)take(sizeof(double) * nsrc);
-  double* drts = (double*)take(sizeof(double) * 3 * nsrc);
-  double* drps = (double*)take(sizeof(double) * 3 * nsrc);
-  double* dtcx = (double*)take(sizeof(double) * 3 * ntcx);
-  long long* drow = (long long*)take(sizeof(long long) * ntcx);
-  long long* dxi = (long long*)take(sizeof(long long) * (npan + 1));
-  double* dvs = (double*)take(sizeof(double) * nout);
-  double* dvd = (double*)take(sizeof(double) * nout);
-  long long* dsi = (long long*)take(sizeof(long long) * nout);
-  long long* dsj = (long long*)take(sizeof(long long) * nout);
-  int out = 0;
-  do {
-#define CKB(x)                                                                        \
-  {                                                                                   \
-    cudaError_t e_ = (x);                                                             \
-    if (e_ != cudaSuccess) { out = fail(QOL_ERR_CUDA, "%s: %s", #x, cudaGetErrorString(e_)); break; } \
+  /* panel chunks with about equal target counts (about 8 on large calls):
+   * the per-pair RRQ phase runs chunk by chunk and each chunk's values leave
+   * the GPU while the next one computes */
+  const int nch = (int)std::max<qol_int>(1, std::min<qol_int>(8, npan / 256));
+  std::vector<long long> cb(nch + 1, 0);
+  cb[nch] = npan;
+  for (int c = 1; c < nch; ++c) {
+    const qol_int want = (ntcx * c) / nch;
+    qol_int k = std::lower_bound(tcxi, tcxi + npan + 1, want + 1) - tcxi;
+    cb[c] = std::min<qol_int>(npan, std::max<qol_int>(cb[c - 1], k));
   }
-    CKB(cudaMemcpyAsync(dsx, sx, sizeof(double) * 3 * nsrc, cudaMemcpyHostToDevice, st));
-    CKB(cudaMemcpyAsync(dsnx, snx, sizeof(double) * 3 * nsrc, cudaMemcpyHostToDevice, st));
-    CKB(cudaMemcpyAsync(dsw, sw, sizeof(double) * nsrc, cudaMemcpyHostToDevice, st));
-    CKB(cudaMemcpyAsync(drts, rts, sizeof(double) * 3 * nsrc, cudaMemcpyHostToDevice, st));
-    CKB(cudaMemcpyAsync(drps, rps, sizeof(double) * 3 * nsrc, cudaMemcpyHostToDevice, st));
-    CKB(cudaMemcpyAsync(dtcx, tcx, sizeof(double) * 3 * ntcx, cudaMemcpyHostToDevice, st));
-    CKB(cudaMemcpyAsync(drow, tcxrow, sizeof(long long) * ntcx, cudaMemcpyHostToDevice, st));
-    CKB(cudaMemcpyAsync(dxi, tcxi, sizeof(long long) * (npan + 1), cudaMemcpyHostToDevice, st));
-    Job J{};
-    J.npan = (int)npan; J.nterms = (int)nterms; J.nquad = (int)nquad; J.orderff = (int)orderff;
-    J.exterior = (iside % 10) == 0; J.subtract_naive = 1; J.distff = distff; J.ntcx = ntcx;
-    J.P = PanelIn{dsx, dsnx, dsw, drts, drps};
-    J.Q = PairIn{dtcx, drow, dxi};
-    J.vs = dvs; J.vd = dvd; J.si = dsi; J.sj = dsj;
-    J.tcxi_host = (const long long*)tcxi;
-    out = run_pipeline(J, st, timeinfo, nullptr, nullptr, nullptr);
-    if (out) break;
-    CKB(cudaMemcpyAsync(sparsevs, dvs, sizeof(double) * nout, cudaMemcpyDeviceToHost, st));
-    CKB(cudaMemcpyAsync(sparsevd, dvd, sizeof(double) * nout, cudaMemcpyDeviceToHost, st));
-    CKB(cudaMemcpyAsync(sparsei, dsi, sizeof(long long) * nout, cudaMemcpyDeviceToHost, st));
-    CKB(cudaMemcpyAsync(sparsej, dsj, sizeof(long long) * nout, cudaMemcpyDeviceToHost, st));
-    CKB(cudaStreamSynchronize(st));
-#undef CKB
-  } while (0);
-  cudaFree(buf);
+  size_t bytes = sizeof(double) * (size_t)(nsrc * 13 + ntcx * 3) + sizeof(long long) * (ntcx + npan + 1) +
+                 sizeof(double) * 2 * nout + 16 * 256;
+  if ((rc = g_arena_io.reserve(bytes))) return rc;
+  g_arena_io.reset();
+  double* dsx = g_arena_io.take<double>(3 * nsrc);
+  double* dsnx = g_arena_io.take<double>(3 * nsrc);
+  double* dsw = g_arena_io.take<double>(nsrc);
+  double* drts = g_arena_io.take<double>(3 * nsrc);
+  double* drps = g_arena_io.take<double>(3 * nsrc);
+  double* dtcx = g_arena_io.take<double>(3 * ntcx);
+  long long* drow = g_arena_io.take<long long>(ntcx);
+  long long* dxi = g_arena_io.take<long long>(npan + 1);
+  double* dval = g_arena_io.take<double>(2 * nout); /* vs then vd */
+  int out = 0;
+  auto cpy = [&](void* d, const void* h, size_t n) {
+    if (!out) {
+      cudaError_t e = cudaMemcpyAsync(d, h, n, cudaMemcpyHostToDevice, st);
+      if (e != cudaSuccess) out = fail(QOL_ERR_CUDA, "input copy: %s", cudaGetErrorString(e));
+    }
+  };
+  cpy(dsx, sx, sizeof(double) * 3 * nsrc);
+  cpy(dsnx, snx, sizeof(double) * 3 * nsrc);
+  cpy(dsw, sw, sizeof(double) * nsrc);
+  cpy(drts, rts, sizeof(double) * 3 * nsrc);
+  cpy(drps, rps, sizeof(double) * 3 * nsrc);
+  cpy(dtcx, tcx, sizeof(double) * 3 * ntcx);
+  cpy(drow, tcxrow, sizeof(long long) * ntcx);
+  cpy(dxi, tcxi, sizeof(long long) * (npan + 1));
+  if (out) { cudaStreamSynchronize(st); return out; }
+  g_host_ms[0] = ms_since(tstart);
+
+  const unsigned hw = std::thread::hardware_concurrency();
+  /* leave two cores to the launching thread and the copy thread */
+  const int nthr = (int)std::min(16u, std::max(2u, hw > 4 ? hw - 2 : 2u));
+  std::atomic<int> werr{0};
+  {
+    Workers W(nthr);
+    /* COO indices on the host, overlapping the device work */
+    const long long per = std::max<long long>(1, ntcx / (4 * nthr));
+    std::atomic<int> fills_left{0};
+    std::vector<std::pair<qol_int, qol_int>> fills;
+    for (qol_int k0 = 0; k0 < npan;) {
+      qol_int k1 = k0 + 1;
+      while (k1 < npan && tcxi[k1] - tcxi[k0] < per) ++k1;
+      fills.emplace_back(k0, k1);
+      k0 = k1;
+    }
+    fills_left = (int)fills.size();
+    for (auto kk : fills)
+      W.submit([=, &fills_left] {
+        fill_indices(kk.first, kk.second, hd, tcxi, tcxrow, sparsei, sparsej);
+        if (--fills_left == 0) g_host_ms[6] = ms_since(tstart);
+      });
+    /* then the value arrays' pages, in chunk order */
+    for (double* arr : {sparsevs, sparsevd})
+      for (size_t o = 0; o < nout; o += (size_t)8 << 20) {
+        const size_t n = std::min((size_t)8 << 20, nout - o);
+        W.submit([=] { prefault(arr + o, n * sizeof(double)); });
+      }
+    /* values: chunk c leaves the GPU once the compute stream passed its event */
+    std::vector<cudaEvent_t> cev(nch, nullptr);
+    for (int c = 0; c < nch && !out; ++c)
+      if (cudaEventCreateWithFlags(&cev[c], cudaEventDisableTiming) != cudaSuccess)
+        out = fail(QOL_ERR_CUDA, "event creation failed");
+    Progress prog;
+    FreeList fl;
+    std::atomic<int> cerr{0};
+    std::thread copier([&] {
+      double* hdst[2] = {sparsevs, sparsevd};
+      for (int c = 0; c < nch; ++c) {
+        if (!prog.wait(c)) return;
+        if (cudaStreamWaitEvent(g_ring.cs, cev[c], 0) != cudaSuccess) { cerr = 1; return; }
+        const size_t t0 = (size_t)(tcxi[cb[c]] - 1), t1 = (size_t)(tcxi[cb[c + 1]] - 1);
+        for (int a = 0; a < 2; ++a) {
+          const char* src = (const char*)(dval + a * nout + t0 * hd);
+          char* dst = (char*)(hdst[a] + t0 * hd);
+          const size_t tot = (t1 - t0) * hd * sizeof(double);
+          for (size_t off = 0; off < tot; off += kStageBytes) {
+            const size_t n = std::min(kStageBytes, tot - off);
+            const int b = fl.take();
+            if (cudaMemcpyAsync(g_ring.buf[b], src + off, n, cudaMemcpyDeviceToHost, g_ring.cs) != cudaSuccess ||
+                cudaEventRecord(g_ring.ev[b], g_ring.cs) != cudaSuccess) {
+              cerr = 1;
+              fl.give(b);
+              return;
+            }
+            W.submit([&, b, dst, off, n] {
+              if (cudaEventSynchronize(g_ring.ev[b]) == cudaSuccess) std::memcpy(dst + off, g_ring.buf[b], n);
+              else werr = 1;
+              fl.give(b);
+            });
+          }
+        }
+      }
+    });
+    if (!out) {
+      Job J{};
+      J.npan = (int)npan; J.nterms = (int)nterms; J.nquad = (int)nquad; J.orderff = (int)orderff;
+      J.exterior = (iside % 10) == 0; J.subtract_naive = 1; J.distff = distff; J.ntcx = ntcx;
+      J.P = PanelIn{dsx, dsnx, dsw, drts, drps};
+      J.Q = PairIn{dtcx, drow, dxi};
+      J.vs = dval; J.vd = dval + nout;
+      J.si = nullptr; J.sj = nullptr;
+      J.chunk_pan = &cb;
+      J.after_chunk = [&](int c) {
+        if (cudaEventRecord(cev[c], st) == cudaSuccess) prog.set(c + 1);
+        else cerr = 1;
+      };
+      out = run_pipeline(J, st, timeinfo, nullptr, nullptr, nullptr);
+    }
+    if (out || cerr) prog.abort();
+    g_host_ms[1] = ms_since(tstart);
+    copier.join();
+    g_host_ms[2] = ms_since(tstart);
+    cudaStreamSynchronize(g_ring.cs);
+    g_host_ms[3] = ms_since(tstart);
+    W.finish();
+    g_host_ms[4] = ms_since(tstart);
+    cudaStreamSynchronize(st);
+    for (cudaEvent_t e : cev) if (e) cudaEventDestroy(e);
+    if (!out && (cerr || werr)) out = fail(QOL_ERR_CUDA, "device-to-host copy of the COO values failed");
+  }
+  g_host_ms[5] = ms_since(tstart);
   return out;
+}
+
+int qol_last_host_times(double* ms7) {
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  if (!ms7) return fail(QOL_ERR_ARG, "null argument");
+  for (int i = 0; i < 7; ++i) ms7[i] = g_host_ms[i];
+  return 0;
 }
 
 int qol_rrq(qol_int m, const double* tx, qol_int n, const double* sx, const double* snx, const double* sw,
@@ -737,7 +1033,6 @@ int qol_rrq(qol_int m, const double* tx, qol_int n, const double* sx, const doub
     J.Q = PairIn{dtx, drow, dxi};
     J.vs = dAs; J.vd = dAd; J.omega = dOm; J.ialpha = dIa; J.si = nullptr; J.sj = nullptr;
     J.chart = ichart == 1 ? dch : nullptr;
-    J.tcxi_host = xi.data();
     out = run_pipeline(J, st, timeinfo, nullptr, nullptr, nullptr);
     if (out) break;
     CKB(cudaMemcpyAsync(As, dAs, sizeof(double) * m * n, cudaMemcpyDeviceToHost, st));

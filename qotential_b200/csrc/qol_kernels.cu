@@ -708,8 +708,8 @@ __device__ double panel_height_warp(const OrderTab& T, const double* scf, const 
  * edge): writes w1 (nq), w3 (nq), ok, Re t0, Im t0 to the pair's edge record */
 __global__ void __launch_bounds__(128) k_rrq_ssq(OrderTab T, PairIn Q, PairWS G, RRQWS R) {
   const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (tid >= 3 * R.nrrq) return;
-  const long long gidx = tid / 3;
+  if (tid >= 3 * (R.ghi - R.glo)) return;
+  const long long gidx = R.glo + tid / 3;
   const int e = (int)(tid % 3);
   int lo = 0, hi = R.npan;
   while (hi - lo > 1) {
@@ -743,8 +743,8 @@ __global__ void __launch_bounds__(128) k_rrq_ssq(OrderTab T, PairIn Q, PairWS G,
 __global__ void __launch_bounds__(32 * RRQ_WARPS) k_rrq_geom(OrderTab T, PairIn Q, PairWS G, RRQWS R, int exterior) {
   __shared__ WarpSM S[RRQ_WARPS];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const long long gidx = (long long)blockIdx.x * RRQ_WARPS + wid;
-  if (gidx >= R.nrrq) return;
+  const long long gidx = R.glo + (long long)blockIdx.x * RRQ_WARPS + wid;
+  if (gidx >= R.ghi) return;
   WarpSM& W = S[wid];
   int lo = 0, hi = R.npan;
   while (hi - lo > 1) {
@@ -930,8 +930,8 @@ __global__ void __launch_bounds__(32 * MOM_WARPS) k_rrq_moments(OrderTab T, Pair
   }
   for (int e = threadIdx.x; e < QOL_MAXL + 2; e += blockDim.x) { s_rd[e] = c_rd[e]; s_ri[e] = c_rinv[e]; }
   __syncthreads();
-  const long long gidx = (long long)blockIdx.x * MOM_WARPS + wid;
-  if (gidx >= R.nrrq) return;
+  const long long gidx = R.glo + (long long)blockIdx.x * MOM_WARPS + wid;
+  if (gidx >= R.ghi) return;
   int lo = 0, hi = R.npan;
   while (hi - lo > 1) {
     int mid = (lo + hi) >> 1;
@@ -1205,7 +1205,7 @@ __device__ __forceinline__ void apply_tile_gemm(const double* __restrict__ M, in
 
 template <int NB>
 __global__ void __launch_bounds__(256) k_rrq_apply(OrderTab T, PanelIn P, PairIn Q, PairWS G, RRQWS R, OutCOO O) {
-  const int pan = blockIdx.x;
+  const int pan = R.plo + blockIdx.x;
   const int cnt = G.cnt[(size_t)pan * 8 + T.nlevel + 1];
   if (cnt == 0) return;
   const int hd = T.hd, N4 = 4 * hd;
@@ -1357,14 +1357,16 @@ cudaError_t qol_launch_rrq_panel(const OrderTab& T, const PanelIn& P, const Pair
   return cudaGetLastError();
 }
 cudaError_t qol_launch_rrq_ssq(const OrderTab& T, const PairIn& Q, const PairWS& G, const RRQWS& R, cudaStream_t st) {
-  if (R.nrrq == 0) return cudaSuccess;
-  k_rrq_ssq<<<(unsigned)((3 * R.nrrq + 127) / 128), 128, 0, st>>>(T, Q, G, R);
+  const long long n = R.ghi - R.glo;
+  if (n <= 0) return cudaSuccess;
+  k_rrq_ssq<<<(unsigned)((3 * n + 127) / 128), 128, 0, st>>>(T, Q, G, R);
   return cudaGetLastError();
 }
 cudaError_t qol_launch_rrq_geom(const OrderTab& T, const PairIn& Q, const PairWS& G, const RRQWS& R, int exterior,
                                 cudaStream_t st) {
-  if (R.nrrq == 0) return cudaSuccess;
-  long long nb = (R.nrrq + RRQ_WARPS - 1) / RRQ_WARPS;
+  const long long n = R.ghi - R.glo;
+  if (n <= 0) return cudaSuccess;
+  long long nb = (n + RRQ_WARPS - 1) / RRQ_WARPS;
   k_rrq_geom<<<(unsigned)nb, 32 * RRQ_WARPS, 0, st>>>(T, Q, G, R, exterior);
   return cudaGetLastError();
 }
@@ -1377,8 +1379,9 @@ cudaError_t qol_launch_rrq_target(const OrderTab& T, const PairIn& Q, const Pair
 }
 cudaError_t qol_launch_rrq_moments(const OrderTab& T, const PairIn& Q, const PairWS& G, const RRQWS& R,
                                    cudaStream_t st) {
-  if (R.nrrq == 0) return cudaSuccess;
-  const unsigned nbm = (unsigned)((R.nrrq + MOM_WARPS - 1) / MOM_WARPS);
+  const long long n = R.ghi - R.glo;
+  if (n <= 0) return cudaSuccess;
+  const unsigned nbm = (unsigned)((n + MOM_WARPS - 1) / MOM_WARPS);
   const size_t smem = sizeof(double) * MOM_WARPS * mom_warp_doubles(T.nterms, 3 * T.nquad);
   auto go = [&](auto kern) {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1394,7 +1397,9 @@ cudaError_t qol_launch_rrq_moments(const OrderTab& T, const PairIn& Q, const Pai
   return cudaGetLastError();
 }
 cudaError_t qol_launch_rrq_apply(const OrderTab& T, const PanelIn& P, const PairIn& Q, const PairWS& G,
-                                 const RRQWS& R, const OutCOO& O, int npan, cudaStream_t st) {
+                                 const RRQWS& R, const OutCOO& O, cudaStream_t st) {
+  const int npan = R.phi - R.plo;
+  if (npan <= 0) return cudaSuccess;
   const int NBn = (T.hd + 15) / 16;
   auto go = [&](auto kern, int nb) {
     size_t smem = sizeof(double) * ((size_t)AQ * 16 * nb + AQ * AT + (size_t)AT * T.hd);

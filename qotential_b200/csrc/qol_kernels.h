@@ -61,6 +61,8 @@ struct RRQWS {
   double* line;    /* per RRQ pair: cD (3 nbd), cS (3 nbd), lint (3), Omega */
   double* edge;    /* per RRQ pair and edge: w1 (nq), w3 (nq), ok, Re t0, Im t0 */
   double* ialpha;  /* per RRQ pair (nullable) */
+  long long glo, ghi; /* RRQ pairs [glo, ghi) of this launch (per-pair kernels) */
+  int plo, phi;       /* panels [plo, phi) of this launch (k_rrq_apply) */
 };
 
 /* output: COO values (block column-major per panel) */
@@ -88,7 +90,7 @@ cudaError_t qol_launch_rrq_moments(const OrderTab& T, const PairIn& Q, const Pai
 cudaError_t qol_launch_rrq_target(const OrderTab& T, const PairIn& Q, const PairWS& G, const RRQWS& R, int exterior,
                                   cudaStream_t st);
 cudaError_t qol_launch_rrq_apply(const OrderTab& T, const PanelIn& P, const PairIn& Q, const PairWS& G,
-                                 const RRQWS& R, const OutCOO& O, int npan, cudaStream_t st);
+                                 const RRQWS& R, const OutCOO& O, cudaStream_t st);
 cudaError_t qol_launch_coo_index(const OrderTab& T, const PairIn& Q, long long* si, long long* sj, int npan,
                                  cudaStream_t st);
 cudaError_t qol_launch_fp64_peak(double* out, int blocks, int iters, cudaStream_t st);

@@ -267,11 +267,12 @@ extern "C" int qol_rrq_noalloc(qol_int m, const double* tx, qol_int n, const dou
   NA_CK(cudaMemcpyAsync(&nrrq, rrq_off + 1, sizeof(long long), cudaMemcpyDeviceToHost, st));
   NA_CK(cudaStreamSynchronize(st));
   R.nrrq = nrrq;
+  R.glo = 0; R.ghi = nrrq; R.plo = 0; R.phi = 1;
   NA_CK(qol_launch_direct(T, P, Q, W, G, O, 1, st));
   if (nrrq > 0) {
     NA_CK(qol_launch_rrq_panel(T, P, G, R, 1, nullptr, st));
     NA_CK(qol_launch_rrq_target(T, Q, G, R, exterior != 0, st));
-    NA_CK(qol_launch_rrq_apply(T, P, Q, G, R, O, 1, st));
+    NA_CK(qol_launch_rrq_apply(T, P, Q, G, R, O, st));
   }
   return 0;
 }

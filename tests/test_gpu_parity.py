@@ -123,6 +123,35 @@ def test_deterministic(qol):
         assert x.tobytes() == y.tobytes()
 
 
+def test_host_entry_chunks_match_device_entry(qol):
+    """The host-pointer entry point runs the pipeline over panel chunks,
+    streams the values out through pinned staging and fills the COO indices
+    on the host; on a surface large enough for several chunks its output must
+    be the device entry point's, byte for byte, with entries beyond the
+    needed nnz left as the caller had them."""
+    import torch
+    from qotential_b200 import geometry as G
+    nterms = 5
+    P, hd, tcxi, tcxrow, tcx, _ = _setup(G, G.stellarator(), 16, 40, nterms, off=500)
+    npan = P["sw"].size // hd
+    assert npan >= 1024  # at least four chunks
+    nq = nterms + 2
+    need = int(tcxrow.size) * hd
+    si, sj, vs, vd, _ = qol.qol_getnearquad_lap_rrq(npan, nterms, hd, nq, npan * hd, P["sx"], P["snx"], P["sw"],
+                                                   P["rts"], P["rps"], tcxrow.size, tcx, tcxrow, tcxi, nq, 1.4, 30,
+                                                   nnz=need + 7)
+    t = lambda a, dt=torch.float64: torch.as_tensor(np.ascontiguousarray(a), dtype=dt).cuda()
+    out = (torch.zeros(need, dtype=torch.int64, device="cuda"), torch.zeros(need, dtype=torch.int64, device="cuda"),
+           torch.zeros(need, dtype=torch.float64, device="cuda"), torch.zeros(need, dtype=torch.float64, device="cuda"))
+    qol.qol_getnearquad_lap_rrq_dev(npan, nterms, nq, t(P["sx"]), t(P["snx"]), t(P["sw"]), t(P["rts"]),
+                                    t(P["rps"]), t(tcx), t(tcxrow, torch.int64), t(tcxi, torch.int64), nq, 1.4, 30,
+                                    out)
+    ref = [o.cpu().numpy() for o in out]
+    for h, d in zip((si, sj, vs, vd), ref):
+        assert h[:need].tobytes() == d.tobytes()
+        assert not h[need:].any()
+
+
 def test_grf_identity_gpu(qol, orc):
     """S[du/dn] - D[u] = 0 (exterior limit) on the torus for a harmonic u from
     exterior point charges, with the GPU near corrections"""
