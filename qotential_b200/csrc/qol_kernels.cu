@@ -193,10 +193,43 @@ __global__ void __launch_bounds__(128) k_classify(OrderTab T, PairIn Q, LevelWS 
 /* with interpmat, minus the self-masked naive block, written as COO     */
 /* values.  One CTA per (panel, level); chunks of 32 targets.            */
 /* ===================================================================== */
-#define DT 32 /* targets per chunk */
-template <int HDMAX>
-__global__ void __launch_bounds__(256) k_direct(OrderTab T, PanelIn P, PairIn Q, LevelWS W, PairWS G,
-                                                OutCOO O) {
+#define DTT 32           /* targets per chunk */
+#define DNT 32           /* level nodes per tile (8 DMMA k-steps) */
+#define DKS (DTT + 4)    /* kernel-tile row stride: fragment loads hit 16 distinct bank pairs */
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+/* D = A (8x4, row) B (4x8, col) + D, FP64 tensor path; per lane a = A[lane/4][lane%4],
+ * b = B[lane%4][lane/4], d = D[lane/4][2 (lane%4) + {0,1}] */
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+/* single-layer kernels S = w/(4 pi r), D = w (x-y).n/(4 pi r^3) of one source
+ * node (zero when |x-y|^2 <= 1e-28, as the reference's sdlpmat) */
+__device__ __forceinline__ void sdl_kernel(double dx, double dy, double dz, double nx, double ny, double nz, double w4,
+                                           double& s, double& d) {
+  const double rr = dx * dx + dy * dy + dz * dz;
+  s = 0.0; d = 0.0;
+  if (rr > 1.0e-28) {
+    const double ri = rsqrt(rr);
+    s = w4 * ri;
+    d = s * ri * ri * (dx * nx + dy * ny + dz * nz);
+  }
+}
+
+/* one CTA per (panel, level); chunks of DTT targets.  Per tile of DNT level
+ * nodes: kernel values KS, KD (DNT x DTT) and interpolation rows It (DNT x hd,
+ * async copy) in shared memory, then S and D (targets x hd) += K It on the
+ * FP64 tensor path.  Warp w: targets 16 (w>>2) .. +15, columns 8 NB (w&3) ..,
+ * NB column blocks of 8 */
+template <int NB>
+__global__ void __launch_bounds__(256, 2) k_direct(OrderTab T, PanelIn P, PairIn Q, LevelWS W,
+                                                                  PairWS G, OutCOO O) {
   const int pan = blockIdx.x, l = blockIdx.y;
   if (l >= T.nlevel) return;
   const int cntl = G.cnt[(size_t)pan * 8 + l + 1];
@@ -206,89 +239,98 @@ __global__ void __launch_bounds__(256) k_direct(OrderTab T, PanelIn P, PairIn Q,
   const long long p0 = Q.tcxi[pan] - 1, m = Q.tcxi[pan + 1] - Q.tcxi[pan];
   const double* node = W.node[l] + (size_t)pan * n * 7;
   const double* I = T.interp[l];
-  __shared__ double tg[DT][3];
-  __shared__ int tloc[DT];
-  constexpr int NT = HDMAX > 96 ? 16 : 32; /* nodes per tile */
-  __shared__ double KS[NT][DT], KD[NT][DT];
-  __shared__ double It[NT][HDMAX];
-  const int t = threadIdx.x & 31, kg = threadIdx.x >> 5;
-  constexpr int NQ = (HDMAX + 7) / 8;
+  constexpr int NCW = 32 * NB;     /* padded columns */
+  constexpr int ICS = NCW + 4;     /* interpolation-tile row stride */
+  extern __shared__ __align__(16) double dsm[];
+  double* KS = dsm;                /* DNT x DKS */
+  double* KD = KS + DNT * DKS;     /* DNT x DKS */
+  double* It = KD + DNT * DKS;     /* DNT x ICS */
+  double* tg = It + DNT * ICS;     /* DTT x 3 */
+  int* tloc = (int*)(tg + 3 * DTT);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int tb0 = 16 * (w >> 2), cb0 = 8 * NB * (w & 3);
+  const int fr = lane >> 2, fc = lane & 3;
   const double i4p = 1.0 / (4.0 * QOL_PI);
-  for (int c0 = 0; c0 < cntl; c0 += DT) {
-    const int nt = min(DT, cntl - c0);
+  for (int c0 = 0; c0 < cntl; c0 += DTT) {
+    const int nt = min(DTT, cntl - c0);
     __syncthreads();
-    if (threadIdx.x < DT) {
-      int tl = threadIdx.x < nt ? G.grp[p0 + offl + c0 + threadIdx.x] : -1;
+    if (threadIdx.x < DTT) {
+      const int tl = threadIdx.x < nt ? G.grp[p0 + offl + c0 + threadIdx.x] : -1;
       tloc[threadIdx.x] = tl;
-      for (int d = 0; d < 3; ++d) tg[threadIdx.x][d] = tl >= 0 ? Q.tcx[3 * (p0 + tl) + d] : 0.0;
+      for (int d = 0; d < 3; ++d) tg[3 * threadIdx.x + d] = tl >= 0 ? Q.tcx[3 * (p0 + tl) + d] : 0.0;
     }
-    double accS[NQ], accD[NQ];
+    double cS[2][NB][2], cD[2][NB][2];
 #pragma unroll
-    for (int q = 0; q < NQ; ++q) { accS[q] = 0.0; accD[q] = 0.0; }
-    for (int n0 = 0; n0 < n; n0 += NT) {
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < NB; ++b) { cS[a][b][0] = cS[a][b][1] = 0.0; cD[a][b][0] = cD[a][b][1] = 0.0; }
+    for (int n0 = 0; n0 < n; n0 += DNT) {
       __syncthreads();
-      for (int e = threadIdx.x; e < NT * DT; e += blockDim.x) {
-        int nn = e / DT, tt = e % DT, i = n0 + nn;
+      for (int e = threadIdx.x; e < DNT * NCW; e += blockDim.x) {
+        const int nn = e / NCW, c = e % NCW, i = n0 + nn;
+        if (i < n && c < hd) cp_async8(&It[nn * ICS + c], I + (size_t)i * hd + c);
+        else It[nn * ICS + c] = 0.0;
+      }
+      asm volatile("cp.async.commit_group;\n" ::: "memory");
+      for (int e = threadIdx.x; e < DNT * DTT; e += blockDim.x) {
+        const int nn = e / DTT, tt = e % DTT, i = n0 + nn;
         double s = 0.0, dv = 0.0;
-        if (i < n && tt < nt) {
-          double dx = tg[tt][0] - node[i], dy = tg[tt][1] - node[n + i], dz = tg[tt][2] - node[2 * n + i];
-          double rr = dx * dx + dy * dy + dz * dz;
-          if (rr > 1.0e-28) {
-            double w4 = node[6 * n + i] * i4p, r = sqrt(rr);
-            s = w4 / r;
-            dv = w4 * (dx * node[3 * n + i] + dy * node[4 * n + i] + dz * node[5 * n + i]) / (r * rr);
-          }
-        }
-        KS[nn][tt] = s;
-        KD[nn][tt] = dv;
+        if (i < n && tt < nt)
+          sdl_kernel(tg[3 * tt] - node[i], tg[3 * tt + 1] - node[n + i], tg[3 * tt + 2] - node[2 * n + i],
+                     node[3 * n + i], node[4 * n + i], node[5 * n + i], node[6 * n + i] * i4p, s, dv);
+        KS[nn * DKS + tt] = s;
+        KD[nn * DKS + tt] = dv;
       }
-      for (int e = threadIdx.x; e < NT * hd; e += blockDim.x) {
-        int nn = e / hd, k = e % hd, i = n0 + nn;
-        It[nn][k] = i < n ? I[(size_t)i * hd + k] : 0.0;
-      }
+      cp_async_wait_all();
       __syncthreads();
-      const int nn_max = min(NT, n - n0);
-      for (int nn = 0; nn < nn_max; ++nn) {
-        double s = KS[nn][t], dv = KD[nn][t];
+#pragma unroll 2
+      for (int ks = 0; ks < DNT / 4; ++ks) {
+        const int kr = 4 * ks + fc;
+        const double aS0 = KS[kr * DKS + tb0 + fr], aS1 = KS[kr * DKS + tb0 + 8 + fr];
+        const double aD0 = KD[kr * DKS + tb0 + fr], aD1 = KD[kr * DKS + tb0 + 8 + fr];
 #pragma unroll
-        for (int q = 0; q < NQ; ++q) {
-          int k = kg + 8 * q;
-          double iv = (k < HDMAX) ? It[nn][k] : 0.0;
-          accS[q] += s * iv;
-          accD[q] += dv * iv;
+        for (int b = 0; b < NB; ++b) {
+          const double bv = It[kr * ICS + cb0 + 8 * b + fr];
+          dmma(cS[0][b][0], cS[0][b][1], aS0, bv);
+          dmma(cS[1][b][0], cS[1][b][1], aS1, bv);
+          dmma(cD[0][b][0], cD[0][b][1], aD0, bv);
+          dmma(cD[1][b][0], cD[1][b][1], aD1, bv);
         }
       }
     }
     /* naive block and the COO write */
-    if (t < nt) {
-      const int tl = tloc[t];
-      const long long row = Q.tcxrow[p0 + tl];
-      const double x0 = tg[t][0], x1 = tg[t][1], x2 = tg[t][2];
 #pragma unroll
-      for (int q = 0; q < NQ; ++q) {
-        int k = kg + 8 * q;
-        if (k >= hd) continue;
-        double vs = accS[q], vd = accD[q];
-        if (O.subtract_naive) {
-          size_t gj = (size_t)pan * hd + k;
-          double ns = 0.0, nd = 0.0;
-          if (row != (long long)gj + 1) {
-            double dx = x0 - P.sx[3 * gj], dy = x1 - P.sx[3 * gj + 1], dz = x2 - P.sx[3 * gj + 2];
-            double rr = dx * dx + dy * dy + dz * dz;
-            if (rr > 1.0e-28) {
-              double w4 = P.sw[gj] * i4p, r = sqrt(rr);
-              ns = w4 / r;
-              nd = w4 * (dx * P.snx[3 * gj] + dy * P.snx[3 * gj + 1] + dz * P.snx[3 * gj + 2]) / (r * rr);
-            }
+    for (int a = 0; a < 2; ++a) {
+      const int tt = tb0 + 8 * a + fr;
+      if (tt >= nt) continue;
+      const int tl = tloc[tt];
+      const long long row = Q.tcxrow[p0 + tl];
+      const double x0 = tg[3 * tt], x1 = tg[3 * tt + 1], x2 = tg[3 * tt + 2];
+#pragma unroll
+      for (int b = 0; b < NB; ++b)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int k = cb0 + 8 * b + 2 * fc + h;
+          if (k >= hd) continue;
+          double vs = cS[a][b][h], vd = cD[a][b][h];
+          if (O.subtract_naive) {
+            const size_t gj = (size_t)pan * hd + k;
+            double ns = 0.0, nd = 0.0;
+            if (row != (long long)gj + 1)
+              sdl_kernel(x0 - P.sx[3 * gj], x1 - P.sx[3 * gj + 1], x2 - P.sx[3 * gj + 2], P.snx[3 * gj],
+                         P.snx[3 * gj + 1], P.snx[3 * gj + 2], P.sw[gj] * i4p, ns, nd);
+            vs -= ns; vd -= nd;
           }
-          vs -= ns; vd -= nd;
+          const size_t o = (size_t)p0 * hd + (size_t)k * m + tl;
+          O.vs[o] = vs;
+          O.vd[o] = vd;
         }
-        size_t o = (size_t)p0 * hd + (size_t)k * m + tl;
-        O.vs[o] = vs;
-        O.vd[o] = vd;
-      }
     }
   }
+}
+template <int NB>
+constexpr size_t direct_smem() {
+  return sizeof(double) * (2 * DNT * DKS + DNT * (32 * NB + 4) + 3 * DTT) + sizeof(int) * DTT;
 }
 
 /* ===================================================================== */
@@ -1339,12 +1381,17 @@ cudaError_t qol_launch_classify(const OrderTab& T, const PairIn& Q, const LevelW
 cudaError_t qol_launch_direct(const OrderTab& T, const PanelIn& P, const PairIn& Q, const LevelWS& W,
                               const PairWS& G, const OutCOO& O, int npan, cudaStream_t st) {
   dim3 grid(npan, T.nlevel);
-  if (T.hd <= 16) k_direct<16><<<grid, 256, 0, st>>>(T, P, Q, W, G, O);
-  else if (T.hd <= 32) k_direct<32><<<grid, 256, 0, st>>>(T, P, Q, W, G, O);
-  else if (T.hd <= 48) k_direct<48><<<grid, 256, 0, st>>>(T, P, Q, W, G, O);
-  else if (T.hd <= 72) k_direct<72><<<grid, 256, 0, st>>>(T, P, Q, W, G, O);
-  else if (T.hd <= 96) k_direct<96><<<grid, 256, 0, st>>>(T, P, Q, W, G, O);
-  else k_direct<136><<<grid, 256, 0, st>>>(T, P, Q, W, G, O);
+  auto go = [&](auto kern, size_t smem) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    kern<<<grid, 256, smem, st>>>(T, P, Q, W, G, O);
+  };
+  switch ((T.hd + 31) / 32) {
+    case 1: go(k_direct<1>, direct_smem<1>()); break;
+    case 2: go(k_direct<2>, direct_smem<2>()); break;
+    case 3: go(k_direct<3>, direct_smem<3>()); break;
+    case 4: go(k_direct<4>, direct_smem<4>()); break;
+    default: go(k_direct<5>, direct_smem<5>()); break;
+  }
   return cudaGetLastError();
 }
 cudaError_t qol_launch_scan(int npan, int lev, const int* cnt, long long* off, cudaStream_t st) {
