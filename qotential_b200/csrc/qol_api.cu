@@ -256,8 +256,7 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
   add(ntcx); add(sizeof(int) * ntcx); add(sizeof(int) * (size_t)npan * 8 * 2);
   add(sizeof(long long) * (npan + 1));
   add(sizeof(double) * (size_t)npan * (RRQ_FRAME + 6 * nbd + 9 * nq + 6 * hd));
-  add(sizeof(double) * (size_t)npan * hd * hd * 11);
-  add(sizeof(int) * (size_t)npan * 272);
+  add(sizeof(double) * (size_t)npan * hd * hd * 7);
   rc = g_arena.reserve(need + 4096);
   if (rc) return rc;
   g_arena.reset();
@@ -281,12 +280,10 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
   R.cf = g_arena.take<double>((size_t)npan * 9 * nq);
   R.scf = g_arena.take<double>((size_t)npan * 3 * hd);
   R.sxf = g_arena.take<double>((size_t)npan * 3 * hd);
-  R.qmat = g_arena.take<double>((size_t)npan * 4 * hd * hd);
   R.hmat = g_arena.take<double>((size_t)npan * hd * hd);
   R.smat = g_arena.take<double>((size_t)npan * hd * hd);
   R.PD = g_arena.take<double>((size_t)npan * 4 * hd * hd);
   R.B = g_arena.take<double>((size_t)npan * hd * hd);
-  R.perm = g_arena.take<int>((size_t)npan * 272);
   R.ialpha = J.ialpha;
   CK(cudaMemsetAsync(G.cnt, 0, sizeof(int) * (size_t)npan * 8, st));
   CK(cudaMemsetAsync(G.off, 0, sizeof(int) * (size_t)npan * 8, st));

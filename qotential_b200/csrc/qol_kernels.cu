@@ -18,6 +18,8 @@
 #include "qol_dev.cuh"
 #include "qol_kernels.h"
 #include <cmath>
+#include <cooperative_groups.h>
+namespace cg = cooperative_groups;
 
 __constant__ double c_hb[QOL_MAXL + 2][QOL_MAXL + 2]; /* sqrt((l+m-1)(l-m-1)) */
 __constant__ double c_hc[QOL_MAXL + 2][QOL_MAXL + 2]; /* 1/sqrt((l-m)(l+m)) */
@@ -377,46 +379,73 @@ __device__ __forceinline__ void qmul(const double* a, const double* b, double* c
   c[3] = a[0] * b[3] + a[1] * b[2] - a[2] * b[1] + a[3] * b[0];
 }
 
-/* block-wide argmax of v over the CTA; returns the winning index */
-__device__ int block_argmax(double v, int idx, double* sv, int* si) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int o = 16; o > 0; o >>= 1) {
-    double v2 = __shfl_down_sync(0xffffffffu, v, o);
-    int i2 = __shfl_down_sync(0xffffffffu, idx, o);
-    if (v2 > v || (v2 == v && i2 < idx)) { v = v2; idx = i2; }
-  }
-  if (lane == 0) { sv[wid] = v; si[wid] = idx; }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double bv = sv[0]; int bi = si[0];
-    for (int w = 1; w < nw; ++w)
-      if (sv[w] > bv || (sv[w] == bv && si[w] < bi)) { bv = sv[w]; bi = si[w]; }
-    si[0] = bi;
-  }
-  __syncthreads();
-  int r = si[0];
-  __syncthreads();
-  return r;
+/* matrix columns per CTA and rows per thread of k_rrq_panel for a cluster
+ * of CS CTAs of NT threads */
+__host__ __device__ constexpr int panel_ncol(int hd, int CS) { return (hd + CS - 1) / CS; }
+__host__ __device__ constexpr int panel_maxr(int hd, int CS, int NT) {
+  return (hd + NT / panel_ncol(hd, CS) - 1) / (NT / panel_ncol(hd, CS));
+}
+/* doubles of shared memory of one CTA: setup copies of the matrix columns,
+ * staging buffers, geometry, pivot bookkeeping, the scaled pivot rows */
+__host__ __device__ constexpr size_t panel_smem_doubles(int hd, int nbd, int CS) {
+  return (size_t)5 * hd * panel_ncol(hd, CS) + 13 * (size_t)hd + 3 * (size_t)(nbd + 3) + 16 +
+         5 * (size_t)panel_ncol(hd, CS) + 8 + (8 * (size_t)hd + 1) / 2 + 2;
 }
 
-__global__ void __launch_bounds__(256) k_rrq_panel(OrderTab T, PanelIn P, PairWS G, RRQWS R,
-                                                   const double* chart /* nullable, per panel 3 x (3nq+3) */) {
-  const int pan = blockIdx.x;
-  if (G.cnt[(size_t)pan * 8 + T.nlevel + 1] == 0 && !R.all_panels) return;
+/* per-panel RRQ precompute, one thread-block cluster of CS CTAs per panel.
+ * The quaternion matrix V (hd x hd, V[j][k] = (0, grad h_k(y_j))) and the real
+ * Msl^T (MS[k][j] = n_j . grad h_k(y_j)) are split by columns over the CTAs;
+ * each thread keeps one column's entries of up to MAXR rows in registers.
+ * Both are inverted in place by Gauss-Jordan with implicit row pivoting
+ * (quaternion pivot by norm; no row moves): step k reads column k from the
+ * staging buffer its owner pushed into every CTA through distributed shared
+ * memory, picks the largest unused row p, scales row p and eliminates every
+ * other row; the owner of column k+1 pushes it as it is updated; one cluster
+ * barrier ends the step.  With pi the pivot sequence the inverse is
+ * X^-1[k][c] = X[pi(k)][pi^-1(c)]. */
+template <int CS, int NT, int MAXR>
+__global__ void __launch_bounds__(NT, 1) k_rrq_panel(OrderTab T, PanelIn P, PairWS G, RRQWS R,
+                                                                const double* chart /* nullable */) {
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+  const int pan = blockIdx.x / CS;
+  if (G.cnt[(size_t)pan * 8 + T.nlevel + 1] == 0 && !R.all_panels) return; /* whole cluster */
   const int hd = T.hd, nq = T.nquad, nbd = 3 * nq, L = T.nterms;
-  __shared__ double s_sx[3 * 136], s_raw[3 * (3 * QOL_MAXNQ + 3)], s_fr[16];
-  __shared__ double sv[8];
-  __shared__ int si[8];
-  __shared__ double s_row[4 * 136], s_col[4 * 136], s_pinv[4];
-  double* fr = R.frame + (size_t)pan * RRQ_FRAME;
-  double* bx = R.bx + (size_t)pan * 3 * nbd;
-  double* bt = R.bt + (size_t)pan * 3 * nbd;
-  double* cf = R.cf + (size_t)pan * 9 * nq;
-  double* scf = R.scf + (size_t)pan * 3 * hd;
-  double* V = R.qmat + (size_t)blockIdx.x * 4 * hd * hd; /* hd x hd quaternions, row-major */
-  double* H = R.hmat + (size_t)pan * hd * hd;            /* H[j*hd+k] = h_k(y_j) */
-  double* MS = R.smat + (size_t)pan * hd * hd;           /* Msl^T, then its inverse (PS) */
+  const int ncol = panel_ncol(hd, CS), c0 = min(hd, rank * ncol), c1 = min(hd, c0 + ncol), nc = c1 - c0;
+  const int RG = NT / ncol, tc = threadIdx.x % ncol, trg = threadIdx.x / ncol;
+  const bool tact = trg < RG && tc < nc;
+  const int gc = c0 + tc; /* this thread's column */
+  extern __shared__ __align__(16) double psm[];
+  double* Vs = psm;                        /* hd x ncol quaternions (setup) */
+  double* Ms = Vs + (size_t)4 * hd * ncol; /* hd x ncol (setup) */
+  double* stg = Ms + (size_t)hd * ncol;    /* 2 buffers x (4 hd quaternion column + hd real column) */
+  double* s_sx = stg + 10 * hd;            /* 3 hd */
+  double* s_raw = s_sx + 3 * hd;           /* 3 (nbd + 3) */
+  double* s_fr = s_raw + 3 * (nbd + 3);    /* 16 */
+  double* rowq = s_fr + 16;                /* 4 ncol: scaled pivot row of V */
+  double* rowr = rowq + 4 * ncol;          /* ncol: scaled pivot row of MS */
+  int* s_piv = (int*)(rowr + ncol + 8);   /* 2 hd: pivot rows of V, of MS (after the 8 pivot values) */
+  int* s_pos = s_piv + 2 * hd;             /* 2 hd: inverse permutations */
+  int* s_used = s_pos + 2 * hd;            /* 2 hd */
+  int* s_pad = s_used + 2 * hd;            /* 2 hd (alignment slack) */
+  (void)s_pad;
+  double* stgr[CS];
+#pragma unroll
+  for (int r = 0; r < CS; ++r) stgr[r] = cl.map_shared_rank(stg, r);
+  auto pushq = [&](int buf, int row, const double* q) {
+#pragma unroll
+    for (int r = 0; r < CS; ++r) {
+      double* d = stgr[r] + buf * 5 * hd + 4 * row;
+      d[0] = q[0]; d[1] = q[1]; d[2] = q[2]; d[3] = q[3];
+    }
+  };
+  auto pushr = [&](int buf, int row, double v) {
+#pragma unroll
+    for (int r = 0; r < CS; ++r) stgr[r][buf * 5 * hd + 4 * hd + row] = v;
+  };
+  double* H = R.hmat + (size_t)pan * hd * hd; /* H[j*hd+k] = h_k(y_j) */
   for (int e = threadIdx.x; e < 3 * hd; e += blockDim.x) s_sx[e] = P.sx[(size_t)pan * hd * 3 + e];
+  for (int e = threadIdx.x; e < 2 * hd; e += blockDim.x) s_used[e] = 0;
   __syncthreads();
   /* boundary + vertices from the interpolant, or the caller's chart */
   for (int i = threadIdx.x; i < nbd + 3; i += blockDim.x) {
@@ -448,202 +477,243 @@ __global__ void __launch_bounds__(256) k_rrq_panel(OrderTab T, PanelIn P, PairWS
     cross3(nn, e1, e2);
     double Rm[9];
     for (int d = 0; d < 3; ++d) { Rm[0 + 3 * d] = e1[d]; Rm[1 + 3 * d] = e2[d]; Rm[2 + 3 * d] = nn[d]; }
-    double axb[3], pp[3], qq[3], c0[3];
+    double axb[3], pp[3], qq[3], cc[3];
     cross3(a, b, axb);
     double aa = dot3(a, a), bb = dot3(b, b), den = 2.0 * dot3(axb, axb);
     for (int d = 0; d < 3; ++d) pp[d] = aa * b[d] - bb * a[d];
     cross3(pp, axb, qq);
-    for (int d = 0; d < 3; ++d) c0[d] = v1[d] + qq[d] / den;
+    for (int d = 0; d < 3; ++d) cc[d] = v1[d] + qq[d] / den;
     double swsum = 0.0;
     for (int j = 0; j < hd; ++j) swsum += P.sw[(size_t)pan * hd + j];
     double alpha = 1.25 / sqrt(2.0 * swsum);
     double zmin = 1e300;
     for (int j = 0; j < hd; ++j) {
-      double d0 = s_sx[3 * j] - c0[0], d1 = s_sx[3 * j + 1] - c0[1], d2 = s_sx[3 * j + 2] - c0[2];
+      double d0 = s_sx[3 * j] - cc[0], d1 = s_sx[3 * j + 1] - cc[1], d2 = s_sx[3 * j + 2] - cc[2];
       double zz = alpha * (Rm[2] * d0 + Rm[5] * d1 + Rm[8] * d2);
       zmin = fmin(zmin, zz);
     }
     double sx3min = fmax(0.0, -zmin);
     for (int i = 0; i < 9; ++i) s_fr[i] = Rm[i];
-    for (int d = 0; d < 3; ++d) s_fr[9 + d] = c0[d] - (1.25 * sx3min / alpha) * Rm[2 + 3 * d];
+    for (int d = 0; d < 3; ++d) s_fr[9 + d] = cc[d] - (1.25 * sx3min / alpha) * Rm[2 + 3 * d];
     s_fr[12] = alpha;
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < RRQ_FRAME; i += blockDim.x) fr[i] = i < 13 ? s_fr[i] : 0.0;
   const double alpha = s_fr[12];
   auto tofr = [&](const double* x, double* y) {
     double d0 = x[0] - s_fr[9], d1 = x[1] - s_fr[10], d2 = x[2] - s_fr[11];
     for (int i = 0; i < 3; ++i) y[i] = alpha * (s_fr[i] * d0 + s_fr[i + 3] * d1 + s_fr[i + 6] * d2);
   };
-  for (int i = threadIdx.x; i < nbd; i += blockDim.x) {
-    double y[3];
-    tofr(&s_raw[3 * i], y);
-    for (int d = 0; d < 3; ++d) bx[3 * i + d] = y[d];
-  }
-  __syncthreads();
-  for (int e = threadIdx.x; e < 3 * 3 * nq; e += blockDim.x) {
-    int ed = e / (3 * nq), r = e % (3 * nq), d = r / nq, q = r % nq;
-    double s = 0.0, sc = 0.0;
-    for (int k = 0; k < nq; ++k) {
-      double v = bx[3 * (ed * nq + k) + d];
-      s += T.Dgl[q + nq * k] * v;
-      sc += T.Leg[q + nq * k] * v;
+  if (rank == 0) { /* per-panel outputs: frame, boundary, Legendre coefficients, node coefficients */
+    double* fr = R.frame + (size_t)pan * RRQ_FRAME;
+    double* bx = R.bx + (size_t)pan * 3 * nbd;
+    double* bt = R.bt + (size_t)pan * 3 * nbd;
+    double* cf = R.cf + (size_t)pan * 9 * nq;
+    double* scf = R.scf + (size_t)pan * 3 * hd;
+    for (int i = threadIdx.x; i < RRQ_FRAME; i += blockDim.x) fr[i] = i < 13 ? s_fr[i] : 0.0;
+    for (int i = threadIdx.x; i < nbd; i += blockDim.x) {
+      double y[3];
+      tofr(&s_raw[3 * i], y);
+      for (int d = 0; d < 3; ++d) { bx[3 * i + d] = y[d]; s_raw[3 * i + d] = y[d]; }
     }
-    bt[3 * (ed * nq + q) + d] = s;
-    cf[ed * 3 * nq + d * nq + q] = sc;
+    __syncthreads();
+    for (int e = threadIdx.x; e < 3 * 3 * nq; e += blockDim.x) {
+      int ed = e / (3 * nq), r = e % (3 * nq), d = r / nq, q = r % nq;
+      double s = 0.0, sc = 0.0;
+      for (int k = 0; k < nq; ++k) {
+        double v = s_raw[3 * (ed * nq + k) + d];
+        s += T.Dgl[q + nq * k] * v;
+        sc += T.Leg[q + nq * k] * v;
+      }
+      bt[3 * (ed * nq + q) + d] = s;
+      cf[ed * 3 * nq + d * nq + q] = sc;
+    }
+    for (int e = threadIdx.x; e < 3 * hd; e += blockDim.x) {
+      int d = e / hd, k = e % hd;
+      double s = 0.0;
+      for (int j = 0; j < hd; ++j) {
+        double y[3];
+        tofr(&s_sx[3 * j], y);
+        s += T.umatr[k + (size_t)hd * j] * y[d];
+      }
+      scf[d * hd + k] = s;
+    }
+    for (int j = threadIdx.x; j < hd; j += blockDim.x) {
+      double y[3];
+      tofr(&s_sx[3 * j], y);
+      for (int d = 0; d < 3; ++d) R.sxf[(size_t)pan * 3 * hd + 3 * j + d] = y[d];
+    }
   }
-  /* basis at the nodes: V (quaternion, pure), H, Msl^T */
+  /* basis at the nodes: this CTA's columns of V (harmonics c0..c1) and of
+   * Msl^T (nodes c0..c1), and H rows of its nodes */
   for (int j = threadIdx.x; j < hd; j += blockDim.x) {
     double y[3], nrm[3];
     tofr(&s_sx[3 * j], y);
     const double* sn = P.snx + ((size_t)pan * hd + j) * 3;
     for (int i = 0; i < 3; ++i) nrm[i] = s_fr[i] * sn[0] + s_fr[i + 3] * sn[1] + s_fr[i + 6] * sn[2];
+    const bool ownj = j >= c0 && j < c1;
     for (int m = 1; m <= L; ++m)
       harm_column(L, m, y[0], y[1], y[2], [&](int l, int k, double h, double gx, double gy, double gz) {
-        double* q = V + ((size_t)j * hd + k) * 4;
-        q[0] = 0.0; q[1] = gx; q[2] = gy; q[3] = gz;
-        H[(size_t)j * hd + k] = h;
-        MS[(size_t)k * hd + j] = nrm[0] * gx + nrm[1] * gy + nrm[2] * gz; /* Msl^T(k,j) row-major */
-      });
-    /* Koornwinder coefficients of the frame node positions, scf[d*hd+k] */
-  }
-  __syncthreads();
-  for (int e = threadIdx.x; e < 3 * hd; e += blockDim.x) {
-    int d = e / hd, k = e % hd;
-    double s = 0.0;
-    for (int j = 0; j < hd; ++j) {
-      double y[3];
-      tofr(&s_sx[3 * j], y);
-      s += T.umatr[k + (size_t)hd * j] * y[d];
-    }
-    scf[d * hd + k] = s;
-  }
-  for (int j = threadIdx.x; j < hd; j += blockDim.x) {
-    double y[3];
-    tofr(&s_sx[3 * j], y);
-    for (int d = 0; d < 3; ++d) R.sxf[(size_t)pan * 3 * hd + 3 * j + d] = y[d];
-  }
-  __syncthreads();
-  /* in-place Gauss-Jordan inverse of the quaternion matrix V (row pivoting,
-   * pivot by quaternion norm), then of Msl^T (real) */
-  int* perm = (int*)(R.perm + (size_t)blockIdx.x * 2 * 136);
-  for (int k = 0; k < hd; ++k) {
-    double bestv = -1.0; int besti = hd;
-    for (int i = k + threadIdx.x; i < hd; i += blockDim.x) {
-      const double* q = V + ((size_t)i * hd + k) * 4;
-      double v = q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
-      if (v > bestv) { bestv = v; besti = i; }
-    }
-    int p = block_argmax(bestv, besti, sv, si);
-    if (threadIdx.x == 0) perm[k] = p;
-    if (p != k)
-      for (int e = threadIdx.x; e < 4 * hd; e += blockDim.x) {
-        double* a = V + (size_t)k * hd * 4 + e;
-        double* b = V + (size_t)p * hd * 4 + e;
-        double t = *a; *a = *b; *b = t;
-      }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      const double* q = V + ((size_t)k * hd + k) * 4;
-      double n2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
-      s_pinv[0] = q[0] / n2; s_pinv[1] = -q[1] / n2; s_pinv[2] = -q[2] / n2; s_pinv[3] = -q[3] / n2;
-    }
-    for (int e = threadIdx.x; e < hd; e += blockDim.x) {
-      const double* q = V + ((size_t)e * hd + k) * 4;
-      for (int c = 0; c < 4; ++c) s_col[4 * e + c] = q[c];
-    }
-    __syncthreads();
-    for (int j = threadIdx.x; j < hd; j += blockDim.x) {
-      double* q = V + ((size_t)k * hd + j) * 4;
-      double r[4];
-      if (j == k) { for (int c = 0; c < 4; ++c) r[c] = s_pinv[c]; }
-      else qmul(s_pinv, q, r);
-      for (int c = 0; c < 4; ++c) { q[c] = r[c]; s_row[4 * j + c] = r[c]; }
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < hd * hd; e += blockDim.x) {
-      int i = e / hd, j = e % hd;
-      if (i == k) continue;
-      double* q = V + ((size_t)i * hd + j) * 4;
-      const double* f = &s_col[4 * i];
-      double r[4];
-      if (j == k) {
-        qmul(f, s_pinv, r);
-        for (int c = 0; c < 4; ++c) q[c] = -r[c];
-      } else {
-        qmul(f, &s_row[4 * j], r);
-        for (int c = 0; c < 4; ++c) q[c] -= r[c];
-      }
-    }
-    __syncthreads();
-  }
-  for (int k = hd - 1; k >= 0; --k) {
-    int p = perm[k];
-    if (p != k)
-      for (int i = threadIdx.x; i < hd; i += blockDim.x)
-        for (int c = 0; c < 4; ++c) {
-          double* a = V + ((size_t)i * hd + k) * 4 + c;
-          double* b = V + ((size_t)i * hd + p) * 4 + c;
-          double t = *a; *a = *b; *b = t;
+        if (k >= c0 && k < c1) {
+          double* q = Vs + ((size_t)j * ncol + (k - c0)) * 4;
+          q[0] = 0.0; q[1] = gx; q[2] = gy; q[3] = gz;
         }
-    __syncthreads();
-  }
-  /* PD(j, c*hd+k) = s_c x_c(k, j), s = (+,-,-,-); stored row-major [j][4hd] */
-  double* PD = R.PD + (size_t)pan * hd * 4 * hd;
-  for (int e = threadIdx.x; e < hd * hd; e += blockDim.x) {
-    int j = e / hd, k = e % hd;
-    const double* x = V + ((size_t)k * hd + j) * 4;
-    PD[(size_t)j * 4 * hd + 0 * hd + k] = x[0];
-    PD[(size_t)j * 4 * hd + 1 * hd + k] = -x[1];
-    PD[(size_t)j * 4 * hd + 2 * hd + k] = -x[2];
-    PD[(size_t)j * 4 * hd + 3 * hd + k] = -x[3];
+        if (ownj) {
+          Ms[(size_t)k * ncol + (j - c0)] = nrm[0] * gx + nrm[1] * gy + nrm[2] * gz;
+          H[(size_t)j * hd + k] = h;
+        }
+      });
   }
   __syncthreads();
-  /* real Gauss-Jordan on Msl^T (row-major MS[k][j]) */
-  int* perm2 = perm + 136;
+  /* this thread's entries into registers */
+  double q[MAXR][4], mv[MAXR];
+#pragma unroll
+  for (int r = 0; r < MAXR; ++r) {
+    const int i = trg + RG * r;
+    const bool own = tact && i < hd;
+    for (int c = 0; c < 4; ++c) q[r][c] = own ? Vs[((size_t)i * ncol + tc) * 4 + c] : 0.0;
+    mv[r] = own ? Ms[(size_t)i * ncol + tc] : 0.0;
+    if (own && gc == 0) { pushq(0, i, q[r]); pushr(0, i, mv[r]); }
+  }
+  cl.sync();
+  double* s_pv = rowr + ncol; /* 8: pivot inverse (4), real pivot inverse, pivot rows (as doubles) */
   for (int k = 0; k < hd; ++k) {
-    double bestv = -1.0; int besti = hd;
-    for (int i = k + threadIdx.x; i < hd; i += blockDim.x) {
-      double v = fabs(MS[(size_t)i * hd + k]);
-      if (v > bestv) { bestv = v; besti = i; }
-    }
-    int p = block_argmax(bestv, besti, sv, si);
-    if (threadIdx.x == 0) perm2[k] = p;
-    if (p != k)
-      for (int e = threadIdx.x; e < hd; e += blockDim.x) {
-        double t = MS[(size_t)k * hd + e]; MS[(size_t)k * hd + e] = MS[(size_t)p * hd + e]; MS[(size_t)p * hd + e] = t;
+    const int b = k & 1;
+    double* cq = stg + b * 5 * hd;
+    double* cr = cq + 4 * hd;
+    /* warp 0: pivots among the unused rows, their inverses; the pivot rows'
+     * multipliers in this CTA's staging copy become 0 (the elimination then
+     * leaves the pivot rows alone) */
+    if (threadIdx.x < 32) {
+      double bv = -1.0, bw = -1.0;
+      int bi = hd, bj = hd;
+      for (int i = threadIdx.x; i < hd; i += 32) {
+        if (!s_used[i]) {
+          const double* f = cq + 4 * i;
+          const double v = f[0] * f[0] + f[1] * f[1] + f[2] * f[2] + f[3] * f[3];
+          if (v > bv) { bv = v; bi = i; }
+        }
+        if (!s_used[hd + i]) {
+          const double w = fabs(cr[i]);
+          if (w > bw) { bw = w; bj = i; }
+        }
       }
-    __syncthreads();
-    if (threadIdx.x == 0) s_pinv[0] = 1.0 / MS[(size_t)k * hd + k];
-    for (int e = threadIdx.x; e < hd; e += blockDim.x) s_col[e] = MS[(size_t)e * hd + k];
-    __syncthreads();
-    for (int j = threadIdx.x; j < hd; j += blockDim.x) {
-      double v = (j == k) ? s_pinv[0] : s_pinv[0] * MS[(size_t)k * hd + j];
-      MS[(size_t)k * hd + j] = v; s_row[j] = v;
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < hd * hd; e += blockDim.x) {
-      int i = e / hd, j = e % hd;
-      if (i == k) continue;
-      if (j == k) MS[(size_t)i * hd + j] = -s_col[i] * s_pinv[0];
-      else MS[(size_t)i * hd + j] -= s_col[i] * s_row[j];
-    }
-    __syncthreads();
-  }
-  for (int k = hd - 1; k >= 0; --k) {
-    int p = perm2[k];
-    if (p != k)
-      for (int i = threadIdx.x; i < hd; i += blockDim.x) {
-        double t = MS[(size_t)i * hd + k]; MS[(size_t)i * hd + k] = MS[(size_t)i * hd + p]; MS[(size_t)i * hd + p] = t;
+      for (int o = 16; o > 0; o >>= 1) {
+        const double a2 = __shfl_xor_sync(0xffffffffu, bv, o);
+        const int ia = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (a2 > bv || (a2 == bv && ia < bi)) { bv = a2; bi = ia; }
+        const double b2 = __shfl_xor_sync(0xffffffffu, bw, o);
+        const int ib = __shfl_xor_sync(0xffffffffu, bj, o);
+        if (b2 > bw || (b2 == bw && ib < bj)) { bw = b2; bj = ib; }
       }
+      if (threadIdx.x == 0) {
+        int p = bi, p2 = bj;
+        if (p >= hd || p2 >= hd) { /* a NaN column: the first unused rows (results NaN, indices in range) */
+          int f1 = 0, f2 = 0;
+          while (f1 < hd - 1 && s_used[f1]) ++f1;
+          while (f2 < hd - 1 && s_used[hd + f2]) ++f2;
+          if (p >= hd) p = f1;
+          if (p2 >= hd) p2 = f2;
+        }
+        double* f = cq + 4 * p;
+        const double n2i = 1.0 / (f[0] * f[0] + f[1] * f[1] + f[2] * f[2] + f[3] * f[3]);
+        s_pv[0] = f[0] * n2i; s_pv[1] = -f[1] * n2i; s_pv[2] = -f[2] * n2i; s_pv[3] = -f[3] * n2i;
+        s_pv[4] = 1.0 / cr[p2];
+        f[0] = 0.0; f[1] = 0.0; f[2] = 0.0; f[3] = 0.0;
+        cr[p2] = 0.0;
+        s_used[p] = 1; s_used[hd + p2] = 1;
+        s_piv[k] = p; s_piv[hd + k] = p2;
+      }
+    }
     __syncthreads();
+    const int p = s_piv[k], p2 = s_piv[hd + k];
+    const double pinv[4] = {s_pv[0], s_pv[1], s_pv[2], s_pv[3]};
+    const double rinv = s_pv[4];
+    /* the pivot rows' owners scale and publish them; the owners of column k
+     * clear their other rows (the elimination then gives -f pinv) */
+    if (tact) {
+      if (trg == p % RG) {
+        const int rp = p / RG;
+#pragma unroll
+        for (int r = 0; r < MAXR; ++r)
+          if (r == rp) {
+            double t[4];
+            if (gc == k) { t[0] = pinv[0]; t[1] = pinv[1]; t[2] = pinv[2]; t[3] = pinv[3]; }
+            else qmul(pinv, q[r], t);
+            for (int c = 0; c < 4; ++c) { q[r][c] = t[c]; rowq[4 * tc + c] = t[c]; }
+          }
+      }
+      if (trg == p2 % RG) {
+        const int rp = p2 / RG;
+#pragma unroll
+        for (int r = 0; r < MAXR; ++r)
+          if (r == rp) {
+            const double t = (gc == k) ? rinv : rinv * mv[r];
+            mv[r] = t;
+            rowr[tc] = t;
+          }
+      }
+      if (gc == k) {
+#pragma unroll
+        for (int r = 0; r < MAXR; ++r) {
+          const int i = trg + RG * r;
+          if (i != p) { q[r][0] = 0.0; q[r][1] = 0.0; q[r][2] = 0.0; q[r][3] = 0.0; }
+          if (i != p2) mv[r] = 0.0;
+        }
+      }
+    }
+    __syncthreads();
+    if (tact) {
+      const double r0 = rowq[4 * tc], r1 = rowq[4 * tc + 1], r2 = rowq[4 * tc + 2], r3 = rowq[4 * tc + 3];
+      const double rr = rowr[tc];
+#pragma unroll
+      for (int r = 0; r < MAXR; ++r) {
+        const int i = min(trg + RG * r, hd - 1); /* rows past hd: harmless repeats, never stored */
+        const double* f = cq + 4 * i;
+        const double f0 = f[0], f1 = f[1], f2 = f[2], f3 = f[3];
+        /* q -= f * row (quaternion product) */
+        q[r][0] -= f0 * r0 - f1 * r1 - f2 * r2 - f3 * r3;
+        q[r][1] -= f0 * r1 + f1 * r0 + f2 * r3 - f3 * r2;
+        q[r][2] -= f0 * r2 - f1 * r3 + f2 * r0 + f3 * r1;
+        q[r][3] -= f0 * r3 + f1 * r2 - f2 * r1 + f3 * r0;
+        mv[r] -= cr[i] * rr;
+      }
+      if (gc == k + 1) /* the next pivot column, to every CTA's other staging buffer */
+#pragma unroll
+        for (int r = 0; r < MAXR; ++r) {
+          const int i = trg + RG * r;
+          if (i < hd) { pushq(b ^ 1, i, q[r]); pushr(b ^ 1, i, mv[r]); }
+        }
+    }
+    cl.sync();
   }
-  /* B = PS H^T: B[i][j] = sum_k PS[i][k] h_k(y_j) */
+  /* inverse positions of the pivot sequences */
+  for (int k = threadIdx.x; k < hd; k += blockDim.x) { s_pos[s_piv[k]] = k; s_pos[hd + s_piv[hd + k]] = k; }
+  __syncthreads();
+  /* X^-1[k][c] = X[pi(k)][pi^-1(c)]: the entry X[i][gc] of this thread is
+   * X^-1[pos(i)][piv(gc)].  PD(j, c*hd+k) = s_c Vinv_c(k, j), s = (+,-,-,-),
+   * row-major [j][4hd]; PS = MS^-1 row-major */
+  double* PD = R.PD + (size_t)pan * hd * 4 * hd;
+  double* PS = R.smat + (size_t)pan * hd * hd;
+  if (tact) {
+    const int jq = s_piv[gc], jm = s_piv[hd + gc];
+#pragma unroll
+    for (int r = 0; r < MAXR; ++r) {
+      const int i = trg + RG * r;
+      if (i >= hd) continue;
+      const int kq = s_pos[i], km = s_pos[hd + i];
+      double* d = PD + (size_t)jq * 4 * hd + kq;
+      d[0] = q[r][0]; d[hd] = -q[r][1]; d[2 * hd] = -q[r][2]; d[3 * hd] = -q[r][3];
+      PS[(size_t)km * hd + jm] = mv[r];
+    }
+  }
+  __threadfence();
+  cl.sync();
+  /* B = PS H^T, rows c0..c1: B[i][j] = sum_k PS[i][k] h_k(y_j) */
   double* B = R.B + (size_t)pan * hd * hd;
-  for (int e = threadIdx.x; e < hd * hd; e += blockDim.x) {
-    int i = e / hd, j = e % hd;
+  for (int e = threadIdx.x; e < nc * hd; e += blockDim.x) {
+    const int i = c0 + e / hd, j = e % hd;
     double s = 0.0;
-    for (int k = 0; k < hd; ++k) s += MS[(size_t)i * hd + k] * H[(size_t)j * hd + k];
+    for (int k = 0; k < hd; ++k) s += PS[(size_t)i * hd + k] * H[(size_t)j * hd + k];
     B[(size_t)i * hd + j] = s;
   }
 }
@@ -1400,8 +1470,44 @@ cudaError_t qol_launch_scan(int npan, int lev, const int* cnt, long long* off, c
 }
 cudaError_t qol_launch_rrq_panel(const OrderTab& T, const PanelIn& P, const PairWS& G, const RRQWS& R, int npan,
                                  const double* chart, cudaStream_t st) {
-  k_rrq_panel<<<npan, 256, 0, st>>>(T, P, G, R, chart);
-  return cudaGetLastError();
+  if (npan <= 0) return cudaSuccess;
+  /* the smallest cluster (then the wider CTA) whose threads hold few enough
+   * rows to keep them in registers: at most 6 rows with 512 threads (128
+   * registers a thread), 12 with 384 */
+  int cs = 0, nt = 0, maxr = 0;
+  for (int c = 1; c <= 8 && !cs; c *= 2)
+    for (int t : {512, 384}) {
+      const int m = panel_maxr(T.hd, c, t);
+      if (m <= (t == 512 ? 6 : 12)) { cs = c; nt = t; maxr = m; break; }
+    }
+  if (!cs) return cudaErrorInvalidConfiguration;
+  const size_t smem = sizeof(double) * panel_smem_doubles(T.hd, 3 * T.nquad, cs);
+  if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
+  auto go = [&](auto kern) -> cudaError_t {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(npan * cs));
+    cfg.blockDim = dim3((unsigned)nt);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)cs;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, T, P, G, R, chart);
+  };
+  /* the configurations of nterms 2..16 */
+#define QOL_PANEL_CASE(C, N, M) \
+  if (cs == C && nt == N && maxr <= M) return go(k_rrq_panel<C, N, M>);
+  QOL_PANEL_CASE(1, 512, 1) QOL_PANEL_CASE(1, 512, 2) QOL_PANEL_CASE(1, 512, 3) QOL_PANEL_CASE(1, 512, 5)
+  QOL_PANEL_CASE(1, 384, 10) QOL_PANEL_CASE(2, 512, 5) QOL_PANEL_CASE(2, 512, 6) QOL_PANEL_CASE(2, 384, 12)
+  QOL_PANEL_CASE(4, 512, 6) QOL_PANEL_CASE(4, 384, 10) QOL_PANEL_CASE(8, 512, 5)
+#undef QOL_PANEL_CASE
+  return cudaErrorInvalidConfiguration;
 }
 cudaError_t qol_launch_rrq_ssq(const OrderTab& T, const PairIn& Q, const PairWS& G, const RRQWS& R, cudaStream_t st) {
   const long long n = R.ghi - R.glo;

@@ -55,8 +55,7 @@ struct RRQWS {
   long long nrrq;
   const long long* rrq_off; /* npan + 1 */
   double *frame, *bx, *bt, *cf, *scf, *sxf;
-  double *qmat, *hmat, *smat, *PD, *B;
-  int* perm;
+  double *hmat, *smat, *PD, *B; /* per panel: H, S inverse, D inverse rows, B = PS H^T */
   double *JD, *RS; /* per RRQ pair: 4hd, hd */
   double* line;    /* per RRQ pair: cD (3 nbd), cS (3 nbd), lint (3), Omega */
   double* edge;    /* per RRQ pair and edge: w1 (nq), w3 (nq), ok, Re t0, Im t0 */

@@ -233,12 +233,10 @@ extern "C" int qol_rrq_noalloc(qol_int m, const double* tx, qol_int n, const dou
   R.cf = (double*)take(sizeof(double) * 9 * nq);
   R.scf = (double*)take(sizeof(double) * 3 * hd);
   R.sxf = (double*)take(sizeof(double) * 3 * hd);
-  R.qmat = (double*)take(sizeof(double) * 4 * hd * hd);
   R.hmat = (double*)take(sizeof(double) * hd * hd);
   R.smat = (double*)take(sizeof(double) * hd * hd);
   R.PD = (double*)take(sizeof(double) * 4 * hd * hd);
   R.B = (double*)take(sizeof(double) * hd * hd);
-  R.perm = (int*)take(sizeof(int) * 272);
   R.JD = (double*)take(sizeof(double) * (size_t)m * 4 * hd);
   R.RS = (double*)take(sizeof(double) * (size_t)m * hd);
   R.line = (double*)take(sizeof(double) * (size_t)m * (6 * nbd + 4));
