@@ -29,6 +29,10 @@ __constant__ double c_rq[QOL_MAXL + 2][QOL_MAXL + 2]; /* 1/((l+m)(l-m)), l > m *
 __constant__ double c_rn[QOL_MAXL + 2][QOL_MAXL + 2]; /* sqrt((l-m)!(l+m)!) */
 __constant__ double c_rd[QOL_MAXL + 2];               /* 1/(2m) */
 __constant__ double c_rinv[QOL_MAXL + 2];             /* 1/l, 0 at l = 0 */
+/* three-term recurrences without divisions (k_rrq_geom) */
+__constant__ double c_la[QOL_MAXNQ + 2];            /* (2k+1)/(k+1) */
+__constant__ double c_lb[QOL_MAXNQ + 2];            /* k/(k+1) */
+__device__ double g_jq[QOL_MAXL + 1][QOL_MAXL + 1][4]; /* Jacobi P^(2a+1,0)_b: (c2, c3, c4)/c1 */
 
 void qol_upload_harm_coefs(const double* hb, const double* hc, const double* hcm, cudaStream_t st) {
   cudaMemcpyToSymbolAsync(c_hb, hb, sizeof(double) * (QOL_MAXL + 2) * (QOL_MAXL + 2), 0,
@@ -52,6 +56,24 @@ void qol_upload_harm_coefs(const double* hb, const double* hc, const double* hcm
   cudaMemcpyToSymbolAsync(c_rn, rn, sizeof(rn), 0, cudaMemcpyHostToDevice, st);
   cudaMemcpyToSymbolAsync(c_rd, rd, sizeof(rd), 0, cudaMemcpyHostToDevice, st);
   cudaMemcpyToSymbolAsync(c_rinv, rinv, sizeof(rinv), 0, cudaMemcpyHostToDevice, st);
+  double la[QOL_MAXNQ + 2] = {}, lb[QOL_MAXNQ + 2] = {};
+  for (int k = 0; k < QOL_MAXNQ + 2; ++k) { la[k] = (2.0 * k + 1.0) / (k + 1.0); lb[k] = k / (k + 1.0); }
+  cudaMemcpyToSymbolAsync(c_la, la, sizeof(la), 0, cudaMemcpyHostToDevice, st);
+  cudaMemcpyToSymbolAsync(c_lb, lb, sizeof(lb), 0, cudaMemcpyHostToDevice, st);
+  static double jq[QOL_MAXL + 1][QOL_MAXL + 1][4];
+  for (int a = 0; a <= QOL_MAXL; ++a)
+    for (int b = 0; b <= QOL_MAXL; ++b) {
+      const double al = 2.0 * a + 1.0, j = b;
+      const double c1 = 2.0 * j * (j + al) * (2.0 * j + al - 2.0);
+      const double c2 = (2.0 * j + al - 1.0) * (al * al);
+      const double c3 = (2.0 * j + al - 2.0) * (2.0 * j + al - 1.0) * (2.0 * j + al);
+      const double c4 = 2.0 * (j + al - 1.0) * (j - 1.0) * (2.0 * j + al);
+      jq[a][b][0] = b >= 2 ? c2 / c1 : 0.0;
+      jq[a][b][1] = b >= 2 ? c3 / c1 : 0.0;
+      jq[a][b][2] = b >= 2 ? c4 / c1 : 0.0;
+      jq[a][b][3] = 0.0;
+    }
+  cudaMemcpyToSymbolAsync(g_jq, jq, sizeof(jq), 0, cudaMemcpyHostToDevice, st);
   cudaStreamSynchronize(st); /* the host tables above are locals */
 }
 
@@ -731,7 +753,8 @@ struct WarpSM {
 /* warp-cooperative surface evaluation for the side test: f[c*3+p] = sum_k
  * pols_k(point p) scf[c*hd+k] for the coordinates c = x,y,z and the points
  * (u,v), (u+h,v), (u,v+h).  Lane a evaluates the polynomials (a, b),
- * b = 0..korder-a, i.e. L_a(s,t) P_b^{(2a+1,0)}(z) (the host basis). */
+ * b = 0..korder-a, i.e. L_a(s,t) P_b^{(2a+1,0)}(z) (the host basis), the
+ * three points as independent recurrences; coefficient tables, no divisions. */
 __device__ void koorn_eval3_warp(int korder, int hd, const double* scf, double u, double v, double h,
                                  double* f /* 9 */) {
   const int lane = threadIdx.x & 31;
@@ -741,35 +764,52 @@ __device__ void koorn_eval3_warp(int korder, int hd, const double* scf, double u
   if (lane <= korder) {
     const int a = lane;
     const double us[3] = {u, u + h, u}, vs[3] = {v, v, v + h};
+    double sv[3], tt[3], zv[3], L0[3], L1[3], La[3];
 #pragma unroll
     for (int p = 0; p < 3; ++p) {
-      double s = 2.0 * us[p] + vs[p] - 1.0, t = 1.0 - vs[p], z = 2.0 * vs[p] - 1.0;
-      double L0 = 1.0, L1 = s, La = 1.0;
-      if (a >= 1) La = s;
-      for (int q = 1; q < a; ++q) {
-        double L2 = ((2.0 * q + 1.0) * s * L1 - q * t * t * L0) / (q + 1.0);
-        L0 = L1; L1 = L2; La = L2;
+      sv[p] = 2.0 * us[p] + vs[p] - 1.0;
+      const double t = 1.0 - vs[p];
+      tt[p] = t * t;
+      zv[p] = 2.0 * vs[p] - 1.0;
+      L0[p] = 1.0; L1[p] = sv[p]; La[p] = a >= 1 ? sv[p] : 1.0;
+    }
+    for (int q = 1; q < a; ++q) {
+      const double ca = c_la[q], cb = c_lb[q];
+#pragma unroll
+      for (int p = 0; p < 3; ++p) {
+        const double L2 = ca * sv[p] * L1[p] - cb * tt[p] * L0[p];
+        L0[p] = L1[p]; L1[p] = L2; La[p] = L2;
       }
-      double alpha = 2.0 * a + 1.0;
-      double p0 = 1.0, p1 = 0.5 * (alpha + 2.0) * z + 0.5 * alpha;
-      for (int b = 0; b <= korder - a; ++b) {
-        double pb;
-        if (b == 0) pb = p0;
-        else if (b == 1) pb = p1;
-        else {
-          double jj = b;
-          double c1 = 2.0 * jj * (jj + alpha) * (2.0 * jj + alpha - 2.0);
-          double c2 = (2.0 * jj + alpha - 1.0) * (alpha * alpha);
-          double c3 = (2.0 * jj + alpha - 2.0) * (2.0 * jj + alpha - 1.0) * (2.0 * jj + alpha);
-          double c4 = 2.0 * (jj + alpha - 1.0) * (jj - 1.0) * (2.0 * jj + alpha);
-          double p2 = ((c2 + c3 * z) * p1 - c4 * p0) / c1;
-          p0 = p1; p1 = p2; pb = p2;
+    }
+    const double alpha = 2.0 * a + 1.0;
+    double p0[3], p1[3];
+#pragma unroll
+    for (int p = 0; p < 3; ++p) { p0[p] = 1.0; p1[p] = 0.5 * (alpha + 2.0) * zv[p] + 0.5 * alpha; }
+    const double* jq = &g_jq[a][0][0];
+    for (int b = 0; b <= korder - a; ++b) {
+      double pb[3];
+      if (b == 0) {
+#pragma unroll
+        for (int p = 0; p < 3; ++p) pb[p] = p0[p];
+      } else if (b == 1) {
+#pragma unroll
+        for (int p = 0; p < 3; ++p) pb[p] = p1[p];
+      } else {
+        const double A = jq[4 * b], B = jq[4 * b + 1], C = jq[4 * b + 2];
+#pragma unroll
+        for (int p = 0; p < 3; ++p) {
+          const double p2 = (A + B * zv[p]) * p1[p] - C * p0[p];
+          p0[p] = p1[p]; p1[p] = p2; pb[p] = p2;
         }
-        int deg = a + b, idx = deg * (deg + 1) / 2 + b;
-        double val = La * pb;
-        acc[0 * 3 + p] += val * scf[idx];
-        acc[1 * 3 + p] += val * scf[hd + idx];
-        acc[2 * 3 + p] += val * scf[2 * hd + idx];
+      }
+      const int deg = a + b, idx = deg * (deg + 1) / 2 + b;
+      const double s0 = scf[idx], s1 = scf[hd + idx], s2 = scf[2 * hd + idx];
+#pragma unroll
+      for (int p = 0; p < 3; ++p) {
+        const double val = La[p] * pb[p];
+        acc[p] += val * s0;
+        acc[3 + p] += val * s1;
+        acc[6 + p] += val * s2;
       }
     }
   }
@@ -778,6 +818,24 @@ __device__ void koorn_eval3_warp(int korder, int hd, const double* scf, double u
     double x = acc[i];
     for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
     f[i] = x;
+  }
+}
+
+/* the three coordinate series (3 x n Legendre coefficients) of one edge and
+ * their derivatives at t, one recurrence for all three, no divisions */
+__device__ __forceinline__ void leg_eval3(int n, const double* c, double t, double* y, double* yp) {
+  double p0 = 1.0, p1 = t, d0 = 0.0, d1 = 1.0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) { y[d] = c[d * n]; yp[d] = 0.0; }
+  if (n > 1)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) { y[d] += c[d * n + 1] * p1; yp[d] += c[d * n + 1] * d1; }
+  for (int k = 1; k + 1 < n; ++k) {
+    const double p2 = c_la[k] * t * p1 - c_lb[k] * p0;
+    const double d2 = d0 + (2.0 * k + 1.0) * p1;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) { y[d] += c[d * n + k + 1] * p2; yp[d] += c[d * n + k + 1] * d2; }
+    p0 = p1; p1 = p2; d0 = d1; d1 = d2;
   }
 }
 
@@ -920,7 +978,7 @@ __global__ void __launch_bounds__(32 * RRQ_WARPS) k_rrq_geom(OrderTab T, PairIn 
       for (int pnt = lane; pnt < 96; pnt += 32) {
         int e = pnt >> 5, q = pnt & 31;
         double t = -1.0 + (2.0 * q + 1.0) / 32.0, y[3], yp[3];
-        for (int d = 0; d < 3; ++d) leg_eval_r(nq, cf + e * 3 * nq + d * nq, t, y[d], yp[d]);
+        leg_eval3(nq, cf + e * 3 * nq, t, y, yp);
         double rho[3] = {y[0] - xt0, y[1] - xt1, y[2] - xt2};
         double r = sqrt(dot3(rho, rho));
         cu = fmin(cu, (r - rho[2]) / r);
@@ -946,7 +1004,7 @@ __global__ void __launch_bounds__(32 * RRQ_WARPS) k_rrq_geom(OrderTab T, PairIn 
         if (!(b > a)) continue;
         double hm = 0.5 * (b - a), cm = 0.5 * (a + b), t = cm + hm * T.gl16x[q];
         double y[3], yp[3];
-        for (int d = 0; d < 3; ++d) leg_eval_r(nq, cf + e * 3 * nq + d * nq, t, y[d], yp[d]);
+        leg_eval3(nq, cf + e * 3 * nq, t, y, yp);
         double rho[3] = {y[0] - xt0, y[1] - xt1, y[2] - xt2};
         double r = sqrt(dot3(rho, rho));
         double s3[3] = {0.0, 0.0, sdir}, c[3];
