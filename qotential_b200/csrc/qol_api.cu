@@ -310,20 +310,24 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
   const long long nrrq = off_h.back();
   R.nrrq = nrrq;
   /* per-pair RRQ moment storage (separate arena: its size is known only now) */
-  rc = g_arena2.reserve(sizeof(double) * (size_t)std::max<long long>(nrrq, 1) * (5 * hd + 6 * nbd + 4 + 3 * (2 * nq + 3)) +
-                        4096);
+  rc = g_arena2.reserve(sizeof(double) * (size_t)std::max<long long>(nrrq, 1) * (5 * hd + 6 * nbd + 4 + 3 * (2 * nq + 3) + 1) +
+                        8192);
   if (rc) return rc;
   g_arena2.reset();
   R.JD = g_arena2.take<double>((size_t)std::max<long long>(nrrq, 1) * 4 * hd);
   R.RS = g_arena2.take<double>((size_t)std::max<long long>(nrrq, 1) * hd);
   R.line = g_arena2.take<double>((size_t)std::max<long long>(nrrq, 1) * (6 * nbd + 4));
   R.edge = g_arena2.take<double>((size_t)std::max<long long>(nrrq, 1) * 3 * (2 * nq + 3));
+  R.pair = g_arena2.take<int2>((size_t)std::max<long long>(nrrq, 1));
   OutCOO O{};
   O.vs = J.vs; O.vd = J.vd; O.omega = J.omega; O.subtract_naive = J.subtract_naive;
   rec(2);
   CK(qol_launch_direct(T, J.P, J.Q, W, G, O, npan, st));
   rec(3);
-  if (nrrq > 0) CK(qol_launch_rrq_panel(T, J.P, G, R, npan, J.chart, st));
+  if (nrrq > 0) {
+    CK(qol_launch_rrq_pairs(T, J.Q, G, R, npan, st));
+    CK(qol_launch_rrq_panel(T, J.P, G, R, npan, J.chart, st));
+  }
   const int nch = J.chunk_pan ? (int)J.chunk_pan->size() - 1 : 1;
   for (int c = 0; c < nch; ++c) {
     const long long a = J.chunk_pan ? (*J.chunk_pan)[c] : 0, b = J.chunk_pan ? (*J.chunk_pan)[c + 1] : npan;

@@ -881,15 +881,9 @@ __global__ void __launch_bounds__(128) k_rrq_ssq(OrderTab T, PairIn Q, PairWS G,
   if (tid >= 3 * (R.ghi - R.glo)) return;
   const long long gidx = R.glo + tid / 3;
   const int e = (int)(tid % 3);
-  int lo = 0, hi = R.npan;
-  while (hi - lo > 1) {
-    int mid = (lo + hi) >> 1;
-    if (R.rrq_off[mid] <= gidx) lo = mid; else hi = mid;
-  }
-  const int pan = lo;
-  const int j_loc = (int)(gidx - R.rrq_off[pan]);
+  const int2 pr = R.pair[gidx]; /* (panel, local target) */
+  const int pan = pr.x, tl = pr.y;
   const long long p0 = Q.tcxi[pan] - 1;
-  const int tl = G.grp[p0 + G.off[(size_t)pan * 8 + T.nlevel + 1] + j_loc];
   const int nq = T.nquad, nbd = 3 * nq;
   const double* fr = R.frame + (size_t)pan * RRQ_FRAME;
   const double* bx = R.bx + (size_t)pan * 3 * nbd;
@@ -916,15 +910,9 @@ __global__ void __launch_bounds__(32 * RRQ_WARPS) k_rrq_geom(OrderTab T, PairIn 
   const long long gidx = R.glo + (long long)blockIdx.x * RRQ_WARPS + wid;
   if (gidx >= R.ghi) return;
   WarpSM& W = S[wid];
-  int lo = 0, hi = R.npan;
-  while (hi - lo > 1) {
-    int mid = (lo + hi) >> 1;
-    if (R.rrq_off[mid] <= gidx) lo = mid; else hi = mid;
-  }
-  const int pan = lo;
-  const int j_loc = (int)(gidx - R.rrq_off[pan]);
+  const int2 pr = R.pair[gidx]; /* (panel, local target) */
+  const int pan = pr.x, tl = pr.y;
   const long long p0 = Q.tcxi[pan] - 1;
-  const int tl = G.grp[p0 + G.off[(size_t)pan * 8 + T.nlevel + 1] + j_loc];
   const int hd = T.hd, nq = T.nquad, nbd = 3 * nq, L = T.nterms, ng = T.ng;
   const double* fr = R.frame + (size_t)pan * RRQ_FRAME;
   const double* bx = R.bx + (size_t)pan * 3 * nbd;
@@ -1079,10 +1067,10 @@ __global__ void __launch_bounds__(32 * RRQ_WARPS) k_rrq_geom(OrderTab T, PairIn 
 
 __host__ __device__ constexpr int mom_rows(int L) { return L * (L + 1); }
 /* doubles of shared memory per warp: line record (rounded to 2), then the
- * node chunk, later reused for M (6 rows), R(x) and T (6 rows) */
+ * node chunk, later reused for M (7 rows: entries padded to 14 doubles), R(x) and T (6 rows) */
 __host__ __device__ constexpr int mom_region(int L) {
-  return mom_rows(L) * MOM_CS > 12 * mom_rows(L) + (L + 1) * (L + 2) ? mom_rows(L) * MOM_CS
-                                                                      : 12 * mom_rows(L) + (L + 1) * (L + 2);
+  return mom_rows(L) * MOM_CS > 13 * mom_rows(L) + (L + 1) * (L + 2) ? mom_rows(L) * MOM_CS
+                                                                      : 13 * mom_rows(L) + (L + 1) * (L + 2);
 }
 __host__ __device__ constexpr int mom_warp_doubles(int L, int nbd) { return ((6 * nbd + 4 + 1) & ~1) + mom_region(L); }
 
@@ -1102,15 +1090,9 @@ __global__ void __launch_bounds__(32 * MOM_WARPS) k_rrq_moments(OrderTab T, Pair
   __syncthreads();
   const long long gidx = R.glo + (long long)blockIdx.x * MOM_WARPS + wid;
   if (gidx >= R.ghi) return;
-  int lo = 0, hi = R.npan;
-  while (hi - lo > 1) {
-    int mid = (lo + hi) >> 1;
-    if (R.rrq_off[mid] <= gidx) lo = mid; else hi = mid;
-  }
-  const int pan = lo;
-  const int j_loc = (int)(gidx - R.rrq_off[pan]);
+  const int2 pr = R.pair[gidx]; /* (panel, local target) */
+  const int pan = pr.x, tl = pr.y;
   const long long p0 = Q.tcxi[pan] - 1;
-  const int tl = G.grp[p0 + G.off[(size_t)pan * 8 + T.nlevel + 1] + j_loc];
   const int hd = T.hd, nq = T.nquad, nbd = 3 * nq, L = T.nterms;
   const double* fr = R.frame + (size_t)pan * RRQ_FRAME;
   const double* bx = R.bx + (size_t)pan * 3 * nbd;
@@ -1212,7 +1194,7 @@ __global__ void __launch_bounds__(32 * MOM_WARPS) k_rrq_moments(OrderTab T, Pair
   /* M[entry][6 components][re,im] with the 1/lam (D) and 1/(lam+1) (S)
    * segment weights; then R(x) up to degree L; then T */
   double* Mt = ch;
-  double* Rx = ch + 6 * NE;
+  double* Rx = ch + 7 * NE; /* M entries 14 doubles apart: double2 gathers spread over all bank slots */
   double* Tt = Rx + (L + 1) * (L + 2);
 #pragma unroll
   for (int r = 0; r < RPL; ++r) {
@@ -1222,7 +1204,7 @@ __global__ void __launch_bounds__(32 * MOM_WARPS) k_rrq_moments(OrderTab T, Pair
       int lam = 0;
       while ((lam + 1) * (lam + 2) / 2 <= ent) ++lam;
       const double wD = s_ri[lam], wS = s_ri[lam + 1];
-      double* dst = Mt + ent * 12 + ri;
+      double* dst = Mt + ent * 14 + ri;
       dst[0] = acc[r][0] * wD; dst[2] = acc[r][1] * wD; dst[4] = acc[r][2] * wD;
       dst[6] = acc[r][3] * wS; dst[8] = acc[r][4] * wS; dst[10] = acc[r][5] * wS;
     }
@@ -1276,7 +1258,7 @@ __global__ void __launch_bounds__(32 * MOM_WARPS) k_rrq_moments(OrderTab T, Pair
       if (w & (1u << 25)) d = -d;
       double p = d, q = c;
       if (w & (1u << 24)) { p = -d; q = -c; }
-      const double2* mv = reinterpret_cast<const double2*>(Mt + em * 12);
+      const double2* mv = reinterpret_cast<const double2*>(Mt + em * 14);
 #pragma unroll
       for (int k = 0; k < 6; ++k) {
         const double2 v = mv[k];
@@ -1459,6 +1441,15 @@ __global__ void __launch_bounds__(256) k_rrq_apply(OrderTab T, PanelIn P, PairIn
 /* ===================================================================== */
 /* K7: COO row/column indices (block column-major per panel)            */
 /* ===================================================================== */
+/* (panel, local target) of every RRQ pair, in RRQ pair order */
+__global__ void __launch_bounds__(128) k_rrq_pairs(OrderTab T, PairIn Q, PairWS G, RRQWS R) {
+  const int pan = blockIdx.x;
+  const long long g0 = R.rrq_off[pan], n = R.rrq_off[pan + 1] - g0;
+  const long long p0 = Q.tcxi[pan] - 1;
+  const int* grp = G.grp + p0 + G.off[(size_t)pan * 8 + T.nlevel + 1];
+  for (long long j = threadIdx.x; j < n; j += blockDim.x) R.pair[g0 + j] = make_int2(pan, grp[j]);
+}
+
 __global__ void __launch_bounds__(256) k_coo_index(OrderTab T, PairIn Q, long long* si, long long* sj) {
   const int pan = blockIdx.x, hd = T.hd;
   const long long p0 = Q.tcxi[pan] - 1, m = Q.tcxi[pan + 1] - Q.tcxi[pan];
@@ -1566,6 +1557,12 @@ cudaError_t qol_launch_rrq_panel(const OrderTab& T, const PanelIn& P, const Pair
   QOL_PANEL_CASE(4, 512, 6) QOL_PANEL_CASE(4, 384, 10) QOL_PANEL_CASE(8, 512, 5)
 #undef QOL_PANEL_CASE
   return cudaErrorInvalidConfiguration;
+}
+cudaError_t qol_launch_rrq_pairs(const OrderTab& T, const PairIn& Q, const PairWS& G, const RRQWS& R, int npan,
+                                 cudaStream_t st) {
+  if (npan <= 0 || R.nrrq == 0) return cudaSuccess;
+  k_rrq_pairs<<<npan, 128, 0, st>>>(T, Q, G, R);
+  return cudaGetLastError();
 }
 cudaError_t qol_launch_rrq_ssq(const OrderTab& T, const PairIn& Q, const PairWS& G, const RRQWS& R, cudaStream_t st) {
   const long long n = R.ghi - R.glo;

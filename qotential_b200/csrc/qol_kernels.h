@@ -60,6 +60,7 @@ struct RRQWS {
   double* line;    /* per RRQ pair: cD (3 nbd), cS (3 nbd), lint (3), Omega */
   double* edge;    /* per RRQ pair and edge: w1 (nq), w3 (nq), ok, Re t0, Im t0 */
   double* ialpha;  /* per RRQ pair (nullable) */
+  int2* pair;      /* per RRQ pair: (panel, local target) */
   long long glo, ghi; /* RRQ pairs [glo, ghi) of this launch (per-pair kernels) */
   int plo, phi;       /* panels [plo, phi) of this launch (k_rrq_apply) */
 };
@@ -80,6 +81,8 @@ cudaError_t qol_launch_direct(const OrderTab& T, const PanelIn& P, const PairIn&
 cudaError_t qol_launch_scan(int npan, int lev, const int* cnt, long long* off, cudaStream_t st);
 cudaError_t qol_launch_rrq_panel(const OrderTab& T, const PanelIn& P, const PairWS& G, const RRQWS& R, int npan,
                                  const double* chart, cudaStream_t st);
+cudaError_t qol_launch_rrq_pairs(const OrderTab& T, const PairIn& Q, const PairWS& G, const RRQWS& R, int npan,
+                                 cudaStream_t st);
 cudaError_t qol_launch_rrq_ssq(const OrderTab& T, const PairIn& Q, const PairWS& G, const RRQWS& R, cudaStream_t st);
 cudaError_t qol_launch_rrq_geom(const OrderTab& T, const PairIn& Q, const PairWS& G, const RRQWS& R, int exterior,
                                 cudaStream_t st);

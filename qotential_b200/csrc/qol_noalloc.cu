@@ -241,6 +241,7 @@ extern "C" int qol_rrq_noalloc(qol_int m, const double* tx, qol_int n, const dou
   R.RS = (double*)take(sizeof(double) * (size_t)m * hd);
   R.line = (double*)take(sizeof(double) * (size_t)m * (6 * nbd + 4));
   R.edge = (double*)take(sizeof(double) * (size_t)m * 3 * (2 * nq + 3));
+  R.pair = (int2*)take(sizeof(int2) * (size_t)(m > 0 ? m : 1));
   if (over) {
     std::snprintf(g_na_msg, sizeof g_na_msg,
                   "qol_rrq_noalloc: m = %lld targets at order %lld need %zu bytes of scratch; the static scratch "
@@ -268,6 +269,7 @@ extern "C" int qol_rrq_noalloc(qol_int m, const double* tx, qol_int n, const dou
   R.glo = 0; R.ghi = nrrq; R.plo = 0; R.phi = 1;
   NA_CK(qol_launch_direct(T, P, Q, W, G, O, 1, st));
   if (nrrq > 0) {
+    NA_CK(qol_launch_rrq_pairs(T, Q, G, R, 1, st));
     NA_CK(qol_launch_rrq_panel(T, P, G, R, 1, nullptr, st));
     NA_CK(qol_launch_rrq_target(T, Q, G, R, exterior != 0, st));
     NA_CK(qol_launch_rrq_apply(T, P, Q, G, R, O, st));
