@@ -10,6 +10,7 @@
 #include <deque>
 #include <functional>
 #include <thread>
+#include <emmintrin.h>
 #include <sys/mman.h>
 #include <unistd.h>
 #include <cmath>
@@ -418,7 +419,9 @@ int tables_match(int nquad, int korder, const double* tgl, const double* wgl, co
  * into the caller's arrays.  The COO indices are a layout function of
  * tcxrow/tcxi (k_coo_index computes the same), so that entry point fills them
  * on host threads while the GPU works instead of moving them over the link. */
-constexpr size_t kStageBytes = (size_t)16 << 20;
+/* small pieces: the ring (32 MiB) can stay in the host's last-level cache
+ * between the DMA write and the copy out */
+constexpr size_t kStageBytes = (size_t)2 << 20;
 /* wall-clock milestones of the last host-pointer call, ms from its start:
  * inputs queued, all chunks queued, value copies queued, values landed,
  * every host task done, end, indices filled */
@@ -446,8 +449,8 @@ struct StageRing {
 } g_ring;
 
 /* host threads draining a task queue in order (the index fills are queued
- * first and run while the GPU computes, the staging copies follow);
- * finish() runs what is queued and joins */
+ * first and run while the GPU computes, then the value pages are mapped,
+ * the staging copies follow); finish() runs what is queued and joins */
 class Workers {
  public:
   explicit Workers(int n) {
@@ -560,6 +563,34 @@ void prefault(void* p, size_t n) {
   if (b > a) madvise((void*)a, b - a, MADV_POPULATE_WRITE);
 }
 
+/* The output arrays are written once and not read back here: streaming
+ * (non-temporal) stores skip the read of each destination line that an
+ * ordinary store makes, which is a third of the host memory traffic. */
+void copy_out(void* dst, const void* src, size_t n /* a multiple of 8 */) {
+  char* d = (char*)dst;
+  const char* s = (const char*)src;
+  if (n >= 8 && ((uintptr_t)d & 15)) {
+    long long v;
+    std::memcpy(&v, s, 8);
+    _mm_stream_si64((long long*)d, v);
+    d += 8; s += 8; n -= 8;
+  }
+  for (; n >= 64; n -= 64, d += 64, s += 64) {
+    const __m128i a = _mm_loadu_si128((const __m128i*)s), b = _mm_loadu_si128((const __m128i*)(s + 16));
+    const __m128i c = _mm_loadu_si128((const __m128i*)(s + 32)), e = _mm_loadu_si128((const __m128i*)(s + 48));
+    _mm_stream_si128((__m128i*)d, a);
+    _mm_stream_si128((__m128i*)(d + 16), b);
+    _mm_stream_si128((__m128i*)(d + 32), c);
+    _mm_stream_si128((__m128i*)(d + 48), e);
+  }
+  for (; n >= 8; n -= 8, d += 8, s += 8) {
+    long long v;
+    std::memcpy(&v, s, 8);
+    _mm_stream_si64((long long*)d, v);
+  }
+  _mm_sfence();
+}
+
 /* COO indices of panels [k0, k1) (reference order (tcxi(k)-1) hd + (j-1) m + i) */
 void fill_indices(long long k0, long long k1, int hd, const long long* tcxi, const long long* tcxrow, long long* si,
                   long long* sj) {
@@ -570,9 +601,12 @@ void fill_indices(long long k0, long long k1, int hd, const long long* tcxi, con
     const long long* row = tcxrow + p0;
     for (int j = 0; j < hd; ++j) {
       const long long col = k * hd + j + 1;
-      for (long long i = 0; i < m; ++i) { oi[(size_t)j * m + i] = row[i]; oj[(size_t)j * m + i] = col; }
+      long long* a = oi + (size_t)j * m;
+      long long* b = oj + (size_t)j * m;
+      for (long long i = 0; i < m; ++i) { _mm_stream_si64(a + i, row[i]); _mm_stream_si64(b + i, col); }
     }
   }
+  _mm_sfence();
 }
 
 } // namespace
@@ -883,11 +917,13 @@ int qol_getnearquad_lap_rrq(qol_int npan, qol_int nterms, qol_int hdim, qol_int 
         if (--fills_left == 0) g_host_ms[6] = ms_since(tstart);
       });
     /* then the value arrays' pages, in chunk order */
-    for (double* arr : {sparsevs, sparsevd})
-      for (size_t o = 0; o < nout; o += (size_t)8 << 20) {
-        const size_t n = std::min((size_t)8 << 20, nout - o);
-        W.submit([=] { prefault(arr + o, n * sizeof(double)); });
+    for (int c = 0; c < nch; ++c) {
+      const size_t t0 = (size_t)(tcxi[cb[c]] - 1) * hd, t1 = (size_t)(tcxi[cb[c + 1]] - 1) * hd;
+      for (size_t o = t0; o < t1; o += (size_t)4 << 20) {
+        const size_t n = std::min((size_t)4 << 20, t1 - o);
+        for (double* arr : {sparsevs, sparsevd}) W.submit([=] { prefault(arr + o, n * sizeof(double)); });
       }
+    }
     /* values: chunk c leaves the GPU once the compute stream passed its event */
     std::vector<cudaEvent_t> cev(nch, nullptr);
     for (int c = 0; c < nch && !out; ++c)
@@ -916,7 +952,7 @@ int qol_getnearquad_lap_rrq(qol_int npan, qol_int nterms, qol_int hdim, qol_int 
               return;
             }
             W.submit([&, b, dst, off, n] {
-              if (cudaEventSynchronize(g_ring.ev[b]) == cudaSuccess) std::memcpy(dst + off, g_ring.buf[b], n);
+              if (cudaEventSynchronize(g_ring.ev[b]) == cudaSuccess) copy_out(dst + off, g_ring.buf[b], n);
               else werr = 1;
               fl.give(b);
             });
