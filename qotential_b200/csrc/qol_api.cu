@@ -187,7 +187,11 @@ int order_tables(int nterms, int orderff, int nquad, OrderCache** out) {
   std::vector<uint32_t> xs;
   qolh::xlate_schedule(nterms, xs, T.xsteps);
   T.xsched = C->up(xs);
-  if (!T.tgl || !T.Mb || !T.vruv || !T.xsched) return fail(QOL_ERR_CUDA, "table upload failed");
+  std::vector<double> tgi((size_t)nquad * nquad, 0.0); /* Bjorck-Pereyra node-difference reciprocals */
+  for (int k = 0; k + 1 < nquad; ++k)
+    for (int i = k + 1; i < nquad; ++i) tgi[(size_t)k * nquad + i] = 1.0 / (tgl[i] - tgl[i - k - 1]);
+  T.tginv = C->up(tgi);
+  if (!T.tgl || !T.Mb || !T.vruv || !T.xsched || !T.tginv) return fail(QOL_ERR_CUDA, "table upload failed");
   *out = C.get();
   g_orders[key] = std::move(C);
   return 0;

@@ -100,14 +100,33 @@ __device__ inline void koorn_pols_dev(double u, double v, int korder, double* po
   }
 }
 
-/* Bjorck-Pereyra dual Vandermonde solve, b overwritten */
-__device__ inline void bjorck_pereyra_dual_dev(int n, const double* x, double* b) {
+/* Bjorck-Pereyra dual Vandermonde solve, b overwritten; xinv[k*n + i] =
+ * 1/(x[i] - x[i-k-1]) (a per-node-set table) */
+__device__ inline void bjorck_pereyra_dual_dev(int n, const double* x, const double* xinv, double* b) {
   int N = n - 1;
   for (int k = 0; k < N; ++k)
     for (int i = N; i >= k + 1; --i) b[i] -= x[k] * b[i - 1];
   for (int k = N - 1; k >= 0; --k) {
-    for (int i = k + 1; i <= N; ++i) b[i] /= (x[i] - x[i - k - 1]);
+    for (int i = k + 1; i <= N; ++i) b[i] *= xinv[k * n + i];
     for (int i = k; i <= N - 1; ++i) b[i] -= b[i + 1];
+  }
+}
+
+/* the three coordinate series (3 x n Legendre coefficients) at complex t,
+ * one recurrence; la[k] = (2k+1)/(k+1), lb[k] = k/(k+1) */
+__device__ inline void leg_eval3_c(int n, const double* c, cd t, const double* la, const double* lb, cd* f, cd* fp) {
+  cd p0 = mk(1.0, 0.0), p1 = t, d0 = mk(0.0, 0.0), d1 = mk(1.0, 0.0);
+  for (int d = 0; d < 3; ++d) { f[d] = mk(c[d * n], 0.0); fp[d] = mk(0.0, 0.0); }
+  if (n > 1)
+    for (int d = 0; d < 3; ++d) { f[d] = cadd(f[d], cscale(c[d * n + 1], p1)); fp[d] = cadd(fp[d], cscale(c[d * n + 1], d1)); }
+  for (int k = 1; k + 1 < n; ++k) {
+    cd p2 = csub(cscale(la[k], cmul(t, p1)), cscale(lb[k], p0));
+    cd d2 = cadd(d0, cscale(2.0 * k + 1.0, p1));
+    for (int d = 0; d < 3; ++d) {
+      f[d] = cadd(f[d], cscale(c[d * n + k + 1], p2));
+      fp[d] = cadd(fp[d], cscale(c[d * n + k + 1], d2));
+    }
+    p0 = p1; p1 = p2; d0 = d1; d1 = d2;
   }
 }
 
@@ -122,7 +141,7 @@ __device__ inline double bernstein_radius_dev(cd t0) {
 /* root of |gamma(t)-x|^2 for one edge; returns ok flag, t0 with Im >= 0 */
 __device__ inline bool edge_root_dev(int n, const double* cf /* 3 x n */, const double* tg,
                                      const double* bx /* 3 x n node positions */, const double* x,
-                                     cd& t0) {
+                                     const double* la, const double* lb, cd& t0) {
   int ib = 0;
   double best = 1e300;
   for (int i = 0; i < n; ++i) {
@@ -131,22 +150,23 @@ __device__ inline bool edge_root_dev(int n, const double* cf /* 3 x n */, const 
     if (d2 < best) { best = d2; ib = i; }
   }
   double g[3], gp[3];
-  for (int d = 0; d < 3; ++d) {
-    double f, fp;
-    leg_eval_r(n, cf + d * n, tg[ib], f, fp);
-    g[d] = f - x[d]; gp[d] = fp;
+  {
+    cd f3[3], fp3[3];
+    leg_eval3_c(n, cf, mk(tg[ib], 0.0), la, lb, f3, fp3);
+    for (int d = 0; d < 3; ++d) { g[d] = f3[d].re - x[d]; gp[d] = fp3[d].re; }
   }
   double aa = dot3(gp, gp), bb = dot3(g, gp), cc = dot3(g, g);
   double disc = fmax(aa * cc - bb * bb, 0.0);
   cd t = mk(tg[ib] - bb / aa, sqrt(disc) / aa);
   for (int it = 0; it < 40; ++it) {
     cd F = mk(0.0, 0.0), Fp = mk(0.0, 0.0);
+    cd f3[3], fp3[3];
+    leg_eval3_c(n, cf, t, la, lb, f3, fp3);
     for (int d = 0; d < 3; ++d) {
-      cd f, fp;
-      leg_eval_c(n, cf + d * n, t, f, fp);
+      cd f = f3[d];
       f.re -= x[d];
       F = cadd(F, cmul(f, f));
-      Fp = cadd(Fp, cscale(2.0, cmul(f, fp)));
+      Fp = cadd(Fp, cscale(2.0, cmul(f, fp3[d])));
     }
     if (Fp.re == 0.0 && Fp.im == 0.0) return false;
     cd dt = cdiv(F, Fp);
@@ -163,8 +183,8 @@ __device__ inline bool edge_root_dev(int n, const double* cf /* 3 x n */, const 
 /* modified singularity-swap weights on one edge (see the oracle for the
  * derivation of the recurrences) */
 __device__ inline void ssq_weights_dev(int n, const double* tg, const double* wg, bool ok, cd t0,
-                                       const double* gl48x, const double* gl48w, double* w1,
-                                       double* w3) {
+                                       const double* gl48x, const double* gl48w, const double* tginv,
+                                       const double* rk /* 1/k */, double* w1, double* w3) {
   double rho = ok ? bernstein_radius_dev(t0) : 1e300;
   bool use = ok && rho < QOL_RHO_SSQ && fabs(t0.im) > 0.0;
   if (!use) {
@@ -182,7 +202,7 @@ __device__ inline void ssq_weights_dev(int n, const double* tg, const double* wg
       double bnd = s1 - ((k - 1) % 2 == 0 ? 1.0 : -1.0) * sm;
       double v = (2.0 * k - 1.0) * a * Q[k - 1] + bnd;
       if (k >= 2) v -= (k - 1.0) * t02 * Q[k - 2];
-      Q[k] = v / k;
+      Q[k] = v * rk[k];
     }
     P[0] = ((1.0 - a) / s1 + (1.0 + a) / sm) / (b * b);
     for (int k = 1; k < n; ++k) {
@@ -200,8 +220,8 @@ __device__ inline void ssq_weights_dev(int n, const double* tg, const double* wg
       for (int k = 0; k < n; ++k) { Q[k] += tk * f1; P[k] += tk * f3; tk *= t; }
     }
   }
-  bjorck_pereyra_dual_dev(n, tg, Q);
-  bjorck_pereyra_dual_dev(n, tg, P);
+  bjorck_pereyra_dual_dev(n, tg, tginv, Q);
+  bjorck_pereyra_dual_dev(n, tg, tginv, P);
   for (int i = 0; i < n; ++i) {
     double s = sqrt((tg[i] - a) * (tg[i] - a) + b * b);
     w1[i] = Q[i] * s;

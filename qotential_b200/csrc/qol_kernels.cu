@@ -32,6 +32,7 @@ __constant__ double c_rinv[QOL_MAXL + 2];             /* 1/l, 0 at l = 0 */
 /* three-term recurrences without divisions (k_rrq_geom) */
 __constant__ double c_la[QOL_MAXNQ + 2];            /* (2k+1)/(k+1) */
 __constant__ double c_lb[QOL_MAXNQ + 2];            /* k/(k+1) */
+__constant__ double c_rk[QOL_MAXNQ + 2];            /* 1/k, 0 at k = 0 */
 __device__ double g_jq[QOL_MAXL + 1][QOL_MAXL + 1][4]; /* Jacobi P^(2a+1,0)_b: (c2, c3, c4)/c1 */
 
 void qol_upload_harm_coefs(const double* hb, const double* hc, const double* hcm, cudaStream_t st) {
@@ -60,6 +61,9 @@ void qol_upload_harm_coefs(const double* hb, const double* hc, const double* hcm
   for (int k = 0; k < QOL_MAXNQ + 2; ++k) { la[k] = (2.0 * k + 1.0) / (k + 1.0); lb[k] = k / (k + 1.0); }
   cudaMemcpyToSymbolAsync(c_la, la, sizeof(la), 0, cudaMemcpyHostToDevice, st);
   cudaMemcpyToSymbolAsync(c_lb, lb, sizeof(lb), 0, cudaMemcpyHostToDevice, st);
+  double rk[QOL_MAXNQ + 2] = {};
+  for (int k = 1; k < QOL_MAXNQ + 2; ++k) rk[k] = 1.0 / k;
+  cudaMemcpyToSymbolAsync(c_rk, rk, sizeof(rk), 0, cudaMemcpyHostToDevice, st);
   static double jq[QOL_MAXL + 1][QOL_MAXL + 1][4];
   for (int a = 0; a <= QOL_MAXL; ++a)
     for (int b = 0; b <= QOL_MAXL; ++b) {
@@ -897,8 +901,8 @@ __global__ void __launch_bounds__(128) k_rrq_ssq(OrderTab T, PairIn Q, PairWS G,
   }
   double* er = R.edge + ((size_t)gidx * 3 + e) * (2 * nq + 3);
   cd t0 = mk(0.0, 0.0);
-  bool ok = edge_root_dev(nq, cf + e * 3 * nq, T.tgl, bx + 3 * e * nq, xt, t0);
-  ssq_weights_dev(nq, T.tgl, T.wgl, ok, t0, T.gl48x, T.gl48w, er, er + nq);
+  bool ok = edge_root_dev(nq, cf + e * 3 * nq, T.tgl, bx + 3 * e * nq, xt, c_la, c_lb, t0);
+  ssq_weights_dev(nq, T.tgl, T.wgl, ok, t0, T.gl48x, T.gl48w, T.tginv, c_rk, er, er + nq);
   er[2 * nq] = ok ? 1.0 : 0.0;
   er[2 * nq + 1] = t0.re;
   er[2 * nq + 2] = t0.im;

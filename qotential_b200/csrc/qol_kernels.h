@@ -19,6 +19,7 @@ struct OrderTab {
   const double* umatr; /* hd x hd col-major (vals -> coefs) */
   const double* vruv;  /* 2 x hd VR nodes of degree korder */
   const unsigned* xsched; /* xsteps x 32 translation terms (qolh::xlate_schedule) */
+  const double* tginv;    /* nquad x nquad: 1/(tgl[i] - tgl[i-k-1]) at [k*nquad + i] */
   int xsteps;
 };
 

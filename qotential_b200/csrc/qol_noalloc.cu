@@ -150,6 +150,10 @@ int na_tables(NoAllocDev& D, int nterms, int orderff, int nquad, cudaStream_t st
   std::vector<uint32_t> xs;
   qolh::xlate_schedule(nterms, xs, T.xsteps);
   size_t o_xs = put(xs.data(), sizeof(uint32_t) * xs.size());
+  std::vector<double> tgi((size_t)nquad * nquad, 0.0); /* Bjorck-Pereyra node-difference reciprocals */
+  for (int k = 0; k + 1 < nquad; ++k)
+    for (int i = k + 1; i < nquad; ++i) tgi[(size_t)k * nquad + i] = 1.0 / (tgl[i] - tgl[i - k - 1]);
+  size_t o_tgi = put(tgi.data(), sizeof(double) * tgi.size());
   size_t bytes = (stage.size() + 255) & ~(size_t)255;
   if (bytes > QOL_NOALLOC_SCRATCH_BYTES / 2)
     return na_fail(QOL_ERR_LIMIT, "qol_rrq_noalloc: tables of this order exceed half of the 16 MiB scratch");
@@ -169,6 +173,7 @@ int na_tables(NoAllocDev& D, int nterms, int orderff, int nquad, cudaStream_t st
   T.tq = (const double*)dp(o_tq); T.wq = (const double*)dp(o_wq);
   T.Mb = (const double*)dp(o_Mb); T.umatr = (const double*)dp(o_um); T.vruv = (const double*)dp(o_vr);
   T.xsched = (const unsigned*)dp(o_xs);
+  T.tginv = (const double*)dp(o_tgi);
   D.T = T;
   D.table_bytes = bytes;
   D.key = key;
