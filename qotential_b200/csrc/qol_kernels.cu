@@ -1323,44 +1323,39 @@ __global__ void __launch_bounds__(32 * MOM_WARPS) k_rrq_moments(OrderTab T, Pair
 /* ===================================================================== */
 /* K6: RRQ solves as matrix products per panel + naive subtraction + COO */
 /* ===================================================================== */
-#define AT 64 /* RRQ targets per chunk */
-#define AQ 32 /* inner-dimension tile */
-/* Out[t][j] (+)= sum_q M[j][q] In[t][q] for AT targets and hd rows j, with
- * the q range tiled through shared memory; thread (tx, ty) holds targets
- * tx + 16a (a < 4) and rows ty + 16b (b < NB). */
-template <int NB>
-__device__ __forceinline__ void apply_tile_gemm(const double* __restrict__ M, int ldm, const double* In, int ldin,
-                                                int hd, int nq, int nt, double (&acc)[4][NB], double* sM,
-                                                double* sI) {
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  for (int q0 = 0; q0 < nq; q0 += AQ) {
+#define AT 64  /* RRQ targets per chunk: 8 warps x 8 */
+#define AK 32  /* inner-dimension tile */
+#define AKS 36 /* tile row stride (doubles): m8n8k4 fragment loads hit 16 distinct bank pairs */
+/* Out[t][j] += sum_k A[t][k] Bt[j][k] over k < K on the FP64 tensor path, for the
+ * chunk's targets t (warp w: 8w..8w+7) and all NB column blocks of 8;
+ * load(k0, sA_tile, sB_tile) fills the K tile [k0, k0+AK) (A: AT x AKS, Bt: 8NB x AKS,
+ * zero outside the data) */
+template <int NB, class Load>
+__device__ __forceinline__ void apply_dmma(int K, double (&acc)[NB][2], double* sAt, double* sBt, Load load) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int fr = lane >> 2, fc = lane & 3;
+  for (int k0 = 0; k0 < K; k0 += AK) {
     __syncthreads();
-    for (int e = threadIdx.x; e < hd * AQ; e += blockDim.x) {
-      int j = e / AQ, q = e % AQ;
-      sM[q * (16 * NB) + j] = (q0 + q < nq) ? M[(size_t)j * ldm + q0 + q] : 0.0;
-    }
-    for (int e = threadIdx.x; e < AT * AQ; e += blockDim.x) {
-      int tt = e / AQ, q = e % AQ;
-      sI[q * AT + tt] = (tt < nt && q0 + q < nq) ? In[(size_t)tt * ldin + q0 + q] : 0.0;
-    }
+    load(k0, sAt, sBt);
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncthreads();
-#pragma unroll 4
-    for (int q = 0; q < AQ; ++q) {
-      double iv[4], mv[NB];
+#pragma unroll 2
+    for (int ks = 0; ks < AK / 4; ++ks) {
+      const double a = sAt[(8 * w + fr) * AKS + 4 * ks + fc];
 #pragma unroll
-      for (int a = 0; a < 4; ++a) iv[a] = sI[q * AT + tx + 16 * a];
-#pragma unroll
-      for (int b = 0; b < NB; ++b) mv[b] = sM[q * (16 * NB) + ty + 16 * b];
-#pragma unroll
-      for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < NB; ++b) acc[a][b] += mv[b] * iv[a];
+      for (int b = 0; b < NB; ++b) dmma(acc[b][0], acc[b][1], a, sBt[(8 * b + fr) * AKS + 4 * ks + fc]);
     }
   }
 }
+__device__ __forceinline__ void cp_or_zero(double* dst, const double* src, bool ok) {
+  if (ok) cp_async8(dst, src);
+  else *dst = 0.0;
+}
 
+/* per panel, chunks of AT RRQ targets: Ad = PD JD, As = (PS RS + B Ad) / alpha,
+ * naive-block subtraction and the COO values (and Omega for qol_rrq) */
 template <int NB>
-__global__ void __launch_bounds__(256) k_rrq_apply(OrderTab T, PanelIn P, PairIn Q, PairWS G, RRQWS R, OutCOO O) {
+__global__ void __launch_bounds__(256, 2) k_rrq_apply(OrderTab T, PanelIn P, PairIn Q, PairWS G, RRQWS R, OutCOO O) {
   const int pan = R.plo + blockIdx.x;
   const int cnt = G.cnt[(size_t)pan * 8 + T.nlevel + 1];
   if (cnt == 0) return;
@@ -1372,65 +1367,84 @@ __global__ void __launch_bounds__(256) k_rrq_apply(OrderTab T, PanelIn P, PairIn
   const double* PS = R.smat + (size_t)pan * hd * hd;
   const double* B = R.B + (size_t)pan * hd * hd;
   const double alpha = R.frame[(size_t)pan * RRQ_FRAME + 12];
-  extern __shared__ double sm[];
-  double* sM = sm;                   /* AQ x 16NB */
-  double* sI = sM + AQ * 16 * NB;    /* AQ x AT */
-  double* sA = sI + AQ * AT;         /* AT x hd: Ad of the chunk, row-major per target */
+  extern __shared__ __align__(16) double sm[];
+  double* sAt = sm;                 /* AT x AKS */
+  double* sBt = sAt + AT * AKS;     /* 8NB x AKS */
+  double* sAd = sBt + 8 * NB * AKS; /* AT x hd: Ad of the chunk */
   __shared__ int tloc[AT];
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int fr = lane >> 2, fc = lane & 3;
   const double i4p = 1.0 / (4.0 * QOL_PI);
   for (int c0 = 0; c0 < cnt; c0 += AT) {
     const int nt = min(AT, cnt - c0);
     __syncthreads();
     if (threadIdx.x < AT) tloc[threadIdx.x] = threadIdx.x < nt ? G.grp[p0 + offl + c0 + threadIdx.x] : 0;
-    double acc[4][NB];
+    double acc[NB][2];
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int b = 0; b < NB; ++b) acc[a][b] = 0.0;
-    /* Ad = PD JD */
-    apply_tile_gemm<NB>(PD, N4, R.JD + (size_t)(g0 + c0) * N4, N4, hd, N4, nt, acc, sM, sI);
-    __syncthreads();
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int b = 0; b < NB; ++b) {
-        int t = tx + 16 * a, j = ty + 16 * b;
-        if (j < hd) sA[t * hd + j] = acc[a][b];
-        acc[a][b] = 0.0;
+    for (int b = 0; b < NB; ++b) { acc[b][0] = 0.0; acc[b][1] = 0.0; }
+    const double* JD = R.JD + (size_t)(g0 + c0) * N4;
+    const double* RS = R.RS + (size_t)(g0 + c0) * hd;
+    /* Ad[t][j] = sum_q JD[t][q] PD[j][q] */
+    apply_dmma<NB>(N4, acc, sAt, sBt, [&](int k0, double* a, double* bt) {
+      for (int e = threadIdx.x; e < AT * AK; e += blockDim.x) {
+        const int t = e / AK, k = e % AK;
+        cp_or_zero(&a[t * AKS + k], JD + (size_t)t * N4 + k0 + k, t < nt && k0 + k < N4);
       }
-    /* As = (PS RS + B Ad) / alpha */
-    apply_tile_gemm<NB>(PS, hd, R.RS + (size_t)(g0 + c0) * hd, hd, hd, hd, nt, acc, sM, sI);
-    apply_tile_gemm<NB>(B, hd, sA, hd, hd, hd, nt, acc, sM, sI);
-    /* naive block, COO values, Omega */
+      for (int e = threadIdx.x; e < 8 * NB * AK; e += blockDim.x) {
+        const int j = e / AK, k = e % AK;
+        cp_or_zero(&bt[j * AKS + k], PD + (size_t)j * N4 + k0 + k, j < hd && k0 + k < N4);
+      }
+      asm volatile("cp.async.commit_group;\n" ::: "memory");
+    });
 #pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      const int t = tx + 16 * a;
-      if (t >= nt) continue;
+    for (int b = 0; b < NB; ++b)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int t = 8 * w + fr, j = 8 * b + 2 * fc + h;
+        if (j < hd) sAd[t * hd + j] = acc[b][h];
+        acc[b][h] = 0.0;
+      }
+    __syncthreads();
+    /* As[t][i] = sum_k RS[t][k] PS[i][k] + sum_j Ad[t][j] B[i][j] */
+    apply_dmma<NB>(2 * hd, acc, sAt, sBt, [&](int k0, double* a, double* bt) {
+      for (int e = threadIdx.x; e < AT * AK; e += blockDim.x) {
+        const int t = e / AK, k = e % AK, kk = k0 + k;
+        if (kk < hd) cp_or_zero(&a[t * AKS + k], RS + (size_t)t * hd + kk, t < nt);
+        else a[t * AKS + k] = (kk < 2 * hd) ? sAd[t * hd + kk - hd] : 0.0;
+      }
+      for (int e = threadIdx.x; e < 8 * NB * AK; e += blockDim.x) {
+        const int i = e / AK, k = e % AK, kk = k0 + k;
+        const bool ok = i < hd && kk < 2 * hd;
+        cp_or_zero(&bt[i * AKS + k], kk < hd ? PS + (size_t)i * hd + kk : B + (size_t)i * hd + (kk - hd), ok);
+      }
+      asm volatile("cp.async.commit_group;\n" ::: "memory");
+    });
+    /* naive block, COO values */
+    const int t = 8 * w + fr;
+    if (t < nt) {
       const int tl = tloc[t];
       const long long row = Q.tcxrow[p0 + tl];
       const double* x = Q.tcx + 3 * (p0 + tl);
+      const double x0 = x[0], x1 = x[1], x2 = x[2];
 #pragma unroll
-      for (int b = 0; b < NB; ++b) {
-        const int j = ty + 16 * b;
-        if (j >= hd) continue;
-        double vs = acc[a][b] / alpha, vd = sA[t * hd + j];
-        if (O.subtract_naive) {
-          size_t gj = (size_t)pan * hd + j;
-          if (row != (long long)gj + 1) {
-            double dx = x[0] - P.sx[3 * gj], dy = x[1] - P.sx[3 * gj + 1], dz = x[2] - P.sx[3 * gj + 2];
-            double rr = dx * dx + dy * dy + dz * dz;
-            if (rr > 1.0e-28) {
-              double w4 = P.sw[gj] * i4p, r = sqrt(rr);
-              vs -= w4 / r;
-              vd -= w4 * (dx * P.snx[3 * gj] + dy * P.snx[3 * gj + 1] + dz * P.snx[3 * gj + 2]) / (r * rr);
-            }
+      for (int b = 0; b < NB; ++b)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int j = 8 * b + 2 * fc + h;
+          if (j >= hd) continue;
+          double vs = acc[b][h] / alpha, vd = sAd[t * hd + j];
+          if (O.subtract_naive) {
+            const size_t gj = (size_t)pan * hd + j;
+            double ns = 0.0, nd = 0.0;
+            if (row != (long long)gj + 1)
+              sdl_kernel(x0 - P.sx[3 * gj], x1 - P.sx[3 * gj + 1], x2 - P.sx[3 * gj + 2], P.snx[3 * gj],
+                         P.snx[3 * gj + 1], P.snx[3 * gj + 2], P.sw[gj] * i4p, ns, nd);
+            vs -= ns; vd -= nd;
           }
+          const size_t o = (size_t)p0 * hd + (size_t)j * m + tl;
+          O.vs[o] = vs;
+          O.vd[o] = vd;
         }
-        size_t o = (size_t)p0 * hd + (size_t)j * m + tl;
-        O.vs[o] = vs;
-        O.vd[o] = vd;
-      }
     }
     /* Omega (reference layout, qol_rrq only): (J_s, -J_x, -J_y, -J_z)/alpha */
     if (O.omega)
@@ -1440,6 +1454,10 @@ __global__ void __launch_bounds__(256) k_rrq_apply(OrderTab T, PanelIn P, PairIn
         O.omega[(size_t)tloc[tt] * N4 + q] = (q < hd ? v : -v) / alpha;
       }
   }
+}
+template <int NB>
+constexpr size_t apply_smem(int hd) {
+  return sizeof(double) * ((size_t)AT * AKS + (size_t)8 * NB * AKS + (size_t)AT * hd);
 }
 
 /* ===================================================================== */
@@ -1612,17 +1630,29 @@ cudaError_t qol_launch_rrq_apply(const OrderTab& T, const PanelIn& P, const Pair
                                  const RRQWS& R, const OutCOO& O, cudaStream_t st) {
   const int npan = R.phi - R.plo;
   if (npan <= 0) return cudaSuccess;
-  const int NBn = (T.hd + 15) / 16;
-  auto go = [&](auto kern, int nb) {
-    size_t smem = sizeof(double) * ((size_t)AQ * 16 * nb + AQ * AT + (size_t)AT * T.hd);
+  auto go = [&](auto kern, size_t smem) {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     kern<<<npan, 256, smem, st>>>(T, P, Q, G, R, O);
   };
-  if (NBn <= 2) go(k_rrq_apply<2>, 2);
-  else if (NBn <= 3) go(k_rrq_apply<3>, 3);
-  else if (NBn <= 4) go(k_rrq_apply<4>, 4);
-  else if (NBn <= 6) go(k_rrq_apply<6>, 6);
-  else go(k_rrq_apply<9>, 9);
+  switch ((T.hd + 7) / 8) { /* column blocks of 8 */
+    case 1: go(k_rrq_apply<1>, apply_smem<1>(T.hd)); break;
+    case 2: go(k_rrq_apply<2>, apply_smem<2>(T.hd)); break;
+    case 3: go(k_rrq_apply<3>, apply_smem<3>(T.hd)); break;
+    case 4: go(k_rrq_apply<4>, apply_smem<4>(T.hd)); break;
+    case 5: go(k_rrq_apply<5>, apply_smem<5>(T.hd)); break;
+    case 6: go(k_rrq_apply<6>, apply_smem<6>(T.hd)); break;
+    case 7: go(k_rrq_apply<7>, apply_smem<7>(T.hd)); break;
+    case 8: go(k_rrq_apply<8>, apply_smem<8>(T.hd)); break;
+    case 9: go(k_rrq_apply<9>, apply_smem<9>(T.hd)); break;
+    case 10: go(k_rrq_apply<10>, apply_smem<10>(T.hd)); break;
+    case 11: go(k_rrq_apply<11>, apply_smem<11>(T.hd)); break;
+    case 12: go(k_rrq_apply<12>, apply_smem<12>(T.hd)); break;
+    case 13: go(k_rrq_apply<13>, apply_smem<13>(T.hd)); break;
+    case 14: go(k_rrq_apply<14>, apply_smem<14>(T.hd)); break;
+    case 15: go(k_rrq_apply<15>, apply_smem<15>(T.hd)); break;
+    case 16: go(k_rrq_apply<16>, apply_smem<16>(T.hd)); break;
+    default: go(k_rrq_apply<17>, apply_smem<17>(T.hd)); break;
+  }
   return cudaGetLastError();
 }
 cudaError_t qol_launch_coo_index(const OrderTab& T, const PairIn& Q, long long* si, long long* sj, int npan,
