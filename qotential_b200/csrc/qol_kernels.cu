@@ -250,14 +250,15 @@ __device__ __forceinline__ void sdl_kernel(double dx, double dy, double dz, doub
   }
 }
 
-/* one CTA per (panel, level); chunks of DTT targets.  Per tile of DNT level
- * nodes: kernel values KS, KD (DNT x DTT) and interpolation rows It (DNT x hd,
- * async copy) in shared memory, then S and D (targets x hd) += K It on the
- * FP64 tensor path.  Warp w: targets 16 (w>>2) .. +15, columns 8 NB (w&3) ..,
- * NB column blocks of 8 */
+/* one CTA per (panel, level); chunks of DTT targets.  Tiles of DNT level nodes,
+ * double-buffered in shared memory: the node data and interpolation rows of
+ * tile t+1 arrive by async copy while the FP64 tensor path accumulates S and D
+ * (targets x hd) += K It over tile t; then the kernel values KS, KD of tile t+1
+ * are formed from the staged nodes.  Warp w: targets 16 (w>>2) .. +15,
+ * columns 8 NB (w&3) .., NB column blocks of 8 */
 template <int NB>
-__global__ void __launch_bounds__(256, 2) k_direct(OrderTab T, PanelIn P, PairIn Q, LevelWS W,
-                                                                  PairWS G, OutCOO O) {
+__global__ void __launch_bounds__(256, 2) k_direct(OrderTab T, PanelIn P, PairIn Q, LevelWS W, PairWS G,
+                                                   OutCOO O) {
   const int pan = blockIdx.x, l = blockIdx.y;
   if (l >= T.nlevel) return;
   const int cntl = G.cnt[(size_t)pan * 8 + l + 1];
@@ -267,52 +268,78 @@ __global__ void __launch_bounds__(256, 2) k_direct(OrderTab T, PanelIn P, PairIn
   const long long p0 = Q.tcxi[pan] - 1, m = Q.tcxi[pan + 1] - Q.tcxi[pan];
   const double* node = W.node[l] + (size_t)pan * n * 7;
   const double* I = T.interp[l];
-  constexpr int NCW = 32 * NB;     /* padded columns */
-  constexpr int ICS = NCW + 4;     /* interpolation-tile row stride */
+  constexpr int NCW = 32 * NB; /* padded columns */
+  constexpr int ICS = NCW + 4; /* interpolation-tile row stride */
+  constexpr int STG = 2 * DNT * DKS + DNT * ICS + 8 * DNT; /* doubles per stage: KS, KD, It, nodes (7 x DNT, padded) */
   extern __shared__ __align__(16) double dsm[];
-  double* KS = dsm;                /* DNT x DKS */
-  double* KD = KS + DNT * DKS;     /* DNT x DKS */
-  double* It = KD + DNT * DKS;     /* DNT x ICS */
-  double* tg = It + DNT * ICS;     /* DTT x 3 */
+  double* tg = dsm + 2 * STG; /* DTT x 3 */
   int* tloc = (int*)(tg + 3 * DTT);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int tb0 = 16 * (w >> 2), cb0 = 8 * NB * (w & 3);
   const int fr = lane >> 2, fc = lane & 3;
   const double i4p = 1.0 / (4.0 * QOL_PI);
+  const int ntile = (n + DNT - 1) / DNT;
+  /* async copies of tile t into stage s: interpolation rows and the 7 node fields */
+  auto fetch = [&](int t, int s) {
+    double* It = dsm + s * STG + 2 * DNT * DKS;
+    double* nd = It + DNT * ICS;
+    const int n0 = t * DNT;
+    for (int e = threadIdx.x; e < DNT * NCW; e += blockDim.x) {
+      const int nn = e / NCW, c = e % NCW, i = n0 + nn;
+      if (i < n && c < hd) cp_async8(&It[nn * ICS + c], I + (size_t)i * hd + c);
+      else It[nn * ICS + c] = 0.0;
+    }
+    for (int e = threadIdx.x; e < 7 * DNT; e += blockDim.x) {
+      const int f = e / DNT, nn = e % DNT, i = n0 + nn;
+      if (i < n) cp_async8(&nd[f * DNT + nn], node + (size_t)f * n + i);
+      else nd[f * DNT + nn] = 0.0;
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  /* kernel values of tile t (its nodes already staged in stage s) */
+  auto kvals = [&](int t, int s, int nt) {
+    double* KS = dsm + s * STG;
+    double* KD = KS + DNT * DKS;
+    const double* nd = KD + DNT * DKS + DNT * ICS;
+    const int n0 = t * DNT;
+    for (int e = threadIdx.x; e < DNT * DTT; e += blockDim.x) {
+      const int nn = e / DTT, tt = e % DTT;
+      double sv = 0.0, dv = 0.0;
+      if (n0 + nn < n && tt < nt)
+        sdl_kernel(tg[3 * tt] - nd[nn], tg[3 * tt + 1] - nd[DNT + nn], tg[3 * tt + 2] - nd[2 * DNT + nn],
+                   nd[3 * DNT + nn], nd[4 * DNT + nn], nd[5 * DNT + nn], nd[6 * DNT + nn] * i4p, sv, dv);
+      KS[nn * DKS + tt] = sv;
+      KD[nn * DKS + tt] = dv;
+    }
+  };
   for (int c0 = 0; c0 < cntl; c0 += DTT) {
     const int nt = min(DTT, cntl - c0);
     __syncthreads();
+    fetch(0, 0);
     if (threadIdx.x < DTT) {
       const int tl = threadIdx.x < nt ? G.grp[p0 + offl + c0 + threadIdx.x] : -1;
       tloc[threadIdx.x] = tl;
       for (int d = 0; d < 3; ++d) tg[3 * threadIdx.x + d] = tl >= 0 ? Q.tcx[3 * (p0 + tl) + d] : 0.0;
     }
+    cp_async_wait_all();
+    __syncthreads();
+    kvals(0, 0, nt);
+    __syncthreads();
     double cS[2][NB][2], cD[2][NB][2];
 #pragma unroll
     for (int a = 0; a < 2; ++a)
 #pragma unroll
       for (int b = 0; b < NB; ++b) { cS[a][b][0] = cS[a][b][1] = 0.0; cD[a][b][0] = cD[a][b][1] = 0.0; }
-    for (int n0 = 0; n0 < n; n0 += DNT) {
-      __syncthreads();
-      for (int e = threadIdx.x; e < DNT * NCW; e += blockDim.x) {
-        const int nn = e / NCW, c = e % NCW, i = n0 + nn;
-        if (i < n && c < hd) cp_async8(&It[nn * ICS + c], I + (size_t)i * hd + c);
-        else It[nn * ICS + c] = 0.0;
-      }
-      asm volatile("cp.async.commit_group;\n" ::: "memory");
-      for (int e = threadIdx.x; e < DNT * DTT; e += blockDim.x) {
-        const int nn = e / DTT, tt = e % DTT, i = n0 + nn;
-        double s = 0.0, dv = 0.0;
-        if (i < n && tt < nt)
-          sdl_kernel(tg[3 * tt] - node[i], tg[3 * tt + 1] - node[n + i], tg[3 * tt + 2] - node[2 * n + i],
-                     node[3 * n + i], node[4 * n + i], node[5 * n + i], node[6 * n + i] * i4p, s, dv);
-        KS[nn * DKS + tt] = s;
-        KD[nn * DKS + tt] = dv;
-      }
-      cp_async_wait_all();
-      __syncthreads();
+    for (int t = 0; t < ntile; ++t) {
+      const int s = t & 1;
+      if (t + 1 < ntile) fetch(t + 1, s ^ 1);
+      const double* KS = dsm + s * STG;
+      const double* KD = KS + DNT * DKS;
+      const double* It = KD + DNT * DKS;
+      const int nn_max = min(DNT, n - t * DNT);
 #pragma unroll 2
       for (int ks = 0; ks < DNT / 4; ++ks) {
+        if (4 * ks >= nn_max) break;
         const int kr = 4 * ks + fc;
         const double aS0 = KS[kr * DKS + tb0 + fr], aS1 = KS[kr * DKS + tb0 + 8 + fr];
         const double aD0 = KD[kr * DKS + tb0 + fr], aD1 = KD[kr * DKS + tb0 + 8 + fr];
@@ -325,6 +352,12 @@ __global__ void __launch_bounds__(256, 2) k_direct(OrderTab T, PanelIn P, PairIn
           dmma(cD[1][b][0], cD[1][b][1], aD1, bv);
         }
       }
+      if (t + 1 < ntile) {
+        cp_async_wait_all();
+        __syncthreads(); /* tile t+1's nodes staged; stage s^1's kernel values no longer read */
+        kvals(t + 1, s ^ 1, nt);
+      }
+      __syncthreads(); /* tile t+1's kernel values visible; stage s free for tile t+2 */
     }
     /* naive block and the COO write */
 #pragma unroll
@@ -358,7 +391,7 @@ __global__ void __launch_bounds__(256, 2) k_direct(OrderTab T, PanelIn P, PairIn
 }
 template <int NB>
 constexpr size_t direct_smem() {
-  return sizeof(double) * (2 * DNT * DKS + DNT * (32 * NB + 4) + 3 * DTT) + sizeof(int) * DTT;
+  return sizeof(double) * (2 * (2 * DNT * DKS + DNT * (32 * NB + 4) + 8 * DNT) + 3 * DTT) + sizeof(int) * DTT;
 }
 
 /* ===================================================================== */
