@@ -185,13 +185,16 @@ int order_tables(int nterms, int orderff, int nquad, OrderCache** out) {
   T.gl48x = C->up(g48x); T.gl48w = C->up(g48w); T.gl16x = C->up(g16x); T.gl16w = C->up(g16w);
   T.tq = C->up(tq); T.wq = C->up(wq); T.Mb = C->up(Mb); T.umatr = C->up(um); T.vruv = C->up(vr);
   std::vector<uint32_t> xs;
-  qolh::xlate_schedule(nterms, xs, T.xsteps);
+  std::vector<uint32_t> xr;
+  qolh::xlate_schedule(nterms, QOL_MOM_THREADS, xs, T.xsteps, xr, T.xslots);
   T.xsched = C->up(xs);
+  T.xred = C->up(xr);
   std::vector<double> tgi((size_t)nquad * nquad, 0.0); /* Bjorck-Pereyra node-difference reciprocals */
   for (int k = 0; k + 1 < nquad; ++k)
     for (int i = k + 1; i < nquad; ++i) tgi[(size_t)k * nquad + i] = 1.0 / (tgl[i] - tgl[i - k - 1]);
   T.tginv = C->up(tgi);
-  if (!T.tgl || !T.Mb || !T.vruv || !T.xsched || !T.tginv) return fail(QOL_ERR_CUDA, "table upload failed");
+  if (!T.tgl || !T.Mb || !T.vruv || !T.xsched || !T.xred || !T.tginv)
+    return fail(QOL_ERR_CUDA, "table upload failed");
   *out = C.get();
   g_orders[key] = std::move(C);
   return 0;

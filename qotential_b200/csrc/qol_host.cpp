@@ -370,8 +370,9 @@ void build_ref(int korder, int order, int nlevel, bool sqmode, RefElem& R) {
   }
 }
 
-void xlate_schedule(int L, std::vector<uint32_t>& tab, int& steps) {
-  struct Out { int idx, cost; std::vector<uint32_t> terms; };
+void xlate_schedule(int L, int lanes, std::vector<uint32_t>& tab, int& steps, std::vector<uint32_t>& red,
+                    int& slots) {
+  struct Out { int idx; std::vector<uint32_t> terms; };
   std::vector<Out> outs;
   for (int n = 0; n < L; ++n)
     for (int k = 0; k <= n; ++k) {
@@ -383,32 +384,55 @@ void xlate_schedule(int L, std::vector<uint32_t>& tab, int& steps) {
           const int kr = k - mu, am = std::abs(mu), ar = std::abs(kr);
           const int neg = ((mu < 0 && (am & 1)) ? 1 : 0) ^ ((kr < 0 && (ar & 1)) ? 1 : 0);
           uint32_t w = (uint32_t)(lam * (lam + 1) / 2 + am) | ((uint32_t)(nu * (nu + 1) / 2 + ar) << 8) |
-                       ((uint32_t)o.idx << 16) | ((uint32_t)(mu < 0) << 24) | ((uint32_t)(kr < 0) << 25) |
-                       ((uint32_t)neg << 26) | (1u << 27);
+                       ((uint32_t)(mu < 0) << 26) | ((uint32_t)(kr < 0) << 27) | ((uint32_t)neg << 28) |
+                       (1u << 29);
           o.terms.push_back(w);
         }
       }
-      o.cost = (int)o.terms.size();
       outs.push_back(std::move(o));
     }
-  /* longest first; ties by output index, lanes by load then index */
-  std::vector<int> ord(outs.size());
+  /* pieces of at most P terms (P = total / lanes, at least 8), each with its
+   * own partial-sum slot; slots of an output are consecutive */
+  size_t total = 0;
+  for (const Out& o : outs) total += o.terms.size();
+  const int P = std::max<int>(8, (int)((total + lanes - 1) / lanes));
+  struct Piece { int slot, cost; std::vector<uint32_t> terms; };
+  std::vector<Piece> pieces;
+  red.assign(2 * outs.size(), 0u);
+  slots = 0;
+  for (const Out& o : outs) {
+    const int c = (int)o.terms.size(), k = (c + P - 1) / P;
+    red[2 * o.idx] = (uint32_t)slots;
+    red[2 * o.idx + 1] = (uint32_t)k;
+    for (int q = 0; q < k; ++q) {
+      const int lo = (int)((long long)c * q / k), hi = (int)((long long)c * (q + 1) / k);
+      Piece pc;
+      pc.slot = slots++;
+      pc.terms.assign(o.terms.begin() + lo, o.terms.begin() + hi);
+      for (uint32_t& w : pc.terms) w |= (uint32_t)pc.slot << 16;
+      pc.terms.back() |= 1u << 30; /* last term: flush to the slot */
+      pc.cost = hi - lo;
+      pieces.push_back(std::move(pc));
+    }
+  }
+  /* longest first; ties by slot, lanes by load then index */
+  std::vector<int> ord(pieces.size());
   for (size_t i = 0; i < ord.size(); ++i) ord[i] = (int)i;
-  std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return outs[a].cost > outs[b].cost; });
-  std::vector<std::vector<uint32_t>> lane(32);
-  std::vector<int> load(32, 0);
-  for (int oi : ord) {
+  std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return pieces[a].cost > pieces[b].cost; });
+  std::vector<std::vector<uint32_t>> lane(lanes);
+  std::vector<int> load(lanes, 0);
+  for (int pi : ord) {
     int best = 0;
-    for (int q = 1; q < 32; ++q)
+    for (int q = 1; q < lanes; ++q)
       if (load[q] < load[best]) best = q;
-    load[best] += outs[oi].cost;
-    lane[best].insert(lane[best].end(), outs[oi].terms.begin(), outs[oi].terms.end());
+    load[best] += pieces[pi].cost;
+    lane[best].insert(lane[best].end(), pieces[pi].terms.begin(), pieces[pi].terms.end());
   }
   steps = 0;
-  for (int q = 0; q < 32; ++q) steps = std::max(steps, load[q]);
-  tab.assign((size_t)steps * 32, 0u);
-  for (int q = 0; q < 32; ++q)
-    for (size_t s = 0; s < lane[q].size(); ++s) tab[s * 32 + q] = lane[q][s];
+  for (int q = 0; q < lanes; ++q) steps = std::max(steps, load[q]);
+  tab.assign((size_t)steps * lanes, 0u);
+  for (int q = 0; q < lanes; ++q)
+    for (size_t s2 = 0; s2 < lane[q].size(); ++s2) tab[s2 * lanes + q] = lane[q][s2];
 }
 
 } // namespace qolh

@@ -58,12 +58,16 @@ void build_ref(int korder, int order, int nlevel, bool sqmode, RefElem& R);
 /* ---------------- harmonic translation schedule ---------------- */
 /* Work list of the regular-solid-harmonic translation
  *   T_n^k = sum_{lam=0..n} sum_mu M_lam^mu R_{n-lam}^{k-mu}(x),  0 <= k <= n <= L-1,
- * spread over 32 lanes: the outputs (n,k) go to lanes by longest-processing-time
- * first, each lane runs its outputs' terms back to back.  tab[s*32 + lane] is
- * one term: bits 0-7 the M entry lam(lam+1)/2+|mu|, 8-15 the R entry
- * nu(nu+1)/2+|k-mu|, 16-23 the output n(n+1)/2+k, 24 conj M (mu < 0),
- * 25 conj R (k-mu < 0), 26 negate ((-1)^|mu| (-1)^|k-mu| = -1), 27 valid. */
-void xlate_schedule(int L, std::vector<uint32_t>& tab, int& steps);
+ * over `lanes` threads.  Each output's terms are cut into pieces of at most
+ * max(8, total/lanes) terms; every piece sums into its own partial slot (slots
+ * of one output consecutive: red[2o] first slot, red[2o+1] count, o =
+ * n(n+1)/2+k); pieces go to lanes longest first (ties by slot, lanes by load
+ * then index) and each lane runs its pieces back to back.  tab[s*lanes +
+ * lane] is one term: bits 0-7 the M entry lam(lam+1)/2+|mu|, 8-15 the R entry
+ * nu(nu+1)/2+|k-mu|, 16-25 the slot, 26 conj M (mu < 0), 27 conj R (k-mu < 0),
+ * 28 negate ((-1)^|mu| (-1)^|k-mu| = -1), 29 valid, 30 last term of its piece. */
+void xlate_schedule(int L, int lanes, std::vector<uint32_t>& tab, int& steps, std::vector<uint32_t>& red,
+                    int& slots);
 
 } // namespace qolh
 #endif

@@ -1098,35 +1098,46 @@ __global__ void __launch_bounds__(32 * RRQ_WARPS) k_rrq_geom(OrderTab T, PairIn 
  * a fraction of the arithmetic.
  * --------------------------------------------------------------------- */
 
-#define MOM_WARPS 2
-#define MOM_NC 8 /* boundary nodes per chunk */
+#define MOM_T QOL_MOM_THREADS /* threads per RRQ pair */
+#define MOM_NC 16 /* boundary nodes per chunk */
 #define MOM_CS (MOM_NC + 1)
 
 __host__ __device__ constexpr int mom_rows(int L) { return L * (L + 1); }
-/* doubles of shared memory per warp: line record (rounded to 2), then the
- * node chunk, later reused for M (7 rows: entries padded to 14 doubles), R(x) and T (6 rows) */
-__host__ __device__ constexpr int mom_region(int L) {
-  return mom_rows(L) * MOM_CS > 13 * mom_rows(L) + (L + 1) * (L + 2) ? mom_rows(L) * MOM_CS
-                                                                      : 13 * mom_rows(L) + (L + 1) * (L + 2);
+__host__ __device__ constexpr int mom_rec(int nbd) { return (6 * nbd + 4 + 1) & ~1; }
+/* doubles of shared memory of one pair after the line record: the node chunk,
+ * later M (entries 14 doubles apart), R(x), the translation's partial sums
+ * (12 per slot); T reuses M's space once the translation is done */
+__host__ __device__ constexpr int mom_region(int L, int slots) {
+  return mom_rows(L) * MOM_CS > 7 * mom_rows(L) + (L + 1) * (L + 2) + 12 * slots
+             ? mom_rows(L) * MOM_CS
+             : 7 * mom_rows(L) + (L + 1) * (L + 2) + 12 * slots;
 }
-__host__ __device__ constexpr int mom_warp_doubles(int L, int nbd) { return ((6 * nbd + 4 + 1) & ~1) + mom_region(L); }
 
+/* one CTA of MOM_T threads per RRQ pair.
+ * (A) R_lam^mu(rho_i), lam <= L-1, mu >= 0, chunks of MOM_NC nodes: thread
+ *     (g, j) evaluates node c0+j over the column pair (g, L-1-g) (L <= 16: at
+ *     most 8 pairs), the two columns as two recurrence chains in flight, into
+ *     ch[row][j], row = 2 entry(lam,mu) + re/im.
+ * (B) each thread contracts its rows e = tid + MOM_T r with the 6 weights.
+ * (C) R(x) up to degree L.
+ * (D) the translation, pieces of the term lists per thread (qolh::xlate_schedule),
+ *     partial sums per piece, then their fixed-order sum per output.
+ * (E) the moments of every h_{l,m}. */
 template <int LB>
-__global__ void __launch_bounds__(32 * MOM_WARPS) k_rrq_moments(OrderTab T, PairIn Q, PairWS G, RRQWS R) {
-  constexpr int RPL = (LB * (LB + 1) + 31) / 32; /* real rows of M per lane */
+__global__ void __launch_bounds__(MOM_T) k_rrq_moments(OrderTab T, PairIn Q, PairWS G, RRQWS R) {
+  constexpr int RPT = (LB * (LB + 1) + MOM_T - 1) / MOM_T; /* real rows of M per thread */
   extern __shared__ __align__(16) double mom_sm[];
   __shared__ double s_rq[(QOL_MAXL + 2) * (QOL_MAXL + 2)];
   __shared__ double s_rn[(QOL_MAXL + 2) * (QOL_MAXL + 2)];
   __shared__ double s_rd[QOL_MAXL + 2], s_ri[QOL_MAXL + 2];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (int e = threadIdx.x; e < (QOL_MAXL + 2) * (QOL_MAXL + 2); e += blockDim.x) {
+  const int tid = threadIdx.x;
+  for (int e = tid; e < (QOL_MAXL + 2) * (QOL_MAXL + 2); e += MOM_T) {
     s_rq[e] = c_rq[e / (QOL_MAXL + 2)][e % (QOL_MAXL + 2)];
     s_rn[e] = c_rn[e / (QOL_MAXL + 2)][e % (QOL_MAXL + 2)];
   }
-  for (int e = threadIdx.x; e < QOL_MAXL + 2; e += blockDim.x) { s_rd[e] = c_rd[e]; s_ri[e] = c_rinv[e]; }
-  __syncthreads();
-  const long long gidx = R.glo + (long long)blockIdx.x * MOM_WARPS + wid;
-  if (gidx >= R.ghi) return;
+  for (int e = tid; e < QOL_MAXL + 2; e += MOM_T) { s_rd[e] = c_rd[e]; s_ri[e] = c_rinv[e]; }
+  const long long gidx = R.glo + blockIdx.x;
+  if (gidx >= R.ghi) return; /* uniform over the CTA */
   const int2 pr = R.pair[gidx]; /* (panel, local target) */
   const int pan = pr.x, tl = pr.y;
   const long long p0 = Q.tcxi[pan] - 1;
@@ -1142,100 +1153,89 @@ __global__ void __launch_bounds__(32 * MOM_WARPS) k_rrq_moments(OrderTab T, Pair
     xt1 = alpha * (fr[1] * d0 + fr[4] * d1 + fr[7] * d2);
     xt2 = alpha * (fr[2] * d0 + fr[5] * d1 + fr[8] * d2);
   }
-  double* rec = mom_sm + (size_t)wid * mom_warp_doubles(L, nbd);
-  double* ch = rec + ((6 * nbd + 4 + 1) & ~1);
+  double* rec = mom_sm;
+  double* ch = rec + mom_rec(nbd);
   {
     const double* grec = R.line + (size_t)gidx * (6 * nbd + 4);
-    for (int e = lane; e < 6 * nbd + 4; e += 32) rec[e] = grec[e];
+    for (int e = tid; e < 6 * nbd + 4; e += MOM_T) rec[e] = grec[e];
   }
-  __syncwarp();
+  __syncthreads();
   const double* cD = rec;
   const double* cS = rec + 3 * nbd;
   const int NE = mom_rows(L);
-  /* (A) R_lam^mu(rho_i), lam <= L-1, mu >= 0, chunks of MOM_NC nodes: lane
-   * (g, j) evaluates node c0+j over the column pairs (p, L-1-p), p = g and
-   * g+4 (L <= 16: at most 8 pairs), the two columns of a pair as two
-   * recurrence chains in flight, into ch[row][j], row = 2 entry(lam,mu) + re/im.
-   * (B) each lane contracts its rows e = lane + 32 r with the 6 weights. */
-  double acc[RPL][6];
+  double acc[RPT][6];
 #pragma unroll
-  for (int r = 0; r < RPL; ++r)
+  for (int r = 0; r < RPT; ++r)
 #pragma unroll
     for (int c = 0; c < 6; ++c) acc[r][c] = 0.0;
-  int erow[RPL];
+  int erow[RPT];
 #pragma unroll
-  for (int r = 0; r < RPL; ++r) erow[r] = min(lane + 32 * r, NE - 1) * MOM_CS;
-  const int np = (L + 1) / 2, g4 = lane >> 3, jn = lane & 7;
-  const int pa = g4, pb = g4 + 4, qa = L - 1 - pa, qb = L - 1 - pb;
+  for (int r = 0; r < RPT; ++r) erow[r] = min(tid + MOM_T * r, NE - 1) * MOM_CS;
+  const int np = (L + 1) / 2, pa = tid >> 4, jn = tid & 15, qa = L - 1 - pa;
   for (int c0 = 0; c0 < nbd; c0 += MOM_NC) {
     if (pa < np) {
       const int i = min(c0 + jn, nbd - 1);
       const double Z = bx[3 * i] - xt0, X = bx[3 * i + 1] - xt1, Y = bx[3 * i + 2] - xt2;
       const double r2 = X * X + Y * Y + Z * Z;
-      /* diagonal R_m^m up to column qa, keeping columns pa, pb, qb, qa */
-      double dr = 1.0, di = 0.0;
-      double a1r = 1.0, a1i = 0.0, b1r = 1.0, b1i = 0.0, b2r = 1.0, b2i = 0.0;
+      /* diagonal R_m^m up to column qa, keeping column pa */
+      double dr = 1.0, di = 0.0, a1r = 1.0, a1i = 0.0;
       for (int mm = 1; mm <= qa; ++mm) {
         const double t = dr * X - di * Y;
         di = (dr * Y + di * X) * s_rd[mm];
         dr = t * s_rd[mm];
         if (mm == pa) { a1r = dr; a1i = di; }
-        if (mm == pb) { b1r = dr; b1i = di; }
-        if (mm == qb) { b2r = dr; b2i = di; }
       }
-      auto pair = [&](int c1, double d1r, double d1i, int c2, double d2r, double d2i) {
-        const int n1 = L - c1, n2 = c2 > c1 ? L - c2 : 0;
-        double ur = d1r, ui = d1i, vr = 0.0, vi = 0.0; /* column c1: R_{l}, R_{l-1} */
-        double sr = d2r, si = d2i, tr = 0.0, ti = 0.0; /* column c2 */
-        for (int e = 0; e < n1; ++e) {
-          if (e > 0) {
-            const int l = c1 + e;
-            const double q = s_rq[l * (QOL_MAXL + 2) + c1], a = (2.0 * l - 1.0) * Z;
-            const double nr = (a * ur - r2 * vr) * q, ni = (a * ui - r2 * vi) * q;
-            vr = ur; vi = ui; ur = nr; ui = ni;
-          }
-          const int row = (c1 + e) * (c1 + e + 1) + 2 * c1;
-          ch[row * MOM_CS + jn] = ur;
-          ch[(row + 1) * MOM_CS + jn] = ui;
-          if (e < n2) {
-            if (e > 0) {
-              const int l = c2 + e;
-              const double q = s_rq[l * (QOL_MAXL + 2) + c2], a = (2.0 * l - 1.0) * Z;
-              const double nr = (a * sr - r2 * tr) * q, ni = (a * si - r2 * ti) * q;
-              tr = sr; ti = si; sr = nr; si = ni;
-            }
-            const int row2 = (c2 + e) * (c2 + e + 1) + 2 * c2;
-            ch[row2 * MOM_CS + jn] = sr;
-            ch[(row2 + 1) * MOM_CS + jn] = si;
-          }
+      /* columns pa (L-pa entries) and qa (L-qa entries, none when qa == pa) */
+      const int n1 = L - pa, n2 = qa > pa ? L - qa : 0;
+      double ur = a1r, ui = a1i, vr = 0.0, vi = 0.0;
+      double sr = dr, si = di, tr = 0.0, ti = 0.0;
+      for (int e = 0; e < n1; ++e) {
+        if (e > 0) {
+          const int l = pa + e;
+          const double q = s_rq[l * (QOL_MAXL + 2) + pa], a = (2.0 * l - 1.0) * Z;
+          const double nr = (a * ur - r2 * vr) * q, ni = (a * ui - r2 * vi) * q;
+          vr = ur; vi = ui; ur = nr; ui = ni;
         }
-      };
-      pair(pa, a1r, a1i, qa, dr, di);
-      if (pb < np) pair(pb, b1r, b1i, qb, b2r, b2i);
+        const int row = (pa + e) * (pa + e + 1) + 2 * pa;
+        ch[row * MOM_CS + jn] = ur;
+        ch[(row + 1) * MOM_CS + jn] = ui;
+        if (e < n2) {
+          if (e > 0) {
+            const int l = qa + e;
+            const double q = s_rq[l * (QOL_MAXL + 2) + qa], a = (2.0 * l - 1.0) * Z;
+            const double nr = (a * sr - r2 * tr) * q, ni = (a * si - r2 * ti) * q;
+            tr = sr; ti = si; sr = nr; si = ni;
+          }
+          const int row2 = (qa + e) * (qa + e + 1) + 2 * qa;
+          ch[row2 * MOM_CS + jn] = sr;
+          ch[(row2 + 1) * MOM_CS + jn] = si;
+        }
+      }
     }
-    __syncwarp();
+    __syncthreads();
     const int nj = min(MOM_NC, nbd - c0);
     for (int jj = 0; jj < nj; ++jj) {
       const int ii = c0 + jj;
       const double w0 = cD[3 * ii], w1 = cD[3 * ii + 1], w2 = cD[3 * ii + 2];
       const double w3 = cS[3 * ii], w4 = cS[3 * ii + 1], w5 = cS[3 * ii + 2];
 #pragma unroll
-      for (int r = 0; r < RPL; ++r) {
+      for (int r = 0; r < RPT; ++r) {
         const double v = ch[erow[r] + jj];
         acc[r][0] += v * w0; acc[r][1] += v * w1; acc[r][2] += v * w2;
         acc[r][3] += v * w3; acc[r][4] += v * w4; acc[r][5] += v * w5;
       }
     }
-    __syncwarp();
+    __syncthreads();
   }
-  /* M[entry][6 components][re,im] with the 1/lam (D) and 1/(lam+1) (S)
-   * segment weights; then R(x) up to degree L; then T */
+  /* M[entry][6 components][re,im] (entries 14 doubles apart) with the 1/lam
+   * (D) and 1/(lam+1) (S) segment weights; then R(x) up to degree L */
   double* Mt = ch;
-  double* Rx = ch + 7 * NE; /* M entries 14 doubles apart: double2 gathers spread over all bank slots */
-  double* Tt = Rx + (L + 1) * (L + 2);
+  double* Rx = ch + 7 * NE;
+  double* Pp = Rx + (L + 1) * (L + 2);
+  double* Tt = ch; /* after the translation */
 #pragma unroll
-  for (int r = 0; r < RPL; ++r) {
-    const int e = lane + 32 * r;
+  for (int r = 0; r < RPT; ++r) {
+    const int e = tid + MOM_T * r;
     if (e < NE) {
       const int ent = e >> 1, ri = e & 1;
       int lam = 0;
@@ -1246,8 +1246,8 @@ __global__ void __launch_bounds__(32 * MOM_WARPS) k_rrq_moments(OrderTab T, Pair
       dst[6] = acc[r][3] * wS; dst[8] = acc[r][4] * wS; dst[10] = acc[r][5] * wS;
     }
   }
-  if (lane <= L) { /* column m = lane of R(x) */
-    const int m = lane;
+  if (tid <= L) { /* column m = tid of R(x) */
+    const int m = tid;
     const double Z = xt0, X = xt1, Y = xt2, r2 = X * X + Y * Y + Z * Z;
     double dr = 1.0, di = 0.0;
     for (int mm = 1; mm <= m; ++mm) {
@@ -1266,35 +1266,26 @@ __global__ void __launch_bounds__(32 * MOM_WARPS) k_rrq_moments(OrderTab T, Pair
       Rx[2 * ent] = ar; Rx[2 * ent + 1] = ai;
     }
   }
-  __syncwarp();
-  /* (D) translation: this lane's terms of the schedule, its outputs one
-   * after the other (each output belongs to one lane) */
+  __syncthreads();
+  /* (D) this thread's pieces of the translation, each flushed to its slot */
   {
     double a[12];
 #pragma unroll
     for (int c = 0; c < 12; ++c) a[c] = 0.0;
-    int cur = -1;
-    const unsigned* tab = T.xsched + lane;
+    const unsigned* tab = T.xsched + tid;
     const int nst = T.xsteps;
     unsigned wn = nst > 0 ? __ldg(tab) : 0u;
     for (int s = 0; s < nst; ++s) {
       const unsigned w = wn;
-      if (s + 1 < nst) wn = __ldg(tab + 32 * (s + 1));
-      if (!(w & (1u << 27))) break; /* a lane's terms are contiguous from step 0 */
-      const int em = w & 255, ex = (w >> 8) & 255, out = (w >> 16) & 255;
-      if (out != cur) {
-        if (cur >= 0) {
-#pragma unroll
-          for (int c = 0; c < 12; ++c) { Tt[cur * 12 + c] = a[c]; a[c] = 0.0; }
-        }
-        cur = out;
-      }
+      if (s + 1 < nst) wn = __ldg(tab + MOM_T * (s + 1));
+      if (!(w & (1u << 29))) break; /* a thread's terms are contiguous from step 0 */
+      const int em = w & 255, ex = (w >> 8) & 255;
       const double2 rv = *reinterpret_cast<const double2*>(Rx + 2 * ex);
       double c = rv.x, d = rv.y;
-      if (w & (1u << 26)) { c = -c; d = -d; }
-      if (w & (1u << 25)) d = -d;
+      if (w & (1u << 28)) { c = -c; d = -d; }
+      if (w & (1u << 27)) d = -d;
       double p = d, q = c;
-      if (w & (1u << 24)) { p = -d; q = -c; }
+      if (w & (1u << 26)) { p = -d; q = -c; }
       const double2* mv = reinterpret_cast<const double2*>(Mt + em * 14);
 #pragma unroll
       for (int k = 0; k < 6; ++k) {
@@ -1302,13 +1293,26 @@ __global__ void __launch_bounds__(32 * MOM_WARPS) k_rrq_moments(OrderTab T, Pair
         a[2 * k] += v.x * c - v.y * p;
         a[2 * k + 1] += v.y * q + v.x * d;
       }
-    }
-    if (cur >= 0) {
+      if (w & (1u << 30)) {
+        double* dst = Pp + 12 * ((w >> 16) & 1023);
 #pragma unroll
-      for (int c = 0; c < 12; ++c) Tt[cur * 12 + c] = a[c];
+        for (int c2 = 0; c2 < 12; ++c2) { dst[c2] = a[c2]; a[c2] = 0.0; }
+      }
     }
   }
-  __syncwarp();
+  __syncthreads();
+  for (int o = tid; o < NE / 2; o += MOM_T) { /* T_o = sum of its pieces, in slot order */
+    const int ps = (int)T.xred[2 * o], npc = (int)T.xred[2 * o + 1];
+    double t[12];
+#pragma unroll
+    for (int c = 0; c < 12; ++c) t[c] = Pp[12 * ps + c];
+    for (int q = 1; q < npc; ++q)
+#pragma unroll
+      for (int c = 0; c < 12; ++c) t[c] += Pp[12 * (ps + q) + c];
+#pragma unroll
+    for (int c = 0; c < 12; ++c) Tt[12 * o + c] = t[c];
+  }
+  __syncthreads();
   /* (E) the moments of h_{l,m}: T of degree l-1 at orders m-1, m, m+1, and
    * the x point: (s0, lint/4pi) (x) (0, grad h(x)) and h(x) Omega/4pi */
   const double i4p = 1.0 / (4.0 * QOL_PI);
@@ -1317,7 +1321,7 @@ __global__ void __launch_bounds__(32 * MOM_WARPS) k_rrq_moments(OrderTab T, Pair
   const double wv0 = lint0 * i4p, wv1 = lint1 * i4p, wv2 = lint2 * i4p;
   double* JD = R.JD + (size_t)gidx * 4 * hd;
   double* RS = R.RS + (size_t)gidx * hd;
-  for (int k = lane; k < hd; k += 32) {
+  for (int k = tid; k < hd; k += MOM_T) {
     int l = 1;
     while ((l + 1) * l / 2 <= k) ++l;
     const int m = k - l * (l - 1) / 2 + 1, n = l - 1;
@@ -1644,11 +1648,10 @@ cudaError_t qol_launch_rrq_moments(const OrderTab& T, const PairIn& Q, const Pai
                                    cudaStream_t st) {
   const long long n = R.ghi - R.glo;
   if (n <= 0) return cudaSuccess;
-  const unsigned nbm = (unsigned)((n + MOM_WARPS - 1) / MOM_WARPS);
-  const size_t smem = sizeof(double) * MOM_WARPS * mom_warp_doubles(T.nterms, 3 * T.nquad);
+  const size_t smem = sizeof(double) * (mom_rec(3 * T.nquad) + mom_region(T.nterms, T.xslots));
   auto go = [&](auto kern) {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    kern<<<nbm, 32 * MOM_WARPS, smem, st>>>(T, Q, G, R);
+    kern<<<(unsigned)n, MOM_T, smem, st>>>(T, Q, G, R);
   };
   if (T.nterms <= 4) go(k_rrq_moments<4>);
   else if (T.nterms <= 6) go(k_rrq_moments<6>);

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #define RRQ_FRAME 16 /* R (9, rows e1,e2,e3 as R[i + 3*d]), c (3), alpha (1), pad */
+#define QOL_MOM_THREADS 128 /* threads per RRQ pair in k_rrq_moments (lanes of its translation schedule) */
 
 /* per-order tables (reference element, quadrature data), device pointers */
 struct OrderTab {
@@ -18,7 +19,9 @@ struct OrderTab {
   const double* Mb;    /* (3 nquad + 3) x hd, row-major: boundary + vertex interpolation */
   const double* umatr; /* hd x hd col-major (vals -> coefs) */
   const double* vruv;  /* 2 x hd VR nodes of degree korder */
-  const unsigned* xsched; /* xsteps x 32 translation terms (qolh::xlate_schedule) */
+  const unsigned* xsched; /* xsteps x QOL_MOM_THREADS translation terms (qolh::xlate_schedule) */
+  const unsigned* xred;   /* per translation output: first partial slot, slot count */
+  int xslots;
   const double* tginv;    /* nquad x nquad: 1/(tgl[i] - tgl[i-k-1]) at [k*nquad + i] */
   int xsteps;
 };

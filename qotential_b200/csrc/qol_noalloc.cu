@@ -147,9 +147,10 @@ int na_tables(NoAllocDev& D, int nterms, int orderff, int nquad, cudaStream_t st
   size_t o_tq = put(tq.data(), 8 * tq.size()), o_wq = put(wq.data(), 8 * wq.size());
   size_t o_Mb = put(Mb.data(), 8 * Mb.size()), o_um = put(um.data(), 8 * um.size());
   size_t o_vr = put(vr.data(), 8 * vr.size());
-  std::vector<uint32_t> xs;
-  qolh::xlate_schedule(nterms, xs, T.xsteps);
+  std::vector<uint32_t> xs, xr;
+  qolh::xlate_schedule(nterms, QOL_MOM_THREADS, xs, T.xsteps, xr, T.xslots);
   size_t o_xs = put(xs.data(), sizeof(uint32_t) * xs.size());
+  size_t o_xr = put(xr.data(), sizeof(uint32_t) * xr.size());
   std::vector<double> tgi((size_t)nquad * nquad, 0.0); /* Bjorck-Pereyra node-difference reciprocals */
   for (int k = 0; k + 1 < nquad; ++k)
     for (int i = k + 1; i < nquad; ++i) tgi[(size_t)k * nquad + i] = 1.0 / (tgl[i] - tgl[i - k - 1]);
@@ -173,6 +174,7 @@ int na_tables(NoAllocDev& D, int nterms, int orderff, int nquad, cudaStream_t st
   T.tq = (const double*)dp(o_tq); T.wq = (const double*)dp(o_wq);
   T.Mb = (const double*)dp(o_Mb); T.umatr = (const double*)dp(o_um); T.vruv = (const double*)dp(o_vr);
   T.xsched = (const unsigned*)dp(o_xs);
+  T.xred = (const unsigned*)dp(o_xr);
   T.tginv = (const double*)dp(o_tgi);
   D.T = T;
   D.table_bytes = bytes;
