@@ -447,7 +447,8 @@ __host__ __device__ constexpr int panel_maxr(int hd, int CS, int NT) {
 /* doubles of shared memory of one CTA: setup copies of the matrix columns,
  * staging buffers, geometry, pivot bookkeeping, the scaled pivot rows */
 __host__ __device__ constexpr size_t panel_smem_doubles(int hd, int nbd, int CS) {
-  return (size_t)5 * hd * panel_ncol(hd, CS) + 13 * (size_t)hd + 3 * (size_t)(nbd + 3) + 16 +
+  return (size_t)4 * hd * panel_ncol(hd, CS) + (((size_t)hd * panel_ncol(hd, CS) + 1) & ~(size_t)1) +
+         2 * (((size_t)5 * hd + 1) & ~(size_t)1) + 3 * (size_t)hd + 3 * (size_t)(nbd + 3) + 16 +
          5 * (size_t)panel_ncol(hd, CS) + 8 + (8 * (size_t)hd + 1) / 2 + 2;
 }
 
@@ -477,8 +478,9 @@ __global__ void __launch_bounds__(NT, 1) k_rrq_panel(OrderTab T, PanelIn P, Pair
   extern __shared__ __align__(16) double psm[];
   double* Vs = psm;                        /* hd x ncol quaternions (setup) */
   double* Ms = Vs + (size_t)4 * hd * ncol; /* hd x ncol (setup) */
-  double* stg = Ms + (size_t)hd * ncol;    /* 2 buffers x (4 hd quaternion column + hd real column) */
-  double* s_sx = stg + 10 * hd;            /* 3 hd */
+  const int SB = (5 * hd + 1) & ~1;       /* staging buffer stride (even: double2 copies) */
+  double* stg = Ms + (((size_t)hd * ncol + 1) & ~(size_t)1); /* 2 buffers x (4 hd quaternion column + hd real column) */
+  double* s_sx = stg + 2 * SB;             /* 3 hd */
   double* s_raw = s_sx + 3 * hd;           /* 3 (nbd + 3) */
   double* s_fr = s_raw + 3 * (nbd + 3);    /* 16 */
   double* rowq = s_fr + 16;                /* 4 ncol: scaled pivot row of V */
@@ -494,13 +496,13 @@ __global__ void __launch_bounds__(NT, 1) k_rrq_panel(OrderTab T, PanelIn P, Pair
   auto pushq = [&](int buf, int row, const double* q) {
 #pragma unroll
     for (int r = 0; r < CS; ++r) {
-      double* d = stgr[r] + buf * 5 * hd + 4 * row;
+      double* d = stgr[r] + buf * SB + 4 * row;
       d[0] = q[0]; d[1] = q[1]; d[2] = q[2]; d[3] = q[3];
     }
   };
   auto pushr = [&](int buf, int row, double v) {
 #pragma unroll
-    for (int r = 0; r < CS; ++r) stgr[r][buf * 5 * hd + 4 * hd + row] = v;
+    for (int r = 0; r < CS; ++r) stgr[r][buf * SB + 4 * hd + row] = v;
   };
   double* H = R.hmat + (size_t)pan * hd * hd; /* H[j*hd+k] = h_k(y_j) */
   for (int e = threadIdx.x; e < 3 * hd; e += blockDim.x) s_sx[e] = P.sx[(size_t)pan * hd * 3 + e];
@@ -637,7 +639,7 @@ __global__ void __launch_bounds__(NT, 1) k_rrq_panel(OrderTab T, PanelIn P, Pair
   double* s_pv = rowr + ncol; /* 8: pivot inverse (4), real pivot inverse, pivot rows (as doubles) */
   for (int k = 0; k < hd; ++k) {
     const int b = k & 1;
-    double* cq = stg + b * 5 * hd;
+    double* cq = stg + b * SB;
     double* cr = cq + 4 * hd;
     /* warp 0: pivots among the unused rows, their inverses; the pivot rows'
      * multipliers in this CTA's staging copy become 0 (the elimination then
@@ -736,12 +738,29 @@ __global__ void __launch_bounds__(NT, 1) k_rrq_panel(OrderTab T, PanelIn P, Pair
         q[r][3] -= f0 * r3 + f1 * r2 - f2 * r1 + f3 * r0;
         mv[r] -= cr[i] * rr;
       }
-      if (gc == k + 1) /* the next pivot column, to every CTA's other staging buffer */
+      if (gc == k + 1) { /* the next pivot column, into this CTA's other staging buffer */
+        double* nb = stg + (b ^ 1) * SB;
 #pragma unroll
         for (int r = 0; r < MAXR; ++r) {
           const int i = trg + RG * r;
-          if (i < hd) { pushq(b ^ 1, i, q[r]); pushr(b ^ 1, i, mv[r]); }
+          if (i < hd) {
+            nb[4 * i] = q[r][0]; nb[4 * i + 1] = q[r][1]; nb[4 * i + 2] = q[r][2]; nb[4 * i + 3] = q[r][3];
+            nb[4 * hd + i] = mv[r];
+          }
         }
+      }
+    }
+    if (CS > 1 && k + 1 < hd) { /* and from there to the other CTAs, coalesced */
+      __syncthreads();
+      if ((k + 1) / ncol == rank) {
+        const double2* src = reinterpret_cast<const double2*>(stg + (b ^ 1) * SB);
+        const int nv = SB / 2;
+        for (int e = threadIdx.x; e < (CS - 1) * nv; e += NT) {
+          const int pr = e / nv, v = e % nv;
+          const int peer = pr < rank ? pr : pr + 1;
+          reinterpret_cast<double2*>(stgr[peer] + (b ^ 1) * SB)[v] = src[v];
+        }
+      }
     }
     cl.sync();
   }
@@ -767,13 +786,48 @@ __global__ void __launch_bounds__(NT, 1) k_rrq_panel(OrderTab T, PanelIn P, Pair
   }
   __threadfence();
   cl.sync();
-  /* B = PS H^T, rows c0..c1: B[i][j] = sum_k PS[i][k] h_k(y_j) */
-  double* B = R.B + (size_t)pan * hd * hd;
-  for (int e = threadIdx.x; e < nc * hd; e += blockDim.x) {
-    const int i = c0 + e / hd, j = e % hd;
-    double s = 0.0;
-    for (int k = 0; k < hd; ++k) s += PS[(size_t)i * hd + k] * H[(size_t)j * hd + k];
-    B[(size_t)i * hd + j] = s;
+  /* B = PS H^T, rows c0..c1: B[i][j] = sum_k PS[i][k] h_k(y_j), K tiles of PS
+   * and H staged in the space of the matrix copies (free now) */
+  {
+    double* B = R.B + (size_t)pan * hd * hd;
+    const int room = 5 * hd * ncol;
+    int KT = 32;
+    while (KT > 4 && (ncol + hd) * (KT + 1) > room) KT >>= 1;
+    const int ks = KT + 1; /* odd stride: consecutive j hit distinct banks */
+    double* sP = psm;
+    double* sH = psm + (size_t)ncol * ks;
+    constexpr int MAXB = 12;
+    double bacc[MAXB];
+#pragma unroll
+    for (int u = 0; u < MAXB; ++u) bacc[u] = 0.0;
+    for (int k0 = 0; k0 < hd; k0 += KT) {
+      __syncthreads();
+      for (int e = threadIdx.x; e < nc * KT; e += NT) {
+        const int i = e / KT, kk = e % KT;
+        sP[i * ks + kk] = k0 + kk < hd ? PS[(size_t)(c0 + i) * hd + k0 + kk] : 0.0;
+      }
+      for (int e = threadIdx.x; e < hd * KT; e += NT) {
+        const int j = e / KT, kk = e % KT;
+        sH[j * ks + kk] = k0 + kk < hd ? H[(size_t)j * hd + k0 + kk] : 0.0;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int u = 0; u < MAXB; ++u) {
+        const int e = threadIdx.x + NT * u;
+        if (e < nc * hd) {
+          const double* pp = sP + (e / hd) * ks;
+          const double* hh = sH + (e % hd) * ks;
+          double sacc = bacc[u];
+          for (int kk = 0; kk < KT; ++kk) sacc += pp[kk] * hh[kk];
+          bacc[u] = sacc;
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < MAXB; ++u) {
+      const int e = threadIdx.x + NT * u;
+      if (e < nc * hd) B[(size_t)(c0 + e / hd) * hd + e % hd] = bacc[u];
+    }
   }
 }
 
