@@ -135,6 +135,24 @@ int qol_rrq_noalloc(qol_int m, const double* tx, qol_int n, const double* sx, co
                     qol_int orderff, double distff, qol_int exterior, double* As, double* Ad, void* stream);
 const char* qol_noalloc_last_error(void);
 
+/* GRF near phase of the reference's stellarator driver
+ * (web/stellarator/fortran/stellarator_grf_core_mod.f90:652-899): for the
+ * surface's own nodes as targets, the ball lists (1.75 sqrt(panel area) about
+ * the panel's node mean, :652-693), the RRQ corrections minus the naive block
+ * of every near pair, contracted per pair with the density (ubn, ub) (:860-875)
+ * and added into u (nsrc, inout) in panel order (:892-896).  xbuf (nullable):
+ * per panel the 3 x (3 nquad + 3) chart boundary (ichart = 1).  nnear: near
+ * pairs; level_hist (nullable, 6): pairs per resolving level (5 = RRQ).
+ * No qol_* counterpart in the reference (its GRF driver calls rrq_r64 itself). */
+int qol_grf_near(qol_int npan, qol_int nterms, qol_int nquad, qol_int orderff, double distff, qol_int iside,
+                 qol_int nsrc, const double* sx, const double* snx, const double* sw, const double* rts,
+                 const double* rps, const double* xbuf, const double* ub, const double* ubn, double* u,
+                 qol_int* nnear, qol_int* level_hist, double* timeinfo);
+/* Direct far field of the same driver (stellarator_grf_core_mod.f90:566-606):
+ * u_i = sum_j S_ij ubn_j - D_ij ub_j over all nodes, zero self term. */
+int qol_direct_farfield(qol_int nsrc, const double* sx, const double* snx, const double* sw, const double* ub,
+                        const double* ubn, double* u);
+
 /* Library status and diagnostics.  qol_kernel_times: when enabled, every
  * pipeline call records CUDA events on its stream around its phases and
  * accumulates the device milliseconds of its QOL_NPHASE phases: [0] refined

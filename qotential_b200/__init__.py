@@ -15,7 +15,7 @@ import numpy as np
 __all__ = [
     "lib", "QolError", "qol_simplex_precomp", "qol_build_patch_levels", "qol_lap3dsdlpmat_levels",
     "qol_clear_patch_levels", "qol_clear_patch_levels_all", "qol_rrq", "qol_getnearquad_lap_rrq",
-    "qol_getnearquad_lap_rrq_dev",
+    "qol_getnearquad_lap_rrq_dev", "qol_grf_near", "qol_direct_farfield",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -191,3 +191,38 @@ def qol_getnearquad_lap_rrq_dev(npan, nterms, nquad, sx, snx, sw, rts, rps, tcx,
         _vp(hist) if want_hist else None)
     _check(rc)
     return hist if want_hist else None
+
+
+def qol_grf_near(npan, nterms, nquad, sx, snx, sw, rts, rps, ub, ubn, u=None, orderff=None, distff=1.4,
+                 iside=30, xbuf=None, timeinfo=None):
+    """GRF near phase of the reference's stellarator driver
+    (stellarator_grf_core_mod.f90:652-899): returns (u + near corrections,
+    number of near pairs, pairs per resolving level [6]).  Targets are the
+    surface's own nodes; ``u`` (default zeros) is added to, as the driver
+    adds the near phase to its far field."""
+    hd = nterms * (nterms + 1) // 2
+    nsrc = npan * hd
+    orderff = nquad if orderff is None else orderff
+    uu = np.zeros(nsrc) if u is None else _f(u, nsrc).copy()
+    nn = np.zeros(1, np.int64)
+    hist = np.zeros(6, np.int64)
+    ti = np.zeros(20) if timeinfo is None else _f(timeinfo, 20).copy()
+    xb = None if xbuf is None else np.ascontiguousarray(np.asarray(xbuf, np.float64).ravel())
+    rc = lib().qol_grf_near(i64(npan), i64(nterms), i64(nquad), i64(orderff), C.c_double(distff), i64(iside),
+                            i64(nsrc), _vp(_f(sx, 3 * nsrc)), _vp(_f(snx, 3 * nsrc)), _vp(_f(sw, nsrc)),
+                            _vp(_f(rts, 3 * nsrc)), _vp(_f(rps, 3 * nsrc)), _vp(xb), _vp(_f(ub, nsrc)),
+                            _vp(_f(ubn, nsrc)), _vp(uu), _vp(nn), _vp(hist), _vp(ti))
+    _check(rc)
+    return uu, int(nn[0]), hist
+
+
+def qol_direct_farfield(sx, snx, sw, ub, ubn):
+    """Direct far field u_i = sum_j S_ij ubn_j - D_ij ub_j, zero self term
+    (stellarator_grf_core_mod.f90:566-606)."""
+    sw = _f(sw)
+    nsrc = sw.size
+    u = np.zeros(nsrc)
+    rc = lib().qol_direct_farfield(i64(nsrc), _vp(_f(sx, 3 * nsrc)), _vp(_f(snx, 3 * nsrc)), _vp(sw),
+                                   _vp(_f(ub, nsrc)), _vp(_f(ubn, nsrc)), _vp(u))
+    _check(rc)
+    return u

@@ -91,7 +91,7 @@ struct OrderCache {
 
 std::map<long long, std::unique_ptr<OrderCache>> g_orders;
 bool g_coefs_uploaded = false;
-Arena g_arena, g_arena2, g_arena_io; /* pipeline, per-pair RRQ storage, host-entry buffers */
+Arena g_arena, g_arena2, g_arena_io, g_arena_grf; /* pipeline, per-pair RRQ storage, host-entry buffers, GRF */
 /* per-phase device milliseconds of the pipeline (diagnostics) */
 int g_ktime_on = 0;
 double g_ktime[QOL_NPHASE] = {};
@@ -1002,6 +1002,118 @@ int qol_last_host_times(double* ms7) {
   std::lock_guard<std::recursive_mutex> g(g_mu);
   if (!ms7) return fail(QOL_ERR_ARG, "null argument");
   for (int i = 0; i < 7; ++i) ms7[i] = g_host_ms[i];
+  return 0;
+}
+
+/* GRF near phase (stellarator_grf_core_mod.f90:652-899): ball lists of the
+ * surface's own nodes, the RRQ corrections of every near pair, contracted with
+ * the density (ubn, ub) and scattered into u in panel order. */
+int qol_grf_near(qol_int npan, qol_int nterms, qol_int nquad, qol_int orderff, double distff, qol_int iside,
+                 qol_int nsrc, const double* sx, const double* snx, const double* sw, const double* rts,
+                 const double* rps, const double* xbuf, const double* ub, const double* ubn, double* u,
+                 qol_int* nnear, qol_int* level_hist, double* timeinfo) {
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  const qol_int hd = nterms * (nterms + 1) / 2;
+  if (!sx || !snx || !sw || !rts || !rps || !ub || !ubn || !u) return fail(QOL_ERR_ARG, "null argument");
+  if (npan < 0 || nsrc != npan * hd) return fail(QOL_ERR_LAYOUT, "the panel order, npan and nsrc are inconsistent");
+  int rc = ensure_device();
+  if (rc) return rc;
+  if (nnear) *nnear = 0;
+  if (level_hist) for (int i = 0; i < 6; ++i) level_hist[i] = 0;
+  if (npan == 0) return 0;
+  cudaStream_t st = g_stream;
+  const int nbd = 3 * (int)nquad;
+  size_t need = sizeof(double) * (size_t)(16 * nsrc + 4 * npan + (xbuf ? 3 * (nbd + 3) * npan : 0)) +
+                sizeof(long long) * (size_t)(3 * npan + 3) + 16 * 256;
+  if ((rc = g_arena_io.reserve(need))) return rc;
+  g_arena_io.reset();
+  double* dsx = g_arena_io.take<double>(3 * nsrc);
+  double* dsnx = g_arena_io.take<double>(3 * nsrc);
+  double* dsw = g_arena_io.take<double>(nsrc);
+  double* drts = g_arena_io.take<double>(3 * nsrc);
+  double* drps = g_arena_io.take<double>(3 * nsrc);
+  double* dub = g_arena_io.take<double>(nsrc);
+  double* dubn = g_arena_io.take<double>(nsrc);
+  double* du = g_arena_io.take<double>(nsrc);
+  double* dball = g_arena_io.take<double>(4 * npan);
+  double* dchart = xbuf ? g_arena_io.take<double>((size_t)3 * (nbd + 3) * npan) : nullptr;
+  long long* dcnt = g_arena_io.take<long long>(npan);
+  long long* doff = g_arena_io.take<long long>(npan + 1); /* 0-based offsets */
+  long long* dxi = g_arena_io.take<long long>(npan + 1);  /* 1-based, the pipeline's tcxi */
+  CK(cudaMemcpyAsync(dsx, sx, sizeof(double) * 3 * nsrc, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dsnx, snx, sizeof(double) * 3 * nsrc, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dsw, sw, sizeof(double) * nsrc, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(drts, rts, sizeof(double) * 3 * nsrc, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(drps, rps, sizeof(double) * 3 * nsrc, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dub, ub, sizeof(double) * nsrc, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dubn, ubn, sizeof(double) * nsrc, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(du, u, sizeof(double) * nsrc, cudaMemcpyHostToDevice, st));
+  if (xbuf) CK(cudaMemcpyAsync(dchart, xbuf, sizeof(double) * 3 * (nbd + 3) * npan, cudaMemcpyHostToDevice, st));
+  CK(qol_launch_grf_balls((int)npan, (int)hd, nsrc, dsx, dsw, dball, dcnt, st));
+  std::vector<long long> cnt(npan), off(npan + 1), xi(npan + 1);
+  CK(cudaMemcpyAsync(cnt.data(), dcnt, sizeof(long long) * npan, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  off[0] = 0;
+  for (qol_int k = 0; k < npan; ++k) off[k + 1] = off[k] + cnt[k];
+  for (qol_int k = 0; k <= npan; ++k) xi[k] = off[k] + 1;
+  const long long nn = off[npan];
+  if (nnear) *nnear = nn;
+  CK(cudaMemcpyAsync(doff, off.data(), sizeof(long long) * (npan + 1), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dxi, xi.data(), sizeof(long long) * (npan + 1), cudaMemcpyHostToDevice, st));
+  if (nn > 0) {
+    need = sizeof(double) * (size_t)nn * (3 + 1 + 2 * hd) + sizeof(long long) * (size_t)nn + 8 * 256;
+    if ((rc = g_arena_grf.reserve(need))) return rc;
+    g_arena_grf.reset();
+    long long* didx = g_arena_grf.take<long long>(nn);
+    double* dtcx = g_arena_grf.take<double>(3 * nn);
+    double* dval = g_arena_grf.take<double>(nn);
+    double* dvs = g_arena_grf.take<double>((size_t)nn * hd);
+    double* dvd = g_arena_grf.take<double>((size_t)nn * hd);
+    CK(qol_launch_grf_csr((int)npan, nsrc, dsx, dball, doff, didx, dtcx, st));
+    Job J{};
+    J.npan = (int)npan; J.nterms = (int)nterms; J.nquad = (int)nquad; J.orderff = (int)orderff;
+    J.exterior = (iside % 10) == 0; J.subtract_naive = 1; J.distff = distff; J.ntcx = nn;
+    J.P = PanelIn{dsx, dsnx, dsw, drts, drps};
+    J.Q = PairIn{dtcx, didx, dxi};
+    J.vs = dvs; J.vd = dvd; J.si = nullptr; J.sj = nullptr;
+    J.chart = dchart;
+    long long hist[6] = {0, 0, 0, 0, 0, 0};
+    if ((rc = run_pipeline(J, st, timeinfo, hist, nullptr, nullptr))) return rc;
+    if (level_hist) for (int i = 0; i < 6; ++i) level_hist[i] = hist[i];
+    CK(qol_launch_grf_apply((int)npan, (int)hd, nsrc, dsx, dball, doff, didx, dvs, dvd, dub, dubn, dval, du, st));
+  }
+  CK(cudaMemcpyAsync(u, du, sizeof(double) * nsrc, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return 0;
+}
+
+/* the blocked Direct far field u_i = sum_j S_ij ubn_j - D_ij ub_j with zero
+ * self term (stellarator_grf_core_mod.f90:566-606) */
+int qol_direct_farfield(qol_int nsrc, const double* sx, const double* snx, const double* sw, const double* ub,
+                        const double* ubn, double* u) {
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  if (!sx || !snx || !sw || !ub || !ubn || !u) return fail(QOL_ERR_ARG, "null argument");
+  if (nsrc < 0) return fail(QOL_ERR_ARG, "negative size");
+  int rc = ensure_device();
+  if (rc) return rc;
+  if (nsrc == 0) return 0;
+  cudaStream_t st = g_stream;
+  if ((rc = g_arena_io.reserve(sizeof(double) * (size_t)10 * nsrc + 8 * 256))) return rc;
+  g_arena_io.reset();
+  double* dsx = g_arena_io.take<double>(3 * nsrc);
+  double* dsnx = g_arena_io.take<double>(3 * nsrc);
+  double* dsw = g_arena_io.take<double>(nsrc);
+  double* dub = g_arena_io.take<double>(nsrc);
+  double* dubn = g_arena_io.take<double>(nsrc);
+  double* du = g_arena_io.take<double>(nsrc);
+  CK(cudaMemcpyAsync(dsx, sx, sizeof(double) * 3 * nsrc, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dsnx, snx, sizeof(double) * 3 * nsrc, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dsw, sw, sizeof(double) * nsrc, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dub, ub, sizeof(double) * nsrc, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dubn, ubn, sizeof(double) * nsrc, cudaMemcpyHostToDevice, st));
+  CK(qol_launch_direct_far(nsrc, dsx, dsnx, dsw, dub, dubn, du, st));
+  CK(cudaMemcpyAsync(u, du, sizeof(double) * nsrc, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
   return 0;
 }
 

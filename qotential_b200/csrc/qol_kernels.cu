@@ -1004,7 +1004,7 @@ __global__ void __launch_bounds__(32 * RRQ_WARPS) k_rrq_geom(OrderTab T, PairIn 
   const int2 pr = R.pair[gidx]; /* (panel, local target) */
   const int pan = pr.x, tl = pr.y;
   const long long p0 = Q.tcxi[pan] - 1;
-  const int hd = T.hd, nq = T.nquad, nbd = 3 * nq, L = T.nterms, ng = T.ng;
+  const int hd = T.hd, nq = T.nquad, nbd = 3 * nq;
   const double* fr = R.frame + (size_t)pan * RRQ_FRAME;
   const double* bx = R.bx + (size_t)pan * 3 * nbd;
   const double* bt = R.bt + (size_t)pan * 3 * nbd;
@@ -1767,5 +1767,180 @@ __global__ void __launch_bounds__(256) k_fp64_peak(double* out, int iters, doubl
 
 cudaError_t qol_launch_fp64_peak(double* out, int blocks, int iters, cudaStream_t st) {
   k_fp64_peak<<<blocks, 256, 0, st>>>(out, iters, 0.999999999, 1e-9);
+  return cudaGetLastError();
+}
+/* ===================================================================== */
+/* GRF near phase (stellarator_grf_core_mod.f90:652-899) and the Direct    */
+/* far field (:566-606) on the GPU                                        */
+/* ===================================================================== */
+/* ball of panel k: centre = mean of its hd nodes (summed in node order),
+ * radius 1.75 sqrt(sum sw); stored (qx, qy, qz, qr^2) */
+__global__ void k_ball_centers(int npan, int hd, const double* sx, const double* sw, double* ball) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= npan) return;
+  double qp0 = 0.0, qp1 = 0.0, qp2 = 0.0, s = 0.0;
+  for (int i = 0; i < hd; ++i) {
+    const size_t j = (size_t)k * hd + i;
+    qp0 = __dadd_rn(qp0, sx[3 * j]); qp1 = __dadd_rn(qp1, sx[3 * j + 1]); qp2 = __dadd_rn(qp2, sx[3 * j + 2]);
+    s = __dadd_rn(s, sw[j]);
+  }
+  const double qr = __dmul_rn(1.75, sqrt(s));
+  ball[4 * k] = qp0 / (double)hd;
+  ball[4 * k + 1] = qp1 / (double)hd;
+  ball[4 * k + 2] = qp2 / (double)hd;
+  ball[4 * k + 3] = __dmul_rn(qr, qr);
+}
+/* the ball test exactly as written in the reference (no fused multiply-adds) */
+__device__ __forceinline__ bool in_ball(const double* x, const double* b) {
+  const double a = __dadd_rn(x[0], -b[0]), c = __dadd_rn(x[1], -b[1]), e = __dadd_rn(x[2], -b[2]);
+  return __dadd_rn(__dadd_rn(__dmul_rn(a, a), __dmul_rn(c, c)), __dmul_rn(e, e)) < b[3];
+}
+/* near sources per panel (CTA per panel) */
+__global__ void __launch_bounds__(256) k_ball_count(long long nsrc, const double* sx, const double* ball,
+                                                    long long* counts) {
+  const int k = blockIdx.x;
+  __shared__ double b[4];
+  __shared__ long long part[8];
+  if (threadIdx.x < 4) b[threadIdx.x] = ball[4 * k + threadIdx.x];
+  __syncthreads();
+  long long c = 0;
+  for (long long j = threadIdx.x; j < nsrc; j += blockDim.x) c += in_ball(sx + 3 * j, b) ? 1 : 0;
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += part[w];
+    counts[k] = t;
+  }
+}
+/* their 1-based indices in source order (the reference's CSR), the target
+ * coordinates gathered alongside */
+__global__ void __launch_bounds__(256) k_ball_fill(long long nsrc, const double* sx, const double* ball,
+                                                   const long long* offs, long long* csr_idx, double* tcx) {
+  const int k = blockIdx.x;
+  __shared__ double b[4];
+  __shared__ int wcnt[8];
+  if (threadIdx.x < 4) b[threadIdx.x] = ball[4 * k + threadIdx.x];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  long long base = offs[k];
+  for (long long j0 = 0; j0 < nsrc; j0 += blockDim.x) {
+    const long long j = j0 + threadIdx.x;
+    const bool hit = j < nsrc && in_ball(sx + 3 * j, b);
+    const unsigned m = __ballot_sync(0xffffffffu, hit);
+    if (lane == 0) wcnt[w] = __popc(m);
+    __syncthreads();
+    int before = 0, total = 0;
+    for (int q = 0; q < nw; ++q) { if (q < w) before += wcnt[q]; total += wcnt[q]; }
+    if (hit) {
+      const long long pos = base + before + __popc(m & ((1u << lane) - 1u));
+      csr_idx[pos] = j + 1;
+      tcx[3 * pos] = sx[3 * j]; tcx[3 * pos + 1] = sx[3 * j + 1]; tcx[3 * pos + 2] = sx[3 * j + 2];
+    }
+    base += total;
+    __syncthreads();
+  }
+}
+/* csr_val[o0+j] = sum_k (S - S_naive)[j][k] ubn_k - (D - D_naive)[j][k] ub_k over
+ * the panel's hd nodes, in node order (the COO values are already minus the
+ * naive block) */
+__global__ void __launch_bounds__(256) k_grf_fill(int hd, const long long* offs, const double* vs, const double* vd,
+                                                  const double* ub, const double* ubn, double* csr_val) {
+  const int k = blockIdx.x;
+  const long long o0 = offs[k], m = offs[k + 1] - o0;
+  for (long long j = threadIdx.x; j < m; j += blockDim.x) {
+    double v = 0.0;
+    for (int i = 0; i < hd; ++i) {
+      const size_t o = (size_t)o0 * hd + (size_t)i * m + j;
+      v = v + vs[o] * ubn[(size_t)k * hd + i] - vd[o] * ub[(size_t)k * hd + i];
+    }
+    csr_val[o0 + j] = v;
+  }
+}
+/* u[t] += csr_val of every panel whose ball holds t, in panel order (the
+ * reference's serial scatter), one thread per source node, no atomics */
+#define GRF_PT 512 /* panels per shared-memory tile */
+__global__ void __launch_bounds__(256) k_grf_scatter(int npan, long long nsrc, const double* sx, const double* ball,
+                                                     const long long* offs, const long long* csr_idx,
+                                                     const double* csr_val, double* u) {
+  __shared__ double sb[GRF_PT * 4];
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double x[3] = {0.0, 0.0, 0.0};
+  if (t < nsrc) { x[0] = sx[3 * t]; x[1] = sx[3 * t + 1]; x[2] = sx[3 * t + 2]; }
+  double acc = t < nsrc ? u[t] : 0.0;
+  for (int k0 = 0; k0 < npan; k0 += GRF_PT) {
+    const int nk = min(GRF_PT, npan - k0);
+    __syncthreads();
+    for (int e = threadIdx.x; e < 4 * nk; e += blockDim.x) sb[e] = ball[4 * (size_t)k0 + e];
+    __syncthreads();
+    if (t < nsrc)
+      for (int kk = 0; kk < nk; ++kk) {
+        if (!in_ball(x, sb + 4 * kk)) continue;
+        /* position of t+1 in the panel's sorted list */
+        long long lo = offs[k0 + kk], hi = offs[k0 + kk + 1] - 1;
+        while (lo < hi) {
+          const long long mid = (lo + hi) >> 1;
+          if (csr_idx[mid] < t + 1) lo = mid + 1; else hi = mid;
+        }
+        if (lo < offs[k0 + kk + 1] && csr_idx[lo] == t + 1) acc += csr_val[lo];
+      }
+  }
+  if (t < nsrc) u[t] = acc;
+}
+/* u_i = sum_j S_ij ubn_j - D_ij ub_j over all sources, zero self term, in
+ * source order (the reference's blocked Direct far field) */
+#define FAR_TILE 256
+__global__ void __launch_bounds__(256) k_direct_far(long long nsrc, const double* sx, const double* snx,
+                                                    const double* sw, const double* ub, const double* ubn, double* u) {
+  __shared__ double sj[FAR_TILE][8]; /* x, y, z, nx, ny, nz, w/4pi ubn, w/4pi ub */
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const double i4p = 1.0 / (4.0 * QOL_PI);
+  double x0 = 0.0, x1 = 0.0, x2 = 0.0;
+  if (i < nsrc) { x0 = sx[3 * i]; x1 = sx[3 * i + 1]; x2 = sx[3 * i + 2]; }
+  double acc = 0.0;
+  for (long long j0 = 0; j0 < nsrc; j0 += FAR_TILE) {
+    const int nj = (int)min((long long)FAR_TILE, nsrc - j0);
+    __syncthreads();
+    for (int e = threadIdx.x; e < nj; e += blockDim.x) {
+      const long long j = j0 + e;
+      sj[e][0] = sx[3 * j]; sj[e][1] = sx[3 * j + 1]; sj[e][2] = sx[3 * j + 2];
+      sj[e][3] = snx[3 * j]; sj[e][4] = snx[3 * j + 1]; sj[e][5] = snx[3 * j + 2];
+      sj[e][6] = sw[j] * i4p * ubn[j]; sj[e][7] = sw[j] * i4p * ub[j];
+    }
+    __syncthreads();
+    for (int e = 0; e < nj; ++e) {
+      const double dx = x0 - sj[e][0], dy = x1 - sj[e][1], dz = x2 - sj[e][2];
+      const double rr = dx * dx + dy * dy + dz * dz;
+      if (rr > 1.0e-28) {
+        const double ri = rsqrt(rr);
+        acc += ri * (sj[e][6] - sj[e][7] * ri * ri * (dx * sj[e][3] + dy * sj[e][4] + dz * sj[e][5]));
+      }
+    }
+  }
+  if (i < nsrc) u[i] = acc;
+}
+
+cudaError_t qol_launch_grf_balls(int npan, int hd, long long nsrc, const double* sx, const double* sw, double* ball,
+                                 long long* counts, cudaStream_t st) {
+  k_ball_centers<<<(npan + 127) / 128, 128, 0, st>>>(npan, hd, sx, sw, ball);
+  k_ball_count<<<npan, 256, 0, st>>>(nsrc, sx, ball, counts);
+  return cudaGetLastError();
+}
+cudaError_t qol_launch_grf_csr(int npan, long long nsrc, const double* sx, const double* ball, const long long* offs,
+                               long long* csr_idx, double* tcx, cudaStream_t st) {
+  k_ball_fill<<<npan, 256, 0, st>>>(nsrc, sx, ball, offs, csr_idx, tcx);
+  return cudaGetLastError();
+}
+cudaError_t qol_launch_grf_apply(int npan, int hd, long long nsrc, const double* sx, const double* ball,
+                                 const long long* offs, const long long* csr_idx, const double* vs, const double* vd,
+                                 const double* ub, const double* ubn, double* csr_val, double* u, cudaStream_t st) {
+  k_grf_fill<<<npan, 256, 0, st>>>(hd, offs, vs, vd, ub, ubn, csr_val);
+  k_grf_scatter<<<(unsigned)((nsrc + 255) / 256), 256, 0, st>>>(npan, nsrc, sx, ball, offs, csr_idx, csr_val, u);
+  return cudaGetLastError();
+}
+cudaError_t qol_launch_direct_far(long long nsrc, const double* sx, const double* snx, const double* sw,
+                                  const double* ub, const double* ubn, double* u, cudaStream_t st) {
+  k_direct_far<<<(unsigned)((nsrc + 255) / 256), 256, 0, st>>>(nsrc, sx, snx, sw, ub, ubn, u);
   return cudaGetLastError();
 }

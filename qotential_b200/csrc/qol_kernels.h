@@ -100,3 +100,13 @@ cudaError_t qol_launch_rrq_apply(const OrderTab& T, const PanelIn& P, const Pair
 cudaError_t qol_launch_coo_index(const OrderTab& T, const PairIn& Q, long long* si, long long* sj, int npan,
                                  cudaStream_t st);
 cudaError_t qol_launch_fp64_peak(double* out, int blocks, int iters, cudaStream_t st);
+/* GRF near phase and Direct far field */
+cudaError_t qol_launch_grf_balls(int npan, int hd, long long nsrc, const double* sx, const double* sw, double* ball,
+                                 long long* counts, cudaStream_t st);
+cudaError_t qol_launch_grf_csr(int npan, long long nsrc, const double* sx, const double* ball, const long long* offs,
+                               long long* csr_idx, double* tcx, cudaStream_t st);
+cudaError_t qol_launch_grf_apply(int npan, int hd, long long nsrc, const double* sx, const double* ball,
+                                 const long long* offs, const long long* csr_idx, const double* vs, const double* vd,
+                                 const double* ub, const double* ubn, double* csr_val, double* u, cudaStream_t st);
+cudaError_t qol_launch_direct_far(long long nsrc, const double* sx, const double* snx, const double* sw,
+                                  const double* ub, const double* ubn, double* u, cudaStream_t st);
