@@ -113,6 +113,37 @@ def roofline_line(W, hist, k_ms, peak):
             "level_hist": [int(x) for x in hist[1:6]]}
 
 
+def grf_sweep(orders=(4, 6, 8, 10, 12)):
+    """The GRF identity on the same stellarator (16x80 quads) per order: far field
+    (qol_direct_farfield) + near phase (qol_grf_near, surface nodes as targets,
+    8 exterior point charges), error max |S[du/dn] - D[u]| / max |du/dn|;
+    near-phase pairs/s from the wall time of qol_grf_near (ball search, RRQ
+    corrections, contraction and scatter, host copies included)."""
+    import qotential_b200 as qol
+    from qotential_b200 import geometry as G
+    out = []
+    surf = G.stellarator()
+    for k in orders:
+        nterms = k + 1
+        hd = nterms * (nterms + 1) // 2
+        P = G.panels(surf, MP, NP, nterms, split=False)
+        ys, q = G.point_charges(surf, 8, seed=SEED)
+        ub, ubn = G.harmonic_density(P["sx"], P["snx"], ys, q)
+        npan = P["sw"].size // hd
+        uf = qol.qol_direct_farfield(P["sx"], P["snx"], P["sw"], ub, ubn)
+        best = None
+        for _ in range(2):
+            t0 = time.perf_counter()
+            un, nn, hist = qol.qol_grf_near(npan, nterms, nterms + 2, P["sx"], P["snx"], P["sw"], P["rts"], P["rps"],
+                                            ub, ubn, u=uf)
+            dt = time.perf_counter() - t0
+            best = dt if best is None else min(best, dt)
+        out.append({"order": k, "nsrc": int(P["sw"].size), "near_pairs": int(nn),
+                     "rrq_pairs": int(hist[5]), "grf_error": float(np.abs(un).max() / np.abs(ubn).max()),
+                     "near_phase_s": round(best, 4), "near_pairs_per_s": nn / best})
+    return out
+
+
 def config_dict(W, world):
     return {"workload": f"stellarator {MP}x{NP} quads ({W['npan_total']} triangles), order {ORDER} "
                         f"(nterms {W['nterms']}, hdim {W['hd']}, nquad=orderff {W['nquad']}), "
@@ -232,6 +263,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--no-grf", action="store_true", help="skip the per-order GRF sweep")
     ap.add_argument("--panels", type=int, default=0, help="use only the leading N panels (profiling)")
     ap.add_argument("--kernels-only", action="store_true",
                     help="only the warm-up and timed steps (for profiler launch lists)")
@@ -353,6 +385,9 @@ def main():
                "note": "qol_getnearquad_lap_rrq with host (numpy) buffers: inputs copied in, the COO values "
                        "copied out through pinned staging overlapping the chunked compute, the COO indices "
                        "filled on host threads from tcxrow/tcxi meanwhile"}
+    grf = None
+    if rank == 0 and world == 1 and not args.no_grf:
+        grf = grf_sweep()
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         nthr = os.cpu_count() or 1
@@ -365,7 +400,8 @@ def main():
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
                 "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": config_dict(W, world), "clocks": clocks, "e2e": e2e,
-                "gpu_launches": LAUNCHES_PER_STEP * args.steps, "roofline": roofline, "cpu_baseline": cpu}
+                "gpu_launches": LAUNCHES_PER_STEP * args.steps, "roofline": roofline, "cpu_baseline": cpu,
+                "grf_sweep": grf}
         print(json.dumps(line))
     if dist:
         dist.barrier()
