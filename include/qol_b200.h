@@ -164,6 +164,14 @@ int qol_direct_farfield(qol_int nsrc, const double* sx, const double* snx, const
  * the switch (-1: read only).  (No counterpart in the reference; its timeinfo
  * is the host-side analogue.) */
 #define QOL_NPHASE 9
+/* Precision of the level-resolved kernel sums for the calls that follow
+ * (library-wide): 0 = FP64 (default; the drop-in), 1 = the precision variant:
+ * kernel values in FP32, contraction with the interpolation rows on the TF32
+ * tensor path with a 3xTF32 split, FP32 accumulation over 32-node tiles and
+ * FP64 across them; the naive block, the RRQ moments, solves and quaternion
+ * fits stay FP64.  qol_rrq_noalloc always uses FP64.  No counterpart in the
+ * reference (all FP64). */
+int qol_set_sum_precision(int mode);
 /* Wall-clock milestones (ms from the start) of the last
  * qol_getnearquad_lap_rrq call: [0] inputs queued, [1] all panel chunks
  * queued, [2] all value copies queued, [3] values landed in pinned staging,

@@ -15,7 +15,7 @@ import numpy as np
 __all__ = [
     "lib", "QolError", "qol_simplex_precomp", "qol_build_patch_levels", "qol_lap3dsdlpmat_levels",
     "qol_clear_patch_levels", "qol_clear_patch_levels_all", "qol_rrq", "qol_getnearquad_lap_rrq",
-    "qol_getnearquad_lap_rrq_dev", "qol_grf_near", "qol_direct_farfield",
+    "qol_getnearquad_lap_rrq_dev", "qol_grf_near", "qol_direct_farfield", "qol_set_sum_precision",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -226,3 +226,9 @@ def qol_direct_farfield(sx, snx, sw, ub, ubn):
                                    _vp(_f(ub, nsrc)), _vp(_f(ubn, nsrc)), _vp(u))
     _check(rc)
     return u
+
+
+def qol_set_sum_precision(mode):
+    """0: FP64 level sums (default, the drop-in); 1: FP32 level sums on the
+    3xTF32 tensor path with FP64 accumulation across tiles (precision variant)."""
+    _check(lib().qol_set_sum_precision(C.c_int(int(mode))))

@@ -94,6 +94,7 @@ bool g_coefs_uploaded = false;
 Arena g_arena, g_arena2, g_arena_io, g_arena_grf; /* pipeline, per-pair RRQ storage, host-entry buffers, GRF */
 /* per-phase device milliseconds of the pipeline (diagnostics) */
 int g_ktime_on = 0;
+int g_sum_precision = 0; /* 0 FP64 (the drop-in), 1 FP32 level sums */
 double g_ktime[QOL_NPHASE] = {};
 long long g_kcalls = 0;
 cudaStream_t g_stream = nullptr;
@@ -148,6 +149,24 @@ int order_tables(int nterms, int orderff, int nquad, OrderCache** out) {
       for (int k = 0; k < hd; ++k) rm[(size_t)i * hd + k] = L.interp[i + (size_t)L.n * k];
     std::vector<int> st(L.subtyp.begin(), L.subtyp.end());
     T.interp[l] = C->up(rm);
+    /* TF32 split of the FP32 rounding (round to nearest, ties away: the
+     * device's cvt.rna.tf32.f32) */
+    auto tf32 = [](float x) {
+      uint32_t u;
+      std::memcpy(&u, &x, 4);
+      u = (u + 0x1000u) & ~0x1FFFu;
+      return u;
+    };
+    std::vector<uint32_t> rh(rm.size()), rl(rm.size());
+    for (size_t e = 0; e < rm.size(); ++e) {
+      const float f = (float)rm[e];
+      rh[e] = tf32(f);
+      float h;
+      std::memcpy(&h, &rh[e], 4);
+      rl[e] = tf32(f - h);
+    }
+    T.interp_hi[l] = C->up(rh);
+    T.interp_lo[l] = C->up(rl);
     T.wt[l] = C->up(L.wt);
     T.suboff[l] = C->up(L.suboff);
     T.subtyp[l] = C->up(st);
@@ -255,6 +274,7 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
   if (rc) return rc;
   OrderTab T = C->T;
   T.dist = J.distff;
+  T.sum_fp32 = g_sum_precision == 1;
   const int hd = T.hd, npan = J.npan, nq = T.nquad, nbd = 3 * nq;
   const long long ntcx = J.ntcx;
   /* workspace size */
@@ -637,6 +657,13 @@ int qol_kernel_times(int enable, double* ms, qol_int* calls) {
   return 0;
 }
 int qol_version(void) { return 100; }
+
+int qol_set_sum_precision(int mode) {
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  if (mode != 0 && mode != 1) return fail(QOL_ERR_ARG, "sum precision must be 0 (FP64) or 1 (FP32 level sums)");
+  g_sum_precision = mode;
+  return 0;
+}
 
 int qol_level_sizes(qol_int nterms, qol_int orderff, qol_int* n4, qol_int* nsub4) {
   std::lock_guard<std::recursive_mutex> g(g_mu);

@@ -394,6 +394,235 @@ constexpr size_t direct_smem() {
   return sizeof(double) * (2 * (2 * DNT * DKS + DNT * (32 * NB + 4) + 8 * DNT) + 3 * DTT) + sizeof(int) * DTT;
 }
 
+/* ---------------------------------------------------------------------
+ * FP32 form of the level sums (the precision variant): kernel values in
+ * FP32 from FP64 coordinate differences, the contraction with the
+ * interpolation rows on the TF32 tensor path with the 3xTF32 split
+ * (a b ~ a_hi b_hi + a_hi b_lo + a_lo b_hi, each a_hi = TF32 rounding of a,
+ * a_lo = TF32 rounding of the rest) accumulated in FP32 over a tile of DNT
+ * nodes and in FP64 across tiles; the naive block in FP64.
+ * --------------------------------------------------------------------- */
+#define FKS (DTT + 8)  /* kernel-tile row stride (floats): fragment loads hit 32 distinct banks */
+__device__ __forceinline__ unsigned tf32_rna(float x) {
+  unsigned r;
+  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ void tf32_split(float x, unsigned& hi, unsigned& lo) {
+  hi = tf32_rna(x);
+  lo = tf32_rna(x - __uint_as_float(hi));
+}
+/* D(16x8) += A(16x8, row) B(8x8, col), TF32 in, FP32 accumulate; per lane
+ * a = A[g][t], A[g+8][t], A[g][t+4], A[g+8][t+4]; b = B[t][g], B[t+4][g];
+ * d = D[g][2t], D[g][2t+1], D[g+8][2t], D[g+8][2t+1] (g = lane/4, t = lane%4) */
+__device__ __forceinline__ void mma_tf32(float* d, const unsigned* a, unsigned b0, unsigned b1) {
+  asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+               : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+               : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+
+/* one CTA per (panel, level), chunks of DTT = 32 targets, tiles of DNT = 32
+ * nodes double-buffered as in k_direct: the next tile's TF32 interpolation
+ * parts arrive by async copy and its node values (panel-relative, in FP32)
+ * are loaded during the current tile's tensor work; coordinates are taken
+ * relative to the panel's first node so that the FP32 differences keep their
+ * relative accuracy.  Warp w: targets 16 (w>>2) .. +15, column blocks
+ * (w&3) NB .. +NB-1 */
+template <int NB>
+__global__ void __launch_bounds__(256, 2) k_direct_tf32(OrderTab T, PanelIn P, PairIn Q, LevelWS W, PairWS G,
+                                                        OutCOO O) {
+  const int pan = blockIdx.x, l = blockIdx.y;
+  if (l >= T.nlevel) return;
+  const int cntl = G.cnt[(size_t)pan * 8 + l + 1];
+  if (cntl == 0) return;
+  const int offl = G.off[(size_t)pan * 8 + l + 1];
+  const int hd = T.hd, n = T.n[l];
+  const long long p0 = Q.tcxi[pan] - 1, m = Q.tcxi[pan + 1] - Q.tcxi[pan];
+  const double* node = W.node[l] + (size_t)pan * n * 7;
+  const unsigned* Ihg = T.interp_hi[l];
+  const unsigned* Ilg = T.interp_lo[l];
+  constexpr int NCW = 32 * NB; /* padded columns */
+  constexpr int ICS = NCW + 8; /* interpolation-tile row stride (words) */
+  constexpr int STG = 4 * DNT * FKS + 2 * DNT * ICS + 8 * DNT; /* words per stage: K parts, I parts, nodes (7 x DNT floats) */
+  extern __shared__ __align__(16) unsigned fsm[];
+  double* tg = reinterpret_cast<double*>(fsm + 2 * STG); /* DTT x 3 */
+  float* xt = reinterpret_cast<float*>(tg + 3 * DTT);    /* DTT x 3, relative to the panel's first node */
+  int* tloc = reinterpret_cast<int*>(xt + 3 * DTT);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int tb0 = 16 * (w >> 2), cb0 = 8 * NB * (w & 3);
+  const int g = lane >> 2, t4 = lane & 3;
+  const double i4p = 1.0 / (4.0 * QOL_PI);
+  const double* pc = P.sx + (size_t)pan * hd * 3; /* the panel's first node */
+  const double c0x = pc[0], c0y = pc[1], c0z = pc[2];
+  const int ntile = (n + DNT - 1) / DNT;
+  /* node value of this thread (field f, node nn of a tile), loaded early */
+  const int nf = threadIdx.x / DNT, nnn = threadIdx.x % DNT;
+  auto node_load = [&](int t) -> double {
+    const int i = t * DNT + nnn;
+    return (nf < 7 && i < n) ? node[(size_t)nf * n + i] : 0.0;
+  };
+  auto node_store = [&](int s, double v) {
+    if (nf < 7) {
+      float* nd = reinterpret_cast<float*>(fsm + s * STG + 4 * DNT * FKS + 2 * DNT * ICS);
+      const double c = nf == 0 ? c0x : nf == 1 ? c0y : nf == 2 ? c0z : 0.0;
+      nd[nf * DNT + nnn] = (float)(nf == 6 ? v * i4p : v - c);
+    }
+  };
+  auto fetch = [&](int t, int s) { /* TF32 parts of the tile's interpolation rows */
+    unsigned* Ih = fsm + s * STG + 4 * DNT * FKS;
+    unsigned* Il = Ih + DNT * ICS;
+    const int n0 = t * DNT;
+    for (int e = threadIdx.x; e < DNT * NCW; e += blockDim.x) {
+      const int nn = e / NCW, c = e % NCW, i = n0 + nn;
+      if (i < n && c < hd) {
+        cp_async4(&Ih[nn * ICS + c], Ihg + (size_t)i * hd + c);
+        cp_async4(&Il[nn * ICS + c], Ilg + (size_t)i * hd + c);
+      } else {
+        Ih[nn * ICS + c] = 0u;
+        Il[nn * ICS + c] = 0u;
+      }
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  auto kvals = [&](int t, int s, int nt) { /* FP32 kernel values of tile t, TF32 parts */
+    unsigned* KSh = fsm + s * STG;
+    unsigned* KSl = KSh + DNT * FKS;
+    unsigned* KDh = KSl + DNT * FKS;
+    unsigned* KDl = KDh + DNT * FKS;
+    const float* nd = reinterpret_cast<const float*>(fsm + s * STG + 4 * DNT * FKS + 2 * DNT * ICS);
+    const int n0 = t * DNT;
+    for (int e = threadIdx.x; e < DNT * DTT; e += blockDim.x) {
+      const int nn = e / DTT, tt = e % DTT;
+      float sv = 0.0f, dv = 0.0f;
+      if (n0 + nn < n && tt < nt) {
+        const float dx = xt[3 * tt] - nd[nn], dy = xt[3 * tt + 1] - nd[DNT + nn], dz = xt[3 * tt + 2] - nd[2 * DNT + nn];
+        const float rr = dx * dx + dy * dy + dz * dz;
+        if (rr > 1.0e-28f) {
+          const float ri = rsqrtf(rr);
+          sv = nd[6 * DNT + nn] * ri;
+          dv = sv * ri * ri * (dx * nd[3 * DNT + nn] + dy * nd[4 * DNT + nn] + dz * nd[5 * DNT + nn]);
+        }
+      }
+      unsigned hi, lo;
+      tf32_split(sv, hi, lo);
+      KSh[nn * FKS + tt] = hi; KSl[nn * FKS + tt] = lo;
+      tf32_split(dv, hi, lo);
+      KDh[nn * FKS + tt] = hi; KDl[nn * FKS + tt] = lo;
+    }
+  };
+  for (int c0 = 0; c0 < cntl; c0 += DTT) {
+    const int nt = min(DTT, cntl - c0);
+    __syncthreads();
+    fetch(0, 0);
+    node_store(0, node_load(0));
+    if (threadIdx.x < DTT) {
+      const int tl = threadIdx.x < nt ? G.grp[p0 + offl + c0 + threadIdx.x] : -1;
+      tloc[threadIdx.x] = tl;
+      for (int d = 0; d < 3; ++d) tg[3 * threadIdx.x + d] = tl >= 0 ? Q.tcx[3 * (p0 + tl) + d] : 0.0;
+      xt[3 * threadIdx.x] = (float)(tg[3 * threadIdx.x] - c0x);
+      xt[3 * threadIdx.x + 1] = (float)(tg[3 * threadIdx.x + 1] - c0y);
+      xt[3 * threadIdx.x + 2] = (float)(tg[3 * threadIdx.x + 2] - c0z);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    kvals(0, 0, nt);
+    __syncthreads();
+    double aS[NB][4], aD[NB][4]; /* FP64 totals of this warp's fragments */
+#pragma unroll
+    for (int b = 0; b < NB; ++b)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) { aS[b][c] = 0.0; aD[b][c] = 0.0; }
+    for (int t = 0; t < ntile; ++t) {
+      const int s = t & 1;
+      double nv = 0.0;
+      if (t + 1 < ntile) { fetch(t + 1, s ^ 1); nv = node_load(t + 1); }
+      const unsigned* KSh = fsm + s * STG;
+      const unsigned* KSl = KSh + DNT * FKS;
+      const unsigned* KDh = KSl + DNT * FKS;
+      const unsigned* KDl = KDh + DNT * FKS;
+      const unsigned* Ih = KDl + DNT * FKS;
+      const unsigned* Il = Ih + DNT * ICS;
+      float fS[NB][4], fD[NB][4];
+#pragma unroll
+      for (int b = 0; b < NB; ++b)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) { fS[b][c] = 0.0f; fD[b][c] = 0.0f; }
+#pragma unroll
+      for (int ks = 0; ks < DNT / 8; ++ks) {
+        const int r0 = 8 * ks + t4, r1 = r0 + 4; /* node rows of the k-slice */
+        const unsigned sh[4] = {KSh[r0 * FKS + tb0 + g], KSh[r0 * FKS + tb0 + 8 + g], KSh[r1 * FKS + tb0 + g],
+                                KSh[r1 * FKS + tb0 + 8 + g]};
+        const unsigned sl[4] = {KSl[r0 * FKS + tb0 + g], KSl[r0 * FKS + tb0 + 8 + g], KSl[r1 * FKS + tb0 + g],
+                                KSl[r1 * FKS + tb0 + 8 + g]};
+        const unsigned dh[4] = {KDh[r0 * FKS + tb0 + g], KDh[r0 * FKS + tb0 + 8 + g], KDh[r1 * FKS + tb0 + g],
+                                KDh[r1 * FKS + tb0 + 8 + g]};
+        const unsigned dl[4] = {KDl[r0 * FKS + tb0 + g], KDl[r0 * FKS + tb0 + 8 + g], KDl[r1 * FKS + tb0 + g],
+                                KDl[r1 * FKS + tb0 + 8 + g]};
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+          const int col = cb0 + 8 * b + g;
+          const unsigned bh0 = Ih[r0 * ICS + col], bh1 = Ih[r1 * ICS + col];
+          const unsigned bl0 = Il[r0 * ICS + col], bl1 = Il[r1 * ICS + col];
+          mma_tf32(fS[b], sl, bh0, bh1);
+          mma_tf32(fS[b], sh, bl0, bl1);
+          mma_tf32(fS[b], sh, bh0, bh1);
+          mma_tf32(fD[b], dl, bh0, bh1);
+          mma_tf32(fD[b], dh, bl0, bl1);
+          mma_tf32(fD[b], dh, bh0, bh1);
+        }
+      }
+#pragma unroll
+      for (int b = 0; b < NB; ++b)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) { aS[b][c] += (double)fS[b][c]; aD[b][c] += (double)fD[b][c]; }
+      if (t + 1 < ntile) {
+        node_store(s ^ 1, nv);
+        cp_async_wait_all();
+        __syncthreads(); /* tile t+1's interpolation parts and nodes staged */
+        kvals(t + 1, s ^ 1, nt);
+      }
+      __syncthreads();
+    }
+    /* naive block (FP64) and the COO write; fragment element c: target
+     * tb0 + g + 8 (c >> 1), column cb0 + 8b + 2 t4 + (c & 1) */
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int tt = tb0 + g + 8 * (c >> 1);
+      if (tt >= nt) continue;
+      const int tl = tloc[tt];
+      const long long row = Q.tcxrow[p0 + tl];
+      const double x0 = tg[3 * tt], x1 = tg[3 * tt + 1], x2 = tg[3 * tt + 2];
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+        const int k = cb0 + 8 * b + 2 * t4 + (c & 1);
+        if (k >= hd) continue;
+        double vs = aS[b][c], vd = aD[b][c];
+        if (O.subtract_naive) {
+          const size_t gj = (size_t)pan * hd + k;
+          double ns = 0.0, nd = 0.0;
+          if (row != (long long)gj + 1)
+            sdl_kernel(x0 - P.sx[3 * gj], x1 - P.sx[3 * gj + 1], x2 - P.sx[3 * gj + 2], P.snx[3 * gj],
+                       P.snx[3 * gj + 1], P.snx[3 * gj + 2], P.sw[gj] * i4p, ns, nd);
+          vs -= ns; vd -= nd;
+        }
+        const size_t o = (size_t)p0 * hd + (size_t)k * m + tl;
+        O.vs[o] = vs;
+        O.vd[o] = vd;
+      }
+    }
+  }
+}
+template <int NB>
+constexpr size_t direct_tf32_smem() {
+  return sizeof(unsigned) * 2 * (4 * DNT * FKS + 2 * DNT * (32 * NB + 8) + 8 * DNT) + sizeof(double) * 3 * DTT +
+         sizeof(float) * 3 * DTT + sizeof(int) * DTT;
+}
+
 /* ===================================================================== */
 /* harmonic column evaluation (shared by K4 and K5)                      */
 /* ===================================================================== */
@@ -1617,6 +1846,16 @@ cudaError_t qol_launch_direct(const OrderTab& T, const PanelIn& P, const PairIn&
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     kern<<<grid, 256, smem, st>>>(T, P, Q, W, G, O);
   };
+  if (T.sum_fp32) { /* the precision variant */
+    switch ((T.hd + 31) / 32) {
+      case 1: go(k_direct_tf32<1>, direct_tf32_smem<1>()); break;
+      case 2: go(k_direct_tf32<2>, direct_tf32_smem<2>()); break;
+      case 3: go(k_direct_tf32<3>, direct_tf32_smem<3>()); break;
+      case 4: go(k_direct_tf32<4>, direct_tf32_smem<4>()); break;
+      default: go(k_direct_tf32<5>, direct_tf32_smem<5>()); break;
+    }
+    return cudaGetLastError();
+  }
   switch ((T.hd + 31) / 32) {
     case 1: go(k_direct<1>, direct_smem<1>()); break;
     case 2: go(k_direct<2>, direct_smem<2>()); break;

@@ -11,6 +11,7 @@ struct OrderTab {
   double dist;
   int n[4], nsub[4];
   const double* interp[4];    /* n_l x hd, row-major */
+  const unsigned* interp_hi[4], *interp_lo[4]; /* the same in FP32 as TF32 high and low parts (precision variant) */
   const double* wt[4];        /* n_l */
   const long long* suboff[4]; /* nsub_l + 1 */
   const int* subtyp[4];       /* nsub_l */
@@ -23,6 +24,7 @@ struct OrderTab {
   const unsigned* xred;   /* per translation output: first partial slot, slot count */
   int xslots;
   const double* tginv;    /* nquad x nquad: 1/(tgl[i] - tgl[i-k-1]) at [k*nquad + i] */
+  int sum_fp32;           /* 1: level sums in FP32 on the 3xTF32 tensor path (precision variant) */
   int xsteps;
 };
 
