@@ -57,9 +57,9 @@ def workload(rank=0, world=1, panels=0):
     return W
 
 
-# kernels of one qol_getnearquad_lap_rrq_dev call: levels, classify, scan, direct,
+# kernels of one qol_getnearquad_lap_rrq_dev call: level nodes, level subs, classify, scan, direct,
 # rrq_pairs, rrq_panel, rrq_ssq, rrq_geom, rrq_moments, rrq_apply, coo_index
-LAUNCHES_PER_STEP = 11
+LAUNCHES_PER_STEP = 12
 
 
 def xlate_terms(L):

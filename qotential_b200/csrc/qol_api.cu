@@ -144,27 +144,30 @@ int order_tables(int nterms, int orderff, int nquad, OrderCache** out) {
   for (int l = 0; l < 4; ++l) {
     const qolh::RefLevel& L = R.lev[l];
     T.n[l] = (int)L.n; T.nsub[l] = (int)L.nsub;
-    std::vector<double> rm((size_t)L.n * hd);
-    for (long long i = 0; i < L.n; ++i)
-      for (int k = 0; k < hd; ++k) rm[(size_t)i * hd + k] = L.interp[i + (size_t)L.n * k];
     std::vector<int> st(L.subtyp.begin(), L.subtyp.end());
-    T.interp[l] = C->up(rm);
-    /* TF32 split of the FP32 rounding (round to nearest, ties away: the
-     * device's cvt.rna.tf32.f32) */
+    /* zero-padded rows of ncw columns, and their TF32 split of the FP32
+     * rounding (round to nearest, ties away: the device's cvt.rna.tf32.f32) */
     auto tf32 = [](float x) {
       uint32_t u;
       std::memcpy(&u, &x, 4);
       u = (u + 0x1000u) & ~0x1FFFu;
       return u;
     };
-    std::vector<uint32_t> rh(rm.size()), rl(rm.size());
-    for (size_t e = 0; e < rm.size(); ++e) {
-      const float f = (float)rm[e];
-      rh[e] = tf32(f);
-      float h;
-      std::memcpy(&h, &rh[e], 4);
-      rl[e] = tf32(f - h);
-    }
+    const int ncw = 32 * ((hd + 31) / 32);
+    std::vector<double> rp((size_t)L.n * ncw, 0.0);
+    std::vector<uint32_t> rh(rp.size(), 0u), rl(rp.size(), 0u);
+    for (long long i = 0; i < L.n; ++i)
+      for (int k = 0; k < hd; ++k) {
+        const size_t e = (size_t)i * ncw + k;
+        rp[e] = L.interp[i + (size_t)L.n * k];
+        const float f = (float)rp[e];
+        rh[e] = tf32(f);
+        float h;
+        std::memcpy(&h, &rh[e], 4);
+        rl[e] = tf32(f - h);
+      }
+    T.ncw = ncw;
+    T.interp[l] = C->up(rp);
     T.interp_hi[l] = C->up(rh);
     T.interp_lo[l] = C->up(rl);
     T.wt[l] = C->up(L.wt);

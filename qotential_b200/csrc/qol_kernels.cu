@@ -1,6 +1,7 @@
 /* qol_b200 kernels: the RRQ near-field hot path on sm_100a, FP64.
  *
- *   k_panel_levels   build_patch_levels_r64 (patch_refine_mod.f90:423-502)
+ *   k_level_nodes,   build_patch_levels_r64 (patch_refine_mod.f90:423-502)
+ *   k_level_subs
  *   k_classify       ball tests of lap3dsdlpmat_levels_r64 (:516-551)
  *   k_direct         level kernel sums fused with the interpmat contraction
  *                    (:553-600) and the naive-block subtraction of
@@ -82,76 +83,6 @@ void qol_upload_harm_coefs(const double* hb, const double* hc, const double* hcm
 }
 
 /* ===================================================================== */
-/* K1: refined levels of every panel                                     */
-/* ===================================================================== */
-__global__ void __launch_bounds__(256) k_panel_levels(OrderTab T, PanelIn P, LevelWS W) {
-  const int pan = blockIdx.x, hd = T.hd;
-  extern __shared__ double sm[];
-  double* src = sm; /* hd x 9 */
-  for (int e = threadIdx.x; e < hd * 3; e += blockDim.x) {
-    int j = e / 3, d = e % 3;
-    size_t g = (size_t)pan * hd + j;
-    src[j * 9 + d] = P.sx[3 * g + d];
-    src[j * 9 + 3 + d] = P.rts[3 * g + d];
-    src[j * 9 + 6 + d] = P.rps[3 * g + d];
-  }
-  __syncthreads();
-  for (int l = 0; l < T.nlevel; ++l) {
-    const int n = T.n[l];
-    const double* I = T.interp[l];
-    double* base = W.node[l] + (size_t)pan * n * 7;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      double g[9];
-#pragma unroll
-      for (int c = 0; c < 9; ++c) g[c] = 0.0;
-      for (int k = 0; k < hd; ++k) {
-        double a = I[(size_t)i * hd + k];
-#pragma unroll
-        for (int c = 0; c < 9; ++c) g[c] += a * src[k * 9 + c];
-      }
-      double nx = g[7] * g[5] - g[8] * g[4];
-      double ny = g[8] * g[3] - g[6] * g[5];
-      double nz = g[6] * g[4] - g[7] * g[3];
-      double sp = sqrt(nx * nx + ny * ny + nz * nz);
-      base[0 * n + i] = g[0];
-      base[1 * n + i] = g[1];
-      base[2 * n + i] = g[2];
-      base[3 * n + i] = nx / sp;
-      base[4 * n + i] = ny / sp;
-      base[5 * n + i] = nz / sp;
-      base[6 * n + i] = sp * T.wt[l][i];
-    }
-    __syncthreads();
-    /* sub-patch centroids and squared near radii, sequential per sub-patch */
-    const int ns = T.nsub[l];
-    for (int s = threadIdx.x; s < ns; s += blockDim.x) {
-      long long i0 = T.suboff[l][s], i1 = T.suboff[l][s + 1];
-      double swsum = 0.0, q[3];
-      for (long long i = i0; i < i1; ++i) swsum += base[6 * n + i];
-      for (int d = 0; d < 3; ++d) {
-        double acc = 0.0;
-        for (long long i = i0; i < i1; ++i) acc += base[d * n + i] * base[6 * n + i];
-        q[d] = acc / swsum;
-      }
-      double rmax2 = 0.0;
-      for (long long i = i0; i < i1; ++i) {
-        double d2 = 0.0;
-        for (int d = 0; d < 3; ++d) {
-          double t = base[d * n + i] - q[d];
-          d2 += t * t;
-        }
-        rmax2 = fmax(rmax2, d2);
-      }
-      double* qp = W.sub[l] + ((size_t)pan * ns + s) * 4;
-      qp[0] = q[0]; qp[1] = q[1]; qp[2] = q[2];
-      double d2 = T.dist * T.dist;
-      qp[3] = (T.subtyp[l][s] == 1) ? d2 * fmax(rmax2, 0.5 * swsum) : d2 * fmax(rmax2, swsum);
-    }
-    __syncthreads();
-  }
-}
-
-/* ===================================================================== */
 /* K2: level of every (target, panel) pair, grouped per panel by level   */
 /* ===================================================================== */
 __global__ void __launch_bounds__(128) k_classify(OrderTab T, PairIn Q, LevelWS W, PairWS G) {
@@ -228,6 +159,11 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
 }
+/* both addresses 16-byte aligned; .cg: through L2 only */
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 /* D = A (8x4, row) B (4x8, col) + D, FP64 tensor path; per lane a = A[lane/4][lane%4],
  * b = B[lane%4][lane/4], d = D[lane/4][2 (lane%4) + {0,1}] */
@@ -250,6 +186,130 @@ __device__ __forceinline__ void sdl_kernel(double dx, double dy, double dz, doub
   }
 }
 
+/* ===================================================================== */
+/* K1: refined levels of every panel                                     */
+/* ===================================================================== */
+/* Level nodes as one batched contraction per level: G_p (n_l x 9) = I_l (n_l x
+ * hd) S_p (hd x 9), S_p = [x | x_t | x_p] at panel p's nodes.  LV_P panels per
+ * CTA share the interpolation rows (B holds their 9 LV_P columns), each CTA
+ * takes a chunk of at most LV_M rows of one level; FP64 tensor path
+ * (m8n8k4), one m-block of 8 rows at a time per warp.  Epilogue per (node,
+ * panel): normal x_p cross x_t normalised, area element |.| wt, the 7-field
+ * SoA record. */
+#define LV_P 8
+#define LV_M 512
+#define LV_CS (9 * LV_P + 4) /* B row stride (doubles, 12 mod 16): conflict-free fragment loads */
+#define LV_ES (9 * LV_P + 1) /* epilogue staging row stride */
+__global__ void __launch_bounds__(256, 2) k_level_nodes(OrderTab T, PanelIn P, LevelWS W, int npan) {
+  const int hd = T.hd, KP = (hd + 3) & ~3, ncw = T.ncw;
+  const int p0 = blockIdx.x * LV_P;
+  int l = 0, c = blockIdx.y;
+  for (; l < T.nlevel; ++l) {
+    const int nc = (T.n[l] + LV_M - 1) / LV_M;
+    if (c < nc) break;
+    c -= nc;
+  }
+  if (l >= T.nlevel) return;
+  const int n = T.n[l], r0 = c * LV_M, r1 = min(n, r0 + LV_M);
+  const double* I = T.interp[l]; /* n x ncw, zero columns hd .. ncw-1 */
+  const double* wt = T.wt[l];
+  extern __shared__ __align__(16) double lsm[];
+  double* S = lsm;                  /* KP x LV_CS */
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double* E = lsm + KP * LV_CS + w * 8 * LV_ES; /* this warp's 8 x LV_ES staging */
+  for (int e = threadIdx.x; e < KP * 9 * LV_P; e += blockDim.x) {
+    const int k = e / (9 * LV_P), col = e % (9 * LV_P), p = col / 9, f = col % 9;
+    double v = 0.0;
+    if (k < hd && p0 + p < npan) {
+      const size_t g = (size_t)(p0 + p) * hd + k;
+      const double* src = f < 3 ? P.sx : (f < 6 ? P.rts : P.rps);
+      v = src[3 * g + f % 3];
+    }
+    S[k * LV_CS + col] = v;
+  }
+  __syncthreads();
+  const int g = lane >> 2, t4 = lane & 3;
+  const int nmb = (r1 - r0 + 7) / 8;
+  for (int mb = w; mb < nmb; mb += 8) {
+    const int row = r0 + 8 * mb + g;
+    const bool rv = row < r1;
+    const double* Ir = I + (size_t)(rv ? row : r0) * ncw + t4;
+    double acc[9][2];
+#pragma unroll
+    for (int j = 0; j < 9; ++j) { acc[j][0] = 0.0; acc[j][1] = 0.0; }
+#pragma unroll 4
+    for (int ks = 0; ks < KP / 4; ++ks) {
+      const double a = rv ? __ldg(Ir + 4 * ks) : 0.0;
+      const double* Sb = S + (4 * ks + t4) * LV_CS + g;
+#pragma unroll
+      for (int j = 0; j < 9; ++j) dmma(acc[j][0], acc[j][1], a, Sb[8 * j]);
+    }
+#pragma unroll
+    for (int j = 0; j < 9; ++j) {
+      E[g * LV_ES + 8 * j + 2 * t4] = acc[j][0];
+      E[g * LV_ES + 8 * j + 2 * t4 + 1] = acc[j][1];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int it = lane + 32 * h, gi = it & 7, p = it >> 3, i = r0 + 8 * mb + gi;
+      if (i < r1 && p0 + p < npan) {
+        const double* v = E + gi * LV_ES + 9 * p;
+        const double nx = v[7] * v[5] - v[8] * v[4];
+        const double ny = v[8] * v[3] - v[6] * v[5];
+        const double nz = v[6] * v[4] - v[7] * v[3];
+        const double sp = sqrt(nx * nx + ny * ny + nz * nz);
+        double* base = W.node[l] + (size_t)(p0 + p) * n * 7;
+        base[0 * n + i] = v[0];
+        base[1 * n + i] = v[1];
+        base[2 * n + i] = v[2];
+        base[3 * n + i] = nx / sp;
+        base[4 * n + i] = ny / sp;
+        base[5 * n + i] = nz / sp;
+        base[6 * n + i] = sp * wt[i];
+      }
+    }
+    __syncwarp();
+  }
+}
+constexpr size_t level_nodes_smem(int hd) { return sizeof(double) * (((hd + 3) & ~3) * LV_CS + 8 * 8 * LV_ES); }
+
+/* sub-patch centroids and squared near radii: one thread per (panel, level,
+ * sub-patch), sums in node order as the reference's loop
+ * (patch_refine_mod.f90:423-502) */
+__global__ void __launch_bounds__(128) k_level_subs(OrderTab T, LevelWS W, int npan) {
+  int nsubt = 0;
+  for (int l = 0; l < T.nlevel; ++l) nsubt += T.nsub[l];
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (long long)npan * nsubt) return;
+  const int pan = (int)(e / nsubt);
+  int s = (int)(e % nsubt), l = 0;
+  while (s >= T.nsub[l]) { s -= T.nsub[l]; ++l; }
+  const int n = T.n[l], ns = T.nsub[l];
+  const double* base = W.node[l] + (size_t)pan * n * 7;
+  const long long i0 = T.suboff[l][s], i1 = T.suboff[l][s + 1];
+  double swsum = 0.0, q[3];
+  for (long long i = i0; i < i1; ++i) swsum += base[6 * n + i];
+  for (int d = 0; d < 3; ++d) {
+    double acc = 0.0;
+    for (long long i = i0; i < i1; ++i) acc += base[d * n + i] * base[6 * n + i];
+    q[d] = acc / swsum;
+  }
+  double rmax2 = 0.0;
+  for (long long i = i0; i < i1; ++i) {
+    double d2 = 0.0;
+    for (int d = 0; d < 3; ++d) {
+      const double t = base[d * n + i] - q[d];
+      d2 += t * t;
+    }
+    rmax2 = fmax(rmax2, d2);
+  }
+  double* qp = W.sub[l] + ((size_t)pan * ns + s) * 4;
+  qp[0] = q[0]; qp[1] = q[1]; qp[2] = q[2];
+  const double d2 = T.dist * T.dist;
+  qp[3] = (T.subtyp[l][s] == 1) ? d2 * fmax(rmax2, 0.5 * swsum) : d2 * fmax(rmax2, swsum);
+}
+
 /* one CTA per (panel, level); chunks of DTT targets.  Tiles of DNT level nodes,
  * double-buffered in shared memory: the node data and interpolation rows of
  * tile t+1 arrive by async copy while the FP64 tensor path accumulates S and D
@@ -267,7 +327,7 @@ __global__ void __launch_bounds__(256, 2) k_direct(OrderTab T, PanelIn P, PairIn
   const int hd = T.hd, n = T.n[l];
   const long long p0 = Q.tcxi[pan] - 1, m = Q.tcxi[pan + 1] - Q.tcxi[pan];
   const double* node = W.node[l] + (size_t)pan * n * 7;
-  const double* I = T.interp[l];
+  const double* I = T.interp[l]; /* rows of NCW = T.ncw columns */
   constexpr int NCW = 32 * NB; /* padded columns */
   constexpr int ICS = NCW + 4; /* interpolation-tile row stride */
   constexpr int STG = 2 * DNT * DKS + DNT * ICS + 8 * DNT; /* doubles per stage: KS, KD, It, nodes (7 x DNT, padded) */
@@ -284,10 +344,10 @@ __global__ void __launch_bounds__(256, 2) k_direct(OrderTab T, PanelIn P, PairIn
     double* It = dsm + s * STG + 2 * DNT * DKS;
     double* nd = It + DNT * ICS;
     const int n0 = t * DNT;
-    for (int e = threadIdx.x; e < DNT * NCW; e += blockDim.x) {
-      const int nn = e / NCW, c = e % NCW, i = n0 + nn;
-      if (i < n && c < hd) cp_async8(&It[nn * ICS + c], I + (size_t)i * hd + c);
-      else It[nn * ICS + c] = 0.0;
+    for (int e = threadIdx.x; e < DNT * NCW / 2; e += blockDim.x) { /* 16-byte pieces */
+      const int nn = e / (NCW / 2), c = 2 * (e % (NCW / 2)), i = n0 + nn;
+      if (i < n) cp_async16(&It[nn * ICS + c], I + (size_t)i * NCW + c);
+      else { It[nn * ICS + c] = 0.0; It[nn * ICS + c + 1] = 0.0; }
     }
     for (int e = threadIdx.x; e < 7 * DNT; e += blockDim.x) {
       const int f = e / DNT, nn = e % DNT, i = n0 + nn;
@@ -421,11 +481,6 @@ __device__ __forceinline__ void mma_tf32(float* d, const unsigned* a, unsigned b
                : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-
 /* one CTA per (panel, level), chunks of DTT = 32 targets, tiles of DNT = 32
  * nodes double-buffered as in k_direct: the next tile's TF32 interpolation
  * parts arrive by async copy and its node values (panel-relative, in FP32)
@@ -477,15 +532,12 @@ __global__ void __launch_bounds__(256, 2) k_direct_tf32(OrderTab T, PanelIn P, P
     unsigned* Ih = fsm + s * STG + 4 * DNT * FKS;
     unsigned* Il = Ih + DNT * ICS;
     const int n0 = t * DNT;
-    for (int e = threadIdx.x; e < DNT * NCW; e += blockDim.x) {
-      const int nn = e / NCW, c = e % NCW, i = n0 + nn;
-      if (i < n && c < hd) {
-        cp_async4(&Ih[nn * ICS + c], Ihg + (size_t)i * hd + c);
-        cp_async4(&Il[nn * ICS + c], Ilg + (size_t)i * hd + c);
-      } else {
-        Ih[nn * ICS + c] = 0u;
-        Il[nn * ICS + c] = 0u;
-      }
+    for (int e = threadIdx.x; e < DNT * NCW / 2; e += blockDim.x) { /* 16-byte pieces of both parts */
+      const int part = e / (DNT * NCW / 4), r = e % (DNT * NCW / 4);
+      const int nn = r / (NCW / 4), c = 4 * (r % (NCW / 4)), i = n0 + nn;
+      unsigned* dst = (part ? Il : Ih) + nn * ICS + c;
+      if (i < n) cp_async16(dst, (part ? Ilg : Ihg) + (size_t)i * NCW + c);
+      else { dst[0] = 0u; dst[1] = 0u; dst[2] = 0u; dst[3] = 0u; }
     }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
   };
@@ -1830,8 +1882,18 @@ __global__ void k_scan_rrq(int npan, int lev, const int* cnt, long long* off) {
 /* launchers                                                             */
 /* ===================================================================== */
 cudaError_t qol_launch_levels(const OrderTab& T, const PanelIn& P, const LevelWS& W, int npan, cudaStream_t st) {
-  size_t smem = sizeof(double) * 9 * T.hd;
-  k_panel_levels<<<npan, 256, smem, st>>>(T, P, W);
+  if (npan <= 0) return cudaSuccess;
+  if (T.ncw < ((T.hd + 3) & ~3)) return cudaErrorInvalidValue; /* the padded rows cover the k-steps */
+  int nch = 0, nsubt = 0;
+  for (int l = 0; l < T.nlevel; ++l) {
+    nch += (T.n[l] + LV_M - 1) / LV_M;
+    nsubt += T.nsub[l];
+  }
+  const size_t smem = level_nodes_smem(T.hd);
+  cudaFuncSetAttribute(k_level_nodes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_level_nodes<<<dim3((npan + LV_P - 1) / LV_P, nch), 256, smem, st>>>(T, P, W, npan);
+  const long long nt = (long long)npan * nsubt;
+  k_level_subs<<<(unsigned)((nt + 127) / 128), 128, 0, st>>>(T, W, npan);
   return cudaGetLastError();
 }
 cudaError_t qol_launch_classify(const OrderTab& T, const PairIn& Q, const LevelWS& W, const PairWS& G, int npan,
@@ -1846,22 +1908,24 @@ cudaError_t qol_launch_direct(const OrderTab& T, const PanelIn& P, const PairIn&
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     kern<<<grid, 256, smem, st>>>(T, P, Q, W, G, O);
   };
+  const int nb = T.ncw / 32; /* the padded interpolation rows fix the column blocks */
+  if (nb < 1 || nb > 5 || T.ncw != 32 * ((T.hd + 31) / 32)) return cudaErrorInvalidValue;
   if (T.sum_fp32) { /* the precision variant */
-    switch ((T.hd + 31) / 32) {
+    switch (nb) {
       case 1: go(k_direct_tf32<1>, direct_tf32_smem<1>()); break;
       case 2: go(k_direct_tf32<2>, direct_tf32_smem<2>()); break;
       case 3: go(k_direct_tf32<3>, direct_tf32_smem<3>()); break;
       case 4: go(k_direct_tf32<4>, direct_tf32_smem<4>()); break;
-      default: go(k_direct_tf32<5>, direct_tf32_smem<5>()); break;
+      case 5: go(k_direct_tf32<5>, direct_tf32_smem<5>()); break;
     }
     return cudaGetLastError();
   }
-  switch ((T.hd + 31) / 32) {
+  switch (nb) {
     case 1: go(k_direct<1>, direct_smem<1>()); break;
     case 2: go(k_direct<2>, direct_smem<2>()); break;
     case 3: go(k_direct<3>, direct_smem<3>()); break;
     case 4: go(k_direct<4>, direct_smem<4>()); break;
-    default: go(k_direct<5>, direct_smem<5>()); break;
+    case 5: go(k_direct<5>, direct_smem<5>()); break;
   }
   return cudaGetLastError();
 }

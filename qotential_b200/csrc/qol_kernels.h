@@ -10,8 +10,9 @@ struct OrderTab {
   int korder, hd, nterms, orderff, nquad, nlevel, ng;
   double dist;
   int n[4], nsub[4];
-  const double* interp[4];    /* n_l x hd, row-major */
-  const unsigned* interp_hi[4], *interp_lo[4]; /* the same in FP32 as TF32 high and low parts (precision variant) */
+  const double* interp[4];    /* n_l x ncw, row-major; columns hd .. ncw-1 zero (16-byte rows) */
+  const unsigned* interp_hi[4], *interp_lo[4]; /* interp in FP32 as TF32 high and low parts (precision variant) */
+  int ncw;                    /* 32 ceil(hd / 32) */
   const double* wt[4];        /* n_l */
   const long long* suboff[4]; /* nsub_l + 1 */
   const int* subtyp[4];       /* nsub_l */

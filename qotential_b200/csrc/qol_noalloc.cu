@@ -104,9 +104,11 @@ int na_tables(NoAllocDev& D, int nterms, int orderff, int nquad, cudaStream_t st
   for (int l = 0; l < 4; ++l) {
     const qolh::RefLevel& L = R.lev[l];
     T.n[l] = (int)L.n; T.nsub[l] = (int)L.nsub;
-    std::vector<double> rm((size_t)L.n * hd);
+    const int ncw = 32 * ((hd + 31) / 32); /* zero-padded 16-byte rows */
+    T.ncw = ncw;
+    std::vector<double> rm((size_t)L.n * ncw, 0.0);
     for (long long i = 0; i < L.n; ++i)
-      for (int k = 0; k < hd; ++k) rm[(size_t)i * hd + k] = L.interp[i + (size_t)L.n * k];
+      for (int k = 0; k < hd; ++k) rm[(size_t)i * ncw + k] = L.interp[i + (size_t)L.n * k];
     std::vector<int> stp(L.subtyp.begin(), L.subtyp.end());
     o_interp[l] = put(rm.data(), sizeof(double) * rm.size());
     o_wt[l] = put(L.wt.data(), sizeof(double) * L.wt.size());
