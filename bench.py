@@ -32,9 +32,9 @@ NOFF = 20000
 SEED = 2026
 
 
-def workload(rank=0, world=1, panels=0):
+def workload(rank=0, world=1, panels=0, order=ORDER):
     from qotential_b200 import geometry as G
-    nterms = ORDER + 1
+    nterms = order + 1
     hd = nterms * (nterms + 1) // 2
     P = G.panels(G.stellarator(), MP, NP, nterms, split=False)
     off = G.off_surface_targets(P, NOFF, SEED, hd)
@@ -114,11 +114,12 @@ def roofline_line(W, hist, k_ms, peak):
 
 
 def grf_sweep(orders=(4, 6, 8, 10, 12)):
-    """The GRF identity on the same stellarator (16x80 quads) per order: far field
+    """The GRF identity on the same stellarator (16x80 quads) per order, in the
+    plain FP64 form and in the chosen form (FP32 level sums): far field
     (qol_direct_farfield) + near phase (qol_grf_near, surface nodes as targets,
     8 exterior point charges), error max |S[du/dn] - D[u]| / max |du/dn|;
     near-phase pairs/s from the wall time of qol_grf_near (ball search, RRQ
-    corrections, contraction and scatter, host copies included)."""
+    corrections, contraction and scatter, host copies included), best of 2."""
     import qotential_b200 as qol
     from qotential_b200 import geometry as G
     out = []
@@ -131,17 +132,89 @@ def grf_sweep(orders=(4, 6, 8, 10, 12)):
         ub, ubn = G.harmonic_density(P["sx"], P["snx"], ys, q)
         npan = P["sw"].size // hd
         uf = qol.qol_direct_farfield(P["sx"], P["snx"], P["sw"], ub, ubn)
-        best = None
-        for _ in range(2):
-            t0 = time.perf_counter()
-            un, nn, hist = qol.qol_grf_near(npan, nterms, nterms + 2, P["sx"], P["snx"], P["sw"], P["rts"], P["rps"],
-                                            ub, ubn, u=uf)
-            dt = time.perf_counter() - t0
-            best = dt if best is None else min(best, dt)
-        out.append({"order": k, "nsrc": int(P["sw"].size), "near_pairs": int(nn),
-                     "rrq_pairs": int(hist[5]), "grf_error": float(np.abs(un).max() / np.abs(ubn).max()),
-                     "near_phase_s": round(best, 4), "near_pairs_per_s": nn / best})
+        row = {"order": k, "nsrc": int(P["sw"].size)}
+        for mode, tag in ((0, "plain"), (1, "chosen")):
+            qol.qol_set_sum_precision(mode)
+            try:
+                best = None
+                for _ in range(2):
+                    t0 = time.perf_counter()
+                    un, nn, hist = qol.qol_grf_near(npan, nterms, nterms + 2, P["sx"], P["snx"], P["sw"], P["rts"],
+                                                    P["rps"], ub, ubn, u=uf)
+                    dt = time.perf_counter() - t0
+                    best = dt if best is None else min(best, dt)
+            finally:
+                qol.qol_set_sum_precision(0)
+            row["near_pairs"], row["rrq_pairs"] = int(nn), int(hist[5])
+            row[f"grf_error_{tag}"] = float(np.abs(un).max() / np.abs(ubn).max())
+            row[f"near_phase_s_{tag}"] = round(best, 4)
+            row[f"near_pairs_per_s_{tag}"] = nn / best
+        row["grf_error_ratio"] = row["grf_error_chosen"] / row["grf_error_plain"]
+        out.append(row)
     return out
+
+
+def row_errors(rows, a, b):
+    """per correction-matrix row (one target): max |a - b| / max |a| over the
+    row's entries; max, p99 and median over rows"""
+    import torch
+    r = rows - rows.min()
+    n = int(r.max()) + 1
+    d = torch.zeros(n, dtype=torch.float64, device=a.device).scatter_reduce_(0, r, (a - b).abs(), "amax")
+    m = torch.zeros(n, dtype=torch.float64, device=a.device).scatter_reduce_(0, r, a.abs(), "amax")
+    e = d[m > 0] / m[m > 0]
+    return {"max": float(e.max()), "p99": float(torch.quantile(e, 0.99)), "median": float(e.median())}
+
+
+def forms_compare(W, steps, warmup, D=None, out=None):
+    """The same device step (qol_getnearquad_lap_rrq_dev, inputs resident) in
+    the plain FP64 form and in the chosen form (qol_set_sum_precision(1)):
+    ms/step by CUDA events on the launching stream, and the chosen form's
+    per-row error against the plain form's sparsevs and sparsevd"""
+    import torch
+    import qotential_b200 as qol
+    dev = torch.device("cuda", torch.cuda.current_device())
+    t = lambda a, dt=torch.float64: torch.as_tensor(a, dtype=dt).to(dev)
+    if D is None:
+        D = {k: t(W[k]) for k in ("sx", "snx", "sw", "rts", "rps", "tcx")}
+        D["tcxrow"] = t(W["tcxrow"], torch.int64)
+        D["tcxi"] = t(W["tcxi"], torch.int64)
+    if out is None:
+        nnz = W["pairs"] * W["hd"]
+        out = (torch.empty(nnz, dtype=torch.int64, device=dev), torch.empty(nnz, dtype=torch.int64, device=dev),
+               torch.empty(nnz, dtype=torch.float64, device=dev), torch.empty(nnz, dtype=torch.float64, device=dev))
+    st = torch.cuda.current_stream()
+
+    def step():
+        qol.qol_getnearquad_lap_rrq_dev(W["npan"], W["nterms"], W["nquad"], D["sx"], D["snx"], D["sw"], D["rts"],
+                                        D["rps"], D["tcx"], D["tcxrow"], D["tcxi"], W["nquad"], 1.4, 30, out,
+                                        stream=st.cuda_stream, sync=False)
+
+    ms, vals = {}, {}
+    for mode in (0, 1):
+        qol.qol_set_sum_precision(mode)
+        try:
+            for _ in range(warmup):
+                step()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for _ in range(steps):
+                step()
+            e1.record(st)
+            torch.cuda.synchronize()
+        finally:
+            qol.qol_set_sum_precision(0)
+        ms[mode] = e0.elapsed_time(e1) / steps
+        vals[mode] = (out[2].clone(), out[3].clone())
+    res = {"order": W["nterms"] - 1, "near_pairs": W["pairs_total"],
+           "plain": {"ms_per_step": ms[0], "pairs_per_s": W["pairs_total"] / (ms[0] * 1e-3)},
+           "chosen": {"ms_per_step": ms[1], "pairs_per_s": W["pairs_total"] / (ms[1] * 1e-3)},
+           "speedup": ms[0] / ms[1],
+           "row_error_vs": row_errors(out[0], vals[0][0], vals[1][0]),
+           "row_error_vd": row_errors(out[0], vals[0][1], vals[1][1])}
+    del vals
+    return res
 
 
 def config_dict(W, world):
@@ -264,6 +337,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--no-grf", action="store_true", help="skip the per-order GRF sweep")
+    ap.add_argument("--no-chosen", action="store_true",
+                    help="skip the chosen-form (FP32 level sums) comparison at orders 12 and 10")
     ap.add_argument("--panels", type=int, default=0, help="use only the leading N panels (profiling)")
     ap.add_argument("--kernels-only", action="store_true",
                     help="only the warm-up and timed steps (for profiler launch lists)")
@@ -385,9 +460,23 @@ def main():
                "note": "qol_getnearquad_lap_rrq with host (numpy) buffers: inputs copied in, the COO values "
                        "copied out through pinned staging overlapping the chunked compute, the COO indices "
                        "filled on host threads from tcxrow/tcxi meanwhile"}
+    chosen = None
+    if rank == 0 and world == 1 and not args.no_chosen:
+        chosen = {"order12": forms_compare(W, args.steps, 2, D, out)}
+        W10 = workload(0, 1, args.panels, order=10)
+        chosen["order10"] = forms_compare(W10, args.steps, 2)
+        del W10
+        torch.cuda.empty_cache()
+        chosen["note"] = ("chosen form = qol_set_sum_precision(1): level kernel sums in FP32 (3xTF32 tensor "
+                          "contraction, FP64 accumulation across tiles); RRQ moments, solves and fits FP64; "
+                          "device step with inputs resident, CUDA events; row_error = per target row, "
+                          "max |chosen - plain| / max |plain| over the row's entries")
     grf = None
     if rank == 0 and world == 1 and not args.no_grf:
         grf = grf_sweep()
+        if chosen is not None:
+            chosen["grf_error"] = {str(r["order"]): {"plain": r["grf_error_plain"], "chosen": r["grf_error_chosen"]}
+                                   for r in grf}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         nthr = os.cpu_count() or 1
@@ -401,7 +490,7 @@ def main():
                 "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": config_dict(W, world), "clocks": clocks, "e2e": e2e,
                 "gpu_launches": LAUNCHES_PER_STEP * args.steps, "roofline": roofline, "cpu_baseline": cpu,
-                "grf_sweep": grf}
+                "chosen_form": chosen, "grf_sweep": grf}
         print(json.dumps(line))
     if dist:
         dist.barrier()

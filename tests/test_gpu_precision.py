@@ -7,7 +7,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-TOL_ROWS = 2e-6   # FP32-form correction values vs FP64, relative to the largest |value|
+TOL_ROWS = 1e-6   # FP32-form correction values vs FP64, per target row: max |diff| / max |value| of the row
 GRF_MATCH = 1.10  # FP32-form GRF error at most 10 % above the FP64 form's
 
 
@@ -32,8 +32,13 @@ def test_fp32_sums_rows_vs_fp64(qol, nterms):
     finally:
         qol.qol_set_sum_precision(0)
     assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    rows = a[0] - a[0].min()
     for x, y in ((a[2], b[2]), (a[3], b[3])):
-        err = np.abs(x - y).max() / np.abs(x).max()
+        d = np.zeros(rows.max() + 1)
+        v = np.zeros(rows.max() + 1)
+        np.maximum.at(d, rows, np.abs(x - y))
+        np.maximum.at(v, rows, np.abs(x))
+        err = (d[v > 0] / v[v > 0]).max()
         assert 0 < err < TOL_ROWS, err  # > 0: the FP32 path did run
 
 
