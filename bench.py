@@ -342,6 +342,8 @@ def main():
     ap.add_argument("--panels", type=int, default=0, help="use only the leading N panels (profiling)")
     ap.add_argument("--kernels-only", action="store_true",
                     help="only the warm-up and timed steps (for profiler launch lists)")
+    ap.add_argument("--form", default="plain", choices=["plain", "chosen"],
+                    help="with --kernels-only: the form the steps run in (chosen = FP32 level sums)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -377,6 +379,8 @@ def main():
                                                D["rts"], D["rps"], D["tcx"], D["tcxrow"], D["tcxi"], W["nquad"], 1.4,
                                                30, out, stream=stream.cuda_stream, sync=False, want_hist=hist)
 
+    if args.kernels_only and args.form == "chosen":
+        qol.qol_set_sum_precision(1)
     hist = step(hist=True)
     for _ in range(max(0, args.warmup - 1)):
         step()
