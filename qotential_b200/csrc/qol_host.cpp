@@ -419,20 +419,56 @@ void xlate_schedule(int L, int lanes, std::vector<uint32_t>& tab, int& steps, st
   std::vector<int> ord(pieces.size());
   for (size_t i = 0; i < ord.size(); ++i) ord[i] = (int)i;
   std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return pieces[a].cost > pieces[b].cost; });
-  std::vector<std::vector<uint32_t>> lane(lanes);
+  std::vector<std::vector<int>> lanep(lanes); /* pieces of each lane, in order */
   std::vector<int> load(lanes, 0);
   for (int pi : ord) {
     int best = 0;
     for (int q = 1; q < lanes; ++q)
       if (load[q] < load[best]) best = q;
     load[best] += pieces[pi].cost;
-    lane[best].insert(lane[best].end(), pieces[pi].terms.begin(), pieces[pi].terms.end());
+    lanep[best].push_back(pi);
   }
   steps = 0;
   for (int q = 0; q < lanes; ++q) steps = std::max(steps, load[q]);
   tab.assign((size_t)steps * lanes, 0u);
-  for (int q = 0; q < lanes; ++q)
-    for (size_t s2 = 0; s2 < lane[q].size(); ++s2) tab[s2 * lanes + q] = lane[q][s2];
+  /* Order of the terms inside each piece (any order sums the same terms): at
+   * every step the 8 lanes of a quarter-warp should read M entries (14 doubles
+   * apart, so 16-byte bank group 7 em + k mod 8) with distinct em mod 8 or the
+   * same em, and R(x) entries (2 doubles apart) with distinct ex mod 8 or the
+   * same ex; greedy per step, lanes in order, fewest clashes first (an M clash
+   * costs its 6 loads, an R(x) clash 1), ties to the earlier term. */
+  for (int g0 = 0; g0 < lanes; g0 += 8) {
+    const int g1 = std::min(lanes, g0 + 8);
+    std::vector<int> pc(lanes, 0);                /* current piece of the lane */
+    std::vector<std::vector<uint32_t>> rem(lanes); /* its terms not yet placed */
+    for (int q = g0; q < g1; ++q)
+      if (!lanep[q].empty()) rem[q] = pieces[lanep[q][0]].terms;
+    for (int s2 = 0; s2 < steps; ++s2) {
+      std::vector<uint32_t> chosen;
+      for (int q = g0; q < g1; ++q) {
+        if (rem[q].empty()) continue; /* this lane is done */
+        int bi = 0, bc = 1 << 30;
+        for (int c = 0; c < (int)rem[q].size(); ++c) {
+          const uint32_t em = rem[q][c] & 255, ex = (rem[q][c] >> 8) & 255;
+          int cost = 0;
+          for (uint32_t w : chosen) {
+            const uint32_t em2 = w & 255, ex2 = (w >> 8) & 255;
+            if (em2 != em && (em2 & 7) == (em & 7)) cost += 6;
+            if (ex2 != ex && (ex2 & 7) == (ex & 7)) cost += 1;
+          }
+          if (cost < bc) { bc = cost; bi = c; }
+        }
+        uint32_t w = rem[q][bi] & ~(1u << 30);
+        rem[q].erase(rem[q].begin() + bi);
+        if (rem[q].empty()) { /* the piece's last term flushes it; then the next piece */
+          w |= 1u << 30;
+          if (++pc[q] < (int)lanep[q].size()) rem[q] = pieces[lanep[q][pc[q]]].terms;
+        }
+        chosen.push_back(w);
+        tab[(size_t)s2 * lanes + q] = w;
+      }
+    }
+  }
 }
 
 } // namespace qolh
