@@ -438,22 +438,34 @@ def main():
         h_in = (W["sx"], W["snx"], W["sw"], W["rts"], W["rps"], W["tcx"], W["tcxrow"], W["tcxi"])
         h2d = sum(a.nbytes for a in h_in)
         d2h = nnz * 16  # sparsevs + sparsevd; the COO indices are filled on host threads
-        reps = min(2, args.steps)
+        # caller-allocated outputs reused across calls, as a Fortran caller of the C ABI passes them;
+        # one untimed call maps their pages
+        outs = tuple(np.empty(nnz, dt) for dt in (np.int64, np.int64, np.float64, np.float64))
+
+        def call(o):
+            return qol.qol_getnearquad_lap_rrq(W["npan"], W["nterms"], hd, nq, W["npan"] * hd, W["sx"], W["snx"],
+                                               W["sw"], W["rts"], W["rps"], W["pairs"], W["tcx"], W["tcxrow"],
+                                               W["tcxi"], nq, 1.4, 30, out=o)
+
+        call(outs)
+        reps = max(2, min(3, args.steps))
         times, host_ms = [], []
         hms = np.zeros(7)
         L.qol_kernel_times(C.c_int(1), None, None)
         for _ in range(reps):
             t0 = time.perf_counter()
-            r = qol.qol_getnearquad_lap_rrq(W["npan"], W["nterms"], hd, nq, W["npan"] * hd, W["sx"], W["snx"],
-                                            W["sw"], W["rts"], W["rps"], W["pairs"], W["tcx"], W["tcxrow"],
-                                            W["tcxi"], nq, 1.4, 30)
+            call(outs)
             times.append(time.perf_counter() - t0)
             L.qol_last_host_times(C.c_void_p(hms.ctypes.data))
             host_ms.append([round(float(x), 2) for x in hms])
-            del r
         kms = np.zeros(9)
         L.qol_kernel_times(C.c_int(-1), C.c_void_p(kms.ctypes.data), None)
         L.qol_kernel_times(C.c_int(0), None, None)
+        del outs
+        t0 = time.perf_counter()  # the same call with fresh outputs (the wrapper allocates zeroed arrays)
+        r = call(None)
+        t_fresh = time.perf_counter() - t0
+        del r
         best = int(np.argmin(times))
         e2e = {"value": W["pairs"] / times[best], "unit": "pairs/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h),
@@ -461,9 +473,12 @@ def main():
                                     "host_tasks_done", "return", "indices_filled"], host_ms[best])),
                "device_ms": round(float(kms.sum()) / reps, 2),
                "device_phase_ms": [round(float(x) / reps, 2) for x in kms],
-               "note": "qol_getnearquad_lap_rrq with host (numpy) buffers: inputs copied in, the COO values "
-                       "copied out through pinned staging overlapping the chunked compute, the COO indices "
-                       "filled on host threads from tcxrow/tcxi meanwhile"}
+               "fresh_outputs": {"value": W["pairs"] / t_fresh, "ms": round(t_fresh * 1e3, 2)},
+               "note": "qol_getnearquad_lap_rrq with host (numpy) buffers, best of the timed calls: inputs "
+                       "copied in, the COO values copied out through pinned staging overlapping the chunked "
+                       "compute, the COO indices filled on host threads from tcxrow/tcxi meanwhile; outputs "
+                       "caller-allocated and reused across calls (fresh_outputs: the wrapper allocating zeroed "
+                       "arrays in the call, whose first-touch page faults the host pays inside it)"}
     chosen = None
     if rank == 0 and world == 1 and not args.no_chosen:
         chosen = {"order12": forms_compare(W, args.steps, 2, D, out)}

@@ -146,11 +146,15 @@ def qol_rrq(tx, sx, snx, sw, rts, rps, order, nquad, orderff, distff=1.4, exteri
 
 
 def qol_getnearquad_lap_rrq(npan, nterms, hdim, nquad, nsrc, sx, snx, sw, rts, rps, ntcx, tcx, tcxrow, tcxi,
-                            orderff, distff, iside, isimd=0, nnz=None, timeinfo=None):
+                            orderff, distff, iside, isimd=0, nnz=None, timeinfo=None, out=None):
     """[sparsei, sparsej, sparsevs, sparsevd, timeinfo] (matlab/qol_getnearquad_lap_rrq_mex.m).
 
     tcxrow/tcxi are 1-based; the COO output follows the reference's order
-    (tcxi(k)-1)*hdim + (j-1)*m_k + i."""
+    (tcxi(k)-1)*hdim + (j-1)*m_k + i.  out=(sparsei, sparsej, sparsevs,
+    sparsevd), contiguous int64/int64/float64/float64 arrays of nnz entries,
+    are filled in place and returned (the C ABI's caller-allocated outputs, as
+    a Fortran caller passes them; entries past the used ones are zeroed);
+    without it fresh zeroed arrays are allocated."""
     tcxi = _i(tcxi)
     if hdim != nterms * (nterms + 1) // 2 or npan * hdim != nsrc:
         raise QolError(1, "The panel order, hdim, npan, and nsrc are inconsistent.")
@@ -160,8 +164,16 @@ def qol_getnearquad_lap_rrq(npan, nterms, hdim, nquad, nsrc, sx, snx, sw, rts, r
     nnz = need if nnz is None else int(nnz)
     if need > nnz:
         raise QolError(2, "nnz is too small for the requested panel-target interactions.")
-    si = np.zeros(nnz, np.int64); sj = np.zeros(nnz, np.int64)
-    vs = np.zeros(nnz); vd = np.zeros(nnz)
+    if out is None:
+        si = np.zeros(nnz, np.int64); sj = np.zeros(nnz, np.int64)
+        vs = np.zeros(nnz); vd = np.zeros(nnz)
+    else:
+        si, sj, vs, vd = out
+        for a, dt in ((si, np.int64), (sj, np.int64), (vs, np.float64), (vd, np.float64)):
+            if not isinstance(a, np.ndarray) or a.dtype != dt or not a.flags.c_contiguous or a.size != nnz:
+                raise QolError(1, "out must be four contiguous arrays (int64, int64, float64, float64) of nnz entries.")
+        for a in (si, sj, vs, vd):
+            a[need:] = 0
     ti = np.zeros(20) if timeinfo is None else _f(timeinfo, 20).copy()
     rc = lib().qol_getnearquad_lap_rrq(
         i64(npan), i64(nterms), i64(hdim), i64(nquad), i64(nsrc), _vp(_f(sx, 3 * nsrc)), _vp(_f(snx, 3 * nsrc)),

@@ -84,3 +84,19 @@ def test_no_cpu_fallback(qol):
     with pytest.raises(qol.QolError) as e:
         qol.qol_rrq(P["sx"][:3], P["sx"][:6], P["snx"][:6], P["sw"][:6], P["rts"][:6], P["rps"][:6], 3, 5, 5)
     assert e.value.code == 5
+
+
+def test_getnearquad_out_checked(qol):
+    """caller-allocated outputs: four contiguous int64/int64/float64/float64
+    arrays of nnz entries, else QolError(1) before any device work"""
+    npan, nterms, hd = 2, 3, 6
+    sx = np.zeros((npan * hd, 3))
+    args = dict(npan=npan, nterms=nterms, hdim=hd, nquad=5, nsrc=npan * hd, sx=sx, snx=sx, sw=np.ones(npan * hd),
+                rts=sx, rps=sx, ntcx=3, tcx=np.zeros((3, 3)), tcxrow=np.array([1, 2, 3]), tcxi=np.array([1, 3, 4]),
+                orderff=5, distff=1.4, iside=30)
+    good = (np.zeros(18, np.int64), np.zeros(18, np.int64), np.zeros(18), np.zeros(18))
+    for bad in ((good[0].astype(np.int32),) + good[1:], good[:2] + (np.zeros(17),) + good[3:],
+                good[:3] + (np.zeros((18, 2))[:, 0],)):
+        with pytest.raises(qol.QolError) as e:
+            qol.qol_getnearquad_lap_rrq(out=bad, **args)
+        assert e.value.code == 1

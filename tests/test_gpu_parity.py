@@ -150,6 +150,15 @@ def test_host_entry_chunks_match_device_entry(qol):
     for h, d in zip((si, sj, vs, vd), ref):
         assert h[:need].tobytes() == d.tobytes()
         assert not h[need:].any()
+    # caller-allocated outputs holding stale contents: filled in place, the same bytes
+    mine = (np.full(need + 7, -5, np.int64), np.full(need + 7, -5, np.int64), np.full(need + 7, np.nan),
+            np.full(need + 7, np.nan))
+    r = qol.qol_getnearquad_lap_rrq(npan, nterms, hd, nq, npan * hd, P["sx"], P["snx"], P["sw"], P["rts"], P["rps"],
+                                    tcxrow.size, tcx, tcxrow, tcxi, nq, 1.4, 30, nnz=need + 7, out=mine)
+    for h, m, d in zip(r[:4], mine, ref):
+        assert h is m
+        assert h[:need].tobytes() == d.tobytes()
+        assert not h[need:].any()
 
 
 def test_grf_identity_gpu(qol, orc):
