@@ -227,7 +227,7 @@ int order_tables(int nterms, int orderff, int nquad, OrderCache** out) {
  * belongs to phase ph[k] (-1: none) */
 struct Timing {
   std::vector<cudaEvent_t> ev;
-  std::vector<int> ph;
+  std::vector<int> ph, sid; /* phase that starts at the event, stream index */
   bool on = false;
 };
 
@@ -236,9 +236,12 @@ struct Timing {
 void finish_timing(Timing& tm, double* timeinfo) {
   if (!tm.on) return;
   double ms[QOL_NPHASE] = {};
-  for (size_t k = 0; k + 1 < tm.ev.size(); ++k) {
+  for (size_t k = 0; k < tm.ev.size(); ++k) { /* a phase ends at the next event on its stream */
+    if (tm.ph[k] < 0) continue;
+    size_t k2 = k + 1;
+    while (k2 < tm.ev.size() && tm.sid[k2] != tm.sid[k]) ++k2;
     float t = 0.f;
-    if (tm.ph[k] >= 0 && cudaEventElapsedTime(&t, tm.ev[k], tm.ev[k + 1]) == cudaSuccess) ms[tm.ph[k]] += t;
+    if (k2 < tm.ev.size() && cudaEventElapsedTime(&t, tm.ev[k], tm.ev[k2]) == cudaSuccess) ms[tm.ph[k]] += t;
   }
   if (timeinfo) {
     timeinfo[0] += 1e-3 * ms[0];                   /* patch levels */
@@ -252,6 +255,7 @@ void finish_timing(Timing& tm, double* timeinfo) {
   for (cudaEvent_t e : tm.ev) cudaEventDestroy(e);
   tm.ev.clear();
   tm.ph.clear();
+  tm.sid.clear();
   tm.on = false;
 }
 
@@ -264,11 +268,24 @@ struct Job {
   double *vs, *vd, *omega, *ialpha;
   long long *si, *sj;
   const double* chart;
-  /* optional: the per-pair phase over these panel chunks (boundaries, first 0,
-   * last npan), after_chunk(c) once chunk c's values are queued */
+  /* optional: the pipeline after classification over these panel chunks
+   * (boundaries, first 0, last npan), alternating between the caller's
+   * stream and a second one; after_chunk(c, s) once chunk c's values are
+   * queued on stream s */
   const std::vector<long long>* chunk_pan;
-  std::function<void(int)> after_chunk;
+  std::function<void(int, cudaStream_t)> after_chunk;
 };
+
+/* the second stream of chunked calls, one per device, created on first use */
+int aux_stream(cudaStream_t* out) {
+  static cudaStream_t s[64] = {};
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(QOL_ERR_CUDA, "device ordinal %d out of range", dev);
+  if (!s[dev]) CK(cudaStreamCreateWithFlags(&s[dev], cudaStreamNonBlocking));
+  *out = s[dev];
+  return 0;
+}
 
 int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* hist_out, std::vector<int>* grp_out,
                  int* cnt_out) {
@@ -320,13 +337,15 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
   CK(cudaMemsetAsync(G.off, 0, sizeof(int) * (size_t)npan * 8, st));
   Timing tm;
   tm.on = timeinfo || g_ktime_on;
-  auto rec = [&](int phase) {
+  cudaStream_t st2 = st; /* chunked calls: odd chunks run here */
+  auto rec = [&](int phase, int sidx = 0) {
     if (!tm.on) return;
     cudaEvent_t e;
     if (cudaEventCreate(&e) != cudaSuccess) return;
-    cudaEventRecord(e, st);
+    cudaEventRecord(e, sidx ? st2 : st);
     tm.ev.push_back(e);
     tm.ph.push_back(phase);
+    tm.sid.push_back(sidx);
   };
   rec(0);
   CK(qol_launch_levels(T, J.P, W, npan, st));
@@ -352,33 +371,57 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
   R.pair = g_arena2.take<int2>((size_t)std::max<long long>(nrrq, 1));
   OutCOO O{};
   O.vs = J.vs; O.vd = J.vd; O.omega = J.omega; O.subtract_naive = J.subtract_naive;
-  rec(2);
-  CK(qol_launch_direct(T, J.P, J.Q, W, G, O, npan, st));
-  rec(3);
-  if (nrrq > 0) {
-    CK(qol_launch_rrq_pairs(T, J.Q, G, R, npan, st));
-    CK(qol_launch_rrq_panel(T, J.P, G, R, npan, J.chart, st));
+  /* one pass over all panels, or (host entry) panel chunks whose every phase
+   * runs before the next chunk's, so that chunk c's values are final early
+   * and leave the GPU while later chunks compute */
+  const bool chunked = J.chunk_pan != nullptr;
+  if (!chunked) {
+    rec(2);
+    CK(qol_launch_direct(T, J.P, J.Q, W, G, O, npan, st));
+    rec(3);
+    if (nrrq > 0) CK(qol_launch_rrq_panel(T, J.P, G, R, npan, J.chart, st));
   }
-  const int nch = J.chunk_pan ? (int)J.chunk_pan->size() - 1 : 1;
+  if (nrrq > 0) CK(qol_launch_rrq_pairs(T, J.Q, G, R, npan, st));
+  const int nch = chunked ? (int)J.chunk_pan->size() - 1 : 1;
+  cudaEvent_t fork = nullptr, join = nullptr;
+  if (chunked && nch > 1) { /* a chunk's kernels fill the SMs the other's tail leaves idle */
+    if ((rc = aux_stream(&st2))) return rc;
+    CK(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+    CK(cudaEventRecord(fork, st));
+    CK(cudaStreamWaitEvent(st2, fork, 0));
+  }
   for (int c = 0; c < nch; ++c) {
-    const long long a = J.chunk_pan ? (*J.chunk_pan)[c] : 0, b = J.chunk_pan ? (*J.chunk_pan)[c + 1] : npan;
+    const long long a = chunked ? (*J.chunk_pan)[c] : 0, b = chunked ? (*J.chunk_pan)[c + 1] : npan;
+    const int si = (c & 1) && st2 != st ? 1 : 0;
+    const cudaStream_t sc = si ? st2 : st;
     R.plo = (int)a; R.phi = (int)b;
-    R.glo = J.chunk_pan ? off_h[a] : 0;
-    R.ghi = J.chunk_pan ? off_h[b] : nrrq;
+    R.glo = chunked ? off_h[a] : 0;
+    R.ghi = chunked ? off_h[b] : nrrq;
+    if (chunked && b > a) {
+      rec(2, si);
+      CK(qol_launch_direct(T, J.P, J.Q, W, G, O, (int)(b - a), sc, (int)a));
+      rec(3, si);
+      if (R.ghi > R.glo) CK(qol_launch_rrq_panel(T, J.P, G, R, (int)(b - a), J.chart, sc));
+    }
     if (R.ghi > R.glo) {
-      rec(4);
-      CK(qol_launch_rrq_ssq(T, J.Q, G, R, st));
-      rec(5);
-      CK(qol_launch_rrq_geom(T, J.Q, G, R, J.exterior, st));
-      rec(6);
-      CK(qol_launch_rrq_moments(T, J.Q, G, R, st));
-      rec(7);
-      CK(qol_launch_rrq_apply(T, J.P, J.Q, G, R, O, st));
+      rec(4, si);
+      CK(qol_launch_rrq_ssq(T, J.Q, G, R, sc));
+      rec(5, si);
+      CK(qol_launch_rrq_geom(T, J.Q, G, R, J.exterior, sc));
+      rec(6, si);
+      CK(qol_launch_rrq_moments(T, J.Q, G, R, sc));
+      rec(7, si);
+      CK(qol_launch_rrq_apply(T, J.P, J.Q, G, R, O, sc));
     }
-    if (J.after_chunk) {
-      rec(-1);
-      J.after_chunk(c);
-    }
+    rec(-1, si);
+    if (J.after_chunk) J.after_chunk(c, sc);
+  }
+  if (join) { /* the caller's stream waits for the second one */
+    CK(cudaEventRecord(join, st2));
+    CK(cudaStreamWaitEvent(st, join, 0));
+    cudaEventDestroy(fork);
+    cudaEventDestroy(join);
   }
   rec(8);
   if (J.si) CK(qol_launch_coo_index(T, J.Q, J.si, J.sj, npan, st));
@@ -1006,8 +1049,8 @@ int qol_getnearquad_lap_rrq(qol_int npan, qol_int nterms, qol_int hdim, qol_int 
       J.vs = dval; J.vd = dval + nout;
       J.si = nullptr; J.sj = nullptr;
       J.chunk_pan = &cb;
-      J.after_chunk = [&](int c) {
-        if (cudaEventRecord(cev[c], st) == cudaSuccess) prog.set(c + 1);
+      J.after_chunk = [&](int c, cudaStream_t sc) {
+        if (cudaEventRecord(cev[c], sc) == cudaSuccess) prog.set(c + 1);
         else cerr = 1;
       };
       out = run_pipeline(J, st, timeinfo, nullptr, nullptr, nullptr);

@@ -318,8 +318,8 @@ __global__ void __launch_bounds__(128) k_level_subs(OrderTab T, LevelWS W, int n
  * columns 8 NB (w&3) .., NB column blocks of 8 */
 template <int NB>
 __global__ void __launch_bounds__(256, 2) k_direct(OrderTab T, PanelIn P, PairIn Q, LevelWS W, PairWS G,
-                                                   OutCOO O) {
-  const int pan = blockIdx.x, l = blockIdx.y;
+                                                   OutCOO O, int pan0) {
+  const int pan = pan0 + blockIdx.x, l = blockIdx.y; /* panels pan0 .. pan0 + gridDim.x - 1 */
   if (l >= T.nlevel) return;
   const int cntl = G.cnt[(size_t)pan * 8 + l + 1];
   if (cntl == 0) return;
@@ -490,8 +490,8 @@ __device__ __forceinline__ void mma_tf32(float* d, const unsigned* a, unsigned b
  * (w&3) NB .. +NB-1 */
 template <int NB>
 __global__ void __launch_bounds__(256, 2) k_direct_tf32(OrderTab T, PanelIn P, PairIn Q, LevelWS W, PairWS G,
-                                                        OutCOO O) {
-  const int pan = blockIdx.x, l = blockIdx.y;
+                                                        OutCOO O, int pan0) {
+  const int pan = pan0 + blockIdx.x, l = blockIdx.y; /* panels pan0 .. pan0 + gridDim.x - 1 */
   if (l >= T.nlevel) return;
   const int cntl = G.cnt[(size_t)pan * 8 + l + 1];
   if (cntl == 0) return;
@@ -749,7 +749,7 @@ __global__ void __launch_bounds__(NT, 1) k_rrq_panel(OrderTab T, PanelIn P, Pair
                                                                 const double* chart /* nullable */) {
   cg::cluster_group cl = cg::this_cluster();
   const int rank = (int)cl.block_rank();
-  const int pan = blockIdx.x / CS;
+  const int pan = R.plo + (int)(blockIdx.x / CS); /* panels R.plo .. R.plo + gridDim.x / CS - 1 */
   if (G.cnt[(size_t)pan * 8 + T.nlevel + 1] == 0 && !R.all_panels) return; /* whole cluster */
   const int hd = T.hd, nq = T.nquad, nbd = 3 * nq, L = T.nterms;
   const int ncol = panel_ncol(hd, CS), c0 = min(hd, rank * ncol), c1 = min(hd, c0 + ncol), nc = c1 - c0;
@@ -1902,11 +1902,12 @@ cudaError_t qol_launch_classify(const OrderTab& T, const PairIn& Q, const LevelW
   return cudaGetLastError();
 }
 cudaError_t qol_launch_direct(const OrderTab& T, const PanelIn& P, const PairIn& Q, const LevelWS& W,
-                              const PairWS& G, const OutCOO& O, int npan, cudaStream_t st) {
+                              const PairWS& G, const OutCOO& O, int npan, cudaStream_t st, int pan0) {
+  if (npan <= 0) return cudaSuccess;
   dim3 grid(npan, T.nlevel);
   auto go = [&](auto kern, size_t smem) {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    kern<<<grid, 256, smem, st>>>(T, P, Q, W, G, O);
+    kern<<<grid, 256, smem, st>>>(T, P, Q, W, G, O, pan0);
   };
   const int nb = T.ncw / 32; /* the padded interpolation rows fix the column blocks */
   if (nb < 1 || nb > 5 || T.ncw != 32 * ((T.hd + 31) / 32)) return cudaErrorInvalidValue;

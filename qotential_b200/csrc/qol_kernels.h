@@ -84,7 +84,8 @@ cudaError_t qol_launch_levels(const OrderTab& T, const PanelIn& P, const LevelWS
 cudaError_t qol_launch_classify(const OrderTab& T, const PairIn& Q, const LevelWS& W, const PairWS& G, int npan,
                                 cudaStream_t st);
 cudaError_t qol_launch_direct(const OrderTab& T, const PanelIn& P, const PairIn& Q, const LevelWS& W,
-                              const PairWS& G, const OutCOO& O, int npan, cudaStream_t st);
+                              const PairWS& G, const OutCOO& O, int npan, cudaStream_t st,
+                              int pan0 = 0 /* first panel of the launch */);
 cudaError_t qol_launch_scan(int npan, int lev, const int* cnt, long long* off, cudaStream_t st);
 cudaError_t qol_launch_rrq_panel(const OrderTab& T, const PanelIn& P, const PairWS& G, const RRQWS& R, int npan,
                                  const double* chart, cudaStream_t st);
