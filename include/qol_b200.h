@@ -172,6 +172,37 @@ int qol_direct_farfield(qol_int nsrc, const double* sx, const double* snx, const
  * fits stay FP64.  qol_rrq_noalloc always uses FP64.  No counterpart in the
  * reference (all FP64). */
 int qol_set_sum_precision(int mode);
+/* Learned level selector (no counterpart in the reference; it stands in for
+ * the ball-test level walk of lap3dsdlpmat_levels_r64,
+ * patch_refine_mod.f90:516-551).  An MLP 8 -> 64 -> 64 -> 5 on geometry
+ * features of each (target, panel) pair predicts the level the plain walk
+ * gives (classes 0..3: direct sums on level 1..4; 4: RRQ).
+ * qol_selector_features: the 8 features (FP32, row-major ntcx x 8) and the
+ *   plain walk's level (1..5) of every near pair of a getnearquad input;
+ * qol_selector_grad: mean cross-entropy and its gradient over n samples with
+ *   weights w (QOL_SELECTOR_NW floats: W1 8x64, b1, W2 64x64, b2, W3 64x5, b3);
+ * qol_selector_train: Adam on the GPU, `epochs` passes over a shuffle seeded
+ *   by `seed`, batches of `batch` (a multiple of 256) samples; w in: initial,
+ *   out: trained; loss[e] the mean loss of epoch e;
+ * qol_selector_set: mode 1 makes the calls that follow use the selector with
+ *   w rounded to BF16 (FP32 accumulation): a prediction with softmax
+ *   probability >= conf of a direct level l is used when the target lies
+ *   outside every level-l sub-patch ball, an RRQ prediction when it lies
+ *   inside a ball of the finest level (else, and below conf, the plain walk
+ *   decides); mode 0 restores the plain walk;
+ * qol_selector_stats: accepted, low-confidence and check-failed pairs since
+ *   the last call. */
+#define QOL_SELECTOR_NW 5061
+int qol_selector_features(qol_int npan, qol_int nterms, qol_int nquad, const double* sx, const double* snx,
+                          const double* sw, const double* rts, const double* rps, qol_int ntcx, const double* tcx,
+                          const qol_int* tcxrow, const qol_int* tcxi, qol_int orderff, double distff, float* feat,
+                          signed char* level);
+int qol_selector_grad(qol_int n, const float* feat, const signed char* label, const float* w, float* grad,
+                      double* loss);
+int qol_selector_train(qol_int n, const float* feat, const signed char* label, qol_int epochs, qol_int batch,
+                       double lr, unsigned long long seed, float* w, double* loss);
+int qol_selector_set(int mode, const float* w, double conf);
+int qol_selector_stats(qol_int* counts3);
 /* Wall-clock milestones (ms from the start) of the last
  * qol_getnearquad_lap_rrq call: [0] inputs queued, [1] all panel chunks
  * queued, [2] all value copies queued, [3] values landed in pinned staging,

@@ -16,6 +16,8 @@ __all__ = [
     "lib", "QolError", "qol_simplex_precomp", "qol_build_patch_levels", "qol_lap3dsdlpmat_levels",
     "qol_clear_patch_levels", "qol_clear_patch_levels_all", "qol_rrq", "qol_getnearquad_lap_rrq",
     "qol_getnearquad_lap_rrq_dev", "qol_grf_near", "qol_direct_farfield", "qol_set_sum_precision",
+    "SELECTOR_NW", "qol_selector_features", "qol_selector_grad", "qol_selector_train", "qol_selector_set",
+    "qol_selector_stats",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -244,3 +246,77 @@ def qol_set_sum_precision(mode):
     """0: FP64 level sums (default, the drop-in); 1: FP32 level sums on the
     3xTF32 tensor path with FP64 accumulation across tiles (precision variant)."""
     _check(lib().qol_set_sum_precision(C.c_int(int(mode))))
+
+
+# ---------------- learned level selector (no reference counterpart) ----------------
+SELECTOR_NW = 5061  # W1 8x64, b1 64, W2 64x64, b2 64, W3 64x5, b3 5
+
+
+def qol_selector_features(npan, nterms, nquad, sx, snx, sw, rts, rps, tcx, tcxrow, tcxi, orderff, distff=1.4):
+    """(features float32 (ntcx, 8), plain-walk level int8 (ntcx,), 1..5) of every
+    near pair of a getnearquad input; the selector's classes are level - 1."""
+    tcxi = _i(tcxi)
+    tcxrow = _i(tcxrow)
+    ntcx = tcxrow.size
+    nsrc = int(npan) * (int(nterms) * (int(nterms) + 1) // 2)
+    feat = np.zeros((ntcx, 8), np.float32)
+    lev = np.zeros(ntcx, np.int8)
+    rc = lib().qol_selector_features(i64(npan), i64(nterms), i64(nquad), _vp(_f(sx, 3 * nsrc)),
+                                     _vp(_f(snx, 3 * nsrc)), _vp(_f(sw, nsrc)), _vp(_f(rts, 3 * nsrc)),
+                                     _vp(_f(rps, 3 * nsrc)), i64(ntcx), _vp(_f(tcx, 3 * ntcx)), _vp(tcxrow),
+                                     _vp(tcxi), i64(orderff), C.c_double(distff), _vp(feat), _vp(lev))
+    _check(rc)
+    return feat, lev
+
+
+def _sel_args(feat, label):
+    feat = np.ascontiguousarray(feat, dtype=np.float32).reshape(-1, 8)
+    label = np.ascontiguousarray(label, dtype=np.int8).reshape(-1)
+    if label.size != feat.shape[0]:
+        raise QolError(8, "one label per feature row")
+    return feat, label
+
+
+def qol_selector_grad(feat, label, w):
+    """(mean cross-entropy, its gradient) of the MLP with weights w over the samples."""
+    feat, label = _sel_args(feat, label)
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    g = np.zeros(SELECTOR_NW, np.float32)
+    loss = np.zeros(1)
+    _check(lib().qol_selector_grad(i64(label.size), _vp(feat), _vp(label), _vp(w), _vp(g), _vp(loss)))
+    return float(loss[0]), g
+
+
+def qol_selector_init(seed=0):
+    """He-initialised weights (zero biases), seeded."""
+    rng = np.random.default_rng(seed)
+    w = np.zeros(SELECTOR_NW, np.float32)
+    w[0:512] = rng.normal(0.0, np.sqrt(2.0 / 8), 512)
+    w[576:576 + 4096] = rng.normal(0.0, np.sqrt(2.0 / 64), 4096)
+    w[4736:4736 + 320] = rng.normal(0.0, np.sqrt(1.0 / 64), 320)
+    return w
+
+
+def qol_selector_train(feat, label, w=None, epochs=20, batch=16384, lr=3e-3, seed=0):
+    """(trained weights, mean loss per epoch): Adam on the GPU."""
+    feat, label = _sel_args(feat, label)
+    w = qol_selector_init(seed) if w is None else np.array(w, dtype=np.float32)
+    loss = np.zeros(int(epochs))
+    _check(lib().qol_selector_train(i64(label.size), _vp(feat), _vp(label), i64(epochs), i64(batch), C.c_double(lr),
+                                    C.c_ulonglong(seed), _vp(w), _vp(loss)))
+    return w, loss
+
+
+def qol_selector_set(mode, w=None, conf=0.9):
+    """mode 1: the calls that follow take their pair levels from the selector
+    (weights w rounded to BF16, softmax confidence >= conf, ball check at the
+    predicted level); mode 0: the plain ball-test walk."""
+    wp = None if w is None else np.ascontiguousarray(w, dtype=np.float32)
+    _check(lib().qol_selector_set(C.c_int(int(mode)), _vp(wp), C.c_double(conf)))
+
+
+def qol_selector_stats():
+    """{accepted, low_confidence, check_failed} pair counts since the last call."""
+    c = np.zeros(3, np.int64)
+    _check(lib().qol_selector_stats(_vp(c)))
+    return {"accepted": int(c[0]), "low_confidence": int(c[1]), "check_failed": int(c[2])}

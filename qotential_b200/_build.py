@@ -5,7 +5,7 @@ import subprocess
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libqol_b200.so")
-SOURCES = ["qol_kernels.cu", "qol_api.cu", "qol_host.cpp", "qol_noalloc.cu"]
+SOURCES = ["qol_kernels.cu", "qol_api.cu", "qol_host.cpp", "qol_noalloc.cu", "qol_selector.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "--expt-relaxed-constexpr", "--expt-extended-lambda", "-Xcompiler", "-fPIC"]
 

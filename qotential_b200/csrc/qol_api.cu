@@ -95,6 +95,12 @@ Arena g_arena, g_arena2, g_arena_io, g_arena_grf; /* pipeline, per-pair RRQ stor
 /* per-phase device milliseconds of the pipeline (diagnostics) */
 int g_ktime_on = 0;
 int g_sum_precision = 0; /* 0 FP64 (the drop-in), 1 FP32 level sums */
+/* learned level selector: off (0) or on (1), its BF16-rounded weights on the
+ * device, the confidence threshold, and the decision counters of the calls */
+int g_sel_mode = 0;
+float g_sel_conf = 0.9f;
+float* g_sel_w = nullptr;
+unsigned long long* g_sel_cnt = nullptr; /* accepted, low confidence, check failed, pairs */
 double g_ktime[QOL_NPHASE] = {};
 long long g_kcalls = 0;
 cudaStream_t g_stream = nullptr;
@@ -350,7 +356,12 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
   rec(0);
   CK(qol_launch_levels(T, J.P, W, npan, st));
   rec(1);
-  CK(qol_launch_classify(T, J.Q, W, G, npan, st));
+  if (g_sel_mode == 1 && g_sel_w) { /* confident, checked predictions first; the plain walk for the rest */
+    CK(qol_launch_sel_infer(T, J.P, J.Q, W, G, npan, g_sel_w, g_sel_conf, g_sel_cnt, st));
+    CK(qol_launch_classify(T, J.Q, W, G, npan, st, 1));
+  } else {
+    CK(qol_launch_classify(T, J.Q, W, G, npan, st));
+  }
   CK(qol_launch_scan(npan, T.nlevel + 1, G.cnt, rrq_off, st));
   /* RRQ pair offsets per panel (all of them when the per-pair phase is chunked) */
   std::vector<long long> off_h(J.chunk_pan ? npan + 1 : 1);
@@ -708,6 +719,241 @@ int qol_set_sum_precision(int mode) {
   std::lock_guard<std::recursive_mutex> g(g_mu);
   if (mode != 0 && mode != 1) return fail(QOL_ERR_ARG, "sum precision must be 0 (FP64) or 1 (FP32 level sums)");
   g_sum_precision = mode;
+  return 0;
+}
+
+/* ---------------- learned level selector (no reference counterpart) ---------------- */
+static_assert(QOL_SELECTOR_NW == QOL_SEL_NW, "selector weight count");
+/* features and plain-walk levels of every near pair (the training data) */
+int qol_selector_features(qol_int npan, qol_int nterms, qol_int nquad, const double* sx, const double* snx,
+                          const double* sw, const double* rts, const double* rps, qol_int ntcx, const double* tcx,
+                          const qol_int* tcxrow, const qol_int* tcxi, qol_int orderff, double distff, float* feat,
+                          signed char* level) {
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  if (!sx || !snx || !sw || !rts || !rps || !tcx || !tcxrow || !tcxi || !feat || !level || npan <= 0 || ntcx < 0)
+    return fail(QOL_ERR_ARG, "qol_selector_features: null argument or bad size");
+  if (tcxi[0] != 1 || tcxi[npan] != ntcx + 1) return fail(QOL_ERR_LAYOUT, "tcxi must be one-based and cover tcx");
+  OrderCache* C = nullptr;
+  int rc = order_tables((int)nterms, (int)orderff, (int)nquad, &C);
+  if (rc) return rc;
+  OrderTab T = C->T;
+  T.dist = distff;
+  const int hd = T.hd;
+  const long long nsrc = (long long)npan * hd;
+  if ((rc = ensure_device())) return rc;
+  cudaStream_t st = g_stream;
+  std::vector<void*> bufs;
+  auto dal = [&](size_t bytes) -> void* {
+    void* p = nullptr;
+    if (cudaMalloc(&p, std::max<size_t>(bytes, 16)) != cudaSuccess) return nullptr;
+    bufs.push_back(p);
+    return p;
+  };
+  auto done = [&](int r) {
+    for (void* p : bufs) cudaFree(p);
+    return r;
+  };
+  double* dsx = (double*)dal(sizeof(double) * 3 * nsrc);
+  double* dsnx = (double*)dal(sizeof(double) * 3 * nsrc);
+  double* dsw = (double*)dal(sizeof(double) * nsrc);
+  double* drts = (double*)dal(sizeof(double) * 3 * nsrc);
+  double* drps = (double*)dal(sizeof(double) * 3 * nsrc);
+  double* dtcx = (double*)dal(sizeof(double) * 3 * std::max<qol_int>(ntcx, 1));
+  long long* drow = (long long*)dal(sizeof(long long) * std::max<qol_int>(ntcx, 1));
+  long long* dxi = (long long*)dal(sizeof(long long) * (npan + 1));
+  float* dfeat = (float*)dal(sizeof(float) * QOL_SEL_F * std::max<qol_int>(ntcx, 1));
+  LevelWS W{};
+  for (int l = 0; l < 4; ++l) {
+    W.node[l] = (double*)dal(sizeof(double) * (size_t)npan * T.n[l] * 7);
+    W.sub[l] = (double*)dal(sizeof(double) * (size_t)npan * T.nsub[l] * 4);
+  }
+  PairWS G{};
+  G.level = (signed char*)dal(std::max<qol_int>(ntcx, 1));
+  G.grp = (int*)dal(sizeof(int) * std::max<qol_int>(ntcx, 1));
+  G.cnt = (int*)dal(sizeof(int) * (size_t)npan * 8);
+  G.off = (int*)dal(sizeof(int) * (size_t)npan * 8);
+  for (void* p : bufs)
+    if (!p) return done(fail(QOL_ERR_CUDA, "qol_selector_features: device allocation failed"));
+  auto ck = [&](cudaError_t e) { return e == cudaSuccess ? 0 : fail(QOL_ERR_CUDA, "%s", cudaGetErrorString(e)); };
+  if ((rc = ck(cudaMemcpyAsync(dsx, sx, sizeof(double) * 3 * nsrc, cudaMemcpyHostToDevice, st))) ||
+      (rc = ck(cudaMemcpyAsync(dsnx, snx, sizeof(double) * 3 * nsrc, cudaMemcpyHostToDevice, st))) ||
+      (rc = ck(cudaMemcpyAsync(dsw, sw, sizeof(double) * nsrc, cudaMemcpyHostToDevice, st))) ||
+      (rc = ck(cudaMemcpyAsync(drts, rts, sizeof(double) * 3 * nsrc, cudaMemcpyHostToDevice, st))) ||
+      (rc = ck(cudaMemcpyAsync(drps, rps, sizeof(double) * 3 * nsrc, cudaMemcpyHostToDevice, st))) ||
+      (rc = ck(cudaMemcpyAsync(dtcx, tcx, sizeof(double) * 3 * ntcx, cudaMemcpyHostToDevice, st))) ||
+      (rc = ck(cudaMemcpyAsync(drow, tcxrow, sizeof(long long) * ntcx, cudaMemcpyHostToDevice, st))) ||
+      (rc = ck(cudaMemcpyAsync(dxi, tcxi, sizeof(long long) * (npan + 1), cudaMemcpyHostToDevice, st))) ||
+      (rc = ck(cudaMemsetAsync(G.cnt, 0, sizeof(int) * (size_t)npan * 8, st))))
+    return done(rc);
+  const PanelIn P{dsx, dsnx, dsw, drts, drps};
+  const PairIn Q{dtcx, drow, dxi};
+  if ((rc = ck(qol_launch_levels(T, P, W, (int)npan, st))) || (rc = ck(qol_launch_classify(T, Q, W, G, (int)npan, st))) ||
+      (rc = ck(qol_launch_sel_features(hd, P, Q, (int)npan, dfeat, st))) ||
+      (rc = ck(cudaMemcpyAsync(feat, dfeat, sizeof(float) * QOL_SEL_F * ntcx, cudaMemcpyDeviceToHost, st))) ||
+      (rc = ck(cudaMemcpyAsync(level, G.level, ntcx, cudaMemcpyDeviceToHost, st))) ||
+      (rc = ck(cudaStreamSynchronize(st))))
+    return done(rc);
+  return done(0);
+}
+
+namespace {
+/* device copies of a training set and the optimiser state */
+struct SelTrain {
+  float *feat = nullptr, *w = nullptr, *m = nullptr, *v = nullptr, *grad = nullptr, *slot = nullptr;
+  signed char* lab = nullptr;
+  int* idx = nullptr;
+  double* sloss = nullptr;
+  ~SelTrain() {
+    for (void* p : {(void*)feat, (void*)w, (void*)m, (void*)v, (void*)grad, (void*)slot, (void*)lab, (void*)idx,
+                    (void*)sloss})
+      if (p) cudaFree(p);
+  }
+};
+int sel_check(qol_int n, const float* feat, const signed char* label, const float* w) {
+  if (n <= 0 || !feat || !label || !w) return fail(QOL_ERR_ARG, "selector: null argument or empty set");
+  for (qol_int i = 0; i < n; ++i)
+    if (label[i] < 0 || label[i] >= QOL_SEL_C) return fail(QOL_ERR_ARG, "selector: labels must be 0..%d", QOL_SEL_C - 1);
+  return 0;
+}
+} // namespace
+
+/* mean cross-entropy gradient and loss over n samples (no update) */
+int qol_selector_grad(qol_int n, const float* feat, const signed char* label, const float* w, float* grad,
+                      double* loss) {
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  int rc = sel_check(n, feat, label, w);
+  if (rc) return rc;
+  if (!grad || !loss) return fail(QOL_ERR_ARG, "qol_selector_grad: null argument");
+  if ((rc = ensure_device())) return rc;
+  cudaStream_t st = g_stream;
+  const int nslot = (int)((n + 255) / 256);
+  SelTrain D;
+  std::vector<int> idx(n);
+  for (qol_int i = 0; i < n; ++i) idx[i] = (int)i;
+  auto ck = [&](cudaError_t e) { return e == cudaSuccess ? 0 : fail(QOL_ERR_CUDA, "%s", cudaGetErrorString(e)); };
+  if ((rc = ck(cudaMalloc(&D.feat, sizeof(float) * QOL_SEL_F * n))) || (rc = ck(cudaMalloc(&D.lab, n))) ||
+      (rc = ck(cudaMalloc(&D.idx, sizeof(int) * n))) || (rc = ck(cudaMalloc(&D.w, sizeof(float) * QOL_SEL_NW))) ||
+      (rc = ck(cudaMalloc(&D.grad, sizeof(float) * QOL_SEL_NW))) ||
+      (rc = ck(cudaMalloc(&D.slot, sizeof(float) * QOL_SEL_NW * (size_t)nslot))) ||
+      (rc = ck(cudaMalloc(&D.sloss, sizeof(double) * nslot))))
+    return rc;
+  std::vector<double> sl(nslot);
+  if ((rc = ck(cudaMemcpyAsync(D.feat, feat, sizeof(float) * QOL_SEL_F * n, cudaMemcpyHostToDevice, st))) ||
+      (rc = ck(cudaMemcpyAsync(D.lab, label, n, cudaMemcpyHostToDevice, st))) ||
+      (rc = ck(cudaMemcpyAsync(D.idx, idx.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st))) ||
+      (rc = ck(cudaMemcpyAsync(D.w, w, sizeof(float) * QOL_SEL_NW, cudaMemcpyHostToDevice, st))) ||
+      (rc = ck(qol_launch_sel_grad(D.feat, D.lab, D.idx, 0, n, D.w, D.slot, D.sloss, nslot, st))) ||
+      (rc = ck(qol_launch_sel_update(D.slot, nslot, 1.0f / (float)n, D.grad, D.w, nullptr, nullptr, 0.0f, 1, st))) ||
+      (rc = ck(cudaMemcpyAsync(grad, D.grad, sizeof(float) * QOL_SEL_NW, cudaMemcpyDeviceToHost, st))) ||
+      (rc = ck(cudaMemcpyAsync(sl.data(), D.sloss, sizeof(double) * nslot, cudaMemcpyDeviceToHost, st))) ||
+      (rc = ck(cudaStreamSynchronize(st))))
+    return rc;
+  double acc = 0.0;
+  for (double v : sl) acc += v;
+  *loss = acc / (double)n;
+  return 0;
+}
+
+/* Adam on the mean cross-entropy: epochs over a seeded shuffle, batches of
+ * `batch` samples (a multiple of 256); w holds the initial weights and
+ * receives the trained ones; loss[e] = mean loss seen during epoch e */
+int qol_selector_train(qol_int n, const float* feat, const signed char* label, qol_int epochs, qol_int batch, double lr,
+                       unsigned long long seed, float* w, double* loss) {
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  int rc = sel_check(n, feat, label, w);
+  if (rc) return rc;
+  if (epochs <= 0 || batch < 256 || batch % 256 || !(lr > 0.0) || !loss)
+    return fail(QOL_ERR_ARG, "qol_selector_train: epochs > 0, batch a positive multiple of 256, lr > 0");
+  if ((rc = ensure_device())) return rc;
+  cudaStream_t st = g_stream;
+  const int nslot = (int)(batch / 256);
+  SelTrain D;
+  auto ck = [&](cudaError_t e) { return e == cudaSuccess ? 0 : fail(QOL_ERR_CUDA, "%s", cudaGetErrorString(e)); };
+  if ((rc = ck(cudaMalloc(&D.feat, sizeof(float) * QOL_SEL_F * n))) || (rc = ck(cudaMalloc(&D.lab, n))) ||
+      (rc = ck(cudaMalloc(&D.idx, sizeof(int) * n))) || (rc = ck(cudaMalloc(&D.w, sizeof(float) * QOL_SEL_NW))) ||
+      (rc = ck(cudaMalloc(&D.m, sizeof(float) * QOL_SEL_NW))) ||
+      (rc = ck(cudaMalloc(&D.v, sizeof(float) * QOL_SEL_NW))) ||
+      (rc = ck(cudaMalloc(&D.slot, sizeof(float) * QOL_SEL_NW * (size_t)nslot))) ||
+      (rc = ck(cudaMalloc(&D.sloss, sizeof(double) * nslot))))
+    return rc;
+  if ((rc = ck(cudaMemcpyAsync(D.feat, feat, sizeof(float) * QOL_SEL_F * n, cudaMemcpyHostToDevice, st))) ||
+      (rc = ck(cudaMemcpyAsync(D.lab, label, n, cudaMemcpyHostToDevice, st))) ||
+      (rc = ck(cudaMemcpyAsync(D.w, w, sizeof(float) * QOL_SEL_NW, cudaMemcpyHostToDevice, st))) ||
+      (rc = ck(cudaMemsetAsync(D.m, 0, sizeof(float) * QOL_SEL_NW, st))) ||
+      (rc = ck(cudaMemsetAsync(D.v, 0, sizeof(float) * QOL_SEL_NW, st))))
+    return rc;
+  std::vector<int> idx(n);
+  for (qol_int i = 0; i < n; ++i) idx[i] = (int)i;
+  unsigned long long sm = seed;
+  auto next = [&]() { /* splitmix64 */
+    unsigned long long z = (sm += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+  };
+  std::vector<double> sl(nslot);
+  int it = 0;
+  for (qol_int e = 0; e < epochs; ++e) {
+    for (qol_int i = n - 1; i > 0; --i) std::swap(idx[i], idx[(qol_int)(next() % (unsigned long long)(i + 1))]);
+    if ((rc = ck(cudaMemcpyAsync(D.idx, idx.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st)))) return rc;
+    double eloss = 0.0;
+    for (qol_int b0 = 0; b0 < n; b0 += batch) {
+      const qol_int b1 = std::min<qol_int>(n, b0 + batch);
+      const int ns = (int)((b1 - b0 + 255) / 256);
+      if ((rc = ck(qol_launch_sel_grad(D.feat, D.lab, D.idx, b0, b1, D.w, D.slot, D.sloss, ns, st))) ||
+          (rc = ck(qol_launch_sel_update(D.slot, ns, 1.0f / (float)(b1 - b0), nullptr, D.w, D.m, D.v, (float)lr, ++it,
+                                         st))) ||
+          (rc = ck(cudaMemcpyAsync(sl.data(), D.sloss, sizeof(double) * ns, cudaMemcpyDeviceToHost, st))) ||
+          (rc = ck(cudaStreamSynchronize(st))))
+        return rc;
+      for (int q = 0; q < ns; ++q) eloss += sl[q];
+    }
+    loss[e] = eloss / (double)n;
+  }
+  if ((rc = ck(cudaMemcpy(w, D.w, sizeof(float) * QOL_SEL_NW, cudaMemcpyDeviceToHost)))) return rc;
+  return 0;
+}
+
+/* mode 0: plain ball-test walk; mode 1: the learned selector with weights w
+ * (FP32, used rounded to BF16) and confidence threshold conf in (0, 1] */
+int qol_selector_set(int mode, const float* w, double conf) {
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  if (mode == 0) { g_sel_mode = 0; return 0; }
+  if (mode != 1 || !w || !(conf > 0.0 && conf <= 1.0))
+    return fail(QOL_ERR_ARG, "qol_selector_set: mode 0 or 1, weights and a confidence in (0, 1]");
+  std::vector<float> wb(QOL_SEL_NW);
+  for (int i = 0; i < QOL_SEL_NW; ++i) { /* round to nearest even BF16 */
+    uint32_t u;
+    std::memcpy(&u, &w[i], 4);
+    if ((u & 0x7F800000u) != 0x7F800000u) u = (u + 0x7FFFu + ((u >> 16) & 1u)) & 0xFFFF0000u;
+    else u &= 0xFFFF0000u;
+    std::memcpy(&wb[i], &u, 4);
+  }
+  auto ck = [&](cudaError_t e) { return e == cudaSuccess ? 0 : fail(QOL_ERR_CUDA, "%s", cudaGetErrorString(e)); };
+  int rc = 0;
+  if (!g_sel_w && ((rc = ck(cudaMalloc(&g_sel_w, sizeof(float) * QOL_SEL_NW))) ||
+                   (rc = ck(cudaMalloc(&g_sel_cnt, sizeof(unsigned long long) * 4))) ||
+                   (rc = ck(cudaMemset(g_sel_cnt, 0, sizeof(unsigned long long) * 4)))))
+    return rc;
+  if ((rc = ck(cudaMemcpy(g_sel_w, wb.data(), sizeof(float) * QOL_SEL_NW, cudaMemcpyHostToDevice)))) return rc;
+  g_sel_mode = 1;
+  g_sel_conf = (float)conf;
+  return 0;
+}
+
+/* the selector's decisions since the last call: accepted, low confidence,
+ * check failed (the last two went to the plain walk); resets them */
+int qol_selector_stats(qol_int* counts3) {
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  if (!counts3) return fail(QOL_ERR_ARG, "null argument");
+  unsigned long long c[4] = {};
+  if (g_sel_cnt) {
+    if (cudaDeviceSynchronize() != cudaSuccess ||
+        cudaMemcpy(c, g_sel_cnt, sizeof(c), cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemset(g_sel_cnt, 0, sizeof(c)) != cudaSuccess)
+      return fail(QOL_ERR_CUDA, "selector counters");
+  }
+  for (int i = 0; i < 3; ++i) counts3[i] = (qol_int)c[i];
   return 0;
 }
 

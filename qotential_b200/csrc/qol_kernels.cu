@@ -85,7 +85,7 @@ void qol_upload_harm_coefs(const double* hb, const double* hc, const double* hcm
 /* ===================================================================== */
 /* K2: level of every (target, panel) pair, grouped per panel by level   */
 /* ===================================================================== */
-__global__ void __launch_bounds__(128) k_classify(OrderTab T, PairIn Q, LevelWS W, PairWS G) {
+__global__ void __launch_bounds__(128) k_classify(OrderTab T, PairIn Q, LevelWS W, PairWS G, int preset) {
   const int pan = blockIdx.x;
   const long long p0 = Q.tcxi[pan] - 1, m = Q.tcxi[pan + 1] - Q.tcxi[pan];
   __shared__ int cnt[8], warpc[4][8];
@@ -98,8 +98,9 @@ __global__ void __launch_bounds__(128) k_classify(OrderTab T, PairIn Q, LevelWS 
     int lv = 0;
     if (t < m) {
       const double* x = Q.tcx + 3 * (p0 + t);
-      lv = T.nlevel + 1;
-      for (int l = 0; l < T.nlevel; ++l) {
+      const int pre = preset ? (int)G.level[p0 + t] : 0; /* a level the selector already accepted */
+      lv = pre ? pre : T.nlevel + 1;
+      for (int l = 0; l < T.nlevel && !pre; ++l) {
         const double* qp = W.sub[l] + (size_t)pan * T.nsub[l] * 4;
         bool outside = true;
         for (int s = 0; s < T.nsub[l]; ++s) {
@@ -1897,8 +1898,8 @@ cudaError_t qol_launch_levels(const OrderTab& T, const PanelIn& P, const LevelWS
   return cudaGetLastError();
 }
 cudaError_t qol_launch_classify(const OrderTab& T, const PairIn& Q, const LevelWS& W, const PairWS& G, int npan,
-                                cudaStream_t st) {
-  k_classify<<<npan, 128, 0, st>>>(T, Q, W, G);
+                                cudaStream_t st, int preset) {
+  k_classify<<<npan, 128, 0, st>>>(T, Q, W, G, preset);
   return cudaGetLastError();
 }
 cudaError_t qol_launch_direct(const OrderTab& T, const PanelIn& P, const PairIn& Q, const LevelWS& W,

@@ -82,7 +82,21 @@ struct OutCOO {
 void qol_upload_harm_coefs(const double* hb, const double* hc, const double* hcm, cudaStream_t st);
 cudaError_t qol_launch_levels(const OrderTab& T, const PanelIn& P, const LevelWS& W, int npan, cudaStream_t st);
 cudaError_t qol_launch_classify(const OrderTab& T, const PairIn& Q, const LevelWS& W, const PairWS& G, int npan,
-                                cudaStream_t st);
+                                cudaStream_t st, int preset = 0 /* nonzero G.level entries are kept */);
+/* learned level selector (qol_selector.cu): MLP F -> H -> H -> C, QOL_SEL_NW weights */
+#define QOL_SEL_F 8
+#define QOL_SEL_H 64
+#define QOL_SEL_C 5
+#define QOL_SEL_NW (QOL_SEL_F * QOL_SEL_H + QOL_SEL_H + QOL_SEL_H * QOL_SEL_H + QOL_SEL_H + QOL_SEL_H * QOL_SEL_C + QOL_SEL_C)
+cudaError_t qol_launch_sel_features(int hd, const PanelIn& P, const PairIn& Q, int npan, float* feat, cudaStream_t st);
+cudaError_t qol_launch_sel_infer(const OrderTab& T, const PanelIn& P, const PairIn& Q, const LevelWS& W,
+                                 const PairWS& G, int npan, const float* wbf, float conf, unsigned long long* cnt,
+                                 cudaStream_t st);
+size_t qol_sel_grad_smem();
+cudaError_t qol_launch_sel_grad(const float* feat, const signed char* lab, const int* idx, long long n0, long long n1,
+                                const float* w, float* slot, double* sloss, int nslot, cudaStream_t st);
+cudaError_t qol_launch_sel_update(const float* slot, int nslot, float inv_n, float* grad, float* w, float* m, float* v,
+                                  float lr, int it, cudaStream_t st);
 cudaError_t qol_launch_direct(const OrderTab& T, const PanelIn& P, const PairIn& Q, const LevelWS& W,
                               const PairWS& G, const OutCOO& O, int npan, cudaStream_t st,
                               int pan0 = 0 /* first panel of the launch */);

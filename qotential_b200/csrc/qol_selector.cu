@@ -1,0 +1,379 @@
+/* Learned level selector (no reference counterpart): an MLP 8 -> 64 -> 64 -> 5
+ * on per-pair geometry features predicts the level the plain ball tests of
+ * lap3dsdlpmat_levels_r64 (patch_refine_mod.f90:516-551) give a (target,
+ * panel) pair: classes 0..3 = direct sums on refined level 1..4, class 4 =
+ * RRQ.  A confident prediction of a direct level l is used only when the
+ * target lies outside every level-l sub-patch ball (the plain criterion at
+ * that level), an RRQ prediction only when the target lies inside a ball of
+ * the finest level (RRQ is accurate near the panel); other pairs keep the
+ * plain walk over the levels.
+ *
+ * Features (FP32, from a per-panel descriptor computed in FP64 with fixed
+ * reduction order): centroid c = sum w y / sum w, diameter D = sqrt(sum w),
+ * mean normal nb, in-plane axes e1 (first node direction), e2 = nb x e1,
+ * curvature k = max |n_j - nb|, aspect a = sqrt(l1 / l2) of the in-plane
+ * second moments.  With d = x - c:
+ *   f0 log10(|d| / D), f1 tanh(d.e1 / D), f2 tanh(d.e2 / D), f3 d.nb / |d|,
+ *   f4 log10(|d.nb| / D), f5 k, f6 ln a, f7 log10(min_j |x - y_j| / D)
+ * (logs of arguments clamped below at 1e-12).
+ *
+ * Weights: W1[f][i] (8 x 64), b1, W2[i][j] (64 x 64), b2, W3[j][k] (64 x 5),
+ * b3, in that order; training keeps them in FP32, inference uses their BF16
+ * roundings with FP32 accumulation. */
+#include <cuda_runtime.h>
+#include <cstdint>
+#include "qol_kernels.h"
+
+namespace {
+
+constexpr int F = QOL_SEL_F, H = QOL_SEL_H, NC = QOL_SEL_C;
+constexpr int OW1 = 0, OB1 = OW1 + F * H, OW2 = OB1 + H, OB2 = OW2 + H * H, OW3 = OB2 + H, OB3 = OW3 + H * NC;
+static_assert(OB3 + NC == QOL_SEL_NW, "weight layout");
+
+/* the panel descriptor: c(3), nb(3), e1(3), e2(3), D, kappa, ln(aspect); one
+ * warp, lanes over the panel's nodes, shuffle sums in a fixed order */
+__device__ void sel_panel(int hd, const double* sx, const double* snx, const double* sw, double* dsc) {
+  const int lane = threadIdx.x & 31;
+  auto wsum = [&](double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+  };
+  auto wmax = [&](double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+  };
+  double s0 = 0, s1 = 0, s2 = 0, s3 = 0, n0 = 0, n1 = 0, n2 = 0;
+  for (int j = lane; j < hd; j += 32) {
+    const double w = sw[j];
+    s0 += w; s1 += w * sx[3 * j]; s2 += w * sx[3 * j + 1]; s3 += w * sx[3 * j + 2];
+    n0 += w * snx[3 * j]; n1 += w * snx[3 * j + 1]; n2 += w * snx[3 * j + 2];
+  }
+  s0 = wsum(s0); s1 = wsum(s1); s2 = wsum(s2); s3 = wsum(s3);
+  n0 = wsum(n0); n1 = wsum(n1); n2 = wsum(n2);
+  const double c0 = s1 / s0, c1 = s2 / s0, c2 = s3 / s0;
+  const double nl = sqrt(n0 * n0 + n1 * n1 + n2 * n2);
+  n0 /= nl; n1 /= nl; n2 /= nl;
+  double a0 = sx[0] - c0, a1 = sx[1] - c1, a2 = sx[2] - c2;
+  const double an = a0 * n0 + a1 * n1 + a2 * n2;
+  a0 -= an * n0; a1 -= an * n1; a2 -= an * n2;
+  const double al = sqrt(a0 * a0 + a1 * a1 + a2 * a2);
+  a0 /= al; a1 /= al; a2 /= al;
+  const double b0 = n1 * a2 - n2 * a1, b1 = n2 * a0 - n0 * a2, b2 = n0 * a1 - n1 * a0;
+  double kap = 0, ixx = 0, iyy = 0, ixy = 0;
+  for (int j = lane; j < hd; j += 32) {
+    const double d0 = snx[3 * j] - n0, d1 = snx[3 * j + 1] - n1, d2 = snx[3 * j + 2] - n2;
+    kap = fmax(kap, sqrt(d0 * d0 + d1 * d1 + d2 * d2));
+    const double y0 = sx[3 * j] - c0, y1 = sx[3 * j + 1] - c1, y2 = sx[3 * j + 2] - c2;
+    const double u = y0 * a0 + y1 * a1 + y2 * a2, v = y0 * b0 + y1 * b1 + y2 * b2, w = sw[j];
+    ixx += w * u * u; iyy += w * v * v; ixy += w * u * v;
+  }
+  kap = wmax(kap); ixx = wsum(ixx); iyy = wsum(iyy); ixy = wsum(ixy);
+  const double tr = 0.5 * (ixx + iyy), dt = sqrt(0.25 * (ixx - iyy) * (ixx - iyy) + ixy * ixy);
+  const double l1 = tr + dt, l2 = fmax(tr - dt, 1e-300);
+  if (lane == 0) {
+    dsc[0] = c0; dsc[1] = c1; dsc[2] = c2; dsc[3] = n0; dsc[4] = n1; dsc[5] = n2;
+    dsc[6] = a0; dsc[7] = a1; dsc[8] = a2; dsc[9] = b0; dsc[10] = b1; dsc[11] = b2;
+    dsc[12] = sqrt(s0); dsc[13] = kap; dsc[14] = 0.5 * log(l1 / l2);
+  }
+}
+
+__device__ __forceinline__ double lg10c(double v) { return log10(fmax(v, 1e-12)); }
+
+/* the 8 features of target x against the panel (descriptor dsc, nodes sx) */
+__device__ void sel_features(const double* x, const double* dsc, int hd, const double* sx, float* f) {
+  const double D = dsc[12];
+  const double d0 = x[0] - dsc[0], d1 = x[1] - dsc[1], d2 = x[2] - dsc[2];
+  const double r = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+  const double u = d0 * dsc[6] + d1 * dsc[7] + d2 * dsc[8], v = d0 * dsc[9] + d1 * dsc[10] + d2 * dsc[11];
+  const double h = d0 * dsc[3] + d1 * dsc[4] + d2 * dsc[5];
+  double m2 = 1e300;
+  for (int j = 0; j < hd; ++j) {
+    const double e0 = x[0] - sx[3 * j], e1 = x[1] - sx[3 * j + 1], e2 = x[2] - sx[3 * j + 2];
+    m2 = fmin(m2, e0 * e0 + e1 * e1 + e2 * e2);
+  }
+  f[0] = (float)lg10c(r / D);
+  f[1] = (float)tanh(u / D);
+  f[2] = (float)tanh(v / D);
+  f[3] = (float)(r > 0.0 ? h / r : 0.0);
+  f[4] = (float)lg10c(fabs(h) / D);
+  f[5] = (float)dsc[13];
+  f[6] = (float)dsc[14];
+  f[7] = (float)lg10c(sqrt(m2) / D);
+}
+
+/* per panel: descriptor into shared memory, node coordinates staged */
+__device__ void sel_stage(int pan, int hd, const PanelIn& P, double* s_sx, double* dsc) {
+  for (int e = threadIdx.x; e < 3 * hd; e += blockDim.x) s_sx[e] = P.sx[(size_t)pan * hd * 3 + e];
+  if (threadIdx.x < 32)
+    sel_panel(hd, P.sx + (size_t)pan * hd * 3, P.snx + (size_t)pan * hd * 3, P.sw + (size_t)pan * hd, dsc);
+  __syncthreads();
+}
+
+/* features of every pair of the panel (dataset for training) */
+__global__ void __launch_bounds__(128) k_sel_features(int hd, PanelIn P, PairIn Q, float* feat) {
+  const int pan = blockIdx.x;
+  extern __shared__ double ssm[];
+  double* dsc = ssm;        /* 16 */
+  double* s_sx = ssm + 16;  /* 3 hd */
+  sel_stage(pan, hd, P, s_sx, dsc);
+  const long long p0 = Q.tcxi[pan] - 1, m = Q.tcxi[pan + 1] - Q.tcxi[pan];
+  for (long long t = threadIdx.x; t < m; t += blockDim.x) {
+    float f[F];
+    sel_features(Q.tcx + 3 * (p0 + t), dsc, hd, s_sx, f);
+#pragma unroll
+    for (int c = 0; c < F; ++c) feat[(size_t)(p0 + t) * F + c] = f[c];
+  }
+}
+
+/* logits of one feature vector with the weights in shared memory */
+__device__ __forceinline__ void sel_forward(const float* w, const float* x, float* z) {
+  float h1[H];
+#pragma unroll
+  for (int i = 0; i < H; ++i) {
+    float a = w[OB1 + i];
+#pragma unroll
+    for (int c = 0; c < F; ++c) a = fmaf(w[OW1 + c * H + i], x[c], a);
+    h1[i] = fmaxf(a, 0.0f);
+  }
+#pragma unroll
+  for (int k = 0; k < NC; ++k) z[k] = w[OB3 + k];
+  for (int j = 0; j < H; ++j) {
+    float a = w[OB2 + j];
+#pragma unroll
+    for (int i = 0; i < H; ++i) a = fmaf(w[OW2 + i * H + j], h1[i], a);
+    a = fmaxf(a, 0.0f);
+#pragma unroll
+    for (int k = 0; k < NC; ++k) z[k] = fmaf(w[OW3 + j * NC + k], a, z[k]);
+  }
+}
+
+/* learned level decision of every pair of the panel: G.level = accepted level
+ * (1..nlevel+1) or 0 (the plain walk decides); counters [accepted, low
+ * confidence, check failed] */
+__global__ void __launch_bounds__(128) k_sel_infer(OrderTab T, PanelIn P, PairIn Q, LevelWS W, PairWS G,
+                                                   const float* wbf, float conf, unsigned long long* cnt) {
+  const int pan = blockIdx.x, hd = T.hd;
+  extern __shared__ double ssm[];
+  double* dsc = ssm;
+  double* s_sx = ssm + 16;
+  float* w = reinterpret_cast<float*>(s_sx + 3 * hd);
+  for (int e = threadIdx.x; e < QOL_SEL_NW; e += blockDim.x) w[e] = wbf[e];
+  sel_stage(pan, hd, P, s_sx, dsc);
+  __shared__ unsigned long long sc[3];
+  if (threadIdx.x < 3) sc[threadIdx.x] = 0;
+  __syncthreads();
+  const long long p0 = Q.tcxi[pan] - 1, m = Q.tcxi[pan + 1] - Q.tcxi[pan];
+  unsigned a = 0, lo = 0, ck = 0;
+  for (long long t = threadIdx.x; t < m; t += blockDim.x) {
+    const double* x = Q.tcx + 3 * (p0 + t);
+    float f[F], z[NC];
+    sel_features(x, dsc, hd, s_sx, f);
+    sel_forward(w, f, z);
+    int best = 0;
+#pragma unroll
+    for (int k = 1; k < NC; ++k) best = z[k] > z[best] ? k : best;
+    float den = 0.0f;
+#pragma unroll
+    for (int k = 0; k < NC; ++k) den += __expf(z[k] - z[best]);
+    const float prob = 1.0f / den;
+    int lv = 0;
+    if (prob < conf) ++lo;
+    else {
+      /* direct level l: outside every level-l ball; RRQ: inside a ball of the
+       * finest level (RRQ is accurate near the panel, not far from it) */
+      const bool rrq = best >= T.nlevel;
+      const int l = rrq ? T.nlevel - 1 : best; /* level index of the balls tested */
+      const double* qp = W.sub[l] + (size_t)pan * T.nsub[l] * 4;
+      bool outside = true;
+      for (int s = 0; s < T.nsub[l]; ++s) {
+        const double b0 = qp[4 * s] - x[0], b1 = qp[4 * s + 1] - x[1], b2 = qp[4 * s + 2] - x[2];
+        if (b0 * b0 + b1 * b1 + b2 * b2 < qp[4 * s + 3]) { outside = false; break; }
+      }
+      if (outside != rrq) lv = rrq ? T.nlevel + 1 : l + 1, ++a;
+      else ++ck;
+    }
+    G.level[p0 + t] = (signed char)lv;
+  }
+  atomicAdd(&sc[0], (unsigned long long)a);
+  atomicAdd(&sc[1], (unsigned long long)lo);
+  atomicAdd(&sc[2], (unsigned long long)ck);
+  __syncthreads();
+  if (threadIdx.x < 3) atomicAdd(&cnt[threadIdx.x], sc[threadIdx.x]);
+}
+
+/* training: one CTA of 256 samples, forward and backward; its partial
+ * gradient (sums over its samples, fixed order) into slot[blockIdx.x] and its
+ * loss sum into sloss[blockIdx.x].  Samples idx[n0 + 256 b + t] (t < 256) below
+ * n1; the rest contribute nothing. */
+constexpr int GT = 256, GS = 65; /* samples per CTA, row stride of the per-sample arrays */
+__global__ void __launch_bounds__(GT) k_sel_grad(const float* feat, const signed char* lab, const int* idx, long long n0,
+                                                 long long n1, const float* wg, float* slot, double* sloss) {
+  extern __shared__ float fsm[];
+  float* w = fsm;                  /* QOL_SEL_NW */
+  float* X = w + QOL_SEL_NW + 3;   /* GT x 9 */
+  float* H1 = X + GT * 9;          /* GT x GS: h1, then dh1 */
+  float* H2 = H1 + GT * GS;        /* GT x GS: h2, then dh2 */
+  float* DZ = H2 + GT * GS;        /* GT x 6 */
+  __shared__ double red[GT / 32];
+  const int t = threadIdx.x;
+  for (int e = t; e < QOL_SEL_NW; e += GT) w[e] = wg[e];
+  const long long gi = n0 + (long long)blockIdx.x * GT + t;
+  const bool ok = gi < n1;
+  const int s = ok ? idx[gi] : 0;
+  float x[F];
+#pragma unroll
+  for (int c = 0; c < F; ++c) x[c] = ok ? feat[(size_t)s * F + c] : 0.0f;
+#pragma unroll
+  for (int c = 0; c < F; ++c) X[t * 9 + c] = x[c];
+  __syncthreads();
+  /* forward */
+  for (int i = 0; i < H; ++i) {
+    float a = w[OB1 + i];
+#pragma unroll
+    for (int c = 0; c < F; ++c) a = fmaf(w[OW1 + c * H + i], x[c], a);
+    H1[t * GS + i] = fmaxf(a, 0.0f);
+  }
+  float z[NC];
+#pragma unroll
+  for (int k = 0; k < NC; ++k) z[k] = w[OB3 + k];
+  for (int j = 0; j < H; ++j) {
+    float a = w[OB2 + j];
+    for (int i = 0; i < H; ++i) a = fmaf(w[OW2 + i * H + j], H1[t * GS + i], a);
+    a = fmaxf(a, 0.0f);
+    H2[t * GS + j] = a;
+#pragma unroll
+    for (int k = 0; k < NC; ++k) z[k] = fmaf(w[OW3 + j * NC + k], a, z[k]);
+  }
+  float zm = z[0];
+#pragma unroll
+  for (int k = 1; k < NC; ++k) zm = fmaxf(zm, z[k]);
+  float den = 0.0f;
+#pragma unroll
+  for (int k = 0; k < NC; ++k) den += expf(z[k] - zm);
+  const int y = ok ? (int)lab[s] : 0;
+  double loss = ok ? (double)(logf(den) + zm - z[y]) : 0.0;
+#pragma unroll
+  for (int k = 0; k < NC; ++k) DZ[t * 6 + k] = ok ? expf(z[k] - zm) / den - (k == y ? 1.0f : 0.0f) : 0.0f;
+  __syncthreads();
+  float* g = slot + (size_t)blockIdx.x * QOL_SEL_NW;
+  /* dW3, db3 */
+  for (int e = t; e < H * NC + NC; e += GT) {
+    float acc = 0.0f;
+    if (e < H * NC) {
+      const int j = e / NC, k = e % NC;
+      for (int u = 0; u < GT; ++u) acc = fmaf(H2[u * GS + j], DZ[u * 6 + k], acc);
+      g[OW3 + e] = acc;
+    } else {
+      const int k = e - H * NC;
+      for (int u = 0; u < GT; ++u) acc += DZ[u * 6 + k];
+      g[OB3 + k] = acc;
+    }
+  }
+  __syncthreads();
+  /* dh2 = relu'(h2) W3 dz, in place */
+  for (int j = 0; j < H; ++j) {
+    float a = 0.0f;
+#pragma unroll
+    for (int k = 0; k < NC; ++k) a = fmaf(w[OW3 + j * NC + k], DZ[t * 6 + k], a);
+    H2[t * GS + j] = H2[t * GS + j] > 0.0f ? a : 0.0f;
+  }
+  __syncthreads();
+  /* dW2[i][j] = sum_u h1[u][i] dh2[u][j]; db2 */
+  for (int e = t; e < H * H; e += GT) {
+    const int i = e / H, j = e % H;
+    float acc = 0.0f;
+    for (int u = 0; u < GT; ++u) acc = fmaf(H1[u * GS + i], H2[u * GS + j], acc);
+    g[OW2 + e] = acc;
+  }
+  if (t < H) {
+    float acc = 0.0f;
+    for (int u = 0; u < GT; ++u) acc += H2[u * GS + t];
+    g[OB2 + t] = acc;
+  }
+  __syncthreads();
+  /* dh1 = relu'(h1) W2 dh2, in place */
+  for (int i = 0; i < H; ++i) {
+    float a = 0.0f;
+    for (int j = 0; j < H; ++j) a = fmaf(w[OW2 + i * H + j], H2[t * GS + j], a);
+    H1[t * GS + i] = H1[t * GS + i] > 0.0f ? a : 0.0f;
+  }
+  __syncthreads();
+  /* dW1[c][i] = sum_u x[u][c] dh1[u][i]; db1 */
+  for (int e = t; e < F * H; e += GT) {
+    const int c = e / H, i = e % H;
+    float acc = 0.0f;
+    for (int u = 0; u < GT; ++u) acc = fmaf(X[u * 9 + c], H1[u * GS + i], acc);
+    g[OW1 + e] = acc;
+  }
+  if (t < H) {
+    float acc = 0.0f;
+    for (int u = 0; u < GT; ++u) acc += H1[u * GS + t];
+    g[OB1 + t] = acc;
+  }
+  /* loss: warp sums, then the CTA's in warp order */
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) loss += __shfl_xor_sync(0xffffffffu, loss, o);
+  if ((t & 31) == 0) red[t >> 5] = loss;
+  __syncthreads();
+  if (t == 0) {
+    double sacc = 0.0;
+    for (int q = 0; q < GT / 32; ++q) sacc += red[q];
+    sloss[blockIdx.x] = sacc;
+  }
+}
+
+/* the batch gradient (slot sums in CTA order, / nvalid) into grad, and, with
+ * lr > 0, one Adam step on w (moments m, v; step number it >= 1) */
+__global__ void __launch_bounds__(256) k_sel_update(const float* slot, int nslot, float inv_n, float* grad, float* w,
+                                                    float* m, float* v, float lr, int it) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= QOL_SEL_NW) return;
+  float gsum = 0.0f;
+  for (int b = 0; b < nslot; ++b) gsum += slot[(size_t)b * QOL_SEL_NW + p];
+  const float gr = gsum * inv_n;
+  if (grad) grad[p] = gr;
+  if (lr > 0.0f) {
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    const float mm = b1 * m[p] + (1.0f - b1) * gr, vv = b2 * v[p] + (1.0f - b2) * gr * gr;
+    m[p] = mm; v[p] = vv;
+    const float mh = mm / (1.0f - powf(b1, (float)it)), vh = vv / (1.0f - powf(b2, (float)it));
+    w[p] -= lr * mh / (sqrtf(vh) + eps);
+  }
+}
+
+} // namespace
+
+cudaError_t qol_launch_sel_features(int hd, const PanelIn& P, const PairIn& Q, int npan, float* feat,
+                                    cudaStream_t st) {
+  if (npan <= 0) return cudaSuccess;
+  k_sel_features<<<npan, 128, sizeof(double) * (16 + 3 * hd), st>>>(hd, P, Q, feat);
+  return cudaGetLastError();
+}
+
+cudaError_t qol_launch_sel_infer(const OrderTab& T, const PanelIn& P, const PairIn& Q, const LevelWS& W,
+                                 const PairWS& G, int npan, const float* wbf, float conf, unsigned long long* cnt,
+                                 cudaStream_t st) {
+  if (npan <= 0) return cudaSuccess;
+  const size_t smem = sizeof(double) * (16 + 3 * T.hd) + sizeof(float) * QOL_SEL_NW;
+  k_sel_infer<<<npan, 128, smem, st>>>(T, P, Q, W, G, wbf, conf, cnt);
+  return cudaGetLastError();
+}
+
+size_t qol_sel_grad_smem() { return sizeof(float) * (QOL_SEL_NW + 3 + GT * 9 + 2 * GT * GS + GT * 6); }
+
+cudaError_t qol_launch_sel_grad(const float* feat, const signed char* lab, const int* idx, long long n0, long long n1,
+                                const float* w, float* slot, double* sloss, int nslot, cudaStream_t st) {
+  const size_t smem = qol_sel_grad_smem();
+  cudaError_t e = cudaFuncSetAttribute(k_sel_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k_sel_grad<<<nslot, GT, smem, st>>>(feat, lab, idx, n0, n1, w, slot, sloss);
+  return cudaGetLastError();
+}
+
+cudaError_t qol_launch_sel_update(const float* slot, int nslot, float inv_n, float* grad, float* w, float* m, float* v,
+                                  float lr, int it, cudaStream_t st) {
+  k_sel_update<<<(QOL_SEL_NW + 255) / 256, 256, 0, st>>>(slot, nslot, inv_n, grad, w, m, v, lr, it);
+  return cudaGetLastError();
+}

@@ -285,3 +285,12 @@ def harmonic_density(x, n, charges, q):
         u += qq / r
         g += -qq * d / r[:, None] ** 3
     return u, (g * n).sum(1)
+
+
+def family_surface(rng):
+    """A seeded surface of the batched family: R = R0 + a cos p + d cos(p - Nfp t),
+    Z = a sin p - d sin(p - Nfp t), R0 ~ U(3, 6), a ~ U(0.5, 1.5), d ~ U(0, 0.3),
+    Nfp in 1..5."""
+    R0, a, d = rng.uniform(3.0, 6.0), rng.uniform(0.5, 1.5), rng.uniform(0.0, 0.3)
+    nfp = int(rng.integers(1, 6))
+    return Surface([(0, 0, R0, 0.0), (1, 0, a, a), (1, 1, d, -d)], nfp=nfp)

@@ -100,3 +100,20 @@ def test_getnearquad_out_checked(qol):
         with pytest.raises(qol.QolError) as e:
             qol.qol_getnearquad_lap_rrq(out=bad, **args)
         assert e.value.code == 1
+
+
+def test_selector_arguments_checked(qol):
+    """selector entry points reject bad arguments before any device work"""
+    w = np.zeros(qol.SELECTOR_NW, np.float32)
+    for mode, conf in ((2, 0.9), (1, 1.5), (1, 0.0)):
+        with pytest.raises(qol.QolError) as e:
+            qol.qol_selector_set(mode, w, conf)
+        assert e.value.code == 8
+    qol.qol_selector_set(0)  # back to the plain walk: no device needed
+    f = np.zeros((4, 8), np.float32)
+    with pytest.raises(qol.QolError) as e:
+        qol.qol_selector_grad(f, np.array([0, 1, 7, 2]), w)  # class out of range
+    assert e.value.code == 8
+    with pytest.raises(qol.QolError) as e:
+        qol.qol_selector_train(f, np.zeros(4), w, epochs=1, batch=100)  # batch not a multiple of 256
+    assert e.value.code == 8

@@ -144,3 +144,33 @@ def test_rrq_converges_to_direct(orc, nterms, bound):
         assert np.abs(Ad @ sig - Bd @ sig).max() / np.abs(Ad @ sig).max() < bound
         # D[1] = -Omega/(4 pi)
         assert np.abs(Bd.sum(1) + Ia / (4 * np.pi)).max() < 1e-10
+
+
+def test_selector_oracle_gradient_matches_finite_differences():
+    """the oracle's selector loss gradient against central differences (the
+    selector has no reference counterpart; this pins the checker itself)"""
+    from oracle import selector as S
+    rng = np.random.default_rng(5)
+    w = rng.normal(0.0, 0.3, S.NW)
+    x = rng.normal(0.0, 1.0, (40, 8))
+    y = rng.integers(0, 5, 40)
+    _, g = S.loss_grad(w, x, y)
+    idx = rng.choice(S.NW, 60, replace=False)
+    h = 1e-6
+    for i in idx:
+        wp, wm = w.copy(), w.copy()
+        wp[i] += h
+        wm[i] -= h
+        fd = (S.loss_grad(wp, x, y)[0] - S.loss_grad(wm, x, y)[0]) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-6 * (1.0 + abs(g[i])), (i, fd, g[i])
+
+
+def test_selector_oracle_features_shape_and_ranges():
+    from oracle import selector as S
+    from qotential_b200 import geometry as G
+    P = G.panels(G.torus(), 6, 12, 4, split=False)
+    hd = 10
+    tcxi, tcxrow, tcx = G.near_lists(P["sx"], P["sw"], hd)
+    f = S.pair_features(P["sw"].size // hd, hd, P["sx"], P["snx"], P["sw"], tcx, tcxi)
+    assert f.shape == (tcxrow.size, 8) and np.isfinite(f).all()
+    assert (np.abs(f[:, 1:4]) <= 1.0 + 1e-12).all() and (f[:, 5] >= 0).all() and (f[:, 6] >= 0).all()
