@@ -217,6 +217,83 @@ def forms_compare(W, steps, warmup, D=None, out=None):
     return res
 
 
+def learned_form(W, D, out, steps, warmup, conf=0.9):
+    """The learned level selector: trained on the GPU on 10^6 pairs of seeded
+    surfaces of the batched family (features, plain-walk labels), evaluated on
+    this workload's pairs, then the device step with its decisions (confident
+    predictions that pass the ball check at their level; the plain walk for
+    the rest): ms/step, decision counts, per-row error against the plain form,
+    and the GRF error of both forms at the bench order."""
+    import torch
+    import qotential_b200 as qol
+    from qotential_b200 import geometry as G
+    from qotential_b200 import selector as Sel
+    t0 = time.perf_counter()
+    feat, lab, nsurf = Sel.training_set(1_000_000, seed=SEED)
+    t1 = time.perf_counter()
+    w, loss = qol.qol_selector_train(feat, lab, epochs=20, batch=16384, lr=3e-3, seed=SEED)
+    t2 = time.perf_counter()
+    cls, _ = Sel.predict(w, feat)
+    f12, lev12 = qol.qol_selector_features(W["npan"], W["nterms"], W["nquad"], W["sx"], W["snx"], W["sw"], W["rts"],
+                                           W["rps"], W["tcx"], W["tcxrow"], W["tcxi"], W["nquad"])
+    c12, p12 = Sel.predict(w, f12)
+    st = torch.cuda.current_stream()
+
+    def step():
+        qol.qol_getnearquad_lap_rrq_dev(W["npan"], W["nterms"], W["nquad"], D["sx"], D["snx"], D["sw"], D["rts"],
+                                        D["rps"], D["tcx"], D["tcxrow"], D["tcxi"], W["nquad"], 1.4, 30, out,
+                                        stream=st.cuda_stream, sync=False)
+
+    step()
+    torch.cuda.synchronize()
+    plain = (out[2].clone(), out[3].clone())
+    qol.qol_selector_set(1, w, conf)
+    try:
+        for _ in range(warmup):
+            step()
+        torch.cuda.synchronize()
+        qol.qol_selector_stats()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(steps):
+            step()
+        e1.record(st)
+        torch.cuda.synchronize()
+        stats = qol.qol_selector_stats()
+        ms = e0.elapsed_time(e1) / steps
+        err = {"row_error_vs": row_errors(out[0], plain[0], out[2]), "row_error_vd": row_errors(out[0], plain[1], out[3])}
+        # GRF identity at the bench order, both forms
+        nterms = W["nterms"]
+        hd = nterms * (nterms + 1) // 2
+        P = G.panels(G.stellarator(), MP, NP, nterms, split=False)
+        ys, q = G.point_charges(G.stellarator(), 8, seed=SEED)
+        ub, ubn = G.harmonic_density(P["sx"], P["snx"], ys, q)
+        npan = P["sw"].size // hd
+        uf = qol.qol_direct_farfield(P["sx"], P["snx"], P["sw"], ub, ubn)
+        un1, _, _ = qol.qol_grf_near(npan, nterms, nterms + 2, P["sx"], P["snx"], P["sw"], P["rts"], P["rps"], ub, ubn,
+                                     u=uf)
+    finally:
+        qol.qol_selector_set(0)
+    un0, _, _ = qol.qol_grf_near(npan, nterms, nterms + 2, P["sx"], P["snx"], P["sw"], P["rts"], P["rps"], ub, ubn,
+                                 u=uf)
+    del plain
+    npairs = W["pairs_total"]
+    return {"training": {"pairs": int(lab.size), "surfaces": nsurf, "epochs": 20, "batch": 16384,
+                         "data_s": round(t1 - t0, 2), "train_s": round(t2 - t1, 2),
+                         "loss_first_last": [float(loss[0]), float(loss[-1])],
+                         "accuracy": float((cls == lab).mean())},
+            "workload_accuracy": float((c12 == lev12 - 1).mean()),
+            "workload_confident": float((p12 >= conf).mean()), "confidence": conf,
+            "ms_per_step": ms, "pairs_per_s": npairs / (ms * 1e-3), "decisions": stats,
+            **err,
+            "grf_error": {"plain": float(np.abs(un0).max() / np.abs(ubn).max()),
+                          "learned": float(np.abs(un1).max() / np.abs(ubn).max())},
+            "note": "a prediction replaces the ball-test walk only when it passes the ball check at its level "
+                    "(direct: outside every ball of that level; RRQ: inside a ball of the finest level), so "
+                    "no pair gets a level the plain criterion rejects; the walk costs 0.2 ms a step here, so "
+                    "the selector does not make this step faster"}
+
+
 def config_dict(W, world):
     return {"workload": f"stellarator {MP}x{NP} quads ({W['npan_total']} triangles), order {ORDER} "
                         f"(nterms {W['nterms']}, hdim {W['hd']}, nquad=orderff {W['nquad']}), "
@@ -337,6 +414,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--no-grf", action="store_true", help="skip the per-order GRF sweep")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-selector measurement")
     ap.add_argument("--no-chosen", action="store_true",
                     help="skip the chosen-form (FP32 level sums) comparison at orders 12 and 10")
     ap.add_argument("--panels", type=int, default=0, help="use only the leading N panels (profiling)")
@@ -490,6 +568,9 @@ def main():
                           "contraction, FP64 accumulation across tiles); RRQ moments, solves and fits FP64; "
                           "device step with inputs resident, CUDA events; row_error = per target row, "
                           "max |chosen - plain| / max |plain| over the row's entries")
+    learned = None
+    if rank == 0 and world == 1 and not args.no_learned:
+        learned = learned_form(W, D, out, args.steps, 2)
     grf = None
     if rank == 0 and world == 1 and not args.no_grf:
         grf = grf_sweep()
@@ -509,7 +590,7 @@ def main():
                 "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": config_dict(W, world), "clocks": clocks, "e2e": e2e,
                 "gpu_launches": LAUNCHES_PER_STEP * args.steps, "roofline": roofline, "cpu_baseline": cpu,
-                "chosen_form": chosen, "grf_sweep": grf}
+                "chosen_form": chosen, "learned_form": learned, "grf_sweep": grf}
         print(json.dumps(line))
     if dist:
         dist.barrier()
