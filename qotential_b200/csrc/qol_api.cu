@@ -161,16 +161,22 @@ int order_tables(int nterms, int orderff, int nquad, OrderCache** out) {
     };
     const int ncw = 32 * ((hd + 31) / 32);
     std::vector<double> rp((size_t)L.n * ncw, 0.0);
-    std::vector<uint32_t> rh(rp.size(), 0u), rl(rp.size(), 0u);
+    /* the TF32 parts in m16n8k8 B-fragment order: tiles of 32 rows (zero
+     * padded), per 8-row k-slice and 8-column block the 32 lanes' (b0, b1) =
+     * (B[t][g], B[t+4][g]), lane = 4 g + t */
+    const long long npad = (L.n + 31) / 32 * 32;
+    const int nbt = ncw / 8;
+    std::vector<uint32_t> rh((size_t)npad * ncw, 0u), rl(rh.size(), 0u);
     for (long long i = 0; i < L.n; ++i)
       for (int k = 0; k < hd; ++k) {
         const size_t e = (size_t)i * ncw + k;
         rp[e] = L.interp[i + (size_t)L.n * k];
         const float f = (float)rp[e];
-        rh[e] = tf32(f);
+        const size_t fe = ((((size_t)(i / 8) * nbt + k / 8) * 32 + (k % 8) * 4 + (i % 4)) * 2) + (i % 8) / 4;
+        rh[fe] = tf32(f);
         float h;
-        std::memcpy(&h, &rh[e], 4);
-        rl[e] = tf32(f - h);
+        std::memcpy(&h, &rh[fe], 4);
+        rl[fe] = tf32(f - h);
       }
     T.ncw = ncw;
     T.interp[l] = C->up(rp);

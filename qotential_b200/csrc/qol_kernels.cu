@@ -463,7 +463,6 @@ constexpr size_t direct_smem() {
  * a_lo = TF32 rounding of the rest) accumulated in FP32 over a tile of DNT
  * nodes and in FP64 across tiles; the naive block in FP64.
  * --------------------------------------------------------------------- */
-#define FKS (DTT + 8)  /* kernel-tile row stride (floats): fragment loads hit 32 distinct banks */
 __device__ __forceinline__ unsigned tf32_rna(float x) {
   unsigned r;
   asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
@@ -500,17 +499,20 @@ __global__ void __launch_bounds__(256, 2) k_direct_tf32(OrderTab T, PanelIn P, P
   const int hd = T.hd, n = T.n[l];
   const long long p0 = Q.tcxi[pan] - 1, m = Q.tcxi[pan + 1] - Q.tcxi[pan];
   const double* node = W.node[l] + (size_t)pan * n * 7;
-  const unsigned* Ihg = T.interp_hi[l];
+  const unsigned* Ihg = T.interp_hi[l]; /* B-fragment order, tiles of 32 rows */
   const unsigned* Ilg = T.interp_lo[l];
-  constexpr int NCW = 32 * NB; /* padded columns */
-  constexpr int ICS = NCW + 8; /* interpolation-tile row stride (words) */
-  constexpr int STG = 4 * DNT * FKS + 2 * DNT * ICS + 8 * DNT; /* words per stage: K parts, I parts, nodes (7 x DNT floats) */
+  constexpr int NCW = 32 * NB;     /* padded columns */
+  constexpr int NBT = NCW / 8;     /* column blocks of 8 */
+  constexpr int KW = DNT * DTT;    /* words of one kernel-value part (A-fragment order) */
+  constexpr int IW = DNT * NCW;    /* words of one interpolation part of a tile */
+  constexpr int STG = 4 * KW + 2 * IW + 8 * DNT; /* words per stage: K parts, I parts, nodes (7 x DNT floats) */
   extern __shared__ __align__(16) unsigned fsm[];
   double* tg = reinterpret_cast<double*>(fsm + 2 * STG); /* DTT x 3 */
   float* xt = reinterpret_cast<float*>(tg + 3 * DTT);    /* DTT x 3, relative to the panel's first node */
   int* tloc = reinterpret_cast<int*>(xt + 3 * DTT);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int tb0 = 16 * (w >> 2), cb0 = 8 * NB * (w & 3);
+  const int mb = w >> 2, nb0 = NB * (w & 3); /* this warp's 16-target block, first column block */
+  const int tb0 = 16 * mb, cb0 = 8 * nb0;
   const int g = lane >> 2, t4 = lane & 3;
   const double i4p = 1.0 / (4.0 * QOL_PI);
   const double* pc = P.sx + (size_t)pan * hd * 3; /* the panel's first node */
@@ -524,33 +526,34 @@ __global__ void __launch_bounds__(256, 2) k_direct_tf32(OrderTab T, PanelIn P, P
   };
   auto node_store = [&](int s, double v) {
     if (nf < 7) {
-      float* nd = reinterpret_cast<float*>(fsm + s * STG + 4 * DNT * FKS + 2 * DNT * ICS);
+      float* nd = reinterpret_cast<float*>(fsm + s * STG + 4 * KW + 2 * IW);
       const double c = nf == 0 ? c0x : nf == 1 ? c0y : nf == 2 ? c0z : 0.0;
       nd[nf * DNT + nnn] = (float)(nf == 6 ? v * i4p : v - c);
     }
   };
-  auto fetch = [&](int t, int s) { /* TF32 parts of the tile's interpolation rows */
-    unsigned* Ih = fsm + s * STG + 4 * DNT * FKS;
-    unsigned* Il = Ih + DNT * ICS;
-    const int n0 = t * DNT;
-    for (int e = threadIdx.x; e < DNT * NCW / 2; e += blockDim.x) { /* 16-byte pieces of both parts */
-      const int part = e / (DNT * NCW / 4), r = e % (DNT * NCW / 4);
-      const int nn = r / (NCW / 4), c = 4 * (r % (NCW / 4)), i = n0 + nn;
-      unsigned* dst = (part ? Il : Ih) + nn * ICS + c;
-      if (i < n) cp_async16(dst, (part ? Ilg : Ihg) + (size_t)i * NCW + c);
-      else { dst[0] = 0u; dst[1] = 0u; dst[2] = 0u; dst[3] = 0u; }
+  auto fetch = [&](int t, int s) { /* TF32 parts of the tile's interpolation rows: one contiguous block each */
+    unsigned* Ih = fsm + s * STG + 4 * KW;
+    for (int e = threadIdx.x; e < IW / 2; e += blockDim.x) { /* 16-byte pieces of both parts */
+      const int part = e / (IW / 4), r = 4 * (e % (IW / 4));
+      cp_async16(Ih + part * IW + r, (part ? Ilg : Ihg) + (size_t)t * IW + r);
     }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
   };
-  auto kvals = [&](int t, int s, int nt) { /* FP32 kernel values of tile t, TF32 parts */
+  /* FP32 kernel values of tile t as TF32 parts, written in A-fragment order:
+   * word q = ((mblock 4 + kslice) 32 + lane) 4 + i, i = rowhalf + 2 colhalf,
+   * holding K[16 mblock + g + 8 rowhalf][8 kslice + t + 4 colhalf] (lane = 4 g + t);
+   * consecutive threads write consecutive words */
+  auto kvals = [&](int t, int s, int nt) {
     unsigned* KSh = fsm + s * STG;
-    unsigned* KSl = KSh + DNT * FKS;
-    unsigned* KDh = KSl + DNT * FKS;
-    unsigned* KDl = KDh + DNT * FKS;
-    const float* nd = reinterpret_cast<const float*>(fsm + s * STG + 4 * DNT * FKS + 2 * DNT * ICS);
+    unsigned* KSl = KSh + KW;
+    unsigned* KDh = KSl + KW;
+    unsigned* KDl = KDh + KW;
+    const float* nd = reinterpret_cast<const float*>(fsm + s * STG + 4 * KW + 2 * IW);
     const int n0 = t * DNT;
-    for (int e = threadIdx.x; e < DNT * DTT; e += blockDim.x) {
-      const int nn = e / DTT, tt = e % DTT;
+    for (int q = threadIdx.x; q < KW; q += blockDim.x) {
+      const int qb = q >> 7, ql = (q >> 2) & 31, qi = q & 3; /* (mblock, kslice), lane, element */
+      const int tt = 16 * (qb / (DNT / 8)) + (ql >> 2) + 8 * (qi & 1);
+      const int nn = 8 * (qb % (DNT / 8)) + (ql & 3) + 4 * (qi >> 1);
       float sv = 0.0f, dv = 0.0f;
       if (n0 + nn < n && tt < nt) {
         const float dx = xt[3 * tt] - nd[nn], dy = xt[3 * tt + 1] - nd[DNT + nn], dz = xt[3 * tt + 2] - nd[2 * DNT + nn];
@@ -563,9 +566,9 @@ __global__ void __launch_bounds__(256, 2) k_direct_tf32(OrderTab T, PanelIn P, P
       }
       unsigned hi, lo;
       tf32_split(sv, hi, lo);
-      KSh[nn * FKS + tt] = hi; KSl[nn * FKS + tt] = lo;
+      KSh[q] = hi; KSl[q] = lo;
       tf32_split(dv, hi, lo);
-      KDh[nn * FKS + tt] = hi; KDl[nn * FKS + tt] = lo;
+      KDh[q] = hi; KDl[q] = lo;
     }
   };
   for (int c0 = 0; c0 < cntl; c0 += DTT) {
@@ -594,12 +597,12 @@ __global__ void __launch_bounds__(256, 2) k_direct_tf32(OrderTab T, PanelIn P, P
       const int s = t & 1;
       double nv = 0.0;
       if (t + 1 < ntile) { fetch(t + 1, s ^ 1); nv = node_load(t + 1); }
-      const unsigned* KSh = fsm + s * STG;
-      const unsigned* KSl = KSh + DNT * FKS;
-      const unsigned* KDh = KSl + DNT * FKS;
-      const unsigned* KDl = KDh + DNT * FKS;
-      const unsigned* Ih = KDl + DNT * FKS;
-      const unsigned* Il = Ih + DNT * ICS;
+      const uint4* KSh = reinterpret_cast<const uint4*>(fsm + s * STG);
+      const uint4* KSl = KSh + KW / 4;
+      const uint4* KDh = KSl + KW / 4;
+      const uint4* KDl = KDh + KW / 4;
+      const uint2* Ih = reinterpret_cast<const uint2*>(fsm + s * STG + 4 * KW);
+      const uint2* Il = Ih + IW / 2;
       float fS[NB][4], fD[NB][4];
 #pragma unroll
       for (int b = 0; b < NB; ++b)
@@ -607,26 +610,20 @@ __global__ void __launch_bounds__(256, 2) k_direct_tf32(OrderTab T, PanelIn P, P
         for (int c = 0; c < 4; ++c) { fS[b][c] = 0.0f; fD[b][c] = 0.0f; }
 #pragma unroll
       for (int ks = 0; ks < DNT / 8; ++ks) {
-        const int r0 = 8 * ks + t4, r1 = r0 + 4; /* node rows of the k-slice */
-        const unsigned sh[4] = {KSh[r0 * FKS + tb0 + g], KSh[r0 * FKS + tb0 + 8 + g], KSh[r1 * FKS + tb0 + g],
-                                KSh[r1 * FKS + tb0 + 8 + g]};
-        const unsigned sl[4] = {KSl[r0 * FKS + tb0 + g], KSl[r0 * FKS + tb0 + 8 + g], KSl[r1 * FKS + tb0 + g],
-                                KSl[r1 * FKS + tb0 + 8 + g]};
-        const unsigned dh[4] = {KDh[r0 * FKS + tb0 + g], KDh[r0 * FKS + tb0 + 8 + g], KDh[r1 * FKS + tb0 + g],
-                                KDh[r1 * FKS + tb0 + 8 + g]};
-        const unsigned dl[4] = {KDl[r0 * FKS + tb0 + g], KDl[r0 * FKS + tb0 + 8 + g], KDl[r1 * FKS + tb0 + g],
-                                KDl[r1 * FKS + tb0 + 8 + g]};
+        const int fa = (mb * (DNT / 8) + ks) * 32 + lane;
+        const uint4 vsh = KSh[fa], vsl = KSl[fa], vdh = KDh[fa], vdl = KDl[fa];
+        const unsigned sh[4] = {vsh.x, vsh.y, vsh.z, vsh.w}, sl[4] = {vsl.x, vsl.y, vsl.z, vsl.w};
+        const unsigned dh[4] = {vdh.x, vdh.y, vdh.z, vdh.w}, dl[4] = {vdl.x, vdl.y, vdl.z, vdl.w};
 #pragma unroll
         for (int b = 0; b < NB; ++b) {
-          const int col = cb0 + 8 * b + g;
-          const unsigned bh0 = Ih[r0 * ICS + col], bh1 = Ih[r1 * ICS + col];
-          const unsigned bl0 = Il[r0 * ICS + col], bl1 = Il[r1 * ICS + col];
-          mma_tf32(fS[b], sl, bh0, bh1);
-          mma_tf32(fS[b], sh, bl0, bl1);
-          mma_tf32(fS[b], sh, bh0, bh1);
-          mma_tf32(fD[b], dl, bh0, bh1);
-          mma_tf32(fD[b], dh, bl0, bl1);
-          mma_tf32(fD[b], dh, bh0, bh1);
+          const int fb = (ks * NBT + nb0 + b) * 32 + lane;
+          const uint2 bh = Ih[fb], bl = Il[fb];
+          mma_tf32(fS[b], sl, bh.x, bh.y);
+          mma_tf32(fS[b], sh, bl.x, bl.y);
+          mma_tf32(fS[b], sh, bh.x, bh.y);
+          mma_tf32(fD[b], dl, bh.x, bh.y);
+          mma_tf32(fD[b], dh, bl.x, bl.y);
+          mma_tf32(fD[b], dh, bh.x, bh.y);
         }
       }
 #pragma unroll
@@ -672,7 +669,7 @@ __global__ void __launch_bounds__(256, 2) k_direct_tf32(OrderTab T, PanelIn P, P
 }
 template <int NB>
 constexpr size_t direct_tf32_smem() {
-  return sizeof(unsigned) * 2 * (4 * DNT * FKS + 2 * DNT * (32 * NB + 8) + 8 * DNT) + sizeof(double) * 3 * DTT +
+  return sizeof(unsigned) * 2 * (4 * DNT * DTT + 2 * DNT * 32 * NB + 8 * DNT) + sizeof(double) * 3 * DTT +
          sizeof(float) * 3 * DTT + sizeof(int) * DTT;
 }
 

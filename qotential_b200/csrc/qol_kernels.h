@@ -11,7 +11,8 @@ struct OrderTab {
   double dist;
   int n[4], nsub[4];
   const double* interp[4];    /* n_l x ncw, row-major; columns hd .. ncw-1 zero (16-byte rows) */
-  const unsigned* interp_hi[4], *interp_lo[4]; /* interp in FP32 as TF32 high and low parts (precision variant) */
+  const unsigned* interp_hi[4], *interp_lo[4]; /* interp in FP32 as TF32 high and low parts (precision variant),
+                                                  in mma B-fragment order, rows zero-padded to tiles of 32 */
   int ncw;                    /* 32 ceil(hd / 32) */
   const double* wt[4];        /* n_l */
   const long long* suboff[4]; /* nsub_l + 1 */
