@@ -58,8 +58,8 @@ def workload(rank=0, world=1, panels=0, order=ORDER):
 
 
 # kernels of one qol_getnearquad_lap_rrq_dev call: level nodes, level subs, classify, scan, direct,
-# rrq_pairs, rrq_panel, rrq_ssq, rrq_geom, rrq_moments, rrq_apply, coo_index
-LAUNCHES_PER_STEP = 12
+# rrq_pairs, rrq_panel, rrq_ssq, rrq_side, rrq_geom, rrq_moments, rrq_apply, coo_index
+LAUNCHES_PER_STEP = 13
 
 
 def xlate_terms(L):

@@ -377,7 +377,7 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
   const long long nrrq = off_h.back();
   R.nrrq = nrrq;
   /* per-pair RRQ moment storage (separate arena: its size is known only now) */
-  rc = g_arena2.reserve(sizeof(double) * (size_t)std::max<long long>(nrrq, 1) * (5 * hd + 6 * nbd + 4 + 3 * (2 * nq + 3) + 1) +
+  rc = g_arena2.reserve(sizeof(double) * (size_t)std::max<long long>(nrrq, 1) * (5 * hd + 6 * nbd + 4 + 3 * (2 * nq + 3) + 2) +
                         8192);
   if (rc) return rc;
   g_arena2.reset();
@@ -386,6 +386,7 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
   R.line = g_arena2.take<double>((size_t)std::max<long long>(nrrq, 1) * (6 * nbd + 4));
   R.edge = g_arena2.take<double>((size_t)std::max<long long>(nrrq, 1) * 3 * (2 * nq + 3));
   R.pair = g_arena2.take<int2>((size_t)std::max<long long>(nrrq, 1));
+  R.side = g_arena2.take<signed char>((size_t)std::max<long long>(nrrq, 1));
   OutCOO O{};
   O.vs = J.vs; O.vd = J.vd; O.omega = J.omega; O.subtract_naive = J.subtract_naive;
   /* one pass over all panels, or (host entry) panel chunks whose every phase

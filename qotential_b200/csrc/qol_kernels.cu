@@ -1120,34 +1120,53 @@ struct WarpSM {
   int nbr[3];
 };
 
-/* warp-cooperative surface evaluation for the side test: f[c*3+p] = sum_k
- * pols_k(point p) scf[c*hd+k] for the coordinates c = x,y,z and the points
- * (u,v), (u+h,v), (u,v+h).  Lane a evaluates the polynomials (a, b),
- * b = 0..korder-a, i.e. L_a(s,t) P_b^{(2a+1,0)}(z) (the host basis), the
- * three points as independent recurrences; coefficient tables, no divisions. */
-__device__ void koorn_eval3_warp(int korder, int hd, const double* scf, double u, double v, double h,
-                                 double* f /* 9 */) {
-  const int lane = threadIdx.x & 31;
+
+/* the three coordinate series (3 x n Legendre coefficients) of one edge and
+ * their derivatives at t, one recurrence for all three, no divisions */
+__device__ __forceinline__ void leg_eval3(int n, const double* c, double t, double* y, double* yp) {
+  double p0 = 1.0, p1 = t, d0 = 0.0, d1 = 1.0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) { y[d] = c[d * n]; yp[d] = 0.0; }
+  if (n > 1)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) { y[d] += c[d * n + 1] * p1; yp[d] += c[d * n + 1] * d1; }
+  for (int k = 1; k + 1 < n; ++k) {
+    const double p2 = c_la[k] * t * p1 - c_lb[k] * p0;
+    const double d2 = d0 + (2.0 * k + 1.0) * p1;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) { y[d] += c[d * n + k + 1] * p2; yp[d] += c[d * n + k + 1] * d2; }
+    p0 = p1; p1 = p2; d0 = d1; d1 = d2;
+  }
+}
+
+
+/* the panel's Koornwinder expansion (coefficients scf, 3 x hd) at (u, v),
+ * (u + h, v) and (u, v + h): f[3 c + p] = coordinate c at point p.  Column a:
+ * the Legendre factor L_a((2u + v - 1)/(1 - v)) (1 - v)^a by its three-term
+ * recurrence (advanced one step per column), the Jacobi P_b^(2a+1,0)(2v - 1)
+ * by its recurrence down the column; terms summed in column order */
+__device__ void koorn_eval3_thread(int korder, int hd, const double* scf, double u, double v, double h,
+                                   double* f /* 9 */) {
   double acc[9];
 #pragma unroll
   for (int i = 0; i < 9; ++i) acc[i] = 0.0;
-  if (lane <= korder) {
-    const int a = lane;
-    const double us[3] = {u, u + h, u}, vs[3] = {v, v, v + h};
-    double sv[3], tt[3], zv[3], L0[3], L1[3], La[3];
+  const double us[3] = {u, u + h, u}, vs[3] = {v, v, v + h};
+  double sv[3], tt[3], zv[3], L0[3], L1[3];
+#pragma unroll
+  for (int p = 0; p < 3; ++p) {
+    sv[p] = 2.0 * us[p] + vs[p] - 1.0;
+    const double t = 1.0 - vs[p];
+    tt[p] = t * t;
+    zv[p] = 2.0 * vs[p] - 1.0;
+    L0[p] = 1.0; L1[p] = sv[p];
+  }
+  for (int a = 0; a <= korder; ++a) {
+    double La[3];
 #pragma unroll
     for (int p = 0; p < 3; ++p) {
-      sv[p] = 2.0 * us[p] + vs[p] - 1.0;
-      const double t = 1.0 - vs[p];
-      tt[p] = t * t;
-      zv[p] = 2.0 * vs[p] - 1.0;
-      L0[p] = 1.0; L1[p] = sv[p]; La[p] = a >= 1 ? sv[p] : 1.0;
-    }
-    for (int q = 1; q < a; ++q) {
-      const double ca = c_la[q], cb = c_lb[q];
-#pragma unroll
-      for (int p = 0; p < 3; ++p) {
-        const double L2 = ca * sv[p] * L1[p] - cb * tt[p] * L0[p];
+      if (a <= 1) La[p] = a == 0 ? 1.0 : sv[p];
+      else {
+        const double L2 = c_la[a - 1] * sv[p] * L1[p] - c_lb[a - 1] * tt[p] * L0[p];
         L0[p] = L1[p]; L1[p] = L2; La[p] = L2;
       }
     }
@@ -1184,64 +1203,55 @@ __device__ void koorn_eval3_warp(int korder, int hd, const double* scf, double u
     }
   }
 #pragma unroll
-  for (int i = 0; i < 9; ++i) {
-    double x = acc[i];
-    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-    f[i] = x;
-  }
+  for (int i = 0; i < 9; ++i) f[i] = acc[i];
 }
 
-/* the three coordinate series (3 x n Legendre coefficients) of one edge and
- * their derivatives at t, one recurrence for all three, no divisions */
-__device__ __forceinline__ void leg_eval3(int n, const double* c, double t, double* y, double* yp) {
-  double p0 = 1.0, p1 = t, d0 = 0.0, d1 = 1.0;
-#pragma unroll
-  for (int d = 0; d < 3; ++d) { y[d] = c[d * n]; yp[d] = 0.0; }
-  if (n > 1)
-#pragma unroll
-    for (int d = 0; d < 3; ++d) { y[d] += c[d * n + 1] * p1; yp[d] += c[d * n + 1] * d1; }
-  for (int k = 1; k + 1 < n; ++k) {
-    const double p2 = c_la[k] * t * p1 - c_lb[k] * p0;
-    const double d2 = d0 + (2.0 * k + 1.0) * p1;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) { y[d] += c[d * n + k + 1] * p2; yp[d] += c[d * n + k + 1] * d2; }
-    p0 = p1; p1 = p2; d0 = d1; d1 = d2;
+/* side test of every RRQ pair of the launch, one thread per pair: the
+ * target's projection onto the panel by Newton from the nearest node's
+ * (u, v) (finite-difference Jacobian), its height over
+ * the panel and whether the projection lies inside the triangle:
+ * R.side = side (-1, 0, 1; 0 within 1e-12) + 4 inside */
+__global__ void __launch_bounds__(128) k_rrq_side(OrderTab T, PairIn Q, RRQWS R) {
+  const long long gidx = R.glo + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gidx >= R.ghi) return;
+  const int2 pr = R.pair[gidx];
+  const int pan = pr.x, tl = pr.y, hd = T.hd;
+  const long long p0 = Q.tcxi[pan] - 1;
+  const double* fr = R.frame + (size_t)pan * RRQ_FRAME;
+  const double* scf = R.scf + (size_t)pan * 3 * hd;
+  const double* sxf = R.sxf + (size_t)pan * 3 * hd;
+  const double alpha = fr[12];
+  double xt[3];
+  {
+    const double* x = Q.tcx + 3 * (p0 + tl);
+    const double d0 = x[0] - fr[9], d1 = x[1] - fr[10], d2 = x[2] - fr[11];
+    for (int i = 0; i < 3; ++i) xt[i] = alpha * (fr[i] * d0 + fr[i + 3] * d1 + fr[i + 6] * d2);
   }
-}
-
-/* height of the target above the panel surface at its in-plane position and
- * whether that position lies inside the triangle (warp-cooperative) */
-__device__ double panel_height_warp(const OrderTab& T, const double* scf, const double* sxf, const double* xt,
-                                    int* inside) {
-  const int hd = T.hd, lane = threadIdx.x & 31;
   double best = 1e300;
   int ib = hd;
-  for (int j = lane; j < hd; j += 32) {
-    double d0 = sxf[3 * j] - xt[0], d1 = sxf[3 * j + 1] - xt[1], d2 = d0 * d0 + d1 * d1;
+  for (int j = 0; j < hd; ++j) { /* the nearest node in the frame's plane (first on ties) */
+    const double d0 = sxf[3 * j] - xt[0], d1 = sxf[3 * j + 1] - xt[1], d2 = d0 * d0 + d1 * d1;
     if (d2 < best) { best = d2; ib = j; }
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    double b2 = __shfl_xor_sync(0xffffffffu, best, o);
-    int i2 = __shfl_xor_sync(0xffffffffu, ib, o);
-    if (b2 < best || (b2 == best && i2 < ib)) { best = b2; ib = i2; }
   }
   double u = T.vruv[2 * ib], v = T.vruv[2 * ib + 1];
   double f[9];
   const double h = 1e-7;
   for (int it = 0; it < 40; ++it) {
-    koorn_eval3_warp(T.korder, hd, scf, u, v, h, f);
-    double J00 = (f[1] - f[0]) / h, J10 = (f[4] - f[3]) / h, J01 = (f[2] - f[0]) / h, J11 = (f[5] - f[3]) / h;
-    double r0 = f[0] - xt[0], r1 = f[3] - xt[1];
-    double det = J00 * J11 - J01 * J10;
+    koorn_eval3_thread(T.korder, hd, scf, u, v, h, f);
+    const double J00 = (f[1] - f[0]) / h, J10 = (f[4] - f[3]) / h, J01 = (f[2] - f[0]) / h, J11 = (f[5] - f[3]) / h;
+    const double r0 = f[0] - xt[0], r1 = f[3] - xt[1];
+    const double det = J00 * J11 - J01 * J10;
     if (det == 0.0) break;
-    double du = (J11 * r0 - J01 * r1) / det, dv = (-J10 * r0 + J00 * r1) / det;
+    const double du = (J11 * r0 - J01 * r1) / det, dv = (-J10 * r0 + J00 * r1) / det;
     u -= du; v -= dv;
     if (fabs(du) + fabs(dv) < 1e-14) break;
   }
-  koorn_eval3_warp(T.korder, hd, scf, u, v, 0.0, f);
+  koorn_eval3_thread(T.korder, hd, scf, u, v, 0.0, f);
   const double tol = 1e-10;
-  *inside = (u >= -tol && v >= -tol && u + v <= 1.0 + tol) ? 1 : 0;
-  return xt[2] - f[6];
+  const int inside = (u >= -tol && v >= -tol && u + v <= 1.0 + tol) ? 1 : 0;
+  const double hgt = xt[2] - f[6];
+  const int side = fabs(hgt) <= 1e-12 ? 0 : (hgt > 0 ? 1 : -1);
+  R.side[gidx] = (signed char)(side + 4 * inside);
 }
 
 /* singularity-swap root and modified weights, one thread per (RRQ pair,
@@ -1283,7 +1293,7 @@ __global__ void __launch_bounds__(32 * RRQ_WARPS) k_rrq_geom(OrderTab T, PairIn 
   const int2 pr = R.pair[gidx]; /* (panel, local target) */
   const int pan = pr.x, tl = pr.y;
   const long long p0 = Q.tcxi[pan] - 1;
-  const int hd = T.hd, nq = T.nquad, nbd = 3 * nq;
+  const int nq = T.nquad, nbd = 3 * nq;
   const double* fr = R.frame + (size_t)pan * RRQ_FRAME;
   const double* bx = R.bx + (size_t)pan * 3 * nbd;
   const double* bt = R.bt + (size_t)pan * 3 * nbd;
@@ -1327,9 +1337,8 @@ __global__ void __launch_bounds__(32 * RRQ_WARPS) k_rrq_geom(OrderTab T, PairIn 
    * inside the triangle; otherwise the one passing farther from the boundary */
   double sdir;
   {
-    int inside = 1;
-    double hgt = panel_height_warp(T, R.scf + (size_t)pan * 3 * hd, R.sxf + (size_t)pan * 3 * hd, xt, &inside);
-    int side = fabs(hgt) <= 1e-12 ? 0 : (hgt > 0 ? 1 : -1);
+    const int sd = R.side[gidx]; /* from k_rrq_side */
+    const int inside = sd >= 3 ? 1 : 0, side = sd - 4 * inside;
     sdir = side == 0 ? (exterior ? 1.0 : -1.0) : (double)side;
     if (!inside) {
       double cu = 2.0, cdn = 2.0;
@@ -1989,6 +1998,7 @@ cudaError_t qol_launch_rrq_geom(const OrderTab& T, const PairIn& Q, const PairWS
                                 cudaStream_t st) {
   const long long n = R.ghi - R.glo;
   if (n <= 0) return cudaSuccess;
+  k_rrq_side<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(T, Q, R);
   long long nb = (n + RRQ_WARPS - 1) / RRQ_WARPS;
   k_rrq_geom<<<(unsigned)nb, 32 * RRQ_WARPS, 0, st>>>(T, Q, G, R, exterior);
   return cudaGetLastError();

@@ -69,6 +69,7 @@ struct RRQWS {
   double* edge;    /* per RRQ pair and edge: w1 (nq), w3 (nq), ok, Re t0, Im t0 */
   double* ialpha;  /* per RRQ pair (nullable) */
   int2* pair;      /* per RRQ pair: (panel, local target) */
+  signed char* side; /* per RRQ pair: side of the panel (-1, 0, 1) + 4 when the target projects inside */
   long long glo, ghi; /* RRQ pairs [glo, ghi) of this launch (per-pair kernels) */
   int plo, phi;       /* panels [plo, phi) of this launch (k_rrq_apply) */
 };

@@ -251,6 +251,7 @@ extern "C" int qol_rrq_noalloc(qol_int m, const double* tx, qol_int n, const dou
   R.line = (double*)take(sizeof(double) * (size_t)m * (6 * nbd + 4));
   R.edge = (double*)take(sizeof(double) * (size_t)m * 3 * (2 * nq + 3));
   R.pair = (int2*)take(sizeof(int2) * (size_t)(m > 0 ? m : 1));
+  R.side = (signed char*)take((size_t)(m > 0 ? m : 1));
   if (over) {
     std::snprintf(g_na_msg, sizeof g_na_msg,
                   "qol_rrq_noalloc: m = %lld targets at order %lld need %zu bytes of scratch; the static scratch "
