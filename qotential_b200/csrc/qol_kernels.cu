@@ -1308,10 +1308,15 @@ __global__ void __launch_bounds__(32 * RRQ_WARPS) k_rrq_geom(OrderTab T, PairIn 
   const double xt0 = xt[0], xt1 = xt[1], xt2 = xt[2];
   /* singularity-swap weights (from k_rrq_ssq) and graded breakpoints, one
    * lane per edge */
+  for (int e2 = lane; e2 < 3 * 2 * nq; e2 += 32) { /* the weights, all lanes */
+    const int e = e2 / (2 * nq), r = e2 % (2 * nq);
+    const double v = R.edge[((size_t)gidx * 3 + e) * (2 * nq + 3) + r];
+    if (r < nq) W.w1[e * nq + r] = v;
+    else W.w3[e * nq + r - nq] = v;
+  }
   if (lane < 3) {
     const int e = lane;
     const double* er = R.edge + ((size_t)gidx * 3 + e) * (2 * nq + 3);
-    for (int q = 0; q < nq; ++q) { W.w1[e * nq + q] = er[q]; W.w3[e * nq + q] = er[nq + q]; }
     const bool ok = er[2 * nq] != 0.0;
     const cd t0 = mk(er[2 * nq + 1], er[2 * nq + 2]);
     double ts = 0.0, dd = 2.0;
@@ -1363,9 +1368,11 @@ __global__ void __launch_bounds__(32 * RRQ_WARPS) k_rrq_geom(OrderTab T, PairIn 
   double Omega;
   {
     double tot = 0.0;
-    for (int e = 0; e < 3; ++e) {
-      const int nint = W.nbr[e] - 1;
-      for (int pnt = lane; pnt < nint * 16; pnt += 32) {
+    /* the three edges' points as one list over the lanes */
+    const int p0n = 16 * (W.nbr[0] - 1), p1n = p0n + 16 * (W.nbr[1] - 1), p2n = p1n + 16 * (W.nbr[2] - 1);
+    for (int pg = lane; pg < p2n; pg += 32) {
+      {
+        const int e = pg < p0n ? 0 : (pg < p1n ? 1 : 2), pnt = pg - (e == 0 ? 0 : (e == 1 ? p0n : p1n));
         int ib = pnt >> 4, q = pnt & 15;
         double a = W.br[e][ib], b = W.br[e][ib + 1];
         if (!(b > a)) continue;
