@@ -1185,14 +1185,23 @@ int qol_getnearquad_lap_rrq(qol_int npan, qol_int nterms, qol_int hdim, qol_int 
   cudaStream_t st = g_stream;
   const int hd = (int)hdim;
   const size_t nout = (size_t)ntcx * hdim;
-  /* panel chunks with about equal target counts (about 8 on large calls):
-   * the per-pair RRQ phase runs chunk by chunk and each chunk's values leave
-   * the GPU while the next one computes */
-  const int nch = (int)std::max<qol_int>(1, std::min<qol_int>(8, npan / 256));
+  /* panel chunks (up to kMaxChunks on large calls): the pipeline runs chunk by
+   * chunk and each chunk's values leave the GPU while later chunks compute.
+   * Target counts follow a tapered schedule: a half-size first chunk (its
+   * values are the first that can leave), full-size ones, then a half- and a
+   * quarter-size last pair (what is left to copy after the last kernel) */
+  constexpr int kMaxChunks = 12;
+  const int nch = (int)std::max<qol_int>(1, std::min<qol_int>(kMaxChunks, npan / 192));
+  std::vector<double> wcum(nch + 1, 0.0);
+  for (int c = 0; c < nch; ++c) {
+    double w = 1.0;
+    if (nch >= 4) w = c == 0 ? 0.5 : (c == nch - 2 ? 0.5 : (c == nch - 1 ? 0.25 : 1.0));
+    wcum[c + 1] = wcum[c] + w;
+  }
   std::vector<long long> cb(nch + 1, 0);
   cb[nch] = npan;
   for (int c = 1; c < nch; ++c) {
-    const qol_int want = (ntcx * c) / nch;
+    const qol_int want = (qol_int)((double)ntcx * wcum[c] / wcum[nch]);
     qol_int k = std::lower_bound(tcxi, tcxi + npan + 1, want + 1) - tcxi;
     cb[c] = std::min<qol_int>(npan, std::max<qol_int>(cb[c - 1], k));
   }
