@@ -885,14 +885,14 @@ __global__ void __launch_bounds__(NT, 1) k_rrq_panel(OrderTab T, PanelIn P, Pair
   }
   /* basis at the nodes: this CTA's columns of V (harmonics c0..c1) and of
    * Msl^T (nodes c0..c1), and H rows of its nodes */
-  for (int j = threadIdx.x; j < hd; j += blockDim.x) {
+  for (int e = threadIdx.x; e < hd * L; e += blockDim.x) { /* (node j, order m) items: distinct entries */
+    const int j = e / L, m = e % L + 1;
     double y[3], nrm[3];
     tofr(&s_sx[3 * j], y);
     const double* sn = P.snx + ((size_t)pan * hd + j) * 3;
     for (int i = 0; i < 3; ++i) nrm[i] = s_fr[i] * sn[0] + s_fr[i + 3] * sn[1] + s_fr[i + 6] * sn[2];
     const bool ownj = j >= c0 && j < c1;
-    for (int m = 1; m <= L; ++m)
-      harm_column(L, m, y[0], y[1], y[2], [&](int l, int k, double h, double gx, double gy, double gz) {
+    harm_column(L, m, y[0], y[1], y[2], [&](int l, int k, double h, double gx, double gy, double gz) {
         if (k >= c0 && k < c1) {
           double* q = Vs + ((size_t)j * ncol + (k - c0)) * 4;
           q[0] = 0.0; q[1] = gx; q[2] = gy; q[3] = gz;
@@ -1065,47 +1065,66 @@ __global__ void __launch_bounds__(NT, 1) k_rrq_panel(OrderTab T, PanelIn P, Pair
   }
   __threadfence();
   cl.sync();
-  /* B = PS H^T, rows c0..c1: B[i][j] = sum_k PS[i][k] h_k(y_j), K tiles of PS
-   * and H staged in the space of the matrix copies (free now) */
+  /* B = PS H^T, rows c0..c1: B[i][j] = sum_k PS[i][k] h_k(y_j) on the FP64
+   * tensor path (m8n8k4): PS rows (A) and H rows (B^T) staged in K tiles in the
+   * CTA's shared memory (free now), zero padded; warp w takes the column
+   * blocks w, w + NT/32, .. with every row block */
   {
     double* B = R.B + (size_t)pan * hd * hd;
-    const int room = 5 * hd * ncol;
-    int KT = 32;
-    while (KT > 4 && (ncol + hd) * (KT + 1) > room) KT >>= 1;
-    const int ks = KT + 1; /* odd stride: consecutive j hit distinct banks */
-    double* sP = psm;
-    double* sH = psm + (size_t)ncol * ks;
-    constexpr int MAXB = 12;
-    double bacc[MAXB];
+    const int room = (int)panel_smem_doubles(hd, nbd, CS); /* the whole allocation: everything in it is dead now */
+    const int MBn = (nc + 7) / 8, NBn = (hd + 7) / 8, rows = 8 * (MBn + NBn), KP = (hd + 3) & ~3;
+    auto skf = [](int kt) { return (kt % 16 == 4 || kt % 16 == 12) ? kt : kt + 4; }; /* conflict-free strides */
+    int KT = KP;
+    while (KT > 4 && rows * skf(KT) > room) KT -= 4;
+    const int SK = skf(KT);
+    double* sP = psm;                         /* 8 MBn x SK */
+    double* sH = psm + (size_t)8 * MBn * SK;  /* 8 NBn x SK */
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    constexpr int NW = NT / 32, MBX = 8, NBX = 2; /* row blocks <= 7, column blocks a warp <= 2 (nterms <= 17) */
+    double acc[NBX][MBX][2];
 #pragma unroll
-    for (int u = 0; u < MAXB; ++u) bacc[u] = 0.0;
-    for (int k0 = 0; k0 < hd; k0 += KT) {
-      __syncthreads();
-      for (int e = threadIdx.x; e < nc * KT; e += NT) {
-        const int i = e / KT, kk = e % KT;
-        sP[i * ks + kk] = k0 + kk < hd ? PS[(size_t)(c0 + i) * hd + k0 + kk] : 0.0;
-      }
-      for (int e = threadIdx.x; e < hd * KT; e += NT) {
-        const int j = e / KT, kk = e % KT;
-        sH[j * ks + kk] = k0 + kk < hd ? H[(size_t)j * hd + k0 + kk] : 0.0;
-      }
-      __syncthreads();
+    for (int u = 0; u < NBX; ++u)
 #pragma unroll
-      for (int u = 0; u < MAXB; ++u) {
-        const int e = threadIdx.x + NT * u;
-        if (e < nc * hd) {
-          const double* pp = sP + (e / hd) * ks;
-          const double* hh = sH + (e % hd) * ks;
-          double sacc = bacc[u];
-          for (int kk = 0; kk < KT; ++kk) sacc += pp[kk] * hh[kk];
-          bacc[u] = sacc;
+      for (int v = 0; v < MBX; ++v) { acc[u][v][0] = 0.0; acc[u][v][1] = 0.0; }
+    for (int k0 = 0; k0 < KP; k0 += KT) {
+      __syncthreads();
+      for (int e = threadIdx.x; e < 8 * MBn * KT; e += NT) {
+        const int i = e / KT, kk = e % KT, k = k0 + kk;
+        sP[i * SK + kk] = (i < nc && k < hd) ? PS[(size_t)(c0 + i) * hd + k] : 0.0;
+      }
+      for (int e = threadIdx.x; e < 8 * NBn * KT; e += NT) {
+        const int j = e / KT, kk = e % KT, k = k0 + kk;
+        sH[j * SK + kk] = (j < hd && k < hd) ? H[(size_t)j * hd + k] : 0.0;
+      }
+      __syncthreads();
+      const int kst = min(KT, KP - k0) / 4;
+      for (int ks = 0; ks < kst; ++ks) {
+        const int kc = 4 * ks + (lane & 3);
+#pragma unroll
+        for (int u = 0; u < NBX; ++u) {
+          const int nb = wid + NW * u;
+          if (nb >= NBn) continue;
+          const double bv = sH[(8 * nb + (lane >> 2)) * SK + kc];
+#pragma unroll
+          for (int v = 0; v < MBX; ++v)
+            if (v < MBn) dmma(acc[u][v][0], acc[u][v][1], sP[(8 * v + (lane >> 2)) * SK + kc], bv);
         }
       }
     }
 #pragma unroll
-    for (int u = 0; u < MAXB; ++u) {
-      const int e = threadIdx.x + NT * u;
-      if (e < nc * hd) B[(size_t)(c0 + e / hd) * hd + e % hd] = bacc[u];
+    for (int u = 0; u < NBX; ++u) {
+      const int nb = wid + NW * u;
+      if (nb >= NBn) continue;
+#pragma unroll
+      for (int v = 0; v < MBX; ++v) {
+        const int i = 8 * v + (lane >> 2);
+        if (v >= MBn || i >= nc) continue;
+#pragma unroll
+        for (int h2 = 0; h2 < 2; ++h2) {
+          const int j = 8 * nb + 2 * (lane & 3) + h2;
+          if (j < hd) B[(size_t)(c0 + i) * hd + j] = acc[u][v][h2];
+        }
+      }
     }
   }
 }
