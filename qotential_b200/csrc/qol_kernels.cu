@@ -1791,13 +1791,16 @@ __global__ void __launch_bounds__(256, 2) k_rrq_apply(OrderTab T, PanelIn P, Pai
     const double* RS = R.RS + (size_t)(g0 + c0) * hd;
     /* Ad[t][j] = sum_q JD[t][q] PD[j][q] */
     apply_dmma<NB>(N4, acc, sAt, sBt, [&](int k0, double* a, double* bt) {
-      for (int e = threadIdx.x; e < AT * AK; e += blockDim.x) {
-        const int t = e / AK, k = e % AK;
-        cp_or_zero(&a[t * AKS + k], JD + (size_t)t * N4 + k0 + k, t < nt && k0 + k < N4);
+      /* 16-byte pieces: N4 is even, so a piece never straddles the row end */
+      for (int e = threadIdx.x; e < AT * AK / 2; e += blockDim.x) {
+        const int t = e / (AK / 2), k = 2 * (e % (AK / 2));
+        if (t < nt && k0 + k < N4) cp_async16(&a[t * AKS + k], JD + (size_t)t * N4 + k0 + k);
+        else { a[t * AKS + k] = 0.0; a[t * AKS + k + 1] = 0.0; }
       }
-      for (int e = threadIdx.x; e < 8 * NB * AK; e += blockDim.x) {
-        const int j = e / AK, k = e % AK;
-        cp_or_zero(&bt[j * AKS + k], PD + (size_t)j * N4 + k0 + k, j < hd && k0 + k < N4);
+      for (int e = threadIdx.x; e < 8 * NB * AK / 2; e += blockDim.x) {
+        const int j = e / (AK / 2), k = 2 * (e % (AK / 2));
+        if (j < hd && k0 + k < N4) cp_async16(&bt[j * AKS + k], PD + (size_t)j * N4 + k0 + k);
+        else { bt[j * AKS + k] = 0.0; bt[j * AKS + k + 1] = 0.0; }
       }
       asm volatile("cp.async.commit_group;\n" ::: "memory");
     });
@@ -1880,12 +1883,23 @@ __global__ void __launch_bounds__(128) k_rrq_pairs(OrderTab T, PairIn Q, PairWS 
 __global__ void __launch_bounds__(256) k_coo_index(OrderTab T, PairIn Q, long long* si, long long* sj) {
   const int pan = blockIdx.x, hd = T.hd;
   const long long p0 = Q.tcxi[pan] - 1, m = Q.tcxi[pan + 1] - Q.tcxi[pan];
-  const long long tot = m * hd;
-  for (long long e = threadIdx.x; e < tot; e += blockDim.x) {
-    long long j = e / m, i = e % m;
-    size_t o = (size_t)p0 * hd + e;
-    si[o] = Q.tcxrow[p0 + i];
-    sj[o] = (long long)pan * hd + j + 1;
+  const long long* row = Q.tcxrow + p0;
+  long long* oi = si + (size_t)p0 * hd;
+  long long* oj = sj + (size_t)p0 * hd;
+  const long long c1 = (long long)pan * hd + 1;
+  if (m * hd < (1LL << 31)) { /* the usual block: 32-bit index arithmetic */
+    const int mi = (int)m, tot = mi * hd;
+    for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+      const int j = e / mi, i = e - j * mi;
+      oi[e] = __ldg(row + i);
+      oj[e] = c1 + j;
+    }
+  } else {
+    for (long long e = threadIdx.x; e < m * hd; e += blockDim.x) {
+      const long long j = e / m, i = e - j * m;
+      oi[e] = __ldg(row + i);
+      oj[e] = c1 + j;
+    }
   }
 }
 
