@@ -1474,7 +1474,7 @@ __host__ __device__ constexpr int mom_rows(int L) { return L * (L + 1); }
 __host__ __device__ constexpr int mom_rec(int nbd) { return (6 * nbd + 4 + 1) & ~1; }
 /* doubles of shared memory of one pair after the line record: the node chunk,
  * later M (entries 14 doubles apart), R(x), the translation's partial sums
- * (12 per slot); T reuses M's space once the translation is done */
+ * (12 per slot, component-major); T reuses M's space once the translation is done */
 __host__ __device__ constexpr int mom_region(int L, int slots) {
   return mom_rows(L) * MOM_CS > 7 * mom_rows(L) + (L + 1) * (L + 2) + 12 * slots
              ? mom_rows(L) * MOM_CS
@@ -1661,10 +1661,10 @@ __global__ void __launch_bounds__(MOM_T) k_rrq_moments(OrderTab T, PairIn Q, Pai
         a[2 * k] += v.x * c - v.y * p;
         a[2 * k + 1] += v.y * q + v.x * d;
       }
-      if (w & (1u << 30)) {
-        double* dst = Pp + 12 * ((w >> 16) & 1023);
+      if (w & (1u << 30)) { /* slots component-major: Pp[c * xslots + slot] */
+        double* dst = Pp + ((w >> 16) & 1023);
 #pragma unroll
-        for (int c2 = 0; c2 < 12; ++c2) { dst[c2] = a[c2]; a[c2] = 0.0; }
+        for (int c2 = 0; c2 < 12; ++c2) { dst[c2 * T.xslots] = a[c2]; a[c2] = 0.0; }
       }
     }
   }
@@ -1673,10 +1673,10 @@ __global__ void __launch_bounds__(MOM_T) k_rrq_moments(OrderTab T, PairIn Q, Pai
     const int ps = (int)T.xred[2 * o], npc = (int)T.xred[2 * o + 1];
     double t[12];
 #pragma unroll
-    for (int c = 0; c < 12; ++c) t[c] = Pp[12 * ps + c];
+    for (int c = 0; c < 12; ++c) t[c] = Pp[c * T.xslots + ps];
     for (int q = 1; q < npc; ++q)
 #pragma unroll
-      for (int c = 0; c < 12; ++c) t[c] += Pp[12 * (ps + q) + c];
+      for (int c = 0; c < 12; ++c) t[c] += Pp[c * T.xslots + ps + q];
 #pragma unroll
     for (int c = 0; c < 12; ++c) Tt[12 * o + c] = t[c];
   }
