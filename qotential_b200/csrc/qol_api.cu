@@ -1219,26 +1219,51 @@ int qol_getnearquad_lap_rrq(qol_int npan, qol_int nterms, qol_int hdim, qol_int 
   long long* dxi = g_arena_io.take<long long>(npan + 1);
   double* dval = g_arena_io.take<double>(2 * nout); /* vs then vd */
   int out = 0;
-  auto cpy = [&](void* d, const void* h, size_t n) {
-    if (!out) {
-      cudaError_t e = cudaMemcpyAsync(d, h, n, cudaMemcpyHostToDevice, st);
-      if (e != cudaSuccess) out = fail(QOL_ERR_CUDA, "input copy: %s", cudaGetErrorString(e));
-    }
-  };
-  cpy(dsx, sx, sizeof(double) * 3 * nsrc);
-  cpy(dsnx, snx, sizeof(double) * 3 * nsrc);
-  cpy(dsw, sw, sizeof(double) * nsrc);
-  cpy(drts, rts, sizeof(double) * 3 * nsrc);
-  cpy(drps, rps, sizeof(double) * 3 * nsrc);
-  cpy(dtcx, tcx, sizeof(double) * 3 * ntcx);
-  cpy(drow, tcxrow, sizeof(long long) * ntcx);
-  cpy(dxi, tcxi, sizeof(long long) * (npan + 1));
-  if (out) { cudaStreamSynchronize(st); return out; }
-  g_host_ms[0] = ms_since(tstart);
-
   const unsigned hw = std::thread::hardware_concurrency();
   /* leave two cores to the launching thread and the copy thread */
   const int nthr = (int)std::min(16u, std::max(2u, hw > 4 ? hw - 2 : 2u));
+  /* inputs through the pinned ring: host threads copy pieces of the caller's
+   * (pageable) arrays into free ring buffers and queue each piece's DMA on the
+   * compute stream; the kernels are queued once every piece has landed */
+  {
+    struct Piece {
+      char* d;
+      const char* h;
+      size_t n;
+    };
+    std::vector<Piece> pcs;
+    auto add = [&](void* d, const void* h, size_t n) {
+      for (size_t off = 0; off < n; off += kStageBytes)
+        pcs.push_back({(char*)d + off, (const char*)h + off, std::min(kStageBytes, n - off)});
+    };
+    add(dsx, sx, sizeof(double) * 3 * nsrc);
+    add(dsnx, snx, sizeof(double) * 3 * nsrc);
+    add(dsw, sw, sizeof(double) * nsrc);
+    add(drts, rts, sizeof(double) * 3 * nsrc);
+    add(drps, rps, sizeof(double) * 3 * nsrc);
+    add(dtcx, tcx, sizeof(double) * 3 * ntcx);
+    add(drow, tcxrow, sizeof(long long) * ntcx);
+    add(dxi, tcxi, sizeof(long long) * (npan + 1));
+    FreeList ifl;
+    std::atomic<int> ierr{0};
+    {
+      Workers IW(nthr);
+      for (const Piece& pc : pcs)
+        IW.submit([&, pc] {
+          const int b = ifl.take();
+          std::memcpy(g_ring.buf[b], pc.h, pc.n);
+          if (cudaMemcpyAsync(pc.d, g_ring.buf[b], pc.n, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+              cudaEventRecord(g_ring.ev[b], st) != cudaSuccess || cudaEventSynchronize(g_ring.ev[b]) != cudaSuccess)
+            ierr = 1;
+          ifl.give(b);
+        });
+    } /* joins the threads: every piece has landed */
+    if (ierr) {
+      cudaStreamSynchronize(st);
+      return fail(QOL_ERR_CUDA, "input copy through the staging ring failed");
+    }
+  }
+  g_host_ms[0] = ms_since(tstart);
   std::atomic<int> werr{0};
   {
     Workers W(nthr);
