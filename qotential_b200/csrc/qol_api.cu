@@ -510,7 +510,7 @@ int tables_match(int nquad, int korder, const double* tgl, const double* wgl, co
  * into the caller's arrays.  The COO indices are a layout function of
  * tcxrow/tcxi (k_coo_index computes the same), so that entry point fills them
  * on host threads while the GPU works instead of moving them over the link. */
-/* small pieces: the ring (32 MiB) can stay in the host's last-level cache
+/* small pieces: the ring (24 x 2 MiB) can stay in the host's last-level cache
  * between the DMA write and the copy out */
 constexpr size_t kStageBytes = (size_t)2 << 20;
 /* wall-clock milestones of the last host-pointer call, ms from its start:
@@ -520,7 +520,7 @@ double g_host_ms[7] = {0, 0, 0, 0, 0, 0, 0};
 inline double ms_since(std::chrono::steady_clock::time_point t0) {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
-constexpr int kNStage = 16;
+constexpr int kNStage = 24;
 
 struct StageRing {
   void* buf[kNStage] = {};
