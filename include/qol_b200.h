@@ -180,10 +180,13 @@ int qol_set_sum_precision(int mode);
  * qol_selector_features: the 8 features (FP32, row-major ntcx x 8) and the
  *   plain walk's level (1..5) of every near pair of a getnearquad input;
  * qol_selector_grad: mean cross-entropy and its gradient over n samples with
- *   weights w (QOL_SELECTOR_NW floats: W1 8x64, b1, W2 64x64, b2, W3 64x5, b3);
+ *   weights w (QOL_SELECTOR_NW floats: W1 8x64, b1, W2 64x64, b2, W3 64x5, b3),
+ *   as training computes it (BF16 operands, FP32 sums);
  * qol_selector_train: Adam on the GPU, `epochs` passes over a shuffle seeded
- *   by `seed`, batches of `batch` (a multiple of 256) samples; w in: initial,
- *   out: trained; loss[e] the mean loss of epoch e;
+ *   by `seed`, batches of `batch` (a multiple of 256) samples; forward and
+ *   backward with BF16 operands (weights, features, activations) and FP32
+ *   sums, FP32 master weights; w in: initial, out: trained; loss[e] the mean
+ *   loss of epoch e;
  * qol_selector_set: mode 1 makes the calls that follow use the selector with
  *   w rounded to BF16 (FP32 accumulation): a prediction with softmax
  *   probability >= conf of a direct level l is used when the target lies

@@ -72,20 +72,31 @@ def pair_features(npan, hd, sx, snx, sw, tcx, tcxi):
     return out
 
 
+def bf16(a):
+    """float32 values rounded to BF16 (nearest, ties to even), as float64"""
+    u = np.asarray(a, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    u = ((u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000).astype(np.uint32)
+    return u.view(np.float32).astype(np.float64)
+
+
 def unpack(w):
     w = np.asarray(w, dtype=np.float64)
     return (w[OW1:OB1].reshape(F, H), w[OB1:OW2], w[OW2:OB2].reshape(H, H), w[OB2:OW3],
             w[OW3:OB3].reshape(H, NC), w[OB3:NW])
 
 
-def loss_grad(w, x, y):
-    """mean cross-entropy of the MLP (ReLU, ReLU, softmax) and its gradient"""
-    W1, b1, W2, b2, W3, b3 = unpack(w)
-    x = np.asarray(x, dtype=np.float64)
+def loss_grad(w, x, y, bf=False):
+    """mean cross-entropy of the MLP (ReLU, ReLU, softmax) and its gradient;
+    bf: the library's BF16 operands (weights, inputs and hidden activations
+    rounded to BF16, sums exact), the gradient taken with respect to the
+    rounded weights"""
+    r = bf16 if bf else (lambda a: np.asarray(a, dtype=np.float64))
+    W1, b1, W2, b2, W3, b3 = unpack(r(w) if bf else w)
+    x = r(x)
     a1 = x @ W1 + b1
-    h1 = np.maximum(a1, 0.0)
+    h1 = r(np.maximum(a1, 0.0))
     a2 = h1 @ W2 + b2
-    h2 = np.maximum(a2, 0.0)
+    h2 = r(np.maximum(a2, 0.0))
     z = h2 @ W3 + b3
     zm = z.max(1, keepdims=True)
     e = np.exp(z - zm)

@@ -18,8 +18,11 @@
  * (logs of arguments clamped below at 1e-12).
  *
  * Weights: W1[f][i] (8 x 64), b1, W2[i][j] (64 x 64), b2, W3[j][k] (64 x 5),
- * b3, in that order; training keeps them in FP32, inference uses their BF16
- * roundings with FP32 accumulation. */
+ * b3, in that order.  Training and inference compute with BF16 operands
+ * (the weights, the features and the hidden activations rounded to BF16) and
+ * FP32 sums; training keeps FP32 master weights for the Adam step and takes
+ * the gradient with respect to the rounded weights. */
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <cstdint>
 #include "qol_kernels.h"
@@ -29,6 +32,11 @@ namespace {
 constexpr int F = QOL_SEL_F, H = QOL_SEL_H, NC = QOL_SEL_C;
 constexpr int OW1 = 0, OB1 = OW1 + F * H, OW2 = OB1 + H, OB2 = OW2 + H * H, OW3 = OB2 + H, OB3 = OW3 + H * NC;
 static_assert(OB3 + NC == QOL_SEL_NW, "weight layout");
+
+/* the BF16 rounding (nearest, ties to even) of x, as a float: the operands
+ * of the MLP (weights, features, hidden activations) are BF16 values, its sums
+ * FP32 */
+__device__ __forceinline__ float bf(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
 
 /* the panel descriptor: c(3), nb(3), e1(3), e2(3), D, kappa, ln(aspect); one
  * warp, lanes over the panel's nodes, shuffle sums in a fixed order */
@@ -128,14 +136,16 @@ __global__ void __launch_bounds__(128) k_sel_features(int hd, PanelIn P, PairIn 
 }
 
 /* logits of one feature vector with the weights in shared memory */
-__device__ __forceinline__ void sel_forward(const float* w, const float* x, float* z) {
-  float h1[H];
+__device__ __forceinline__ void sel_forward(const float* w, const float* xin, float* z) {
+  float x[F], h1[H];
+#pragma unroll
+  for (int c = 0; c < F; ++c) x[c] = bf(xin[c]);
 #pragma unroll
   for (int i = 0; i < H; ++i) {
     float a = w[OB1 + i];
 #pragma unroll
     for (int c = 0; c < F; ++c) a = fmaf(w[OW1 + c * H + i], x[c], a);
-    h1[i] = fmaxf(a, 0.0f);
+    h1[i] = bf(fmaxf(a, 0.0f));
   }
 #pragma unroll
   for (int k = 0; k < NC; ++k) z[k] = w[OB3 + k];
@@ -143,7 +153,7 @@ __device__ __forceinline__ void sel_forward(const float* w, const float* x, floa
     float a = w[OB2 + j];
 #pragma unroll
     for (int i = 0; i < H; ++i) a = fmaf(w[OW2 + i * H + j], h1[i], a);
-    a = fmaxf(a, 0.0f);
+    a = bf(fmaxf(a, 0.0f));
 #pragma unroll
     for (int k = 0; k < NC; ++k) z[k] = fmaf(w[OW3 + j * NC + k], a, z[k]);
   }
@@ -218,13 +228,13 @@ __global__ void __launch_bounds__(GT) k_sel_grad(const float* feat, const signed
   float* DZ = H2 + GT * GS;        /* GT x 6 */
   __shared__ double red[GT / 32];
   const int t = threadIdx.x;
-  for (int e = t; e < QOL_SEL_NW; e += GT) w[e] = wg[e];
+  for (int e = t; e < QOL_SEL_NW; e += GT) w[e] = bf(wg[e]); /* BF16 operands of the FP32 master weights */
   const long long gi = n0 + (long long)blockIdx.x * GT + t;
   const bool ok = gi < n1;
   const int s = ok ? idx[gi] : 0;
   float x[F];
 #pragma unroll
-  for (int c = 0; c < F; ++c) x[c] = ok ? feat[(size_t)s * F + c] : 0.0f;
+  for (int c = 0; c < F; ++c) x[c] = ok ? bf(feat[(size_t)s * F + c]) : 0.0f;
 #pragma unroll
   for (int c = 0; c < F; ++c) X[t * 9 + c] = x[c];
   __syncthreads();
@@ -233,7 +243,7 @@ __global__ void __launch_bounds__(GT) k_sel_grad(const float* feat, const signed
     float a = w[OB1 + i];
 #pragma unroll
     for (int c = 0; c < F; ++c) a = fmaf(w[OW1 + c * H + i], x[c], a);
-    H1[t * GS + i] = fmaxf(a, 0.0f);
+    H1[t * GS + i] = bf(fmaxf(a, 0.0f));
   }
   float z[NC];
 #pragma unroll
@@ -241,7 +251,7 @@ __global__ void __launch_bounds__(GT) k_sel_grad(const float* feat, const signed
   for (int j = 0; j < H; ++j) {
     float a = w[OB2 + j];
     for (int i = 0; i < H; ++i) a = fmaf(w[OW2 + i * H + j], H1[t * GS + i], a);
-    a = fmaxf(a, 0.0f);
+    a = bf(fmaxf(a, 0.0f));
     H2[t * GS + j] = a;
 #pragma unroll
     for (int k = 0; k < NC; ++k) z[k] = fmaf(w[OW3 + j * NC + k], a, z[k]);

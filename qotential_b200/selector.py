@@ -39,8 +39,9 @@ def training_set(n_pairs=1_000_000, seed=11, orders=(4, 6, 8, 10, 12), noff=5000
 
 
 def predict(w, feat):
-    """class and softmax probability of each feature row with weights w (FP32,
-    rounded to BF16 as the library uses them)"""
+    """class and softmax probability of each feature row with weights w (FP32
+    masters; weights, features and activations rounded to BF16 as the library's
+    kernels use them)"""
     w = np.asarray(w, dtype=np.float32)
     u = w.view(np.uint32).astype(np.uint64)
     u = ((u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000).astype(np.uint32)
@@ -48,8 +49,14 @@ def predict(w, feat):
     W1, b1 = wb[0:512].reshape(8, 64), wb[512:576]
     W2, b2 = wb[576:4672].reshape(64, 64), wb[4672:4736]
     W3, b3 = wb[4736:5056].reshape(64, 5), wb[5056:5061]
-    h = np.maximum(np.asarray(feat, np.float64) @ W1 + b1, 0.0)
-    z = np.maximum(h @ W2 + b2, 0.0) @ W3 + b3
+
+    def r(a):  # BF16 operands, as the library's kernels
+        v = np.asarray(a, np.float32).view(np.uint32).astype(np.uint64)
+        v = ((v + 0x7FFF + ((v >> 16) & 1)) & 0xFFFF0000).astype(np.uint32)
+        return v.view(np.float32).astype(np.float64)
+
+    h = r(np.maximum(r(feat) @ W1 + b1, 0.0))
+    z = r(np.maximum(h @ W2 + b2, 0.0)) @ W3 + b3
     e = np.exp(z - z.max(1, keepdims=True))
     p = e / e.sum(1, keepdims=True)
     return p.argmax(1), p.max(1)
