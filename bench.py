@@ -582,6 +582,7 @@ def main():
     peak = C.c_double(0.0)
     L.qol_probe_fp64_peak(C.byref(peak))
     roofline = roofline_line(W, hist, dict(zip(names, (float(v) for v in ms_ph))), peak.value)
+    roofline["panel_shape"] = list(qol.qol_panel_shape(W["nterms"], W["nquad"], W["nquad"]))  # (cluster, threads)
 
     if args.kernels_only:
         if rank == 0:

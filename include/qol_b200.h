@@ -172,6 +172,14 @@ int qol_direct_farfield(qol_int nsrc, const double* sx, const double* snx, const
  * fits stay FP64.  qol_rrq_noalloc always uses FP64.  No counterpart in the
  * reference (all FP64). */
 int qol_set_sum_precision(int mode);
+/* Autotuning of the per-panel precompute kernel (no counterpart in the
+ * reference): with on = 1 (default) the first call of an order with at least
+ * 256 panels times each (cluster size, CTA threads) shape the kernel has for
+ * that order on 512 panels and keeps the fastest with the order's tables
+ * (every shape gives the same results); 0 keeps the built-in choice.
+ * qol_panel_shape returns the shape kept for an order (0, 0 before one is). */
+int qol_set_autotune(int on);
+int qol_panel_shape(qol_int nterms, qol_int orderff, qol_int nquad, int* cs, int* nt);
 /* Learned level selector (no counterpart in the reference; it stands in for
  * the ball-test level walk of lap3dsdlpmat_levels_r64,
  * patch_refine_mod.f90:516-551).  An MLP 8 -> 64 -> 64 -> 5 on geometry

@@ -17,7 +17,7 @@ __all__ = [
     "qol_clear_patch_levels", "qol_clear_patch_levels_all", "qol_rrq", "qol_getnearquad_lap_rrq",
     "qol_getnearquad_lap_rrq_dev", "qol_grf_near", "qol_direct_farfield", "qol_set_sum_precision",
     "SELECTOR_NW", "qol_selector_features", "qol_selector_grad", "qol_selector_train", "qol_selector_set",
-    "qol_selector_stats",
+    "qol_selector_stats", "qol_set_autotune", "qol_panel_shape",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -320,3 +320,16 @@ def qol_selector_stats():
     c = np.zeros(3, np.int64)
     _check(lib().qol_selector_stats(_vp(c)))
     return {"accepted": int(c[0]), "low_confidence": int(c[1]), "check_failed": int(c[2])}
+
+
+def qol_set_autotune(on):
+    """1 (default): the first call of an order with >= 256 panels measures the
+    per-panel precompute kernel's shapes and keeps the fastest; 0: built-in shape."""
+    _check(lib().qol_set_autotune(C.c_int(int(on))))
+
+
+def qol_panel_shape(nterms, orderff, nquad):
+    """(cluster size, CTA threads) kept for an order, (0, 0) before any"""
+    cs, nt = C.c_int(0), C.c_int(0)
+    _check(lib().qol_panel_shape(i64(nterms), i64(orderff), i64(nquad), C.byref(cs), C.byref(nt)))
+    return cs.value, nt.value

@@ -95,6 +95,7 @@ Arena g_arena, g_arena2, g_arena_io, g_arena_grf; /* pipeline, per-pair RRQ stor
 /* per-phase device milliseconds of the pipeline (diagnostics) */
 int g_ktime_on = 0;
 int g_sum_precision = 0; /* 0 FP64 (the drop-in), 1 FP32 level sums */
+int g_autotune = 1;      /* measure k_rrq_panel's shape once per order */
 /* learned level selector: off (0) or on (1), its BF16-rounded weights on the
  * device, the confidence threshold, and the decision counters of the calls */
 int g_sel_mode = 0;
@@ -389,6 +390,41 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
   R.side = g_arena2.take<signed char>((size_t)std::max<long long>(nrrq, 1));
   OutCOO O{};
   O.vs = J.vs; O.vd = J.vd; O.omega = J.omega; O.subtract_naive = J.subtract_naive;
+  /* k_rrq_panel's (cluster, threads) shape, measured once per order on the
+   * first call with enough panels: each shape on the first 512 panels, one
+   * warm-up and one timed launch; every shape gives the same results, the
+   * fastest is kept with the order's tables */
+  if (nrrq > 0 && g_autotune && !C->T.panel_cs && npan >= 256) {
+    int cs[8], nt[8];
+    const int ns = qol_panel_shapes(hd, nq, cs, nt, 8);
+    int best = 0;
+    if (ns > 1) {
+      cudaEvent_t e0 = nullptr, e1 = nullptr;
+      CK(cudaEventCreate(&e0));
+      CK(cudaEventCreate(&e1));
+      float bms = 0.f;
+      for (int i = 0; i < ns; ++i) {
+        OrderTab Tt = T;
+        Tt.panel_cs = cs[i];
+        Tt.panel_nt = nt[i];
+        const int np2 = std::min(npan, 512);
+        CK(qol_launch_rrq_panel(Tt, J.P, G, R, np2, J.chart, st));
+        CK(cudaEventRecord(e0, st));
+        CK(qol_launch_rrq_panel(Tt, J.P, G, R, np2, J.chart, st));
+        CK(cudaEventRecord(e1, st));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        if (i == 0 || ms < bms) { best = i; bms = ms; }
+      }
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+    }
+    if (ns > 0) {
+      C->T.panel_cs = T.panel_cs = cs[best];
+      C->T.panel_nt = T.panel_nt = nt[best];
+    }
+  }
   /* one pass over all panels, or (host entry) panel chunks whose every phase
    * runs before the next chunk's, so that chunk c's values are final early
    * and leave the GPU while later chunks compute */
@@ -721,6 +757,23 @@ int qol_kernel_times(int enable, double* ms, qol_int* calls) {
   return 0;
 }
 int qol_version(void) { return 100; }
+
+int qol_set_autotune(int on) {
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  if (on != 0 && on != 1) return fail(QOL_ERR_ARG, "autotune must be 0 or 1");
+  g_autotune = on;
+  return 0;
+}
+
+int qol_panel_shape(qol_int nterms, qol_int orderff, qol_int nquad, int* cs, int* nt) {
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  if (!cs || !nt) return fail(QOL_ERR_ARG, "null argument");
+  *cs = 0; *nt = 0;
+  const long long key = nterms + 100LL * orderff + 10000LL * nquad;
+  auto it = g_orders.find(key);
+  if (it != g_orders.end()) { *cs = it->second->T.panel_cs; *nt = it->second->T.panel_nt; }
+  return 0;
+}
 
 int qol_set_sum_precision(int mode) {
   std::lock_guard<std::recursive_mutex> g(g_mu);

@@ -1988,11 +1988,15 @@ cudaError_t qol_launch_rrq_panel(const OrderTab& T, const PanelIn& P, const Pair
    * rows to keep them in registers: at most 6 rows with 512 threads (128
    * registers a thread), 12 with 384 */
   int cs = 0, nt = 0, maxr = 0;
-  for (int c = 1; c <= 8 && !cs; c *= 2)
-    for (int t : {512, 384}) {
-      const int m = panel_maxr(T.hd, c, t);
-      if (m <= (t == 512 ? 6 : 12)) { cs = c; nt = t; maxr = m; break; }
-    }
+  if (T.panel_cs) { /* a shape chosen by measurement (qol_panel_shapes lists them) */
+    cs = T.panel_cs; nt = T.panel_nt; maxr = panel_maxr(T.hd, cs, nt);
+  } else {
+    for (int c = 1; c <= 8 && !cs; c *= 2)
+      for (int t : {512, 384}) {
+        const int m = panel_maxr(T.hd, c, t);
+        if (m <= (t == 512 ? 6 : 12)) { cs = c; nt = t; maxr = m; break; }
+      }
+  }
   if (!cs) return cudaErrorInvalidConfiguration;
   const size_t smem = sizeof(double) * panel_smem_doubles(T.hd, 3 * T.nquad, cs);
   if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
@@ -2021,6 +2025,21 @@ cudaError_t qol_launch_rrq_panel(const OrderTab& T, const PanelIn& P, const Pair
   QOL_PANEL_CASE(4, 512, 6) QOL_PANEL_CASE(4, 384, 10) QOL_PANEL_CASE(8, 512, 5)
 #undef QOL_PANEL_CASE
   return cudaErrorInvalidConfiguration;
+}
+int qol_panel_shapes(int hd, int nquad, int* cs, int* nt, int cap) {
+  /* the instantiated (cluster, threads, row bound) triples of qol_launch_rrq_panel */
+  static const int inst[][3] = {{1, 512, 5}, {1, 384, 10}, {2, 512, 6}, {2, 384, 12}, {4, 512, 6}, {4, 384, 10}, {8, 512, 5}};
+  int n = 0;
+  for (const auto& in : inst) {
+    const int c = in[0], t = in[1];
+    if (panel_maxr(hd, c, t) > in[2] || panel_ncol(hd, c) > t) continue;
+    if (sizeof(double) * panel_smem_doubles(hd, 3 * nquad, c) > 227 * 1024) continue;
+    const int mbn = (panel_ncol(hd, c) + 7) / 8, nbn = (hd + 7) / 8;
+    if (mbn > 8 || nbn > 2 * (t / 32)) continue; /* the B epilogue's blocks a warp */
+    if (n < cap) { cs[n] = c; nt[n] = t; }
+    ++n;
+  }
+  return n < cap ? n : cap;
 }
 cudaError_t qol_launch_rrq_pairs(const OrderTab& T, const PairIn& Q, const PairWS& G, const RRQWS& R, int npan,
                                  cudaStream_t st) {

@@ -14,6 +14,7 @@ struct OrderTab {
   const unsigned* interp_hi[4], *interp_lo[4]; /* interp in FP32 as TF32 high and low parts (precision variant),
                                                   in mma B-fragment order, rows zero-padded to tiles of 32 */
   int ncw;                    /* 32 ceil(hd / 32) */
+  int panel_cs, panel_nt;     /* k_rrq_panel's cluster size and CTA threads (0: the default choice) */
   const double* wt[4];        /* n_l */
   const long long* suboff[4]; /* nsub_l + 1 */
   const int* subtyp[4];       /* nsub_l */
@@ -105,6 +106,9 @@ cudaError_t qol_launch_direct(const OrderTab& T, const PanelIn& P, const PairIn&
 cudaError_t qol_launch_scan(int npan, int lev, const int* cnt, long long* off, cudaStream_t st);
 cudaError_t qol_launch_rrq_panel(const OrderTab& T, const PanelIn& P, const PairWS& G, const RRQWS& R, int npan,
                                  const double* chart, cudaStream_t st);
+/* the (cluster size, CTA threads) shapes k_rrq_panel has for hdim hd (results do
+ * not depend on the shape); returns how many, at most cap */
+int qol_panel_shapes(int hd, int nquad, int* cs, int* nt, int cap);
 cudaError_t qol_launch_rrq_pairs(const OrderTab& T, const PairIn& Q, const PairWS& G, const RRQWS& R, int npan,
                                  cudaStream_t st);
 cudaError_t qol_launch_rrq_ssq(const OrderTab& T, const PairIn& Q, const PairWS& G, const RRQWS& R, cudaStream_t st);

@@ -117,3 +117,13 @@ def test_selector_arguments_checked(qol):
     with pytest.raises(qol.QolError) as e:
         qol.qol_selector_train(f, np.zeros(4), w, epochs=1, batch=100)  # batch not a multiple of 256
     assert e.value.code == 8
+
+
+def test_autotune_switch_host_only(qol):
+    """the autotune switch accepts 0 and 1 only; an order never run has no kept shape"""
+    with pytest.raises(qol.QolError) as e:
+        qol.qol_set_autotune(2)
+    assert e.value.code == 8
+    qol.qol_set_autotune(0)
+    qol.qol_set_autotune(1)
+    assert qol.qol_panel_shape(15, 17, 17) == (0, 0)

@@ -180,3 +180,26 @@ def test_grf_identity_gpu(qol, orc):
         errs.append(np.abs(un).max() / np.abs(ubn).max())
     # oracle on the same inputs: 4.1e-4, 9.0e-6, 8.8e-7
     assert errs[0] < 1e-3 and errs[1] < 2e-5 and errs[2] < 2e-6, errs
+
+
+def test_autotuned_panel_shape_same_results(qol):
+    """the panel kernel's shape chosen by measurement gives the built-in
+    shape's results byte for byte (the shapes only split the same arithmetic)"""
+    from qotential_b200 import geometry as G
+    nterms = 7  # an order no other test here uses, so its shape is not chosen yet
+    P, hd, tcxi, tcxrow, tcx, _ = _setup(G, G.stellarator(), 16, 40, nterms)
+    npan = P["sw"].size // hd
+    assert npan >= 256
+    args = (npan, nterms, hd, nterms + 2, npan * hd, P["sx"], P["snx"], P["sw"], P["rts"], P["rps"], tcxrow.size, tcx,
+            tcxrow, tcxi, nterms + 2, 1.4, 30)
+    qol.qol_set_autotune(0)
+    try:
+        a = qol.qol_getnearquad_lap_rrq(*args)
+        assert qol.qol_panel_shape(nterms, nterms + 2, nterms + 2) == (0, 0)
+    finally:
+        qol.qol_set_autotune(1)
+    b = qol.qol_getnearquad_lap_rrq(*args)
+    cs, nt = qol.qol_panel_shape(nterms, nterms + 2, nterms + 2)
+    assert cs in (1, 2, 4, 8) and nt in (384, 512)
+    for x, y in zip(a[:4], b[:4]):
+        assert x.tobytes() == y.tobytes()
