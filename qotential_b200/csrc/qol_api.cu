@@ -400,25 +400,26 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
     int best = 0;
     if (ns > 1) {
       cudaEvent_t e0 = nullptr, e1 = nullptr;
-      CK(cudaEventCreate(&e0));
-      CK(cudaEventCreate(&e1));
+      cudaError_t te = cudaEventCreate(&e0);
+      if (te == cudaSuccess) te = cudaEventCreate(&e1);
       float bms = 0.f;
-      for (int i = 0; i < ns; ++i) {
+      for (int i = 0; i < ns && te == cudaSuccess; ++i) {
         OrderTab Tt = T;
         Tt.panel_cs = cs[i];
         Tt.panel_nt = nt[i];
         const int np2 = std::min(npan, 512);
-        CK(qol_launch_rrq_panel(Tt, J.P, G, R, np2, J.chart, st));
-        CK(cudaEventRecord(e0, st));
-        CK(qol_launch_rrq_panel(Tt, J.P, G, R, np2, J.chart, st));
-        CK(cudaEventRecord(e1, st));
-        CK(cudaEventSynchronize(e1));
         float ms = 0.f;
-        CK(cudaEventElapsedTime(&ms, e0, e1));
+        if ((te = qol_launch_rrq_panel(Tt, J.P, G, R, np2, J.chart, st)) != cudaSuccess ||
+            (te = cudaEventRecord(e0, st)) != cudaSuccess ||
+            (te = qol_launch_rrq_panel(Tt, J.P, G, R, np2, J.chart, st)) != cudaSuccess ||
+            (te = cudaEventRecord(e1, st)) != cudaSuccess || (te = cudaEventSynchronize(e1)) != cudaSuccess ||
+            (te = cudaEventElapsedTime(&ms, e0, e1)) != cudaSuccess)
+          break;
         if (i == 0 || ms < bms) { best = i; bms = ms; }
       }
-      cudaEventDestroy(e0);
-      cudaEventDestroy(e1);
+      if (e0) cudaEventDestroy(e0);
+      if (e1) cudaEventDestroy(e1);
+      CK(te);
     }
     if (ns > 0) {
       C->T.panel_cs = T.panel_cs = cs[best];
