@@ -295,7 +295,7 @@ def learned_form(W, D, out, steps, warmup, conf=0.9):
 
 
 def batched_config(reps=2):
-    """64 seeded surfaces of the family R = R0 + a cos p +
+    """The batched-surfaces workload: 64 seeded surfaces of the family R = R0 + a cos p +
     d cos(p - Nfp t) (R0 ~ U(3,6), a ~ U(0.5,1.5), d ~ U(0,0.3), Nfp in 1..5),
     grids 4x8 .. 16x64, orders drawn from {4,6,8,10,12}, all surface nodes plus
     5000 off-surface targets each; the device entry point with inputs resident,
