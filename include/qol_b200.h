@@ -118,18 +118,23 @@ int qol_getnearquad_lap_rrq_dev(qol_int npan, qol_int nterms, qol_int hdim, qol_
  * codes on a latency-critical path where cudaMalloc's implicit device-wide
  * synchronisation is not allowed.  Allocates no GPU memory: all workspace and
  * the per-order tables live in one static device array of 16 MiB, held by
- * every GPU that loads the library until exit.  Every array argument is a
- * device pointer; work is queued on `stream` (0 = the legacy default stream)
- * with one host synchronisation inside.
+ * every GPU that loads the library until exit.  Every array argument must be
+ * device (or managed) memory of the current device (checked: QOL_ERR_ARG
+ * otherwise); work is queued on `stream` (0 = the legacy default stream), and
+ * every call waits once on the host for `stream` (it reads the number of RRQ
+ * targets back before sizing the per-target launches).
  *  - The first call on a device sets up (takes the array's device address with
  *    cudaGetSymbolAddress, uploads constants); make that first call before
  *    any stream capture.  A call with a new (order, orderff, nquad) re-uploads
  *    the tables into the array.
  *  - Calls share the array: calls that overlap on the GPU (other streams, other
  *    host threads' work still running) race.  Serialize them.
- *  - Limit: the tables plus 5*hdim doubles per target must fit in 16 MiB
- *    (order 12, orderff 15: about 2,500 targets per call); larger requests
- *    return QOL_ERR_LIMIT (9) with a message from qol_noalloc_last_error(). */
+ *  - Limit: the order's tables, the refined levels of the panel and the panel's
+ *    matrices (7 hdim^2 doubles), plus per target 8 (5 hdim + 24 nquad + 13)
+ *    + 22 bytes, must fit in 16 MiB: at order 13 (hdim 91), nquad = orderff
+ *    = 15, that is 6,646 bytes a target and at most 1,649 targets a call
+ *    (5,324 at order 7); larger requests return QOL_ERR_LIMIT (9) with the
+ *    bytes needed in qol_noalloc_last_error(). */
 int qol_rrq_noalloc(qol_int m, const double* tx, qol_int n, const double* sx, const double* snx,
                     const double* sw, const double* rts, const double* rps, qol_int order, qol_int nquad,
                     qol_int orderff, double distff, qol_int exterior, double* As, double* Ad, void* stream);

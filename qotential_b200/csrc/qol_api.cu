@@ -122,8 +122,7 @@ int ensure_device() {
         hc[l * (QOL_MAXL + 2) + m] = 1.0 / std::sqrt((double)(l - m) * (double)(l + m));
       }
     }
-    qol_upload_harm_coefs(hb.data(), hc.data(), hcm.data(), g_stream);
-    CK(cudaStreamSynchronize(g_stream));
+    CK(qol_upload_harm_coefs(hb.data(), hc.data(), hcm.data(), g_stream));
     g_coefs_uploaded = true;
   }
   return 0;

@@ -36,12 +36,14 @@ __constant__ double c_lb[QOL_MAXNQ + 2];            /* k/(k+1) */
 __constant__ double c_rk[QOL_MAXNQ + 2];            /* 1/k, 0 at k = 0 */
 __device__ double g_jq[QOL_MAXL + 1][QOL_MAXL + 1][4]; /* Jacobi P^(2a+1,0)_b: (c2, c3, c4)/c1 */
 
-void qol_upload_harm_coefs(const double* hb, const double* hc, const double* hcm, cudaStream_t st) {
-  cudaMemcpyToSymbolAsync(c_hb, hb, sizeof(double) * (QOL_MAXL + 2) * (QOL_MAXL + 2), 0,
-                          cudaMemcpyHostToDevice, st);
-  cudaMemcpyToSymbolAsync(c_hc, hc, sizeof(double) * (QOL_MAXL + 2) * (QOL_MAXL + 2), 0,
-                          cudaMemcpyHostToDevice, st);
-  cudaMemcpyToSymbolAsync(c_hcm, hcm, sizeof(double) * (QOL_MAXL + 2), 0, cudaMemcpyHostToDevice, st);
+cudaError_t qol_upload_harm_coefs(const double* hb, const double* hc, const double* hcm, cudaStream_t st) {
+  cudaError_t err = cudaSuccess;
+  auto keep = [&](cudaError_t e) { if (err == cudaSuccess) err = e; };
+  keep(cudaMemcpyToSymbolAsync(c_hb, hb, sizeof(double) * (QOL_MAXL + 2) * (QOL_MAXL + 2), 0,
+                          cudaMemcpyHostToDevice, st));
+  keep(cudaMemcpyToSymbolAsync(c_hc, hc, sizeof(double) * (QOL_MAXL + 2) * (QOL_MAXL + 2), 0,
+                          cudaMemcpyHostToDevice, st));
+  keep(cudaMemcpyToSymbolAsync(c_hcm, hcm, sizeof(double) * (QOL_MAXL + 2), 0, cudaMemcpyHostToDevice, st));
   const int M = QOL_MAXL + 2;
   double rq[M][M] = {}, rn[M][M] = {}, rd[M] = {}, rinv[M] = {};
   double fact[2 * M];
@@ -54,17 +56,17 @@ void qol_upload_harm_coefs(const double* hb, const double* hc, const double* hcm
       rn[l][m] = std::sqrt(fact[l - m] * fact[l + m]);
     }
   }
-  cudaMemcpyToSymbolAsync(c_rq, rq, sizeof(rq), 0, cudaMemcpyHostToDevice, st);
-  cudaMemcpyToSymbolAsync(c_rn, rn, sizeof(rn), 0, cudaMemcpyHostToDevice, st);
-  cudaMemcpyToSymbolAsync(c_rd, rd, sizeof(rd), 0, cudaMemcpyHostToDevice, st);
-  cudaMemcpyToSymbolAsync(c_rinv, rinv, sizeof(rinv), 0, cudaMemcpyHostToDevice, st);
+  keep(cudaMemcpyToSymbolAsync(c_rq, rq, sizeof(rq), 0, cudaMemcpyHostToDevice, st));
+  keep(cudaMemcpyToSymbolAsync(c_rn, rn, sizeof(rn), 0, cudaMemcpyHostToDevice, st));
+  keep(cudaMemcpyToSymbolAsync(c_rd, rd, sizeof(rd), 0, cudaMemcpyHostToDevice, st));
+  keep(cudaMemcpyToSymbolAsync(c_rinv, rinv, sizeof(rinv), 0, cudaMemcpyHostToDevice, st));
   double la[QOL_MAXNQ + 2] = {}, lb[QOL_MAXNQ + 2] = {};
   for (int k = 0; k < QOL_MAXNQ + 2; ++k) { la[k] = (2.0 * k + 1.0) / (k + 1.0); lb[k] = k / (k + 1.0); }
-  cudaMemcpyToSymbolAsync(c_la, la, sizeof(la), 0, cudaMemcpyHostToDevice, st);
-  cudaMemcpyToSymbolAsync(c_lb, lb, sizeof(lb), 0, cudaMemcpyHostToDevice, st);
+  keep(cudaMemcpyToSymbolAsync(c_la, la, sizeof(la), 0, cudaMemcpyHostToDevice, st));
+  keep(cudaMemcpyToSymbolAsync(c_lb, lb, sizeof(lb), 0, cudaMemcpyHostToDevice, st));
   double rk[QOL_MAXNQ + 2] = {};
   for (int k = 1; k < QOL_MAXNQ + 2; ++k) rk[k] = 1.0 / k;
-  cudaMemcpyToSymbolAsync(c_rk, rk, sizeof(rk), 0, cudaMemcpyHostToDevice, st);
+  keep(cudaMemcpyToSymbolAsync(c_rk, rk, sizeof(rk), 0, cudaMemcpyHostToDevice, st));
   static double jq[QOL_MAXL + 1][QOL_MAXL + 1][4];
   for (int a = 0; a <= QOL_MAXL; ++a)
     for (int b = 0; b <= QOL_MAXL; ++b) {
@@ -78,8 +80,9 @@ void qol_upload_harm_coefs(const double* hb, const double* hc, const double* hcm
       jq[a][b][2] = b >= 2 ? c4 / c1 : 0.0;
       jq[a][b][3] = 0.0;
     }
-  cudaMemcpyToSymbolAsync(g_jq, jq, sizeof(jq), 0, cudaMemcpyHostToDevice, st);
-  cudaStreamSynchronize(st); /* the host tables above are locals */
+  keep(cudaMemcpyToSymbolAsync(g_jq, jq, sizeof(jq), 0, cudaMemcpyHostToDevice, st));
+  keep(cudaStreamSynchronize(st)); /* the host tables above are locals */
+  return err;
 }
 
 /* ===================================================================== */

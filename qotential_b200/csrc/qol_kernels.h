@@ -82,7 +82,7 @@ struct OutCOO {
   int subtract_naive;
 };
 
-void qol_upload_harm_coefs(const double* hb, const double* hc, const double* hcm, cudaStream_t st);
+cudaError_t qol_upload_harm_coefs(const double* hb, const double* hc, const double* hcm, cudaStream_t st);
 cudaError_t qol_launch_levels(const OrderTab& T, const PanelIn& P, const LevelWS& W, int npan, cudaStream_t st);
 cudaError_t qol_launch_classify(const OrderTab& T, const PairIn& Q, const LevelWS& W, const PairWS& G, int npan,
                                 cudaStream_t st, int preset = 0 /* nonzero G.level entries are kept */);

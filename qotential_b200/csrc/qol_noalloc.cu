@@ -72,8 +72,7 @@ int na_setup(int dev, cudaStream_t st) {
       hc[l * (QOL_MAXL + 2) + m] = 1.0 / std::sqrt((double)(l - m) * (double)(l + m));
     }
   }
-  qol_upload_harm_coefs(hb.data(), hc.data(), hcm.data(), st);
-  NA_CK(cudaStreamSynchronize(st));
+  NA_CK(qol_upload_harm_coefs(hb.data(), hc.data(), hcm.data(), st));
   D.ready = true;
   return 0;
 }
@@ -160,6 +159,9 @@ int na_tables(NoAllocDev& D, int nterms, int orderff, int nquad, cudaStream_t st
   size_t bytes = (stage.size() + 255) & ~(size_t)255;
   if (bytes > QOL_NOALLOC_SCRATCH_BYTES / 2)
     return na_fail(QOL_ERR_LIMIT, "qol_rrq_noalloc: tables of this order exceed half of the 16 MiB scratch");
+  /* the copy overwrites the front of the scratch: until it has landed no
+   * order's tables are resident, so a failed copy leaves none marked */
+  D.key = -1;
   NA_CK(cudaMemcpyAsync(D.base, stage.data(), stage.size(), cudaMemcpyHostToDevice, st));
   NA_CK(cudaStreamSynchronize(st));
   auto dp = [&](size_t off) { return (const void*)(D.base + off); };
@@ -184,6 +186,24 @@ int na_tables(NoAllocDev& D, int nterms, int orderff, int nquad, cudaStream_t st
   return 0;
 }
 
+/* every array argument must be device (or managed) memory of the current
+ * device: a host pointer handed to the kernels would fault the GPU */
+int na_check_device_ptr(const void* p, int dev, const char* name) {
+  cudaPointerAttributes a{};
+  cudaError_t e = cudaPointerGetAttributes(&a, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError(); /* clear the error the query left */
+    std::snprintf(g_na_msg, sizeof g_na_msg, "qol_rrq_noalloc: %s is not a CUDA pointer", name);
+    return QOL_ERR_ARG;
+  }
+  if (a.type == cudaMemoryTypeManaged) return 0;
+  if (a.type != cudaMemoryTypeDevice || a.device != dev) {
+    std::snprintf(g_na_msg, sizeof g_na_msg, "qol_rrq_noalloc: %s must be device memory of the current device", name);
+    return QOL_ERR_ARG;
+  }
+  return 0;
+}
+
 } // namespace
 
 extern "C" const char* qol_noalloc_last_error(void) { return g_na_msg; }
@@ -204,6 +224,14 @@ extern "C" int qol_rrq_noalloc(qol_int m, const double* tx, qol_int n, const dou
   int dev = 0;
   NA_CK(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) return na_fail(QOL_ERR_ARG, "qol_rrq_noalloc: device index out of range");
+  {
+    const void* ptrs[8] = {tx, sx, snx, sw, rts, rps, As, Ad};
+    const char* names[8] = {"tx", "sx", "snx", "sw", "rts", "rps", "As", "Ad"};
+    for (int i = 0; i < 8; ++i) {
+      int prc = na_check_device_ptr(ptrs[i], dev, names[i]);
+      if (prc) return prc;
+    }
+  }
   int rc = na_setup(dev, st);
   if (rc) return rc;
   NoAllocDev& D = g_na[dev];
