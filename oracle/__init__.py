@@ -120,22 +120,39 @@ def rrq(tx, sx, snx, sw, rts, rps, nterms, nquad, orderff, distff=1.4, exterior=
     return (As.reshape(n, m).T.copy(), Ad.reshape(n, m).T.copy(), Om.reshape(m, 4 * hd).T.copy(), Ia, lvl)
 
 
+def rrq_panel_systems(sx, snx, sw, nterms):
+    """The D system A (4hd x 4hd, real form of the quaternion system) and the
+    S system Msl^T (hd x hd) that the panel precompute factors
+    (src/lap3d_close_mod.f90:851-863), as row-major math matrices."""
+    hd = nterms * (nterms + 1) // 2
+    DT = np.zeros(16 * hd * hd); MT = np.zeros(hd * hd)
+    rc = lib().orc_rrq_panel_systems(C.c_int(nterms), _vp(_f64(sx)), _vp(_f64(snx)), _vp(_f64(sw)), _vp(DT), _vp(MT))
+    if rc != 0:
+        raise RuntimeError(f"orc_rrq_panel_systems failed ({rc})")
+    # DT holds A^T column-major, i.e. A row-major; MT holds Msl^T column-major
+    return DT.reshape(4 * hd, 4 * hd).copy(), MT.reshape(hd, hd).T.copy()
+
+
 def getnearquad(npan, nterms, nquad, sx, snx, sw, rts, rps, tcx, tcxrow, tcxi, orderff,
-                distff=1.4, iside=30, nthreads=0):
-    """qol_getnearquad_lap_rrq restated; tcxrow/tcxi 1-based like the reference."""
+                distff=1.4, iside=30, nthreads=0, pair_levels=False):
+    """qol_getnearquad_lap_rrq restated; tcxrow/tcxi 1-based like the reference.
+    With pair_levels, also returns each pair's resolving level (1-4 direct
+    levels, 5 RRQ) in CSR order."""
     hdim = nterms * (nterms + 1) // 2
     sx = _f64(sx); snx = _f64(snx); sw = _f64(sw); rts = _f64(rts); rps = _f64(rps)
     tcx = _f64(tcx); tcxrow = _i64(tcxrow); tcxi = _i64(tcxi)
     ntcx = tcxrow.size; nsrc = sw.size; nnz = ntcx * hdim
     si = np.zeros(nnz, np.int64); sj = np.zeros(nnz, np.int64)
     vs = np.zeros(nnz); vd = np.zeros(nnz); hist = np.zeros(6, np.int64)
+    lv = np.zeros(ntcx, np.int64) if pair_levels else None
     rc = lib().orc_getnearquad(i64(npan), C.c_int(nterms), i64(hdim), C.c_int(nquad), i64(nsrc),
                                _vp(sx), _vp(snx), _vp(sw), _vp(rts), _vp(rps), i64(ntcx), _vp(tcx),
                                _vp(tcxrow), _vp(tcxi), C.c_int(orderff), C.c_double(distff), i64(iside),
-                               i64(nnz), _vp(si), _vp(sj), _vp(vs), _vp(vd), C.c_int(nthreads), _vp(hist))
+                               i64(nnz), _vp(si), _vp(sj), _vp(vs), _vp(vd), C.c_int(nthreads), _vp(hist),
+                               _vp(lv))
     if rc != 0:
         raise RuntimeError(f"orc_getnearquad failed ({rc})")
-    return si, sj, vs, vd, hist
+    return (si, sj, vs, vd, hist, lv) if pair_levels else (si, sj, vs, vd, hist)
 
 
 def ballcsr(npan, hdim, sx, sw, nthreads=0):

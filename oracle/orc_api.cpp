@@ -39,6 +39,16 @@ int orc_debug_target(int nterms, int nquad, int orderff, const double* sx, const
   debug_target(cfg, sx, snx, sw, x, out);
   return 0;
 }
+/* the D and S systems of one panel's RRQ precompute (conditioning checks) */
+int orc_rrq_panel_systems(int nterms, const double* sx, const double* snx, const double* sw, double* DT, double* MT) {
+  RRQConfig cfg{nterms, nterms + 2, nterms + 2, 1.4, true, 0};
+  try {
+    panel_systems(cfg, sx, snx, sw, DT, MT);
+  } catch (const std::exception&) {
+    return 4;
+  }
+  return 0;
+}
 int orc_set_flags(int f) { orc::g_orc_flags = f; return 0; }
 
 int orc_vr_nodes_export(int deg, double* uv, double* w) {
@@ -142,7 +152,7 @@ int orc_getnearquad(long long npan, int nterms, long long hdim, int nquad, long 
                     const double* rps, long long ntcx, const double* tcx, const long long* tcxrow,
                     const long long* tcxi, int orderff, double distff, long long iside,
                     long long nnz, long long* sparsei, long long* sparsej, double* sparsevs,
-                    double* sparsevd, int nthreads, long long* level_hist) {
+                    double* sparsevd, int nthreads, long long* level_hist, long long* pair_level) {
   if (hdim != (long long)nterms * (nterms + 1) / 2 || npan * hdim != nsrc) return 1;
   if (tcxi[0] != 1 || tcxi[npan] != ntcx + 1) return 1;
   for (long long k = 0; k < npan; ++k) if (tcxi[k + 1] < tcxi[k]) return 1;
@@ -176,6 +186,7 @@ int orc_getnearquad(long long npan, int nterms, long long hdim, int nquad, long 
         An[i + m * c] = 0.0; Bn[i + m * c] = 0.0;
       }
       hist[std::min<long long>(lvl[i], 5)]++;
+      if (pair_level) pair_level[jlo + i] = lvl[i];
     }
     for (long long j = 0; j < hdim; ++j)
       for (long long i = 0; i < m; ++i) {

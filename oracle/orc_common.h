@@ -101,6 +101,8 @@ void rrq(const RRQConfig& cfg, i8 m, const double* tx, const double* sx,
 
 /* experiment switches, 0 in normal use (test hook) */
 extern int g_orc_flags;
+void panel_systems(const RRQConfig& cfg, const double* sx, const double* snx, const double* sw, double* DT,
+                   double* MT);
 void debug_target(const RRQConfig& cfg, const double* sx, const double* snx, const double* sw,
                   const double* x, double* out);
 

@@ -184,26 +184,41 @@ static const double RHO_REC = 3.0;   /* recurrence moments inside, 48-pt GL outs
 /* modified weights w1, w3 on the nquad Gauss nodes of one edge for target x */
 static void ssq_weights(int n, const double* tg, const double* wg, const EdgeRoot& R,
                         const double* gl48x, const double* gl48w, double* w1, double* w3) {
-  bool use = R.ok && bernstein_radius(R.t0) < RHO_SSQ && std::fabs(R.t0.imag()) > 0.0;
+  double a = R.t0.real(), b = std::fabs(R.t0.imag());
+  /* a real root on the edge itself (the target on the boundary curve) has no
+   * finite moments: plain Gauss there; a real root beyond an endpoint (the
+   * target on the curve's continuation, e.g. a node of a neighbouring panel
+   * near a shared vertex) keeps the singularity swap */
+  bool use = R.ok && bernstein_radius(R.t0) < RHO_SSQ && (b > 0.0 || std::fabs(a) > 1.0);
   if (g_orc_flags & 4) use = false;
   if (!use) {
     for (int i = 0; i < n; ++i) { w1[i] = wg[i]; w3[i] = wg[i]; }
     return;
   }
-  double a = R.t0.real(), b = std::fabs(R.t0.imag());
   double Q[64], P[64];
   if (bernstein_radius(R.t0) < RHO_REC) {
     double s1 = std::sqrt((1.0 - a) * (1.0 - a) + b * b);
     double sm = std::sqrt((1.0 + a) * (1.0 + a) + b * b);
     double t02 = a * a + b * b;
-    Q[0] = std::asinh((1.0 - a) / b) + std::asinh((1.0 + a) / b);
+    /* Q0 = int dt/s and P0 = int dt/s^3 over [-1,1], s = |t - t0|: for a root
+     * beyond an endpoint in the cancellation-free forms (valid down to b = 0),
+     * otherwise asinh((1-a)/b) + asinh((1+a)/b) and [(t-a)/(b^2 s)] */
+    if (a > 1.0) {
+      Q[0] = std::log((sm + 1.0 + a) / (s1 + a - 1.0));
+      P[0] = 1.0 / (s1 * (s1 + a - 1.0)) - 1.0 / (sm * (sm + a + 1.0));
+    } else if (a < -1.0) {
+      Q[0] = std::log((s1 + 1.0 - a) / (sm - 1.0 - a));
+      P[0] = 1.0 / (sm * (sm - a - 1.0)) - 1.0 / (s1 * (s1 - a + 1.0));
+    } else {
+      Q[0] = std::asinh((1.0 - a) / b) + std::asinh((1.0 + a) / b);
+      P[0] = ((1.0 - a) / s1 + (1.0 + a) / sm) / (b * b);
+    }
     for (int k = 1; k < n; ++k) {
       double bnd = s1 - ((k - 1) % 2 == 0 ? 1.0 : -1.0) * sm; /* [t^{k-1} s]_{-1}^{1} */
       double v = (2.0 * k - 1.0) * a * Q[k - 1] + bnd;
       if (k >= 2) v -= (k - 1.0) * t02 * Q[k - 2];
       Q[k] = v / k;
     }
-    P[0] = ((1.0 - a) / s1 + (1.0 + a) / sm) / (b * b);
     for (int k = 1; k < n; ++k) {
       double bnd = 1.0 / s1 - ((k - 1) % 2 == 0 ? 1.0 : -1.0) / sm; /* [t^{k-1}/s] */
       double v = a * P[k - 1] - bnd;
@@ -238,6 +253,8 @@ struct RRQPanel {
   std::vector<double> tq, wq, tgl, wgl, gl48x, gl48w, tsa, wsa;
   std::vector<double> scf; /* Koornwinder coefficients of the frame node positions, 3 x hdim */
   bool exterior;
+  bool keep_systems = false;      /* keep copies of the two systems before factoring (conditioning checks) */
+  std::vector<double> Dsys, Ssys; /* A^T (4hd x 4hd) and Msl^T (hd x hd), column-major */
 };
 
 static void circum_frame(const double* v1, const double* v2, const double* v3, double* R,
@@ -401,6 +418,7 @@ static void build_rrq_panel(const RRQConfig& cfg, const double* sx, const double
   Aset(1, 0, G1, +1); Aset(1, 2, G3, +1); Aset(1, 3, G2, -1);
   Aset(2, 0, G2, +1); Aset(2, 1, G3, -1); Aset(2, 3, G1, +1);
   Aset(3, 0, G3, +1); Aset(3, 1, G2, +1); Aset(3, 2, G1, -1);
+  if (P.keep_systems) P.Dsys = AT;
   std::vector<int> piv(N4);
   if (lu_factor(N4, AT.data(), piv.data())) throw std::runtime_error("singular RRQ D system");
   std::vector<double> Z((size_t)N4 * hd, 0.0);
@@ -413,6 +431,7 @@ static void build_rrq_panel(const RRQConfig& cfg, const double* sx, const double
   std::vector<double> MT((size_t)hd * hd);
   for (int k = 0; k < hd; ++k)
     for (int j = 0; j < hd; ++j) MT[k + (size_t)hd * j] = Msl[j + (size_t)hd * k];
+  if (P.keep_systems) P.Ssys = MT;
   std::vector<int> piv2(hd);
   if (lu_factor(hd, MT.data(), piv2.data())) throw std::runtime_error("singular RRQ S system");
   P.PS.assign((size_t)hd * hd, 0.0);
@@ -698,6 +717,18 @@ void rrq(const RRQConfig& cfg, i8 m, const double* tx, const double* sx, const d
   }
 }
 
+
+/* the panel's two linear systems, as factored by build_rrq_panel: the D
+ * system A^T (4hd x 4hd) and the S system Msl^T (hd x hd), column-major
+ * (lap3d_close_mod.f90:851-863).  Conditioning checks of the tests use it. */
+void panel_systems(const RRQConfig& cfg, const double* sx, const double* snx, const double* sw, double* DT,
+                   double* MT) {
+  RRQPanel P;
+  P.keep_systems = true;
+  build_rrq_panel(cfg, sx, snx, sw, nullptr, nullptr, P);
+  std::copy(P.Dsys.begin(), P.Dsys.end(), DT);
+  std::copy(P.Ssys.begin(), P.Ssys.end(), MT);
+}
 
 /* debug hook: per-edge roots and the solid angle on the graded mesh and on
  * a uniform 512-interval mesh, for one panel and one target */

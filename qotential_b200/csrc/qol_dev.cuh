@@ -186,25 +186,38 @@ __device__ inline void ssq_weights_dev(int n, const double* tg, const double* wg
                                        const double* gl48x, const double* gl48w, const double* tginv,
                                        const double* rk /* 1/k */, double* w1, double* w3) {
   double rho = ok ? bernstein_radius_dev(t0) : 1e300;
-  bool use = ok && rho < QOL_RHO_SSQ && fabs(t0.im) > 0.0;
+  double a = t0.re, b = fabs(t0.im);
+  /* a real root on the edge itself (target on the boundary curve): plain
+   * Gauss; a real root beyond an endpoint (target on the curve's
+   * continuation) keeps the singularity swap */
+  bool use = ok && rho < QOL_RHO_SSQ && (b > 0.0 || fabs(a) > 1.0);
   if (!use) {
     for (int i = 0; i < n; ++i) { w1[i] = wg[i]; w3[i] = wg[i]; }
     return;
   }
-  double a = t0.re, b = fabs(t0.im);
   double Q[QOL_MAXNQ], P[QOL_MAXNQ];
   if (rho < QOL_RHO_REC) {
     double s1 = sqrt((1.0 - a) * (1.0 - a) + b * b);
     double sm = sqrt((1.0 + a) * (1.0 + a) + b * b);
     double t02 = a * a + b * b;
-    Q[0] = asinh((1.0 - a) / b) + asinh((1.0 + a) / b);
+    /* int dt/s, int dt/s^3 over [-1,1]: cancellation-free forms for a root
+     * beyond an endpoint (valid down to b = 0), else the asinh forms */
+    if (a > 1.0) {
+      Q[0] = log((sm + 1.0 + a) / (s1 + a - 1.0));
+      P[0] = 1.0 / (s1 * (s1 + a - 1.0)) - 1.0 / (sm * (sm + a + 1.0));
+    } else if (a < -1.0) {
+      Q[0] = log((s1 + 1.0 - a) / (sm - 1.0 - a));
+      P[0] = 1.0 / (sm * (sm - a - 1.0)) - 1.0 / (s1 * (s1 - a + 1.0));
+    } else {
+      Q[0] = asinh((1.0 - a) / b) + asinh((1.0 + a) / b);
+      P[0] = ((1.0 - a) / s1 + (1.0 + a) / sm) / (b * b);
+    }
     for (int k = 1; k < n; ++k) {
       double bnd = s1 - ((k - 1) % 2 == 0 ? 1.0 : -1.0) * sm;
       double v = (2.0 * k - 1.0) * a * Q[k - 1] + bnd;
       if (k >= 2) v -= (k - 1.0) * t02 * Q[k - 2];
       Q[k] = v * rk[k];
     }
-    P[0] = ((1.0 - a) / s1 + (1.0 + a) / sm) / (b * b);
     for (int k = 1; k < n; ++k) {
       double bnd = 1.0 / s1 - ((k - 1) % 2 == 0 ? 1.0 : -1.0) / sm;
       double v = a * P[k - 1] - bnd;

@@ -5,8 +5,9 @@ web/stellarator/test/native-direct-parity.py:41-97).
 
 Writes tests/golden/grf_order{4,6}.npz with u, ub, ubn, the GRF scalar, a
 strided subset of sx/snx/sw (every 7th node) and the SHA-256 of the full
-f64 sx/snx/sw arrays.  Run in a container that has the reference checkout:
-    python tests/golden/make_golden.py /root/reference
+f64 sx/snx/sw arrays.  Run in a container that has the reference checkout,
+naming its root (the argument, or the QOL_REFERENCE_DIR environment variable):
+    python tests/golden/make_golden.py <reference checkout>
 """
 import hashlib
 import os
@@ -30,7 +31,9 @@ def load(path):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("QOL_REFERENCE_DIR")
+    if not ref:
+        sys.exit("usage: make_golden.py <reference checkout> (or set QOL_REFERENCE_DIR)")
     here = os.path.dirname(os.path.abspath(__file__))
     for order in (4, 6):
         f = load(os.path.join(ref, "web/stellarator/fixtures/native", f"order{order}-direct.bin"))

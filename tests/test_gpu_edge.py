@@ -6,7 +6,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-TOL_RRQ = 1e-8  # as the parity tests: rows relative to the largest magnitude
+TOL_LOW = 1e-12  # as the parity tests at nterms <= 6: whole matrix relative to its largest entry
 
 
 def _case(G, nterms=5):
@@ -32,7 +32,7 @@ def _compare(orc, P, hd, nterms, npan, tcxi, tcxrow, tcx, got):
     assert np.array_equal(got[0], oi) and np.array_equal(got[1], oj)
     for a, b in ((got[2], ovs), (got[3], ovd)):
         if b.size:
-            assert np.abs(a - b).max() <= TOL_RRQ * np.abs(b).max()
+            assert np.abs(a - b).max() <= TOL_LOW * np.abs(b).max()
     return hist
 
 

@@ -1,17 +1,20 @@
 """GPU parity: the CUDA path through the C ABI vs the oracle on the same
-inputs.  Tolerances: COO indices bit-exact; values relative to the largest
-magnitude of the compared block (rows are ill-conditioned moment solves, so
-rounding differences from a different summation order are amplified; the
-bounds below are the measured agreement with headroom)."""
+inputs.  Tolerances: COO indices bit-exact; level-resolved rows TOL_LEVEL
+relative to the panel's largest level-row entry; RRQ rows condition-scaled
+((C_KAPPA kappa u + FLOOR_RRQ) relative to the panel's largest RRQ entry,
+kappa the condition number of the panel's D system: conftest.row_errors); at
+nterms <= 6, where kappa is below 1e4, the whole matrix also to TOL_LOW
+relative to its largest entry (measured 5e-13 at nterms 4 and 5, 1.2e-12 at
+nterms 6)."""
 import numpy as np
 import pytest
 
-from conftest import grf_apply
+from conftest import C_KAPPA, FLOOR_RRQ, grf_apply, row_errors
 
 pytestmark = pytest.mark.gpu
 
 TOL_LEVEL = 1e-12     # level-resolved rows: direct sums + contraction
-TOL_RRQ = 1e-8        # RRQ rows: moment solves
+TOL_LOW = {4: 1e-12, 5: 1e-12, 6: 2e-12}  # whole matrix at nterms <= 6
 
 
 def _setup(G, surf, mp, np_, nterms, split=False, off=0, seed=1):
@@ -29,9 +32,12 @@ def _compare(qol, orc, P, hd, nterms, tcxi, tcxrow, tcx):
     nq = nterms + 2
     si, sj, vs, vd, ti = qol.qol_getnearquad_lap_rrq(npan, nterms, hd, nq, npan * hd, P["sx"], P["snx"], P["sw"],
                                                      P["rts"], P["rps"], tcxrow.size, tcx, tcxrow, tcxi, nq, 1.4, 30)
-    oi, oj, ovs, ovd, hist = orc.getnearquad(npan, nterms, nq, P["sx"], P["snx"], P["sw"], P["rts"], P["rps"], tcx,
-                                             tcxrow, tcxi, nq)
+    oi, oj, ovs, ovd, hist, lv = orc.getnearquad(npan, nterms, nq, P["sx"], P["snx"], P["sw"], P["rts"], P["rps"],
+                                                 tcx, tcxrow, tcxi, nq, pair_levels=True)
     assert np.array_equal(si, oi) and np.array_equal(sj, oj)
+    worst_level, worst_ratio = row_errors(orc, P, hd, nterms, tcxi, lv, ((vs, ovs), (vd, ovd)))
+    assert worst_level < TOL_LEVEL, worst_level
+    assert worst_ratio < 1.0, worst_ratio
     return (vs, vd, ovs, ovd, hist, ti)
 
 
@@ -43,7 +49,7 @@ def test_getnearquad_torus(qol, orc, nterms):
     assert hist[5] > 0 and hist[1] > 0
     for a, b in ((vs, ovs), (vd, ovd)):
         err = np.abs(a - b).max() / np.abs(b).max()
-        assert err < TOL_RRQ, err
+        assert err < TOL_LOW[nterms], err
 
 
 @pytest.mark.parametrize("nterms", [5, 8])
@@ -51,11 +57,11 @@ def test_getnearquad_stellarator_offsurface(qol, orc, nterms):
     from qotential_b200 import geometry as G
     P, hd, tcxi, tcxrow, tcx, _ = _setup(G, G.stellarator(), 4, 10, nterms, off=300)
     vs, vd, ovs, ovd, hist, ti = _compare(qol, orc, P, hd, nterms, tcxi, tcxrow, tcx)
-    # per-pair relative errors
-    npan = P["sw"].size // hd
-    for a, b in ((vs, ovs), (vd, ovd)):
-        err = np.abs(a - b).max() / np.abs(b).max()
-        assert err < TOL_RRQ, err
+    assert hist[5] > 0 and hist[1] > 0
+    if nterms <= 6:
+        for a, b in ((vs, ovs), (vd, ovd)):
+            err = np.abs(a - b).max() / np.abs(b).max()
+            assert err < TOL_LOW[nterms], err
 
 
 def test_rrq_single_panel(qol, orc):
@@ -77,12 +83,17 @@ def test_rrq_single_panel(qol, orc):
     As, Ad, Om, Ia, ti = qol.qol_rrq(tx, sx, snx, sw, rts, rps, nterms, nterms + 2, nterms + 2)
     Bs, Bd, Om2, Ia2, lv = orc.rrq(tx, sx, snx, sw, rts, rps, nterms, nterms + 2, nterms + 2)
     assert (lv == 5).sum() > 10
-    for a, b in ((As, Bs), (Ad, Bd)):
-        err = np.abs(a - b).max(1) / np.abs(b).max(1)
-        assert err.max() < TOL_RRQ, err
-    assert np.abs(Ia - Ia2).max() < 1e-11
     rr = lv == 5
-    assert np.abs(Om[:, rr] - Om2[:, rr]).max() / np.abs(Om2[:, rr]).max() < TOL_RRQ
+    kap = np.linalg.cond(orc.rrq_panel_systems(sx, snx, sw, nterms)[0])
+    for a, b in ((As, Bs), (Ad, Bd)):
+        err = np.abs(a[~rr] - b[~rr]).max() / np.abs(b[~rr]).max()
+        assert err < TOL_LEVEL, err
+        err = np.abs(a[rr] - b[rr]).max() / np.abs(b[rr]).max()
+        assert err < C_KAPPA * kap * 2.0 ** -53 + FLOOR_RRQ, (err, kap)
+    assert np.abs(Ia - Ia2).max() < 1e-11
+    # the moments (the D system's right-hand sides): translation vs segment rule,
+    # measured 1.7e-12 relative to the largest
+    assert np.abs(Om[:, rr] - Om2[:, rr]).max() / np.abs(Om2[:, rr]).max() < 1e-11
     assert ti[:8].sum() > 0
 
 

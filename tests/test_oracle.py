@@ -4,6 +4,8 @@ import os
 import numpy as np
 import pytest
 
+from conftest import fixture_case
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
@@ -76,30 +78,13 @@ def test_geometry_matches_fixture(order):
 
 
 def _fixture_run(orc, order):
-    from qotential_b200 import geometry as G
-    P = G.panels(G.BuiltinSurface(), 12, 36, order)
-    hd = order * (order + 1) // 2; nq = order + 2; npan = P["ntri"]
-    x = P["sx"]
-    ub = np.exp(0.5 * x[:, 0]) * np.cos(0.5 * x[:, 1])
-    gr = np.stack([0.5 * ub, -0.5 * np.exp(0.5 * x[:, 0]) * np.sin(0.5 * x[:, 1]), 0 * ub], 1)
-    ubn = (P["snx"] * gr).sum(1)
-    u = orc.direct_farfield(P["sx"], P["snx"], P["sw"], ub, ubn)
-    offs, idx = orc.ballcsr(npan, hd, P["sx"], P["sw"])
-    # chart boundary (ichart = 1) from the surface map at the edge Gauss nodes
-    tgl, _, _ = orc.gauss(nq)
-    uv = []
-    for k in range(3):
-        for i in range(nq):
-            tt = k * 2 * np.pi / 3 + 0.5 * (1 + tgl[i]) * (2 * np.pi / 3)
-            th1, th2 = 2 * np.pi / 3, 4 * np.pi / 3
-            if tt < th1: uv.append((0.0, 1 - tt / th1))
-            elif tt < th2: uv.append(((tt - th1) / th1, 0.0))
-            else: uv.append((1 - (tt - th2) / th1, (tt - th2) / th1))
-    uv += [(0, 0), (1, 0), (0, 1)]
-    xbuf = G.panel_uv2x(G.BuiltinSurface(), 12, 36, order, np.array(uv))
-    un, cv, hist = orc.grf_near(npan, order, nq, nq, P["sx"], P["snx"], P["sw"], P["rts"], P["rps"], ub, ubn,
-                                offs, idx, u, xbuf=xbuf)
-    return un, ubn, int(offs[-1]), hist
+    F = fixture_case(orc, order)
+    P = F["P"]
+    u = orc.direct_farfield(P["sx"], P["snx"], P["sw"], F["ub"], F["ubn"])
+    offs, idx = orc.ballcsr(F["npan"], F["hd"], P["sx"], P["sw"])
+    un, cv, hist = orc.grf_near(F["npan"], order, F["nq"], F["nq"], P["sx"], P["snx"], P["sw"], P["rts"], P["rps"],
+                                F["ub"], F["ubn"], offs, idx, u, xbuf=F["xbuf"])
+    return un, F["ubn"], int(offs[-1]), hist
 
 
 @pytest.mark.parametrize("order,pairs,fs_bound,mean_bound,grf_rel", [
@@ -174,3 +159,37 @@ def test_selector_oracle_features_shape_and_ranges():
     f = S.pair_features(P["sw"].size // hd, hd, P["sx"], P["snx"], P["sw"], tcx, tcxi)
     assert f.shape == (tcxrow.size, 8) and np.isfinite(f).all()
     assert (np.abs(f[:, 1:4]) <= 1.0 + 1e-12).all() and (f[:, 5] >= 0).all() and (f[:, 6] >= 0).all()
+
+
+@pytest.mark.parametrize("nterms,kappa_range", [(9, (1e6, 1e8)), (13, (1e10, 1e12))])
+def test_rrq_rows_move_by_kappa_u(orc, nterms, kappa_range):
+    """The RRQ weights solve the panel's D system (src/lap3d_close_mod.f90:851-863),
+    whose 2-norm condition number kappa grows about 25-fold per order (3e8 at
+    nterms 11, 5e10 at nterms 13).  A one-ulp change of the node coordinates
+    moves the oracle's own RRQ rows by O(kappa u), relative to the panel's
+    largest RRQ entry: the scale the GPU parity bound at the headline orders
+    uses (tests/test_gpu_headline_orders.py)."""
+    from qotential_b200 import geometry as G
+    U = 2.0 ** -53
+    P = G.panels(G.stellarator(), 4, 10, nterms, split=False)
+    hd = nterms * (nterms + 1) // 2; k = 29
+    sl = slice(k * hd, (k + 1) * hd)
+    sx, snx, sw, rts, rps = (P[a][sl] for a in ("sx", "snx", "sw", "rts", "rps"))
+    diam = np.sqrt(sw.sum())
+    rng = np.random.default_rng(k)
+    tx = [sx]
+    for d in (1e-6, 1e-3, 0.05, 0.3):
+        j = rng.integers(0, hd, 6)
+        tx.append(sx[j] + (d * diam * np.where(rng.random(6) < 0.5, -1, 1))[:, None] * snx[j])
+    tx = np.concatenate(tx)
+    A, M = orc.rrq_panel_systems(sx, snx, sw, nterms)
+    kap = np.linalg.cond(A)
+    assert kappa_range[0] < kap < kappa_range[1], kap
+    Bs, Bd, _, _, lv = orc.rrq(tx, sx, snx, sw, rts, rps, nterms, nterms + 2, nterms + 2)
+    rr = lv == 5
+    assert rr.sum() > 20
+    f = 1.0 + np.random.default_rng(100).integers(-1, 2, sx.shape) * 2.0 ** -52
+    Cs, Cd, _, _, lv2 = orc.rrq(tx, sx * f, snx, sw, rts, rps, nterms, nterms + 2, nterms + 2)
+    assert np.array_equal(lv, lv2)
+    r = max(np.abs(Cs - Bs)[rr].max() / np.abs(Bs[rr]).max(), np.abs(Cd - Bd)[rr].max() / np.abs(Bd[rr]).max())
+    assert 0.05 < r / (kap * U) < 8.0, r / (kap * U)
