@@ -34,6 +34,7 @@ SEED = 2026
 
 def workload(rank=0, world=1, panels=0, order=ORDER):
     from qotential_b200 import geometry as G
+    from qotential_b200 import sharding
     nterms = order + 1
     hd = nterms * (nterms + 1) // 2
     P = G.panels(G.stellarator(), MP, NP, nterms, split=False)
@@ -44,15 +45,15 @@ def workload(rank=0, world=1, panels=0, order=ORDER):
     if panels:  # a leading slice of the same workload (profiling captures)
         npan = min(npan, panels)
         tcxrow = tcxrow[:tcxi[npan] - 1]
-    a, b = (rank * npan) // world, ((rank + 1) * npan) // world
-    sl = slice(a * hd, b * hd)
-    lo, hi = tcxi[a] - 1, tcxi[b] - 1
-    W = dict(nterms=nterms, hd=hd, nquad=nterms + 2, npan=b - a, npan_total=npan,
-             sx=np.ascontiguousarray(P["sx"][sl]), snx=np.ascontiguousarray(P["snx"][sl]),
-             sw=np.ascontiguousarray(P["sw"][sl]), rts=np.ascontiguousarray(P["rts"][sl]),
-             rps=np.ascontiguousarray(P["rps"][sl]), tcx=np.ascontiguousarray(tcx[lo:hi]),
-             tcxrow=np.ascontiguousarray(tcxrow[lo:hi]), tcxi=np.ascontiguousarray(tcxi[a:b + 1] - lo),
-             pairs_total=int(tcxrow.size))
+    tcxi = tcxi[:npan + 1]
+    # this rank's cost-balanced panel range, rows renumbered relative to it
+    # (qotential_b200.sharding: the ranks' COO outputs, shifted back,
+    # concatenate to the single-GPU output)
+    S, (a, b), shift = sharding.shard_inputs(rank, world, hd, P["sx"][:npan * hd], P["snx"][:npan * hd],
+                                             P["sw"][:npan * hd], P["rts"][:npan * hd], P["rps"][:npan * hd],
+                                             tcx, tcxrow, tcxi)
+    W = dict(nterms=nterms, hd=hd, nquad=nterms + 2, npan=b - a, npan_total=npan, panel_range=(a, b),
+             row_shift=shift, pairs_total=int(tcxrow.size), **S)
     W["pairs"] = int(W["tcxrow"].size)
     return W
 

@@ -157,6 +157,19 @@ int qol_grf_near(qol_int npan, qol_int nterms, qol_int nquad, qol_int orderff, d
  * u_i = sum_j S_ij ubn_j - D_ij ub_j over all nodes, zero self term. */
 int qol_direct_farfield(qol_int nsrc, const double* sx, const double* snx, const double* sw, const double* ub,
                         const double* ubn, double* u);
+/* Panel and target ranges of the two GRF phases, for work split over GPUs
+ * (no counterpart in the reference, which runs the driver on one host):
+ * qol_grf_near_range adds into u the near corrections of panels [plo, phi)
+ * only (their ball lists, RRQ/level corrections and scatter; all nodes stay
+ * targets), so the ranges of a partition of [0, npan) sum to qol_grf_near's
+ * corrections; qol_direct_farfield_range writes u_i for the targets
+ * i in [tlo, thi) only.  xbuf, when given, holds every panel's chart. */
+int qol_grf_near_range(qol_int npan, qol_int nterms, qol_int nquad, qol_int orderff, double distff, qol_int iside,
+                       qol_int nsrc, const double* sx, const double* snx, const double* sw, const double* rts,
+                       const double* rps, const double* xbuf, const double* ub, const double* ubn, qol_int plo,
+                       qol_int phi, double* u, qol_int* nnear, qol_int* level_hist, double* timeinfo);
+int qol_direct_farfield_range(qol_int nsrc, const double* sx, const double* snx, const double* sw,
+                              const double* ub, const double* ubn, qol_int tlo, qol_int thi, double* u);
 
 /* Library status and diagnostics.  qol_kernel_times: when enabled, every
  * pipeline call records CUDA events on its stream around its phases and

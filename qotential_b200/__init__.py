@@ -15,7 +15,8 @@ import numpy as np
 __all__ = [
     "lib", "QolError", "qol_simplex_precomp", "qol_build_patch_levels", "qol_lap3dsdlpmat_levels",
     "qol_clear_patch_levels", "qol_clear_patch_levels_all", "qol_rrq", "qol_getnearquad_lap_rrq",
-    "qol_getnearquad_lap_rrq_dev", "qol_grf_near", "qol_direct_farfield", "qol_set_sum_precision",
+    "qol_getnearquad_lap_rrq_dev", "qol_grf_near", "qol_grf_near_range", "qol_direct_farfield",
+    "qol_direct_farfield_range", "qol_set_sum_precision",
     "SELECTOR_NW", "qol_selector_features", "qol_selector_grad", "qol_selector_train", "qol_selector_set",
     "qol_selector_stats", "qol_set_autotune", "qol_panel_shape",
 ]
@@ -228,6 +229,40 @@ def qol_grf_near(npan, nterms, nquad, sx, snx, sw, rts, rps, ub, ubn, u=None, or
                             _vp(_f(ubn, nsrc)), _vp(uu), _vp(nn), _vp(hist), _vp(ti))
     _check(rc)
     return uu, int(nn[0]), hist
+
+
+def qol_grf_near_range(npan, nterms, nquad, sx, snx, sw, rts, rps, ub, ubn, plo, phi, u=None, orderff=None,
+                       distff=1.4, iside=30, xbuf=None, timeinfo=None):
+    """qol_grf_near restricted to the panels [plo, phi): returns u plus their
+    near corrections (all nodes stay targets).  The ranges of a partition of
+    [0, npan) add up to qol_grf_near's corrections (multi-GPU split)."""
+    hd = nterms * (nterms + 1) // 2
+    nsrc = npan * hd
+    orderff = nquad if orderff is None else orderff
+    uu = np.zeros(nsrc) if u is None else _f(u, nsrc).copy()
+    nn = np.zeros(1, np.int64)
+    hist = np.zeros(6, np.int64)
+    ti = np.zeros(20) if timeinfo is None else _f(timeinfo, 20).copy()
+    xb = None if xbuf is None else np.ascontiguousarray(np.asarray(xbuf, np.float64).ravel())
+    rc = lib().qol_grf_near_range(i64(npan), i64(nterms), i64(nquad), i64(orderff), C.c_double(distff), i64(iside),
+                                  i64(nsrc), _vp(_f(sx, 3 * nsrc)), _vp(_f(snx, 3 * nsrc)), _vp(_f(sw, nsrc)),
+                                  _vp(_f(rts, 3 * nsrc)), _vp(_f(rps, 3 * nsrc)), _vp(xb), _vp(_f(ub, nsrc)),
+                                  _vp(_f(ubn, nsrc)), i64(plo), i64(phi), _vp(uu), _vp(nn), _vp(hist), _vp(ti))
+    _check(rc)
+    return uu
+
+
+def qol_direct_farfield_range(sx, snx, sw, ub, ubn, tlo, thi, u):
+    """Direct far field for the targets [tlo, thi) only, written into u
+    (float64, nsrc, contiguous) in place."""
+    sw = _f(sw)
+    nsrc = sw.size
+    if not (isinstance(u, np.ndarray) and u.dtype == np.float64 and u.flags.c_contiguous and u.size == nsrc):
+        raise QolError(8, "u must be a contiguous float64 array of nsrc entries")
+    rc = lib().qol_direct_farfield_range(i64(nsrc), _vp(_f(sx, 3 * nsrc)), _vp(_f(snx, 3 * nsrc)), _vp(sw),
+                                         _vp(_f(ub, nsrc)), _vp(_f(ubn, nsrc)), i64(tlo), i64(thi), _vp(u))
+    _check(rc)
+    return u
 
 
 def qol_direct_farfield(sx, snx, sw, ub, ubn):

@@ -1421,23 +1421,25 @@ int qol_last_host_times(double* ms7) {
 /* GRF near phase (stellarator_grf_core_mod.f90:652-899): ball lists of the
  * surface's own nodes, the RRQ corrections of every near pair, contracted with
  * the density (ubn, ub) and scattered into u in panel order. */
-int qol_grf_near(qol_int npan, qol_int nterms, qol_int nquad, qol_int orderff, double distff, qol_int iside,
-                 qol_int nsrc, const double* sx, const double* snx, const double* sw, const double* rts,
-                 const double* rps, const double* xbuf, const double* ub, const double* ubn, double* u,
-                 qol_int* nnear, qol_int* level_hist, double* timeinfo) {
+int qol_grf_near_range(qol_int npan, qol_int nterms, qol_int nquad, qol_int orderff, double distff, qol_int iside,
+                       qol_int nsrc, const double* sx, const double* snx, const double* sw, const double* rts,
+                       const double* rps, const double* xbuf, const double* ub, const double* ubn, qol_int plo,
+                       qol_int phi, double* u, qol_int* nnear, qol_int* level_hist, double* timeinfo) {
   std::lock_guard<std::recursive_mutex> g(g_mu);
   const qol_int hd = nterms * (nterms + 1) / 2;
   if (!sx || !snx || !sw || !rts || !rps || !ub || !ubn || !u) return fail(QOL_ERR_ARG, "null argument");
   if (npan < 0 || nsrc != npan * hd) return fail(QOL_ERR_LAYOUT, "the panel order, npan and nsrc are inconsistent");
+  if (plo < 0 || phi < plo || phi > npan) return fail(QOL_ERR_ARG, "panel range outside [0, npan]");
   int rc = ensure_device();
   if (rc) return rc;
   if (nnear) *nnear = 0;
   if (level_hist) for (int i = 0; i < 6; ++i) level_hist[i] = 0;
-  if (npan == 0) return 0;
+  const qol_int nloc = phi - plo; /* this call's panels [plo, phi): ball lists, corrections, scatter */
+  if (nloc == 0) return 0;
   cudaStream_t st = g_stream;
   const int nbd = 3 * (int)nquad;
   size_t need = sizeof(double) * (size_t)(16 * nsrc + 4 * npan + (xbuf ? 3 * (nbd + 3) * npan : 0)) +
-                sizeof(long long) * (size_t)(3 * npan + 3) + 16 * 256;
+                sizeof(long long) * (size_t)(3 * nloc + 3) + 16 * 256;
   if ((rc = g_arena_io.reserve(need))) return rc;
   g_arena_io.reset();
   double* dsx = g_arena_io.take<double>(3 * nsrc);
@@ -1449,10 +1451,10 @@ int qol_grf_near(qol_int npan, qol_int nterms, qol_int nquad, qol_int orderff, d
   double* dubn = g_arena_io.take<double>(nsrc);
   double* du = g_arena_io.take<double>(nsrc);
   double* dball = g_arena_io.take<double>(4 * npan);
-  double* dchart = xbuf ? g_arena_io.take<double>((size_t)3 * (nbd + 3) * npan) : nullptr;
-  long long* dcnt = g_arena_io.take<long long>(npan);
-  long long* doff = g_arena_io.take<long long>(npan + 1); /* 0-based offsets */
-  long long* dxi = g_arena_io.take<long long>(npan + 1);  /* 1-based, the pipeline's tcxi */
+  double* dchart = xbuf ? g_arena_io.take<double>((size_t)3 * (nbd + 3) * nloc) : nullptr;
+  long long* dcnt = g_arena_io.take<long long>(nloc);
+  long long* doff = g_arena_io.take<long long>(nloc + 1); /* 0-based offsets */
+  long long* dxi = g_arena_io.take<long long>(nloc + 1);  /* 1-based, the pipeline's tcxi */
   CK(cudaMemcpyAsync(dsx, sx, sizeof(double) * 3 * nsrc, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(dsnx, snx, sizeof(double) * 3 * nsrc, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(dsw, sw, sizeof(double) * nsrc, cudaMemcpyHostToDevice, st));
@@ -1461,39 +1463,46 @@ int qol_grf_near(qol_int npan, qol_int nterms, qol_int nquad, qol_int orderff, d
   CK(cudaMemcpyAsync(dub, ub, sizeof(double) * nsrc, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(dubn, ubn, sizeof(double) * nsrc, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(du, u, sizeof(double) * nsrc, cudaMemcpyHostToDevice, st));
-  if (xbuf) CK(cudaMemcpyAsync(dchart, xbuf, sizeof(double) * 3 * (nbd + 3) * npan, cudaMemcpyHostToDevice, st));
-  CK(qol_launch_grf_balls((int)npan, (int)hd, nsrc, dsx, dsw, dball, dcnt, st));
-  std::vector<long long> cnt(npan), off(npan + 1), xi(npan + 1);
-  CK(cudaMemcpyAsync(cnt.data(), dcnt, sizeof(long long) * npan, cudaMemcpyDeviceToHost, st));
+  if (xbuf)
+    CK(cudaMemcpyAsync(dchart, xbuf + (size_t)3 * (nbd + 3) * plo, sizeof(double) * 3 * (nbd + 3) * nloc,
+                       cudaMemcpyHostToDevice, st));
+  CK(qol_launch_grf_balls((int)npan, (int)hd, nsrc, dsx, dsw, dball, dcnt, (int)plo, (int)phi, st));
+  std::vector<long long> cnt(nloc), off(nloc + 1), xi(nloc + 1);
+  CK(cudaMemcpyAsync(cnt.data(), dcnt, sizeof(long long) * nloc, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   off[0] = 0;
-  for (qol_int k = 0; k < npan; ++k) off[k + 1] = off[k] + cnt[k];
-  for (qol_int k = 0; k <= npan; ++k) xi[k] = off[k] + 1;
-  const long long nn = off[npan];
+  for (qol_int k = 0; k < nloc; ++k) off[k + 1] = off[k] + cnt[k];
+  for (qol_int k = 0; k <= nloc; ++k) xi[k] = off[k] + 1;
+  const long long nn = off[nloc];
   if (nnear) *nnear = nn;
-  CK(cudaMemcpyAsync(doff, off.data(), sizeof(long long) * (npan + 1), cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(dxi, xi.data(), sizeof(long long) * (npan + 1), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(doff, off.data(), sizeof(long long) * (nloc + 1), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dxi, xi.data(), sizeof(long long) * (nloc + 1), cudaMemcpyHostToDevice, st));
   if (nn > 0) {
-    need = sizeof(double) * (size_t)nn * (3 + 1 + 2 * hd) + sizeof(long long) * (size_t)nn + 8 * 256;
+    need = sizeof(double) * (size_t)nn * (3 + 1 + 2 * hd) + sizeof(long long) * (size_t)nn * 2 + 8 * 256;
     if ((rc = g_arena_grf.reserve(need))) return rc;
     g_arena_grf.reset();
     long long* didx = g_arena_grf.take<long long>(nn);
+    long long* dloc = plo ? g_arena_grf.take<long long>(nn) : didx; /* rows in the range's own numbering */
     double* dtcx = g_arena_grf.take<double>(3 * nn);
     double* dval = g_arena_grf.take<double>(nn);
     double* dvs = g_arena_grf.take<double>((size_t)nn * hd);
     double* dvd = g_arena_grf.take<double>((size_t)nn * hd);
-    CK(qol_launch_grf_csr((int)npan, nsrc, dsx, dball, doff, didx, dtcx, st));
+    const double* ball = dball + 4 * (size_t)plo;
+    CK(qol_launch_grf_csr((int)nloc, nsrc, dsx, ball, doff, didx, dtcx, plo ? dloc : nullptr,
+                          (long long)plo * hd, st));
     Job J{};
-    J.npan = (int)npan; J.nterms = (int)nterms; J.nquad = (int)nquad; J.orderff = (int)orderff;
+    J.npan = (int)nloc; J.nterms = (int)nterms; J.nquad = (int)nquad; J.orderff = (int)orderff;
     J.exterior = (iside % 10) == 0; J.subtract_naive = 1; J.distff = distff; J.ntcx = nn;
-    J.P = PanelIn{dsx, dsnx, dsw, drts, drps};
-    J.Q = PairIn{dtcx, didx, dxi};
+    const size_t o = (size_t)plo * hd; /* the range's panels; the self-pair mask compares their rows */
+    J.P = PanelIn{dsx + 3 * o, dsnx + 3 * o, dsw + o, drts + 3 * o, drps + 3 * o};
+    J.Q = PairIn{dtcx, dloc, dxi};
     J.vs = dvs; J.vd = dvd; J.si = nullptr; J.sj = nullptr;
     J.chart = dchart;
     long long hist[6] = {0, 0, 0, 0, 0, 0};
     if ((rc = run_pipeline(J, st, timeinfo, hist, nullptr, nullptr))) return rc;
     if (level_hist) for (int i = 0; i < 6; ++i) level_hist[i] = hist[i];
-    CK(qol_launch_grf_apply((int)npan, (int)hd, nsrc, dsx, dball, doff, didx, dvs, dvd, dub, dubn, dval, du, st));
+    CK(qol_launch_grf_apply((int)nloc, (int)hd, nsrc, dsx, ball, doff, didx, dvs, dvd, dub + o, dubn + o, dval, du,
+                            st));
   }
   CK(cudaMemcpyAsync(u, du, sizeof(double) * nsrc, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
@@ -1502,14 +1511,23 @@ int qol_grf_near(qol_int npan, qol_int nterms, qol_int nquad, qol_int orderff, d
 
 /* the blocked Direct far field u_i = sum_j S_ij ubn_j - D_ij ub_j with zero
  * self term (stellarator_grf_core_mod.f90:566-606) */
-int qol_direct_farfield(qol_int nsrc, const double* sx, const double* snx, const double* sw, const double* ub,
-                        const double* ubn, double* u) {
+int qol_grf_near(qol_int npan, qol_int nterms, qol_int nquad, qol_int orderff, double distff, qol_int iside,
+                 qol_int nsrc, const double* sx, const double* snx, const double* sw, const double* rts,
+                 const double* rps, const double* xbuf, const double* ub, const double* ubn, double* u,
+                 qol_int* nnear, qol_int* level_hist, double* timeinfo) {
+  return qol_grf_near_range(npan, nterms, nquad, orderff, distff, iside, nsrc, sx, snx, sw, rts, rps, xbuf, ub, ubn,
+                            0, npan, u, nnear, level_hist, timeinfo);
+}
+
+int qol_direct_farfield_range(qol_int nsrc, const double* sx, const double* snx, const double* sw,
+                              const double* ub, const double* ubn, qol_int tlo, qol_int thi, double* u) {
   std::lock_guard<std::recursive_mutex> g(g_mu);
   if (!sx || !snx || !sw || !ub || !ubn || !u) return fail(QOL_ERR_ARG, "null argument");
   if (nsrc < 0) return fail(QOL_ERR_ARG, "negative size");
+  if (tlo < 0 || thi < tlo || thi > nsrc) return fail(QOL_ERR_ARG, "target range outside [0, nsrc]");
   int rc = ensure_device();
   if (rc) return rc;
-  if (nsrc == 0) return 0;
+  if (thi == tlo) return 0;
   cudaStream_t st = g_stream;
   if ((rc = g_arena_io.reserve(sizeof(double) * (size_t)10 * nsrc + 8 * 256))) return rc;
   g_arena_io.reset();
@@ -1524,10 +1542,15 @@ int qol_direct_farfield(qol_int nsrc, const double* sx, const double* snx, const
   CK(cudaMemcpyAsync(dsw, sw, sizeof(double) * nsrc, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(dub, ub, sizeof(double) * nsrc, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(dubn, ubn, sizeof(double) * nsrc, cudaMemcpyHostToDevice, st));
-  CK(qol_launch_direct_far(nsrc, dsx, dsnx, dsw, dub, dubn, du, st));
-  CK(cudaMemcpyAsync(u, du, sizeof(double) * nsrc, cudaMemcpyDeviceToHost, st));
+  CK(qol_launch_direct_far(nsrc, dsx, dsnx, dsw, dub, dubn, du, tlo, thi, st));
+  CK(cudaMemcpyAsync(u + tlo, du + tlo, sizeof(double) * (thi - tlo), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   return 0;
+}
+
+int qol_direct_farfield(qol_int nsrc, const double* sx, const double* snx, const double* sw, const double* ub,
+                        const double* ubn, double* u) {
+  return qol_direct_farfield_range(nsrc, sx, snx, sw, ub, ubn, 0, nsrc, u);
 }
 
 int qol_rrq(qol_int m, const double* tx, qol_int n, const double* sx, const double* snx, const double* sw,

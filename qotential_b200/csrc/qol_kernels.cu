@@ -734,61 +734,17 @@ __host__ __device__ constexpr size_t panel_smem_doubles(int hd, int nbd, int CS)
          5 * (size_t)panel_ncol(hd, CS) + 8 + (8 * (size_t)hd + 1) / 2 + 2;
 }
 
-/* per-panel RRQ precompute, one thread-block cluster of CS CTAs per panel.
- * The quaternion matrix V (hd x hd, V[j][k] = (0, grad h_k(y_j))) and the real
- * Msl^T (MS[k][j] = n_j . grad h_k(y_j)) are split by columns over the CTAs;
- * each thread keeps one column's entries of up to MAXR rows in registers.
- * Both are inverted in place by Gauss-Jordan with implicit row pivoting
- * (quaternion pivot by norm; no row moves): step k reads column k from the
- * staging buffer its owner pushed into every CTA through distributed shared
- * memory, picks the largest unused row p, scales row p and eliminates every
- * other row; the owner of column k+1 pushes it as it is updated; one cluster
- * barrier ends the step.  With pi the pivot sequence the inverse is
- * X^-1[k][c] = X[pi(k)][pi^-1(c)]. */
-template <int CS, int NT, int MAXR>
-__global__ void __launch_bounds__(NT, 1) k_rrq_panel(OrderTab T, PanelIn P, PairWS G, RRQWS R,
-                                                                const double* chart /* nullable */) {
-  cg::cluster_group cl = cg::this_cluster();
-  const int rank = (int)cl.block_rank();
-  const int pan = R.plo + (int)(blockIdx.x / CS); /* panels R.plo .. R.plo + gridDim.x / CS - 1 */
-  if (G.cnt[(size_t)pan * 8 + T.nlevel + 1] == 0 && !R.all_panels) return; /* whole cluster */
-  const int hd = T.hd, nq = T.nquad, nbd = 3 * nq, L = T.nterms;
-  const int ncol = panel_ncol(hd, CS), c0 = min(hd, rank * ncol), c1 = min(hd, c0 + ncol), nc = c1 - c0;
-  const int RG = NT / ncol, tc = threadIdx.x % ncol, trg = threadIdx.x / ncol;
-  const bool tact = trg < RG && tc < nc;
-  const int gc = c0 + tc; /* this thread's column */
-  extern __shared__ __align__(16) double psm[];
-  double* Vs = psm;                        /* hd x ncol quaternions (setup) */
-  double* Ms = Vs + (size_t)4 * hd * ncol; /* hd x ncol (setup) */
-  const int SB = (5 * hd + 1) & ~1;       /* staging buffer stride (even: double2 copies) */
-  double* stg = Ms + (((size_t)hd * ncol + 1) & ~(size_t)1); /* 2 buffers x (4 hd quaternion column + hd real column) */
-  double* s_sx = stg + 2 * SB;             /* 3 hd */
-  double* s_raw = s_sx + 3 * hd;           /* 3 (nbd + 3) */
-  double* s_fr = s_raw + 3 * (nbd + 3);    /* 16 */
-  double* rowq = s_fr + 16;                /* 4 ncol: scaled pivot row of V */
-  double* rowr = rowq + 4 * ncol;          /* ncol: scaled pivot row of MS */
-  int* s_piv = (int*)(rowr + ncol + 8);   /* 2 hd: pivot rows of V, of MS (after the 8 pivot values) */
-  int* s_pos = s_piv + 2 * hd;             /* 2 hd: inverse permutations */
-  int* s_used = s_pos + 2 * hd;            /* 2 hd */
-  int* s_pad = s_used + 2 * hd;            /* 2 hd (alignment slack) */
-  (void)s_pad;
-  double* stgr[CS];
-#pragma unroll
-  for (int r = 0; r < CS; ++r) stgr[r] = cl.map_shared_rank(stg, r);
-  auto pushq = [&](int buf, int row, const double* q) {
-#pragma unroll
-    for (int r = 0; r < CS; ++r) {
-      double* d = stgr[r] + buf * SB + 4 * row;
-      d[0] = q[0]; d[1] = q[1]; d[2] = q[2]; d[3] = q[3];
-    }
-  };
-  auto pushr = [&](int buf, int row, double v) {
-#pragma unroll
-    for (int r = 0; r < CS; ++r) stgr[r][buf * SB + 4 * hd + row] = v;
-  };
-  double* H = R.hmat + (size_t)pan * hd * hd; /* H[j*hd+k] = h_k(y_j) */
+/* per-panel RRQ frame and boundary (shared by the panel kernels; every thread
+ * of the CTA calls it): the panel's nodes into s_sx, the boundary and vertices
+ * from the interpolant (or the caller's chart) into s_raw, the frame
+ * (R, c, alpha: lap3d_close_mod.f90:503-509, alpha = 1.25/sqrt(2 sum sw)
+ * :709) into s_fr; rank 0 of the cluster writes the per-panel outputs (frame,
+ * boundary in the frame, its t-derivative and Legendre coefficients, the
+ * Koornwinder coefficients of the frame node positions). */
+__device__ void panel_frame_setup(const OrderTab& T, const PanelIn& P, const RRQWS& R, const double* chart, int pan,
+                                  int rank, double* s_sx, double* s_raw, double* s_fr) {
+  const int hd = T.hd, nq = T.nquad, nbd = 3 * nq;
   for (int e = threadIdx.x; e < 3 * hd; e += blockDim.x) s_sx[e] = P.sx[(size_t)pan * hd * 3 + e];
-  for (int e = threadIdx.x; e < 2 * hd; e += blockDim.x) s_used[e] = 0;
   __syncthreads();
   /* boundary + vertices from the interpolant, or the caller's chart */
   for (int i = threadIdx.x; i < nbd + 3; i += blockDim.x) {
@@ -886,6 +842,137 @@ __global__ void __launch_bounds__(NT, 1) k_rrq_panel(OrderTab T, PanelIn P, Pair
       for (int d = 0; d < 3; ++d) R.sxf[(size_t)pan * 3 * hd + 3 * j + d] = y[d];
     }
   }
+}
+
+/* B = PS H^T for rows c0 .. c0 + nc - 1 of one panel: B[i][j] = sum_k PS[i][k]
+ * h_k(y_j) on the FP64 tensor path (m8n8k4): PS rows (A) and H rows (B^T)
+ * staged in K tiles in the CTA's shared memory (room doubles, all dead by
+ * now), zero padded; warp w takes the column blocks w, w + NW, .. with every
+ * row block.  PS (global) must be complete and visible: the caller fences and
+ * synchronises the cluster first. */
+__device__ void panel_b_epilogue(const RRQWS& R, int hd, int pan, int c0, int nc, int room, double* psm) {
+  const double* PS = R.smat + (size_t)pan * hd * hd;
+  const double* H = R.hmat + (size_t)pan * hd * hd;
+  {
+    double* B = R.B + (size_t)pan * hd * hd;
+    const int MBn = (nc + 7) / 8, NBn = (hd + 7) / 8, rows = 8 * (MBn + NBn), KP = (hd + 3) & ~3;
+    auto skf = [](int kt) { return (kt % 16 == 4 || kt % 16 == 12) ? kt : kt + 4; }; /* conflict-free strides */
+    int KT = KP;
+    while (KT > 4 && rows * skf(KT) > room) KT -= 4;
+    const int SK = skf(KT);
+    double* sP = psm;                         /* 8 MBn x SK */
+    double* sH = psm + (size_t)8 * MBn * SK;  /* 8 NBn x SK */
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int NT = blockDim.x, NW = NT / 32;
+    constexpr int MBX = 9, NBX = 2; /* row blocks <= 9, column blocks a warp <= 2 */
+    double acc[NBX][MBX][2];
+#pragma unroll
+    for (int u = 0; u < NBX; ++u)
+#pragma unroll
+      for (int v = 0; v < MBX; ++v) { acc[u][v][0] = 0.0; acc[u][v][1] = 0.0; }
+    for (int k0 = 0; k0 < KP; k0 += KT) {
+      __syncthreads();
+      for (int e = threadIdx.x; e < 8 * MBn * KT; e += NT) {
+        const int i = e / KT, kk = e % KT, k = k0 + kk;
+        sP[i * SK + kk] = (i < nc && k < hd) ? PS[(size_t)(c0 + i) * hd + k] : 0.0;
+      }
+      for (int e = threadIdx.x; e < 8 * NBn * KT; e += NT) {
+        const int j = e / KT, kk = e % KT, k = k0 + kk;
+        sH[j * SK + kk] = (j < hd && k < hd) ? H[(size_t)j * hd + k] : 0.0;
+      }
+      __syncthreads();
+      const int kst = min(KT, KP - k0) / 4;
+      for (int ks = 0; ks < kst; ++ks) {
+        const int kc = 4 * ks + (lane & 3);
+#pragma unroll
+        for (int u = 0; u < NBX; ++u) {
+          const int nb = wid + NW * u;
+          if (nb >= NBn) continue;
+          const double bv = sH[(8 * nb + (lane >> 2)) * SK + kc];
+#pragma unroll
+          for (int v = 0; v < MBX; ++v)
+            if (v < MBn) dmma(acc[u][v][0], acc[u][v][1], sP[(8 * v + (lane >> 2)) * SK + kc], bv);
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < NBX; ++u) {
+      const int nb = wid + NW * u;
+      if (nb >= NBn) continue;
+#pragma unroll
+      for (int v = 0; v < MBX; ++v) {
+        const int i = 8 * v + (lane >> 2);
+        if (v >= MBn || i >= nc) continue;
+#pragma unroll
+        for (int h2 = 0; h2 < 2; ++h2) {
+          const int j = 8 * nb + 2 * (lane & 3) + h2;
+          if (j < hd) B[(size_t)(c0 + i) * hd + j] = acc[u][v][h2];
+        }
+      }
+    }
+  }
+}
+
+/* per-panel RRQ precompute, one thread-block cluster of CS CTAs per panel.
+ * The quaternion matrix V (hd x hd, V[j][k] = (0, grad h_k(y_j))) and the real
+ * Msl^T (MS[k][j] = n_j . grad h_k(y_j)) are split by columns over the CTAs;
+ * each thread keeps one column's entries of up to MAXR rows in registers.
+ * Both are inverted in place by Gauss-Jordan with implicit row pivoting
+ * (quaternion pivot by norm; no row moves): step k reads column k from the
+ * staging buffer its owner pushed into every CTA through distributed shared
+ * memory, picks the largest unused row p, scales row p and eliminates every
+ * other row; the owner of column k+1 pushes it as it is updated; one cluster
+ * barrier ends the step.  With pi the pivot sequence the inverse is
+ * X^-1[k][c] = X[pi(k)][pi^-1(c)]. */
+template <int CS, int NT, int MAXR>
+__global__ void __launch_bounds__(NT, 1) k_rrq_panel(OrderTab T, PanelIn P, PairWS G, RRQWS R,
+                                                                const double* chart /* nullable */) {
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+  const int pan = R.plo + (int)(blockIdx.x / CS); /* panels R.plo .. R.plo + gridDim.x / CS - 1 */
+  if (G.cnt[(size_t)pan * 8 + T.nlevel + 1] == 0 && !R.all_panels) return; /* whole cluster */
+  const int hd = T.hd, nq = T.nquad, nbd = 3 * nq, L = T.nterms;
+  const int ncol = panel_ncol(hd, CS), c0 = min(hd, rank * ncol), c1 = min(hd, c0 + ncol), nc = c1 - c0;
+  const int RG = NT / ncol, tc = threadIdx.x % ncol, trg = threadIdx.x / ncol;
+  const bool tact = trg < RG && tc < nc;
+  const int gc = c0 + tc; /* this thread's column */
+  extern __shared__ __align__(16) double psm[];
+  double* Vs = psm;                        /* hd x ncol quaternions (setup) */
+  double* Ms = Vs + (size_t)4 * hd * ncol; /* hd x ncol (setup) */
+  const int SB = (5 * hd + 1) & ~1;       /* staging buffer stride (even: double2 copies) */
+  double* stg = Ms + (((size_t)hd * ncol + 1) & ~(size_t)1); /* 2 buffers x (4 hd quaternion column + hd real column) */
+  double* s_sx = stg + 2 * SB;             /* 3 hd */
+  double* s_raw = s_sx + 3 * hd;           /* 3 (nbd + 3) */
+  double* s_fr = s_raw + 3 * (nbd + 3);    /* 16 */
+  double* rowq = s_fr + 16;                /* 4 ncol: scaled pivot row of V */
+  double* rowr = rowq + 4 * ncol;          /* ncol: scaled pivot row of MS */
+  int* s_piv = (int*)(rowr + ncol + 8);   /* 2 hd: pivot rows of V, of MS (after the 8 pivot values) */
+  int* s_pos = s_piv + 2 * hd;             /* 2 hd: inverse permutations */
+  int* s_used = s_pos + 2 * hd;            /* 2 hd */
+  int* s_pad = s_used + 2 * hd;            /* 2 hd (alignment slack) */
+  (void)s_pad;
+  double* stgr[CS];
+#pragma unroll
+  for (int r = 0; r < CS; ++r) stgr[r] = cl.map_shared_rank(stg, r);
+  auto pushq = [&](int buf, int row, const double* q) {
+#pragma unroll
+    for (int r = 0; r < CS; ++r) {
+      double* d = stgr[r] + buf * SB + 4 * row;
+      d[0] = q[0]; d[1] = q[1]; d[2] = q[2]; d[3] = q[3];
+    }
+  };
+  auto pushr = [&](int buf, int row, double v) {
+#pragma unroll
+    for (int r = 0; r < CS; ++r) stgr[r][buf * SB + 4 * hd + row] = v;
+  };
+  double* H = R.hmat + (size_t)pan * hd * hd; /* H[j*hd+k] = h_k(y_j) */
+  for (int e = threadIdx.x; e < 2 * hd; e += blockDim.x) s_used[e] = 0;
+  panel_frame_setup(T, P, R, chart, pan, rank, s_sx, s_raw, s_fr);
+  const double alpha = s_fr[12];
+  auto tofr = [&](const double* x, double* y) {
+    double d0 = x[0] - s_fr[9], d1 = x[1] - s_fr[10], d2 = x[2] - s_fr[11];
+    for (int i = 0; i < 3; ++i) y[i] = alpha * (s_fr[i] * d0 + s_fr[i + 3] * d1 + s_fr[i + 6] * d2);
+  };
   /* basis at the nodes: this CTA's columns of V (harmonics c0..c1) and of
    * Msl^T (nodes c0..c1), and H rows of its nodes */
   for (int e = threadIdx.x; e < hd * L; e += blockDim.x) { /* (node j, order m) items: distinct entries */
@@ -1068,68 +1155,453 @@ __global__ void __launch_bounds__(NT, 1) k_rrq_panel(OrderTab T, PanelIn P, Pair
   }
   __threadfence();
   cl.sync();
-  /* B = PS H^T, rows c0..c1: B[i][j] = sum_k PS[i][k] h_k(y_j) on the FP64
-   * tensor path (m8n8k4): PS rows (A) and H rows (B^T) staged in K tiles in the
-   * CTA's shared memory (free now), zero padded; warp w takes the column
-   * blocks w, w + NT/32, .. with every row block */
-  {
-    double* B = R.B + (size_t)pan * hd * hd;
-    const int room = (int)panel_smem_doubles(hd, nbd, CS); /* the whole allocation: everything in it is dead now */
-    const int MBn = (nc + 7) / 8, NBn = (hd + 7) / 8, rows = 8 * (MBn + NBn), KP = (hd + 3) & ~3;
-    auto skf = [](int kt) { return (kt % 16 == 4 || kt % 16 == 12) ? kt : kt + 4; }; /* conflict-free strides */
-    int KT = KP;
-    while (KT > 4 && rows * skf(KT) > room) KT -= 4;
-    const int SK = skf(KT);
-    double* sP = psm;                         /* 8 MBn x SK */
-    double* sH = psm + (size_t)8 * MBn * SK;  /* 8 NBn x SK */
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    constexpr int NW = NT / 32, MBX = 8, NBX = 2; /* row blocks <= 7, column blocks a warp <= 2 (nterms <= 17) */
-    double acc[NBX][MBX][2];
+  panel_b_epilogue(R, hd, pan, c0, nc, (int)panel_smem_doubles(hd, nbd, CS), psm);
+}
+
+
+/* ---------------------------------------------------------------------
+ * Blocked Gauss-Jordan panel precompute (orders whose matrix columns fit a
+ * cluster's shared memory: hdim <= 136 with up to 4 CTAs).
+ *
+ * The same inverses as k_rrq_panel, computed as a blocked Gauss-Jordan
+ * elimination with the same pivot rule (largest quaternion norm / largest
+ * magnitude among the unused rows of the pivot column, no row moves): columns
+ * are taken PB_NB = 8 at a time.  The CTA owning a block eliminates within the
+ * block's 8 columns alone (the panel phase: 8 steps of the unblocked method on
+ * hd x 8 entries, CTA barriers only) and publishes the block M and its pivot
+ * rows P to every CTA of the cluster through distributed shared memory; every
+ * CTA then applies the block's 8 steps to all its other columns at once,
+ *     X[:, J] <- X[:, J] (rows P set to 0) + M X[P, J],
+ * on the FP64 tensor path (mma m8n8k4): for the quaternion system the real
+ * GEMM (4 hd x 32) (32 x ncol) with A the left-multiplication matrices of M's
+ * entries, built in the fragment loads (entry c^d of M[i][b], sign from a
+ * table), B the pivot rows' components; for the real system the GEMM
+ * (hd x 8) (8 x ncol).  Two cluster barriers a block (12 blocks at hdim 91)
+ * instead of one a column.  The in-place result equals the unblocked
+ * method's, so the write-out X^-1[k][c] = X[pi(k)][pi^-1(c)] and the B
+ * epilogue are k_rrq_panel's.
+ * Shared memory per CTA (doubles): Xq 4 planes of hq x ncol (V's columns of
+ * this CTA, component-major), Xr hr x ncol (MS's columns), Mq hq x 8 x 4 and
+ * Mr hr x 8 (the published block), the pivot column, the scaled pivot rows,
+ * pivot bookkeeping.  hq = hd rounded up to 2 (8 real rows), hr to 8, ncol
+ * = ceil(hd / CS) rounded up to 8.
+ * --------------------------------------------------------------------- */
+constexpr int PB_NB = 8;
+constexpr int PB_MAXT = 576; /* threads a CTA: two warps per 8-column tile, at most 9 tiles */
+__host__ __device__ constexpr int pblk_ncol(int hd, int CS) { return (((hd + CS - 1) / CS) + 7) & ~7; }
+__host__ __device__ constexpr int pblk_hq(int hd) { return (hd + 1) & ~1; }
+__host__ __device__ constexpr int pblk_hr(int hd) { return (hd + 7) & ~7; }
+/* row stride of the matrices: odd, so a column's rows fall in distinct banks */
+__host__ __device__ constexpr int pblk_rs(int hd, int CS) { return pblk_ncol(hd, CS) + 1; }
+/* plane stride of V's components: 8 (mod 16) doubles, so the four components
+ * of a tensor-core tile row fall in different banks */
+__host__ __device__ constexpr int pblk_plane(int hd, int CS) {
+  return pblk_hq(hd) * pblk_rs(hd, CS) + ((8 - (pblk_hq(hd) * pblk_rs(hd, CS)) % 16) + 16) % 16;
+}
+__host__ __device__ constexpr size_t pblk_smem_bytes(int hd, int CS) {
+  return sizeof(double) * ((size_t)4 * pblk_plane(hd, CS) + (size_t)pblk_hr(hd) * pblk_rs(hd, CS) +
+                           (size_t)pblk_hq(hd) * PB_NB * 4 + (size_t)pblk_hr(hd) * PB_NB + (size_t)pblk_hq(hd) * 8 +
+                           (size_t)pblk_hr(hd) * 2 + 4 * 32) +
+         sizeof(int) * ((size_t)2 * pblk_hq(hd) + 2 * pblk_hr(hd) + 4 * (size_t)hd + 2 + 4 * 32);
+}
+__host__ __device__ constexpr int pblk_threads(int hd, int CS) {
+  return 64 * (pblk_ncol(hd, CS) / 8) > PB_MAXT ? PB_MAXT : 64 * (pblk_ncol(hd, CS) / 8);
+}
+/* sign of entry (c, d) of the left-multiplication matrix of a quaternion a,
+ * whose entry is sign * a[c ^ d]: rows (+---), (++-+), (+++-), (+-++) */
+__device__ __forceinline__ double lmul_sign(int c, int d) {
+  return ((0x284Eu >> (4 * c + d)) & 1u) ? -1.0 : 1.0;
+}
+
+template <int CS>
+__global__ void __launch_bounds__(PB_MAXT, 1) k_rrq_panel_blk(OrderTab T, PanelIn P, PairWS G, RRQWS R,
+                                                                const double* chart /* nullable */) {
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+  const int pan = R.plo + (int)(blockIdx.x / CS);
+  if (G.cnt[(size_t)pan * 8 + T.nlevel + 1] == 0 && !R.all_panels) return; /* whole cluster */
+  const int hd = T.hd, nq = T.nquad, nbd = 3 * nq, L = T.nterms;
+  const int ncol = pblk_ncol(hd, CS), hq = pblk_hq(hd), hr = pblk_hr(hd), PL = pblk_plane(hd, CS);
+  const int RS = pblk_rs(hd, CS); /* row stride of Xq's planes and of Xr */
+  const int c0 = rank * ncol; /* this CTA's columns c0 .. c0 + ncol - 1 (those < hd valid) */
+  const int NT = blockDim.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, NW = NT >> 5;
+  extern __shared__ __align__(16) double psm[];
+  double* Xq = psm;                           /* [comp][row][col], plane stride PL */
+  double* Xr = Xq + 4 * (size_t)PL;           /* [row][col] */
+  double* Mq = Xr + (size_t)hr * RS;          /* [row][b][comp] */
+  double* Mr = Mq + (size_t)hq * PB_NB * 4;   /* [row][b] */
+  double* fq = Mr + (size_t)hr * PB_NB;       /* pivot column of V, 2 buffers: [buf][comp][row] */
+  double* fr = fq + (size_t)hq * 8;           /* pivot column of MS, 2 buffers */
+  double* cv = fr + (size_t)hr * 2;           /* next-pivot candidates a warp: [buf][V, MS][warp] */
+  int* usedq = (int*)(cv + 4 * 32);
+  int* usedr = usedq + hq;
+  int* isPq = usedr + hr; /* rows of the current block's pivots */
+  int* isPr = isPq + hq;
+  int* pivq = isPr + hr;  /* pivot row of each column, V then MS */
+  int* pivr = pivq + hd;
+  int* posq = pivr + hd;  /* inverse permutations */
+  int* posr = posq + hd;
+  int* pidx = posr + hd;  /* 2: the first step's pivot rows (explicit search) */
+  int* ci = pidx + 2;     /* candidate rows, as cv */
+  /* geometry staging aliases the block buffers (free until the first block) */
+  double* s_sx = Mq;
+  double* s_raw = s_sx + 3 * hd;
+  double* s_fr = s_raw + 3 * (nbd + 3);
+  panel_frame_setup(T, P, R, chart, pan, rank, s_sx, s_raw, s_fr);
+  const double alpha = s_fr[12];
+  double fr9[13];
 #pragma unroll
-    for (int u = 0; u < NBX; ++u)
-#pragma unroll
-      for (int v = 0; v < MBX; ++v) { acc[u][v][0] = 0.0; acc[u][v][1] = 0.0; }
-    for (int k0 = 0; k0 < KP; k0 += KT) {
-      __syncthreads();
-      for (int e = threadIdx.x; e < 8 * MBn * KT; e += NT) {
-        const int i = e / KT, kk = e % KT, k = k0 + kk;
-        sP[i * SK + kk] = (i < nc && k < hd) ? PS[(size_t)(c0 + i) * hd + k] : 0.0;
-      }
-      for (int e = threadIdx.x; e < 8 * NBn * KT; e += NT) {
-        const int j = e / KT, kk = e % KT, k = k0 + kk;
-        sH[j * SK + kk] = (j < hd && k < hd) ? H[(size_t)j * hd + k] : 0.0;
-      }
-      __syncthreads();
-      const int kst = min(KT, KP - k0) / 4;
-      for (int ks = 0; ks < kst; ++ks) {
-        const int kc = 4 * ks + (lane & 3);
-#pragma unroll
-        for (int u = 0; u < NBX; ++u) {
-          const int nb = wid + NW * u;
-          if (nb >= NBn) continue;
-          const double bv = sH[(8 * nb + (lane >> 2)) * SK + kc];
-#pragma unroll
-          for (int v = 0; v < MBX; ++v)
-            if (v < MBn) dmma(acc[u][v][0], acc[u][v][1], sP[(8 * v + (lane >> 2)) * SK + kc], bv);
+  for (int i = 0; i < 13; ++i) fr9[i] = s_fr[i];
+  auto tofr = [&](const double* x, double* y) {
+    double d0 = x[0] - fr9[9], d1 = x[1] - fr9[10], d2 = x[2] - fr9[11];
+    for (int i = 0; i < 3; ++i) y[i] = alpha * (fr9[i] * d0 + fr9[i + 3] * d1 + fr9[i + 6] * d2);
+  };
+  /* zero the matrices (padding rows and columns stay zero) and the bookkeeping */
+  for (int e = tid; e < 4 * PL + hr * RS; e += NT) Xq[e] = 0.0;
+  for (int e = tid; e < hq; e += NT) usedq[e] = e >= hd; /* padding rows never pivot */
+  for (int e = tid; e < hr; e += NT) usedr[e] = e >= hd;
+  __syncthreads();
+  /* basis at the nodes: V[j][k] = (0, grad h_k(y_j)) for this CTA's harmonics
+   * k, MS[k][j] = n_j . grad h_k(y_j) for this CTA's nodes j, H rows of its nodes */
+  double* H = R.hmat + (size_t)pan * hd * hd; /* H[j*hd+k] = h_k(y_j) */
+  for (int e = tid; e < hd * L; e += NT) {
+    const int j = e / L, m = e % L + 1;
+    double y[3], nrm[3];
+    tofr(&s_sx[3 * j], y);
+    const double* sn = P.snx + ((size_t)pan * hd + j) * 3;
+    for (int i = 0; i < 3; ++i) nrm[i] = fr9[i] * sn[0] + fr9[i + 3] * sn[1] + fr9[i + 6] * sn[2];
+    const bool ownj = j >= c0 && j < c0 + ncol;
+    harm_column(L, m, y[0], y[1], y[2], [&](int l, int k, double h, double gx, double gy, double gz) {
+        if (k >= c0 && k < c0 + ncol) {
+          const int lc = k - c0;
+          Xq[PL + (size_t)j * RS + lc] = gx;
+          Xq[2 * PL + (size_t)j * RS + lc] = gy;
+          Xq[3 * PL + (size_t)j * RS + lc] = gz;
         }
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < NBX; ++u) {
-      const int nb = wid + NW * u;
-      if (nb >= NBn) continue;
-#pragma unroll
-      for (int v = 0; v < MBX; ++v) {
-        const int i = 8 * v + (lane >> 2);
-        if (v >= MBn || i >= nc) continue;
-#pragma unroll
-        for (int h2 = 0; h2 < 2; ++h2) {
-          const int j = 8 * nb + 2 * (lane & 3) + h2;
-          if (j < hd) B[(size_t)(c0 + i) * hd + j] = acc[u][v][h2];
+        if (ownj) {
+          Xr[(size_t)k * RS + (j - c0)] = nrm[0] * gx + nrm[1] * gy + nrm[2] * gz;
+          H[(size_t)j * hd + k] = h;
         }
-      }
-    }
+      });
   }
+  __syncthreads();
+  double* Mq_r[CS];
+  double* Mr_r[CS];
+  int* pivq_r[CS];
+#pragma unroll
+  for (int r = 0; r < CS; ++r) {
+    Mq_r[r] = cl.map_shared_rank(Mq, r);
+    Mr_r[r] = cl.map_shared_rank(Mr, r);
+    pivq_r[r] = cl.map_shared_rank(pivq, r);
+  }
+  const int nblk = (hd + PB_NB - 1) / PB_NB;
+  for (int blk = 0; blk < nblk; ++blk) {
+    const int k0 = blk * PB_NB, owner = k0 / ncol, lb0 = k0 - owner * ncol;
+    const int nbk = min(PB_NB, hd - k0);
+    if (rank == owner) {
+      /* panel phase: the unblocked steps on the block's columns alone, one
+       * barrier a step.  Step j: every thread forms the pivot inverses from
+       * the pivot column (kept in fq/fr) and the scaled pivot row entries it
+       * needs from the pivot row, left unscaled in shared memory until the
+       * next step (whose items scale it first, the deferred scaling), and
+       * eliminates; the items of column j+1 also copy their new entries into
+       * the other fq/fr buffer and propose the next pivot (largest norm among
+       * the unused rows, smallest row on ties: the unblocked rule), reduced a
+       * warp at a time into cv/ci and over the warps by every thread at the
+       * start of the next step.  The first column of the block is searched
+       * explicitly. */
+      for (int e = tid; e < hq; e += NT)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) fq[c * hq + e] = Xq[c * PL + (size_t)e * RS + lb0];
+      for (int e = tid; e < hr; e += NT) fr[e] = Xr[(size_t)e * RS + lb0];
+      if (wid < 2) { /* warp 0: V's pivot, warp 1: MS's pivot */
+        double bv = -1.0;
+        int bi = hd;
+        for (int i = lane; i < hd; i += 32) {
+          double v;
+          if (wid == 0) {
+            if (usedq[i]) continue;
+            const double a0 = Xq[(size_t)i * RS + lb0], a1 = Xq[PL + (size_t)i * RS + lb0];
+            const double a2 = Xq[2 * PL + (size_t)i * RS + lb0], a3 = Xq[3 * PL + (size_t)i * RS + lb0];
+            v = a0 * a0 + a1 * a1 + a2 * a2 + a3 * a3;
+          } else {
+            if (usedr[i]) continue;
+            v = fabs(Xr[(size_t)i * RS + lb0]);
+          }
+          if (v > bv) { bv = v; bi = i; }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+          const double b2 = __shfl_xor_sync(0xffffffffu, bv, o);
+          const int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
+          if (b2 > bv || (b2 == bv && i2 < bi)) { bv = b2; bi = i2; }
+        }
+        if (lane == 0) pidx[wid] = bi;
+      }
+      __syncthreads();
+      int pq_prev = -1, pr_prev = -1;
+      double pvq[4] = {0.0, 0.0, 0.0, 0.0}, pvr = 0.0; /* previous step's pivot inverses */
+      for (int j = 0; j < nbk; ++j) {
+        const int cur = j & 1, nxt = cur ^ 1;
+        const double* fqc = fq + (size_t)cur * 4 * hq;
+        double* fqn = fq + (size_t)nxt * 4 * hq;
+        const double* frc = fr + (size_t)cur * hr;
+        double* frn = fr + (size_t)nxt * hr;
+        /* this step's pivot rows */
+        int p, p2;
+        if (j == 0) {
+          p = pidx[0]; p2 = pidx[1];
+        } else {
+          const double* cvb = cv + (size_t)cur * 64; /* written by step j-1 (its "next" buffer) */
+          const int* cib = ci + (size_t)cur * 64;
+          double b1 = -1.0, b2 = -1.0;
+          p = hd; p2 = hd;
+          for (int w = 0; w < NW; ++w) {
+            const double v1 = cvb[w], v2 = cvb[32 + w];
+            const int i1 = cib[w], i2 = cib[32 + w];
+            if (v1 > b1 || (v1 == b1 && i1 < p)) { b1 = v1; p = i1; }
+            if (v2 > b2 || (v2 == b2 && i2 < p2)) { b2 = v2; p2 = i2; }
+          }
+        }
+        /* rows pivoted in earlier steps of this block (usedq/usedr hold earlier
+         * blocks' pivots; this block's are marked after it) */
+        auto blk_q = [&](int i) { for (int jj = 0; jj < j; ++jj) if (pivq[k0 + jj] == i) return true; return false; };
+        auto blk_r = [&](int i) { for (int jj = 0; jj < j; ++jj) if (pivr[k0 + jj] == i) return true; return false; };
+        if (p >= hd) { /* a NaN column: the first unused row (results NaN, indices in range) */
+          p = 0;
+          while (p < hd - 1 && (usedq[p] || blk_q(p))) ++p;
+        }
+        if (p2 >= hd) {
+          p2 = 0;
+          while (p2 < hd - 1 && (usedr[p2] || blk_r(p2))) ++p2;
+        }
+        double pi4[4];
+        {
+          const double f0 = fqc[p], f1 = fqc[hq + p], f2 = fqc[2 * hq + p], f3 = fqc[3 * hq + p];
+          const double n2i = 1.0 / (f0 * f0 + f1 * f1 + f2 * f2 + f3 * f3);
+          pi4[0] = f0 * n2i; pi4[1] = -f1 * n2i; pi4[2] = -f2 * n2i; pi4[3] = -f3 * n2i;
+        }
+        const double rinv = 1.0 / frc[p2];
+        if (tid == 0) pivq[k0 + j] = p; /* read from the next step on */
+        if (tid == 32) pivr[k0 + j] = p2;
+        double bv = -1.0, bw = -1.0;
+        int bi = hd, bj = hd;
+        for (int e = tid; e < hq * PB_NB; e += NT) { /* consecutive threads: consecutive rows */
+          const int i = e % hq, b = e / hq;
+          double* x0 = Xq + (size_t)i * RS + lb0 + b;
+          double x[4];
+#pragma unroll
+          for (int c = 0; c < 4; ++c) x[c] = x0[c * PL];
+          if (i == pq_prev) { /* the previous pivot row: its deferred scaling */
+            if (b == j - 1) {
+#pragma unroll
+              for (int c = 0; c < 4; ++c) x[c] = pvq[c];
+            } else {
+              double t[4];
+              qmul(pvq, x, t);
+#pragma unroll
+              for (int c = 0; c < 4; ++c) x[c] = t[c];
+            }
+          }
+          if (i == p) { /* this step's pivot row: scaled in the next step; its next-column entry */
+            if (b == j + 1) {
+              double t[4];
+              qmul(pi4, x, t);
+#pragma unroll
+              for (int c = 0; c < 4; ++c) fqn[c * hq + i] = t[c];
+            }
+            continue;
+          }
+          const double f[4] = {fqc[i], fqc[hq + i], fqc[2 * hq + i], fqc[3 * hq + i]};
+          double t[4];
+          if (b == j) {
+            qmul(f, pi4, t);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) x[c] = -t[c];
+          } else {
+            double xp[4], r[4];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) xp[c] = Xq[c * PL + (size_t)p * RS + lb0 + b];
+            qmul(pi4, xp, r); /* the scaled pivot row entry */
+            qmul(f, r, t);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) x[c] -= t[c];
+          }
+#pragma unroll
+          for (int c = 0; c < 4; ++c) x0[c * PL] = x[c];
+          if (b == j + 1) {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) fqn[c * hq + i] = x[c];
+            if (i < hd && !usedq[i] && !blk_q(i)) {
+              const double v = x[0] * x[0] + x[1] * x[1] + x[2] * x[2] + x[3] * x[3];
+              if (v > bv || (v == bv && i < bi)) { bv = v; bi = i; }
+            }
+          }
+        }
+        for (int e = tid; e < hr * PB_NB; e += NT) {
+          const int i = e % hr, b = e / hr;
+          double* x0 = Xr + (size_t)i * RS + lb0 + b;
+          double x = *x0;
+          if (i == pr_prev) x = (b == j - 1) ? pvr : pvr * x;
+          if (i == p2) {
+            if (b == j + 1) frn[i] = rinv * x;
+            continue;
+          }
+          if (b == j) x = -frc[i] * rinv;
+          else x -= frc[i] * (rinv * Xr[(size_t)p2 * RS + lb0 + b]);
+          *x0 = x;
+          if (b == j + 1) {
+            frn[i] = x;
+            if (i < hd && !usedr[i] && !blk_r(i)) {
+              const double v = fabs(x);
+              if (v > bw || (v == bw && i < bj)) { bw = v; bj = i; }
+            }
+          }
+        }
+        if (j + 1 < nbk) { /* this warp's next-pivot candidates */
+          for (int o = 16; o > 0; o >>= 1) {
+            const double v2 = __shfl_xor_sync(0xffffffffu, bv, o);
+            const int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
+            if (v2 > bv || (v2 == bv && i2 < bi)) { bv = v2; bi = i2; }
+            const double w2 = __shfl_xor_sync(0xffffffffu, bw, o);
+            const int j2 = __shfl_xor_sync(0xffffffffu, bj, o);
+            if (w2 > bw || (w2 == bw && j2 < bj)) { bw = w2; bj = j2; }
+          }
+          if (lane == 0) {
+            cv[(size_t)nxt * 64 + wid] = bv; ci[(size_t)nxt * 64 + wid] = bi;
+            cv[(size_t)nxt * 64 + 32 + wid] = bw; ci[(size_t)nxt * 64 + 32 + wid] = bj;
+          }
+        }
+        __syncthreads();
+        pq_prev = p; pr_prev = p2;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) pvq[c] = pi4[c];
+        pvr = rinv;
+      }
+      /* the last pivot rows' deferred scaling */
+      if (tid < PB_NB) {
+        const int b = tid;
+        double* x0 = Xq + (size_t)pq_prev * RS + lb0 + b;
+        double t[4];
+        if (b == nbk - 1) {
+#pragma unroll
+          for (int c = 0; c < 4; ++c) t[c] = pvq[c];
+        } else {
+          double x[4];
+#pragma unroll
+          for (int c = 0; c < 4; ++c) x[c] = x0[c * PL];
+          qmul(pvq, x, t);
+        }
+#pragma unroll
+        for (int c = 0; c < 4; ++c) x0[c * PL] = t[c];
+      } else if (tid >= 32 && tid < 32 + PB_NB) {
+        const int b = tid - 32;
+        double* x0 = Xr + (size_t)pr_prev * RS + lb0 + b;
+        *x0 = (b == nbk - 1) ? pvr : pvr * *x0;
+      }
+      __syncthreads();
+      /* publish the block and its pivot rows to every CTA of the cluster */
+      for (int e = tid; e < hq * PB_NB * 4; e += NT) {
+        const int c = e & 3, b = (e >> 2) & 7, i = e >> 5;
+        const double v = Xq[c * PL + (size_t)i * RS + lb0 + b];
+#pragma unroll
+        for (int r = 0; r < CS; ++r) Mq_r[r][e] = v;
+      }
+      for (int e = tid; e < hr * PB_NB; e += NT) {
+        const double v = Xr[(size_t)(e >> 3) * RS + lb0 + (e & 7)];
+#pragma unroll
+        for (int r = 0; r < CS; ++r) Mr_r[r][e] = v;
+      }
+      if (tid < nbk) {
+#pragma unroll
+        for (int r = 0; r < CS; ++r) { pivq_r[r][k0 + tid] = pivq[k0 + tid]; pivq_r[r][hd + k0 + tid] = pivr[k0 + tid]; }
+      }
+    }
+    cl.sync();
+    /* this block's pivot rows */
+    for (int e = tid; e < hq; e += NT) {
+      int f = 0;
+      for (int j = 0; j < nbk; ++j) f |= pivq[k0 + j] == e;
+      isPq[e] = f;
+      if (f) usedq[e] = 1;
+    }
+    for (int e = tid; e < hr; e += NT) {
+      int f = 0;
+      for (int j = 0; j < nbk; ++j) f |= pivr[k0 + j] == e;
+      isPr[e] = f;
+      if (f) usedr[e] = 1;
+    }
+    __syncthreads();
+    /* trailing update of this CTA's other columns: warp w takes column tile
+     * w % ntl and every G-th row tile, B fragments (the pivot rows) read
+     * before any tile is stored */
+    {
+      const int ntl = ncol / 8, skip = rank == owner ? lb0 / 8 : -1;
+      const int Gq = NW >= ntl ? NW / ntl : 1;
+      const bool act = wid < Gq * ntl;
+      const int nt = wid % ntl, g0 = wid / ntl;
+      const int J = 8 * nt + (lane >> 2);
+      double bq[PB_NB], br2[2];
+      const int d = lane & 3;
+#pragma unroll
+      for (int ks = 0; ks < PB_NB; ++ks) {
+        const int prow = ks < nbk ? pivq[k0 + ks] : 0;
+        bq[ks] = (act && ks < nbk) ? Xq[d * PL + (size_t)prow * RS + J] : 0.0;
+      }
+#pragma unroll
+      for (int ks = 0; ks < 2; ++ks) {
+        const int b = 4 * ks + d;
+        const int prow = b < nbk ? pivr[k0 + b] : 0;
+        br2[ks] = (act && b < nbk) ? Xr[(size_t)prow * RS + J] : 0.0;
+      }
+      __syncthreads();
+      if (act && nt != skip) {
+        /* quaternion system: row tiles of 8 real rows = 2 quaternion rows */
+        const int cc = (lane >> 2) & 3, ci = cc ^ d;
+        const double sg = lmul_sign(cc, d);
+        const int jc = 8 * nt + 2 * (lane & 3);
+        for (int mt = g0; mt < hq / 2; mt += Gq) {
+          const int i = 2 * mt + (lane >> 4);
+          double* xr = Xq + cc * PL + (size_t)i * RS + jc;
+          const bool zp = isPq[i] != 0;
+          double a0 = zp ? 0.0 : xr[0], a1 = zp ? 0.0 : xr[1];
+          const double* mrow = Mq + (size_t)i * PB_NB * 4;
+#pragma unroll
+          for (int ks = 0; ks < PB_NB; ++ks) dmma(a0, a1, sg * mrow[4 * ks + ci], bq[ks]);
+          xr[0] = a0; xr[1] = a1;
+        }
+        /* real system */
+        for (int mt = g0; mt < hr / 8; mt += Gq) {
+          const int i = 8 * mt + (lane >> 2);
+          double* xr = Xr + (size_t)i * RS + jc;
+          const bool zp = isPr[i] != 0;
+          double a0 = zp ? 0.0 : xr[0], a1 = zp ? 0.0 : xr[1];
+#pragma unroll
+          for (int ks = 0; ks < 2; ++ks) dmma(a0, a1, Mr[(size_t)i * PB_NB + 4 * ks + d], br2[ks]);
+          xr[0] = a0; xr[1] = a1;
+        }
+      }
+    }
+    cl.sync(); /* every CTA is done with the block before the next is published */
+  }
+  /* inverse positions of the pivot sequences (every CTA holds all pivots) */
+  for (int k = tid; k < hd; k += NT) { posq[pivq[k]] = k; posr[pivr[k]] = k; }
+  __syncthreads();
+  double* PD = R.PD + (size_t)pan * hd * 4 * hd;
+  double* PS = R.smat + (size_t)pan * hd * hd;
+  const int nc = min(ncol, hd - c0);
+  for (int e = tid; e < hd * nc; e += NT) {
+    const int i = e / nc, tc = e % nc, gc = c0 + tc;
+    const int jq = pivq[gc], kq = posq[i];
+    double* d = PD + (size_t)jq * 4 * hd + kq;
+    d[0] = Xq[(size_t)i * RS + tc];
+    d[hd] = -Xq[PL + (size_t)i * RS + tc];
+    d[2 * hd] = -Xq[2 * PL + (size_t)i * RS + tc];
+    d[3 * hd] = -Xq[3 * PL + (size_t)i * RS + tc];
+    PS[(size_t)posr[i] * hd + pivr[gc]] = Xr[(size_t)i * RS + tc];
+  }
+  __threadfence();
+  cl.sync();
+  panel_b_epilogue(R, hd, pan, c0, nc, (int)(pblk_smem_bytes(hd, CS) / sizeof(double)), psm);
 }
 
 /* ===================================================================== */
@@ -1984,28 +2456,37 @@ cudaError_t qol_launch_scan(int npan, int lev, const int* cnt, long long* off, c
   k_scan_rrq<<<1, 1024, 0, st>>>(npan, lev, cnt, off);
   return cudaGetLastError();
 }
+/* the blocked panel kernel's cluster sizes for hd: every CS whose columns fit
+ * (shared memory <= 227 KB, at most 9 column tiles a CTA), smallest first */
+static int pblk_cluster_sizes(int hd, int* out) {
+  int n = 0;
+  for (int cs : {1, 2, 4, 8}) {
+    if (pblk_ncol(hd, cs) > 72 || pblk_smem_bytes(hd, cs) > 227 * 1024) continue;
+    if (cs > 1 && pblk_ncol(hd, cs) * (cs - 1) >= hd) continue; /* every CTA owns a valid column */
+    out[n++] = cs;
+  }
+  return n;
+}
 cudaError_t qol_launch_rrq_panel(const OrderTab& T, const PanelIn& P, const PairWS& G, const RRQWS& R, int npan,
                                  const double* chart, cudaStream_t st) {
   if (npan <= 0) return cudaSuccess;
-  /* the smallest cluster (then the wider CTA) whose threads hold few enough
-   * rows to keep them in registers: at most 6 rows with 512 threads (128
-   * registers a thread), 12 with 384 */
-  int cs = 0, nt = 0, maxr = 0;
-  if (T.panel_cs) { /* a shape chosen by measurement (qol_panel_shapes lists them) */
-    cs = T.panel_cs; nt = T.panel_nt; maxr = panel_maxr(T.hd, cs, nt);
-  } else {
-    for (int c = 1; c <= 8 && !cs; c *= 2)
-      for (int t : {512, 384}) {
-        const int m = panel_maxr(T.hd, c, t);
-        if (m <= (t == 512 ? 6 : 12)) { cs = c; nt = t; maxr = m; break; }
-      }
-  }
-  if (!cs) return cudaErrorInvalidConfiguration;
-  const size_t smem = sizeof(double) * panel_smem_doubles(T.hd, 3 * T.nquad, cs);
-  if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
+  int sizes[4];
+  const int nsz = pblk_cluster_sizes(T.hd, sizes);
+  if (nsz == 0) return cudaErrorInvalidConfiguration;
+  /* a cluster size chosen by measurement (qol_panel_shapes lists them), else the smallest */
+  int cs = sizes[0];
+  if (T.panel_cs)
+    for (int i = 0; i < nsz; ++i)
+      if (sizes[i] == T.panel_cs) cs = T.panel_cs;
+  const size_t smem = pblk_smem_bytes(T.hd, cs);
+  const int nt = pblk_threads(T.hd, cs);
   auto go = [&](auto kern) -> cudaError_t {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
+    if (cs > 1) {
+      e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+      if (e != cudaSuccess) return e;
+    }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(npan * cs));
     cfg.blockDim = dim3((unsigned)nt);
@@ -2020,29 +2501,20 @@ cudaError_t qol_launch_rrq_panel(const OrderTab& T, const PanelIn& P, const Pair
     cfg.numAttrs = 1;
     return cudaLaunchKernelEx(&cfg, kern, T, P, G, R, chart);
   };
-  /* the configurations of nterms 2..16 */
-#define QOL_PANEL_CASE(C, N, M) \
-  if (cs == C && nt == N && maxr <= M) return go(k_rrq_panel<C, N, M>);
-  QOL_PANEL_CASE(1, 512, 1) QOL_PANEL_CASE(1, 512, 2) QOL_PANEL_CASE(1, 512, 3) QOL_PANEL_CASE(1, 512, 5)
-  QOL_PANEL_CASE(1, 384, 10) QOL_PANEL_CASE(2, 512, 5) QOL_PANEL_CASE(2, 512, 6) QOL_PANEL_CASE(2, 384, 12)
-  QOL_PANEL_CASE(4, 512, 6) QOL_PANEL_CASE(4, 384, 10) QOL_PANEL_CASE(8, 512, 5)
-#undef QOL_PANEL_CASE
-  return cudaErrorInvalidConfiguration;
+  switch (cs) {
+    case 1: return go(k_rrq_panel_blk<1>);
+    case 2: return go(k_rrq_panel_blk<2>);
+    case 4: return go(k_rrq_panel_blk<4>);
+    default: return go(k_rrq_panel_blk<8>);
+  }
 }
 int qol_panel_shapes(int hd, int nquad, int* cs, int* nt, int cap) {
-  /* the instantiated (cluster, threads, row bound) triples of qol_launch_rrq_panel */
-  static const int inst[][3] = {{1, 512, 5}, {1, 384, 10}, {2, 512, 6}, {2, 384, 12}, {4, 512, 6}, {4, 384, 10}, {8, 512, 5}};
-  int n = 0;
-  for (const auto& in : inst) {
-    const int c = in[0], t = in[1];
-    if (panel_maxr(hd, c, t) > in[2] || panel_ncol(hd, c) > t) continue;
-    if (sizeof(double) * panel_smem_doubles(hd, 3 * nquad, c) > 227 * 1024) continue;
-    const int mbn = (panel_ncol(hd, c) + 7) / 8, nbn = (hd + 7) / 8;
-    if (mbn > 8 || nbn > 2 * (t / 32)) continue; /* the B epilogue's blocks a warp */
-    if (n < cap) { cs[n] = c; nt[n] = t; }
-    ++n;
-  }
-  return n < cap ? n : cap;
+  (void)nquad;
+  int sizes[4];
+  const int n = pblk_cluster_sizes(hd, sizes);
+  int k = 0;
+  for (int i = 0; i < n && k < cap; ++i, ++k) { cs[k] = sizes[i]; nt[k] = pblk_threads(hd, sizes[i]); }
+  return k;
 }
 cudaError_t qol_launch_rrq_pairs(const OrderTab& T, const PairIn& Q, const PairWS& G, const RRQWS& R, int npan,
                                  cudaStream_t st) {
@@ -2191,7 +2663,8 @@ __global__ void __launch_bounds__(256) k_ball_count(long long nsrc, const double
 /* their 1-based indices in source order (the reference's CSR), the target
  * coordinates gathered alongside */
 __global__ void __launch_bounds__(256) k_ball_fill(long long nsrc, const double* sx, const double* ball,
-                                                   const long long* offs, long long* csr_idx, double* tcx) {
+                                                   const long long* offs, long long* csr_idx, double* tcx,
+                                                   long long* csr_loc /* nullable */, long long row_shift) {
   const int k = blockIdx.x;
   __shared__ double b[4];
   __shared__ int wcnt[8];
@@ -2210,6 +2683,7 @@ __global__ void __launch_bounds__(256) k_ball_fill(long long nsrc, const double*
     if (hit) {
       const long long pos = base + before + __popc(m & ((1u << lane) - 1u));
       csr_idx[pos] = j + 1;
+      if (csr_loc) csr_loc[pos] = j + 1 - row_shift; /* the pipeline's numbering of a panel range */
       tcx[3 * pos] = sx[3 * j]; tcx[3 * pos + 1] = sx[3 * j + 1]; tcx[3 * pos + 2] = sx[3 * j + 2];
     }
     base += total;
@@ -2266,12 +2740,13 @@ __global__ void __launch_bounds__(256) k_grf_scatter(int npan, long long nsrc, c
  * source order (the reference's blocked Direct far field) */
 #define FAR_TILE 256
 __global__ void __launch_bounds__(256) k_direct_far(long long nsrc, const double* sx, const double* snx,
-                                                    const double* sw, const double* ub, const double* ubn, double* u) {
+                                                    const double* sw, const double* ub, const double* ubn, double* u,
+                                                    long long tlo, long long thi) {
   __shared__ double sj[FAR_TILE][8]; /* x, y, z, nx, ny, nz, w/4pi ubn, w/4pi ub */
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long i = tlo + (long long)blockIdx.x * blockDim.x + threadIdx.x; /* targets [tlo, thi) */
   const double i4p = 1.0 / (4.0 * QOL_PI);
   double x0 = 0.0, x1 = 0.0, x2 = 0.0;
-  if (i < nsrc) { x0 = sx[3 * i]; x1 = sx[3 * i + 1]; x2 = sx[3 * i + 2]; }
+  if (i < thi) { x0 = sx[3 * i]; x1 = sx[3 * i + 1]; x2 = sx[3 * i + 2]; }
   double acc = 0.0;
   for (long long j0 = 0; j0 < nsrc; j0 += FAR_TILE) {
     const int nj = (int)min((long long)FAR_TILE, nsrc - j0);
@@ -2292,18 +2767,19 @@ __global__ void __launch_bounds__(256) k_direct_far(long long nsrc, const double
       }
     }
   }
-  if (i < nsrc) u[i] = acc;
+  if (i < thi) u[i] = acc;
 }
 
 cudaError_t qol_launch_grf_balls(int npan, int hd, long long nsrc, const double* sx, const double* sw, double* ball,
-                                 long long* counts, cudaStream_t st) {
+                                 long long* counts, int plo, int phi, cudaStream_t st) {
   k_ball_centers<<<(npan + 127) / 128, 128, 0, st>>>(npan, hd, sx, sw, ball);
-  k_ball_count<<<npan, 256, 0, st>>>(nsrc, sx, ball, counts);
+  if (phi > plo) k_ball_count<<<phi - plo, 256, 0, st>>>(nsrc, sx, ball + 4 * (size_t)plo, counts);
   return cudaGetLastError();
 }
 cudaError_t qol_launch_grf_csr(int npan, long long nsrc, const double* sx, const double* ball, const long long* offs,
-                               long long* csr_idx, double* tcx, cudaStream_t st) {
-  k_ball_fill<<<npan, 256, 0, st>>>(nsrc, sx, ball, offs, csr_idx, tcx);
+                               long long* csr_idx, double* tcx, long long* csr_loc, long long row_shift,
+                               cudaStream_t st) {
+  k_ball_fill<<<npan, 256, 0, st>>>(nsrc, sx, ball, offs, csr_idx, tcx, csr_loc, row_shift);
   return cudaGetLastError();
 }
 cudaError_t qol_launch_grf_apply(int npan, int hd, long long nsrc, const double* sx, const double* ball,
@@ -2314,7 +2790,9 @@ cudaError_t qol_launch_grf_apply(int npan, int hd, long long nsrc, const double*
   return cudaGetLastError();
 }
 cudaError_t qol_launch_direct_far(long long nsrc, const double* sx, const double* snx, const double* sw,
-                                  const double* ub, const double* ubn, double* u, cudaStream_t st) {
-  k_direct_far<<<(unsigned)((nsrc + 255) / 256), 256, 0, st>>>(nsrc, sx, snx, sw, ub, ubn, u);
+                                  const double* ub, const double* ubn, double* u, long long tlo, long long thi,
+                                  cudaStream_t st) {
+  if (thi <= tlo) return cudaSuccess;
+  k_direct_far<<<(unsigned)((thi - tlo + 255) / 256), 256, 0, st>>>(nsrc, sx, snx, sw, ub, ubn, u, tlo, thi);
   return cudaGetLastError();
 }

@@ -125,12 +125,18 @@ cudaError_t qol_launch_coo_index(const OrderTab& T, const PairIn& Q, long long* 
                                  cudaStream_t st);
 cudaError_t qol_launch_fp64_peak(double* out, int blocks, int iters, cudaStream_t st);
 /* GRF near phase and Direct far field */
+/* ball centres of all npan panels; near counts of panels [plo, phi) into counts[0 .. phi - plo) */
 cudaError_t qol_launch_grf_balls(int npan, int hd, long long nsrc, const double* sx, const double* sw, double* ball,
-                                 long long* counts, cudaStream_t st);
+                                 long long* counts, int plo, int phi, cudaStream_t st);
+/* CSR of npan panels (ball points at their first ball); csr_loc (nullable) gets the
+ * rows minus row_shift */
 cudaError_t qol_launch_grf_csr(int npan, long long nsrc, const double* sx, const double* ball, const long long* offs,
-                               long long* csr_idx, double* tcx, cudaStream_t st);
+                               long long* csr_idx, double* tcx, long long* csr_loc, long long row_shift,
+                               cudaStream_t st);
 cudaError_t qol_launch_grf_apply(int npan, int hd, long long nsrc, const double* sx, const double* ball,
                                  const long long* offs, const long long* csr_idx, const double* vs, const double* vd,
                                  const double* ub, const double* ubn, double* csr_val, double* u, cudaStream_t st);
+/* u_i for the targets i in [tlo, thi) over all nsrc sources */
 cudaError_t qol_launch_direct_far(long long nsrc, const double* sx, const double* snx, const double* sw,
-                                  const double* ub, const double* ubn, double* u, cudaStream_t st);
+                                  const double* ub, const double* ubn, double* u, long long tlo, long long thi,
+                                  cudaStream_t st);

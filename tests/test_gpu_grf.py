@@ -63,3 +63,42 @@ def test_grf_identity_gpu_only(qol):
                                     ubn, u=u)
         errs.append(np.abs(un).max() / np.abs(ubn).max())
     assert errs[0] < 1e-3 and errs[1] < 2e-5 and errs[2] < 2e-6, errs
+
+
+def test_ranges_add_up_to_the_whole(qol):
+    """The multi-GPU split on one GPU: qol_grf_near_range over a partition of
+    the panels and qol_direct_farfield_range over a partition of the targets
+    add up to the single calls (to rounding: only the order in which a node's
+    corrections are added differs), and getnearquad shards with renumbered
+    rows concatenate to the single call's output byte for byte."""
+    from qotential_b200 import geometry as G
+    from qotential_b200 import sharding as S
+    nterms = 6
+    P, ub, ubn = _surface(G, G.stellarator(), 4, 10, nterms)
+    hd = nterms * (nterms + 1) // 2
+    npan = P["sw"].size // hd
+    nsrc = npan * hd
+    nq = nterms + 2
+    full_far = qol.qol_direct_farfield(P["sx"], P["snx"], P["sw"], ub, ubn)
+    full, nn, hist = qol.qol_grf_near(npan, nterms, nq, P["sx"], P["snx"], P["sw"], P["rts"], P["rps"], ub, ubn,
+                                      u=full_far)
+    tcxi, _, tcx = G.near_lists(P["sx"], P["sw"], hd)
+    ranges = S.balanced_ranges(S.panel_costs(tcxi, tcx, P["sx"], P["sw"], hd), 3)
+    total = np.zeros(nsrc)
+    for r, (a, b) in enumerate(ranges):
+        part = np.zeros(nsrc)
+        qol.qol_direct_farfield_range(P["sx"], P["snx"], P["sw"], ub, ubn, (r * nsrc) // 3, ((r + 1) * nsrc) // 3,
+                                      part)
+        part = qol.qol_grf_near_range(npan, nterms, nq, P["sx"], P["snx"], P["sw"], P["rts"], P["rps"], ub, ubn, a, b,
+                                      u=part)
+        total += part
+    assert np.abs(total - full).max() <= 1e-13 * np.abs(full).max()
+    # getnearquad: per-rank shards
+    T = np.concatenate([P["sx"], G.off_surface_targets(P, 200, 4, hd)])
+    tcxi, tcxrow, tcx = G.near_lists(P["sx"], P["sw"], hd, targets=T)
+    one = qol.qol_getnearquad_lap_rrq(npan, nterms, hd, nq, nsrc, P["sx"], P["snx"], P["sw"], P["rts"], P["rps"],
+                                      tcxrow.size, tcx, tcxrow, tcxi, nq, 1.4, 30)
+    parts = [S.getnearquad_shard(r, 2, npan, nterms, hd, nq, P["sx"], P["snx"], P["sw"], P["rts"], P["rps"], tcx,
+                                 tcxrow, tcxi, nq) for r in range(2)]
+    for k in range(4):
+        assert np.concatenate([p[k] for p in parts]).tobytes() == one[k].tobytes()

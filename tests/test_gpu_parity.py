@@ -211,6 +211,6 @@ def test_autotuned_panel_shape_same_results(qol):
         qol.qol_set_autotune(1)
     b = qol.qol_getnearquad_lap_rrq(*args)
     cs, nt = qol.qol_panel_shape(nterms, nterms + 2, nterms + 2)
-    assert cs in (1, 2, 4, 8) and nt in (384, 512)
+    assert cs in (1, 2, 4, 8) and nt % 64 == 0 and 64 <= nt <= 576
     for x, y in zip(a[:4], b[:4]):
         assert x.tobytes() == y.tobytes()

@@ -1,8 +1,9 @@
 """The N > 1 path of bench.py on CPU: two gloo ranks, each building its panel
-shard of the workload (bench.workload(rank, world)) and taking the step time
-as the maximum over ranks (all_reduce MAX), as the GPU run does over NCCL.
-The shards must partition the single-rank workload exactly: panels, near
-pairs and their CSR, in order."""
+shard of the workload (bench.workload(rank, world): a cost-balanced panel
+range, qotential_b200.sharding) and taking the step time as the maximum over
+ranks (all_reduce MAX), as the GPU run does over NCCL.  The shards must
+partition the single-rank workload exactly: panels, near pairs (rows shifted
+back by each shard's row shift) and their CSR, in order."""
 import os
 import socket
 import sys
@@ -36,8 +37,8 @@ def _rank(rank, world, port, q):
         ms = torch.tensor([10.0 * (rank + 1)])
         dist.all_reduce(ms, op=dist.ReduceOp.MAX)
         dist.barrier()
-        q.put((rank, [e.tolist() for e in every], float(ms.item()), W["tcxrow"].tolist(), W["tcxi"].tolist(),
-               W["sw"].tolist()))
+        q.put((rank, [e.tolist() for e in every], float(ms.item()), (W["tcxrow"] + W["row_shift"]).tolist(),
+               W["tcxi"].tolist(), W["sw"].tolist(), W["panel_range"]))
     finally:
         dist.destroy_process_group()
 
@@ -72,6 +73,7 @@ def test_two_gloo_ranks_partition_the_workload():
     assert np.array_equal(rows, full["tcxrow"])
     sw = np.concatenate([np.asarray(res[r][5]) for r in range(2)])
     assert np.array_equal(sw, full["sw"])
+    assert res[0][6][0] == 0 and res[0][6][1] == res[1][6][0] and res[1][6][1] == full["npan"]
     for r in range(2):  # each shard's CSR is one-based and covers its own pairs
         xi = np.asarray(res[r][4])
         assert xi[0] == 1 and xi[-1] == len(res[r][3]) + 1 and np.all(np.diff(xi) >= 0)
