@@ -1187,7 +1187,11 @@ __global__ void __launch_bounds__(NT, 1) k_rrq_panel(OrderTab T, PanelIn P, Pair
  * = ceil(hd / CS) rounded up to 8.
  * --------------------------------------------------------------------- */
 constexpr int PB_NB = 8;
-constexpr int PB_MAXT = 576; /* threads a CTA: two warps per 8-column tile, at most 9 tiles */
+constexpr int PB_MAXT = 512; /* threads a CTA: two warps per 8-column tile, at most 8 tiles */
+/* barrier of the first nthreads threads of the CTA (a multiple of 32) */
+__device__ __forceinline__ void named_bar(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(nthreads) : "memory");
+}
 __host__ __device__ constexpr int pblk_ncol(int hd, int CS) { return (((hd + CS - 1) / CS) + 7) & ~7; }
 __host__ __device__ constexpr int pblk_hq(int hd) { return (hd + 1) & ~1; }
 __host__ __device__ constexpr int pblk_hr(int hd) { return (hd + 7) & ~7; }
@@ -1200,12 +1204,13 @@ __host__ __device__ constexpr int pblk_plane(int hd, int CS) {
 }
 __host__ __device__ constexpr size_t pblk_smem_bytes(int hd, int CS) {
   return sizeof(double) * ((size_t)4 * pblk_plane(hd, CS) + (size_t)pblk_hr(hd) * pblk_rs(hd, CS) +
-                           (size_t)pblk_hq(hd) * PB_NB * 4 + (size_t)pblk_hr(hd) * PB_NB + (size_t)pblk_hq(hd) * 8 +
-                           (size_t)pblk_hr(hd) * 2 + 4 * 32) +
-         sizeof(int) * ((size_t)2 * pblk_hq(hd) + 2 * pblk_hr(hd) + 4 * (size_t)hd + 2 + 4 * 32);
+                           (size_t)pblk_hq(hd) * PB_NB * 4 + (size_t)pblk_hr(hd) * PB_NB +
+                           2 * ((size_t)pblk_hq(hd) * 4 + pblk_hr(hd) + 8)) +
+         sizeof(int) * ((size_t)2 * pblk_hq(hd) + 2 * pblk_hr(hd) + 4 * (size_t)hd + 4);
 }
 __host__ __device__ constexpr int pblk_threads(int hd, int CS) {
-  return 64 * (pblk_ncol(hd, CS) / 8) > PB_MAXT ? PB_MAXT : 64 * (pblk_ncol(hd, CS) / 8);
+  return 64 * (pblk_ncol(hd, CS) / 8) > PB_MAXT ? PB_MAXT
+         : (64 * (pblk_ncol(hd, CS) / 8) < 32 * PB_NB ? 32 * PB_NB : 64 * (pblk_ncol(hd, CS) / 8));
 }
 /* sign of entry (c, d) of the left-multiplication matrix of a quaternion a,
  * whose entry is sign * a[c ^ d]: rows (+---), (++-+), (+++-), (+-++) */
@@ -1213,7 +1218,7 @@ __device__ __forceinline__ double lmul_sign(int c, int d) {
   return ((0x284Eu >> (4 * c + d)) & 1u) ? -1.0 : 1.0;
 }
 
-template <int CS>
+template <int CS, int PB_MAXS /* row slots of a lane in the panel phase: hq <= 32 PB_MAXS */>
 __global__ void __launch_bounds__(PB_MAXT, 1) k_rrq_panel_blk(OrderTab T, PanelIn P, PairWS G, RRQWS R,
                                                                 const double* chart /* nullable */) {
   cg::cluster_group cl = cg::this_cluster();
@@ -1230,10 +1235,8 @@ __global__ void __launch_bounds__(PB_MAXT, 1) k_rrq_panel_blk(OrderTab T, PanelI
   double* Xr = Xq + 4 * (size_t)PL;           /* [row][col] */
   double* Mq = Xr + (size_t)hr * RS;          /* [row][b][comp] */
   double* Mr = Mq + (size_t)hq * PB_NB * 4;   /* [row][b] */
-  double* fq = Mr + (size_t)hr * PB_NB;       /* pivot column of V, 2 buffers: [buf][comp][row] */
-  double* fr = fq + (size_t)hq * 8;           /* pivot column of MS, 2 buffers */
-  double* cv = fr + (size_t)hr * 2;           /* next-pivot candidates a warp: [buf][V, MS][warp] */
-  int* usedq = (int*)(cv + 4 * 32);
+  double* fq = Mr + (size_t)hr * PB_NB;       /* the step's pivot columns, 2 buffers: [buf][V comp][row], MS */
+  int* usedq = (int*)(fq + 2 * ((size_t)4 * hq + hr + 8));
   int* usedr = usedq + hq;
   int* isPq = usedr + hr; /* rows of the current block's pivots */
   int* isPr = isPq + hq;
@@ -1241,21 +1244,13 @@ __global__ void __launch_bounds__(PB_MAXT, 1) k_rrq_panel_blk(OrderTab T, PanelI
   int* pivr = pivq + hd;
   int* posq = pivr + hd;  /* inverse permutations */
   int* posr = posq + hd;
-  int* pidx = posr + hd;  /* 2: the first step's pivot rows (explicit search) */
-  int* ci = pidx + 2;     /* candidate rows, as cv */
+  int* pidx = posr + hd;  /* the step's pivot rows (V, MS), 2 buffers */
   /* geometry staging aliases the block buffers (free until the first block) */
   double* s_sx = Mq;
   double* s_raw = s_sx + 3 * hd;
   double* s_fr = s_raw + 3 * (nbd + 3);
   panel_frame_setup(T, P, R, chart, pan, rank, s_sx, s_raw, s_fr);
   const double alpha = s_fr[12];
-  double fr9[13];
-#pragma unroll
-  for (int i = 0; i < 13; ++i) fr9[i] = s_fr[i];
-  auto tofr = [&](const double* x, double* y) {
-    double d0 = x[0] - fr9[9], d1 = x[1] - fr9[10], d2 = x[2] - fr9[11];
-    for (int i = 0; i < 3; ++i) y[i] = alpha * (fr9[i] * d0 + fr9[i + 3] * d1 + fr9[i + 6] * d2);
-  };
   /* zero the matrices (padding rows and columns stay zero) and the bookkeeping */
   for (int e = tid; e < 4 * PL + hr * RS; e += NT) Xq[e] = 0.0;
   for (int e = tid; e < hq; e += NT) usedq[e] = e >= hd; /* padding rows never pivot */
@@ -1267,9 +1262,14 @@ __global__ void __launch_bounds__(PB_MAXT, 1) k_rrq_panel_blk(OrderTab T, PanelI
   for (int e = tid; e < hd * L; e += NT) {
     const int j = e / L, m = e % L + 1;
     double y[3], nrm[3];
-    tofr(&s_sx[3 * j], y);
+    {
+      const double d0 = s_sx[3 * j] - s_fr[9], d1 = s_sx[3 * j + 1] - s_fr[10], d2 = s_sx[3 * j + 2] - s_fr[11];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) y[i] = alpha * (s_fr[i] * d0 + s_fr[i + 3] * d1 + s_fr[i + 6] * d2);
+    }
     const double* sn = P.snx + ((size_t)pan * hd + j) * 3;
-    for (int i = 0; i < 3; ++i) nrm[i] = fr9[i] * sn[0] + fr9[i + 3] * sn[1] + fr9[i + 6] * sn[2];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) nrm[i] = s_fr[i] * sn[0] + s_fr[i + 3] * sn[1] + s_fr[i + 6] * sn[2];
     const bool ownj = j >= c0 && j < c0 + ncol;
     harm_column(L, m, y[0], y[1], y[2], [&](int l, int k, double h, double gx, double gy, double gz) {
         if (k >= c0 && k < c0 + ncol) {
@@ -1299,206 +1299,162 @@ __global__ void __launch_bounds__(PB_MAXT, 1) k_rrq_panel_blk(OrderTab T, PanelI
     const int k0 = blk * PB_NB, owner = k0 / ncol, lb0 = k0 - owner * ncol;
     const int nbk = min(PB_NB, hd - k0);
     if (rank == owner) {
-      /* panel phase: the unblocked steps on the block's columns alone, one
-       * barrier a step.  Step j: every thread forms the pivot inverses from
-       * the pivot column (kept in fq/fr) and the scaled pivot row entries it
-       * needs from the pivot row, left unscaled in shared memory until the
-       * next step (whose items scale it first, the deferred scaling), and
-       * eliminates; the items of column j+1 also copy their new entries into
-       * the other fq/fr buffer and propose the next pivot (largest norm among
-       * the unused rows, smallest row on ties: the unblocked rule), reduced a
-       * warp at a time into cv/ci and over the warps by every thread at the
-       * start of the next step.  The first column of the block is searched
-       * explicitly. */
-      for (int e = tid; e < hq; e += NT)
+      /* panel phase: the unblocked steps on the block's 8 columns alone, held
+       * in registers by warps 0..7 (warp c: local block column c of both
+       * systems, lane l: rows l, l + 32, ..).  Step j: warp j picks the pivot
+       * rows of its column (largest norm / magnitude among the unused rows,
+       * smallest row on ties: the unblocked rule), publishes the pivots and its
+       * whole column (the elimination factors) in shared memory (two buffers
+       * by step parity) and one named barrier of the 8 warps later every warp
+       * scales its entry of the pivot rows and eliminates its column. */
+      if (wid < PB_NB) {
+        const int c = wid, lcol = lb0 + c;
+        double xq[PB_MAXS][4], xr[PB_MAXS];
 #pragma unroll
-        for (int c = 0; c < 4; ++c) fq[c * hq + e] = Xq[c * PL + (size_t)e * RS + lb0];
-      for (int e = tid; e < hr; e += NT) fr[e] = Xr[(size_t)e * RS + lb0];
-      if (wid < 2) { /* warp 0: V's pivot, warp 1: MS's pivot */
-        double bv = -1.0;
-        int bi = hd;
-        for (int i = lane; i < hd; i += 32) {
-          double v;
-          if (wid == 0) {
-            if (usedq[i]) continue;
-            const double a0 = Xq[(size_t)i * RS + lb0], a1 = Xq[PL + (size_t)i * RS + lb0];
-            const double a2 = Xq[2 * PL + (size_t)i * RS + lb0], a3 = Xq[3 * PL + (size_t)i * RS + lb0];
-            v = a0 * a0 + a1 * a1 + a2 * a2 + a3 * a3;
-          } else {
-            if (usedr[i]) continue;
-            v = fabs(Xr[(size_t)i * RS + lb0]);
+        for (int sl = 0; sl < PB_MAXS; ++sl) {
+          const int r = lane + 32 * sl;
+#pragma unroll
+          for (int cc = 0; cc < 4; ++cc) xq[sl][cc] = r < hq ? Xq[cc * PL + (size_t)r * RS + lcol] : 0.0;
+          xr[sl] = r < hr ? Xr[(size_t)r * RS + lcol] : 0.0;
+        }
+        /* rows pivoted in earlier blocks, and then in this one: bit masks */
+        unsigned long long uq[3] = {0ull, 0ull, 0ull}, ur[3] = {0ull, 0ull, 0ull};
+        for (int r = lane; r < 192; r += 32) {
+          const bool a1 = r >= hd || usedq[min(r, hq - 1)] != 0, a2 = r >= hd || usedr[min(r, hr - 1)] != 0;
+          const unsigned m1 = __ballot_sync(0xffffffffu, a1), m2 = __ballot_sync(0xffffffffu, a2);
+          const int w64 = (r - lane) >> 6, sh = ((r - lane) & 63);
+#pragma unroll
+          for (int w = 0; w < 3; ++w)
+            if (w64 == w) { uq[w] |= (unsigned long long)m1 << sh; ur[w] |= (unsigned long long)m2 << sh; }
+        }
+#define PB_USED(m, r) ((((r) < 64 ? m[0] : ((r) < 128 ? m[1] : m[2])) >> ((r) & 63)) & 1ull)
+        for (int j = 0; j < nbk; ++j) {
+          double* fb = fq + (size_t)(j & 1) * (4 * hq + hr + 8); /* the step's factors: [comp][row], MS, inverses */
+          if (c == j) {
+            /* pivot rows of this column */
+            double bv = -1.0, bw = -1.0;
+            int bi = hd, bj = hd;
+#pragma unroll
+            for (int sl = 0; sl < PB_MAXS; ++sl) {
+              const int r = lane + 32 * sl;
+              if (r < hd && !PB_USED(uq, r)) {
+                const double v = xq[sl][0] * xq[sl][0] + xq[sl][1] * xq[sl][1] + xq[sl][2] * xq[sl][2] +
+                                 xq[sl][3] * xq[sl][3];
+                if (v > bv) { bv = v; bi = r; }
+              }
+              if (r < hd && !PB_USED(ur, r)) {
+                const double v = fabs(xr[sl]);
+                if (v > bw) { bw = v; bj = r; }
+              }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+              const double v2 = __shfl_xor_sync(0xffffffffu, bv, o);
+              const int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
+              if (v2 > bv || (v2 == bv && i2 < bi)) { bv = v2; bi = i2; }
+              const double w2 = __shfl_xor_sync(0xffffffffu, bw, o);
+              const int j2 = __shfl_xor_sync(0xffffffffu, bj, o);
+              if (w2 > bw || (w2 == bw && j2 < bj)) { bw = w2; bj = j2; }
+            }
+            if (bi >= hd) { /* a NaN column: the first unused row (results NaN, indices in range) */
+              bi = 0;
+              while (bi < hd - 1 && PB_USED(uq, bi)) ++bi;
+            }
+            if (bj >= hd) {
+              bj = 0;
+              while (bj < hd - 1 && PB_USED(ur, bj)) ++bj;
+            }
+#pragma unroll
+            for (int sl = 0; sl < PB_MAXS; ++sl) {
+              const int r = lane + 32 * sl;
+              if (r < hq)
+#pragma unroll
+                for (int cc = 0; cc < 4; ++cc) fb[cc * hq + r] = xq[sl][cc];
+              if (r < hr) fb[4 * hq + r] = xr[sl];
+            }
+            __syncwarp();
+            if (lane == 0) { /* the pivot inverses, once: conj(f)/|f|^2 and 1/f */
+              const double f0 = fb[bi], f1 = fb[hq + bi], f2 = fb[2 * hq + bi], f3 = fb[3 * hq + bi];
+              const double n2i = 1.0 / (f0 * f0 + f1 * f1 + f2 * f2 + f3 * f3);
+              double* pvb = fb + 4 * hq + hr; /* after the step's columns */
+              pvb[0] = f0 * n2i; pvb[1] = -f1 * n2i; pvb[2] = -f2 * n2i; pvb[3] = -f3 * n2i;
+              pvb[4] = 1.0 / fb[4 * hq + bj];
+              pidx[2 * (j & 1)] = bi; pidx[2 * (j & 1) + 1] = bj; pivq[k0 + j] = bi; pivr[k0 + j] = bj;
+            }
           }
-          if (v > bv) { bv = v; bi = i; }
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-          const double b2 = __shfl_xor_sync(0xffffffffu, bv, o);
-          const int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
-          if (b2 > bv || (b2 == bv && i2 < bi)) { bv = b2; bi = i2; }
-        }
-        if (lane == 0) pidx[wid] = bi;
-      }
-      __syncthreads();
-      int pq_prev = -1, pr_prev = -1;
-      double pvq[4] = {0.0, 0.0, 0.0, 0.0}, pvr = 0.0; /* previous step's pivot inverses */
-      for (int j = 0; j < nbk; ++j) {
-        const int cur = j & 1, nxt = cur ^ 1;
-        const double* fqc = fq + (size_t)cur * 4 * hq;
-        double* fqn = fq + (size_t)nxt * 4 * hq;
-        const double* frc = fr + (size_t)cur * hr;
-        double* frn = fr + (size_t)nxt * hr;
-        /* this step's pivot rows */
-        int p, p2;
-        if (j == 0) {
-          p = pidx[0]; p2 = pidx[1];
-        } else {
-          const double* cvb = cv + (size_t)cur * 64; /* written by step j-1 (its "next" buffer) */
-          const int* cib = ci + (size_t)cur * 64;
-          double b1 = -1.0, b2 = -1.0;
-          p = hd; p2 = hd;
-          for (int w = 0; w < NW; ++w) {
-            const double v1 = cvb[w], v2 = cvb[32 + w];
-            const int i1 = cib[w], i2 = cib[32 + w];
-            if (v1 > b1 || (v1 == b1 && i1 < p)) { b1 = v1; p = i1; }
-            if (v2 > b2 || (v2 == b2 && i2 < p2)) { b2 = v2; p2 = i2; }
-          }
-        }
-        /* rows pivoted in earlier steps of this block (usedq/usedr hold earlier
-         * blocks' pivots; this block's are marked after it) */
-        auto blk_q = [&](int i) { for (int jj = 0; jj < j; ++jj) if (pivq[k0 + jj] == i) return true; return false; };
-        auto blk_r = [&](int i) { for (int jj = 0; jj < j; ++jj) if (pivr[k0 + jj] == i) return true; return false; };
-        if (p >= hd) { /* a NaN column: the first unused row (results NaN, indices in range) */
-          p = 0;
-          while (p < hd - 1 && (usedq[p] || blk_q(p))) ++p;
-        }
-        if (p2 >= hd) {
-          p2 = 0;
-          while (p2 < hd - 1 && (usedr[p2] || blk_r(p2))) ++p2;
-        }
-        double pi4[4];
-        {
-          const double f0 = fqc[p], f1 = fqc[hq + p], f2 = fqc[2 * hq + p], f3 = fqc[3 * hq + p];
-          const double n2i = 1.0 / (f0 * f0 + f1 * f1 + f2 * f2 + f3 * f3);
-          pi4[0] = f0 * n2i; pi4[1] = -f1 * n2i; pi4[2] = -f2 * n2i; pi4[3] = -f3 * n2i;
-        }
-        const double rinv = 1.0 / frc[p2];
-        if (tid == 0) pivq[k0 + j] = p; /* read from the next step on */
-        if (tid == 32) pivr[k0 + j] = p2;
-        double bv = -1.0, bw = -1.0;
-        int bi = hd, bj = hd;
-        for (int e = tid; e < hq * PB_NB; e += NT) { /* consecutive threads: consecutive rows */
-          const int i = e % hq, b = e / hq;
-          double* x0 = Xq + (size_t)i * RS + lb0 + b;
-          double x[4];
+          named_bar(1, 32 * PB_NB);
+          const int p = pidx[2 * (j & 1)], p2 = pidx[2 * (j & 1) + 1];
+          const double* pvb = fb + 4 * hq + hr;
+          const double pi4[4] = {pvb[0], pvb[1], pvb[2], pvb[3]};
+          const double rinv = pvb[4];
+          /* this column's entries of the pivot rows, scaled */
+          double rq4[4], rr1;
+          {
+            const int sp = p >> 5, lp = p & 31, sp2 = p2 >> 5, lp2 = p2 & 31;
+            double v[4] = {0.0, 0.0, 0.0, 0.0}, w = 0.0;
 #pragma unroll
-          for (int c = 0; c < 4; ++c) x[c] = x0[c * PL];
-          if (i == pq_prev) { /* the previous pivot row: its deferred scaling */
-            if (b == j - 1) {
+            for (int sl = 0; sl < PB_MAXS; ++sl) {
+              if (sl == sp)
 #pragma unroll
-              for (int c = 0; c < 4; ++c) x[c] = pvq[c];
+                for (int cc = 0; cc < 4; ++cc) v[cc] = xq[sl][cc];
+              if (sl == sp2) w = xr[sl];
+            }
+#pragma unroll
+            for (int cc = 0; cc < 4; ++cc) v[cc] = __shfl_sync(0xffffffffu, v[cc], lp);
+            w = __shfl_sync(0xffffffffu, w, lp2);
+            if (c == j) {
+#pragma unroll
+              for (int cc = 0; cc < 4; ++cc) rq4[cc] = pi4[cc];
+              rr1 = rinv;
             } else {
-              double t[4];
-              qmul(pvq, x, t);
-#pragma unroll
-              for (int c = 0; c < 4; ++c) x[c] = t[c];
+              qmul(pi4, v, rq4);
+              rr1 = rinv * w;
             }
           }
-          if (i == p) { /* this step's pivot row: scaled in the next step; its next-column entry */
-            if (b == j + 1) {
-              double t[4];
-              qmul(pi4, x, t);
+          /* eliminate: row p takes the scaled entry, the others subtract */
 #pragma unroll
-              for (int c = 0; c < 4; ++c) fqn[c * hq + i] = t[c];
+          for (int sl = 0; sl < PB_MAXS; ++sl) {
+            const int r = lane + 32 * sl;
+            if (r < hq) {
+              if (r == p) {
+#pragma unroll
+                for (int cc = 0; cc < 4; ++cc) xq[sl][cc] = rq4[cc];
+              } else {
+                const double f[4] = {fb[r], fb[hq + r], fb[2 * hq + r], fb[3 * hq + r]};
+                double t[4];
+                if (c == j) {
+                  qmul(f, pi4, t);
+#pragma unroll
+                  for (int cc = 0; cc < 4; ++cc) xq[sl][cc] = -t[cc];
+                } else {
+                  qmul(f, rq4, t);
+#pragma unroll
+                  for (int cc = 0; cc < 4; ++cc) xq[sl][cc] -= t[cc];
+                }
+              }
             }
-            continue;
-          }
-          const double f[4] = {fqc[i], fqc[hq + i], fqc[2 * hq + i], fqc[3 * hq + i]};
-          double t[4];
-          if (b == j) {
-            qmul(f, pi4, t);
-#pragma unroll
-            for (int c = 0; c < 4; ++c) x[c] = -t[c];
-          } else {
-            double xp[4], r[4];
-#pragma unroll
-            for (int c = 0; c < 4; ++c) xp[c] = Xq[c * PL + (size_t)p * RS + lb0 + b];
-            qmul(pi4, xp, r); /* the scaled pivot row entry */
-            qmul(f, r, t);
-#pragma unroll
-            for (int c = 0; c < 4; ++c) x[c] -= t[c];
-          }
-#pragma unroll
-          for (int c = 0; c < 4; ++c) x0[c * PL] = x[c];
-          if (b == j + 1) {
-#pragma unroll
-            for (int c = 0; c < 4; ++c) fqn[c * hq + i] = x[c];
-            if (i < hd && !usedq[i] && !blk_q(i)) {
-              const double v = x[0] * x[0] + x[1] * x[1] + x[2] * x[2] + x[3] * x[3];
-              if (v > bv || (v == bv && i < bi)) { bv = v; bi = i; }
+            if (r < hr) {
+              if (r == p2) xr[sl] = rr1;
+              else if (c == j) xr[sl] = -fb[4 * hq + r] * rinv;
+              else xr[sl] -= fb[4 * hq + r] * rr1;
             }
           }
-        }
-        for (int e = tid; e < hr * PB_NB; e += NT) {
-          const int i = e % hr, b = e / hr;
-          double* x0 = Xr + (size_t)i * RS + lb0 + b;
-          double x = *x0;
-          if (i == pr_prev) x = (b == j - 1) ? pvr : pvr * x;
-          if (i == p2) {
-            if (b == j + 1) frn[i] = rinv * x;
-            continue;
-          }
-          if (b == j) x = -frc[i] * rinv;
-          else x -= frc[i] * (rinv * Xr[(size_t)p2 * RS + lb0 + b]);
-          *x0 = x;
-          if (b == j + 1) {
-            frn[i] = x;
-            if (i < hd && !usedr[i] && !blk_r(i)) {
-              const double v = fabs(x);
-              if (v > bw || (v == bw && i < bj)) { bw = v; bj = i; }
-            }
+#pragma unroll
+          for (int w = 0; w < 3; ++w) {
+            if ((p >> 6) == w) uq[w] |= 1ull << (p & 63);
+            if ((p2 >> 6) == w) ur[w] |= 1ull << (p2 & 63);
           }
         }
-        if (j + 1 < nbk) { /* this warp's next-pivot candidates */
-          for (int o = 16; o > 0; o >>= 1) {
-            const double v2 = __shfl_xor_sync(0xffffffffu, bv, o);
-            const int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
-            if (v2 > bv || (v2 == bv && i2 < bi)) { bv = v2; bi = i2; }
-            const double w2 = __shfl_xor_sync(0xffffffffu, bw, o);
-            const int j2 = __shfl_xor_sync(0xffffffffu, bj, o);
-            if (w2 > bw || (w2 == bw && j2 < bj)) { bw = w2; bj = j2; }
-          }
-          if (lane == 0) {
-            cv[(size_t)nxt * 64 + wid] = bv; ci[(size_t)nxt * 64 + wid] = bi;
-            cv[(size_t)nxt * 64 + 32 + wid] = bw; ci[(size_t)nxt * 64 + 32 + wid] = bj;
-          }
+#pragma unroll
+        for (int sl = 0; sl < PB_MAXS; ++sl) {
+          const int r = lane + 32 * sl;
+          if (r < hq)
+#pragma unroll
+            for (int cc = 0; cc < 4; ++cc) Xq[cc * PL + (size_t)r * RS + lcol] = xq[sl][cc];
+          if (r < hr) Xr[(size_t)r * RS + lcol] = xr[sl];
         }
-        __syncthreads();
-        pq_prev = p; pr_prev = p2;
-#pragma unroll
-        for (int c = 0; c < 4; ++c) pvq[c] = pi4[c];
-        pvr = rinv;
-      }
-      /* the last pivot rows' deferred scaling */
-      if (tid < PB_NB) {
-        const int b = tid;
-        double* x0 = Xq + (size_t)pq_prev * RS + lb0 + b;
-        double t[4];
-        if (b == nbk - 1) {
-#pragma unroll
-          for (int c = 0; c < 4; ++c) t[c] = pvq[c];
-        } else {
-          double x[4];
-#pragma unroll
-          for (int c = 0; c < 4; ++c) x[c] = x0[c * PL];
-          qmul(pvq, x, t);
-        }
-#pragma unroll
-        for (int c = 0; c < 4; ++c) x0[c * PL] = t[c];
-      } else if (tid >= 32 && tid < 32 + PB_NB) {
-        const int b = tid - 32;
-        double* x0 = Xr + (size_t)pr_prev * RS + lb0 + b;
-        *x0 = (b == nbk - 1) ? pvr : pvr * *x0;
       }
       __syncthreads();
+#undef PB_USED
       /* publish the block and its pivot rows to every CTA of the cluster */
       for (int e = tid; e < hq * PB_NB * 4; e += NT) {
         const int c = e & 3, b = (e >> 2) & 7, i = e >> 5;
@@ -2461,7 +2417,7 @@ cudaError_t qol_launch_scan(int npan, int lev, const int* cnt, long long* off, c
 static int pblk_cluster_sizes(int hd, int* out) {
   int n = 0;
   for (int cs : {1, 2, 4, 8}) {
-    if (pblk_ncol(hd, cs) > 72 || pblk_smem_bytes(hd, cs) > 227 * 1024) continue;
+    if (pblk_ncol(hd, cs) > 64 || pblk_smem_bytes(hd, cs) > 227 * 1024) continue;
     if (cs > 1 && pblk_ncol(hd, cs) * (cs - 1) >= hd) continue; /* every CTA owns a valid column */
     out[n++] = cs;
   }
@@ -2501,11 +2457,12 @@ cudaError_t qol_launch_rrq_panel(const OrderTab& T, const PanelIn& P, const Pair
     cfg.numAttrs = 1;
     return cudaLaunchKernelEx(&cfg, kern, T, P, G, R, chart);
   };
+  const bool wide = pblk_hq(T.hd) > 96;
   switch (cs) {
-    case 1: return go(k_rrq_panel_blk<1>);
-    case 2: return go(k_rrq_panel_blk<2>);
-    case 4: return go(k_rrq_panel_blk<4>);
-    default: return go(k_rrq_panel_blk<8>);
+    case 1: return wide ? go(k_rrq_panel_blk<1, 5>) : go(k_rrq_panel_blk<1, 3>);
+    case 2: return wide ? go(k_rrq_panel_blk<2, 5>) : go(k_rrq_panel_blk<2, 3>);
+    case 4: return wide ? go(k_rrq_panel_blk<4, 5>) : go(k_rrq_panel_blk<4, 3>);
+    default: return wide ? go(k_rrq_panel_blk<8, 5>) : go(k_rrq_panel_blk<8, 3>);
   }
 }
 int qol_panel_shapes(int hd, int nquad, int* cs, int* nt, int cap) {
