@@ -436,27 +436,54 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_sample(W, budget_s=15.0, nthreads=0):
-    """The oracle (CPU restatement, OpenMP over panels) on a bounded sample of
-    the same workload: leading panels until about budget_s of work."""
+CPU_SAMPLE_PANELS = 256  # the CPU legs' sample: the workload's leading 256 panels (1/10 of it)
+
+
+def cpu_sample(W, panels=CPU_SAMPLE_PANELS, nthreads=0):
+    """The oracle (CPU restatement of the reference's algorithm, OpenMP over
+    panels, kernel-matrix sums with AVX2: the reference's isimd = 256 path) on
+    the leading `panels` panels of the same workload, one timed call.
+    Returns (pairs, seconds, panels)."""
     import oracle
     if not os.path.exists(os.path.join(ROOT, "oracle", "liborc.so")):
         oracle.build()
     hd = W["hd"]
-    tot_pairs, tot_t, k0, chunk = 0, 0.0, 0, 4
-    while tot_t < budget_s and k0 < W["npan"]:
-        k1 = min(W["npan"], k0 + chunk)
-        lo, hi = W["tcxi"][k0] - 1, W["tcxi"][k1] - 1
-        xi = W["tcxi"][k0:k1 + 1] - lo
-        sl = slice(k0 * hd, k1 * hd)
+    k1 = min(W["npan"], panels)
+    hi = W["tcxi"][k1] - 1
+    sl = slice(0, k1 * hd)
+    oracle.set_simd(256)
+    try:
         t0 = time.perf_counter()
-        oracle.getnearquad(k1 - k0, W["nterms"], W["nquad"], W["sx"][sl], W["snx"][sl], W["sw"][sl], W["rts"][sl],
-                           W["rps"][sl], W["tcx"][lo:hi], W["tcxrow"][lo:hi], xi, W["nquad"], nthreads=nthreads)
-        tot_t += time.perf_counter() - t0
-        tot_pairs += int(hi - lo)
-        k0 = k1
-        chunk *= 2
-    return tot_pairs, tot_t, k0
+        oracle.getnearquad(k1, W["nterms"], W["nquad"], W["sx"][sl], W["snx"][sl], W["sw"][sl], W["rts"][sl],
+                           W["rps"][sl], W["tcx"][:hi], W["tcxrow"][:hi], W["tcxi"][:k1 + 1], W["nquad"],
+                           nthreads=nthreads)
+        t = time.perf_counter() - t0
+    finally:
+        oracle.set_simd(0)
+    return int(hi), t, k1
+
+
+def cpu_config0_one_thread():
+    """The CPU configuration of the benchmark set: plain RRQ on the torus
+    R = 2 + cos p, Z = sin p, 6 x 12 quads (144 triangles), order 4 (15 nodes a
+    triangle, 2160 nodes), SLP + DLP near corrections for every on-surface
+    node, one thread, isimd = 256.  Returns (pairs/s, pairs, seconds)."""
+    import oracle
+    from qotential_b200 import geometry as G
+    nterms = 5
+    hd = nterms * (nterms + 1) // 2
+    P = G.panels(G.torus(), 6, 12, nterms, split=False)
+    tcxi, tcxrow, tcx = G.near_lists(P["sx"], P["sw"], hd)
+    npan = P["sw"].size // hd
+    oracle.set_simd(256)
+    try:
+        t0 = time.perf_counter()
+        oracle.getnearquad(npan, nterms, nterms + 2, P["sx"], P["snx"], P["sw"], P["rts"], P["rps"], tcx, tcxrow,
+                           tcxi, nterms + 2, nthreads=1)
+        t = time.perf_counter() - t0
+    finally:
+        oracle.set_simd(0)
+    return tcxrow.size / t, int(tcxrow.size), t
 
 
 def run_reference(args):
@@ -470,7 +497,7 @@ def run_reference(args):
     per_step = []
     pairs_step = None
     for s in range(args.warmup + args.steps):
-        p, t, k = cpu_sample(W, budget_s=6.0, nthreads=nthr)
+        p, t, k = cpu_sample(W, nthreads=nthr)
         if s >= args.warmup:
             per_step.append((p, t))
             pairs_step = p
@@ -481,9 +508,10 @@ def run_reference(args):
             "warmup": args.warmup, "ms_per_step": 1e3 * t / max(1, args.steps), "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
             "config": config_dict(W, 1),
-            "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": nthr, "kind": "port",
-                             "sample": f"{pairs_step} near pairs (leading panels, ~6 s of CPU work) per step, "
-                                       f"OpenMP over panels on {nthr} threads"},
+            "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": nthr, "kind": "port", "isimd": 256,
+                             "sample": f"{pairs_step} near pairs per step: the leading {CPU_SAMPLE_PANELS} of "
+                                       f"{W['npan']} panels of the workload, oracle (C++ restatement, OpenMP over "
+                                       f"panels, AVX2 kernel sums) on {nthr} threads"},
             "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -668,10 +696,15 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         nthr = os.cpu_count() or 1
-        p, tcpu, kk = cpu_sample(W, budget_s=15.0, nthreads=nthr)
-        cpu = {"value": p / tcpu, "unit": "pairs/s", "cores": nthr, "kind": "port",
-               "sample": f"{p} near pairs of the leading {kk} panels of the same workload, oracle (C++ restatement, "
-                         f"OpenMP over panels) on {nthr} threads, {tcpu:.1f} s"}
+        p, tcpu, kk = cpu_sample(W, nthreads=nthr)
+        c0v, c0p, c0t = cpu_config0_one_thread()
+        cpu = {"value": p / tcpu, "unit": "pairs/s", "cores": nthr, "kind": "port", "isimd": 256,
+               "sample": f"{p} near pairs of the leading {kk} of {W['npan']} panels of the same workload (the "
+                         f"reference arm's sample), oracle (C++ restatement, OpenMP over panels, AVX2 kernel sums) "
+                         f"on {nthr} threads, {tcpu:.1f} s",
+               "config0_one_thread": {"value": c0v, "unit": "pairs/s", "pairs": c0p, "seconds": c0t,
+                                      "workload": "torus 6x12 quads (144 triangles), order 4, 2160 on-surface "
+                                                  "targets, 1 thread, isimd 256"}}
     if rank == 0:
         line = {"metric": "near-pair evals/s", "value": value, "unit": "pairs/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,

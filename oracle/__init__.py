@@ -52,6 +52,12 @@ def _i64(a):
     return np.ascontiguousarray(a, dtype=np.int64)
 
 
+def set_simd(isimd):
+    """Kernel-matrix sums with AVX2 over 4 targets (isimd = 256, the
+    reference's SIMD path) or scalar (0); both give the same results."""
+    lib().orc_set_simd(C.c_int(int(isimd)))
+
+
 def gauss(n):
     x = np.zeros(n); w = np.zeros(n); D = np.zeros((n, n))
     lib().orc_gauss(C.c_int(n), _vp(x), _vp(w), _vp(D))

@@ -50,6 +50,8 @@ int orc_rrq_panel_systems(int nterms, const double* sx, const double* snx, const
   return 0;
 }
 int orc_set_flags(int f) { orc::g_orc_flags = f; return 0; }
+/* isimd for the kernel-matrix sums: 0 scalar, 256 AVX2 (same results) */
+int orc_set_simd(int isimd) { orc::g_orc_simd = isimd == 256 ? 256 : 0; return 0; }
 
 int orc_vr_nodes_export(int deg, double* uv, double* w) {
   vr_nodes(deg, uv, w);

@@ -55,6 +55,7 @@ void interp_matrix(int korder, int n, const double* uv, double* M);
 struct RefLevel {
   i8 n = 0, nsub = 0;
   std::vector<double> uv, wt, interp; /* interp n x npols col-major */
+  std::vector<double> interp_t;       /* the same, row-major (npols per node: the contraction's order) */
   std::vector<i8> suboff, subtyp;
 };
 struct RefElem {
@@ -99,6 +100,10 @@ void rrq(const RRQConfig& cfg, i8 m, const double* tx, const double* sx,
          const double* sxbd_chart, const double* rv_chart, double* As, double* Ad,
          double* Omega, double* Ialpha, i8* level_of);
 
+/* kernel-matrix evaluation: 0 scalar, 256 AVX2 over 4 targets (the
+ * reference's isimd = 256 path, src/patch_refine_mod.f90:575-591); both give
+ * the same bits */
+extern int g_orc_simd;
 /* experiment switches, 0 in normal use (test hook) */
 extern int g_orc_flags;
 void panel_systems(const RRQConfig& cfg, const double* sx, const double* snx, const double* sw, double* DT,

@@ -2,6 +2,9 @@
  * per-panel refined levels and the level-resolved direct SLP/DLP sums.
  * TEST INFRASTRUCTURE ONLY (see orc_common.h). */
 #include "orc_common.h"
+#ifdef __AVX2__
+#include <immintrin.h>
+#endif
 #include "vr_table.h"
 #include <algorithm>
 #include <cfloat>
@@ -365,6 +368,9 @@ void build_ref(int korder, int order, int nlevel, bool sqmode, RefElem& R) {
     }
     L.interp.assign((size_t)L.n * npols, 0.0);
     interp_matrix(korder, (int)L.n, L.uv.data(), L.interp.data());
+    L.interp_t.assign((size_t)L.n * npols, 0.0);
+    for (i8 q = 0; q < L.n; ++q)
+      for (int k = 0; k < npols; ++k) L.interp_t[(size_t)q * npols + k] = L.interp[q + (size_t)L.n * k];
   }
 }
 
@@ -428,8 +434,57 @@ void build_panel_levels(const RefElem& R, const double* sx, const double* rts,
   }
 }
 
+int g_orc_simd = 0;
+
+#ifdef __AVX2__
+/* isimd = 256: four targets a lane group, the scalar formula's operations in
+ * the same order (separate multiplies and adds, IEEE sqrt and division), so
+ * the same bits */
+static void sdlpmat_avx2(i8 m, const double* tx, i8 n, const double* sx, const double* snx, const double* sw,
+                         double* A, double* B) {
+  const double pi4inv = 1.0 / (4.0 * PI);
+  const i8 m4 = m & ~(i8)3;
+  std::vector<double> xs(m), ys(m), zs(m);
+  for (i8 i = 0; i < m; ++i) { xs[i] = tx[3 * i]; ys[i] = tx[3 * i + 1]; zs[i] = tx[3 * i + 2]; }
+  const __m256d tiny = _mm256_set1_pd(1.0e-28), zero = _mm256_setzero_pd();
+  for (i8 j = 0; j < n; ++j) {
+    const double w4 = sw[j] * pi4inv;
+    const __m256d vw = _mm256_set1_pd(w4), sxj = _mm256_set1_pd(sx[3 * j]), syj = _mm256_set1_pd(sx[3 * j + 1]),
+                  szj = _mm256_set1_pd(sx[3 * j + 2]), nxj = _mm256_set1_pd(snx[3 * j]),
+                  nyj = _mm256_set1_pd(snx[3 * j + 1]), nzj = _mm256_set1_pd(snx[3 * j + 2]);
+    for (i8 i = 0; i < m4; i += 4) {
+      const __m256d dx = _mm256_sub_pd(_mm256_loadu_pd(&xs[i]), sxj), dy = _mm256_sub_pd(_mm256_loadu_pd(&ys[i]), syj),
+                    dz = _mm256_sub_pd(_mm256_loadu_pd(&zs[i]), szj);
+      const __m256d rr = _mm256_add_pd(_mm256_add_pd(_mm256_mul_pd(dx, dx), _mm256_mul_pd(dy, dy)), _mm256_mul_pd(dz, dz));
+      const __m256d ok = _mm256_cmp_pd(rr, tiny, _CMP_GT_OQ);
+      const __m256d r = _mm256_sqrt_pd(rr);
+      if (A) _mm256_storeu_pd(&A[i + m * j], _mm256_blendv_pd(zero, _mm256_div_pd(vw, r), ok));
+      if (B) {
+        const __m256d dn = _mm256_add_pd(_mm256_add_pd(_mm256_mul_pd(dx, nxj), _mm256_mul_pd(dy, nyj)), _mm256_mul_pd(dz, nzj));
+        _mm256_storeu_pd(&B[i + m * j], _mm256_blendv_pd(zero, _mm256_div_pd(_mm256_mul_pd(vw, dn), _mm256_mul_pd(r, rr)), ok));
+      }
+    }
+    for (i8 i = m4; i < m; ++i) {
+      double dx = xs[i] - sx[3 * j], dy = ys[i] - sx[3 * j + 1], dz = zs[i] - sx[3 * j + 2];
+      double rr = dx * dx + dy * dy + dz * dz;
+      if (rr > 1.0e-28) {
+        double r = std::sqrt(rr);
+        if (A) A[i + m * j] = w4 / r;
+        if (B) B[i + m * j] = w4 * (dx * snx[3 * j] + dy * snx[3 * j + 1] + dz * snx[3 * j + 2]) / (r * rr);
+      } else {
+        if (A) A[i + m * j] = 0.0;
+        if (B) B[i + m * j] = 0.0;
+      }
+    }
+  }
+}
+#endif
+
 void sdlpmat(i8 m, const double* tx, i8 n, const double* sx, const double* snx,
              const double* sw, double* A, double* B) {
+#ifdef __AVX2__
+  if (g_orc_simd == 256) { sdlpmat_avx2(m, tx, n, sx, snx, sw, A, B); return; }
+#endif
   const double pi4inv = 1.0 / (4.0 * PI);
   for (i8 j = 0; j < n; ++j) {
     double w4 = sw[j] * pi4inv;
@@ -476,18 +531,21 @@ void sdlpmat_levels(const RefElem& R, const std::vector<PanelLevel>& lv, i8 m,
       for (i8 i = 0; i < nbat; ++i)
         for (int d = 0; d < 3; ++d) txb[3 * i + d] = tx[3 * ibat[i] + d];
       sdlpmat(nbat, txb.data(), nl, P.sx.data(), P.snx.data(), P.sw.data(), Ab.data(), Bb.data());
-      const double* I = R.lev[il].interp.data();
+      /* contraction with interpmat (the reference's dgemm), each output
+       * summed over the level nodes in node order; the loop over the hd
+       * outputs innermost (contiguous, vectorisable) */
+      const double* It = R.lev[il].interp_t.data();
+      std::vector<double> ss(np), sd(np);
       for (i8 i = 0; i < nbat; ++i) {
         i8 t = ibat[i];
-        for (int k = 0; k < np; ++k) {
-          double ss = 0.0, sd = 0.0;
-          const double* Ik = I + (size_t)k * nl;
-          for (i8 q = 0; q < nl; ++q) {
-            ss += Ab[i + nbat * q] * Ik[q];
-            sd += Bb[i + nbat * q] * Ik[q];
-          }
-          As[t + m * k] = ss; Ad[t + m * k] = sd;
+        std::fill(ss.begin(), ss.end(), 0.0);
+        std::fill(sd.begin(), sd.end(), 0.0);
+        for (i8 q = 0; q < nl; ++q) {
+          const double a = Ab[i + nbat * q], b = Bb[i + nbat * q];
+          const double* Iq = It + (size_t)q * np;
+          for (int k = 0; k < np; ++k) { ss[k] += a * Iq[k]; sd[k] += b * Iq[k]; }
         }
+        for (int k = 0; k < np; ++k) { As[t + m * k] = ss[k]; Ad[t + m * k] = sd[k]; }
         if (level_of) level_of[t] = il + 1;
       }
     }

@@ -95,7 +95,7 @@ Arena g_arena, g_arena2, g_arena_io, g_arena_grf; /* pipeline, per-pair RRQ stor
 /* per-phase device milliseconds of the pipeline (diagnostics) */
 int g_ktime_on = 0;
 int g_sum_precision = 0; /* 0 FP64 (the drop-in), 1 FP32 level sums */
-int g_autotune = 1;      /* measure k_rrq_panel's shape once per order */
+int g_autotune = 1;      /* measure the panel kernel's cluster size once per order */
 /* learned level selector: off (0) or on (1), its BF16-rounded weights on the
  * device, the confidence threshold, and the decision counters of the calls */
 int g_sel_mode = 0;
@@ -389,10 +389,11 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
   R.side = g_arena2.take<signed char>((size_t)std::max<long long>(nrrq, 1));
   OutCOO O{};
   O.vs = J.vs; O.vd = J.vd; O.omega = J.omega; O.subtract_naive = J.subtract_naive;
-  /* k_rrq_panel's (cluster, threads) shape, measured once per order on the
-   * first call with enough panels: each shape on the first 512 panels, one
-   * warm-up and one timed launch; every shape gives the same results, the
-   * fastest is kept with the order's tables */
+  /* the panel kernel's (cluster size, threads) shape, measured once per order
+   * on the first call with enough panels: each shape on the first 512 panels,
+   * one warm-up and one timed launch; every shape gives the same results
+   * (the same arithmetic split over more or fewer CTAs), the fastest is kept
+   * with the order's tables */
   if (nrrq > 0 && g_autotune && !C->T.panel_cs && npan >= 256) {
     int cs[8], nt[8];
     const int ns = qol_panel_shapes(hd, nq, cs, nt, 8);

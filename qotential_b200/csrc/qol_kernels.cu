@@ -6,9 +6,10 @@
  *   k_direct         level kernel sums fused with the interpmat contraction
  *                    (:553-600) and the naive-block subtraction of
  *                    getnearquad_lap_rrq_r64 (lap3d_close_mod.f90:935-956)
- *   k_rrq_panel      per-panel RRQ precompute (lap3d_close_mod.f90:472-620,
+ *   k_rrq_panel_blk  per-panel RRQ precompute (lap3d_close_mod.f90:472-620,
  *                    843-863): frame, boundary, harmonic basis, inverse of the
- *                    quaternion system and of the S system
+ *                    quaternion system and of the S system (blocked
+ *                    Gauss-Jordan, trailing updates on the FP64 tensor path)
  *   k_rrq_geom       per-pair SSQ weights, string direction, solid angle,
  *                    boundary weights (:789-832), one warp per pair
  *   k_rrq_moments    per-pair harmonic moments (:832-841) by solid-harmonic
@@ -720,22 +721,7 @@ __device__ __forceinline__ void qmul(const double* a, const double* b, double* c
   c[3] = a[0] * b[3] + a[1] * b[2] - a[2] * b[1] + a[3] * b[0];
 }
 
-/* matrix columns per CTA and rows per thread of k_rrq_panel for a cluster
- * of CS CTAs of NT threads */
-__host__ __device__ constexpr int panel_ncol(int hd, int CS) { return (hd + CS - 1) / CS; }
-__host__ __device__ constexpr int panel_maxr(int hd, int CS, int NT) {
-  return (hd + NT / panel_ncol(hd, CS) - 1) / (NT / panel_ncol(hd, CS));
-}
-/* doubles of shared memory of one CTA: setup copies of the matrix columns,
- * staging buffers, geometry, pivot bookkeeping, the scaled pivot rows */
-__host__ __device__ constexpr size_t panel_smem_doubles(int hd, int nbd, int CS) {
-  return (size_t)4 * hd * panel_ncol(hd, CS) + (((size_t)hd * panel_ncol(hd, CS) + 1) & ~(size_t)1) +
-         2 * (((size_t)5 * hd + 1) & ~(size_t)1) + 3 * (size_t)hd + 3 * (size_t)(nbd + 3) + 16 +
-         5 * (size_t)panel_ncol(hd, CS) + 8 + (8 * (size_t)hd + 1) / 2 + 2;
-}
-
-/* per-panel RRQ frame and boundary (shared by the panel kernels; every thread
- * of the CTA calls it): the panel's nodes into s_sx, the boundary and vertices
+/* per-panel RRQ frame and boundary (every thread of the CTA calls it): the panel's nodes into s_sx, the boundary and vertices
  * from the interpolant (or the caller's chart) into s_raw, the frame
  * (R, c, alpha: lap3d_close_mod.f90:503-509, alpha = 1.25/sqrt(2 sum sw)
  * :709) into s_fr; rank 0 of the cluster writes the per-panel outputs (frame,
@@ -913,278 +899,32 @@ __device__ void panel_b_epilogue(const RRQWS& R, int hd, int pan, int c0, int nc
   }
 }
 
-/* per-panel RRQ precompute, one thread-block cluster of CS CTAs per panel.
- * The quaternion matrix V (hd x hd, V[j][k] = (0, grad h_k(y_j))) and the real
- * Msl^T (MS[k][j] = n_j . grad h_k(y_j)) are split by columns over the CTAs;
- * each thread keeps one column's entries of up to MAXR rows in registers.
- * Both are inverted in place by Gauss-Jordan with implicit row pivoting
- * (quaternion pivot by norm; no row moves): step k reads column k from the
- * staging buffer its owner pushed into every CTA through distributed shared
- * memory, picks the largest unused row p, scales row p and eliminates every
- * other row; the owner of column k+1 pushes it as it is updated; one cluster
- * barrier ends the step.  With pi the pivot sequence the inverse is
- * X^-1[k][c] = X[pi(k)][pi^-1(c)]. */
-template <int CS, int NT, int MAXR>
-__global__ void __launch_bounds__(NT, 1) k_rrq_panel(OrderTab T, PanelIn P, PairWS G, RRQWS R,
-                                                                const double* chart /* nullable */) {
-  cg::cluster_group cl = cg::this_cluster();
-  const int rank = (int)cl.block_rank();
-  const int pan = R.plo + (int)(blockIdx.x / CS); /* panels R.plo .. R.plo + gridDim.x / CS - 1 */
-  if (G.cnt[(size_t)pan * 8 + T.nlevel + 1] == 0 && !R.all_panels) return; /* whole cluster */
-  const int hd = T.hd, nq = T.nquad, nbd = 3 * nq, L = T.nterms;
-  const int ncol = panel_ncol(hd, CS), c0 = min(hd, rank * ncol), c1 = min(hd, c0 + ncol), nc = c1 - c0;
-  const int RG = NT / ncol, tc = threadIdx.x % ncol, trg = threadIdx.x / ncol;
-  const bool tact = trg < RG && tc < nc;
-  const int gc = c0 + tc; /* this thread's column */
-  extern __shared__ __align__(16) double psm[];
-  double* Vs = psm;                        /* hd x ncol quaternions (setup) */
-  double* Ms = Vs + (size_t)4 * hd * ncol; /* hd x ncol (setup) */
-  const int SB = (5 * hd + 1) & ~1;       /* staging buffer stride (even: double2 copies) */
-  double* stg = Ms + (((size_t)hd * ncol + 1) & ~(size_t)1); /* 2 buffers x (4 hd quaternion column + hd real column) */
-  double* s_sx = stg + 2 * SB;             /* 3 hd */
-  double* s_raw = s_sx + 3 * hd;           /* 3 (nbd + 3) */
-  double* s_fr = s_raw + 3 * (nbd + 3);    /* 16 */
-  double* rowq = s_fr + 16;                /* 4 ncol: scaled pivot row of V */
-  double* rowr = rowq + 4 * ncol;          /* ncol: scaled pivot row of MS */
-  int* s_piv = (int*)(rowr + ncol + 8);   /* 2 hd: pivot rows of V, of MS (after the 8 pivot values) */
-  int* s_pos = s_piv + 2 * hd;             /* 2 hd: inverse permutations */
-  int* s_used = s_pos + 2 * hd;            /* 2 hd */
-  int* s_pad = s_used + 2 * hd;            /* 2 hd (alignment slack) */
-  (void)s_pad;
-  double* stgr[CS];
-#pragma unroll
-  for (int r = 0; r < CS; ++r) stgr[r] = cl.map_shared_rank(stg, r);
-  auto pushq = [&](int buf, int row, const double* q) {
-#pragma unroll
-    for (int r = 0; r < CS; ++r) {
-      double* d = stgr[r] + buf * SB + 4 * row;
-      d[0] = q[0]; d[1] = q[1]; d[2] = q[2]; d[3] = q[3];
-    }
-  };
-  auto pushr = [&](int buf, int row, double v) {
-#pragma unroll
-    for (int r = 0; r < CS; ++r) stgr[r][buf * SB + 4 * hd + row] = v;
-  };
-  double* H = R.hmat + (size_t)pan * hd * hd; /* H[j*hd+k] = h_k(y_j) */
-  for (int e = threadIdx.x; e < 2 * hd; e += blockDim.x) s_used[e] = 0;
-  panel_frame_setup(T, P, R, chart, pan, rank, s_sx, s_raw, s_fr);
-  const double alpha = s_fr[12];
-  auto tofr = [&](const double* x, double* y) {
-    double d0 = x[0] - s_fr[9], d1 = x[1] - s_fr[10], d2 = x[2] - s_fr[11];
-    for (int i = 0; i < 3; ++i) y[i] = alpha * (s_fr[i] * d0 + s_fr[i + 3] * d1 + s_fr[i + 6] * d2);
-  };
-  /* basis at the nodes: this CTA's columns of V (harmonics c0..c1) and of
-   * Msl^T (nodes c0..c1), and H rows of its nodes */
-  for (int e = threadIdx.x; e < hd * L; e += blockDim.x) { /* (node j, order m) items: distinct entries */
-    const int j = e / L, m = e % L + 1;
-    double y[3], nrm[3];
-    tofr(&s_sx[3 * j], y);
-    const double* sn = P.snx + ((size_t)pan * hd + j) * 3;
-    for (int i = 0; i < 3; ++i) nrm[i] = s_fr[i] * sn[0] + s_fr[i + 3] * sn[1] + s_fr[i + 6] * sn[2];
-    const bool ownj = j >= c0 && j < c1;
-    harm_column(L, m, y[0], y[1], y[2], [&](int l, int k, double h, double gx, double gy, double gz) {
-        if (k >= c0 && k < c1) {
-          double* q = Vs + ((size_t)j * ncol + (k - c0)) * 4;
-          q[0] = 0.0; q[1] = gx; q[2] = gy; q[3] = gz;
-        }
-        if (ownj) {
-          Ms[(size_t)k * ncol + (j - c0)] = nrm[0] * gx + nrm[1] * gy + nrm[2] * gz;
-          H[(size_t)j * hd + k] = h;
-        }
-      });
-  }
-  __syncthreads();
-  /* this thread's entries into registers */
-  double q[MAXR][4], mv[MAXR];
-#pragma unroll
-  for (int r = 0; r < MAXR; ++r) {
-    const int i = trg + RG * r;
-    const bool own = tact && i < hd;
-    for (int c = 0; c < 4; ++c) q[r][c] = own ? Vs[((size_t)i * ncol + tc) * 4 + c] : 0.0;
-    mv[r] = own ? Ms[(size_t)i * ncol + tc] : 0.0;
-    if (own && gc == 0) { pushq(0, i, q[r]); pushr(0, i, mv[r]); }
-  }
-  cl.sync();
-  double* s_pv = rowr + ncol; /* 8: pivot inverse (4), real pivot inverse, pivot rows (as doubles) */
-  for (int k = 0; k < hd; ++k) {
-    const int b = k & 1;
-    double* cq = stg + b * SB;
-    double* cr = cq + 4 * hd;
-    /* warp 0: pivots among the unused rows, their inverses; the pivot rows'
-     * multipliers in this CTA's staging copy become 0 (the elimination then
-     * leaves the pivot rows alone) */
-    if (threadIdx.x < 32) {
-      double bv = -1.0, bw = -1.0;
-      int bi = hd, bj = hd;
-      for (int i = threadIdx.x; i < hd; i += 32) {
-        if (!s_used[i]) {
-          const double* f = cq + 4 * i;
-          const double v = f[0] * f[0] + f[1] * f[1] + f[2] * f[2] + f[3] * f[3];
-          if (v > bv) { bv = v; bi = i; }
-        }
-        if (!s_used[hd + i]) {
-          const double w = fabs(cr[i]);
-          if (w > bw) { bw = w; bj = i; }
-        }
-      }
-      for (int o = 16; o > 0; o >>= 1) {
-        const double a2 = __shfl_xor_sync(0xffffffffu, bv, o);
-        const int ia = __shfl_xor_sync(0xffffffffu, bi, o);
-        if (a2 > bv || (a2 == bv && ia < bi)) { bv = a2; bi = ia; }
-        const double b2 = __shfl_xor_sync(0xffffffffu, bw, o);
-        const int ib = __shfl_xor_sync(0xffffffffu, bj, o);
-        if (b2 > bw || (b2 == bw && ib < bj)) { bw = b2; bj = ib; }
-      }
-      if (threadIdx.x == 0) {
-        int p = bi, p2 = bj;
-        if (p >= hd || p2 >= hd) { /* a NaN column: the first unused rows (results NaN, indices in range) */
-          int f1 = 0, f2 = 0;
-          while (f1 < hd - 1 && s_used[f1]) ++f1;
-          while (f2 < hd - 1 && s_used[hd + f2]) ++f2;
-          if (p >= hd) p = f1;
-          if (p2 >= hd) p2 = f2;
-        }
-        double* f = cq + 4 * p;
-        const double n2i = 1.0 / (f[0] * f[0] + f[1] * f[1] + f[2] * f[2] + f[3] * f[3]);
-        s_pv[0] = f[0] * n2i; s_pv[1] = -f[1] * n2i; s_pv[2] = -f[2] * n2i; s_pv[3] = -f[3] * n2i;
-        s_pv[4] = 1.0 / cr[p2];
-        f[0] = 0.0; f[1] = 0.0; f[2] = 0.0; f[3] = 0.0;
-        cr[p2] = 0.0;
-        s_used[p] = 1; s_used[hd + p2] = 1;
-        s_piv[k] = p; s_piv[hd + k] = p2;
-      }
-    }
-    __syncthreads();
-    const int p = s_piv[k], p2 = s_piv[hd + k];
-    const double pinv[4] = {s_pv[0], s_pv[1], s_pv[2], s_pv[3]};
-    const double rinv = s_pv[4];
-    /* the pivot rows' owners scale and publish them; the owners of column k
-     * clear their other rows (the elimination then gives -f pinv) */
-    if (tact) {
-      if (trg == p % RG) {
-        const int rp = p / RG;
-#pragma unroll
-        for (int r = 0; r < MAXR; ++r)
-          if (r == rp) {
-            double t[4];
-            if (gc == k) { t[0] = pinv[0]; t[1] = pinv[1]; t[2] = pinv[2]; t[3] = pinv[3]; }
-            else qmul(pinv, q[r], t);
-            for (int c = 0; c < 4; ++c) { q[r][c] = t[c]; rowq[4 * tc + c] = t[c]; }
-          }
-      }
-      if (trg == p2 % RG) {
-        const int rp = p2 / RG;
-#pragma unroll
-        for (int r = 0; r < MAXR; ++r)
-          if (r == rp) {
-            const double t = (gc == k) ? rinv : rinv * mv[r];
-            mv[r] = t;
-            rowr[tc] = t;
-          }
-      }
-      if (gc == k) {
-#pragma unroll
-        for (int r = 0; r < MAXR; ++r) {
-          const int i = trg + RG * r;
-          if (i != p) { q[r][0] = 0.0; q[r][1] = 0.0; q[r][2] = 0.0; q[r][3] = 0.0; }
-          if (i != p2) mv[r] = 0.0;
-        }
-      }
-    }
-    __syncthreads();
-    if (tact) {
-      const double r0 = rowq[4 * tc], r1 = rowq[4 * tc + 1], r2 = rowq[4 * tc + 2], r3 = rowq[4 * tc + 3];
-      const double rr = rowr[tc];
-#pragma unroll
-      for (int r = 0; r < MAXR; ++r) {
-        const int i = min(trg + RG * r, hd - 1); /* rows past hd: harmless repeats, never stored */
-        const double* f = cq + 4 * i;
-        const double f0 = f[0], f1 = f[1], f2 = f[2], f3 = f[3];
-        /* q -= f * row (quaternion product) */
-        q[r][0] -= f0 * r0 - f1 * r1 - f2 * r2 - f3 * r3;
-        q[r][1] -= f0 * r1 + f1 * r0 + f2 * r3 - f3 * r2;
-        q[r][2] -= f0 * r2 - f1 * r3 + f2 * r0 + f3 * r1;
-        q[r][3] -= f0 * r3 + f1 * r2 - f2 * r1 + f3 * r0;
-        mv[r] -= cr[i] * rr;
-      }
-      if (gc == k + 1) { /* the next pivot column, into this CTA's other staging buffer */
-        double* nb = stg + (b ^ 1) * SB;
-#pragma unroll
-        for (int r = 0; r < MAXR; ++r) {
-          const int i = trg + RG * r;
-          if (i < hd) {
-            nb[4 * i] = q[r][0]; nb[4 * i + 1] = q[r][1]; nb[4 * i + 2] = q[r][2]; nb[4 * i + 3] = q[r][3];
-            nb[4 * hd + i] = mv[r];
-          }
-        }
-      }
-    }
-    if (CS > 1 && k + 1 < hd) { /* and from there to the other CTAs, coalesced */
-      __syncthreads();
-      if ((k + 1) / ncol == rank) {
-        const double2* src = reinterpret_cast<const double2*>(stg + (b ^ 1) * SB);
-        const int nv = SB / 2;
-        for (int e = threadIdx.x; e < (CS - 1) * nv; e += NT) {
-          const int pr = e / nv, v = e % nv;
-          const int peer = pr < rank ? pr : pr + 1;
-          reinterpret_cast<double2*>(stgr[peer] + (b ^ 1) * SB)[v] = src[v];
-        }
-      }
-    }
-    cl.sync();
-  }
-  /* inverse positions of the pivot sequences */
-  for (int k = threadIdx.x; k < hd; k += blockDim.x) { s_pos[s_piv[k]] = k; s_pos[hd + s_piv[hd + k]] = k; }
-  __syncthreads();
-  /* X^-1[k][c] = X[pi(k)][pi^-1(c)]: the entry X[i][gc] of this thread is
-   * X^-1[pos(i)][piv(gc)].  PD(j, c*hd+k) = s_c Vinv_c(k, j), s = (+,-,-,-),
-   * row-major [j][4hd]; PS = MS^-1 row-major */
-  double* PD = R.PD + (size_t)pan * hd * 4 * hd;
-  double* PS = R.smat + (size_t)pan * hd * hd;
-  if (tact) {
-    const int jq = s_piv[gc], jm = s_piv[hd + gc];
-#pragma unroll
-    for (int r = 0; r < MAXR; ++r) {
-      const int i = trg + RG * r;
-      if (i >= hd) continue;
-      const int kq = s_pos[i], km = s_pos[hd + i];
-      double* d = PD + (size_t)jq * 4 * hd + kq;
-      d[0] = q[r][0]; d[hd] = -q[r][1]; d[2 * hd] = -q[r][2]; d[3 * hd] = -q[r][3];
-      PS[(size_t)km * hd + jm] = mv[r];
-    }
-  }
-  __threadfence();
-  cl.sync();
-  panel_b_epilogue(R, hd, pan, c0, nc, (int)panel_smem_doubles(hd, nbd, CS), psm);
-}
-
-
 /* ---------------------------------------------------------------------
- * Blocked Gauss-Jordan panel precompute (orders whose matrix columns fit a
- * cluster's shared memory: hdim <= 136 with up to 4 CTAs).
- *
- * The same inverses as k_rrq_panel, computed as a blocked Gauss-Jordan
- * elimination with the same pivot rule (largest quaternion norm / largest
- * magnitude among the unused rows of the pivot column, no row moves): columns
- * are taken PB_NB = 8 at a time.  The CTA owning a block eliminates within the
- * block's 8 columns alone (the panel phase: 8 steps of the unblocked method on
- * hd x 8 entries, CTA barriers only) and publishes the block M and its pivot
- * rows P to every CTA of the cluster through distributed shared memory; every
- * CTA then applies the block's 8 steps to all its other columns at once,
- *     X[:, J] <- X[:, J] (rows P set to 0) + M X[P, J],
- * on the FP64 tensor path (mma m8n8k4): for the quaternion system the real
- * GEMM (4 hd x 32) (32 x ncol) with A the left-multiplication matrices of M's
- * entries, built in the fragment loads (entry c^d of M[i][b], sign from a
- * table), B the pivot rows' components; for the real system the GEMM
- * (hd x 8) (8 x ncol).  Two cluster barriers a block (12 blocks at hdim 91)
- * instead of one a column.  The in-place result equals the unblocked
- * method's, so the write-out X^-1[k][c] = X[pi(k)][pi^-1(c)] and the B
- * epilogue are k_rrq_panel's.
- * Shared memory per CTA (doubles): Xq 4 planes of hq x ncol (V's columns of
- * this CTA, component-major), Xr hr x ncol (MS's columns), Mq hq x 8 x 4 and
- * Mr hr x 8 (the published block), the pivot column, the scaled pivot rows,
- * pivot bookkeeping.  hq = hd rounded up to 2 (8 real rows), hr to 8, ncol
- * = ceil(hd / CS) rounded up to 8.
+ * Per-panel RRQ precompute: the inverses of the quaternion system V (hd x hd,
+ * V[j][k] = (0, grad h_k(y_j)), the real form of the reference's MD,
+ * lap3d_close_mod.f90:851-858) and of the real S system MS (Msl^T, :861-863)
+ * by a blocked Gauss-Jordan elimination with row pivoting (largest quaternion
+ * norm / magnitude among the unused rows of the pivot column, no row moves;
+ * the inverse is X^-1[k][c] = X[pi(k)][pi^-1(c)] with pi the pivot sequence),
+ * one cluster of CS CTAs a panel, each CTA holding ncol of the columns of
+ * both systems in shared memory (orders up to nterms 16 with CS <= 8).
+ * Columns are taken PB_NB = 8 at a time.  The CTA owning a block eliminates
+ * within the block's 8 columns alone (the panel phase: 8 column steps,
+ * register-resident, one named barrier a step) and publishes the block M and
+ * its pivot rows P to every CTA of the cluster through distributed shared
+ * memory; every CTA then applies the block's 8 steps to its other columns at
+ * once, X[:, J] <- X[:, J] (rows P set to 0) + M X[P, J], on the FP64 tensor
+ * path (mma m8n8k4): for the quaternion system the real GEMM (4 hd x 32)
+ * (32 x ncol) with A the left-multiplication matrices of M's entries, built
+ * in the fragment loads (entry c^d of M[i][b], sign from a table), B the
+ * pivot rows' components; for the real system the GEMM (hd x 8) (8 x ncol).
+ * Two cluster barriers a block (12 blocks at hdim 91).  Then PD, PS and
+ * B = PS H^T (tensor path).
+ * Shared memory per CTA (doubles): Xq 4 planes of hq x RS (V's columns of this
+ * CTA, component-major), Xr hr x RS (MS's columns), Mq hq x 8 x 4 and Mr
+ * hr x 8 (the published block), the step's pivot column (two buffers),
+ * pivot bookkeeping.  hq = hd rounded up to 2 (8 real rows), hr to 8, ncol =
+ * ceil(hd / CS) rounded up to 8, RS = ncol + 1.
  * --------------------------------------------------------------------- */
 constexpr int PB_NB = 8;
 constexpr int PB_MAXT = 512; /* threads a CTA: two warps per 8-column tile, at most 8 tiles */
