@@ -171,6 +171,26 @@ int qol_grf_near_range(qol_int npan, qol_int nterms, qol_int nquad, qol_int orde
 int qol_direct_farfield_range(qol_int nsrc, const double* sx, const double* snx, const double* sw,
                               const double* ub, const double* ubn, qol_int tlo, qol_int thi, double* u);
 
+/* The reference's geometry generator on the GPU (utils/stellarator_geo_mex.c:
+ * stellarator_geo_ntri / stellarator_geo, geo_core :636-750; build_charts
+ * :125-160): a Fourier surface in the VMEC convention of surf_eval (:91-102),
+ * R = sum rc cos(m p - nfp n t), Z = sum zs sin(m p - nfp n t), modes
+ * (m, n, rc, zs) x nmode, cut into mp x np charts of the (t, p) torus (split at
+ * aspect 1.65 when split != 0), each chart sampled on the nterms x nterms
+ * Gauss grid and cut into two triangles whose Vioreanu-Rokhlin nodes of degree
+ * nterms-1 are interpolated from it.  Outputs in the reference layout
+ * (sx(3, nsrc), snx, sw, rts, rps; nsrc = ntri * nterms (nterms+1)/2), host
+ * arrays.  With sx == NULL only *ntri is set (the size query); otherwise *ntri
+ * must be at least the panel count (QOL_ERR_NNZ) and receives it. */
+int qol_surface_panels(qol_int nmode, const double* modes, qol_int nfp, qol_int mp, qol_int np, qol_int nterms,
+                       qol_int split, qol_int* ntri, double* sx, double* snx, double* sw, double* rts,
+                       double* rps);
+/* Host helper: the matrix M (n x npols, column-major) interpolating values at
+ * the Vioreanu-Rokhlin nodes of degree korder to the points uv (2 x n) of the
+ * reference triangle (koorn_pols_batch_r64 times umatr, as
+ * stellarator_grf_core_mod.f90:1009-1015 builds its render interpolation). */
+int qol_interp_matrix(qol_int korder, qol_int n, const double* uv, double* M);
+
 /* Library status and diagnostics.  qol_kernel_times: when enabled, every
  * pipeline call records CUDA events on its stream around its phases and
  * accumulates the device milliseconds of its QOL_NPHASE phases: [0] refined

@@ -16,7 +16,7 @@ __all__ = [
     "lib", "QolError", "qol_simplex_precomp", "qol_build_patch_levels", "qol_lap3dsdlpmat_levels",
     "qol_clear_patch_levels", "qol_clear_patch_levels_all", "qol_rrq", "qol_getnearquad_lap_rrq",
     "qol_getnearquad_lap_rrq_dev", "qol_grf_near", "qol_grf_near_range", "qol_direct_farfield",
-    "qol_direct_farfield_range", "qol_set_sum_precision",
+    "qol_direct_farfield_range", "qol_surface_panels", "qol_interp_matrix", "qol_set_sum_precision",
     "SELECTOR_NW", "qol_selector_features", "qol_selector_grad", "qol_selector_train", "qol_selector_set",
     "qol_selector_stats", "qol_set_autotune", "qol_panel_shape",
 ]
@@ -263,6 +263,37 @@ def qol_direct_farfield_range(sx, snx, sw, ub, ubn, tlo, thi, u):
                                          _vp(_f(ub, nsrc)), _vp(_f(ubn, nsrc)), i64(tlo), i64(thi), _vp(u))
     _check(rc)
     return u
+
+
+def qol_surface_panels(surface, mp, np_, nterms, split=True):
+    """The surface's panels from the GPU geometry generator (the reference's
+    utils/stellarator_geo_mex.c geo_core): dict(sx, snx, sw, rts, rps) as
+    (nsrc, 3)/(nsrc,) arrays, ntri, hdim, the layout geometry.panels gives.
+    ``surface`` has vmec_modes() (geometry.Surface, geometry.BuiltinSurface)."""
+    modes, nfp = surface.vmec_modes()
+    modes = np.ascontiguousarray(np.asarray(modes, np.float64).reshape(-1, 4))
+    nt = np.zeros(1, np.int64)
+    args = (i64(modes.shape[0]), _vp(modes), i64(nfp), i64(mp), i64(np_), i64(nterms), i64(int(bool(split))))
+    _check(lib().qol_surface_panels(*args, _vp(nt), None, None, None, None, None))
+    hd = nterms * (nterms + 1) // 2
+    nsrc = int(nt[0]) * hd
+    out = {k: np.zeros((nsrc, 3)) for k in ("sx", "snx", "rts", "rps")}
+    out["sw"] = np.zeros(nsrc)
+    _check(lib().qol_surface_panels(*args, _vp(nt), _vp(out["sx"]), _vp(out["snx"]), _vp(out["sw"]),
+                                    _vp(out["rts"]), _vp(out["rps"])))
+    out["ntri"] = int(nt[0])
+    out["hdim"] = hd
+    return out
+
+
+def qol_interp_matrix(korder, uv):
+    """Matrix (n x npols) interpolating values at the degree-korder VR nodes to
+    the reference-triangle points uv (n x 2)."""
+    uv = np.ascontiguousarray(np.asarray(uv, np.float64).reshape(-1, 2))
+    npols = (korder + 1) * (korder + 2) // 2
+    M = np.zeros(uv.shape[0] * npols)
+    _check(lib().qol_interp_matrix(i64(korder), i64(uv.shape[0]), _vp(uv), _vp(M)))
+    return M.reshape(npols, uv.shape[0]).T.copy()
 
 
 def qol_direct_farfield(sx, snx, sw, ub, ubn):

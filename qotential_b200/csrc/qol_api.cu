@@ -1439,7 +1439,8 @@ int qol_grf_near_range(qol_int npan, qol_int nterms, qol_int nquad, qol_int orde
   if (nloc == 0) return 0;
   cudaStream_t st = g_stream;
   const int nbd = 3 * (int)nquad;
-  size_t need = sizeof(double) * (size_t)(16 * nsrc + 4 * npan + (xbuf ? 3 * (nbd + 3) * npan : 0)) +
+  size_t need = sizeof(double) * (size_t)(16 * nsrc + 4 * npan + 6 * ((nsrc + 255) / 256) +
+                                          (xbuf ? 3 * (nbd + 3) * npan : 0)) +
                 sizeof(long long) * (size_t)(3 * nloc + 3) + 16 * 256;
   if ((rc = g_arena_io.reserve(need))) return rc;
   g_arena_io.reset();
@@ -1452,6 +1453,7 @@ int qol_grf_near_range(qol_int npan, qol_int nterms, qol_int nquad, qol_int orde
   double* dubn = g_arena_io.take<double>(nsrc);
   double* du = g_arena_io.take<double>(nsrc);
   double* dball = g_arena_io.take<double>(4 * npan);
+  double* dbox = g_arena_io.take<double>(6 * (size_t)((nsrc + 255) / 256)); /* node-chunk boxes of the near search */
   double* dchart = xbuf ? g_arena_io.take<double>((size_t)3 * (nbd + 3) * nloc) : nullptr;
   long long* dcnt = g_arena_io.take<long long>(nloc);
   long long* doff = g_arena_io.take<long long>(nloc + 1); /* 0-based offsets */
@@ -1467,7 +1469,7 @@ int qol_grf_near_range(qol_int npan, qol_int nterms, qol_int nquad, qol_int orde
   if (xbuf)
     CK(cudaMemcpyAsync(dchart, xbuf + (size_t)3 * (nbd + 3) * plo, sizeof(double) * 3 * (nbd + 3) * nloc,
                        cudaMemcpyHostToDevice, st));
-  CK(qol_launch_grf_balls((int)npan, (int)hd, nsrc, dsx, dsw, dball, dcnt, (int)plo, (int)phi, st));
+  CK(qol_launch_grf_balls((int)npan, (int)hd, nsrc, dsx, dsw, dball, dbox, dcnt, (int)plo, (int)phi, st));
   std::vector<long long> cnt(nloc), off(nloc + 1), xi(nloc + 1);
   CK(cudaMemcpyAsync(cnt.data(), dcnt, sizeof(long long) * nloc, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
@@ -1489,7 +1491,7 @@ int qol_grf_near_range(qol_int npan, qol_int nterms, qol_int nquad, qol_int orde
     double* dvs = g_arena_grf.take<double>((size_t)nn * hd);
     double* dvd = g_arena_grf.take<double>((size_t)nn * hd);
     const double* ball = dball + 4 * (size_t)plo;
-    CK(qol_launch_grf_csr((int)nloc, nsrc, dsx, ball, doff, didx, dtcx, plo ? dloc : nullptr,
+    CK(qol_launch_grf_csr((int)nloc, nsrc, dsx, ball, dbox, doff, didx, dtcx, plo ? dloc : nullptr,
                           (long long)plo * hd, st));
     Job J{};
     J.npan = (int)nloc; J.nterms = (int)nterms; J.nquad = (int)nquad; J.orderff = (int)orderff;
@@ -1518,6 +1520,72 @@ int qol_grf_near(qol_int npan, qol_int nterms, qol_int nquad, qol_int orderff, d
                  qol_int* nnear, qol_int* level_hist, double* timeinfo) {
   return qol_grf_near_range(npan, nterms, nquad, orderff, distff, iside, nsrc, sx, snx, sw, rts, rps, xbuf, ub, ubn,
                             0, npan, u, nnear, level_hist, timeinfo);
+}
+
+int qol_surface_panels(qol_int nmode, const double* modes, qol_int nfp, qol_int mp, qol_int np, qol_int nterms,
+                       qol_int split, qol_int* ntri, double* sx, double* snx, double* sw, double* rts,
+                       double* rps) {
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  if (!modes || !ntri || nmode < 1 || mp < 1 || np < 1) return fail(QOL_ERR_ARG, "bad arguments");
+  if (nterms < 2 || nterms > 16) return fail(QOL_ERR_ORDER, "nterms outside 2..16");
+  const std::vector<qolh::Chart> cl =
+      qolh::surface_charts((int)nmode, modes, (int)nfp, (int)mp, (int)np, (int)nterms, split != 0);
+  const qol_int nchart = (qol_int)cl.size(), nt = 2 * nchart;
+  if (!sx) { *ntri = nt; return 0; } /* the size query (as stellarator_geo_ntri) */
+  if (!snx || !sw || !rts || !rps) return fail(QOL_ERR_ARG, "null output");
+  if (*ntri < nt) return fail(QOL_ERR_NNZ, "ntri is smaller than the panel count");
+  *ntri = nt;
+  int rc = ensure_device();
+  if (rc) return rc;
+  const int p = (int)nterms, hd = p * (p + 1) / 2;
+  const size_t nsrc = (size_t)nt * hd;
+  std::vector<double> x0(p), w0(p), Dm((size_t)p * p), uv(2 * hd), wts(hd), tables, chv(6 * (size_t)nchart);
+  qolh::gauss(p, x0.data(), w0.data(), Dm.data());
+  qolh::vr_nodes(p - 1, uv.data(), wts.data());
+  qolh::surface_interp_tables(p, tables);
+  for (qol_int c = 0; c < nchart; ++c) {
+    const qolh::Chart& h = cl[c];
+    const double v[6] = {h.a1, h.b1, h.a2, h.b2, h.jj, h.ii};
+    for (int k = 0; k < 6; ++k) chv[6 * c + k] = v[k];
+  }
+  cudaStream_t st = g_stream;
+  const size_t need = sizeof(double) * (4 * (size_t)nmode + chv.size() + 2 * (size_t)p + Dm.size() + hd +
+                                        tables.size() + 13 * nsrc) + 16 * 256;
+  if ((rc = g_arena_io.reserve(need))) return rc;
+  g_arena_io.reset();
+  double* dmodes = g_arena_io.take<double>(4 * (size_t)nmode);
+  double* dch = g_arena_io.take<double>(chv.size());
+  double* dx0 = g_arena_io.take<double>(p);
+  double* dD = g_arena_io.take<double>(Dm.size());
+  double* dw = g_arena_io.take<double>(hd);
+  double* dtab = g_arena_io.take<double>(tables.size());
+  double* dsx = g_arena_io.take<double>(3 * nsrc);
+  double* dsnx = g_arena_io.take<double>(3 * nsrc);
+  double* dsw = g_arena_io.take<double>(nsrc);
+  double* drts = g_arena_io.take<double>(3 * nsrc);
+  double* drps = g_arena_io.take<double>(3 * nsrc);
+  CK(cudaMemcpyAsync(dmodes, modes, sizeof(double) * 4 * nmode, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dch, chv.data(), sizeof(double) * chv.size(), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dx0, x0.data(), sizeof(double) * p, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dD, Dm.data(), sizeof(double) * Dm.size(), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dw, wts.data(), sizeof(double) * hd, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dtab, tables.data(), sizeof(double) * tables.size(), cudaMemcpyHostToDevice, st));
+  const double pi = 3.14159265358979323846;
+  CK(qol_launch_surface_panels((int)nchart, (int)nmode, dmodes, (int)nfp, p, dch, pi / (double)np, pi / (double)mp,
+                               dx0, dD, dw, dtab, dsx, dsnx, dsw, drts, drps, st));
+  CK(cudaMemcpyAsync(sx, dsx, sizeof(double) * 3 * nsrc, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(snx, dsnx, sizeof(double) * 3 * nsrc, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(sw, dsw, sizeof(double) * nsrc, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(rts, drts, sizeof(double) * 3 * nsrc, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(rps, drps, sizeof(double) * 3 * nsrc, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return 0;
+}
+
+int qol_interp_matrix(qol_int korder, qol_int n, const double* uv, double* M) {
+  if (korder < 0 || korder > 20 || n < 0 || (n > 0 && (!uv || !M))) return fail(QOL_ERR_ARG, "bad arguments");
+  qolh::interp_matrix((int)korder, (int)n, uv, M);
+  return 0;
 }
 
 int qol_direct_farfield_range(qol_int nsrc, const double* sx, const double* snx, const double* sw,

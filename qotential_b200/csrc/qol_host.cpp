@@ -10,6 +10,7 @@
 #include <stdexcept>
 
 namespace qolh {
+static const double QOL_PI_H = 3.14159265358979323846;
 
 int lu_factor(int n, double* A, int* piv) {
   for (int k = 0; k < n; ++k) {
@@ -368,6 +369,69 @@ void build_ref(int korder, int order, int nlevel, bool sqmode, RefElem& R) {
     L.interp.assign((size_t)L.n * npols, 0.0);
     interp_matrix(korder, (int)L.n, L.uv.data(), L.interp.data());
   }
+}
+
+void surface_eval(int nmode, const double* modes, int nfp, double t, double p, double* x) {
+  double R = 0.0, Z = 0.0;
+  for (int k = 0; k < nmode; ++k) {
+    const double ang = modes[4 * k] * p - nfp * modes[4 * k + 1] * t;
+    R = R + modes[4 * k + 2] * std::cos(ang);
+    Z = Z + modes[4 * k + 3] * std::sin(ang);
+  }
+  x[0] = R * std::cos(t); x[1] = R * std::sin(t); x[2] = Z;
+}
+
+std::vector<Chart> surface_charts(int nmode, const double* modes, int nfp, int mp, int np, int nterms, bool split) {
+  const double ASPECT = 1.65;
+  std::vector<double> x0(nterms), w0(nterms);
+  gauss(nterms, x0.data(), w0.data(), nullptr);
+  const double ts1 = QOL_PI_H / np, ts2 = QOL_PI_H / mp;
+  std::vector<Chart> cl;
+  for (int j = 1; j <= np; ++j)
+    for (int i = 1; i <= mp; ++i) {
+      auto ev = [&](double t1, double t2, double* x) {
+        surface_eval(nmode, modes, nfp, (t1 + 2.0 * j) * ts1, (t2 + 2.0 * i) * ts2, x);
+      };
+      double xll[3], xul[3], xlr[3];
+      ev(x0[0], x0[0], xll); ev(x0[0], x0[nterms - 1], xul); ev(x0[nterms - 1], x0[0], xlr);
+      double dt = 0.0, dp = 0.0;
+      for (int d = 0; d < 3; ++d) { dt += (xll[d] - xlr[d]) * (xll[d] - xlr[d]); dp += (xll[d] - xul[d]) * (xll[d] - xul[d]); }
+      dt = std::sqrt(dt); dp = std::sqrt(dp);
+      const Chart base{1.0, 0.0, 1.0, 0.0, (double)j, (double)i};
+      if (split && dt / dp > ASPECT) {
+        Chart c1 = base, c2 = base; c1.a1 = 0.5; c1.b1 = -0.5; c2.a1 = 0.5; c2.b1 = 0.5;
+        cl.push_back(c1); cl.push_back(c2);
+      } else if (split && dp / dt > ASPECT) {
+        Chart c1 = base, c2 = base; c1.a2 = 0.5; c1.b2 = -0.5; c2.a2 = 0.5; c2.b2 = 0.5;
+        cl.push_back(c1); cl.push_back(c2);
+      } else {
+        cl.push_back(base);
+      }
+    }
+  return cl;
+}
+
+void surface_interp_tables(int p, std::vector<double>& tables) {
+  const int hd = p * (p + 1) / 2;
+  std::vector<double> x0(p), w0(p), uv(2 * hd);
+  gauss(p, x0.data(), w0.data(), nullptr);
+  vr_nodes(p - 1, uv.data(), nullptr);
+  tables.assign((size_t)4 * hd * p * p, 0.0);
+  auto lag = [&](double t, int j) { /* Lagrange basis j at t */
+    double num = 1.0, den = 1.0;
+    for (int k = 0; k < p; ++k)
+      if (k != j) { num *= (t - x0[k]); den *= (x0[j] - x0[k]); }
+    return num / den;
+  };
+  for (int key = 0; key < 4; ++key)
+    for (int i = 0; i < hd; ++i) {
+      const double u = 2.0 * uv[2 * i] - 1.0, v = 2.0 * uv[2 * i + 1] - 1.0;
+      const double t1 = key == 0 ? u : key == 1 ? -u : key == 2 ? v : -v;
+      const double t2 = key == 0 ? v : key == 1 ? -v : key == 2 ? -u : u;
+      for (int b = 0; b < p; ++b)
+        for (int a = 0; a < p; ++a)
+          tables[((size_t)key * hd + i) * p * p + a + (size_t)b * p] = lag(t1, b) * lag(t2, a);
+    }
 }
 
 void xlate_schedule(int L, int lanes, std::vector<uint32_t>& tab, int& steps, std::vector<uint32_t>& red,

@@ -66,6 +66,20 @@ void build_ref(int korder, int order, int nlevel, bool sqmode, RefElem& R);
  * lane] is one term: bits 0-7 the M entry lam(lam+1)/2+|mu|, 8-15 the R entry
  * nu(nu+1)/2+|k-mu|, 16-25 the slot, 26 conj M (mu < 0), 27 conj R (k-mu < 0),
  * 28 negate ((-1)^|mu| (-1)^|k-mu| = -1), 29 valid, 30 last term of its piece. */
+/* Fourier surface (VMEC convention of utils/stellarator_geo_mex.c surf_eval,
+ * :91-102): R = sum rc cos(m p - nfp n t), Z = sum zs sin(m p - nfp n t),
+ * x = (R cos t, R sin t, Z); modes (m, n, rc, zs) x nmode */
+void surface_eval(int nmode, const double* modes, int nfp, double t, double p, double* x);
+/* one chart of the mp x np (t, p) grid: t = ((a1 s + b1) + 2 jj) pi/np,
+ * p = ((a2 s + b2) + 2 ii) pi/mp for s in [-1, 1] (build_charts,
+ * utils/stellarator_geo_mex.c:125-160; split at aspect 1.65 when requested) */
+struct Chart { double a1, b1, a2, b2, jj, ii; };
+std::vector<Chart> surface_charts(int nmode, const double* modes, int nfp, int mp, int np, int nterms, bool split);
+/* Lagrange interpolation from the p Gauss nodes, tensor form: M (hd x p^2,
+ * row-major, column m = a + b p) for the VR nodes of degree p-1 under the
+ * four chart orientations (geo_core, :636-750): keys lA (u, v), rA (-u, -v),
+ * lB (v, -u), rB (-v, u) with (u, v) = 2 uv - 1 */
+void surface_interp_tables(int p, std::vector<double>& tables /* 4 x hd x p^2 */);
 void xlate_schedule(int L, int lanes, std::vector<uint32_t>& tab, int& steps, std::vector<uint32_t>& red,
                     int& slots);
 

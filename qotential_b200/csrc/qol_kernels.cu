@@ -2294,6 +2294,95 @@ cudaError_t qol_launch_coo_index(const OrderTab& T, const PairIn& Q, long long* 
   return cudaGetLastError();
 }
 
+
+/* ===================================================================== */
+/* surface panels (the reference's geometry generator, geo_core,          */
+/* utils/stellarator_geo_mex.c:636-750): one CTA per chart, p^2 threads   */
+/* ===================================================================== */
+/* chart c: (a1, b1, a2, b2, jj, ii) at charts[6c..]; the Fourier surface
+ * sampled on the p x p Gauss grid of the chart, its t- and p-derivatives by
+ * the spectral differentiation matrix D, and the chart's two triangles'
+ * Vioreanu-Rokhlin nodes by tensor Lagrange interpolation (tables: 4
+ * orientations x hd x p^2); outputs in the reference layout, triangle 2c + s */
+__global__ void __launch_bounds__(256) k_surface_panels(int nmode, const double* modes, int nfp, int p, int hd,
+                                                        const double* charts, double ts1, double ts2,
+                                                        const double* x0, const double* D, const double* wts,
+                                                        const double* tables, double* sx, double* snx, double* sw,
+                                                        double* rts, double* rps) {
+  extern __shared__ double gsm[];
+  const int P2 = p * p, c = blockIdx.x, tid = threadIdx.x;
+  double* G = gsm;           /* p^2 x 9: x, x_t, x_p */
+  const double* ch = charts + 6 * (size_t)c;
+  if (tid < P2) {
+    const int a = tid % p, b = tid / p;
+    const double uu = ((ch[0] * x0[b] + ch[1]) + 2.0 * ch[4]) * ts1;
+    const double vv = ((ch[2] * x0[a] + ch[3]) + 2.0 * ch[5]) * ts2;
+    double R = 0.0, Z = 0.0;
+    for (int k = 0; k < nmode; ++k) {
+      const double ang = modes[4 * k] * vv - nfp * modes[4 * k + 1] * uu;
+      R = R + modes[4 * k + 2] * cos(ang);
+      Z = Z + modes[4 * k + 3] * sin(ang);
+    }
+    G[9 * tid] = R * cos(uu); G[9 * tid + 1] = R * sin(uu); G[9 * tid + 2] = Z;
+  }
+  __syncthreads();
+  if (tid < P2) { /* node m = a + b p: d/da along the row, d/db along the column */
+    const int a = tid % p, b = tid / p;
+    double ta[3] = {0.0, 0.0, 0.0}, tb[3] = {0.0, 0.0, 0.0};
+    for (int k = 0; k < p; ++k) {
+      const double da = D[a + (size_t)p * k], db = D[b + (size_t)p * k]; /* D[row][k], column-major */
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        ta[d] += da * G[9 * (k + b * p) + d];
+        tb[d] += db * G[9 * (a + k * p) + d];
+      }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) { G[9 * tid + 3 + d] = ta[d]; G[9 * tid + 6 + d] = tb[d]; }
+  }
+  __syncthreads();
+  double d1 = 0.0, d2 = 0.0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double e1 = G[d] - G[9 * (P2 - 1) + d], e2 = G[9 * (p - 1) + d] - G[9 * (P2 - p) + d];
+    d1 += e1 * e1; d2 += e2 * e2;
+  }
+  const int key0 = d1 + 1e-13 > d2 ? 0 : 2; /* (lA, rA) or (lB, rB) */
+  for (int e = tid; e < 2 * hd; e += blockDim.x) {
+    const int s = e / hd, i = e % hd, key = key0 + s;
+    const double* M = tables + ((size_t)key * hd + i) * P2;
+    double acc[9];
+#pragma unroll
+    for (int f = 0; f < 9; ++f) acc[f] = 0.0;
+    for (int m = 0; m < P2; ++m) {
+      const double w = M[m];
+#pragma unroll
+      for (int f = 0; f < 9; ++f) acc[f] += w * G[9 * m + f];
+    }
+    /* xt = d/d(row index) = acc[3..5], xp = acc[6..8] (geometry.panels' rts, rps) */
+    const double n0 = acc[7] * acc[5] - acc[8] * acc[4], n1 = acc[8] * acc[3] - acc[6] * acc[5],
+                 n2 = acc[6] * acc[4] - acc[7] * acc[3];
+    const double sp = sqrt(n0 * n0 + n1 * n1 + n2 * n2);
+    const size_t o = (size_t)(2 * c + s) * hd + i;
+    sx[3 * o] = acc[0]; sx[3 * o + 1] = acc[1]; sx[3 * o + 2] = acc[2];
+    snx[3 * o] = n0 / sp; snx[3 * o + 1] = n1 / sp; snx[3 * o + 2] = n2 / sp;
+    rts[3 * o] = 2.0 * acc[3]; rts[3 * o + 1] = 2.0 * acc[4]; rts[3 * o + 2] = 2.0 * acc[5];
+    rps[3 * o] = 2.0 * acc[6]; rps[3 * o + 1] = 2.0 * acc[7]; rps[3 * o + 2] = 2.0 * acc[8];
+    sw[o] = sp * wts[i] * 4.0;
+  }
+}
+cudaError_t qol_launch_surface_panels(int nchart, int nmode, const double* modes, int nfp, int p,
+                                      const double* charts, double ts1, double ts2, const double* x0,
+                                      const double* D, const double* wts, const double* tables, double* sx,
+                                      double* snx, double* sw, double* rts, double* rps, cudaStream_t st) {
+  if (nchart <= 0) return cudaSuccess;
+  const int hd = p * (p + 1) / 2;
+  const size_t smem = sizeof(double) * 9 * (size_t)p * p;
+  k_surface_panels<<<nchart, 256, smem, st>>>(nmode, modes, nfp, p, hd, charts, ts1, ts2, x0, D, wts, tables, sx,
+                                               snx, sw, rts, rps);
+  return cudaGetLastError();
+}
+
 /* ===================================================================== */
 /* FP64 FMA throughput probe (roofline denominator for the FP64 kernels)  */
 /* ===================================================================== */
@@ -2338,16 +2427,83 @@ __device__ __forceinline__ bool in_ball(const double* x, const double* b) {
   const double a = __dadd_rn(x[0], -b[0]), c = __dadd_rn(x[1], -b[1]), e = __dadd_rn(x[2], -b[2]);
   return __dadd_rn(__dadd_rn(__dmul_rn(a, a), __dmul_rn(c, c)), __dmul_rn(e, e)) < b[3];
 }
+/* Near search by node chunks: the nodes in source order are cut into chunks of
+ * BALL_CH; a chunk's axis-aligned bounding box is tested against a panel's
+ * ball first (conservatively: the box distance is at most any node's) and only
+ * the nodes of chunks that can reach the ball get the exact test.  Sources of
+ * consecutive panels are neighbours on the surface, so a ball reaches a few
+ * chunks; the panel's list stays in source order (chunks in order, nodes in
+ * order within a chunk): the reference's CSR, without a sort. */
+#define BALL_CH 256
+__global__ void __launch_bounds__(BALL_CH) k_chunk_boxes(long long nsrc, const double* sx, double* box) {
+  __shared__ double red[6][BALL_CH / 32];
+  const long long j = (long long)blockIdx.x * BALL_CH + threadIdx.x;
+  double v[6];
+  if (j < nsrc) {
+    for (int d = 0; d < 3; ++d) { v[d] = sx[3 * j + d]; v[3 + d] = v[d]; }
+  } else {
+    for (int d = 0; d < 3; ++d) { v[d] = 1e300; v[3 + d] = -1e300; }
+  }
+  for (int o = 16; o > 0; o >>= 1)
+    for (int d = 0; d < 3; ++d) {
+      v[d] = fmin(v[d], __shfl_xor_sync(0xffffffffu, v[d], o));
+      v[3 + d] = fmax(v[3 + d], __shfl_xor_sync(0xffffffffu, v[3 + d], o));
+    }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0)
+    for (int d = 0; d < 6; ++d) red[d][w] = v[d];
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    const int d = threadIdx.x;
+    double r = red[d][0];
+    for (int q = 1; q < BALL_CH / 32; ++q) r = d < 3 ? fmin(r, red[d][q]) : fmax(r, red[d][q]);
+    box[6 * (size_t)blockIdx.x + d] = r;
+  }
+}
+__device__ __forceinline__ bool ball_reaches_box(const double* b, const double* box) {
+  double d2 = 0.0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double t = fmax(fmax(box[d] - b[d], b[d] - box[3 + d]), 0.0);
+    d2 += t * t;
+  }
+  return d2 <= b[3] * (1.0 + 1e-12);
+}
+/* this CTA's chunks that reach ball b among chunks [c0, c0 + blockDim.x),
+ * in order, into list[0 .. return) */
+__device__ int reaching_chunks(const double* b, const double* box, long long nchunk, long long c0, int* list,
+                               int* wcnt) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const long long c = c0 + threadIdx.x;
+  const bool hit = c < nchunk && ball_reaches_box(b, box + 6 * c);
+  const unsigned m = __ballot_sync(0xffffffffu, hit);
+  if (lane == 0) wcnt[w] = __popc(m);
+  __syncthreads();
+  int before = 0, total = 0;
+  for (int q = 0; q < nw; ++q) { if (q < w) before += wcnt[q]; total += wcnt[q]; }
+  if (hit) list[before + __popc(m & ((1u << lane) - 1u))] = (int)(c - c0);
+  __syncthreads();
+  return total;
+}
 /* near sources per panel (CTA per panel) */
-__global__ void __launch_bounds__(256) k_ball_count(long long nsrc, const double* sx, const double* ball,
-                                                    long long* counts) {
+__global__ void __launch_bounds__(BALL_CH) k_ball_count(long long nsrc, const double* sx, const double* ball,
+                                                        const double* box, long long* counts) {
   const int k = blockIdx.x;
   __shared__ double b[4];
-  __shared__ long long part[8];
+  __shared__ long long part[BALL_CH / 32];
+  __shared__ int list[BALL_CH], wcnt[BALL_CH / 32];
   if (threadIdx.x < 4) b[threadIdx.x] = ball[4 * k + threadIdx.x];
   __syncthreads();
+  const long long nchunk = (nsrc + BALL_CH - 1) / BALL_CH;
   long long c = 0;
-  for (long long j = threadIdx.x; j < nsrc; j += blockDim.x) c += in_ball(sx + 3 * j, b) ? 1 : 0;
+  for (long long c0 = 0; c0 < nchunk; c0 += BALL_CH) {
+    const int nl = reaching_chunks(b, box, nchunk, c0, list, wcnt);
+    for (int q = 0; q < nl; ++q) {
+      const long long j = (c0 + list[q]) * BALL_CH + threadIdx.x;
+      c += (j < nsrc && in_ball(sx + 3 * j, b)) ? 1 : 0;
+    }
+    __syncthreads();
+  }
   for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
   if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = c;
   __syncthreads();
@@ -2359,32 +2515,37 @@ __global__ void __launch_bounds__(256) k_ball_count(long long nsrc, const double
 }
 /* their 1-based indices in source order (the reference's CSR), the target
  * coordinates gathered alongside */
-__global__ void __launch_bounds__(256) k_ball_fill(long long nsrc, const double* sx, const double* ball,
-                                                   const long long* offs, long long* csr_idx, double* tcx,
-                                                   long long* csr_loc /* nullable */, long long row_shift) {
+__global__ void __launch_bounds__(BALL_CH) k_ball_fill(long long nsrc, const double* sx, const double* ball,
+                                                       const double* box, const long long* offs, long long* csr_idx,
+                                                       double* tcx, long long* csr_loc /* nullable */,
+                                                       long long row_shift) {
   const int k = blockIdx.x;
   __shared__ double b[4];
-  __shared__ int wcnt[8];
+  __shared__ int wcnt[BALL_CH / 32], list[BALL_CH], lcnt[BALL_CH / 32];
   if (threadIdx.x < 4) b[threadIdx.x] = ball[4 * k + threadIdx.x];
   __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const long long nchunk = (nsrc + BALL_CH - 1) / BALL_CH;
   long long base = offs[k];
-  for (long long j0 = 0; j0 < nsrc; j0 += blockDim.x) {
-    const long long j = j0 + threadIdx.x;
-    const bool hit = j < nsrc && in_ball(sx + 3 * j, b);
-    const unsigned m = __ballot_sync(0xffffffffu, hit);
-    if (lane == 0) wcnt[w] = __popc(m);
-    __syncthreads();
-    int before = 0, total = 0;
-    for (int q = 0; q < nw; ++q) { if (q < w) before += wcnt[q]; total += wcnt[q]; }
-    if (hit) {
-      const long long pos = base + before + __popc(m & ((1u << lane) - 1u));
-      csr_idx[pos] = j + 1;
-      if (csr_loc) csr_loc[pos] = j + 1 - row_shift; /* the pipeline's numbering of a panel range */
-      tcx[3 * pos] = sx[3 * j]; tcx[3 * pos + 1] = sx[3 * j + 1]; tcx[3 * pos + 2] = sx[3 * j + 2];
+  for (long long c0 = 0; c0 < nchunk; c0 += BALL_CH) {
+    const int nl = reaching_chunks(b, box, nchunk, c0, list, lcnt);
+    for (int q = 0; q < nl; ++q) {
+      const long long j = (c0 + list[q]) * BALL_CH + threadIdx.x;
+      const bool hit = j < nsrc && in_ball(sx + 3 * j, b);
+      const unsigned m = __ballot_sync(0xffffffffu, hit);
+      if (lane == 0) wcnt[w] = __popc(m);
+      __syncthreads();
+      int before = 0, total = 0;
+      for (int qq = 0; qq < nw; ++qq) { if (qq < w) before += wcnt[qq]; total += wcnt[qq]; }
+      if (hit) {
+        const long long pos = base + before + __popc(m & ((1u << lane) - 1u));
+        csr_idx[pos] = j + 1;
+        if (csr_loc) csr_loc[pos] = j + 1 - row_shift; /* the pipeline's numbering of a panel range */
+        tcx[3 * pos] = sx[3 * j]; tcx[3 * pos + 1] = sx[3 * j + 1]; tcx[3 * pos + 2] = sx[3 * j + 2];
+      }
+      base += total;
+      __syncthreads();
     }
-    base += total;
-    __syncthreads();
   }
 }
 /* csr_val[o0+j] = sum_k (S - S_naive)[j][k] ubn_k - (D - D_naive)[j][k] ub_k over
@@ -2468,15 +2629,17 @@ __global__ void __launch_bounds__(256) k_direct_far(long long nsrc, const double
 }
 
 cudaError_t qol_launch_grf_balls(int npan, int hd, long long nsrc, const double* sx, const double* sw, double* ball,
-                                 long long* counts, int plo, int phi, cudaStream_t st) {
+                                 double* box, long long* counts, int plo, int phi, cudaStream_t st) {
   k_ball_centers<<<(npan + 127) / 128, 128, 0, st>>>(npan, hd, sx, sw, ball);
-  if (phi > plo) k_ball_count<<<phi - plo, 256, 0, st>>>(nsrc, sx, ball + 4 * (size_t)plo, counts);
+  const long long nchunk = (nsrc + BALL_CH - 1) / BALL_CH;
+  if (nchunk > 0) k_chunk_boxes<<<(unsigned)nchunk, BALL_CH, 0, st>>>(nsrc, sx, box);
+  if (phi > plo) k_ball_count<<<phi - plo, BALL_CH, 0, st>>>(nsrc, sx, ball + 4 * (size_t)plo, box, counts);
   return cudaGetLastError();
 }
-cudaError_t qol_launch_grf_csr(int npan, long long nsrc, const double* sx, const double* ball, const long long* offs,
-                               long long* csr_idx, double* tcx, long long* csr_loc, long long row_shift,
-                               cudaStream_t st) {
-  k_ball_fill<<<npan, 256, 0, st>>>(nsrc, sx, ball, offs, csr_idx, tcx, csr_loc, row_shift);
+cudaError_t qol_launch_grf_csr(int npan, long long nsrc, const double* sx, const double* ball, const double* box,
+                               const long long* offs, long long* csr_idx, double* tcx, long long* csr_loc,
+                               long long row_shift, cudaStream_t st) {
+  k_ball_fill<<<npan, BALL_CH, 0, st>>>(nsrc, sx, ball, box, offs, csr_idx, tcx, csr_loc, row_shift);
   return cudaGetLastError();
 }
 cudaError_t qol_launch_grf_apply(int npan, int hd, long long nsrc, const double* sx, const double* ball,

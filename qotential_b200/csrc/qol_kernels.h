@@ -125,17 +125,24 @@ cudaError_t qol_launch_coo_index(const OrderTab& T, const PairIn& Q, long long* 
                                  cudaStream_t st);
 cudaError_t qol_launch_fp64_peak(double* out, int blocks, int iters, cudaStream_t st);
 /* GRF near phase and Direct far field */
-/* ball centres of all npan panels; near counts of panels [plo, phi) into counts[0 .. phi - plo) */
+/* ball centres of all npan panels, node-chunk boxes (6 doubles a chunk of 256
+ * nodes, ceil(nsrc / 256) chunks); near counts of panels [plo, phi) into
+ * counts[0 .. phi - plo) */
 cudaError_t qol_launch_grf_balls(int npan, int hd, long long nsrc, const double* sx, const double* sw, double* ball,
-                                 long long* counts, int plo, int phi, cudaStream_t st);
+                                 double* box, long long* counts, int plo, int phi, cudaStream_t st);
 /* CSR of npan panels (ball points at their first ball); csr_loc (nullable) gets the
  * rows minus row_shift */
-cudaError_t qol_launch_grf_csr(int npan, long long nsrc, const double* sx, const double* ball, const long long* offs,
-                               long long* csr_idx, double* tcx, long long* csr_loc, long long row_shift,
-                               cudaStream_t st);
+cudaError_t qol_launch_grf_csr(int npan, long long nsrc, const double* sx, const double* ball, const double* box,
+                               const long long* offs, long long* csr_idx, double* tcx, long long* csr_loc,
+                               long long row_shift, cudaStream_t st);
 cudaError_t qol_launch_grf_apply(int npan, int hd, long long nsrc, const double* sx, const double* ball,
                                  const long long* offs, const long long* csr_idx, const double* vs, const double* vd,
                                  const double* ub, const double* ubn, double* csr_val, double* u, cudaStream_t st);
+/* the geometry generator: nchart charts -> 2 nchart panels (reference layout) */
+cudaError_t qol_launch_surface_panels(int nchart, int nmode, const double* modes, int nfp, int p,
+                                      const double* charts, double ts1, double ts2, const double* x0,
+                                      const double* D, const double* wts, const double* tables, double* sx,
+                                      double* snx, double* sw, double* rts, double* rps, cudaStream_t st);
 /* u_i for the targets i in [tlo, thi) over all nsrc sources */
 cudaError_t qol_launch_direct_far(long long nsrc, const double* sx, const double* snx, const double* sw,
                                   const double* ub, const double* ubn, double* u, long long tlo, long long thi,

@@ -57,6 +57,10 @@ class Surface:
             Z = Z + zs * np.sin(ang)
         return np.stack([R * np.cos(t), R * np.sin(t), Z], axis=-1)
 
+    def vmec_modes(self):
+        """(modes (nmode x 4: m, n, rc, zs), nfp) for the GPU generator."""
+        return np.ascontiguousarray(self.modes), self.nfp
+
     def rz(self, t, p):
         R = 0.0 * t; Z = 0.0 * t
         for m, n, rc, zs in self.modes:
@@ -71,6 +75,14 @@ class BuiltinSurface:
     utils/stellarator_geo_mex.c:61-77), t toroidal, p poloidal."""
 
     nfp = 1
+
+    def vmec_modes(self):
+        """The same surface in the VMEC convention (nfp 1): R = sum rc cos(m p -
+        n t), Z = sum zs sin(m p - n t), x = (R cos t, R sin t, Z); the cos p and
+        sin p terms of the reference's formula combine into one mode (0.75, 1.25)."""
+        modes = [(2, 1, 0.17, 0.17), (2, 0, 0.11, 0.11), (1, 0, 0.75, 1.25), (0, 0, 4.5, 0.0),
+                 (1, -1, 0.07, 0.07), (1, 1, -0.45, 0.45)]
+        return np.ascontiguousarray(np.array(modes, dtype=np.float64)), 1
 
     def eval(self, t, p):
         t = np.asarray(t, dtype=np.float64); p = np.asarray(p, dtype=np.float64)

@@ -5,7 +5,9 @@ web/stellarator/test/native-direct-parity.py:41-97).
 
 Writes tests/golden/grf_order{4,6}.npz with u, ub, ubn, the GRF scalar, a
 strided subset of sx/snx/sw (every 7th node) and the SHA-256 of the full
-f64 sx/snx/sw arrays.  Run in a container that has the reference checkout,
+f64 sx/snx/sw arrays, and tests/golden/render_order{4,6}.npz with the render
+lattice's sizes, every 11th render vertex (position and log error) and the
+SHA-256 of the render triangles.  Run in a container that has the reference checkout,
 naming its root (the argument, or the QOL_REFERENCE_DIR environment variable):
     python tests/golden/make_golden.py <reference checkout>
 """
@@ -22,10 +24,12 @@ def load(path):
     magic, ntri, nsrc, nrender, nfaces, grf = struct.unpack_from("<8s4qd", blob)
     assert magic == b"STGRF001", magic
     off = 48
-    out = dict(ntri=ntri, nsrc=nsrc, grf=grf)
-    for name, cnt in [("sx", 3 * nsrc), ("snx", 3 * nsrc), ("sw", nsrc), ("ub", nsrc), ("ubn", nsrc), ("u", nsrc)]:
+    out = dict(ntri=ntri, nsrc=nsrc, grf=grf, nrender=nrender, nfaces=nfaces)
+    for name, cnt in [("sx", 3 * nsrc), ("snx", 3 * nsrc), ("sw", nsrc), ("ub", nsrc), ("ubn", nsrc), ("u", nsrc),
+                      ("render_xyz", 3 * nrender), ("render_log_error", nrender)]:
         out[name] = np.frombuffer(blob, dtype="<f8", count=cnt, offset=off).copy()
         off += 8 * cnt
+    out["render_triangles"] = np.frombuffer(blob, dtype="<i8", count=3 * nfaces, offset=off).copy()
     out["sha256"] = hashlib.sha256(blob).hexdigest()
     return out
 
@@ -46,6 +50,11 @@ def main():
             sha_snx=hashlib.sha256(f["snx"].tobytes()).hexdigest(),
             sha_sw=hashlib.sha256(f["sw"].tobytes()).hexdigest(),
             sha_bin=f["sha256"], mp=12, np_=36, order=order)
+        rsub = np.arange(0, f["nrender"], 11)
+        np.savez_compressed(
+            os.path.join(here, f"render_order{order}.npz"), nrender=f["nrender"], nfaces=f["nfaces"], rsub=rsub,
+            render_xyz_sub=f["render_xyz"].reshape(-1, 3)[rsub], render_log_error_sub=f["render_log_error"][rsub],
+            sha_render_triangles=hashlib.sha256(f["render_triangles"].astype("<i8").tobytes()).hexdigest())
         print(order, f["sha256"])
 
 
