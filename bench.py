@@ -218,6 +218,89 @@ def forms_compare(W, steps, warmup, D=None, out=None):
     return res
 
 
+def config4(steps=2, warmup=1):
+    """The benchmark set's largest configuration: the same stellarator refined to
+    32 x 256 quads (16,384 triangles, 1,490,944 surface nodes) at order 12
+    (nterms 13), targets all surface nodes + 200,000 seeded off-surface points
+    (the workload's distance law), geometry from the GPU generator.  The device
+    step (inputs and the COO outputs resident, about 51 GB) in the plain FP64
+    form and in the chosen form (FP32 level sums, qol_set_sum_precision(1)),
+    and the GRF identity error of both forms on the surface nodes (8 point
+    charges on |y| = 6 clear of the surface, Direct far field on the GPU)."""
+    import torch
+    import qotential_b200 as qol
+    from qotential_b200 import geometry as G
+    nterms = ORDER + 1
+    hd = nterms * (nterms + 1) // 2
+    t0 = time.perf_counter()
+    P = qol.qol_surface_panels(G.stellarator(), 32, 256, nterms, split=False)
+    t_geo = time.perf_counter() - t0
+    off = G.off_surface_targets(P, 200000, SEED, hd)
+    T = np.concatenate([P["sx"], off])
+    tcxi, tcxrow, tcx = G.near_lists(P["sx"], P["sw"], hd, targets=T)
+    t_near = time.perf_counter() - t0 - t_geo
+    npan = P["ntri"]
+    pairs = int(tcxrow.size)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    t = lambda a, dt=torch.float64: torch.as_tensor(np.ascontiguousarray(a), dtype=dt).to(dev)
+    D = {k: t(P[k]) for k in ("sx", "snx", "sw", "rts", "rps")}
+    D["tcx"] = t(tcx)
+    D["tcxrow"] = t(tcxrow, torch.int64)
+    D["tcxi"] = t(tcxi, torch.int64)
+    nnz = pairs * hd
+    out = (torch.empty(nnz, dtype=torch.int64, device=dev), torch.empty(nnz, dtype=torch.int64, device=dev),
+           torch.empty(nnz, dtype=torch.float64, device=dev), torch.empty(nnz, dtype=torch.float64, device=dev))
+    st = torch.cuda.current_stream()
+    hist = None
+
+    def step(want=False):
+        return qol.qol_getnearquad_lap_rrq_dev(npan, nterms, nterms + 2, D["sx"], D["snx"], D["sw"], D["rts"],
+                                               D["rps"], D["tcx"], D["tcxrow"], D["tcxi"], nterms + 2, 1.4, 30, out,
+                                               stream=st.cuda_stream, sync=want, want_hist=want)
+
+    ms = {}
+    for mode in (0, 1):
+        qol.qol_set_sum_precision(mode)
+        try:
+            hist = step(True)
+            for _ in range(warmup):
+                step()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for _ in range(steps):
+                step()
+            e1.record(st)
+            torch.cuda.synchronize()
+        finally:
+            qol.qol_set_sum_precision(0)
+        ms[mode] = e0.elapsed_time(e1) / steps
+    del out, D
+    torch.cuda.empty_cache()
+    ys, q = G.point_charges(G.stellarator(), 8, seed=SEED)
+    ub, ubn = G.harmonic_density(P["sx"], P["snx"], ys, q)
+    uf = qol.qol_direct_farfield(P["sx"], P["snx"], P["sw"], ub, ubn)
+    grf = {}
+    for mode, tag in ((0, "plain"), (1, "chosen")):
+        qol.qol_set_sum_precision(mode)
+        try:
+            un, _, _ = qol.qol_grf_near(npan, nterms, nterms + 2, P["sx"], P["snx"], P["sw"], P["rts"], P["rps"], ub,
+                                        ubn, u=uf)
+        finally:
+            qol.qol_set_sum_precision(0)
+        grf[tag] = float(np.abs(un).max() / np.abs(ubn).max())
+    return {"workload": "stellarator 32x256 quads (16384 triangles), order 12 (nterms 13, hdim 91), "
+                        "1490944 surface-node + 200000 off-surface targets",
+            "near_pairs": pairs, "level_hist": [int(x) for x in hist[1:6]],
+            "geometry_s": round(t_geo, 2), "near_lists_s": round(t_near, 2),
+            "plain": {"ms_per_step": ms[0], "pairs_per_s": pairs / (ms[0] * 1e-3)},
+            "chosen": {"ms_per_step": ms[1], "pairs_per_s": pairs / (ms[1] * 1e-3)},
+            "speedup": ms[0] / ms[1], "grf_error": grf,
+            "grf_error_ratio": grf["chosen"] / grf["plain"],
+            "note": "chosen = FP32 level sums with FP64 accumulation; CSR identical (the same input lists, the same "
+                    "level per pair)"}
+
+
 def learned_form(W, D, out, steps, warmup, conf=0.9):
     """The learned level selector: trained on the GPU on 10^6 pairs of seeded
     surfaces of the batched family (features, plain-walk labels), evaluated on
@@ -527,6 +610,7 @@ def main():
     ap.add_argument("--no-grf", action="store_true", help="skip the per-order GRF sweep")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-selector measurement")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-surface batched configuration")
+    ap.add_argument("--no-config4", action="store_true", help="skip the 32x256-quad (16384-triangle) configuration")
     ap.add_argument("--no-chosen", action="store_true",
                     help="skip the chosen-form (FP32 level sums) comparison at orders 12 and 10")
     ap.add_argument("--panels", type=int, default=0, help="use only the leading N panels (profiling)")
@@ -693,6 +777,9 @@ def main():
         if chosen is not None:
             chosen["grf_error"] = {str(r["order"]): {"plain": r["grf_error_plain"], "chosen": r["grf_error_chosen"]}
                                    for r in grf}
+    c4 = None
+    if rank == 0 and world == 1 and not args.no_config4:
+        c4 = config4(args.steps, 1)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         nthr = os.cpu_count() or 1
@@ -711,7 +798,8 @@ def main():
                 "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": config_dict(W, world), "clocks": clocks, "e2e": e2e,
                 "gpu_launches": LAUNCHES_PER_STEP * args.steps, "roofline": roofline, "cpu_baseline": cpu,
-                "chosen_form": chosen, "learned_form": learned, "batched": batched, "grf_sweep": grf}
+                "chosen_form": chosen, "learned_form": learned, "batched": batched, "grf_sweep": grf,
+                "config4": c4}
         print(json.dumps(line))
     if dist:
         dist.barrier()
