@@ -373,7 +373,7 @@ def learned_form(W, D, out, steps, warmup, conf=0.9):
             "grf_error": {"plain": float(np.abs(un0).max() / np.abs(ubn).max()),
                           "learned": float(np.abs(un1).max() / np.abs(ubn).max())},
             "note": "a prediction replaces the ball-test walk only when it passes the ball check at its level "
-                    "(direct: outside every ball of that level; RRQ: inside a ball of the finest level), so "
+                    "(direct: outside every ball of that level; RRQ: where the walk gives RRQ), so "
                     "no pair gets a level the plain criterion rejects; the walk costs 0.2 ms a step here, so "
                     "the selector does not make this step faster"}
 

@@ -221,8 +221,10 @@ int qol_panel_shape(qol_int nterms, qol_int orderff, qol_int nquad, int* cs, int
 /* Learned level selector (no counterpart in the reference; it stands in for
  * the ball-test level walk of lap3dsdlpmat_levels_r64,
  * patch_refine_mod.f90:516-551).  An MLP 8 -> 64 -> 64 -> 5 on geometry
- * features of each (target, panel) pair predicts the level the plain walk
- * gives (classes 0..3: direct sums on level 1..4; 4: RRQ).
+ * features of each (target, panel) pair predicts a level (classes 0..3:
+ * direct sums on level 1..4; 4: RRQ): the level the plain walk gives (mode 1)
+ * or the lowest level whose row is within a tolerance of the finest level's
+ * (mode 2, error-judged labels).
  * qol_selector_features: the 8 features (FP32, row-major ntcx x 8) and the
  *   plain walk's level (1..5) of every near pair of a getnearquad input;
  * qol_selector_grad: mean cross-entropy and its gradient over n samples with
@@ -236,9 +238,19 @@ int qol_panel_shape(qol_int nterms, qol_int orderff, qol_int nquad, int* cs, int
  * qol_selector_set: mode 1 makes the calls that follow use the selector with
  *   w rounded to BF16 (FP32 accumulation): a prediction with softmax
  *   probability >= conf of a direct level l is used when the target lies
- *   outside every level-l sub-patch ball, an RRQ prediction when it lies
- *   inside a ball of the finest level (else, and below conf, the plain walk
- *   decides); mode 0 restores the plain walk;
+ *   outside every level-l sub-patch ball, an RRQ prediction when the walk
+ *   gives RRQ (else, and below conf, the plain walk
+ *   decides); mode 2: a prediction l below the walk's level is used when the
+ *   two-level check passes (else the walk's level; RRQ pairs of the walk stay
+ *   RRQ, so the selector only lowers levels): the row of level l and of the
+ *   next finer level applied to 4 fixed +-1 vectors, for the single- and
+ *   double-layer kernels, differ by at most tol / 10, single-layer values
+ *   over the panel's diameter sqrt(sum w); mode 0 restores the plain
+ *   walk.  The COO indices never depend on the mode;
+ * qol_selector_set_tol: the mode-2 tolerance (default 1e-8);
+ * qol_selector_force_level: 1..4 computes every pair that the plain walk
+ *   resolves by a direct sum on that level instead (RRQ pairs unchanged; the
+ *   selector is off meanwhile), for error-judged labels; 0 restores the walk;
  * qol_selector_stats: accepted, low-confidence and check-failed pairs since
  *   the last call. */
 #define QOL_SELECTOR_NW 5061
@@ -251,6 +263,8 @@ int qol_selector_grad(qol_int n, const float* feat, const signed char* label, co
 int qol_selector_train(qol_int n, const float* feat, const signed char* label, qol_int epochs, qol_int batch,
                        double lr, unsigned long long seed, float* w, double* loss);
 int qol_selector_set(int mode, const float* w, double conf);
+int qol_selector_set_tol(double tol);
+int qol_selector_force_level(int level);
 int qol_selector_stats(qol_int* counts3);
 /* Wall-clock milestones (ms from the start) of the last
  * qol_getnearquad_lap_rrq call: [0] inputs queued, [1] all panel chunks

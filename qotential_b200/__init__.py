@@ -18,7 +18,7 @@ __all__ = [
     "qol_getnearquad_lap_rrq_dev", "qol_grf_near", "qol_grf_near_range", "qol_direct_farfield",
     "qol_direct_farfield_range", "qol_surface_panels", "qol_interp_matrix", "qol_set_sum_precision",
     "SELECTOR_NW", "qol_selector_features", "qol_selector_grad", "qol_selector_train", "qol_selector_set",
-    "qol_selector_stats", "qol_set_autotune", "qol_panel_shape",
+    "qol_selector_stats", "qol_selector_force_level", "qol_set_autotune", "qol_panel_shape",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -373,12 +373,21 @@ def qol_selector_train(feat, label, w=None, epochs=20, batch=16384, lr=3e-3, see
     return w, loss
 
 
-def qol_selector_set(mode, w=None, conf=0.9):
+def qol_selector_set(mode, w=None, conf=0.9, tol=None):
     """mode 1: the calls that follow take their pair levels from the selector
     (weights w rounded to BF16, softmax confidence >= conf, ball check at the
-    predicted level); mode 0: the plain ball-test walk."""
+    predicted level); mode 2: the same with the two-level check at tolerance
+    tol (error-judged labels); mode 0: the plain ball-test walk."""
+    if tol is not None:
+        _check(lib().qol_selector_set_tol(C.c_double(tol)))
     wp = None if w is None else np.ascontiguousarray(w, dtype=np.float32)
     _check(lib().qol_selector_set(C.c_int(int(mode)), _vp(wp), C.c_double(conf)))
+
+
+def qol_selector_force_level(level):
+    """1..4: the calls that follow compute every pair that the plain walk
+    resolves by a direct sum on that level (RRQ pairs unchanged); 0: the walk."""
+    _check(lib().qol_selector_force_level(C.c_int(int(level))))
 
 
 def qol_selector_stats():

@@ -100,6 +100,8 @@ int g_autotune = 1;      /* measure the panel kernel's cluster size once per ord
  * device, the confidence threshold, and the decision counters of the calls */
 int g_sel_mode = 0;
 float g_sel_conf = 0.9f;
+double g_sel_tol = 1e-8;  /* mode 2: the two-level check's row-error tolerance */
+int g_force_level = 0;    /* labelling runs: direct pairs all on this level (0: off) */
 float* g_sel_w = nullptr;
 unsigned long long* g_sel_cnt = nullptr; /* accepted, low confidence, check failed, pairs */
 double g_ktime[QOL_NPHASE] = {};
@@ -178,6 +180,21 @@ int order_tables(int nterms, int orderff, int nquad, OrderCache** out) {
         std::memcpy(&h, &rh[fe], 4);
         rl[fe] = tf32(f - h);
       }
+    /* the selector check's sketch vectors on this level's nodes: I_l v for 4
+     * fixed +-1 vectors v over the hd node values (a hash of (node, vector)) */
+    auto sign = [](int k, int v) {
+      uint32_t h = (uint32_t)(4 * k + v + 1) * 0x9E3779B1u;
+      h ^= h >> 15; h *= 0x85EBCA77u; h ^= h >> 13;
+      return (h & 1u) ? -1.0 : 1.0;
+    };
+    std::vector<double> sk((size_t)L.n * 4, 0.0);
+    for (long long i = 0; i < L.n; ++i)
+      for (int v = 0; v < 4; ++v) {
+        double a = 0.0;
+        for (int k = 0; k < hd; ++k) a += L.interp[i + (size_t)L.n * k] * sign(k, v);
+        sk[(size_t)i * 4 + v] = a;
+      }
+    T.sk[l] = C->up(sk);
     T.ncw = ncw;
     T.interp[l] = C->up(rp);
     T.interp_hi[l] = C->up(rh);
@@ -307,6 +324,7 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
   OrderTab T = C->T;
   T.dist = J.distff;
   T.sum_fp32 = g_sum_precision == 1;
+  T.force_level = g_force_level;
   const int hd = T.hd, npan = J.npan, nq = T.nquad, nbd = 3 * nq;
   const long long ntcx = J.ntcx;
   /* workspace size */
@@ -362,8 +380,9 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
   rec(0);
   CK(qol_launch_levels(T, J.P, W, npan, st));
   rec(1);
-  if (g_sel_mode == 1 && g_sel_w) { /* confident, checked predictions first; the plain walk for the rest */
-    CK(qol_launch_sel_infer(T, J.P, J.Q, W, G, npan, g_sel_w, g_sel_conf, g_sel_cnt, st));
+  if (g_sel_mode && g_sel_w && !g_force_level) { /* confident, checked predictions first; the walk for the rest */
+    CK(qol_launch_sel_infer(T, J.P, J.Q, W, G, npan, g_sel_w, g_sel_conf, g_sel_cnt, g_sel_mode, st));
+    if (g_sel_mode == 2) CK(qol_launch_sel_check(T, J.P, J.Q, W, G, npan, g_sel_tol, g_sel_cnt, st));
     CK(qol_launch_classify(T, J.Q, W, G, npan, st, 1));
   } else {
     CK(qol_launch_classify(T, J.Q, W, G, npan, st));
@@ -976,12 +995,14 @@ int qol_selector_train(qol_int n, const float* feat, const signed char* label, q
 }
 
 /* mode 0: plain ball-test walk; mode 1: the learned selector with weights w
- * (FP32, used rounded to BF16) and confidence threshold conf in (0, 1] */
+ * (FP32, used rounded to BF16), confidence threshold conf in (0, 1] and the
+ * ball check; mode 2: the same with the two-level check at the tolerance of
+ * qol_selector_set_tol */
 int qol_selector_set(int mode, const float* w, double conf) {
   std::lock_guard<std::recursive_mutex> g(g_mu);
   if (mode == 0) { g_sel_mode = 0; return 0; }
-  if (mode != 1 || !w || !(conf > 0.0 && conf <= 1.0))
-    return fail(QOL_ERR_ARG, "qol_selector_set: mode 0 or 1, weights and a confidence in (0, 1]");
+  if ((mode != 1 && mode != 2) || !w || !(conf > 0.0 && conf <= 1.0))
+    return fail(QOL_ERR_ARG, "qol_selector_set: mode 0, 1 or 2, weights and a confidence in (0, 1]");
   std::vector<float> wb(QOL_SEL_NW);
   for (int i = 0; i < QOL_SEL_NW; ++i) { /* round to nearest even BF16 */
     uint32_t u;
@@ -997,8 +1018,27 @@ int qol_selector_set(int mode, const float* w, double conf) {
                    (rc = ck(cudaMemset(g_sel_cnt, 0, sizeof(unsigned long long) * 4)))))
     return rc;
   if ((rc = ck(cudaMemcpy(g_sel_w, wb.data(), sizeof(float) * QOL_SEL_NW, cudaMemcpyHostToDevice)))) return rc;
-  g_sel_mode = 1;
+  g_sel_mode = mode;
   g_sel_conf = (float)conf;
+  return 0;
+}
+
+/* the two-level check's tolerance on a row's error (single-layer rows over
+ * the panel's diameter, double-layer rows as they are; 1-norm scale) */
+int qol_selector_set_tol(double tol) {
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  if (!(tol > 0.0 && tol < 1.0)) return fail(QOL_ERR_ARG, "qol_selector_set_tol: tol in (0, 1)");
+  g_sel_tol = tol;
+  return 0;
+}
+
+/* labelling: level 1..4 puts every pair that the plain walk resolves by a
+ * direct sum on that level in the calls that follow (RRQ pairs unchanged,
+ * the selector off); 0 restores the walk */
+int qol_selector_force_level(int level) {
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  if (level < 0 || level > 4) return fail(QOL_ERR_ARG, "qol_selector_force_level: level 0..4");
+  g_force_level = level;
   return 0;
 }
 

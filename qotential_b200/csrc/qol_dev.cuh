@@ -13,6 +13,19 @@
 #define QOL_MAXNQ 24      /* max nquad */
 #define QOL_PI 3.14159265358979323846264338327950288
 
+/* single-layer kernels S = w/(4 pi r), D = w (x-y).n/(4 pi r^3) of one source
+ * node (zero when |x-y|^2 <= 1e-28, as the reference's sdlpmat) */
+__device__ __forceinline__ void sdl_kernel(double dx, double dy, double dz, double nx, double ny, double nz, double w4,
+                                           double& s, double& d) {
+  const double rr = dx * dx + dy * dy + dz * dz;
+  s = 0.0; d = 0.0;
+  if (rr > 1.0e-28) {
+    const double ri = rsqrt(rr);
+    s = w4 * ri;
+    d = s * ri * ri * (dx * nx + dy * ny + dz * nz);
+  }
+}
+
 struct cd {
   double re, im;
 };

@@ -113,6 +113,7 @@ __global__ void __launch_bounds__(128) k_classify(OrderTab T, PairIn Q, LevelWS 
         }
         if (outside) { lv = l + 1; break; }
       }
+      if (T.force_level > 0 && !pre && lv <= T.nlevel) lv = T.force_level;
       G.level[p0 + t] = (signed char)lv;
       atomicAdd(&cnt[lv], 1);
     }
@@ -178,18 +179,6 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
                : "d"(a), "d"(b));
 }
 
-/* single-layer kernels S = w/(4 pi r), D = w (x-y).n/(4 pi r^3) of one source
- * node (zero when |x-y|^2 <= 1e-28, as the reference's sdlpmat) */
-__device__ __forceinline__ void sdl_kernel(double dx, double dy, double dz, double nx, double ny, double nz, double w4,
-                                           double& s, double& d) {
-  const double rr = dx * dx + dy * dy + dz * dz;
-  s = 0.0; d = 0.0;
-  if (rr > 1.0e-28) {
-    const double ri = rsqrt(rr);
-    s = w4 * ri;
-    d = s * ri * ri * (dx * nx + dy * ny + dz * nz);
-  }
-}
 
 /* ===================================================================== */
 /* K1: refined levels of every panel                                     */

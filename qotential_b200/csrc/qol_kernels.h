@@ -29,6 +29,8 @@ struct OrderTab {
   const double* tginv;    /* nquad x nquad: 1/(tgl[i] - tgl[i-k-1]) at [k*nquad + i] */
   int sum_fp32;           /* 1: level sums in FP32 on the 3xTF32 tensor path (precision variant) */
   int xsteps;
+  const double* sk[4];    /* n_l x 4: the selector check's sketch vectors on the level nodes (I_l v, v = +-1) */
+  int force_level;        /* 1..nlevel: every pair the walk resolves by a direct sum takes this level (labels) */
 };
 
 /* panel geometry (reference layouts: sx(3,nsrc) etc.) */
@@ -92,9 +94,15 @@ cudaError_t qol_launch_classify(const OrderTab& T, const PairIn& Q, const LevelW
 #define QOL_SEL_C 5
 #define QOL_SEL_NW (QOL_SEL_F * QOL_SEL_H + QOL_SEL_H + QOL_SEL_H * QOL_SEL_H + QOL_SEL_H + QOL_SEL_H * QOL_SEL_C + QOL_SEL_C)
 cudaError_t qol_launch_sel_features(int hd, const PanelIn& P, const PairIn& Q, int npan, float* feat, cudaStream_t st);
+/* mode 1: a direct-level prediction is kept when the target is outside every
+ * ball of that level; mode 2: it is marked a candidate (G.level = -l) for the
+ * two-level check of qol_launch_sel_check */
 cudaError_t qol_launch_sel_infer(const OrderTab& T, const PanelIn& P, const PairIn& Q, const LevelWS& W,
                                  const PairWS& G, int npan, const float* wbf, float conf, unsigned long long* cnt,
-                                 cudaStream_t st);
+                                 int mode, cudaStream_t st);
+#define QOL_SEL_BETA 10.0 /* safety factor of the two-level check */
+cudaError_t qol_launch_sel_check(const OrderTab& T, const PanelIn& P, const PairIn& Q, const LevelWS& W,
+                                 const PairWS& G, int npan, double tol, unsigned long long* cnt, cudaStream_t st);
 size_t qol_sel_grad_smem();
 cudaError_t qol_launch_sel_grad(const float* feat, const signed char* lab, const int* idx, long long n0, long long n1,
                                 const float* w, float* slot, double* sloss, int nslot, cudaStream_t st);

@@ -1,12 +1,28 @@
 /* Learned level selector (no reference counterpart): an MLP 8 -> 64 -> 64 -> 5
- * on per-pair geometry features predicts the level the plain ball tests of
- * lap3dsdlpmat_levels_r64 (patch_refine_mod.f90:516-551) give a (target,
- * panel) pair: classes 0..3 = direct sums on refined level 1..4, class 4 =
- * RRQ.  A confident prediction of a direct level l is used only when the
- * target lies outside every level-l sub-patch ball (the plain criterion at
- * that level), an RRQ prediction only when the target lies inside a ball of
- * the finest level (RRQ is accurate near the panel); other pairs keep the
- * plain walk over the levels.
+ * on per-pair geometry features predicts a (target, panel) pair's level:
+ * classes 0..3 = direct sums on refined level 1..4, class 4 = RRQ.  Two
+ * label sets and two acceptance rules (the mode):
+ *   mode 1 - labels are the levels the plain ball tests of
+ *     lap3dsdlpmat_levels_r64 (patch_refine_mod.f90:516-551) give; a
+ *     confident direct prediction l is used only when the target lies
+ *     outside every level-l sub-patch ball (the plain criterion at that
+ *     level), an RRQ prediction only when the walk gives RRQ;
+ *   mode 2 - labels are the lowest level whose row is within a tolerance of
+ *     the finest level's, capped at the walk's level (error-judged,
+ *     qotential_b200/selector.py); a confident prediction l below the walk's
+ *     level is used only when the two-level check below estimates its row
+ *     error within that tolerance; otherwise the walk's level is kept, and
+ *     pairs the walk sends to RRQ stay RRQ (close to the panel the direct
+ *     sums may converge to another value than RRQ's).
+ * Pairs of low confidence, or whose check fails, keep the plain walk.
+ *
+ * The two-level check (k_sel_check): sketch sums s_v = sum_q K(x, y_q) w_q
+ * (I_l v)_q over the level-l nodes and over the nodes of level l + 1, for the
+ * single- and double-layer kernels and 4 fixed +-1 vectors v over the
+ * panel's node values, so s_v is the row of that level applied to v.  The
+ * difference e = max_v max(|dS_v| / D, |dD_v|) (D = sqrt(sum w), the panel's
+ * diameter; single-layer rows scale with length) estimates the level-l row's
+ * error; the prediction passes when QOL_SEL_BETA e <= tol.
  *
  * Features (FP32, from a per-panel descriptor computed in FP64 with fixed
  * reduction order): centroid c = sum w y / sum w, diameter D = sqrt(sum w),
@@ -25,6 +41,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <cstdint>
+#include "qol_dev.cuh"
 #include "qol_kernels.h"
 
 namespace {
@@ -163,7 +180,7 @@ __device__ __forceinline__ void sel_forward(const float* w, const float* xin, fl
  * (1..nlevel+1) or 0 (the plain walk decides); counters [accepted, low
  * confidence, check failed] */
 __global__ void __launch_bounds__(128) k_sel_infer(OrderTab T, PanelIn P, PairIn Q, LevelWS W, PairWS G,
-                                                   const float* wbf, float conf, unsigned long long* cnt) {
+                                                   const float* wbf, float conf, unsigned long long* cnt, int mode) {
   const int pan = blockIdx.x, hd = T.hd;
   extern __shared__ double ssm[];
   double* dsc = ssm;
@@ -188,22 +205,36 @@ __global__ void __launch_bounds__(128) k_sel_infer(OrderTab T, PanelIn P, PairIn
 #pragma unroll
     for (int k = 0; k < NC; ++k) den += __expf(z[k] - z[best]);
     const float prob = 1.0f / den;
-    int lv = 0;
-    if (prob < conf) ++lo;
-    else {
-      /* direct level l: outside every level-l ball; RRQ: inside a ball of the
-       * finest level (RRQ is accurate near the panel, not far from it) */
-      const bool rrq = best >= T.nlevel;
-      const int l = rrq ? T.nlevel - 1 : best; /* level index of the balls tested */
+    /* outside every ball of level index l (the plain criterion at that level) */
+    auto outside = [&](int l) {
       const double* qp = W.sub[l] + (size_t)pan * T.nsub[l] * 4;
-      bool outside = true;
       for (int s = 0; s < T.nsub[l]; ++s) {
         const double b0 = qp[4 * s] - x[0], b1 = qp[4 * s + 1] - x[1], b2 = qp[4 * s + 2] - x[2];
-        if (b0 * b0 + b1 * b1 + b2 * b2 < qp[4 * s + 3]) { outside = false; break; }
+        if (b0 * b0 + b1 * b1 + b2 * b2 < qp[4 * s + 3]) return false;
       }
-      if (outside != rrq) lv = rrq ? T.nlevel + 1 : l + 1, ++a;
+      return true;
+    };
+    /* the walk's level: RRQ (nlevel + 1) when inside a ball at every level */
+    auto walk = [&]() {
+      for (int l = 0; l < T.nlevel; ++l)
+        if (outside(l)) return l + 1;
+      return T.nlevel + 1;
+    };
+    int lv = 0;
+    if (prob < conf) ++lo;
+    else if (mode == 2) {
+      /* a level below the walk's, for the two-level check; the walk's own
+       * level otherwise (RRQ pairs stay RRQ: near the panel the direct sums
+       * can converge to a value other than RRQ's, which no check of their
+       * convergence sees) */
+      const int w = walk();
+      if (w <= T.nlevel && best + 1 < w) lv = -(best + 1);
+      else lv = w, ++a;
+    } else if (best >= T.nlevel) { /* RRQ: when the walk gives it */
+      if (walk() > T.nlevel) lv = T.nlevel + 1, ++a;
       else ++ck;
-    }
+    } else if (outside(best)) lv = best + 1, ++a;
+    else ++ck;
     G.level[p0 + t] = (signed char)lv;
   }
   atomicAdd(&sc[0], (unsigned long long)a);
@@ -211,6 +242,120 @@ __global__ void __launch_bounds__(128) k_sel_infer(OrderTab T, PanelIn P, PairIn
   atomicAdd(&sc[2], (unsigned long long)ck);
   __syncthreads();
   if (threadIdx.x < 3) atomicAdd(&cnt[threadIdx.x], sc[threadIdx.x]);
+}
+
+/* the two-level check of the direct-level candidates (G.level = -l, l =
+ * 1..nlevel-1): accepted -> l, rejected -> 0 (the plain walk); counters
+ * [accepted, -, check failed].  One CTA per panel; per level, candidates are
+ * gathered SC_T at a time in target order, one thread each, the nodes and
+ * sketch values of both levels streamed through shared-memory tiles; each
+ * thread sums its nodes in node order (deterministic). */
+constexpr int SC_T = 128, SC_NT = 64;
+__global__ void __launch_bounds__(SC_T) k_sel_check(OrderTab T, PanelIn P, PairIn Q, LevelWS W, PairWS G, double tol,
+                                                    unsigned long long* cnt) {
+  const int pan = blockIdx.x, hd = T.hd;
+  const long long p0 = Q.tcxi[pan] - 1, m = Q.tcxi[pan + 1] - Q.tcxi[pan];
+  if (m <= 0) return;
+  __shared__ double nd[11 * SC_NT]; /* x, y, z, nx, ny, nz, w, then the 4 sketch values, SC_NT nodes each */
+  __shared__ int cand[2 * SC_T];
+  __shared__ int ncand, wc[SC_T / 32];
+  __shared__ double sdiam;
+  __shared__ unsigned long long sc[2];
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  if (tid < 32) {
+    double sw = 0.0;
+    for (int j = lane; j < hd; j += 32) sw += P.sw[(size_t)pan * hd + j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sw += __shfl_xor_sync(0xffffffffu, sw, o);
+    if (lane == 0) sdiam = sqrt(sw);
+  }
+  if (tid < 2) sc[tid] = 0;
+  __syncthreads();
+  const double Dp = sdiam, i4p = 1.0 / (4.0 * QOL_PI);
+  for (int l = 1; l < T.nlevel; ++l) { /* candidates lie below the walk's level, so below the finest */
+    const int la = l - 1, lb = l;
+    if (tid == 0) ncand = 0;
+    __syncthreads();
+    for (long long w0 = 0;; w0 += SC_T) {
+      const bool more = w0 < m;
+      if (more) { /* append this window's candidates in target order */
+        const long long t = w0 + tid;
+        const bool c = t < m && G.level[p0 + t] == -l;
+        const unsigned b = __ballot_sync(0xffffffffu, c);
+        if (lane == 0) wc[wid] = __popc(b);
+        __syncthreads();
+        int before = ncand;
+        for (int w = 0; w < wid; ++w) before += wc[w];
+        if (c) cand[before + __popc(b & ((1u << lane) - 1u))] = (int)t;
+        __syncthreads();
+        if (tid == 0) {
+          int tot = 0;
+          for (int w = 0; w < SC_T / 32; ++w) tot += wc[w];
+          ncand += tot;
+        }
+        __syncthreads();
+      }
+      const int nc = ncand;
+      if (nc >= SC_T || (!more && nc > 0)) {
+        const int nb = min(nc, SC_T);
+        const int my = tid < nb ? cand[tid] : -1;
+        double x0 = 0.0, x1 = 0.0, x2 = 0.0;
+        if (my >= 0) {
+          const double* x = Q.tcx + 3 * (p0 + my);
+          x0 = x[0]; x1 = x[1]; x2 = x[2];
+        }
+        double S[2][4] = {}, Dd[2][4] = {};
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+          const int lv = s ? lb : la, n = T.n[lv];
+          const double* node = W.node[lv] + (size_t)pan * n * 7;
+          const double* skv = T.sk[lv];
+          for (int n0 = 0; n0 < n; n0 += SC_NT) {
+            __syncthreads();
+            for (int e = tid; e < 11 * SC_NT; e += SC_T) {
+              const int f = e / SC_NT, q = e % SC_NT, i = n0 + q;
+              nd[e] = i < n ? (f < 7 ? node[(size_t)f * n + i] : skv[(size_t)i * 4 + f - 7]) : 0.0;
+            }
+            __syncthreads();
+            if (my >= 0) {
+              const int nn = min(SC_NT, n - n0);
+              for (int q = 0; q < nn; ++q) {
+                double sv, dv;
+                sdl_kernel(x0 - nd[q], x1 - nd[SC_NT + q], x2 - nd[2 * SC_NT + q], nd[3 * SC_NT + q],
+                           nd[4 * SC_NT + q], nd[5 * SC_NT + q], nd[6 * SC_NT + q] * i4p, sv, dv);
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                  S[s][v] = fma(sv, nd[(7 + v) * SC_NT + q], S[s][v]);
+                  Dd[s][v] = fma(dv, nd[(7 + v) * SC_NT + q], Dd[s][v]);
+                }
+              }
+            }
+          }
+        }
+        if (my >= 0) {
+          double e = 0.0;
+#pragma unroll
+          for (int v = 0; v < 4; ++v) e = fmax(e, fmax(fabs(S[0][v] - S[1][v]) / Dp, fabs(Dd[0][v] - Dd[1][v])));
+          const bool ok = QOL_SEL_BETA * e <= tol;
+          G.level[p0 + my] = (signed char)(ok ? l : 0);
+          atomicAdd(&sc[ok ? 0 : 1], 1ull);
+        }
+        __syncthreads(); /* every thread has read its candidate: move the rest to the front */
+        const int rest = nc - nb;
+        const int keep = tid < rest ? cand[nb + tid] : 0;
+        __syncthreads();
+        if (tid < rest) cand[tid] = keep;
+        if (tid == 0) ncand = rest;
+        __syncthreads();
+      }
+      if (!more && ncand == 0) break;
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    atomicAdd(&cnt[0], sc[0]);
+    atomicAdd(&cnt[2], sc[1]);
+  }
 }
 
 /* training: one CTA of 256 samples, forward and backward; its partial
@@ -364,10 +509,17 @@ cudaError_t qol_launch_sel_features(int hd, const PanelIn& P, const PairIn& Q, i
 
 cudaError_t qol_launch_sel_infer(const OrderTab& T, const PanelIn& P, const PairIn& Q, const LevelWS& W,
                                  const PairWS& G, int npan, const float* wbf, float conf, unsigned long long* cnt,
-                                 cudaStream_t st) {
+                                 int mode, cudaStream_t st) {
   if (npan <= 0) return cudaSuccess;
   const size_t smem = sizeof(double) * (16 + 3 * T.hd) + sizeof(float) * QOL_SEL_NW;
-  k_sel_infer<<<npan, 128, smem, st>>>(T, P, Q, W, G, wbf, conf, cnt);
+  k_sel_infer<<<npan, 128, smem, st>>>(T, P, Q, W, G, wbf, conf, cnt, mode);
+  return cudaGetLastError();
+}
+
+cudaError_t qol_launch_sel_check(const OrderTab& T, const PanelIn& P, const PairIn& Q, const LevelWS& W,
+                                 const PairWS& G, int npan, double tol, unsigned long long* cnt, cudaStream_t st) {
+  if (npan <= 0) return cudaSuccess;
+  k_sel_check<<<npan, SC_T, 0, st>>>(T, P, Q, W, G, tol, cnt);
   return cudaGetLastError();
 }
 

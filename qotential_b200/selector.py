@@ -1,20 +1,81 @@
 """Training data and training for the learned level selector (no reference
 counterpart): seeded surfaces of the batched family, their near pairs
 (on-surface nodes plus off-surface points at seeded normal offsets), each
-pair's 8 features and the level the plain ball-test walk gives it, and Adam
-on the GPU (qol_selector_train).  The labels are the plain walk's own
-decisions, so a selector trained here reproduces the plain walk where it is
-confident; the library accepts a prediction only after the ball check at the
-predicted level."""
+pair's 8 features and a label, and Adam on the GPU (qol_selector_train).
+
+Two label sets.  "walk": the level the plain ball-test walk gives the pair,
+so a selector trained on them reproduces the walk where it is confident (the
+library's mode 1).  "error": the lowest level whose row is within a
+tolerance of the finest level's (error_levels: every direct pair computed on
+each level by qol_selector_force_level), capped at the walk's level, RRQ for
+the pairs the walk sends to RRQ; the library's mode 2 uses a prediction below
+the walk's level after its two-level check."""
 import numpy as np
 
 from . import geometry as G
-from . import qol_selector_features, qol_selector_train
+from . import qol_getnearquad_lap_rrq_dev, qol_selector_features, qol_selector_force_level, qol_selector_train
 
 
-def training_set(n_pairs=1_000_000, seed=11, orders=(4, 6, 8, 10, 12), noff=5000, max_grid=(8, 32)):
+def error_levels(npan, nterms, P, tcx, tcxrow, tcxi, walk_level, distff=1.4):
+    """(ntcx, 4) row errors of levels 1..4 against level 4 per near pair:
+    max(1-norm of the single-layer row difference / D, 1-norm of the
+    double-layer row difference), D = sqrt(panel area) (the check's scale);
+    zero for RRQ pairs (walk level 5).  Computed on the GPU from four
+    getnearquad runs with every direct pair forced onto one level."""
+    import torch
+    dev = torch.device("cuda", torch.cuda.current_device())
+    hd = nterms * (nterms + 1) // 2
+    nq = nterms + 2
+    t = lambda a, dt=torch.float64: torch.as_tensor(np.ascontiguousarray(a), dtype=dt).to(dev)
+    D = {k: t(P[k]) for k in ("sx", "snx", "sw", "rts", "rps")}
+    xi = np.asarray(tcxi, np.int64)
+    ntcx = int(xi[-1] - 1)
+    tx, row, xid = t(tcx), t(tcxrow, torch.int64), t(xi, torch.int64)
+    nnz = ntcx * hd
+    out = (torch.empty(nnz, dtype=torch.int64, device=dev), torch.empty(nnz, dtype=torch.int64, device=dev),
+           torch.empty(nnz, dtype=torch.float64, device=dev), torch.empty(nnz, dtype=torch.float64, device=dev))
+    m = torch.as_tensor(np.diff(xi), device=dev)
+    pan = torch.repeat_interleave(torch.arange(npan, device=dev), hd * m)      # panel of each COO entry
+    local = torch.arange(nnz, device=dev) - (xid[:-1] - 1)[pan] * hd
+    pair = (xid[:-1] - 1)[pan] + local % m[pan]                               # block column-major order
+    diam = torch.sqrt(D["sw"].reshape(npan, hd).sum(1))[pan]
+    err = torch.zeros((ntcx, 4), dtype=torch.float64, device=dev)
+
+    def run(level):
+        qol_selector_force_level(level)
+        qol_getnearquad_lap_rrq_dev(npan, nterms, nq, D["sx"], D["snx"], D["sw"], D["rts"], D["rps"], tx, row, xid,
+                                    nq, distff, 30, out, stream=torch.cuda.current_stream().cuda_stream)
+
+    try:
+        run(4)
+        vs4, vd4 = out[2].clone(), out[3].clone()
+        for lv in (1, 2, 3):
+            run(lv)
+            es = torch.zeros(ntcx, dtype=torch.float64, device=dev).index_add_(0, pair, (out[2] - vs4).abs() / diam)
+            ed = torch.zeros(ntcx, dtype=torch.float64, device=dev).index_add_(0, pair, (out[3] - vd4).abs())
+            err[:, lv - 1] = torch.maximum(es, ed)
+    finally:
+        qol_selector_force_level(0)
+    e = err.cpu().numpy()
+    e[np.asarray(walk_level) > 4] = 0.0
+    return e
+
+
+def error_labels(err, walk_level, tol):
+    """classes 0..4: the lowest level (0-based) whose row error is <= tol,
+    capped at the walk's level (the library lowers the walk's level, never
+    raises it); 4 (RRQ) where the walk gives RRQ"""
+    ok = np.asarray(err) <= tol
+    walk = np.asarray(walk_level).astype(np.int64)
+    low = np.minimum(np.where(ok.any(1), ok.argmax(1), 3), walk - 1)
+    return np.where(walk > 4, 4, low).astype(np.int8)
+
+
+def training_set(n_pairs=1_000_000, seed=11, orders=(4, 6, 8, 10, 12), noff=5000, max_grid=(8, 32), labels="walk",
+                 tol=1e-8):
     """(features (n, 8) float32, classes (n,) int8, surfaces used) from seeded
-    family surfaces until at least n_pairs pairs are collected"""
+    family surfaces until at least n_pairs pairs are collected; labels "walk"
+    or "error" (at tolerance tol)"""
     rng = np.random.default_rng(seed)
     feats, labs, used = [], [], 0
     total = 0
@@ -32,7 +93,10 @@ def training_set(n_pairs=1_000_000, seed=11, orders=(4, 6, 8, 10, 12), noff=5000
         f, lev = qol_selector_features(npan, nterms, nterms + 2, P["sx"], P["snx"], P["sw"], P["rts"], P["rps"], tcx,
                                        tcxrow, tcxi, nterms + 2)
         feats.append(f)
-        labs.append((lev - 1).astype(np.int8))
+        if labels == "error":
+            labs.append(error_labels(error_levels(npan, nterms, P, tcx, tcxrow, tcxi, lev), lev, tol))
+        else:
+            labs.append((lev - 1).astype(np.int8))
         total += f.shape[0]
         used += 1
     return np.concatenate(feats), np.concatenate(labs), used

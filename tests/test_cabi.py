@@ -105,11 +105,20 @@ def test_getnearquad_out_checked(qol):
 def test_selector_arguments_checked(qol):
     """selector entry points reject bad arguments before any device work"""
     w = np.zeros(qol.SELECTOR_NW, np.float32)
-    for mode, conf in ((2, 0.9), (1, 1.5), (1, 0.0)):
+    for mode, conf in ((3, 0.9), (1, 1.5), (2, 0.0)):
         with pytest.raises(qol.QolError) as e:
             qol.qol_selector_set(mode, w, conf)
         assert e.value.code == 8
     qol.qol_selector_set(0)  # back to the plain walk: no device needed
+    for tol in (0.0, -1e-8, 1.0):
+        with pytest.raises(qol.QolError) as e:
+            qol.qol_selector_set(0, tol=tol)
+        assert e.value.code == 8
+    for level in (-1, 5):
+        with pytest.raises(qol.QolError) as e:
+            qol.qol_selector_force_level(level)
+        assert e.value.code == 8
+    qol.qol_selector_force_level(0)
     f = np.zeros((4, 8), np.float32)
     with pytest.raises(qol.QolError) as e:
         qol.qol_selector_grad(f, np.array([0, 1, 7, 2]), w)  # class out of range

@@ -3,7 +3,7 @@ the training gradient against the oracle's numpy restatement (FP32 vs FP64),
 deterministic training that learns the plain walk's levels, and the learned
 form of qol_getnearquad_lap_rrq against the plain one (a prediction is used
 only after the ball check at its level, so no pair gets a level the plain walk
-would reject, and RRQ only near the panel)."""
+would reject, and RRQ only where the walk gives it)."""
 import numpy as np
 import pytest
 
