@@ -61,6 +61,9 @@ def workload(rank=0, world=1, panels=0, order=ORDER):
 # kernels of one qol_getnearquad_lap_rrq_dev call: level nodes, level subs, classify, scan, direct,
 # rrq_pairs, rrq_panel, rrq_ssq, rrq_side, rrq_geom, rrq_moments, rrq_apply, coo_index
 LAUNCHES_PER_STEP = 13
+# the library's timed phases (qol_kernel_times)
+PHASES = ["levels", "classify", "direct", "rrq_panel", "rrq_ssq", "rrq_geom", "rrq_moments", "rrq_apply",
+          "coo_index", "select"]
 
 
 def xlate_terms(L):
@@ -218,15 +221,124 @@ def forms_compare(W, steps, warmup, D=None, out=None):
     return res
 
 
-def config4(steps=2, warmup=1):
+SEL_TOL = 1e-8   # the error-judged selector's row tolerance at order 12 (the walk's own rows reach ~1e-7)
+SEL_CONF = 0.8   # the selector's softmax confidence threshold (0.5 checks twice the pairs for little more gain)
+# form: (qol_set_sum_precision, qol_selector_set mode)
+FORMS = {"plain": (0, 0), "fp32_sums": (1, 0), "learned": (0, 2), "chosen": (1, 2)}
+
+
+def set_form(form, w=None):
+    import qotential_b200 as qol
+    prec, sel = FORMS[form]
+    qol.qol_set_sum_precision(prec)
+    if sel:
+        qol.qol_selector_set(sel, w, SEL_CONF, tol=SEL_TOL)
+    else:
+        qol.qol_selector_set(0)
+
+
+def level_nodes(nterms, nquad):
+    import ctypes as C
+    from qotential_b200 import lib
+    n4 = np.zeros(4, np.int64); s4 = np.zeros(4, np.int64)
+    lib().qol_level_sizes(C.c_longlong(nterms), C.c_longlong(nquad), C.c_void_p(n4.ctypes.data),
+                          C.c_void_p(s4.ctypes.data))
+    return n4
+
+
+def time_forms(npan, nterms, pairs, D, out, w, steps, warmup, forms=tuple(FORMS)):
+    """The device step (qol_getnearquad_lap_rrq_dev, inputs and outputs
+    resident) in each form: ms/step by CUDA events on the launching stream,
+    the level histogram, the level-sum work (level nodes x pairs) and, against
+    the plain form, the speedup and each row's error (sparsevs, sparsevd)"""
+    import ctypes as C
+    import torch
+    import qotential_b200 as qol
+    L = qol.lib()
+    st = torch.cuda.current_stream()
+    nq = nterms + 2
+    n4 = level_nodes(nterms, nq)
+
+    def step(want=False):
+        return qol.qol_getnearquad_lap_rrq_dev(npan, nterms, nq, D["sx"], D["snx"], D["sw"], D["rts"], D["rps"],
+                                               D["tcx"], D["tcxrow"], D["tcxi"], nq, 1.4, 30, out,
+                                               stream=st.cuda_stream, sync=want, want_hist=want)
+
+    res, plain = {}, None
+    try:
+        for f in forms:
+            set_form(f, w)
+            hist = step(True)
+            for _ in range(warmup):
+                step()
+            torch.cuda.synchronize()
+            qol.qol_selector_stats()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for _ in range(steps):
+                step()
+            e1.record(st)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / steps
+            r = {"ms_per_step": ms, "pairs_per_s": pairs / (ms * 1e-3), "level_hist": [int(x) for x in hist[1:6]],
+                 "level_work": int(n4 @ hist[1:5])}
+            if FORMS[f][1]:
+                r["decisions_per_step"] = {k: v // steps for k, v in qol.qol_selector_stats().items()}
+            ph = np.zeros(len(PHASES))  # per-phase device ms of one more step
+            L.qol_kernel_times(C.c_int(1), None, None)
+            step()
+            torch.cuda.synchronize()
+            L.qol_kernel_times(C.c_int(-1), C.c_void_p(ph.ctypes.data), None)
+            L.qol_kernel_times(C.c_int(0), None, None)
+            r["phase_ms"] = {k: round(float(v), 3) for k, v in zip(PHASES, ph)}
+            if f == "plain":
+                plain = (out[2].clone(), out[3].clone())
+            elif plain is not None:
+                r["row_error_vs"] = row_errors(out[0], plain[0], out[2])
+                r["row_error_vd"] = row_errors(out[0], plain[1], out[3])
+            res[f] = r
+    finally:
+        set_form("plain")
+    del plain
+    torch.cuda.empty_cache()
+    if "plain" in res:
+        for f, r in res.items():
+            r["speedup"] = res["plain"]["ms_per_step"] / r["ms_per_step"]
+            r["level_work_ratio"] = r["level_work"] / res["plain"]["level_work"]
+    return res
+
+
+def grf_forms(P, nterms, w, forms=tuple(FORMS)):
+    """GRF identity error max |S[du/dn] - D[u]| / max |du/dn| on the surface
+    nodes (8 point charges on |y| = 6, Direct far field on the GPU) with the
+    near phase (qol_grf_near) in each form"""
+    import qotential_b200 as qol
+    from qotential_b200 import geometry as G
+    hd = nterms * (nterms + 1) // 2
+    npan = P["sw"].size // hd
+    ys, q = G.point_charges(G.stellarator(), 8, seed=SEED)
+    ub, ubn = G.harmonic_density(P["sx"], P["snx"], ys, q)
+    uf = qol.qol_direct_farfield(P["sx"], P["snx"], P["sw"], ub, ubn)
+    out = {}
+    try:
+        for f in forms:
+            set_form(f, w)
+            un, _, _ = qol.qol_grf_near(npan, nterms, nterms + 2, P["sx"], P["snx"], P["sw"], P["rts"], P["rps"], ub,
+                                        ubn, u=uf)
+            out[f] = float(np.abs(un).max() / np.abs(ubn).max())
+    finally:
+        set_form("plain")
+    return out
+
+
+def config4(w, steps=2, warmup=1):
     """The benchmark set's largest configuration: the same stellarator refined to
     32 x 256 quads (16,384 triangles, 1,490,944 surface nodes) at order 12
     (nterms 13), targets all surface nodes + 200,000 seeded off-surface points
     (the workload's distance law), geometry from the GPU generator.  The device
     step (inputs and the COO outputs resident, about 51 GB) in the plain FP64
-    form and in the chosen form (FP32 level sums, qol_set_sum_precision(1)),
-    and the GRF identity error of both forms on the surface nodes (8 point
-    charges on |y| = 6 clear of the surface, Direct far field on the GPU)."""
+    form, with FP32 level sums, with the error-judged selector, and in the
+    chosen form (both), and the GRF identity error of each form."""
     import torch
     import qotential_b200 as qol
     from qotential_b200 import geometry as G
@@ -239,7 +351,6 @@ def config4(steps=2, warmup=1):
     T = np.concatenate([P["sx"], off])
     tcxi, tcxrow, tcx = G.near_lists(P["sx"], P["sw"], hd, targets=T)
     t_near = time.perf_counter() - t0 - t_geo
-    npan = P["ntri"]
     pairs = int(tcxrow.size)
     dev = torch.device("cuda", torch.cuda.current_device())
     t = lambda a, dt=torch.float64: torch.as_tensor(np.ascontiguousarray(a), dtype=dt).to(dev)
@@ -250,132 +361,77 @@ def config4(steps=2, warmup=1):
     nnz = pairs * hd
     out = (torch.empty(nnz, dtype=torch.int64, device=dev), torch.empty(nnz, dtype=torch.int64, device=dev),
            torch.empty(nnz, dtype=torch.float64, device=dev), torch.empty(nnz, dtype=torch.float64, device=dev))
-    st = torch.cuda.current_stream()
-    hist = None
-
-    def step(want=False):
-        return qol.qol_getnearquad_lap_rrq_dev(npan, nterms, nterms + 2, D["sx"], D["snx"], D["sw"], D["rts"],
-                                               D["rps"], D["tcx"], D["tcxrow"], D["tcxi"], nterms + 2, 1.4, 30, out,
-                                               stream=st.cuda_stream, sync=want, want_hist=want)
-
-    ms = {}
-    for mode in (0, 1):
-        qol.qol_set_sum_precision(mode)
-        try:
-            hist = step(True)
-            for _ in range(warmup):
-                step()
-            torch.cuda.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(st)
-            for _ in range(steps):
-                step()
-            e1.record(st)
-            torch.cuda.synchronize()
-        finally:
-            qol.qol_set_sum_precision(0)
-        ms[mode] = e0.elapsed_time(e1) / steps
+    fl = tuple(FORMS) if w is not None else ("plain", "fp32_sums")
+    forms = time_forms(P["ntri"], nterms, pairs, D, out, w, steps, warmup, fl)
     del out, D
     torch.cuda.empty_cache()
-    ys, q = G.point_charges(G.stellarator(), 8, seed=SEED)
-    ub, ubn = G.harmonic_density(P["sx"], P["snx"], ys, q)
-    uf = qol.qol_direct_farfield(P["sx"], P["snx"], P["sw"], ub, ubn)
-    grf = {}
-    for mode, tag in ((0, "plain"), (1, "chosen")):
-        qol.qol_set_sum_precision(mode)
-        try:
-            un, _, _ = qol.qol_grf_near(npan, nterms, nterms + 2, P["sx"], P["snx"], P["sw"], P["rts"], P["rps"], ub,
-                                        ubn, u=uf)
-        finally:
-            qol.qol_set_sum_precision(0)
-        grf[tag] = float(np.abs(un).max() / np.abs(ubn).max())
+    grf = grf_forms(P, nterms, w, fl)
+    for f in forms:
+        forms[f]["grf_error"] = grf[f]
+        forms[f]["grf_error_ratio"] = grf[f] / grf["plain"]
     return {"workload": "stellarator 32x256 quads (16384 triangles), order 12 (nterms 13, hdim 91), "
                         "1490944 surface-node + 200000 off-surface targets",
-            "near_pairs": pairs, "level_hist": [int(x) for x in hist[1:6]],
-            "geometry_s": round(t_geo, 2), "near_lists_s": round(t_near, 2),
-            "plain": {"ms_per_step": ms[0], "pairs_per_s": pairs / (ms[0] * 1e-3)},
-            "chosen": {"ms_per_step": ms[1], "pairs_per_s": pairs / (ms[1] * 1e-3)},
-            "speedup": ms[0] / ms[1], "grf_error": grf,
-            "grf_error_ratio": grf["chosen"] / grf["plain"],
-            "note": "chosen = FP32 level sums with FP64 accumulation; CSR identical (the same input lists, the same "
-                    "level per pair)"}
+            "near_pairs": pairs, "geometry_s": round(t_geo, 2), "near_lists_s": round(t_near, 2),
+            "forms": forms,
+            "note": "fp32_sums = FP32 level sums with FP64 accumulation; learned = the error-judged selector "
+                    f"(mode 2, tol {SEL_TOL:g}, confidence {SEL_CONF}); chosen = both; the CSR (COO indices) is "
+                    "the same in every form; row errors are against the plain form's values"}
 
 
-def learned_form(W, D, out, steps, warmup, conf=0.9):
-    """The learned level selector: trained on the GPU on 10^6 pairs of seeded
-    surfaces of the batched family (features, plain-walk labels), evaluated on
-    this workload's pairs, then the device step with its decisions (confident
-    predictions that pass the ball check at their level; the plain walk for
-    the rest): ms/step, decision counts, per-row error against the plain form,
-    and the GRF error of both forms at the bench order."""
-    import torch
+def chosen_summary(learned, c4):
+    """the chosen form (error-judged selector + FP32 level sums) against the
+    plain FP64 form on both order-12 stellarator workloads"""
+    if learned is None and c4 is None:
+        return None
+    out = {"form": "error-judged level selector (mode 2) + FP32 level sums; batching does not apply to one surface"}
+    for tag, r in (("16x80", learned), ("32x256", c4)):
+        if r is not None and "chosen" in r["forms"]:
+            c, p = r["forms"]["chosen"], r["forms"]["plain"]
+            out[tag] = {"pairs_per_s": c["pairs_per_s"], "plain_pairs_per_s": p["pairs_per_s"],
+                        "speedup": c["speedup"], "grf_error": c["grf_error"], "plain_grf_error": p["grf_error"],
+                        "grf_error_ratio": c["grf_error_ratio"], "level_work_ratio": c["level_work_ratio"]}
+    return out
+
+
+def learned_form(W, D, out, steps, warmup):
+    """The error-judged level selector: trained on the GPU on 10^6 pairs of
+    seeded surfaces of the batched family at orders 4..12 (features; labels:
+    the lowest level whose row is within SEL_TOL of the finest level's, capped
+    at the walk's level, from four forced-level runs), then this workload's
+    step in every form (plain, FP32 sums, selector, both) and the GRF error of
+    each form at the bench order.  Returns the result and the weights."""
     import qotential_b200 as qol
     from qotential_b200 import geometry as G
     from qotential_b200 import selector as Sel
     t0 = time.perf_counter()
-    feat, lab, nsurf = Sel.training_set(1_000_000, seed=SEED)
+    feat, lab, nsurf = Sel.training_set(1_000_000, seed=SEED, labels="error", tol=SEL_TOL)
     t1 = time.perf_counter()
     w, loss = qol.qol_selector_train(feat, lab, epochs=20, batch=16384, lr=3e-3, seed=SEED)
     t2 = time.perf_counter()
     cls, _ = Sel.predict(w, feat)
     f12, lev12 = qol.qol_selector_features(W["npan"], W["nterms"], W["nquad"], W["sx"], W["snx"], W["sw"], W["rts"],
                                            W["rps"], W["tcx"], W["tcxrow"], W["tcxi"], W["nquad"])
+    P = {k: W[k] for k in ("sx", "snx", "sw", "rts", "rps")}
+    err12 = Sel.error_levels(W["npan"], W["nterms"], P, W["tcx"], W["tcxrow"], W["tcxi"], lev12)
+    lab12 = Sel.error_labels(err12, lev12, SEL_TOL)
     c12, p12 = Sel.predict(w, f12)
-    st = torch.cuda.current_stream()
-
-    def step():
-        qol.qol_getnearquad_lap_rrq_dev(W["npan"], W["nterms"], W["nquad"], D["sx"], D["snx"], D["sw"], D["rts"],
-                                        D["rps"], D["tcx"], D["tcxrow"], D["tcxi"], W["nquad"], 1.4, 30, out,
-                                        stream=st.cuda_stream, sync=False)
-
-    step()
-    torch.cuda.synchronize()
-    plain = (out[2].clone(), out[3].clone())
-    qol.qol_selector_set(1, w, conf)
-    try:
-        for _ in range(warmup):
-            step()
-        torch.cuda.synchronize()
-        qol.qol_selector_stats()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(st)
-        for _ in range(steps):
-            step()
-        e1.record(st)
-        torch.cuda.synchronize()
-        stats = qol.qol_selector_stats()
-        ms = e0.elapsed_time(e1) / steps
-        err = {"row_error_vs": row_errors(out[0], plain[0], out[2]), "row_error_vd": row_errors(out[0], plain[1], out[3])}
-        # GRF identity at the bench order, both forms
-        nterms = W["nterms"]
-        hd = nterms * (nterms + 1) // 2
-        P = G.panels(G.stellarator(), MP, NP, nterms, split=False)
-        ys, q = G.point_charges(G.stellarator(), 8, seed=SEED)
-        ub, ubn = G.harmonic_density(P["sx"], P["snx"], ys, q)
-        npan = P["sw"].size // hd
-        uf = qol.qol_direct_farfield(P["sx"], P["snx"], P["sw"], ub, ubn)
-        un1, _, _ = qol.qol_grf_near(npan, nterms, nterms + 2, P["sx"], P["snx"], P["sw"], P["rts"], P["rps"], ub, ubn,
-                                     u=uf)
-    finally:
-        qol.qol_selector_set(0)
-    un0, _, _ = qol.qol_grf_near(npan, nterms, nterms + 2, P["sx"], P["snx"], P["sw"], P["rts"], P["rps"], ub, ubn,
-                                 u=uf)
-    del plain
-    npairs = W["pairs_total"]
+    forms = time_forms(W["npan"], W["nterms"], W["pairs_total"], D, out, w, steps, warmup)
+    Pg = G.panels(G.stellarator(), MP, NP, W["nterms"], split=False)
+    grf = grf_forms(Pg, W["nterms"], w)
+    for f in forms:
+        forms[f]["grf_error"] = grf[f]
+        forms[f]["grf_error_ratio"] = grf[f] / grf["plain"]
     return {"training": {"pairs": int(lab.size), "surfaces": nsurf, "epochs": 20, "batch": 16384,
-                         "data_s": round(t1 - t0, 2), "train_s": round(t2 - t1, 2),
-                         "loss_first_last": [float(loss[0]), float(loss[-1])],
+                         "labels": f"error-judged, tol {SEL_TOL:g}", "data_s": round(t1 - t0, 2),
+                         "train_s": round(t2 - t1, 2), "loss_first_last": [float(loss[0]), float(loss[-1])],
                          "accuracy": float((cls == lab).mean())},
-            "workload_accuracy": float((c12 == lev12 - 1).mean()),
-            "workload_confident": float((p12 >= conf).mean()), "confidence": conf,
-            "ms_per_step": ms, "pairs_per_s": npairs / (ms * 1e-3), "decisions": stats,
-            **err,
-            "grf_error": {"plain": float(np.abs(un0).max() / np.abs(ubn).max()),
-                          "learned": float(np.abs(un1).max() / np.abs(ubn).max())},
-            "note": "a prediction replaces the ball-test walk only when it passes the ball check at its level "
-                    "(direct: outside every ball of that level; RRQ: where the walk gives RRQ), so "
-                    "no pair gets a level the plain criterion rejects; the walk costs 0.2 ms a step here, so "
-                    "the selector does not make this step faster"}
+            "workload_label_hist": [int(x) for x in np.bincount(lab12, minlength=5)],
+            "workload_accuracy": float((c12 == lab12).mean()),
+            "workload_confident": float((p12 >= SEL_CONF).mean()), "confidence": SEL_CONF,
+            "forms": forms,
+            "note": "a prediction below the walk's level is used after the two-level check (level l against l+1, "
+                    "4 sketch vectors, 10x safety); otherwise the walk's level; the walk's RRQ pairs stay RRQ; "
+                    "level_work = level nodes x pairs of the direct sums"}, w
 
 
 def batched_config(reps=2):
@@ -683,15 +739,14 @@ def main():
     value = pairs_total / (ms * 1e-3)
     # per-kernel device times of one more (untimed) step, for the roofline
     import ctypes as C
-    NPH = 9
+    NPH = 10
     ms_ph = np.zeros(NPH); calls = np.zeros(1, np.int64)
     L.qol_kernel_times(C.c_int(1), None, None)
     step()
     torch.cuda.synchronize()
     L.qol_kernel_times(C.c_int(-1), C.c_void_p(ms_ph.ctypes.data), C.c_void_p(calls.ctypes.data))
     L.qol_kernel_times(C.c_int(0), None, None)
-    names = ["levels", "classify", "direct", "rrq_panel", "rrq_ssq", "rrq_geom", "rrq_moments", "rrq_apply",
-             "coo_index"]
+    names = PHASES
     peak = C.c_double(0.0)
     L.qol_probe_fp64_peak(C.byref(peak))
     roofline = roofline_line(W, hist, dict(zip(names, (float(v) for v in ms_ph))), peak.value)
@@ -733,7 +788,7 @@ def main():
             times.append(time.perf_counter() - t0)
             L.qol_last_host_times(C.c_void_p(hms.ctypes.data))
             host_ms.append([round(float(x), 2) for x in hms])
-        kms = np.zeros(9)
+        kms = np.zeros(10)
         L.qol_kernel_times(C.c_int(-1), C.c_void_p(kms.ctypes.data), None)
         L.qol_kernel_times(C.c_int(0), None, None)
         del outs
@@ -768,9 +823,9 @@ def main():
     batched = None
     if rank == 0 and world == 1 and not args.no_batch:
         batched = batched_config()
-    learned = None
+    learned, wsel = None, None
     if rank == 0 and world == 1 and not args.no_learned:
-        learned = learned_form(W, D, out, args.steps, 2)
+        learned, wsel = learned_form(W, D, out, args.steps, 2)
     grf = None
     if rank == 0 and world == 1 and not args.no_grf:
         grf = grf_sweep()
@@ -779,7 +834,9 @@ def main():
                                    for r in grf}
     c4 = None
     if rank == 0 and world == 1 and not args.no_config4:
-        c4 = config4(args.steps, 1)
+        del out, D
+        torch.cuda.empty_cache()
+        c4 = config4(wsel, args.steps, 1)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         nthr = os.cpu_count() or 1
@@ -798,8 +855,8 @@ def main():
                 "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": config_dict(W, world), "clocks": clocks, "e2e": e2e,
                 "gpu_launches": LAUNCHES_PER_STEP * args.steps, "roofline": roofline, "cpu_baseline": cpu,
-                "chosen_form": chosen, "learned_form": learned, "batched": batched, "grf_sweep": grf,
-                "config4": c4}
+                "precision_variant": chosen, "chosen_form": chosen_summary(learned, c4), "learned_form": learned,
+                "batched": batched, "grf_sweep": grf, "config4": c4}
         print(json.dumps(line))
     if dist:
         dist.barrier()

@@ -197,11 +197,12 @@ int qol_interp_matrix(qol_int korder, qol_int n, const double* uv, double* M);
  * levels, [1] classification (with the host read of the RRQ pair count),
  * [2] level sums, [3] per-panel RRQ precompute, [4] singularity-swap roots and
  * weights, [5] string direction, solid angle and boundary weights, [6]
- * harmonic moments, [7] RRQ solves + COO values, [8] COO indices.  Returns the
+ * harmonic moments, [7] RRQ solves + COO values, [8] COO indices, [9] the
+ * learned selector's inference and two-level check.  Returns the
  * sums (ms[QOL_NPHASE]) and the call count; enable >= 0 resets them and sets
  * the switch (-1: read only).  (No counterpart in the reference; its timeinfo
  * is the host-side analogue.) */
-#define QOL_NPHASE 9
+#define QOL_NPHASE 10
 /* Precision of the level-resolved kernel sums for the calls that follow
  * (library-wide): 0 = FP64 (default; the drop-in), 1 = the precision variant:
  * kernel values in FP32, contraction with the interpolation rows on the TF32

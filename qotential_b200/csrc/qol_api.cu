@@ -275,7 +275,7 @@ void finish_timing(Timing& tm, double* timeinfo) {
   if (timeinfo) {
     timeinfo[0] += 1e-3 * ms[0];                   /* patch levels */
     timeinfo[1] += 1e-3 * ms[3];                   /* per-panel RRQ precompute */
-    timeinfo[2] += 1e-3 * (ms[1] + ms[2]);         /* classification + level sums */
+    timeinfo[2] += 1e-3 * (ms[1] + ms[2] + ms[9]); /* classification (selector) + level sums */
     timeinfo[5] += 1e-3 * (ms[4] + ms[5] + ms[6]); /* SSQ / solid angle / moments */
     timeinfo[7] += 1e-3 * (ms[7] + ms[8]);         /* solves + COO */
   }
@@ -381,8 +381,10 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
   CK(qol_launch_levels(T, J.P, W, npan, st));
   rec(1);
   if (g_sel_mode && g_sel_w && !g_force_level) { /* confident, checked predictions first; the walk for the rest */
+    rec(9);
     CK(qol_launch_sel_infer(T, J.P, J.Q, W, G, npan, g_sel_w, g_sel_conf, g_sel_cnt, g_sel_mode, st));
     if (g_sel_mode == 2) CK(qol_launch_sel_check(T, J.P, J.Q, W, G, npan, g_sel_tol, g_sel_cnt, st));
+    rec(1);
     CK(qol_launch_classify(T, J.Q, W, G, npan, st, 1));
   } else {
     CK(qol_launch_classify(T, J.Q, W, G, npan, st));

@@ -246,18 +246,61 @@ __global__ void __launch_bounds__(128) k_sel_infer(OrderTab T, PanelIn P, PairIn
 
 /* the two-level check of the direct-level candidates (G.level = -l, l =
  * 1..nlevel-1): accepted -> l, rejected -> 0 (the plain walk); counters
- * [accepted, -, check failed].  One CTA per panel; per level, candidates are
- * gathered SC_T at a time in target order, one thread each, the nodes and
- * sketch values of both levels streamed through shared-memory tiles; each
- * thread sums its nodes in node order (deterministic). */
-constexpr int SC_T = 128, SC_NT = 64;
-__global__ void __launch_bounds__(SC_T) k_sel_check(OrderTab T, PanelIn P, PairIn Q, LevelWS W, PairWS G, double tol,
+ * [accepted, -, check failed].  One CTA per (panel, candidate level);
+ * candidates are gathered SC_C at a time in target order, SC_J per thread,
+ * the nodes of both levels (coordinates, normal, weight, the 4 sketch values)
+ * staged SC_NT at a time in shared memory and read as 16-byte pairs by every
+ * thread; each thread sums its nodes in node order (deterministic). */
+#ifndef QOL_SC_T
+#define QOL_SC_T 128 /* check threads a CTA */
+#endif
+#ifndef QOL_SC_J
+#define QOL_SC_J 1   /* candidates a thread */
+#endif
+#ifndef QOL_SC_MINB
+#define QOL_SC_MINB 8 /* resident CTAs an SM (64 registers a thread) */
+#endif
+constexpr int SC_T = QOL_SC_T, SC_J = QOL_SC_J, SC_C = SC_T * SC_J, SC_NT = 64, SC_F = 12; /* fields a staged node, padded */
+
+/* the sketch sums of one level's nodes for the thread's targets, added
+ * (sign + 1) to or subtracted (sign - 1) from S and Dd */
+__device__ __forceinline__ void sk_level(const double* node, const double* skv, int n, const double (&x)[SC_J][3],
+                                         const bool (&on)[SC_J], double (&S)[SC_J][4], double (&Dd)[SC_J][4],
+                                         double* nd, double w4s) {
+  const int tid = threadIdx.x;
+  for (int n0 = 0; n0 < n; n0 += SC_NT) {
+    __syncthreads();
+    for (int e = tid; e < 11 * SC_NT; e += SC_T) {
+      const int f = e / SC_NT, q = e % SC_NT, i = n0 + q;
+      nd[q * SC_F + f] = i < n ? (f < 7 ? node[(size_t)f * n + i] : skv[(size_t)i * 4 + f - 7]) : 0.0;
+    }
+    __syncthreads();
+    const int nn = min(SC_NT, n - n0);
+    for (int q = 0; q < nn; ++q) {
+      const double2* r = reinterpret_cast<const double2*>(nd + q * SC_F);
+      const double2 p01 = r[0], p2n0 = r[1], n12 = r[2], wk0 = r[3], k12 = r[4], k3 = r[5];
+      const double w4 = wk0.x * w4s;
+#pragma unroll
+      for (int j = 0; j < SC_J; ++j) {
+        if (!on[j]) continue;
+        double sv, dv;
+        sdl_kernel(x[j][0] - p01.x, x[j][1] - p01.y, x[j][2] - p2n0.x, p2n0.y, n12.x, n12.y, w4, sv, dv);
+        S[j][0] = fma(sv, wk0.y, S[j][0]); Dd[j][0] = fma(dv, wk0.y, Dd[j][0]);
+        S[j][1] = fma(sv, k12.x, S[j][1]); Dd[j][1] = fma(dv, k12.x, Dd[j][1]);
+        S[j][2] = fma(sv, k12.y, S[j][2]); Dd[j][2] = fma(dv, k12.y, Dd[j][2]);
+        S[j][3] = fma(sv, k3.x, S[j][3]);  Dd[j][3] = fma(dv, k3.x, Dd[j][3]);
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(SC_T, QOL_SC_MINB) k_sel_check(OrderTab T, PanelIn P, PairIn Q, LevelWS W, PairWS G, double tol,
                                                     unsigned long long* cnt) {
-  const int pan = blockIdx.x, hd = T.hd;
+  const int pan = blockIdx.x, l = blockIdx.y + 1, hd = T.hd; /* candidate level l, checked against l + 1 */
   const long long p0 = Q.tcxi[pan] - 1, m = Q.tcxi[pan + 1] - Q.tcxi[pan];
   if (m <= 0) return;
-  __shared__ double nd[11 * SC_NT]; /* x, y, z, nx, ny, nz, w, then the 4 sketch values, SC_NT nodes each */
-  __shared__ int cand[2 * SC_T];
+  __shared__ __align__(16) double nd[SC_NT * SC_F];
+  __shared__ int cand[2 * SC_C];
   __shared__ int ncand, wc[SC_T / 32];
   __shared__ double sdiam;
   __shared__ unsigned long long sc[2];
@@ -270,86 +313,75 @@ __global__ void __launch_bounds__(SC_T) k_sel_check(OrderTab T, PanelIn P, PairI
     if (lane == 0) sdiam = sqrt(sw);
   }
   if (tid < 2) sc[tid] = 0;
+  if (tid == 0) ncand = 0;
   __syncthreads();
   const double Dp = sdiam, i4p = 1.0 / (4.0 * QOL_PI);
-  for (int l = 1; l < T.nlevel; ++l) { /* candidates lie below the walk's level, so below the finest */
-    const int la = l - 1, lb = l;
-    if (tid == 0) ncand = 0;
-    __syncthreads();
-    for (long long w0 = 0;; w0 += SC_T) {
-      const bool more = w0 < m;
-      if (more) { /* append this window's candidates in target order */
-        const long long t = w0 + tid;
-        const bool c = t < m && G.level[p0 + t] == -l;
-        const unsigned b = __ballot_sync(0xffffffffu, c);
-        if (lane == 0) wc[wid] = __popc(b);
-        __syncthreads();
-        int before = ncand;
-        for (int w = 0; w < wid; ++w) before += wc[w];
-        if (c) cand[before + __popc(b & ((1u << lane) - 1u))] = (int)t;
-        __syncthreads();
-        if (tid == 0) {
-          int tot = 0;
-          for (int w = 0; w < SC_T / 32; ++w) tot += wc[w];
-          ncand += tot;
-        }
-        __syncthreads();
+  const int la = l - 1, lb = l, na = T.n[la], nb_ = T.n[lb];
+  const double* nodea = W.node[la] + (size_t)pan * na * 7;
+  const double* nodeb = W.node[lb] + (size_t)pan * nb_ * 7;
+  for (long long w0 = 0;; w0 += SC_T) {
+    const bool more = w0 < m;
+    if (more) { /* append this window's candidates in target order */
+      const long long t = w0 + tid;
+      const bool c = t < m && G.level[p0 + t] == -l;
+      const unsigned b = __ballot_sync(0xffffffffu, c);
+      if (lane == 0) wc[wid] = __popc(b);
+      __syncthreads();
+      int before = ncand;
+      for (int w = 0; w < wid; ++w) before += wc[w];
+      if (c) cand[before + __popc(b & ((1u << lane) - 1u))] = (int)t;
+      __syncthreads();
+      if (tid == 0) {
+        int tot = 0;
+        for (int w = 0; w < SC_T / 32; ++w) tot += wc[w];
+        ncand += tot;
       }
-      const int nc = ncand;
-      if (nc >= SC_T || (!more && nc > 0)) {
-        const int nb = min(nc, SC_T);
-        const int my = tid < nb ? cand[tid] : -1;
-        double x0 = 0.0, x1 = 0.0, x2 = 0.0;
-        if (my >= 0) {
-          const double* x = Q.tcx + 3 * (p0 + my);
-          x0 = x[0]; x1 = x[1]; x2 = x[2];
-        }
-        double S[2][4] = {}, Dd[2][4] = {};
-#pragma unroll
-        for (int s = 0; s < 2; ++s) {
-          const int lv = s ? lb : la, n = T.n[lv];
-          const double* node = W.node[lv] + (size_t)pan * n * 7;
-          const double* skv = T.sk[lv];
-          for (int n0 = 0; n0 < n; n0 += SC_NT) {
-            __syncthreads();
-            for (int e = tid; e < 11 * SC_NT; e += SC_T) {
-              const int f = e / SC_NT, q = e % SC_NT, i = n0 + q;
-              nd[e] = i < n ? (f < 7 ? node[(size_t)f * n + i] : skv[(size_t)i * 4 + f - 7]) : 0.0;
-            }
-            __syncthreads();
-            if (my >= 0) {
-              const int nn = min(SC_NT, n - n0);
-              for (int q = 0; q < nn; ++q) {
-                double sv, dv;
-                sdl_kernel(x0 - nd[q], x1 - nd[SC_NT + q], x2 - nd[2 * SC_NT + q], nd[3 * SC_NT + q],
-                           nd[4 * SC_NT + q], nd[5 * SC_NT + q], nd[6 * SC_NT + q] * i4p, sv, dv);
-#pragma unroll
-                for (int v = 0; v < 4; ++v) {
-                  S[s][v] = fma(sv, nd[(7 + v) * SC_NT + q], S[s][v]);
-                  Dd[s][v] = fma(dv, nd[(7 + v) * SC_NT + q], Dd[s][v]);
-                }
-              }
-            }
-          }
-        }
-        if (my >= 0) {
-          double e = 0.0;
-#pragma unroll
-          for (int v = 0; v < 4; ++v) e = fmax(e, fmax(fabs(S[0][v] - S[1][v]) / Dp, fabs(Dd[0][v] - Dd[1][v])));
-          const bool ok = QOL_SEL_BETA * e <= tol;
-          G.level[p0 + my] = (signed char)(ok ? l : 0);
-          atomicAdd(&sc[ok ? 0 : 1], 1ull);
-        }
-        __syncthreads(); /* every thread has read its candidate: move the rest to the front */
-        const int rest = nc - nb;
-        const int keep = tid < rest ? cand[nb + tid] : 0;
-        __syncthreads();
-        if (tid < rest) cand[tid] = keep;
-        if (tid == 0) ncand = rest;
-        __syncthreads();
-      }
-      if (!more && ncand == 0) break;
+      __syncthreads();
     }
+    const int nc = ncand;
+    if (nc >= SC_C || (!more && nc > 0)) {
+      const int nb = min(nc, SC_C);
+      int my[SC_J];
+      double x[SC_J][3];
+      bool on[SC_J];
+#pragma unroll
+      for (int j = 0; j < SC_J; ++j) {
+        const int k = tid + j * SC_T;
+        my[j] = k < nb ? cand[k] : -1;
+        on[j] = my[j] >= 0;
+        const double* xp = Q.tcx + 3 * (p0 + (on[j] ? my[j] : 0));
+        x[j][0] = xp[0]; x[j][1] = xp[1]; x[j][2] = xp[2];
+      }
+      double S[SC_J][4], Dd[SC_J][4]; /* level l's sketch sums minus level l + 1's */
+#pragma unroll
+      for (int j = 0; j < SC_J; ++j)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) S[j][v] = Dd[j][v] = 0.0;
+      sk_level(nodea, T.sk[la], na, x, on, S, Dd, nd, i4p);
+      sk_level(nodeb, T.sk[lb], nb_, x, on, S, Dd, nd, -i4p);
+#pragma unroll
+      for (int j = 0; j < SC_J; ++j) {
+        if (!on[j]) continue;
+        double e = 0.0;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) e = fmax(e, fmax(fabs(S[j][v]) / Dp, fabs(Dd[j][v])));
+        const bool ok = QOL_SEL_BETA * e <= tol;
+        G.level[p0 + my[j]] = (signed char)(ok ? l : 0);
+        atomicAdd(&sc[ok ? 0 : 1], 1ull);
+      }
+      __syncthreads(); /* every thread has read its candidates: move the rest to the front */
+      const int rest = nc - nb;
+      int keep[SC_J];
+#pragma unroll
+      for (int j = 0; j < SC_J; ++j) keep[j] = tid + j * SC_T < rest ? cand[nb + tid + j * SC_T] : 0;
+      __syncthreads();
+#pragma unroll
+      for (int j = 0; j < SC_J; ++j)
+        if (tid + j * SC_T < rest) cand[tid + j * SC_T] = keep[j];
+      if (tid == 0) ncand = rest;
+      __syncthreads();
+    }
+    if (!more && ncand == 0) break;
   }
   __syncthreads();
   if (tid == 0) {
@@ -519,7 +551,8 @@ cudaError_t qol_launch_sel_infer(const OrderTab& T, const PanelIn& P, const Pair
 cudaError_t qol_launch_sel_check(const OrderTab& T, const PanelIn& P, const PairIn& Q, const LevelWS& W,
                                  const PairWS& G, int npan, double tol, unsigned long long* cnt, cudaStream_t st) {
   if (npan <= 0) return cudaSuccess;
-  k_sel_check<<<npan, SC_T, 0, st>>>(T, P, Q, W, G, tol, cnt);
+  if (T.nlevel < 2) return cudaSuccess;
+  k_sel_check<<<dim3(npan, T.nlevel - 1), SC_T, 0, st>>>(T, P, Q, W, G, tol, cnt);
   return cudaGetLastError();
 }
 
