@@ -263,6 +263,25 @@ int qol_selector_grad(qol_int n, const float* feat, const signed char* label, co
                       double* loss);
 int qol_selector_train(qol_int n, const float* feat, const signed char* label, qol_int epochs, qol_int batch,
                        double lr, unsigned long long seed, float* w, double* loss);
+/* Patch refinement of the level sums for the calls that follow (library
+ * wide; replaces the reference's module switches PR_SQUARE / PR_ADAPTIVE,
+ * patch_refine_mod.f90:53-56, with the codes of its GRF test's iadap
+ * argument, test/stellarator_grf.f90:46-47): 0 square-regrouped levels (the
+ * default, PR_SQUARE), 1 the adaptive tree walk (PR_ADAPTIVE: plain 4-split
+ * levels, a per-target cut of sub-patches over the first three levels, the
+ * finest level's ball test for the rest; an adaptive cut counts in
+ * level_hist[0]), 3 plain 4-split levels with the level walk.  Any other
+ * value: QOL_ERR_ARG (the reference refuses square + adaptive).  The learned
+ * selector applies to the default levels only; a patch-level handle takes
+ * the mode at evaluation.  No effect on qol_rrq_noalloc (square levels). */
+int qol_set_patch_refine(int iadap);
+/* Diagnostics: the reference element's level `level` (0..3) under the current
+ * refinement mode -- n nodes, nsub sub-patches, uv (2 x n), wt (n), suboff
+ * (nsub + 1, node offsets), subtyp (nsub; 1 = a Gauss-Legendre square); with
+ * uv == NULL only n and nsub (build_patch_ref_r64's REF%lev, no counterpart in
+ * the reference's API). */
+int qol_ref_level_table(qol_int nterms, qol_int orderff, qol_int level, qol_int* n, qol_int* nsub, double* uv,
+                        double* wt, qol_int* suboff, qol_int* subtyp);
 int qol_selector_set(int mode, const float* w, double conf);
 int qol_selector_set_tol(double tol);
 int qol_selector_force_level(int level);

@@ -52,6 +52,12 @@ def _i64(a):
     return np.ascontiguousarray(a, dtype=np.int64)
 
 
+def set_refine(iadap):
+    """the reference test's iadap (test/stellarator_grf.f90:46-47): 0 square
+    levels (default), 1 the adaptive tree walk, 3 plain 4-split levels"""
+    assert lib().orc_set_refine(C.c_int(int(iadap))) == 0
+
+
 def set_simd(isimd):
     """Kernel-matrix sums with AVX2 over 4 targets (isimd = 256, the
     reference's SIMD path) or scalar (0); both give the same results."""

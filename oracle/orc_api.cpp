@@ -12,18 +12,8 @@
 using namespace orc;
 
 namespace {
-std::mutex g_ref_mu;
-std::map<long long, RefElem*> g_refs;
-const RefElem& ref_for(int korder, int orderff, int nlevel, bool sq) {
-  long long key = korder + 1000LL * orderff + 1000000LL * nlevel + (sq ? 1000000000LL : 0);
-  std::lock_guard<std::mutex> g(g_ref_mu);
-  auto it = g_refs.find(key);
-  if (it != g_refs.end()) return *it->second;
-  RefElem* R = new RefElem();
-  build_ref(korder, orderff, nlevel, sq, *R);
-  g_refs[key] = R;
-  return *R;
-}
+const RefElem& ref_for(int korder, int orderff, int nlevel, bool sq) { return ref_cached(korder, orderff, nlevel, sq); }
+bool square() { return g_orc_refine == 0; }
 } // namespace
 
 extern "C" {
@@ -50,6 +40,12 @@ int orc_rrq_panel_systems(int nterms, const double* sx, const double* snx, const
   return 0;
 }
 int orc_set_flags(int f) { orc::g_orc_flags = f; return 0; }
+/* the reference test's iadap: 0 square levels, 1 adaptive tree walk, 3 plain levels */
+int orc_set_refine(int iadap) {
+  if (iadap != 0 && iadap != 1 && iadap != 3) return 1;
+  orc::g_orc_refine = iadap;
+  return 0;
+}
 /* isimd for the kernel-matrix sums: 0 scalar, 256 AVX2 (same results) */
 int orc_set_simd(int isimd) { orc::g_orc_simd = isimd == 256 ? 256 : 0; return 0; }
 
@@ -92,7 +88,7 @@ int orc_panel_levels(int korder, int npols, const double* sx, const double* rts,
                      const double* rps, int order, double dist, int nlevel, double* osx,
                      double* osnx, double* osw, double* oqp, double* oqr2) {
   if (npols != npols_of(korder)) return 3;
-  const RefElem& R = ref_for(korder, order, nlevel, true);
+  const RefElem& R = ref_for(korder, order, nlevel, square());
   std::vector<PanelLevel> lv;
   build_panel_levels(R, sx, rts, rps, dist, lv);
   long long on = 0, os = 0;
@@ -114,7 +110,7 @@ int orc_sdlpmat_levels(int korder, int npols, const double* sx, const double* rt
                        const double* tx, double* As, double* Ad, long long* idxs,
                        long long* ms, long long* level_of) {
   if (npols != npols_of(korder)) return 3;
-  const RefElem& R = ref_for(korder, order, nlevel, true);
+  const RefElem& R = ref_for(korder, order, nlevel, square());
   std::vector<PanelLevel> lv;
   build_panel_levels(R, sx, rts, rps, dist, lv);
   for (long long i = 0; i < m * npols; ++i) { As[i] = 0.0; Ad[i] = 0.0; }
@@ -161,7 +157,7 @@ int orc_getnearquad(long long npan, int nterms, long long hdim, int nquad, long 
   if ((tcxi[npan] - 1) * hdim > nnz) return 2;
   bool exterior = (iside % 10) == 0;
   RRQConfig cfg{nterms, nquad, orderff, distff, exterior, 0};
-  (void)ref_for(nterms - 1, orderff, 4, true);
+  (void)ref_for(nterms - 1, orderff, 4, square());
   int err = 0;
   long long hist[6] = {0, 0, 0, 0, 0, 0};
   if (nthreads > 0) omp_set_num_threads(nthreads);
@@ -286,7 +282,7 @@ int orc_grf_near(long long npan, int nterms, int nquad, int orderff, double dist
                  long long* level_hist) {
   long long hdim = (long long)nterms * (nterms + 1) / 2, nbd = 3LL * nquad;
   RRQConfig cfg{nterms, nquad, orderff, distff, exterior != 0, ichart};
-  (void)ref_for(nterms - 1, orderff, 4, true);
+  (void)ref_for(nterms - 1, orderff, 4, square());
   int err = 0;
   long long hist[6] = {0, 0, 0, 0, 0, 0};
   if (nthreads > 0) omp_set_num_threads(nthreads);

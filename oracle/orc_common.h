@@ -80,10 +80,22 @@ void build_panel_levels(const RefElem& R, const double* sx, const double* rts,
 void sdlpmat(i8 m, const double* tx, i8 n, const double* sx, const double* snx,
              const double* sw, double* A, double* B);
 
-/* lap3dsdlpmat_levels_r64 (patch_refine_mod.f90:516-615), uniform mode */
+/* the patch refinement of the reference test's iadap switch
+ * (test/stellarator_grf.f90:46-47 over patch_refine_mod.f90:53-56):
+ * 0 square-regrouped levels (PR_SQUARE, the default), 1 the adaptive tree walk
+ * on plain 4-split levels (PR_ADAPTIVE), 3 plain 4-split levels, level walk */
+extern int g_orc_refine;
+/* build_patch_ref_r64's cached reference element (patch_refine_mod.f90:100-121
+ * returns early for the element it already holds), one per (korder, order,
+ * nlevel, square mode) */
+const RefElem& ref_cached(int korder, int order, int nlevel, bool sqmode);
+
+/* lap3dsdlpmat_levels_r64 (patch_refine_mod.f90:516-615); with g_orc_refine
+ * == 1 and nlevel >= 3 its adaptive branch (adaptive_pass, walk, cut_gI,
+ * one_level at the finest level: :532-539, 617-771) */
 void sdlpmat_levels(const RefElem& R, const std::vector<PanelLevel>& lv, i8 m,
                     const double* tx, double* As, double* Ad, i8* idxs, i8* ms,
-                    i8* level_of /* nullable: per target level 1..4 or 5=unresolved */);
+                    i8* level_of /* nullable: per target level 1..4, 0 = an adaptive cut, 5 = unresolved */);
 
 /* ---------------- RRQ ---------------- */
 struct RRQConfig {

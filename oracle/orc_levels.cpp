@@ -2,6 +2,8 @@
  * per-panel refined levels and the level-resolved direct SLP/DLP sums.
  * TEST INFRASTRUCTURE ONLY (see orc_common.h). */
 #include "orc_common.h"
+#include <map>
+#include <mutex>
 #ifdef __AVX2__
 #include <immintrin.h>
 #endif
@@ -504,6 +506,75 @@ void sdlpmat(i8 m, const double* tx, i8 n, const double* sx, const double* snx,
   }
 }
 
+int g_orc_refine = 0;
+
+const RefElem& ref_cached(int korder, int order, int nlevel, bool sqmode) {
+  static std::mutex mu;
+  static std::map<long long, RefElem*> refs;
+  const long long key = korder + 1000LL * order + 1000000LL * nlevel + (sqmode ? 1000000000LL : 0);
+  std::lock_guard<std::mutex> g(mu);
+  auto it = refs.find(key);
+  if (it != refs.end()) return *it->second;
+  RefElem* R = new RefElem();
+  build_ref(korder, order, nlevel, sqmode, *R);
+  refs[key] = R;
+  return *R;
+}
+
+/* walk (patch_refine_mod.f90:740-771): from the whole patch down the
+ * quadtree of the first ntree levels (children of sub-patch q: 4q..4q+3), a
+ * sub-patch whose ball excludes x joins the cut, one that contains it is
+ * split, and containment at the last tree level fails the walk */
+static bool cut_walk(const std::vector<PanelLevel>& lv, int ntree, const double* x,
+                     std::vector<std::pair<int, i8>>& cut) {
+  std::vector<i8> act(1, 0), nxt;
+  cut.clear();
+  for (int il = 0; il < ntree; ++il) {
+    nxt.clear();
+    const PanelLevel& P = lv[il];
+    for (i8 q : act) {
+      double d2 = 0.0;
+      for (int d = 0; d < 3; ++d) { double t = x[d] - P.qpoint[3 * q + d]; d2 += t * t; }
+      if (d2 > P.qradii2[q]) cut.push_back({il, q});
+      else if (il == ntree - 1) return false;
+      else for (int b = 0; b < 4; ++b) nxt.push_back(4 * q + b);
+    }
+    if (nxt.empty()) break;
+    act.swap(nxt);
+  }
+  return true;
+}
+
+/* adaptive_pass (patch_refine_mod.f90:617-718): the targets the walk resolves
+ * get the kernel on their cut's nodes contracted with the matching rows of
+ * each level's interpmat (cut_gI, :720-738), summed node by node in cut
+ * order; the rest stay in irem */
+static void adaptive_cuts(const RefElem& R, const std::vector<PanelLevel>& lv, i8 m, const double* tx,
+                          double* As, double* Ad, std::vector<i8>& irem, i8& nrem, i8* level_of) {
+  const int np = R.npols, ntree = R.nlevel - 1;
+  const i8 n1 = R.lev[0].n;
+  std::vector<std::pair<int, i8>> cut;
+  std::vector<double> a(n1), b(n1), ss(np), sd(np);
+  i8 keep = 0;
+  for (i8 jj = 0; jj < nrem; ++jj) {
+    const i8 t = irem[jj];
+    if (!cut_walk(lv, ntree, tx + 3 * t, cut)) { irem[keep++] = t; continue; }
+    std::fill(ss.begin(), ss.end(), 0.0);
+    std::fill(sd.begin(), sd.end(), 0.0);
+    for (const auto& c : cut) {
+      const PanelLevel& P = lv[c.first];
+      const i8 i0 = c.second * n1;
+      sdlpmat(1, tx + 3 * t, n1, P.sx.data() + 3 * i0, P.snx.data() + 3 * i0, P.sw.data() + i0, a.data(), b.data());
+      const double* It = R.lev[c.first].interp_t.data() + (size_t)i0 * np;
+      for (i8 q = 0; q < n1; ++q)
+        for (int k = 0; k < np; ++k) { ss[k] += a[q] * It[(size_t)q * np + k]; sd[k] += b[q] * It[(size_t)q * np + k]; }
+    }
+    for (int k = 0; k < np; ++k) { As[t + m * k] = ss[k]; Ad[t + m * k] = sd[k]; }
+    if (level_of) level_of[t] = 0;
+  }
+  nrem = keep;
+}
+
 void sdlpmat_levels(const RefElem& R, const std::vector<PanelLevel>& lv, i8 m,
                     const double* tx, double* As, double* Ad, i8* idxs, i8* ms,
                     i8* level_of) {
@@ -511,7 +582,12 @@ void sdlpmat_levels(const RefElem& R, const std::vector<PanelLevel>& lv, i8 m,
   std::vector<i8> irem(m), ibat, inext;
   for (i8 j = 0; j < m; ++j) irem[j] = j;
   i8 nrem = m;
-  for (int il = 0; il < R.nlevel && nrem > 0; ++il) {
+  int il0 = 0;
+  if (g_orc_refine == 1 && R.nlevel >= 3) { /* the walk, then one_level at the finest level */
+    adaptive_cuts(R, lv, m, tx, As, Ad, irem, nrem, level_of);
+    il0 = R.nlevel - 1;
+  }
+  for (int il = il0; il < R.nlevel && nrem > 0; ++il) {
     const PanelLevel& P = lv[il];
     ibat.clear(); inext.clear();
     for (i8 jj = 0; jj < nrem; ++jj) {

@@ -689,8 +689,7 @@ void rrq(const RRQConfig& cfg, i8 m, const double* tx, const double* sx, const d
   for (i8 i = 0; i < m * hd; ++i) { As[i] = 0.0; Ad[i] = 0.0; }
   if (Omega) for (i8 i = 0; i < m * 4 * hd; ++i) Omega[i] = 0.0;
   if (Ialpha) for (i8 i = 0; i < m; ++i) Ialpha[i] = 0.0;
-  RefElem R;
-  build_ref(L - 1, cfg.orderff, 4, true, R);
+  const RefElem& R = ref_cached(L - 1, cfg.orderff, 4, g_orc_refine == 0);
   std::vector<PanelLevel> lv;
   build_panel_levels(R, sx, rts, rps, cfg.distff, lv);
   std::vector<i8> idxs(m);

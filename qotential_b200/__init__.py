@@ -18,7 +18,9 @@ __all__ = [
     "qol_getnearquad_lap_rrq_dev", "qol_grf_near", "qol_grf_near_range", "qol_direct_farfield",
     "qol_direct_farfield_range", "qol_surface_panels", "qol_interp_matrix", "qol_set_sum_precision",
     "SELECTOR_NW", "qol_selector_features", "qol_selector_grad", "qol_selector_train", "qol_selector_set",
-    "qol_selector_stats", "qol_selector_force_level", "qol_set_autotune", "qol_panel_shape",
+    "qol_selector_stats", "qol_selector_force_level", "qol_set_patch_refine", "qol_ref_level_table",
+    "qol_set_autotune",
+    "qol_panel_shape",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -382,6 +384,25 @@ def qol_selector_set(mode, w=None, conf=0.9, tol=None):
         _check(lib().qol_selector_set_tol(C.c_double(tol)))
     wp = None if w is None else np.ascontiguousarray(w, dtype=np.float32)
     _check(lib().qol_selector_set(C.c_int(int(mode)), _vp(wp), C.c_double(conf)))
+
+
+def qol_set_patch_refine(iadap):
+    """patch refinement of the calls that follow, the reference GRF test's
+    iadap: 0 square levels (default), 1 the adaptive tree walk (PR_ADAPTIVE),
+    3 plain 4-split levels"""
+    _check(lib().qol_set_patch_refine(C.c_int(int(iadap))))
+
+
+def qol_ref_level_table(nterms, orderff, level):
+    """dict(uv (n, 2), wt, suboff, subtyp) of the reference element's level
+    0..3 under the current refinement mode"""
+    n, ns = np.zeros(1, np.int64), np.zeros(1, np.int64)
+    _check(lib().qol_ref_level_table(i64(nterms), i64(orderff), i64(level), _vp(n), _vp(ns), None, None, None, None))
+    uv, wt = np.zeros(2 * n[0]), np.zeros(n[0])
+    so, st = np.zeros(ns[0] + 1, np.int64), np.zeros(ns[0], np.int64)
+    _check(lib().qol_ref_level_table(i64(nterms), i64(orderff), i64(level), _vp(n), _vp(ns), _vp(uv), _vp(wt),
+                                     _vp(so), _vp(st)))
+    return dict(uv=uv.reshape(-1, 2), wt=wt, suboff=so, subtyp=st)
 
 
 def qol_selector_force_level(level):

@@ -102,6 +102,11 @@ int g_sel_mode = 0;
 float g_sel_conf = 0.9f;
 double g_sel_tol = 1e-8;  /* mode 2: the two-level check's row-error tolerance */
 int g_force_level = 0;    /* labelling runs: direct pairs all on this level (0: off) */
+/* patch refinement, the reference test's iadap (test/stellarator_grf.f90:46-47
+ * over patch_refine_mod.f90:53-56): 0 square-regrouped levels (PR_SQUARE, the
+ * default), 1 the adaptive tree walk on plain 4-split levels (PR_ADAPTIVE),
+ * 3 plain 4-split levels with the level walk */
+int g_refine = 0;
 float* g_sel_w = nullptr;
 unsigned long long* g_sel_cnt = nullptr; /* accepted, low confidence, check failed, pairs */
 double g_ktime[QOL_NPHASE] = {};
@@ -131,11 +136,12 @@ int ensure_device() {
 }
 
 /* build (or fetch) the device tables for one (nterms, orderff, nquad) */
-int order_tables(int nterms, int orderff, int nquad, OrderCache** out) {
+int order_tables(int nterms, int orderff, int nquad, OrderCache** out, int refine = -1) {
+  if (refine < 0) refine = g_refine;
   if (nterms < 2 || nterms > QOL_MAXL || orderff < 2 || orderff - 1 > 20 || nquad < 2 || nquad > QOL_MAXNQ ||
       nterms - 1 > 20)
     return fail(QOL_ERR_ORDER, "unsupported order nterms=%d orderff=%d nquad=%d", nterms, orderff, nquad);
-  long long key = nterms + 100LL * orderff + 10000LL * nquad;
+  long long key = nterms + 100LL * orderff + 10000LL * nquad + 1000000LL * refine;
   auto it = g_orders.find(key);
   if (it != g_orders.end()) { *out = it->second.get(); return 0; }
   std::unique_ptr<OrderCache> C(new OrderCache());
@@ -143,11 +149,12 @@ int order_tables(int nterms, int orderff, int nquad, OrderCache** out) {
   const int korder = nterms - 1, hd = nterms * (nterms + 1) / 2;
   qolh::RefElem R;
   try {
-    qolh::build_ref(korder, orderff, 4, true, R);
+    qolh::build_ref(korder, orderff, 4, refine == 0, R);
   } catch (const std::exception& e) {
     return fail(QOL_ERR_ORDER, "reference element: %s", e.what());
   }
   T.korder = korder; T.hd = hd; T.nterms = nterms; T.orderff = orderff; T.nquad = nquad; T.nlevel = 4;
+  T.adaptive = refine == 1;
   T.ng = std::max(1, (nterms + 1) / 2);
   for (int l = 0; l < 4; ++l) {
     const qolh::RefLevel& L = R.lev[l];
@@ -380,7 +387,7 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
   rec(0);
   CK(qol_launch_levels(T, J.P, W, npan, st));
   rec(1);
-  if (g_sel_mode && g_sel_w && !g_force_level) { /* confident, checked predictions first; the walk for the rest */
+  if (g_sel_mode && g_sel_w && !g_force_level && !g_refine) { /* confident, checked predictions first; the walk for the rest */
     rec(9);
     CK(qol_launch_sel_infer(T, J.P, J.Q, W, G, npan, g_sel_w, g_sel_conf, g_sel_cnt, g_sel_mode, st));
     if (g_sel_mode == 2) CK(qol_launch_sel_check(T, J.P, J.Q, W, G, npan, g_sel_tol, g_sel_cnt, st));
@@ -454,6 +461,7 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
   if (!chunked) {
     rec(2);
     CK(qol_launch_direct(T, J.P, J.Q, W, G, O, npan, st));
+    CK(qol_launch_direct_cut(T, J.P, J.Q, W, G, O, npan, st));
     rec(3);
     if (nrrq > 0) CK(qol_launch_rrq_panel(T, J.P, G, R, npan, J.chart, st));
   }
@@ -477,6 +485,7 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
     if (chunked && b > a) {
       rec(2, si);
       CK(qol_launch_direct(T, J.P, J.Q, W, G, O, (int)(b - a), sc, (int)a));
+      CK(qol_launch_direct_cut(T, J.P, J.Q, W, G, O, (int)(b - a), sc, (int)a));
       rec(3, si);
       if (R.ghi > R.glo) CK(qol_launch_rrq_panel(T, J.P, G, R, (int)(b - a), J.chart, sc));
     }
@@ -510,8 +519,10 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
     CK(cudaMemcpy(cnt.data(), G.cnt, sizeof(int) * cnt.size(), cudaMemcpyDeviceToHost));
     if (hist_out) {
       for (int i = 0; i < 6; ++i) hist_out[i] = 0;
-      for (int p = 0; p < npan; ++p)
+      for (int p = 0; p < npan; ++p) {
         for (int l = 1; l <= 5; ++l) hist_out[l] += cnt[(size_t)p * 8 + l];
+        hist_out[0] += cnt[(size_t)p * 8 + QOL_LV_CUT]; /* adaptive cuts */
+      }
     }
     if (cnt_out) for (int l = 0; l < 8; ++l) cnt_out[l] = cnt[l];
   }
@@ -1025,6 +1036,18 @@ int qol_selector_set(int mode, const float* w, double conf) {
   return 0;
 }
 
+/* patch refinement mode of the calls that follow: the reference test's iadap
+ * (0 square levels, 1 adaptive tree walk, 3 plain levels); 2 or any other
+ * value is refused (PR_SQUARE and PR_ADAPTIVE cannot be combined,
+ * patch_refine_mod.f90:116-117) */
+int qol_set_patch_refine(int iadap) {
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  if (iadap != 0 && iadap != 1 && iadap != 3)
+    return fail(QOL_ERR_ARG, "qol_set_patch_refine: iadap 0 (square), 1 (adaptive) or 3 (plain levels)");
+  g_refine = iadap;
+  return 0;
+}
+
 /* the two-level check's tolerance on a row's error (single-layer rows over
  * the panel's diameter, double-layer rows as they are; 1-norm scale) */
 int qol_selector_set_tol(double tol) {
@@ -1064,11 +1087,36 @@ int qol_level_sizes(qol_int nterms, qol_int orderff, qol_int* n4, qol_int* nsub4
   std::lock_guard<std::recursive_mutex> g(g_mu);
   qolh::RefElem R;
   try {
-    qolh::build_ref((int)nterms - 1, (int)orderff, 4, true, R);
+    qolh::build_ref((int)nterms - 1, (int)orderff, 4, g_refine == 0, R);
   } catch (const std::exception& e) {
     return fail(QOL_ERR_ORDER, "reference element: %s", e.what());
   }
   for (int l = 0; l < 4; ++l) { n4[l] = R.lev[l].n; nsub4[l] = R.lev[l].nsub; }
+  return 0;
+}
+
+/* the reference element's level `level` (0..3) for the current refinement
+ * mode: uv (2 x n), wt (n), suboff (nsub + 1), subtyp (nsub); with uv == NULL
+ * only the sizes (diagnostics: tests compare the tables with an independent
+ * restatement) */
+int qol_ref_level_table(qol_int nterms, qol_int orderff, qol_int level, qol_int* n, qol_int* nsub, double* uv,
+                        double* wt, qol_int* suboff, qol_int* subtyp) {
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  if (!n || !nsub || level < 0 || level > 3) return fail(QOL_ERR_ARG, "qol_ref_level_table: bad arguments");
+  qolh::RefElem R;
+  try {
+    qolh::build_ref((int)nterms - 1, (int)orderff, 4, g_refine == 0, R);
+  } catch (const std::exception& e) {
+    return fail(QOL_ERR_ORDER, "reference element: %s", e.what());
+  }
+  const qolh::RefLevel& L = R.lev[level];
+  *n = L.n; *nsub = L.nsub;
+  if (!uv) return 0;
+  if (!wt || !suboff || !subtyp) return fail(QOL_ERR_ARG, "qol_ref_level_table: null output");
+  std::copy(L.uv.begin(), L.uv.end(), uv);
+  std::copy(L.wt.begin(), L.wt.end(), wt);
+  for (size_t i = 0; i < L.suboff.size(); ++i) suboff[i] = L.suboff[i];
+  for (size_t i = 0; i < L.subtyp.size(); ++i) subtyp[i] = L.subtyp[i];
   return 0;
 }
 
@@ -1189,6 +1237,7 @@ int qol_lap3dsdlpmat_levels(qol_int m, const double* tx, qol_int npols, qol_int 
   CK(qol_launch_levels(T, P, W, 1, st));
   CK(qol_launch_classify(T, Q, W, G, 1, st));
   CK(qol_launch_direct(T, P, Q, W, G, O, 1, st));
+  CK(qol_launch_direct_cut(T, P, Q, W, G, O, 1, st));
   int cnt[8], off[8];
   std::vector<int> grp(m);
   CK(cudaMemcpyAsync(cnt, G.cnt, sizeof cnt, cudaMemcpyDeviceToHost, st));

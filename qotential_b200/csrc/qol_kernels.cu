@@ -89,6 +89,34 @@ cudaError_t qol_upload_harm_coefs(const double* hb, const double* hc, const doub
 /* ===================================================================== */
 /* K2: level of every (target, panel) pair, grouped per panel by level   */
 /* ===================================================================== */
+/* walk (patch_refine_mod.f90:740-771) over the quadtree of the first
+ * nlevel-1 levels of plain 4-split sub-patches (children of q: 4q..4q+3): a
+ * sub-patch whose ball excludes x joins the cut (bit: the sub-patch's index
+ * after all coarser levels' sub-patches), one that contains it is split, and
+ * containment at the last tree level fails the walk */
+__device__ __forceinline__ bool cut_walk(const OrderTab& T, const LevelWS& W, int pan, const double* x,
+                                         unsigned& cut) {
+  unsigned act = 1u;
+  int off = 0;
+  cut = 0u;
+  const int ntree = T.nlevel - 1;
+  for (int il = 0; il < ntree; ++il) {
+    const double* qp = W.sub[il] + (size_t)pan * T.nsub[il] * 4;
+    unsigned nxt = 0u;
+    for (int q = 0; q < T.nsub[il]; ++q) {
+      if (!((act >> q) & 1u)) continue;
+      const double a = x[0] - qp[4 * q], b = x[1] - qp[4 * q + 1], c = x[2] - qp[4 * q + 2];
+      if (a * a + b * b + c * c > qp[4 * q + 3]) cut |= 1u << (off + q);
+      else if (il == ntree - 1) return false;
+      else nxt |= 0xFu << (4 * q);
+    }
+    if (!nxt) break;
+    act = nxt;
+    off += T.nsub[il];
+  }
+  return true;
+}
+
 __global__ void __launch_bounds__(128) k_classify(OrderTab T, PairIn Q, LevelWS W, PairWS G, int preset) {
   const int pan = blockIdx.x;
   const long long p0 = Q.tcxi[pan] - 1, m = Q.tcxi[pan + 1] - Q.tcxi[pan];
@@ -104,7 +132,21 @@ __global__ void __launch_bounds__(128) k_classify(OrderTab T, PairIn Q, LevelWS 
       const double* x = Q.tcx + 3 * (p0 + t);
       const int pre = preset ? (int)G.level[p0 + t] : 0; /* a level the selector already accepted */
       lv = pre ? pre : T.nlevel + 1;
-      for (int l = 0; l < T.nlevel && !pre; ++l) {
+      if (T.adaptive && !pre) { /* the walk, then the finest level's balls (one_level at nlevel) */
+        unsigned cut;
+        if (cut_walk(T, W, pan, x, cut)) lv = QOL_LV_CUT;
+        else {
+          const int l = T.nlevel - 1;
+          const double* qp = W.sub[l] + (size_t)pan * T.nsub[l] * 4;
+          bool outside = true;
+          for (int s = 0; s < T.nsub[l]; ++s) {
+            double a = qp[4 * s] - x[0], b = qp[4 * s + 1] - x[1], c = qp[4 * s + 2] - x[2];
+            if (a * a + b * b + c * c < qp[4 * s + 3]) { outside = false; break; }
+          }
+          lv = outside ? T.nlevel : T.nlevel + 1;
+        }
+      }
+      for (int l = 0; l < T.nlevel && !pre && !T.adaptive; ++l) {
         const double* qp = W.sub[l] + (size_t)pan * T.nsub[l] * 4;
         bool outside = true;
         for (int s = 0; s < T.nsub[l]; ++s) {
@@ -119,9 +161,10 @@ __global__ void __launch_bounds__(128) k_classify(OrderTab T, PairIn Q, LevelWS 
     }
   }
   __syncthreads();
+  const int lmax = T.adaptive ? QOL_LV_CUT : T.nlevel + 1; /* the pair classes */
   if (threadIdx.x == 0) {
     int acc = 0;
-    for (int l = 1; l <= T.nlevel + 1; ++l) {
+    for (int l = 1; l <= lmax; ++l) {
       base_l[l] = acc;
       G.cnt[(size_t)pan * 8 + l] = cnt[l];
       G.off[(size_t)pan * 8 + l] = acc;
@@ -134,7 +177,7 @@ __global__ void __launch_bounds__(128) k_classify(OrderTab T, PairIn Q, LevelWS 
   for (long long t0 = 0; t0 < m; t0 += blockDim.x) {
     long long t = t0 + threadIdx.x;
     int lv = (t < m) ? (int)G.level[p0 + t] : 0;
-    for (int l = 1; l <= T.nlevel + 1; ++l) {
+    for (int l = 1; l <= lmax; ++l) {
       unsigned b = __ballot_sync(0xffffffffu, lv == l);
       if (lane == 0) warpc[wid][l] = __popc(b);
       __syncthreads();
@@ -443,6 +486,84 @@ __global__ void __launch_bounds__(256, 2) k_direct(OrderTab T, PanelIn P, PairIn
     }
   }
 }
+/* level sums of the adaptive cuts (adaptive_pass, patch_refine_mod.f90:617-718,
+ * with cut_gI :720-738): one warp per pair, lanes over the hd output columns.
+ * The cut's sub-patches in walk order (level by level, sub-patch order), their
+ * nodes 32 at a time (one kernel value a lane, then shuffled), each node's
+ * interpmat row contracted into the columns; minus the self-masked naive
+ * block and written as COO values as k_direct does. */
+#define CUT_MAXC 5 /* columns a lane: hd <= 160 */
+__global__ void __launch_bounds__(256) k_direct_cut(OrderTab T, PanelIn P, PairIn Q, LevelWS W, PairWS G, OutCOO O,
+                                                    int pan0) {
+  const int pan = pan0 + blockIdx.x;
+  const int cnt = G.cnt[(size_t)pan * 8 + QOL_LV_CUT];
+  if (cnt == 0) return;
+  const int off = G.off[(size_t)pan * 8 + QOL_LV_CUT];
+  const long long p0 = Q.tcxi[pan] - 1, m = Q.tcxi[pan + 1] - Q.tcxi[pan];
+  const int hd = T.hd, ncw = T.ncw, n1 = T.n[0];
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const double i4p = 1.0 / (4.0 * QOL_PI);
+  for (int i = threadIdx.x >> 5; i < cnt; i += nw) {
+    const int tl = G.grp[p0 + off + i];
+    const double x[3] = {Q.tcx[3 * (p0 + tl)], Q.tcx[3 * (p0 + tl) + 1], Q.tcx[3 * (p0 + tl) + 2]};
+    unsigned cut;
+    cut_walk(T, W, pan, x, cut);
+    double aS[CUT_MAXC], aD[CUT_MAXC];
+#pragma unroll
+    for (int j = 0; j < CUT_MAXC; ++j) aS[j] = aD[j] = 0.0;
+    int lbase = 0;
+    for (int il = 0; il < T.nlevel - 1; ++il) {
+      const int n = T.n[il];
+      const double* node = W.node[il] + (size_t)pan * n * 7;
+      const double* I = T.interp[il];
+      for (int q = 0; q < T.nsub[il]; ++q) {
+        if (!((cut >> (lbase + q)) & 1u)) continue;
+        const int kend = (q + 1) * n1;
+        for (int k0 = q * n1; k0 < kend; k0 += 32) {
+          const int k = k0 + lane;
+          double sv = 0.0, dv = 0.0;
+          if (k < kend)
+            sdl_kernel(x[0] - node[k], x[1] - node[n + k], x[2] - node[2 * n + k], node[3 * n + k], node[4 * n + k],
+                       node[5 * n + k], node[6 * n + k] * i4p, sv, dv);
+          const int nk = min(32, kend - k0);
+          for (int kk = 0; kk < nk; ++kk) {
+            const double s = __shfl_sync(0xffffffffu, sv, kk), d = __shfl_sync(0xffffffffu, dv, kk);
+            const double* Ir = I + (size_t)(k0 + kk) * ncw;
+#pragma unroll
+            for (int j = 0; j < CUT_MAXC; ++j) {
+              const int c = lane + 32 * j;
+              if (c < hd) {
+                const double iv = Ir[c];
+                aS[j] = fma(s, iv, aS[j]);
+                aD[j] = fma(d, iv, aD[j]);
+              }
+            }
+          }
+        }
+      }
+      lbase += T.nsub[il];
+    }
+    const long long row = Q.tcxrow[p0 + tl];
+#pragma unroll
+    for (int j = 0; j < CUT_MAXC; ++j) {
+      const int c = lane + 32 * j;
+      if (c >= hd) continue;
+      double vs = aS[j], vd = aD[j];
+      if (O.subtract_naive) {
+        const size_t gj = (size_t)pan * hd + c;
+        double ns = 0.0, nd = 0.0;
+        if (row != (long long)gj + 1)
+          sdl_kernel(x[0] - P.sx[3 * gj], x[1] - P.sx[3 * gj + 1], x[2] - P.sx[3 * gj + 2], P.snx[3 * gj],
+                     P.snx[3 * gj + 1], P.snx[3 * gj + 2], P.sw[gj] * i4p, ns, nd);
+        vs -= ns; vd -= nd;
+      }
+      const size_t o = (size_t)p0 * hd + (size_t)c * m + tl;
+      O.vs[o] = vs;
+      O.vd[o] = vd;
+    }
+  }
+}
+
 template <int NB>
 constexpr size_t direct_smem() {
   return sizeof(double) * (2 * (2 * DNT * DKS + DNT * (32 * NB + 4) + 8 * DNT) + 3 * DTT) + sizeof(int) * DTT;
@@ -2135,6 +2256,13 @@ cudaError_t qol_launch_direct(const OrderTab& T, const PanelIn& P, const PairIn&
     case 4: go(k_direct<4>, direct_smem<4>()); break;
     case 5: go(k_direct<5>, direct_smem<5>()); break;
   }
+  return cudaGetLastError();
+}
+cudaError_t qol_launch_direct_cut(const OrderTab& T, const PanelIn& P, const PairIn& Q, const LevelWS& W,
+                                  const PairWS& G, const OutCOO& O, int npan, cudaStream_t st, int pan0) {
+  if (npan <= 0 || !T.adaptive) return cudaSuccess;
+  if (T.hd > 32 * CUT_MAXC || T.nlevel != 4 || T.nsub[T.nlevel - 2] > 32) return cudaErrorInvalidValue;
+  k_direct_cut<<<npan, 256, 0, st>>>(T, P, Q, W, G, O, pan0);
   return cudaGetLastError();
 }
 cudaError_t qol_launch_scan(int npan, int lev, const int* cnt, long long* off, cudaStream_t st) {

@@ -31,7 +31,10 @@ struct OrderTab {
   int xsteps;
   const double* sk[4];    /* n_l x 4: the selector check's sketch vectors on the level nodes (I_l v, v = +-1) */
   int force_level;        /* 1..nlevel: every pair the walk resolves by a direct sum takes this level (labels) */
+  int adaptive;           /* 1: the adaptive tree walk over the first nlevel-1 (plain 4-split) levels */
 };
+/* pair class of an adaptive cut (G.level, G.cnt slot) */
+#define QOL_LV_CUT 6
 
 /* panel geometry (reference layouts: sx(3,nsrc) etc.) */
 struct PanelIn {
@@ -111,6 +114,9 @@ cudaError_t qol_launch_sel_update(const float* slot, int nslot, float inv_n, flo
 cudaError_t qol_launch_direct(const OrderTab& T, const PanelIn& P, const PairIn& Q, const LevelWS& W,
                               const PairWS& G, const OutCOO& O, int npan, cudaStream_t st,
                               int pan0 = 0 /* first panel of the launch */);
+/* the level sums of the adaptive cuts (pairs of class QOL_LV_CUT) */
+cudaError_t qol_launch_direct_cut(const OrderTab& T, const PanelIn& P, const PairIn& Q, const LevelWS& W,
+                                  const PairWS& G, const OutCOO& O, int npan, cudaStream_t st, int pan0 = 0);
 cudaError_t qol_launch_scan(int npan, int lev, const int* cnt, long long* off, cudaStream_t st);
 cudaError_t qol_launch_rrq_panel(const OrderTab& T, const PanelIn& P, const PairWS& G, const RRQWS& R, int npan,
                                  const double* chart, cudaStream_t st);

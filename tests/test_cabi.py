@@ -128,6 +128,17 @@ def test_selector_arguments_checked(qol):
     assert e.value.code == 8
 
 
+def test_patch_refine_switch_host_only(qol):
+    """iadap 0, 1 and 3 only (square + adaptive is refused, as the reference's
+    build_patch_ref_r64 refuses it)"""
+    for bad in (2, 4, -1):
+        with pytest.raises(qol.QolError) as e:
+            qol.qol_set_patch_refine(bad)
+        assert e.value.code == 8
+    for ok in (1, 3, 0):
+        qol.qol_set_patch_refine(ok)
+
+
 def test_autotune_switch_host_only(qol):
     """the autotune switch accepts 0 and 1 only; an order never run has no kept shape"""
     with pytest.raises(qol.QolError) as e:

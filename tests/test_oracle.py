@@ -55,8 +55,62 @@ def test_reference_levels(orc, nterms):
         assert np.abs(L["interp"] @ f(uvn) - f(L["uv"])).max() < 1e-13 * np.abs(f(L["uv"])).max()
 
 
+@pytest.mark.parametrize("nterms", [4, 7, 13])
+def test_reference_element_matches_independent_restatement(orc, qol, nterms):
+    """the library's refined reference element (levels 1-4, square and plain
+    modes) against oracle/ref_element.py, a numpy derivation from the
+    algorithm that shares no code with the library or the C++ oracle:
+    sub-patch structure exact, nodes to 1e-15, weights to 5e-14 relative
+    (the Gauss-Legendre squares use numpy's rule)"""
+    from oracle import ref_element as RE
+    korder, order = nterms - 1, nterms + 2
+    n1 = order * (order + 1) // 2
+    uv = np.zeros(2 * n1); wt = np.zeros(n1)
+    orc.lib().orc_vr_nodes_export(orc.C.c_int(order - 1), orc._vp(uv), orc._vp(wt))
+    try:
+        for square, iadap in ((True, 0), (False, 3)):
+            qol.qol_set_patch_refine(iadap)
+            ref = RE.reference_element(korder, order, uv, wt, 4, square)
+            for lev in range(4):
+                t = qol.qol_ref_level_table(nterms, order, lev)
+                r = ref[lev]
+                assert np.array_equal(t["suboff"], r["suboff"]) and np.array_equal(t["subtyp"], r["subtyp"])
+                assert np.abs(t["uv"] - r["uv"]).max() <= 1e-15
+                assert np.abs(t["wt"] / r["wt"] - 1.0).max() <= 5e-14
+    finally:
+        qol.qol_set_patch_refine(0)
+
+
+def test_gauss_legendre_matches_numpy(qol):
+    """the library's Gauss-Legendre rule against numpy's"""
+    for nq in (6, 15, 24):
+        tgl, wgl = qol.qol_simplex_precomp(nq, 3)[:2]
+        t, w = np.polynomial.legendre.leggauss(nq)
+        assert np.abs(np.asarray(tgl).ravel() - t).max() < 1e-14
+        assert np.abs(np.asarray(wgl).ravel() - w).max() < 1e-14
+
+
+@pytest.mark.parametrize("korder", [3, 8, 12])
+def test_interp_matrix_reproduces_polynomials(qol, korder):
+    """the interpolation from the Vioreanu-Rokhlin nodes (koorn_pols with
+    umatr) is exact for every monomial u^a v^b, a + b <= korder"""
+    nodes = qol.qol_ref_level_table(korder + 1, korder + 1, 0)["uv"]
+    rng = np.random.default_rng(korder)
+    pts = rng.random((50, 2))
+    pts = pts[pts.sum(1) <= 1.0]
+    M = qol.qol_interp_matrix(korder, pts)
+    worst = 0.0
+    for a in range(korder + 1):
+        for b in range(korder + 1 - a):
+            f = lambda x: x[:, 0] ** a * x[:, 1] ** b
+            worst = max(worst, np.abs(M @ f(nodes) - f(pts)).max())
+    assert worst < 1e-11, worst
+
+
 def test_product_tables_match_oracle(orc, qol):
-    """the library's host tables (qol_simplex_precomp) equal the oracle's"""
+    """the library's host tables (qol_simplex_precomp) equal the oracle's, so
+    both compute with the same rules (their correctness is checked above
+    against numpy and by polynomial reproduction)"""
     for nq, ko in ((6, 3), (15, 12)):
         a = qol.qol_simplex_precomp(nq, ko)
         b = orc.simplex_precomp(nq, ko)
