@@ -185,6 +185,22 @@ int qol_direct_farfield_range(qol_int nsrc, const double* sx, const double* snx,
 int qol_surface_panels(qol_int nmode, const double* modes, qol_int nfp, qol_int mp, qol_int np, qol_int nterms,
                        qol_int split, qol_int* ntri, double* sx, double* snx, double* sw, double* rts,
                        double* rps);
+/* The adaptive chart list (stellarator_charts over build_charts_adaptive,
+ * :427-546, 775-808): the mp x np charts split at aspect 1.65 (repeated
+ * passes), then for restol > 0 quartered while the Legendre tail (the last two
+ * degrees) of the chart's mean curvature on its p x p Gauss grid carries more
+ * than restol of the spectrum, and quartered for 2:1 balance across faces.
+ * charts: 6 doubles a chart (a1, b1, a2, b2, jj, ii: t1 -> a1 t1 + b1 in panel
+ * jj, t2 -> a2 t2 + b2 in panel ii); with charts == NULL only *nchart (the
+ * count); QOL_ERR_NNZ past cap charts or when *nchart is too small.
+ * qol_surface_panels_charts: the GPU geometry generator over such a list
+ * (stellarator_geo_charts :837-856), outputs and size query as
+ * qol_surface_panels. */
+int qol_surface_charts(qol_int nmode, const double* modes, qol_int nfp, qol_int mp, qol_int np, qol_int p,
+                       double restol, qol_int cap, qol_int* nchart, double* charts);
+int qol_surface_panels_charts(qol_int nmode, const double* modes, qol_int nfp, qol_int mp, qol_int np,
+                              qol_int nterms, qol_int nchart, const double* charts, qol_int* ntri, double* sx,
+                              double* snx, double* sw, double* rts, double* rps);
 /* Host helper: the matrix M (n x npols, column-major) interpolating values at
  * the Vioreanu-Rokhlin nodes of degree korder to the points uv (2 x n) of the
  * reference triangle (koorn_pols_batch_r64 times umatr, as

@@ -234,6 +234,53 @@ def ref_geometry(mp, np_, nterms):
     return dict(ntri=int(ntri), sx=sx, snx=snx, sw=sw, rts=rts, rps=rps, x0=x0, D=Dcm)
 
 
+def _modes_args(modes, nfp):
+    m = np.asarray(modes, float).reshape(-1, 4)
+    mn = np.ascontiguousarray(m[:, :2].ravel())
+    rc, zs = np.ascontiguousarray(m[:, 2]), np.ascontiguousarray(m[:, 3])
+    return [C.byref(i64(nfp)), C.byref(i64(m.shape[0])), _vp(mn), _vp(rc), _vp(zs)], (mn, rc, zs)
+
+
+def ref_charts(mp, np_, p, modes, nfp, restol, cap=200000):
+    """utils/stellarator_geo_mex.c:stellarator_charts (build_charts_adaptive)
+    on the surface with VMEC modes (m, n, rc, zs): (nchart, 6) charts"""
+    g = refgeo()
+    if g is None:
+        raise RuntimeError("oracle/_ref/libstellgeo.so missing")
+    x0, _, D = gauss(p)
+    Dcm = np.asfortranarray(D).ravel(order="F").copy()
+    sargs, keep = _modes_args(modes, nfp)
+    g.stellarator_charts.restype = i64
+    args = [C.byref(i64(mp)), C.byref(i64(np_)), C.byref(i64(p)), _vp(x0), _vp(Dcm)] + sargs + \
+           [C.byref(C.c_double(restol)), C.byref(i64(cap))]
+    n = g.stellarator_charts(*args, None)
+    if n < 0:
+        raise RuntimeError("stellarator_charts: over cap")
+    cl = np.zeros(6 * n)
+    g.stellarator_charts(*args, _vp(cl))
+    return cl.reshape(-1, 6)
+
+
+def ref_geometry_charts(charts, mp, np_, nterms, modes, nfp):
+    """utils/stellarator_geo_mex.c:stellarator_geo_charts: the panels of a chart list"""
+    g = refgeo()
+    x0, _, D = gauss(nterms)
+    Dcm = np.asfortranarray(D).ravel(order="F").copy()
+    hd = nterms * (nterms + 1) // 2
+    uvs = np.zeros(2 * hd); wts = np.zeros(hd)
+    lib().orc_vr_nodes_export(C.c_int(nterms - 1), _vp(uvs), _vp(wts))
+    cl = np.ascontiguousarray(np.asarray(charts, float).ravel())
+    n = cl.size // 6
+    nsrc = 2 * n * hd
+    out = {k: np.zeros(3 * nsrc) for k in ("sx", "snx", "rts", "rps")}
+    out["sw"] = np.zeros(nsrc)
+    sargs, keep = _modes_args(modes, nfp)
+    g.stellarator_geo_charts(_vp(cl), C.byref(i64(n)), C.byref(i64(mp)), C.byref(i64(np_)), C.byref(i64(nterms)),
+                             _vp(x0), _vp(Dcm), _vp(uvs), _vp(wts), *sargs, _vp(out["sx"]), _vp(out["snx"]),
+                             _vp(out["sw"]), _vp(out["rts"]), _vp(out["rps"]))
+    return out
+
+
 def ref_uv2x(mp, np_, nterms, itri, uv):
     g = refgeo()
     x0, _, _ = gauss(nterms)

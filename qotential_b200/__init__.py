@@ -16,7 +16,8 @@ __all__ = [
     "lib", "QolError", "qol_simplex_precomp", "qol_build_patch_levels", "qol_lap3dsdlpmat_levels",
     "qol_clear_patch_levels", "qol_clear_patch_levels_all", "qol_rrq", "qol_getnearquad_lap_rrq",
     "qol_getnearquad_lap_rrq_dev", "qol_grf_near", "qol_grf_near_range", "qol_direct_farfield",
-    "qol_direct_farfield_range", "qol_surface_panels", "qol_interp_matrix", "qol_set_sum_precision",
+    "qol_direct_farfield_range", "qol_surface_panels", "qol_surface_charts", "qol_surface_panels_charts",
+    "qol_interp_matrix", "qol_set_sum_precision",
     "SELECTOR_NW", "qol_selector_features", "qol_selector_grad", "qol_selector_train", "qol_selector_set",
     "qol_selector_stats", "qol_selector_force_level", "qol_set_patch_refine", "qol_ref_level_table",
     "qol_set_autotune",
@@ -283,6 +284,39 @@ def qol_surface_panels(surface, mp, np_, nterms, split=True):
     out["sw"] = np.zeros(nsrc)
     _check(lib().qol_surface_panels(*args, _vp(nt), _vp(out["sx"]), _vp(out["snx"]), _vp(out["sw"]),
                                     _vp(out["rts"]), _vp(out["rps"])))
+    out["ntri"] = int(nt[0])
+    out["hdim"] = hd
+    return out
+
+
+def qol_surface_charts(surface, mp, np_, p, restol, cap=200000):
+    """(nchart, 6) adaptive charts (a1, b1, a2, b2, jj, ii) of the surface
+    (utils/stellarator_geo_mex.c build_charts_adaptive): aspect splits, then
+    for restol > 0 curvature refinement and 2:1 balance"""
+    modes, nfp = surface.vmec_modes()
+    modes = np.ascontiguousarray(np.asarray(modes, np.float64).reshape(-1, 4))
+    n = np.zeros(1, np.int64)
+    args = (i64(modes.shape[0]), _vp(modes), i64(nfp), i64(mp), i64(np_), i64(p), C.c_double(restol), i64(cap))
+    _check(lib().qol_surface_charts(*args, _vp(n), None))
+    cl = np.zeros(6 * int(n[0]))
+    _check(lib().qol_surface_charts(*args, _vp(n), _vp(cl)))
+    return cl.reshape(-1, 6)
+
+
+def qol_surface_panels_charts(surface, mp, np_, nterms, charts):
+    """the GPU geometry generator over a chart list: dict as qol_surface_panels"""
+    modes, nfp = surface.vmec_modes()
+    modes = np.ascontiguousarray(np.asarray(modes, np.float64).reshape(-1, 4))
+    cl = np.ascontiguousarray(np.asarray(charts, np.float64).ravel())
+    nt = np.zeros(1, np.int64)
+    args = (i64(modes.shape[0]), _vp(modes), i64(nfp), i64(mp), i64(np_), i64(nterms), i64(cl.size // 6), _vp(cl))
+    _check(lib().qol_surface_panels_charts(*args, _vp(nt), None, None, None, None, None))
+    hd = nterms * (nterms + 1) // 2
+    nsrc = int(nt[0]) * hd
+    out = {k: np.zeros((nsrc, 3)) for k in ("sx", "snx", "rts", "rps")}
+    out["sw"] = np.zeros(nsrc)
+    _check(lib().qol_surface_panels_charts(*args, _vp(nt), _vp(out["sx"]), _vp(out["snx"]), _vp(out["sw"]),
+                                           _vp(out["rts"]), _vp(out["rps"])))
     out["ntri"] = int(nt[0])
     out["hdim"] = hd
     return out

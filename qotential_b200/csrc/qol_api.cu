@@ -1613,14 +1613,10 @@ int qol_grf_near(qol_int npan, qol_int nterms, qol_int nquad, qol_int orderff, d
                             0, npan, u, nnear, level_hist, timeinfo);
 }
 
-int qol_surface_panels(qol_int nmode, const double* modes, qol_int nfp, qol_int mp, qol_int np, qol_int nterms,
-                       qol_int split, qol_int* ntri, double* sx, double* snx, double* sw, double* rts,
-                       double* rps) {
-  std::lock_guard<std::recursive_mutex> g(g_mu);
-  if (!modes || !ntri || nmode < 1 || mp < 1 || np < 1) return fail(QOL_ERR_ARG, "bad arguments");
-  if (nterms < 2 || nterms > 16) return fail(QOL_ERR_ORDER, "nterms outside 2..16");
-  const std::vector<qolh::Chart> cl =
-      qolh::surface_charts((int)nmode, modes, (int)nfp, (int)mp, (int)np, (int)nterms, split != 0);
+/* the GPU geometry generator over a chart list (geo_core, :636-750) */
+static int panels_of_charts(const std::vector<qolh::Chart>& cl, qol_int nmode, const double* modes, qol_int nfp,
+                            qol_int mp, qol_int np, qol_int nterms, qol_int* ntri, double* sx, double* snx,
+                            double* sw, double* rts, double* rps) {
   const qol_int nchart = (qol_int)cl.size(), nt = 2 * nchart;
   if (!sx) { *ntri = nt; return 0; } /* the size query (as stellarator_geo_ntri) */
   if (!snx || !sw || !rts || !rps) return fail(QOL_ERR_ARG, "null output");
@@ -1671,6 +1667,50 @@ int qol_surface_panels(qol_int nmode, const double* modes, qol_int nfp, qol_int 
   CK(cudaMemcpyAsync(rps, drps, sizeof(double) * 3 * nsrc, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   return 0;
+}
+
+int qol_surface_panels(qol_int nmode, const double* modes, qol_int nfp, qol_int mp, qol_int np, qol_int nterms,
+                       qol_int split, qol_int* ntri, double* sx, double* snx, double* sw, double* rts,
+                       double* rps) {
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  if (!modes || !ntri || nmode < 1 || mp < 1 || np < 1) return fail(QOL_ERR_ARG, "bad arguments");
+  if (nterms < 2 || nterms > 16) return fail(QOL_ERR_ORDER, "nterms outside 2..16");
+  const std::vector<qolh::Chart> cl =
+      qolh::surface_charts((int)nmode, modes, (int)nfp, (int)mp, (int)np, (int)nterms, split != 0);
+  return panels_of_charts(cl, nmode, modes, nfp, mp, np, nterms, ntri, sx, snx, sw, rts, rps);
+}
+
+int qol_surface_charts(qol_int nmode, const double* modes, qol_int nfp, qol_int mp, qol_int np, qol_int p,
+                       double restol, qol_int cap, qol_int* nchart, double* charts) {
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  if (!modes || !nchart || nmode < 1 || mp < 1 || np < 1) return fail(QOL_ERR_ARG, "bad arguments");
+  if (p < 2 || p > 16) return fail(QOL_ERR_ORDER, "p outside 2..16");
+  std::vector<qolh::Chart> cl;
+  if (!qolh::surface_charts_adaptive((int)nmode, modes, (int)nfp, (int)mp, (int)np, (int)p, restol, cap, cl))
+    return fail(QOL_ERR_NNZ, "qol_surface_charts: more than cap charts");
+  if (charts) {
+    if (*nchart < (qol_int)cl.size()) return fail(QOL_ERR_NNZ, "nchart is smaller than the chart count");
+    for (size_t k = 0; k < cl.size(); ++k) {
+      const double v[6] = {cl[k].a1, cl[k].b1, cl[k].a2, cl[k].b2, cl[k].jj, cl[k].ii};
+      for (int d = 0; d < 6; ++d) charts[6 * k + d] = v[d];
+    }
+  }
+  *nchart = (qol_int)cl.size();
+  return 0;
+}
+
+int qol_surface_panels_charts(qol_int nmode, const double* modes, qol_int nfp, qol_int mp, qol_int np,
+                              qol_int nterms, qol_int nchart, const double* charts, qol_int* ntri, double* sx,
+                              double* snx, double* sw, double* rts, double* rps) {
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  if (!modes || !ntri || !charts || nmode < 1 || mp < 1 || np < 1 || nchart < 1)
+    return fail(QOL_ERR_ARG, "bad arguments");
+  if (nterms < 2 || nterms > 16) return fail(QOL_ERR_ORDER, "nterms outside 2..16");
+  std::vector<qolh::Chart> cl((size_t)nchart);
+  for (qol_int k = 0; k < nchart; ++k)
+    cl[k] = qolh::Chart{charts[6 * k], charts[6 * k + 1], charts[6 * k + 2], charts[6 * k + 3], charts[6 * k + 4],
+                        charts[6 * k + 5]};
+  return panels_of_charts(cl, nmode, modes, nfp, mp, np, nterms, ntri, sx, snx, sw, rts, rps);
 }
 
 int qol_interp_matrix(qol_int korder, qol_int n, const double* uv, double* M) {

@@ -411,6 +411,237 @@ std::vector<Chart> surface_charts(int nmode, const double* modes, int nfp, int m
   return cl;
 }
 
+namespace {
+/* a chart's point: t1, t2 in [-1, 1] -> the surface at toroidal
+ * ((a1 t1 + b1) + 2 jj) ts1, poloidal ((a2 t2 + b2) + 2 ii) ts2 */
+struct ChartMap {
+  int nmode, nfp;
+  const double* modes;
+  double ts1, ts2;
+  void point(const Chart& c, double t1, double t2, double* x) const {
+    surface_eval(nmode, modes, nfp, ((c.a1 * t1 + c.b1) + 2.0 * c.jj) * ts1, ((c.a2 * t2 + c.b2) + 2.0 * c.ii) * ts2,
+                 x);
+  }
+};
+
+double dist3(const double* a, const double* b) {
+  return std::sqrt((a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1]) + (a[2] - b[2]) * (a[2] - b[2]));
+}
+
+/* the chart's parameter box [t1lo, t1hi, t2lo, t2hi] in units of ts1, ts2 */
+void chart_box(const Chart& c, double ts1, double ts2, double* bx) {
+  bx[0] = ((c.b1 - c.a1) + 2.0 * c.jj) * ts1;
+  bx[1] = ((c.b1 + c.a1) + 2.0 * c.jj) * ts1;
+  bx[2] = ((c.b2 - c.a2) + 2.0 * c.ii) * ts2;
+  bx[3] = ((c.b2 + c.a2) + 2.0 * c.ii) * ts2;
+}
+
+/* the four quarters of a chart, (-,-), (+,-), (-,+), (+,+) in (t1, t2) */
+void quarters(const Chart& c, Chart* q) {
+  for (int k = 0; k < 4; ++k) {
+    q[k] = c;
+    q[k].a1 = c.a1 / 2.0;
+    q[k].a2 = c.a2 / 2.0;
+    q[k].b1 = c.b1 + ((k & 1) ? c.a1 / 2.0 : -c.a1 / 2.0);
+    q[k].b2 = c.b2 + ((k & 2) ? c.a2 / 2.0 : -c.a2 / 2.0);
+  }
+}
+
+/* A X = B in place (A p x p, B p x q, column-major), partial pivoting by
+ * rows of the augmented system */
+void solve_inplace(double* A, int p, double* B, int q) {
+  for (int k = 0; k < p; ++k) {
+    int ipv = k;
+    double pmax = std::fabs(A[k + k * p]);
+    for (int i = k + 1; i < p; ++i)
+      if (std::fabs(A[i + k * p]) > pmax) { pmax = std::fabs(A[i + k * p]); ipv = i; }
+    if (ipv != k) {
+      for (int j = 0; j < p; ++j) std::swap(A[k + j * p], A[ipv + j * p]);
+      for (int j = 0; j < q; ++j) std::swap(B[k + j * p], B[ipv + j * p]);
+    }
+    for (int i = k + 1; i < p; ++i) {
+      const double f = A[i + k * p] / A[k + k * p];
+      A[i + k * p] = f;
+      for (int j = k + 1; j < p; ++j) A[i + j * p] -= f * A[k + j * p];
+      for (int j = 0; j < q; ++j) B[i + j * p] -= f * B[k + j * p];
+    }
+  }
+  for (int j = 0; j < q; ++j)
+    for (int i = p - 1; i >= 0; --i) {
+      double v = B[i + j * p];
+      for (int k = i + 1; k < p; ++k) v -= A[i + k * p] * B[k + j * p];
+      B[i + j * p] = v / A[i + i * p];
+    }
+}
+
+/* panel_resolution (:338-416): the mean curvature H of the chart on its p x p
+ * Gauss grid (node a + b p at (t1, t2) = (x0[b], x0[a])), from spectral
+ * first and second derivatives (D), expanded in the tensor Legendre basis
+ * (C = V^-1 H V^-T); the 2-norm share of the coefficients of degree p-2 or
+ * p-1 in either direction */
+double curvature_tail(const ChartMap& S, const Chart& c, int p, const std::vector<double>& x0,
+                      const std::vector<double>& D, const std::vector<double>& V) {
+  const int n2 = p * p;
+  std::vector<double> X(3 * n2), r1(3 * n2), r2(3 * n2), r11(3 * n2), r12(3 * n2), r22(3 * n2), H(n2), Cf(n2),
+      Tt(n2), A(n2);
+  for (int b = 0; b < p; ++b)
+    for (int a = 0; a < p; ++a) S.point(c, x0[b], x0[a], &X[3 * (a + b * p)]);
+  auto along_t2 = [&](const std::vector<double>& f, std::vector<double>& g) { /* d/d(index a) */
+    for (int b = 0; b < p; ++b)
+      for (int a = 0; a < p; ++a)
+        for (int d = 0; d < 3; ++d) {
+          double v = 0.0;
+          for (int k = 0; k < p; ++k) v += D[a + k * p] * f[3 * (k + b * p) + d];
+          g[3 * (a + b * p) + d] = v;
+        }
+  };
+  auto along_t1 = [&](const std::vector<double>& f, std::vector<double>& g) { /* d/d(index b) */
+    for (int b = 0; b < p; ++b)
+      for (int a = 0; a < p; ++a)
+        for (int d = 0; d < 3; ++d) {
+          double v = 0.0;
+          for (int k = 0; k < p; ++k) v += D[b + k * p] * f[3 * (a + k * p) + d];
+          g[3 * (a + b * p) + d] = v;
+        }
+  };
+  along_t1(X, r1); along_t2(X, r2);
+  along_t1(r1, r11); along_t1(r2, r12); along_t2(r2, r22);
+  for (int k = 0; k < n2; ++k) {
+    const double* u = &r1[3 * k];
+    const double* v = &r2[3 * k];
+    double nv[3] = {u[1] * v[2] - u[2] * v[1], u[2] * v[0] - u[0] * v[2], u[0] * v[1] - u[1] * v[0]};
+    double nn = std::sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]);
+    if (nn <= 0.0) nn = 1.0;
+    for (double& t : nv) t /= nn;
+    const double E = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+    const double F = u[0] * v[0] + u[1] * v[1] + u[2] * v[2];
+    const double G = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    const double L = nv[0] * r11[3 * k] + nv[1] * r11[3 * k + 1] + nv[2] * r11[3 * k + 2];
+    const double M = nv[0] * r12[3 * k] + nv[1] * r12[3 * k + 1] + nv[2] * r12[3 * k + 2];
+    const double N = nv[0] * r22[3 * k] + nv[1] * r22[3 * k + 1] + nv[2] * r22[3 * k + 2];
+    double den = 2.0 * (E * G - F * F);
+    if (den == 0.0) den = 1.0;
+    H[k] = (E * N - 2.0 * F * M + G * L) / den;
+  }
+  Cf = H;
+  A = V;
+  solve_inplace(A.data(), p, Cf.data(), p);
+  for (int a = 0; a < p; ++a)
+    for (int b = 0; b < p; ++b) Tt[b + a * p] = Cf[a + b * p];
+  A = V;
+  solve_inplace(A.data(), p, Tt.data(), p);
+  double tail = 0.0, tot = 0.0;
+  for (int a = 0; a < p; ++a)
+    for (int b = 0; b < p; ++b) {
+      const double z = Tt[b + a * p];
+      tot += z * z;
+      if (a >= p - 2 || b >= p - 2) tail += z * z;
+    }
+  return std::sqrt(tail / (tot > 0.0 ? tot : 1.0));
+}
+} // namespace
+
+bool surface_charts_adaptive(int nmode, const double* modes, int nfp, int mp, int np, int p, double restol,
+                             long long cap, std::vector<Chart>& L) {
+  const double ASPECT = 1.65;
+  const int ASPECT_PASSES = 8, CURV_LEVELS = 12, BALANCE_SWEEPS = 20;
+  if (cap <= 0) cap = 200000;
+  std::vector<double> x0(p), w0(p), D((size_t)p * p), V((size_t)p * p);
+  gauss(p, x0.data(), w0.data(), D.data());
+  for (int i = 0; i < p; ++i) { /* Legendre Vandermonde V[i + k p] = P_k(x0_i) */
+    V[i] = 1.0;
+    if (p > 1) V[i + p] = x0[i];
+    for (int k = 1; k < p - 1; ++k)
+      V[i + (k + 1) * p] = ((2.0 * k + 1.0) * x0[i] * V[i + k * p] - k * V[i + (k - 1) * p]) / (k + 1.0);
+  }
+  const ChartMap S{nmode, nfp, modes, QOL_PI_H / np, QOL_PI_H / mp};
+  L.clear();
+  for (int j = 1; j <= np; ++j)
+    for (int i = 1; i <= mp; ++i) L.push_back(Chart{1.0, 0.0, 1.0, 0.0, (double)j, (double)i});
+  if ((long long)L.size() > cap) return false;
+  /* 1. aspect: halve along the longer side, the second half appended (and
+   * tested again within the same pass) */
+  for (int pass = 0; pass < ASPECT_PASSES; ++pass) {
+    int nsplit = 0;
+    for (size_t k = 0; k < L.size(); ++k) {
+      const Chart c = L[k];
+      double xll[3], xul[3], xlr[3];
+      S.point(c, x0[0], x0[0], xll);
+      S.point(c, x0[0], x0[p - 1], xul);
+      S.point(c, x0[p - 1], x0[0], xlr);
+      const double dt = dist3(xll, xlr), dp = dist3(xll, xul);
+      if (dt / dp > ASPECT || dp / dt > ASPECT) {
+        if ((long long)L.size() >= cap) return false;
+        Chart lo = c, hi = c;
+        if (dt / dp > ASPECT) { lo.a1 = hi.a1 = c.a1 / 2.0; lo.b1 = c.b1 - c.a1 / 2.0; hi.b1 = c.b1 + c.a1 / 2.0; }
+        else { lo.a2 = hi.a2 = c.a2 / 2.0; lo.b2 = c.b2 - c.a2 / 2.0; hi.b2 = c.b2 + c.a2 / 2.0; }
+        L[k] = lo;
+        L.push_back(hi);
+        ++nsplit;
+      }
+    }
+    if (!nsplit) break;
+  }
+  if (restol <= 0.0) return true;
+  /* 2. curvature: quarter a chart while its curvature tail exceeds restol;
+   * a chart that passes is not tested again */
+  std::vector<char> done(L.size(), 0);
+  for (int pass = 0; pass < CURV_LEVELS; ++pass) {
+    int nsplit = 0;
+    const size_t n0 = L.size();
+    for (size_t k = 0; k < n0; ++k) {
+      if (done[k]) continue;
+      if (curvature_tail(S, L[k], p, x0, D, V) <= restol) { done[k] = 1; continue; }
+      if ((long long)L.size() + 3 > cap) return false;
+      Chart q[4];
+      quarters(L[k], q);
+      L[k] = q[0];
+      for (int t = 1; t < 4; ++t) { L.push_back(q[t]); done.push_back(0); }
+      ++nsplit;
+    }
+    if (!nsplit) break;
+  }
+  /* 3. 2:1 balance: quarter a chart whose face is longer than twice a face
+   * neighbour's (periodic in both panel indices) */
+  const double ts1 = S.ts1, ts2 = S.ts2;
+  for (int pass = 0; pass < BALANCE_SWEEPS; ++pass) {
+    const size_t n0 = L.size();
+    std::vector<char> split(n0, 0);
+    for (size_t k = 0; k < n0; ++k) {
+      double bk[4];
+      chart_box(L[k], ts1, ts2, bk);
+      for (size_t q = 0; q < n0; ++q) {
+        if (q == k) continue;
+        const double dj = std::fabs(L[q].jj - L[k].jj), di = std::fabs(L[q].ii - L[k].ii);
+        if (dj > 1.5 && std::fabs(dj - np) > 1.5) continue;
+        if (di > 1.5 && std::fabs(di - mp) > 1.5) continue;
+        double bq[4];
+        chart_box(L[q], ts1, ts2, bq);
+        const double du = 1e-9 * ts1, dv = 1e-9 * ts2;
+        if ((std::fabs(bk[1] - bq[0]) < du || std::fabs(bk[0] - bq[1]) < du) &&
+            std::fmin(bk[3], bq[3]) - std::fmax(bk[2], bq[2]) > dv) {
+          if (bk[3] - bk[2] > 2.0 * (bq[3] - bq[2]) + dv) split[k] = 1;
+        } else if ((std::fabs(bk[3] - bq[2]) < dv || std::fabs(bk[2] - bq[3]) < dv) &&
+                   std::fmin(bk[1], bq[1]) - std::fmax(bk[0], bq[0]) > du) {
+          if (bk[1] - bk[0] > 2.0 * (bq[1] - bq[0]) + du) split[k] = 1;
+        }
+      }
+    }
+    int nsplit = 0;
+    for (size_t k = 0; k < n0; ++k) {
+      if (!split[k]) continue;
+      if ((long long)L.size() + 3 > cap) return false;
+      Chart q[4];
+      quarters(L[k], q);
+      L[k] = q[0];
+      for (int t = 1; t < 4; ++t) L.push_back(q[t]);
+      ++nsplit;
+    }
+    if (!nsplit) break;
+  }
+  return true;
+}
+
 void surface_interp_tables(int p, std::vector<double>& tables) {
   const int hd = p * (p + 1) / 2;
   std::vector<double> x0(p), w0(p), uv(2 * hd);

@@ -75,6 +75,12 @@ void surface_eval(int nmode, const double* modes, int nfp, double t, double p, d
  * utils/stellarator_geo_mex.c:125-160; split at aspect 1.65 when requested) */
 struct Chart { double a1, b1, a2, b2, jj, ii; };
 std::vector<Chart> surface_charts(int nmode, const double* modes, int nfp, int mp, int np, int nterms, bool split);
+/* build_charts_adaptive (utils/stellarator_geo_mex.c:427-546): aspect passes,
+ * then, for restol > 0, curvature refinement (the Legendre tail of the mean
+ * curvature on the chart's p x p Gauss grid above restol) and 2:1 balance.
+ * false when the list would exceed cap charts. */
+bool surface_charts_adaptive(int nmode, const double* modes, int nfp, int mp, int np, int p, double restol,
+                             long long cap, std::vector<Chart>& out);
 /* Lagrange interpolation from the p Gauss nodes, tensor form: M (hd x p^2,
  * row-major, column m = a + b p) for the VR nodes of degree p-1 under the
  * four chart orientations (geo_core, :636-750): keys lA (u, v), rA (-u, -v),

@@ -7,7 +7,12 @@ Writes tests/golden/grf_order{4,6}.npz with u, ub, ubn, the GRF scalar, a
 strided subset of sx/snx/sw (every 7th node) and the SHA-256 of the full
 f64 sx/snx/sw arrays, and tests/golden/render_order{4,6}.npz with the render
 lattice's sizes, every 11th render vertex (position and log error) and the
-SHA-256 of the render triangles.  Run in a container that has the reference checkout,
+SHA-256 of the render triangles, and tests/golden/adaptive_charts.npz: the
+adaptive chart list of the reference's own geometry generator
+(utils/stellarator_geo_mex.c stellarator_charts, compiled into oracle/_ref by
+oracle/Makefile) for the stellarator surface, mp 6 x np 16, p 6, restol 1e-2,
+and a strided subset of the panels its stellarator_geo_charts makes of that
+list at nterms 6.  Run in a container that has the reference checkout,
 naming its root (the argument, or the QOL_REFERENCE_DIR environment variable):
     python tests/golden/make_golden.py <reference checkout>
 """
@@ -56,6 +61,22 @@ def main():
             render_xyz_sub=f["render_xyz"].reshape(-1, 3)[rsub], render_log_error_sub=f["render_log_error"][rsub],
             sha_render_triangles=hashlib.sha256(f["render_triangles"].astype("<i8").tobytes()).hexdigest())
         print(order, f["sha256"])
+    adaptive_charts(here)
+
+
+def adaptive_charts(here, mp=6, np_=16, p=6, restol=1e-2):
+    sys.path.insert(0, os.path.dirname(os.path.dirname(here)))
+    import oracle as O
+    from qotential_b200 import geometry as G
+    modes, nfp = G.stellarator().vmec_modes()
+    cl = O.ref_charts(mp, np_, p, modes, nfp, restol)
+    geo = O.ref_geometry_charts(cl, mp, np_, p, modes, nfp)
+    sub = np.arange(0, geo["sw"].size, 13)
+    np.savez_compressed(os.path.join(here, "adaptive_charts.npz"), mp=mp, np_=np_, p=p, restol=restol, charts=cl,
+                        sub=sub, sx_sub=geo["sx"].reshape(-1, 3)[sub], snx_sub=geo["snx"].reshape(-1, 3)[sub],
+                        sw_sub=geo["sw"][sub], rts_sub=geo["rts"].reshape(-1, 3)[sub],
+                        rps_sub=geo["rps"].reshape(-1, 3)[sub])
+    print("adaptive charts", cl.shape[0])
 
 
 if __name__ == "__main__":

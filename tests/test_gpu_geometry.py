@@ -70,3 +70,18 @@ def test_fixture_run_from_gpu_geometry_as_stgrf001(qol, orc, tmp_path, order, pa
     assert np.abs(d["ubn"] - z["ubn"]).max() < 1e-11          # the reference's gate (:362-363)
     du = np.abs(d["u"] - z["u"])
     assert du.max() / max(1.0, np.abs(z["u"]).max()) < fs_bound
+
+
+def test_adaptive_chart_panels_match_reference_fixture(qol):
+    """the GPU generator over the reference's adaptive chart list
+    (qol_surface_panels_charts) against the panels the reference's
+    stellarator_geo_charts made of it (tests/golden/adaptive_charts.npz)"""
+    from qotential_b200 import geometry as G
+    z = np.load(os.path.join(HERE, "golden", "adaptive_charts.npz"))
+    p = int(z["p"])
+    a = qol.qol_surface_panels_charts(G.stellarator(), int(z["mp"]), int(z["np_"]), p, z["charts"])
+    assert a["ntri"] == 2 * z["charts"].shape[0]
+    sub = z["sub"]
+    for k in ("sx", "snx", "sw", "rts", "rps"):
+        x, y = np.asarray(a[k])[sub], z[k + "_sub"]
+        assert np.abs(x - y).max() <= TOL * np.abs(y).max(), (k, np.abs(x - y).max())
