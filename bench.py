@@ -440,8 +440,9 @@ def batched_config(reps=2):
     grids 4x8 .. 16x64, orders drawn from {4,6,8,10,12}, all surface nodes plus
     5000 off-surface targets each; the device entry point with inputs resident,
     (a) one call per surface, back to back, (b) one call per order group of the
-    concatenated surfaces (qotential_b200.batch); CUDA events around the whole
-    set, best of `reps`.  The config's 4 right-hand sides belong to the GRF
+    concatenated surfaces (qotential_b200.batch), (c) one call for all groups
+    (qol_getnearquad_lap_rrq_batch_dev: the level sums of every group in one
+    persistent launch); CUDA events around the whole set, best of `reps`.  The config's 4 right-hand sides belong to the GRF
     apply, which this near-correction step does not include."""
     import torch
     from qotential_b200 import batch as B
@@ -504,7 +505,14 @@ def batched_config(reps=2):
         combs.append((comb, B.device_inputs(comb, dev)))
     o = outbuf(max(int(c["tcxrow"].size) * c["hd"] for c, _ in combs))
     ms_b = timed([lambda c=c, D=D: B.run_device(c, D, o, stream=st.cuda_stream) for c, D in combs])
-    del combs, o
+    del o
+    torch.cuda.empty_cache()
+    # (c) one library call for all order groups: the level sums of every group in one persistent
+    # launch fed by a level-binned work queue (each group needs its own outputs: about 50 GB)
+    outs = [outbuf(int(c["tcxrow"].size) * c["hd"]) for c, _ in combs]
+    cs, Ds = [c for c, _ in combs], [D for _, D in combs]
+    ms_c = timed([lambda: B.run_device_batch(cs, Ds, outs, stream=st.cuda_stream)])
+    del combs, outs, cs, Ds
     torch.cuda.empty_cache()
     orders = {}
     for p in probs:
@@ -513,7 +521,13 @@ def batched_config(reps=2):
             "orders": orders, "geometry_s": round(t_geo, 1),
             "per_surface": {"ms": ms_a, "pairs_per_s": npairs / (ms_a * 1e-3), "calls": len(probs)},
             "batched": {"ms": ms_b, "pairs_per_s": npairs / (ms_b * 1e-3), "calls": len(groups)},
-            "speedup": ms_a / ms_b}
+            "one_call": {"ms": ms_c, "pairs_per_s": npairs / (ms_c * 1e-3), "calls": 1,
+                         "level_sum_launches": 1},
+            "speedup": ms_a / ms_b, "speedup_one_call": ms_a / ms_c,
+            "note": "per_surface: 64 device calls; batched: the surfaces of each order concatenated, one call per "
+                    "order (5); one_call: qol_getnearquad_lap_rrq_batch_dev over the 5 order groups, the level sums "
+                    "of all in one persistent kernel over a (job, panel, level) queue, finest level first; the "
+                    "config's 4 right-hand sides belong to the GRF apply, which this step does not include"}
 
 
 def config_dict(W, world):

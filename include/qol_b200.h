@@ -111,6 +111,32 @@ int qol_getnearquad_lap_rrq_dev(qol_int npan, qol_int nterms, qol_int hdim, qol_
                                 qol_int nnz, qol_int* sparsei, qol_int* sparsej, double* sparsevs,
                                 double* sparsevd, void* stream, int sync, qol_int* level_hist);
 
+/* Batched device form (no counterpart in the reference, which computes one
+ * surface a call; its GRF driver loops over panels, stellarator_grf_core_mod.
+ * f90:760-888): njob getnearquad problems, each with the arguments of
+ * qol_getnearquad_lap_rrq_dev (device pointers), of any orders, in one call.
+ * Every job's refined levels and pair classes are computed first; then the
+ * FP64 level sums of all jobs run in ONE persistent kernel that takes (job,
+ * panel, level) items from a device work queue ordered by level (finest, the
+ * longest items, first); then every job's RRQ phases and COO indices.  The
+ * outputs are each job's own qol_getnearquad_lap_rrq_dev outputs byte for
+ * byte.  With the FP32 level sums (qol_set_sum_precision(1)) the level sums
+ * run per job instead.  level_hist: 6 entries a job (nullable).  Returns
+ * after the work on `stream` is done. */
+typedef struct {
+  qol_int npan, nterms, hdim, nquad, nsrc;
+  const double *sx, *snx, *sw, *rts, *rps;
+  qol_int ntcx;
+  const double* tcx;
+  const qol_int *tcxrow, *tcxi;
+  qol_int orderff;
+  double distff;
+  qol_int iside, nnz;
+  qol_int *sparsei, *sparsej;
+  double *sparsevs, *sparsevd;
+} qol_near_job;
+int qol_getnearquad_lap_rrq_batch_dev(qol_int njob, const qol_near_job* jobs, void* stream, qol_int* level_hist);
+
 /* No counterpart in the reference.  The work of qol_rrq for one panel (As, Ad;
  * no Omega/IalphaAsvestas/timeinfo) for callers that cannot allocate GPU
  * memory: codes inside a host application that owns all GPU memory through its

@@ -15,7 +15,7 @@ import numpy as np
 __all__ = [
     "lib", "QolError", "qol_simplex_precomp", "qol_build_patch_levels", "qol_lap3dsdlpmat_levels",
     "qol_clear_patch_levels", "qol_clear_patch_levels_all", "qol_rrq", "qol_getnearquad_lap_rrq",
-    "qol_getnearquad_lap_rrq_dev", "qol_grf_near", "qol_grf_near_range", "qol_direct_farfield",
+    "qol_getnearquad_lap_rrq_dev", "qol_getnearquad_lap_rrq_batch_dev", "qol_grf_near", "qol_grf_near_range", "qol_direct_farfield",
     "qol_direct_farfield_range", "qol_surface_panels", "qol_surface_charts", "qol_surface_panels_charts",
     "qol_interp_matrix", "qol_set_sum_precision",
     "SELECTOR_NW", "qol_selector_features", "qol_selector_grad", "qol_selector_train", "qol_selector_set",
@@ -209,6 +209,38 @@ def qol_getnearquad_lap_rrq_dev(npan, nterms, nquad, sx, snx, sw, rts, rps, tcx,
         _vp(hist) if want_hist else None)
     _check(rc)
     return hist if want_hist else None
+
+
+class _NearJob(C.Structure):
+    _fields_ = [("npan", C.c_longlong), ("nterms", C.c_longlong), ("hdim", C.c_longlong), ("nquad", C.c_longlong),
+                ("nsrc", C.c_longlong), ("sx", C.c_void_p), ("snx", C.c_void_p), ("sw", C.c_void_p),
+                ("rts", C.c_void_p), ("rps", C.c_void_p), ("ntcx", C.c_longlong), ("tcx", C.c_void_p),
+                ("tcxrow", C.c_void_p), ("tcxi", C.c_void_p), ("orderff", C.c_longlong), ("distff", C.c_double),
+                ("iside", C.c_longlong), ("nnz", C.c_longlong), ("sparsei", C.c_void_p), ("sparsej", C.c_void_p),
+                ("sparsevs", C.c_void_p), ("sparsevd", C.c_void_p)]
+
+
+def qol_getnearquad_lap_rrq_batch_dev(jobs, stream=0):
+    """Batched device form: ``jobs`` is a list of dicts with npan, nterms,
+    nquad, orderff (default nquad), distff (1.4), iside (30) and device arrays
+    (objects with data_ptr(), e.g. CUDA tensors) sx, snx, sw, rts, rps, tcx,
+    tcxrow, tcxi and out = (sparsei, sparsej, sparsevs, sparsevd).  One call;
+    the level sums of all jobs in one persistent launch.  Returns the level
+    histograms (njob x 6)."""
+    ptr = lambda a: a if isinstance(a, int) else a.data_ptr()
+    arr = (_NearJob * max(1, len(jobs)))()
+    for k, j in enumerate(jobs):
+        nterms = int(j["nterms"])
+        hd = nterms * (nterms + 1) // 2
+        si, sj, vs, vd = j["out"]
+        nq = int(j["nquad"])
+        arr[k] = _NearJob(int(j["npan"]), nterms, hd, nq, int(j["npan"]) * hd, ptr(j["sx"]), ptr(j["snx"]),
+                          ptr(j["sw"]), ptr(j["rts"]), ptr(j["rps"]), int(j["tcxrow"].numel()), ptr(j["tcx"]),
+                          ptr(j["tcxrow"]), ptr(j["tcxi"]), int(j.get("orderff", nq)), float(j.get("distff", 1.4)),
+                          int(j.get("iside", 30)), int(vs.numel()), ptr(si), ptr(sj), ptr(vs), ptr(vd))
+    hist = np.zeros((max(1, len(jobs)), 6), np.int64)
+    _check(lib().qol_getnearquad_lap_rrq_batch_dev(i64(len(jobs)), arr, C.c_void_p(stream), _vp(hist)))
+    return hist[:len(jobs)]
 
 
 def qol_grf_near(npan, nterms, nquad, sx, snx, sw, rts, rps, ub, ubn, u=None, orderff=None, distff=1.4,

@@ -16,7 +16,7 @@ orderff, sx, snx, sw, rts, rps (hd nodes a panel), tcx (ntcx x 3), tcxrow
 """
 import numpy as np
 
-from . import qol_getnearquad_lap_rrq, qol_getnearquad_lap_rrq_dev
+from . import qol_getnearquad_lap_rrq, qol_getnearquad_lap_rrq_batch_dev, qol_getnearquad_lap_rrq_dev
 
 
 def _key(p):
@@ -94,3 +94,13 @@ def run_device(comb, D, out, stream=0, sync=False, distff=1.4, iside=30):
     return qol_getnearquad_lap_rrq_dev(comb["npan"], comb["nterms"], comb["nquad"], D["sx"], D["snx"], D["sw"],
                                        D["rts"], D["rps"], D["tcx"], D["tcxrow"], D["tcxi"], comb["orderff"], distff,
                                        iside, out, stream=stream, sync=sync)
+
+
+def run_device_batch(combs, Ds, outs, stream=0, distff=1.4, iside=30):
+    """every combined problem (any orders) in ONE library call: the level sums
+    of all of them in one persistent launch fed by a level-binned work queue;
+    returns the level histograms"""
+    jobs = [dict(npan=c["npan"], nterms=c["nterms"], nquad=c["nquad"], orderff=c["orderff"], distff=distff,
+                 iside=iside, out=o, **{k: D[k] for k in ("sx", "snx", "sw", "rts", "rps", "tcx", "tcxrow", "tcxi")})
+            for c, D, o in zip(combs, Ds, outs)]
+    return qol_getnearquad_lap_rrq_batch_dev(jobs, stream=stream)

@@ -323,17 +323,54 @@ int aux_stream(cudaStream_t* out) {
   return 0;
 }
 
-int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* hist_out, std::vector<int>* grp_out,
-                 int* cnt_out) {
+/* one pipeline call, in two stages: front() sizes and lays out the
+ * workspace, computes the refined levels, classifies the pairs and sizes the
+ * per-pair RRQ storage (one host read of the RRQ count); back() runs the level
+ * sums (unless done elsewhere: the batched entry's persistent kernel), the
+ * RRQ phases and the COO indices */
+struct PipeRun {
+  const Job& J;
+  cudaStream_t st;
+  double* timeinfo;
+  Arena* A1;
+  Arena* A2;
   OrderCache* C = nullptr;
+  OrderTab T{};
+  int hd = 0, npan = 0, nq = 0, nbd = 0;
+  long long ntcx = 0, nrrq = 0;
+  LevelWS W{};
+  PairWS G{};
+  RRQWS R{};
+  OutCOO O{};
+  long long* rrq_off = nullptr;
+  std::vector<long long> off_h;
+  Timing tm;
+  cudaStream_t st2 = nullptr;
+  PipeRun(const Job& j, cudaStream_t s, double* ti, Arena* a1 = &g_arena, Arena* a2 = &g_arena2)
+      : J(j), st(s), timeinfo(ti), A1(a1), A2(a2) {}
+  void rec(int phase, int sidx = 0) {
+    if (!tm.on) return;
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return;
+    cudaEventRecord(e, sidx ? st2 : st);
+    tm.ev.push_back(e);
+    tm.ph.push_back(phase);
+    tm.sid.push_back(sidx);
+  }
+  int front();
+  int back(long long* hist_out, std::vector<int>* grp_out, int* cnt_out, bool direct_done);
+};
+
+int PipeRun::front() {
+  C = nullptr;
   int rc = order_tables(J.nterms, J.orderff, J.nquad, &C);
   if (rc) return rc;
-  OrderTab T = C->T;
+  T = C->T;
   T.dist = J.distff;
   T.sum_fp32 = g_sum_precision == 1;
   T.force_level = g_force_level;
-  const int hd = T.hd, npan = J.npan, nq = T.nquad, nbd = 3 * nq;
-  const long long ntcx = J.ntcx;
+  hd = T.hd; npan = J.npan; nq = T.nquad; nbd = 3 * nq;
+  ntcx = J.ntcx;
   /* workspace size */
   size_t need = 0;
   auto add = [&](size_t bytes) { need += (bytes + 255) & ~(size_t)255; };
@@ -342,48 +379,38 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
   add(sizeof(long long) * (npan + 1));
   add(sizeof(double) * (size_t)npan * (RRQ_FRAME + 6 * nbd + 9 * nq + 6 * hd));
   add(sizeof(double) * (size_t)npan * hd * hd * 7);
-  rc = g_arena.reserve(need + 4096);
+  rc = A1->reserve(need + 4096);
   if (rc) return rc;
-  g_arena.reset();
-  LevelWS W{};
+  A1->reset();
+  W = LevelWS{};
   for (int l = 0; l < 4; ++l) {
-    W.node[l] = g_arena.take<double>((size_t)npan * T.n[l] * 7);
-    W.sub[l] = g_arena.take<double>((size_t)npan * T.nsub[l] * 4);
+    W.node[l] = A1->take<double>((size_t)npan * T.n[l] * 7);
+    W.sub[l] = A1->take<double>((size_t)npan * T.nsub[l] * 4);
   }
-  PairWS G{};
-  G.level = g_arena.take<signed char>(ntcx);
-  G.grp = g_arena.take<int>(ntcx);
-  G.cnt = g_arena.take<int>((size_t)npan * 8);
-  G.off = g_arena.take<int>((size_t)npan * 8);
-  RRQWS R{};
+  G = PairWS{};
+  G.level = A1->take<signed char>(ntcx);
+  G.grp = A1->take<int>(ntcx);
+  G.cnt = A1->take<int>((size_t)npan * 8);
+  G.off = A1->take<int>((size_t)npan * 8);
+  R = RRQWS{};
   R.npan = npan;
-  long long* rrq_off = g_arena.take<long long>(npan + 1);
+  rrq_off = A1->take<long long>(npan + 1);
   R.rrq_off = rrq_off;
-  R.frame = g_arena.take<double>((size_t)npan * RRQ_FRAME);
-  R.bx = g_arena.take<double>((size_t)npan * 3 * nbd);
-  R.bt = g_arena.take<double>((size_t)npan * 3 * nbd);
-  R.cf = g_arena.take<double>((size_t)npan * 9 * nq);
-  R.scf = g_arena.take<double>((size_t)npan * 3 * hd);
-  R.sxf = g_arena.take<double>((size_t)npan * 3 * hd);
-  R.hmat = g_arena.take<double>((size_t)npan * hd * hd);
-  R.smat = g_arena.take<double>((size_t)npan * hd * hd);
-  R.PD = g_arena.take<double>((size_t)npan * 4 * hd * hd);
-  R.B = g_arena.take<double>((size_t)npan * hd * hd);
+  R.frame = A1->take<double>((size_t)npan * RRQ_FRAME);
+  R.bx = A1->take<double>((size_t)npan * 3 * nbd);
+  R.bt = A1->take<double>((size_t)npan * 3 * nbd);
+  R.cf = A1->take<double>((size_t)npan * 9 * nq);
+  R.scf = A1->take<double>((size_t)npan * 3 * hd);
+  R.sxf = A1->take<double>((size_t)npan * 3 * hd);
+  R.hmat = A1->take<double>((size_t)npan * hd * hd);
+  R.smat = A1->take<double>((size_t)npan * hd * hd);
+  R.PD = A1->take<double>((size_t)npan * 4 * hd * hd);
+  R.B = A1->take<double>((size_t)npan * hd * hd);
   R.ialpha = J.ialpha;
   CK(cudaMemsetAsync(G.cnt, 0, sizeof(int) * (size_t)npan * 8, st));
   CK(cudaMemsetAsync(G.off, 0, sizeof(int) * (size_t)npan * 8, st));
-  Timing tm;
   tm.on = timeinfo || g_ktime_on;
-  cudaStream_t st2 = st; /* chunked calls: odd chunks run here */
-  auto rec = [&](int phase, int sidx = 0) {
-    if (!tm.on) return;
-    cudaEvent_t e;
-    if (cudaEventCreate(&e) != cudaSuccess) return;
-    cudaEventRecord(e, sidx ? st2 : st);
-    tm.ev.push_back(e);
-    tm.ph.push_back(phase);
-    tm.sid.push_back(sidx);
-  };
+  st2 = st; /* chunked calls: odd chunks run here */
   rec(0);
   CK(qol_launch_levels(T, J.P, W, npan, st));
   rec(1);
@@ -398,24 +425,24 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
   }
   CK(qol_launch_scan(npan, T.nlevel + 1, G.cnt, rrq_off, st));
   /* RRQ pair offsets per panel (all of them when the per-pair phase is chunked) */
-  std::vector<long long> off_h(J.chunk_pan ? npan + 1 : 1);
+  off_h.assign(J.chunk_pan ? npan + 1 : 1, 0);
   CK(cudaMemcpyAsync(off_h.data(), J.chunk_pan ? rrq_off : rrq_off + npan, sizeof(long long) * off_h.size(),
                      cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
-  const long long nrrq = off_h.back();
+  nrrq = off_h.back();
   R.nrrq = nrrq;
   /* per-pair RRQ moment storage (separate arena: its size is known only now) */
-  rc = g_arena2.reserve(sizeof(double) * (size_t)std::max<long long>(nrrq, 1) * (5 * hd + 6 * nbd + 4 + 3 * (2 * nq + 3) + 2) +
+  rc = A2->reserve(sizeof(double) * (size_t)std::max<long long>(nrrq, 1) * (5 * hd + 6 * nbd + 4 + 3 * (2 * nq + 3) + 2) +
                         8192);
   if (rc) return rc;
-  g_arena2.reset();
-  R.JD = g_arena2.take<double>((size_t)std::max<long long>(nrrq, 1) * 4 * hd);
-  R.RS = g_arena2.take<double>((size_t)std::max<long long>(nrrq, 1) * hd);
-  R.line = g_arena2.take<double>((size_t)std::max<long long>(nrrq, 1) * (6 * nbd + 4));
-  R.edge = g_arena2.take<double>((size_t)std::max<long long>(nrrq, 1) * 3 * (2 * nq + 3));
-  R.pair = g_arena2.take<int2>((size_t)std::max<long long>(nrrq, 1));
-  R.side = g_arena2.take<signed char>((size_t)std::max<long long>(nrrq, 1));
-  OutCOO O{};
+  A2->reset();
+  R.JD = A2->take<double>((size_t)std::max<long long>(nrrq, 1) * 4 * hd);
+  R.RS = A2->take<double>((size_t)std::max<long long>(nrrq, 1) * hd);
+  R.line = A2->take<double>((size_t)std::max<long long>(nrrq, 1) * (6 * nbd + 4));
+  R.edge = A2->take<double>((size_t)std::max<long long>(nrrq, 1) * 3 * (2 * nq + 3));
+  R.pair = A2->take<int2>((size_t)std::max<long long>(nrrq, 1));
+  R.side = A2->take<signed char>((size_t)std::max<long long>(nrrq, 1));
+  O = OutCOO{};
   O.vs = J.vs; O.vd = J.vd; O.omega = J.omega; O.subtract_naive = J.subtract_naive;
   /* the panel kernel's (cluster size, threads) shape, measured once per order
    * on the first call with enough panels: each shape on the first 512 panels,
@@ -454,14 +481,21 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
       C->T.panel_nt = T.panel_nt = nt[best];
     }
   }
+  return 0;
+}
+
+int PipeRun::back(long long* hist_out, std::vector<int>* grp_out, int* cnt_out, bool direct_done) {
+  int rc = 0;
   /* one pass over all panels, or (host entry) panel chunks whose every phase
    * runs before the next chunk's, so that chunk c's values are final early
    * and leave the GPU while later chunks compute */
   const bool chunked = J.chunk_pan != nullptr;
   if (!chunked) {
-    rec(2);
-    CK(qol_launch_direct(T, J.P, J.Q, W, G, O, npan, st));
-    CK(qol_launch_direct_cut(T, J.P, J.Q, W, G, O, npan, st));
+    if (!direct_done) {
+      rec(2);
+      CK(qol_launch_direct(T, J.P, J.Q, W, G, O, npan, st));
+      CK(qol_launch_direct_cut(T, J.P, J.Q, W, G, O, npan, st));
+    }
     rec(3);
     if (nrrq > 0) CK(qol_launch_rrq_panel(T, J.P, G, R, npan, J.chart, st));
   }
@@ -532,6 +566,14 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
   }
   finish_timing(tm, timeinfo);
   return 0;
+}
+
+int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* hist_out, std::vector<int>* grp_out,
+                 int* cnt_out) {
+  PipeRun P(J, st, timeinfo);
+  int rc = P.front();
+  if (rc) return rc;
+  return P.back(hist_out, grp_out, cnt_out, false);
 }
 
 /* ---------------- patch-level handles ---------------- */
@@ -1309,6 +1351,102 @@ int qol_getnearquad_lap_rrq_dev(qol_int npan, qol_int nterms, qol_int hdim, qol_
   rc = run_pipeline(J, st, nullptr, level_hist, nullptr, nullptr);
   if (rc) return rc;
   if (sync) CK(cudaStreamSynchronize(st));
+  return 0;
+}
+
+int qol_getnearquad_lap_rrq_batch_dev(qol_int njob, const qol_near_job* jobs, void* stream, qol_int* level_hist) {
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  if (njob < 0 || (njob > 0 && !jobs)) return fail(QOL_ERR_ARG, "bad arguments");
+  int rc = ensure_device();
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  /* per job: validation (the CSR offsets read back), the pipeline job, two arenas */
+  static std::vector<std::unique_ptr<Arena>> arenas;
+  while (arenas.size() < 2 * (size_t)njob + 1) arenas.emplace_back(new Arena());
+  std::vector<Job> Js((size_t)njob);
+  std::vector<char> live((size_t)njob, 0);
+  for (qol_int k = 0; k < njob; ++k) {
+    const qol_near_job& q = jobs[k];
+    std::vector<long long> xi(q.npan + 1);
+    CK(cudaMemcpyAsync(xi.data(), q.tcxi, sizeof(long long) * (q.npan + 1), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if ((rc = validate_near(q.npan, q.nterms, q.hdim, q.nsrc, q.ntcx, xi.data(), q.nnz))) return rc;
+    if (level_hist) for (int i = 0; i < 6; ++i) level_hist[6 * k + i] = 0;
+    if (q.npan == 0 || q.ntcx == 0) continue;
+    Job& J = Js[k];
+    J.npan = (int)q.npan; J.nterms = (int)q.nterms; J.nquad = (int)q.nquad; J.orderff = (int)q.orderff;
+    J.exterior = (q.iside % 10) == 0; J.subtract_naive = 1; J.distff = q.distff; J.ntcx = q.ntcx;
+    J.P = PanelIn{q.sx, q.snx, q.sw, q.rts, q.rps};
+    J.Q = PairIn{q.tcx, (const long long*)q.tcxrow, (const long long*)q.tcxi};
+    J.vs = q.sparsevs; J.vd = q.sparsevd; J.si = (long long*)q.sparsei; J.sj = (long long*)q.sparsej;
+    live[k] = 1;
+  }
+  /* front of every job, each on its own workspace */
+  std::vector<std::unique_ptr<PipeRun>> runs((size_t)njob);
+  for (qol_int k = 0; k < njob; ++k) {
+    if (!live[k]) continue;
+    runs[k].reset(new PipeRun(Js[k], st, nullptr, arenas[2 * k].get(), arenas[2 * k + 1].get()));
+    if ((rc = runs[k]->front())) return rc;
+  }
+  /* the level sums of all jobs: one persistent launch over the level-binned queue */
+  if (g_sum_precision == 1) {
+    for (qol_int k = 0; k < njob; ++k)
+      if (live[k]) {
+        PipeRun& P = *runs[k];
+        CK(qol_launch_direct(P.T, P.J.P, P.J.Q, P.W, P.G, P.O, P.npan, st));
+      }
+  } else {
+    std::vector<DirectJob> dj;
+    std::vector<int> items;
+    int nbmax = 1;
+    for (qol_int k = 0; k < njob; ++k)
+      if (live[k]) {
+        PipeRun& P = *runs[k];
+        dj.push_back(DirectJob{P.T, P.J.P, P.J.Q, P.W, P.G, P.O});
+        nbmax = std::max(nbmax, P.T.ncw / 32);
+      }
+    for (int l = 3; l >= 0; --l) /* finest level first */
+      for (size_t j = 0, k = 0; k < (size_t)njob; ++k) {
+        if (!live[k]) continue;
+        for (int p = 0; p < runs[k]->npan; ++p) { items.push_back((int)j); items.push_back(p); items.push_back(l); }
+        ++j;
+      }
+    Arena& A = *arenas[2 * njob];
+    const size_t need = sizeof(DirectJob) * dj.size() + sizeof(int) * (items.size() + 1) + 3 * 256;
+    if ((rc = A.reserve(need))) return rc;
+    A.reset();
+    DirectJob* ddj = A.take<DirectJob>(dj.size());
+    int* ditems = A.take<int>(items.size());
+    int* dhead = A.take<int>(1);
+    CK(cudaMemcpyAsync(ddj, dj.data(), sizeof(DirectJob) * dj.size(), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ditems, items.data(), sizeof(int) * items.size(), cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(dhead, 0, sizeof(int), st));
+    CK(qol_launch_direct_queue(ddj, nbmax, ditems, (int)(items.size() / 3), dhead, st));
+    CK(cudaStreamSynchronize(st)); /* the host vectors above are the copies' sources */
+  }
+  for (qol_int k = 0; k < njob; ++k)
+    if (live[k]) {
+      PipeRun& P = *runs[k];
+      CK(qol_launch_direct_cut(P.T, P.J.P, P.J.Q, P.W, P.G, P.O, P.npan, st));
+    }
+  /* the rest of every job (one stream: the per-pair RRQ kernels fill the GPU;
+   * jobs on separate streams measured 3 % slower) */
+  for (qol_int k = 0; k < njob; ++k) {
+    if (!live[k]) continue;
+    if ((rc = runs[k]->back(nullptr, nullptr, nullptr, true))) return rc;
+  }
+  CK(cudaStreamSynchronize(st));
+  if (level_hist)
+    for (qol_int k = 0; k < njob; ++k) {
+      if (!live[k]) continue;
+      const PipeRun& P = *runs[k];
+      std::vector<int> cnt((size_t)P.npan * 8);
+      CK(cudaMemcpy(cnt.data(), P.G.cnt, sizeof(int) * cnt.size(), cudaMemcpyDeviceToHost));
+      for (int p = 0; p < P.npan; ++p) {
+        for (int l = 1; l <= 5; ++l) level_hist[6 * k + l] += cnt[(size_t)p * 8 + l];
+        level_hist[6 * k] += cnt[(size_t)p * 8 + QOL_LV_CUT];
+      }
+    }
   return 0;
 }
 

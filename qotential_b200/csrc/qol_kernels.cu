@@ -347,16 +347,16 @@ __global__ void __launch_bounds__(128) k_level_subs(OrderTab T, LevelWS W, int n
   qp[3] = (T.subtyp[l][s] == 1) ? d2 * fmax(rmax2, 0.5 * swsum) : d2 * fmax(rmax2, swsum);
 }
 
-/* one CTA per (panel, level); chunks of DTT targets.  Tiles of DNT level nodes,
- * double-buffered in shared memory: the node data and interpolation rows of
- * tile t+1 arrive by async copy while the FP64 tensor path accumulates S and D
- * (targets x hd) += K It over tile t; then the kernel values KS, KD of tile t+1
- * are formed from the staged nodes.  Warp w: targets 16 (w>>2) .. +15,
- * columns 8 NB (w&3) .., NB column blocks of 8 */
+/* the level sums of one (panel, level) item, by all threads of the CTA, in
+ * chunks of DTT targets.  Tiles of DNT level nodes, double-buffered in shared
+ * memory: the node data and interpolation rows of tile t+1 arrive by async
+ * copy while the FP64 tensor path accumulates S and D (targets x hd) += K It
+ * over tile t; then the kernel values KS, KD of tile t+1 are formed from the
+ * staged nodes.  Warp w: targets 16 (w>>2) .. +15, columns 8 NB (w&3) .., NB
+ * column blocks of 8.  dsm: direct_smem<NB>() bytes of dynamic shared memory */
 template <int NB>
-__global__ void __launch_bounds__(256, 2) k_direct(OrderTab T, PanelIn P, PairIn Q, LevelWS W, PairWS G,
-                                                   OutCOO O, int pan0) {
-  const int pan = pan0 + blockIdx.x, l = blockIdx.y; /* panels pan0 .. pan0 + gridDim.x - 1 */
+__device__ __forceinline__ void direct_item(const OrderTab& T, const PanelIn& P, const PairIn& Q, const LevelWS& W,
+                                            const PairWS& G, const OutCOO& O, int pan, int l, double* dsm) {
   if (l >= T.nlevel) return;
   const int cntl = G.cnt[(size_t)pan * 8 + l + 1];
   if (cntl == 0) return;
@@ -368,7 +368,6 @@ __global__ void __launch_bounds__(256, 2) k_direct(OrderTab T, PanelIn P, PairIn
   constexpr int NCW = 32 * NB; /* padded columns */
   constexpr int ICS = NCW + 4; /* interpolation-tile row stride */
   constexpr int STG = 2 * DNT * DKS + DNT * ICS + 8 * DNT; /* doubles per stage: KS, KD, It, nodes (7 x DNT, padded) */
-  extern __shared__ __align__(16) double dsm[];
   double* tg = dsm + 2 * STG; /* DTT x 3 */
   int* tloc = (int*)(tg + 3 * DTT);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -560,6 +559,43 @@ __global__ void __launch_bounds__(256) k_direct_cut(OrderTab T, PanelIn P, PairI
       const size_t o = (size_t)p0 * hd + (size_t)c * m + tl;
       O.vs[o] = vs;
       O.vd[o] = vd;
+    }
+  }
+}
+
+/* one CTA per (panel, level) */
+template <int NB>
+__global__ void __launch_bounds__(256, 2) k_direct(OrderTab T, PanelIn P, PairIn Q, LevelWS W, PairWS G,
+                                                   OutCOO O, int pan0) {
+  extern __shared__ __align__(16) double dsm[];
+  direct_item<NB>(T, P, Q, W, G, O, pan0 + blockIdx.x, blockIdx.y, dsm); /* panels pan0 .. pan0 + gridDim.x - 1 */
+}
+
+/* the level sums of many pipeline jobs (surfaces, orders) in one persistent
+ * launch: every CTA takes the next (job, panel, level) item from a device
+ * queue (items[3 i .. 3 i + 2], ordered by the host: finest level first, so
+ * the longest items start first) until the queue is empty, and runs the same
+ * item code as k_direct, so the values are k_direct's bit for bit */
+template <int NBMAX>
+__global__ void __launch_bounds__(256, 2) k_direct_queue(const DirectJob* jobs, const int* items, int nitems,
+                                                         int* head) {
+  extern __shared__ __align__(16) double dsm[];
+  __shared__ int s_it;
+  for (;;) {
+    __syncthreads(); /* the previous item is done with shared memory */
+    if (threadIdx.x == 0) s_it = atomicAdd(head, 1);
+    __syncthreads();
+    const int it = s_it;
+    if (it >= nitems) return;
+    const DirectJob& D = jobs[items[3 * it]];
+    const int pan = items[3 * it + 1], l = items[3 * it + 2];
+    switch (D.T.ncw / 32) {
+      case 1: direct_item<1>(D.T, D.P, D.Q, D.W, D.G, D.O, pan, l, dsm); break;
+      case 2: if (NBMAX >= 2) direct_item<(NBMAX >= 2 ? 2 : 1)>(D.T, D.P, D.Q, D.W, D.G, D.O, pan, l, dsm); break;
+      case 3: if (NBMAX >= 3) direct_item<(NBMAX >= 3 ? 3 : 1)>(D.T, D.P, D.Q, D.W, D.G, D.O, pan, l, dsm); break;
+      case 4: if (NBMAX >= 4) direct_item<(NBMAX >= 4 ? 4 : 1)>(D.T, D.P, D.Q, D.W, D.G, D.O, pan, l, dsm); break;
+      case 5: if (NBMAX >= 5) direct_item<(NBMAX >= 5 ? 5 : 1)>(D.T, D.P, D.Q, D.W, D.G, D.O, pan, l, dsm); break;
+      default: break;
     }
   }
 }
@@ -2258,6 +2294,29 @@ cudaError_t qol_launch_direct(const OrderTab& T, const PanelIn& P, const PairIn&
   }
   return cudaGetLastError();
 }
+cudaError_t qol_launch_direct_queue(const DirectJob* jobs, int nbmax, const int* items, int nitems, int* head,
+                                    cudaStream_t st) {
+  if (nitems <= 0) return cudaSuccess;
+  int dev = 0, nsm = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  const unsigned grid = (unsigned)std::min(2 * nsm, nitems); /* two resident CTAs an SM */
+  auto go = [&](auto kern, size_t smem) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    kern<<<grid, 256, smem, st>>>(jobs, items, nitems, head);
+  };
+  switch (nbmax) {
+    case 1: go(k_direct_queue<1>, direct_smem<1>()); break;
+    case 2: go(k_direct_queue<2>, direct_smem<2>()); break;
+    case 3: go(k_direct_queue<3>, direct_smem<3>()); break;
+    case 4: go(k_direct_queue<4>, direct_smem<4>()); break;
+    case 5: go(k_direct_queue<5>, direct_smem<5>()); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t qol_launch_direct_cut(const OrderTab& T, const PanelIn& P, const PairIn& Q, const LevelWS& W,
                                   const PairWS& G, const OutCOO& O, int npan, cudaStream_t st, int pan0) {
   if (npan <= 0 || !T.adaptive) return cudaSuccess;

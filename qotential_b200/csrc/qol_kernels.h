@@ -114,6 +114,21 @@ cudaError_t qol_launch_sel_update(const float* slot, int nslot, float inv_n, flo
 cudaError_t qol_launch_direct(const OrderTab& T, const PanelIn& P, const PairIn& Q, const LevelWS& W,
                               const PairWS& G, const OutCOO& O, int npan, cudaStream_t st,
                               int pan0 = 0 /* first panel of the launch */);
+/* one pipeline job's level-sum inputs (the batched entry's persistent launch) */
+struct DirectJob {
+  OrderTab T;
+  PanelIn P;
+  PairIn Q;
+  LevelWS W;
+  PairWS G;
+  OutCOO O;
+};
+/* the FP64 level sums of many jobs in one persistent launch over the (job,
+ * panel, level) items (3 ints each, device memory) taken in order from a queue
+ * whose head (*head, device memory) starts at 0; nbmax: the largest
+ * interpolation column-block count (ncw / 32) among the jobs */
+cudaError_t qol_launch_direct_queue(const DirectJob* jobs, int nbmax, const int* items, int nitems, int* head,
+                                    cudaStream_t st);
 /* the level sums of the adaptive cuts (pairs of class QOL_LV_CUT) */
 cudaError_t qol_launch_direct_cut(const OrderTab& T, const PanelIn& P, const PairIn& Q, const LevelWS& W,
                                   const PairWS& G, const OutCOO& O, int npan, cudaStream_t st, int pan0 = 0);

@@ -59,3 +59,40 @@ def test_batch_matches_single_calls(qol):
                                           1.4, 30)
         for x, y in zip(r, one[:4]):
             assert np.asarray(x).tobytes() == np.asarray(y).tobytes()
+
+
+@pytest.mark.gpu
+def test_one_call_batch_matches_single_calls(qol):
+    """surfaces of orders 4, 7 and 12 (one to three interpolation column
+    blocks) in one qol_getnearquad_lap_rrq_batch_dev call, the level sums of
+    all in one persistent launch: every job's COO and level histogram equal its
+    own device call's, byte for byte"""
+    import torch
+    from qotential_b200 import batch as B
+    from qotential_b200 import geometry as G
+    probs = _problems(G, [(5, 4, 8), (8, 4, 9), (13, 3, 8), (5, 5, 10), (13, 3, 6)], seed=6)
+    groups = {}
+    for p in probs:
+        groups.setdefault(B._key(p), []).append(p)
+    combs = [B.combine(ps)[0] for ps in groups.values()]
+    dev = torch.device("cuda", torch.cuda.current_device())
+    Ds = [B.device_inputs(c, dev) for c in combs]
+
+    def outbuf(c):
+        n = int(c["tcxrow"].size) * c["hd"]
+        return (torch.full((n,), -1, dtype=torch.int64, device=dev), torch.full((n,), -1, dtype=torch.int64, device=dev),
+                torch.full((n,), np.nan, dtype=torch.float64, device=dev),
+                torch.full((n,), np.nan, dtype=torch.float64, device=dev))
+
+    batch_out = [outbuf(c) for c in combs]
+    hist = B.run_device_batch(combs, Ds, batch_out)
+    torch.cuda.synchronize()
+    for c, D, bo, h in zip(combs, Ds, batch_out, hist):
+        so = outbuf(c)
+        hs = qol.qol_getnearquad_lap_rrq_dev(c["npan"], c["nterms"], c["nquad"], D["sx"], D["snx"], D["sw"], D["rts"],
+                                             D["rps"], D["tcx"], D["tcxrow"], D["tcxi"], c["orderff"], 1.4, 30, so,
+                                             want_hist=True)
+        torch.cuda.synchronize()
+        assert np.array_equal(np.asarray(h), np.asarray(hs))
+        for x, y in zip(bo, so):
+            assert x.cpu().numpy().tobytes() == y.cpu().numpy().tobytes()
