@@ -158,6 +158,36 @@ def grf_sweep(orders=(4, 6, 8, 10, 12)):
     return out
 
 
+def grf_multi_rhs(nrhs=4, reps=2):
+    """BASELINE config 3's right-hand sides on the order-12 stellarator (16x80):
+    the GRF near phase for nrhs point-charge densities, nrhs qol_grf_near calls
+    against one qol_grf_near_multi call (corrections computed once); wall time,
+    best of reps, and the largest difference between the two (zero: the same
+    corrections applied in the same order)"""
+    import qotential_b200 as qol
+    from qotential_b200 import geometry as G
+    nterms = ORDER + 1
+    hd = nterms * (nterms + 1) // 2
+    surf = G.stellarator()
+    P = G.panels(surf, MP, NP, nterms, split=False)
+    npan = P["sw"].size // hd
+    cols = [G.harmonic_density(P["sx"], P["snx"], *G.point_charges(surf, 8, seed=SEED + r)) for r in range(nrhs)]
+    ub, ubn = np.stack([c[0] for c in cols], 1), np.stack([c[1] for c in cols], 1)
+    args = (npan, nterms, nterms + 2, P["sx"], P["snx"], P["sw"], P["rts"], P["rps"])
+    t_single, t_multi = [], []
+    for _ in range(reps + 1):
+        t0 = time.perf_counter()
+        single = [qol.qol_grf_near(*args, ub[:, r], ubn[:, r])[0] for r in range(nrhs)]
+        t_single.append(time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        multi, nn, _ = qol.qol_grf_near_multi(*args, ub, ubn)
+        t_multi.append(time.perf_counter() - t0)
+    diff = max(float(np.abs(multi[:, r] - single[r]).max()) for r in range(nrhs))
+    ts, tm = min(t_single[1:]), min(t_multi[1:])
+    return {"nrhs": nrhs, "near_pairs": int(nn), "single_calls_s": round(ts, 4), "multi_s": round(tm, 4),
+            "speedup": ts / tm, "max_difference": diff}
+
+
 def row_errors(rows, a, b):
     """per correction-matrix row (one target): max |a - b| / max |a| over the
     row's entries; max, p99 and median over rows"""
@@ -846,6 +876,8 @@ def main():
         if chosen is not None:
             chosen["grf_error"] = {str(r["order"]): {"plain": r["grf_error_plain"], "chosen": r["grf_error_chosen"]}
                                    for r in grf}
+    if batched is not None and not args.no_grf:
+        batched["grf_rhs"] = grf_multi_rhs()
     c4 = None
     if rank == 0 and world == 1 and not args.no_config4:
         del out, D

@@ -194,6 +194,14 @@ int qol_grf_near_range(qol_int npan, qol_int nterms, qol_int nquad, qol_int orde
                        qol_int nsrc, const double* sx, const double* snx, const double* sw, const double* rts,
                        const double* rps, const double* xbuf, const double* ub, const double* ubn, qol_int plo,
                        qol_int phi, double* u, qol_int* nnear, qol_int* level_hist, double* timeinfo);
+/* qol_grf_near for nrhs densities at once (no counterpart in the reference,
+ * whose driver takes one density a run): ub, ubn and u are nsrc x nrhs,
+ * column-major; the near search and the corrections are computed once and
+ * applied to every density (u(:, r) += the near phase of density r). */
+int qol_grf_near_multi(qol_int npan, qol_int nterms, qol_int nquad, qol_int orderff, double distff, qol_int iside,
+                       qol_int nsrc, const double* sx, const double* snx, const double* sw, const double* rts,
+                       const double* rps, const double* xbuf, qol_int nrhs, const double* ub, const double* ubn,
+                       double* u, qol_int* nnear, qol_int* level_hist, double* timeinfo);
 int qol_direct_farfield_range(qol_int nsrc, const double* sx, const double* snx, const double* sw,
                               const double* ub, const double* ubn, qol_int tlo, qol_int thi, double* u);
 

@@ -15,7 +15,7 @@ import numpy as np
 __all__ = [
     "lib", "QolError", "qol_simplex_precomp", "qol_build_patch_levels", "qol_lap3dsdlpmat_levels",
     "qol_clear_patch_levels", "qol_clear_patch_levels_all", "qol_rrq", "qol_getnearquad_lap_rrq",
-    "qol_getnearquad_lap_rrq_dev", "qol_getnearquad_lap_rrq_batch_dev", "qol_grf_near", "qol_grf_near_range", "qol_direct_farfield",
+    "qol_getnearquad_lap_rrq_dev", "qol_getnearquad_lap_rrq_batch_dev", "qol_grf_near", "qol_grf_near_multi", "qol_grf_near_range", "qol_direct_farfield",
     "qol_direct_farfield_range", "qol_surface_panels", "qol_surface_charts", "qol_surface_panels_charts",
     "qol_interp_matrix", "qol_set_sum_precision",
     "SELECTOR_NW", "qol_selector_features", "qol_selector_grad", "qol_selector_train", "qol_selector_set",
@@ -54,7 +54,10 @@ def _check(rc):
 
 
 def _vp(a):
-    return None if a is None else C.c_void_p(a.ctypes.data)
+    """a pointer to a's data that keeps a alive for the call (a temporary copy,
+    e.g. of a strided column, would otherwise be freed before the call and its
+    memory reused by the next argument's copy)"""
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
 
 
 def _f(a, n=None):
@@ -262,6 +265,33 @@ def qol_grf_near(npan, nterms, nquad, sx, snx, sw, rts, rps, ub, ubn, u=None, or
                             i64(nsrc), _vp(_f(sx, 3 * nsrc)), _vp(_f(snx, 3 * nsrc)), _vp(_f(sw, nsrc)),
                             _vp(_f(rts, 3 * nsrc)), _vp(_f(rps, 3 * nsrc)), _vp(xb), _vp(_f(ub, nsrc)),
                             _vp(_f(ubn, nsrc)), _vp(uu), _vp(nn), _vp(hist), _vp(ti))
+    _check(rc)
+    return uu, int(nn[0]), hist
+
+
+def qol_grf_near_multi(npan, nterms, nquad, sx, snx, sw, rts, rps, ub, ubn, u=None, orderff=None, distff=1.4,
+                       iside=30, xbuf=None, timeinfo=None):
+    """qol_grf_near for several densities: ub, ubn (and u) of shape (nsrc,
+    nrhs); the corrections are computed once and applied to each.  Returns
+    (u (nsrc, nrhs), near pairs, level histogram)."""
+    hd = nterms * (nterms + 1) // 2
+    nsrc = npan * hd
+    orderff = nquad if orderff is None else orderff
+    ubm = np.asfortranarray(np.asarray(ub, np.float64).reshape(nsrc, -1))
+    ubnm = np.asfortranarray(np.asarray(ubn, np.float64).reshape(nsrc, -1))
+    nrhs = ubm.shape[1]
+    if ubnm.shape != ubm.shape:
+        raise QolError(8, "ub and ubn must have the same shape")
+    uu = np.zeros((nsrc, nrhs), order="F") if u is None else np.array(np.asarray(u, np.float64).reshape(nsrc, nrhs),
+                                                                      order="F")
+    nn = np.zeros(1, np.int64)
+    hist = np.zeros(6, np.int64)
+    ti = np.zeros(20) if timeinfo is None else _f(timeinfo, 20).copy()
+    xb = None if xbuf is None else np.ascontiguousarray(np.asarray(xbuf, np.float64).ravel())
+    rc = lib().qol_grf_near_multi(i64(npan), i64(nterms), i64(nquad), i64(orderff), C.c_double(distff), i64(iside),
+                                  i64(nsrc), _vp(_f(sx, 3 * nsrc)), _vp(_f(snx, 3 * nsrc)), _vp(_f(sw, nsrc)),
+                                  _vp(_f(rts, 3 * nsrc)), _vp(_f(rps, 3 * nsrc)), _vp(xb), i64(nrhs), _vp(ubm),
+                                  _vp(ubnm), _vp(uu), _vp(nn), _vp(hist), _vp(ti))
     _check(rc)
     return uu, int(nn[0]), hist
 

@@ -1651,15 +1651,18 @@ int qol_last_host_times(double* ms7) {
 /* GRF near phase (stellarator_grf_core_mod.f90:652-899): ball lists of the
  * surface's own nodes, the RRQ corrections of every near pair, contracted with
  * the density (ubn, ub) and scattered into u in panel order. */
-int qol_grf_near_range(qol_int npan, qol_int nterms, qol_int nquad, qol_int orderff, double distff, qol_int iside,
-                       qol_int nsrc, const double* sx, const double* snx, const double* sw, const double* rts,
-                       const double* rps, const double* xbuf, const double* ub, const double* ubn, qol_int plo,
-                       qol_int phi, double* u, qol_int* nnear, qol_int* level_hist, double* timeinfo) {
-  std::lock_guard<std::recursive_mutex> g(g_mu);
+/* the GRF near phase of panels [plo, phi) for nrhs densities (ub, ubn, u:
+ * nsrc x nrhs, column-major): the near search and the corrections once, their
+ * application once a density */
+static int grf_near_impl(qol_int npan, qol_int nterms, qol_int nquad, qol_int orderff, double distff, qol_int iside,
+                         qol_int nsrc, const double* sx, const double* snx, const double* sw, const double* rts,
+                         const double* rps, const double* xbuf, qol_int nrhs, const double* ub, const double* ubn,
+                         qol_int plo, qol_int phi, double* u, qol_int* nnear, qol_int* level_hist, double* timeinfo) {
   const qol_int hd = nterms * (nterms + 1) / 2;
   if (!sx || !snx || !sw || !rts || !rps || !ub || !ubn || !u) return fail(QOL_ERR_ARG, "null argument");
   if (npan < 0 || nsrc != npan * hd) return fail(QOL_ERR_LAYOUT, "the panel order, npan and nsrc are inconsistent");
   if (plo < 0 || phi < plo || phi > npan) return fail(QOL_ERR_ARG, "panel range outside [0, npan]");
+  if (nrhs < 1) return fail(QOL_ERR_ARG, "nrhs must be positive");
   int rc = ensure_device();
   if (rc) return rc;
   if (nnear) *nnear = 0;
@@ -1668,7 +1671,7 @@ int qol_grf_near_range(qol_int npan, qol_int nterms, qol_int nquad, qol_int orde
   if (nloc == 0) return 0;
   cudaStream_t st = g_stream;
   const int nbd = 3 * (int)nquad;
-  size_t need = sizeof(double) * (size_t)(16 * nsrc + 4 * npan + 6 * ((nsrc + 255) / 256) +
+  size_t need = sizeof(double) * (size_t)(16 * nsrc + 3 * (nrhs - 1) * nsrc + 4 * npan + 6 * ((nsrc + 255) / 256) +
                                           (xbuf ? 3 * (nbd + 3) * npan : 0)) +
                 sizeof(long long) * (size_t)(3 * nloc + 3) + 16 * 256;
   if ((rc = g_arena_io.reserve(need))) return rc;
@@ -1678,9 +1681,9 @@ int qol_grf_near_range(qol_int npan, qol_int nterms, qol_int nquad, qol_int orde
   double* dsw = g_arena_io.take<double>(nsrc);
   double* drts = g_arena_io.take<double>(3 * nsrc);
   double* drps = g_arena_io.take<double>(3 * nsrc);
-  double* dub = g_arena_io.take<double>(nsrc);
-  double* dubn = g_arena_io.take<double>(nsrc);
-  double* du = g_arena_io.take<double>(nsrc);
+  double* dub = g_arena_io.take<double>(nsrc * nrhs);
+  double* dubn = g_arena_io.take<double>(nsrc * nrhs);
+  double* du = g_arena_io.take<double>(nsrc * nrhs);
   double* dball = g_arena_io.take<double>(4 * npan);
   double* dbox = g_arena_io.take<double>(6 * (size_t)((nsrc + 255) / 256)); /* node-chunk boxes of the near search */
   double* dchart = xbuf ? g_arena_io.take<double>((size_t)3 * (nbd + 3) * nloc) : nullptr;
@@ -1692,9 +1695,9 @@ int qol_grf_near_range(qol_int npan, qol_int nterms, qol_int nquad, qol_int orde
   CK(cudaMemcpyAsync(dsw, sw, sizeof(double) * nsrc, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(drts, rts, sizeof(double) * 3 * nsrc, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(drps, rps, sizeof(double) * 3 * nsrc, cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(dub, ub, sizeof(double) * nsrc, cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(dubn, ubn, sizeof(double) * nsrc, cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(du, u, sizeof(double) * nsrc, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dub, ub, sizeof(double) * nsrc * nrhs, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dubn, ubn, sizeof(double) * nsrc * nrhs, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(du, u, sizeof(double) * nsrc * nrhs, cudaMemcpyHostToDevice, st));
   if (xbuf)
     CK(cudaMemcpyAsync(dchart, xbuf + (size_t)3 * (nbd + 3) * plo, sizeof(double) * 3 * (nbd + 3) * nloc,
                        cudaMemcpyHostToDevice, st));
@@ -1733,12 +1736,33 @@ int qol_grf_near_range(qol_int npan, qol_int nterms, qol_int nquad, qol_int orde
     long long hist[6] = {0, 0, 0, 0, 0, 0};
     if ((rc = run_pipeline(J, st, timeinfo, hist, nullptr, nullptr))) return rc;
     if (level_hist) for (int i = 0; i < 6; ++i) level_hist[i] = hist[i];
-    CK(qol_launch_grf_apply((int)nloc, (int)hd, nsrc, dsx, ball, doff, didx, dvs, dvd, dub + o, dubn + o, dval, du,
-                            st));
+    for (qol_int r = 0; r < nrhs; ++r) {
+      const size_t ro = (size_t)r * nsrc;
+      CK(qol_launch_grf_apply((int)nloc, (int)hd, nsrc, dsx, ball, doff, didx, dvs, dvd, dub + ro + o, dubn + ro + o,
+                              dval, du + ro, st));
+    }
   }
-  CK(cudaMemcpyAsync(u, du, sizeof(double) * nsrc, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(u, du, sizeof(double) * nsrc * nrhs, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   return 0;
+}
+
+int qol_grf_near_range(qol_int npan, qol_int nterms, qol_int nquad, qol_int orderff, double distff, qol_int iside,
+                       qol_int nsrc, const double* sx, const double* snx, const double* sw, const double* rts,
+                       const double* rps, const double* xbuf, const double* ub, const double* ubn, qol_int plo,
+                       qol_int phi, double* u, qol_int* nnear, qol_int* level_hist, double* timeinfo) {
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  return grf_near_impl(npan, nterms, nquad, orderff, distff, iside, nsrc, sx, snx, sw, rts, rps, xbuf, 1, ub, ubn, plo,
+                       phi, u, nnear, level_hist, timeinfo);
+}
+
+int qol_grf_near_multi(qol_int npan, qol_int nterms, qol_int nquad, qol_int orderff, double distff, qol_int iside,
+                       qol_int nsrc, const double* sx, const double* snx, const double* sw, const double* rts,
+                       const double* rps, const double* xbuf, qol_int nrhs, const double* ub, const double* ubn,
+                       double* u, qol_int* nnear, qol_int* level_hist, double* timeinfo) {
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  return grf_near_impl(npan, nterms, nquad, orderff, distff, iside, nsrc, sx, snx, sw, rts, rps, xbuf, nrhs, ub, ubn, 0,
+                       npan, u, nnear, level_hist, timeinfo);
 }
 
 /* the blocked Direct far field u_i = sum_j S_ij ubn_j - D_ij ub_j with zero

@@ -147,3 +147,29 @@ def test_autotune_switch_host_only(qol):
     qol.qol_set_autotune(0)
     qol.qol_set_autotune(1)
     assert qol.qol_panel_shape(15, 17, 17) == (0, 0)
+
+
+def test_wrappers_keep_argument_copies_alive(qol, monkeypatch):
+    """strided (non-contiguous) array arguments are copied by the wrappers; the
+    pointers handed to the C ABI must stay valid through the call (a stand-in
+    library records what each pointer holds during the call)"""
+    import ctypes as C
+    nterms, npan = 6, 4
+    nsrc = npan * 21
+    seen = {}
+
+    class Rec:
+        def __getattr__(self, name):
+            def f(*a):
+                get = lambda p: np.ctypeslib.as_array((C.c_double * nsrc).from_address(p.value)).copy()
+                seen["ub"], seen["ubn"], seen["u"] = get(a[13]), get(a[14]), get(a[15])
+                return 0
+            return f
+
+    monkeypatch.setattr(qol, "_lib", Rec())
+    rng = np.random.default_rng(3)
+    ub, ubn, u = rng.random((nsrc, 3)), rng.random((nsrc, 3)), rng.random((nsrc, 3))
+    z = np.zeros((nsrc, 3))
+    qol.qol_grf_near(npan, nterms, 8, z, z, np.zeros(nsrc), z, z, ub[:, 1], ubn[:, 1], u=u[:, 1])
+    assert np.array_equal(seen["ub"], ub[:, 1]) and np.array_equal(seen["ubn"], ubn[:, 1])
+    assert np.array_equal(seen["u"], u[:, 1])

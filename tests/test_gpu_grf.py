@@ -102,3 +102,29 @@ def test_ranges_add_up_to_the_whole(qol):
                                  tcxrow, tcxi, nq) for r in range(2)]
     for k in range(4):
         assert np.concatenate([p[k] for p in parts]).tobytes() == one[k].tobytes()
+
+
+def test_multi_density_matches_single_calls(qol):
+    """qol_grf_near_multi with 4 point-charge densities (BASELINE config 3's 4
+    right-hand sides): each column equals its own qol_grf_near call byte for
+    byte (the same corrections, applied once a density)"""
+    from qotential_b200 import geometry as G
+    nterms = 6
+    surf = G.stellarator()
+    P = G.panels(surf, 4, 12, nterms, split=False)
+    hd = nterms * (nterms + 1) // 2
+    npan = P["sw"].size // hd
+    ubs, ubns = [], []
+    for seed in range(4):
+        ys, q = G.point_charges(surf, 8, seed=seed)
+        ub, ubn = G.harmonic_density(P["sx"], P["snx"], ys, q)
+        ubs.append(ub); ubns.append(ubn)
+    ub, ubn = np.stack(ubs, 1), np.stack(ubns, 1)
+    u0 = np.random.default_rng(1).random(ub.shape)
+    um, nn, hist = qol.qol_grf_near_multi(npan, nterms, nterms + 2, P["sx"], P["snx"], P["sw"], P["rts"], P["rps"], ub,
+                                          ubn, u=u0)
+    for r in range(4):
+        us, ns, hs = qol.qol_grf_near(npan, nterms, nterms + 2, P["sx"], P["snx"], P["sw"], P["rts"], P["rps"],
+                                      ub[:, r], ubn[:, r], u=u0[:, r])
+        assert ns == nn and np.array_equal(hs, hist)
+        assert np.ascontiguousarray(um[:, r]).tobytes() == us.tobytes()
