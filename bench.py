@@ -800,7 +800,7 @@ def main():
         if rank == 0:
             print(json.dumps({"metric": "near-pair evals/s", "value": value, "ms_per_step": ms,
                               "steps": args.steps, "note": "kernels-only run", "kernel_ms": roofline["kernel_ms"],
-                              "kernel_tflops": roofline["kernel_tflops"]}))
+                              "kernel_tflops": roofline["kernel_tflops"], "level_hist": roofline["level_hist"]}))
         if dist:
             dist.destroy_process_group()
         return 0
