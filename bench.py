@@ -475,6 +475,7 @@ def batched_config(reps=2):
     persistent launch); CUDA events around the whole set, best of `reps`.  The config's 4 right-hand sides belong to the GRF
     apply, which this near-correction step does not include."""
     import torch
+    import qotential_b200 as qol
     from qotential_b200 import batch as B
     from qotential_b200 import geometry as G
     rng = np.random.default_rng(SEED)
@@ -544,6 +545,7 @@ def batched_config(reps=2):
     ms_c = timed([lambda: B.run_device_batch(cs, Ds, outs, stream=st.cuda_stream)])
     del combs, outs, cs, Ds
     torch.cuda.empty_cache()
+    qol.qol_release_workspace()
     orders = {}
     for p in probs:
         orders[str(p["nterms"] - 1)] = orders.get(str(p["nterms"] - 1), 0) + 1
@@ -882,6 +884,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_config4:
         del out, D
         torch.cuda.empty_cache()
+        qol.qol_release_workspace()  # the earlier legs' workspace (the batch keeps one a job)
         c4 = config4(wsel, args.steps, 1)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

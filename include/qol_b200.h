@@ -123,6 +123,10 @@ int qol_getnearquad_lap_rrq_dev(qol_int npan, qol_int nterms, qol_int hdim, qol_
  * byte.  With the FP32 level sums (qol_set_sum_precision(1)) the level sums
  * run per job instead.  level_hist: 6 entries a job (nullable).  Returns
  * after the work on `stream` is done. */
+/* Frees the device workspace the library keeps between calls (it grows to
+ * the largest call's needs and is reused; the batched entry keeps one per
+ * job); the next call allocates again.  No counterpart in the reference. */
+int qol_release_workspace(void);
 typedef struct {
   qol_int npan, nterms, hdim, nquad, nsrc;
   const double *sx, *snx, *sw, *rts, *rps;

@@ -15,7 +15,7 @@ import numpy as np
 __all__ = [
     "lib", "QolError", "qol_simplex_precomp", "qol_build_patch_levels", "qol_lap3dsdlpmat_levels",
     "qol_clear_patch_levels", "qol_clear_patch_levels_all", "qol_rrq", "qol_getnearquad_lap_rrq",
-    "qol_getnearquad_lap_rrq_dev", "qol_getnearquad_lap_rrq_batch_dev", "qol_grf_near", "qol_grf_near_multi", "qol_grf_near_range", "qol_direct_farfield",
+    "qol_getnearquad_lap_rrq_dev", "qol_getnearquad_lap_rrq_batch_dev", "qol_release_workspace", "qol_grf_near", "qol_grf_near_multi", "qol_grf_near_range", "qol_direct_farfield",
     "qol_direct_farfield_range", "qol_surface_panels", "qol_surface_charts", "qol_surface_panels_charts",
     "qol_interp_matrix", "qol_set_sum_precision",
     "SELECTOR_NW", "qol_selector_features", "qol_selector_grad", "qol_selector_train", "qol_selector_set",
@@ -244,6 +244,11 @@ def qol_getnearquad_lap_rrq_batch_dev(jobs, stream=0):
     hist = np.zeros((max(1, len(jobs)), 6), np.int64)
     _check(lib().qol_getnearquad_lap_rrq_batch_dev(i64(len(jobs)), arr, C.c_void_p(stream), _vp(hist)))
     return hist[:len(jobs)]
+
+
+def qol_release_workspace():
+    """free the device workspace the library keeps between calls"""
+    _check(lib().qol_release_workspace())
 
 
 def qol_grf_near(npan, nterms, nquad, sx, snx, sw, rts, rps, ub, ubn, u=None, orderff=None, distff=1.4,

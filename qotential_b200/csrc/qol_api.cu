@@ -66,6 +66,11 @@ struct Arena {
     return 0;
   }
   void reset() { used = 0; }
+  void release() {
+    if (base) cudaFree(base);
+    base = nullptr;
+    cap = used = 0;
+  }
   template <class T>
   T* take(size_t n) {
     size_t off = (used + 255) & ~(size_t)255;
@@ -92,6 +97,7 @@ struct OrderCache {
 std::map<long long, std::unique_ptr<OrderCache>> g_orders;
 bool g_coefs_uploaded = false;
 Arena g_arena, g_arena2, g_arena_io, g_arena_grf; /* pipeline, per-pair RRQ storage, host-entry buffers, GRF */
+std::vector<std::unique_ptr<Arena>> g_batch_arenas; /* the batched entry: two a job, one for its queue */
 /* per-phase device milliseconds of the pipeline (diagnostics) */
 int g_ktime_on = 0;
 int g_sum_precision = 0; /* 0 FP64 (the drop-in), 1 FP32 level sums */
@@ -1354,6 +1360,14 @@ int qol_getnearquad_lap_rrq_dev(qol_int npan, qol_int nterms, qol_int hdim, qol_
   return 0;
 }
 
+int qol_release_workspace(void) {
+  std::lock_guard<std::recursive_mutex> g(g_mu);
+  if (cudaDeviceSynchronize() != cudaSuccess) return fail(QOL_ERR_CUDA, "qol_release_workspace: device sync");
+  for (Arena* a : {&g_arena, &g_arena2, &g_arena_io, &g_arena_grf}) a->release();
+  g_batch_arenas.clear();
+  return 0;
+}
+
 int qol_getnearquad_lap_rrq_batch_dev(qol_int njob, const qol_near_job* jobs, void* stream, qol_int* level_hist) {
   std::lock_guard<std::recursive_mutex> g(g_mu);
   if (njob < 0 || (njob > 0 && !jobs)) return fail(QOL_ERR_ARG, "bad arguments");
@@ -1361,7 +1375,7 @@ int qol_getnearquad_lap_rrq_batch_dev(qol_int njob, const qol_near_job* jobs, vo
   if (rc) return rc;
   cudaStream_t st = (cudaStream_t)stream;
   /* per job: validation (the CSR offsets read back), the pipeline job, two arenas */
-  static std::vector<std::unique_ptr<Arena>> arenas;
+  std::vector<std::unique_ptr<Arena>>& arenas = g_batch_arenas;
   while (arenas.size() < 2 * (size_t)njob + 1) arenas.emplace_back(new Arena());
   std::vector<Job> Js((size_t)njob);
   std::vector<char> live((size_t)njob, 0);
