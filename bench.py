@@ -99,6 +99,12 @@ def kernel_flops(W, hist):
     }
 
 
+# k_direct's DRAM bytes per level-resolved pair: one ncu capture of the kernel on the leading
+# 256 panels of this workload (profiles/k_direct_dram_order12_256panels.md: 718,468,352 read +
+# 610,090,752 written for 190,817 level-resolved pairs), scaled to a full launch by its pairs
+DIRECT_DRAM_BYTES_PER_PAIR = (718468352 + 610090752) / 190817
+
+
 def roofline_line(W, hist, k_ms, peak):
     fl = kernel_flops(W, hist)
     dom = max(k_ms, key=k_ms.get)
@@ -108,8 +114,12 @@ def roofline_line(W, hist, k_ms, peak):
              "rrq_moments": "k_rrq_moments: per RRQ pair 8 ne nbd + 24 ne nbd + 48 x (translation terms), "
                             "ne = L(L+1)/2",
              "rrq_apply": "k_rrq_apply: per RRQ pair 12 hdim^2"}
+    traffic = DIRECT_DRAM_BYTES_PER_PAIR * int(sum(hist[1:5])) if rl_kernel == "direct" and W["nterms"] == 13 else None
     return {"bound": "fp64", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
-            "frac": ach / peak if peak else None, "traffic": None, "kernel": rl_kernel,
+            "frac": ach / peak if peak else None, "traffic": traffic,
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of k_direct on the leading 256 "
+                              "panels, scaled by level-resolved pairs (profiles/k_direct_dram_order12_256panels.md)",
+            "kernel": rl_kernel,
             "dominant_kernel": dom,
             "peak_source": "measured: in-library FP64 FMA probe (MEASURED_PEAKS.json has no FP64 figure)",
             "flops": notes[rl_kernel], "kernel_ms": k_ms,
