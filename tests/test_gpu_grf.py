@@ -128,3 +128,29 @@ def test_multi_density_matches_single_calls(qol):
                                       ub[:, r], ubn[:, r], u=u0[:, r])
         assert ns == nn and np.array_equal(hs, hist)
         assert np.ascontiguousarray(um[:, r]).tobytes() == us.tobytes()
+
+
+def test_grf_error_converges_with_order(qol):
+    """the GRF identity on the stellarator (16 x 80 quads) with charges the
+    panels resolve (8 on |y| = 12), nquad = nterms + 6 (the edge quadrature
+    that resolves the moment integrands at high order): the error falls at
+    every order through nterms 11, and at nterms 13 stays within the rounding
+    floor that the systems' conditioning sets (kappa u ~ 6e-6 of a panel's near
+    correction; measured 1.2e-6 against 4.0e-7 at nterms 11)"""
+    from qotential_b200 import geometry as G
+    surf = G.stellarator()
+    ys, q = G.point_charges(surf, 8, seed=5, radius=12.0)
+    errs = {}
+    for nterms in (5, 7, 9, 11, 13):
+        P = G.panels(surf, 16, 80, nterms, split=False)
+        hd = nterms * (nterms + 1) // 2
+        npan = P["sw"].size // hd
+        ub, ubn = G.harmonic_density(P["sx"], P["snx"], ys, q)
+        u = qol.qol_direct_farfield(P["sx"], P["snx"], P["sw"], ub, ubn)
+        un, _, _ = qol.qol_grf_near(npan, nterms, nterms + 6, P["sx"], P["snx"], P["sw"], P["rts"], P["rps"], ub, ubn,
+                                    u=u)
+        errs[nterms] = float(np.abs(un).max() / np.abs(ubn).max())
+    print("GRF error by nterms:", errs)
+    for a, b in ((5, 7), (7, 9), (9, 11)):
+        assert errs[b] < errs[a], errs
+    assert errs[11] < 1e-6 and errs[13] < 5e-6, errs
