@@ -1858,22 +1858,32 @@ __global__ void __launch_bounds__(MOM_T) k_rrq_moments(OrderTab T, PairIn Q, Pai
   for (int r = 0; r < RPT; ++r) erow[r] = min(tid + MOM_T * r, NE - 1) * MOM_CS;
   const int np = (L + 1) / 2, pa = tid >> 4, jn = tid & 15, qa = L - 1 - pa;
   for (int c0 = 0; c0 < nbd; c0 += MOM_NC) {
+    if (tid < MOM_NC) { /* the diagonal R_m^m, m < L, of node c0 + tid, once, into its rows */
+      const int i = min(c0 + tid, nbd - 1);
+      const double X = bx[3 * i + 1] - xt1, Y = bx[3 * i + 2] - xt2;
+      double dr = 1.0, di = 0.0;
+      ch[0 * MOM_CS + tid] = 1.0;
+      ch[1 * MOM_CS + tid] = 0.0;
+      for (int mm = 1; mm < L; ++mm) {
+        const double t = dr * X - di * Y;
+        di = (dr * Y + di * X) * s_rd[mm];
+        dr = t * s_rd[mm];
+        const int row = mm * (mm + 1) + 2 * mm;
+        ch[row * MOM_CS + tid] = dr;
+        ch[(row + 1) * MOM_CS + tid] = di;
+      }
+    }
+    __syncthreads();
     if (pa < np) {
       const int i = min(c0 + jn, nbd - 1);
       const double Z = bx[3 * i] - xt0, X = bx[3 * i + 1] - xt1, Y = bx[3 * i + 2] - xt2;
       const double r2 = X * X + Y * Y + Z * Z;
-      /* diagonal R_m^m up to column qa, keeping column pa */
-      double dr = 1.0, di = 0.0, a1r = 1.0, a1i = 0.0;
-      for (int mm = 1; mm <= qa; ++mm) {
-        const double t = dr * X - di * Y;
-        di = (dr * Y + di * X) * s_rd[mm];
-        dr = t * s_rd[mm];
-        if (mm == pa) { a1r = dr; a1i = di; }
-      }
-      /* columns pa (L-pa entries) and qa (L-qa entries, none when qa == pa) */
+      /* columns pa (L-pa entries) and qa (L-qa entries, none when qa == pa), from
+       * their diagonal entries */
       const int n1 = L - pa, n2 = qa > pa ? L - qa : 0;
-      double ur = a1r, ui = a1i, vr = 0.0, vi = 0.0;
-      double sr = dr, si = di, tr = 0.0, ti = 0.0;
+      const int dpa = pa * (pa + 1) + 2 * pa, dqa = qa * (qa + 1) + 2 * qa;
+      double ur = ch[dpa * MOM_CS + jn], ui = ch[(dpa + 1) * MOM_CS + jn], vr = 0.0, vi = 0.0;
+      double sr = n2 ? ch[dqa * MOM_CS + jn] : 0.0, si = n2 ? ch[(dqa + 1) * MOM_CS + jn] : 0.0, tr = 0.0, ti = 0.0;
       for (int e = 0; e < n1; ++e) {
         if (e > 0) {
           const int l = pa + e;
