@@ -176,18 +176,17 @@ int order_tables(int nterms, int orderff, int nquad, OrderCache** out, int refin
     };
     const int ncw = 32 * ((hd + 31) / 32);
     std::vector<double> rp((size_t)L.n * ncw, 0.0);
-    /* the TF32 parts in m16n8k8 B-fragment order: tiles of 32 rows (zero
-     * padded), per 8-row k-slice and 8-column block the 32 lanes' (b0, b1) =
-     * (B[t][g], B[t+4][g]), lane = 4 g + t */
+    /* the TF32 parts as the tcgen05.mma B operand (K-major, no swizzle):
+     * tiles of 32 rows (zero padded), each [row quad][column][4 rows of the
+     * quad], so a column's 8-column groups are 128-byte core matrices */
     const long long npad = (L.n + 31) / 32 * 32;
-    const int nbt = ncw / 8;
     std::vector<uint32_t> rh((size_t)npad * ncw, 0u), rl(rh.size(), 0u);
     for (long long i = 0; i < L.n; ++i)
       for (int k = 0; k < hd; ++k) {
         const size_t e = (size_t)i * ncw + k;
         rp[e] = L.interp[i + (size_t)L.n * k];
         const float f = (float)rp[e];
-        const size_t fe = ((((size_t)(i / 8) * nbt + k / 8) * 32 + (k % 8) * 4 + (i % 4)) * 2) + (i % 8) / 4;
+        const size_t fe = (size_t)(i / 32) * 32 * ncw + ((size_t)((i % 32) / 4) * ncw + k) * 4 + (i % 4);
         rh[fe] = tf32(f);
         float h;
         std::memcpy(&h, &rh[fe], 4);
@@ -551,6 +550,11 @@ int PipeRun::back(long long* hist_out, std::vector<int>* grp_out, int* cnt_out, 
   rec(8);
   if (J.si) CK(qol_launch_coo_index(T, J.Q, J.si, J.sj, npan, st));
   rec(-1);
+  if (T.sum_fp32) { /* the FP32 level-sum kernel's waits are bounded: a timeout is reported here */
+    unsigned werr = 0;
+    CK(qol_wait_error(&werr, st));
+    if (werr) return fail(QOL_ERR_CUDA, "FP32 level sums: a wait on the tensor cores timed out");
+  }
   if (hist_out || grp_out || cnt_out || tm.on) {
     CK(cudaStreamSynchronize(st));
   }

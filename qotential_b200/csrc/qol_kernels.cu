@@ -606,221 +606,346 @@ constexpr size_t direct_smem() {
 }
 
 /* ---------------------------------------------------------------------
- * FP32 form of the level sums (the precision variant): kernel values in
- * FP32 from FP64 coordinate differences, the contraction with the
- * interpolation rows on the TF32 tensor path with the 3xTF32 split
- * (a b ~ a_hi b_hi + a_hi b_lo + a_lo b_hi, each a_hi = TF32 rounding of a,
- * a_lo = TF32 rounding of the rest) accumulated in FP32 over a tile of DNT
- * nodes and in FP64 across tiles; the naive block in FP64.
+ * FP32 form of the level sums (the precision variant) on the fifth-
+ * generation tensor cores: kernel values in FP32 from coordinates taken
+ * relative to the panel's first node (so that the FP32 differences keep
+ * their relative accuracy), the contraction with the interpolation rows by
+ * tcgen05.mma kind::tf32 with the 3xTF32 split (a b ~ a_lo b_hi + a_hi b_lo
+ * + a_hi b_hi, a_hi = TF32 rounding of a, a_lo = TF32 rounding of the rest),
+ * accumulated in FP32 in tensor memory over UG tiles of UNT nodes and in
+ * FP64 registers across those groups; the naive block in FP64.
+ *
+ * One CTA of UTHREADS threads per (panel, level), the finest level first,
+ * chunks of UTT = 64 targets.  The MMA's 128 rows are the single-layer rows
+ * of the chunk's targets (rows 0..63) and their double-layer rows (64..127),
+ * its N the padded interpolation columns (ncw), its K the level nodes, UNT
+ * to a tile.  Shared-memory operands in the K-major canonical layout without
+ * swizzle (core matrices of 8 rows x 16 bytes): A as [node quad][row][4],
+ * B as [node quad][column][4] (the host lays the interpolation tables out
+ * so, tile after tile, and one bulk copy a part moves a tile).  UNS
+ * pipeline stages: while the tensor cores work on tile t, the threads
+ * compute tile t+1's kernel values and thread 0 has its interpolation rows
+ * copied (an mbarrier counts their bytes); a stage is released by the
+ * tcgen05.commit of the MMAs that read it, and two accumulator buffers in
+ * tensor memory alternate between groups, so one is added into the FP64
+ * registers while the MMAs fill the other.  Every wait
+ * on an mbarrier is bounded (about a second); after a timeout the CTA sets
+ * g_qol_wait_err, waits (bounded) for its MMAs in flight, frees its tensor
+ * memory and returns.
  * --------------------------------------------------------------------- */
-__device__ __forceinline__ unsigned tf32_rna(float x) {
-  unsigned r;
-  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
-  return r;
+#define UTT 64        /* targets per chunk */
+#define UNT 32        /* level nodes per tile (4 MMA k-steps of 8) */
+#define UNS 3         /* pipeline stages */
+#define UG 2          /* tiles per FP32 accumulation group */
+#define UTHREADS 512
+__device__ unsigned g_qol_wait_err; /* nonzero: a bounded wait of the FP32 level-sum kernel timed out */
+
+/* TF32 rounding of an FP32 bit pattern: to nearest, ties away from zero (the
+ * rounding of cvt.rna.tf32.f32), done on the integer pipes */
+__device__ __forceinline__ unsigned tf32_rna_bits(unsigned u) { return (u + 0x1000u) & 0xFFFFE000u; }
+/* hi = TF32 rounding of x, lo = TF32 rounding of x - hi */
+__device__ __forceinline__ void tf32_split(float x, float& hi, float& lo) {
+  hi = __uint_as_float(tf32_rna_bits(__float_as_uint(x)));
+  lo = __uint_as_float(tf32_rna_bits(__float_as_uint(x - hi)));
 }
-__device__ __forceinline__ void tf32_split(float x, unsigned& hi, unsigned& lo) {
-  hi = tf32_rna(x);
-  lo = tf32_rna(x - __uint_as_float(hi));
+__device__ __forceinline__ unsigned long long gtimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+  return t;
 }
-/* D(16x8) += A(16x8, row) B(8x8, col), TF32 in, FP32 accumulate; per lane
- * a = A[g][t], A[g+8][t], A[g][t+4], A[g+8][t+4]; b = B[t][g], B[t+4][g];
- * d = D[g][2t], D[g][2t+1], D[g+8][2t], D[g+8][2t+1] (g = lane/4, t = lane%4) */
-__device__ __forceinline__ void mma_tf32(float* d, const unsigned* a, unsigned b0, unsigned b1) {
-  asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-               : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-               : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+__device__ __forceinline__ bool mbar_test(unsigned a, unsigned parity) {
+  unsigned ok;
+  asm volatile("{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+               : "=r"(ok)
+               : "r"(a), "r"(parity)
+               : "memory");
+  return ok != 0;
+}
+/* wait until the phase of the given parity of the mbarrier at shared address
+ * a has completed; false after about a second without it */
+__device__ bool mbar_wait_bounded(unsigned a, unsigned parity) {
+  if (mbar_test(a, parity)) return true;
+  const unsigned long long t0 = gtimer_ns();
+  do {
+    __nanosleep(64);
+    if (mbar_test(a, parity)) return true;
+  } while (gtimer_ns() - t0 < 1000000000ull);
+  return false;
+}
+/* shared-memory matrix descriptor of tcgen05.mma: K-major, no swizzle;
+ * lbo: bytes between the two core matrices along K, sbo: bytes between
+ * 8-row groups; bit 46: the descriptor version of sm_100 */
+__device__ __forceinline__ unsigned long long umma_desc(unsigned saddr, unsigned lbo, unsigned sbo) {
+  return (unsigned long long)((saddr >> 4) & 0x3FFFu) | ((unsigned long long)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((unsigned long long)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+/* D[tmem] (+)= A B, TF32 operands from shared memory, FP32 accumulate;
+ * acc = 0 overwrites D */
+__device__ __forceinline__ void umma_tf32(unsigned d, unsigned long long a, unsigned long long b, unsigned idesc,
+                                          unsigned acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc)
+      : "memory");
+}
+/* 8 consecutive FP32 columns of this warp's 32 tensor-memory lanes, one lane
+ * a thread, added into a[0..7] (the wait takes the registers, so nothing
+ * reads them before the load has completed) */
+__device__ __forceinline__ void tmem_add8(unsigned taddr, double* a) {
+  unsigned v0, v1, v2, v3, v4, v5, v6, v7;
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+               : "=r"(v0), "=r"(v1), "=r"(v2), "=r"(v3), "=r"(v4), "=r"(v5), "=r"(v6), "=r"(v7)
+               : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n"
+               : "+r"(v0), "+r"(v1), "+r"(v2), "+r"(v3), "+r"(v4), "+r"(v5), "+r"(v6), "+r"(v7)
+               :
+               : "memory");
+  a[0] += (double)__uint_as_float(v0); a[1] += (double)__uint_as_float(v1);
+  a[2] += (double)__uint_as_float(v2); a[3] += (double)__uint_as_float(v3);
+  a[4] += (double)__uint_as_float(v4); a[5] += (double)__uint_as_float(v5);
+  a[6] += (double)__uint_as_float(v6); a[7] += (double)__uint_as_float(v7);
+}
+template <int NB>
+struct UmmaShape {
+  static constexpr int NCW = 32 * NB;                 /* MMA N: padded interpolation columns */
+  static constexpr int ABYTES = 128 * UNT * 4;        /* one TF32 part of the A tile */
+  static constexpr int BBYTES = NCW * UNT * 4;        /* one TF32 part of the B tile */
+  static constexpr int NDOFF = 2 * ABYTES + 2 * BBYTES; /* the tile's node values: 7 x UNT floats */
+  static constexpr int STG = (NDOFF + 7 * UNT * 4 + 1023) / 1024 * 1024;
+  static constexpr unsigned NCOL = 2 * NCW <= 32 ? 32u : 2 * NCW <= 64 ? 64u : 2 * NCW <= 128 ? 128u
+                                 : 2 * NCW <= 256 ? 256u : 512u; /* two accumulator buffers, a power of 2 */
+  /* instruction descriptor: FP32 accumulator, TF32 A and B, both K-major, N, M = 128 */
+  static constexpr unsigned IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((unsigned)(NCW >> 3) << 17) | (8u << 24);
+  /* after the stages: 2 UNS mbarriers, the tensor-memory address, and per
+   * target of the chunk its FP64 coordinates, row and local id */
+  static constexpr size_t SMEM = (size_t)UNS * STG + 16 * UNS + 16 + (size_t)UTT * (24 + 8 + 4);
+};
+/* global -> shared bulk copy (no tensor map), completing on the mbarrier bar */
+__device__ __forceinline__ void bulk_g2s(unsigned dst, const void* src, unsigned bytes, unsigned bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
 }
 
-/* one CTA per (panel, level), chunks of DTT = 32 targets, tiles of DNT = 32
- * nodes double-buffered as in k_direct: the next tile's TF32 interpolation
- * parts arrive by async copy and its node values (panel-relative, in FP32)
- * are loaded during the current tile's tensor work; coordinates are taken
- * relative to the panel's first node so that the FP32 differences keep their
- * relative accuracy.  Warp w: targets 16 (w>>2) .. +15, column blocks
- * (w&3) NB .. +NB-1 */
 template <int NB>
-__global__ void __launch_bounds__(256, 2) k_direct_tf32(OrderTab T, PanelIn P, PairIn Q, LevelWS W, PairWS G,
-                                                        OutCOO O, int pan0) {
-  const int pan = pan0 + blockIdx.x, l = blockIdx.y; /* panels pan0 .. pan0 + gridDim.x - 1 */
-  if (l >= T.nlevel) return;
+__global__ void __launch_bounds__(UTHREADS, 1) k_direct_umma(OrderTab T, PanelIn P, PairIn Q, LevelWS W, PairWS G,
+                                                            OutCOO O, int pan0) {
+  using U = UmmaShape<NB>;
+  constexpr int NCW = U::NCW, ABYTES = U::ABYTES, BBYTES = U::BBYTES, STG = U::STG;
+  constexpr int ACOL = NCW / 4; /* accumulator columns of a thread */
+  const int pan = pan0 + blockIdx.x, l = T.nlevel - 1 - (int)blockIdx.y; /* panels pan0 .., the finest level first */
+  if (l < 0) return;
   const int cntl = G.cnt[(size_t)pan * 8 + l + 1];
   if (cntl == 0) return;
+  extern __shared__ __align__(1024) unsigned char usm[];
+  unsigned long long* mbar = reinterpret_cast<unsigned long long*>(usm + UNS * STG);
+  unsigned* tslot = reinterpret_cast<unsigned*>(mbar + 2 * UNS);
+  double* tg = reinterpret_cast<double*>(tslot + 4); /* UTT x 3 */
+  long long* trow = reinterpret_cast<long long*>(tg + 3 * UTT);
+  int* tloc = reinterpret_cast<int*>(trow + UTT);
+  double* accs = reinterpret_cast<double*>(usm); /* [layer][NCW][UTT], the epilogue's sums: overlays the stages */
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const unsigned sbase = (unsigned)__cvta_generic_to_shared(usm);
+  const unsigned md0 = (unsigned)__cvta_generic_to_shared(mbar); /* per stage: its MMAs are done */
+  const unsigned bf0 = md0 + 8 * UNS;                             /* per stage: its interpolation rows have landed */
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     (unsigned)__cvta_generic_to_shared(tslot)),
+                 "r"(U::NCOL)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int s = 0; s < 2 * UNS; ++s)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(md0 + 8 * s) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const unsigned tmem = *tslot;
+
   const int offl = G.off[(size_t)pan * 8 + l + 1];
   const int hd = T.hd, n = T.n[l];
   const long long p0 = Q.tcxi[pan] - 1, m = Q.tcxi[pan + 1] - Q.tcxi[pan];
   const double* node = W.node[l] + (size_t)pan * n * 7;
-  const unsigned* Ihg = T.interp_hi[l]; /* B-fragment order, tiles of 32 rows */
+  const unsigned* Ihg = T.interp_hi[l]; /* tiles of UNT rows in the B layout above */
   const unsigned* Ilg = T.interp_lo[l];
-  constexpr int NCW = 32 * NB;     /* padded columns */
-  constexpr int NBT = NCW / 8;     /* column blocks of 8 */
-  constexpr int KW = DNT * DTT;    /* words of one kernel-value part (A-fragment order) */
-  constexpr int IW = DNT * NCW;    /* words of one interpolation part of a tile */
-  constexpr int STG = 4 * KW + 2 * IW + 8 * DNT; /* words per stage: K parts, I parts, nodes (7 x DNT floats) */
-  extern __shared__ __align__(16) unsigned fsm[];
-  double* tg = reinterpret_cast<double*>(fsm + 2 * STG); /* DTT x 3 */
-  float* xt = reinterpret_cast<float*>(tg + 3 * DTT);    /* DTT x 3, relative to the panel's first node */
-  int* tloc = reinterpret_cast<int*>(xt + 3 * DTT);
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int mb = w >> 2, nb0 = NB * (w & 3); /* this warp's 16-target block, first column block */
-  const int tb0 = 16 * mb, cb0 = 8 * nb0;
-  const int g = lane >> 2, t4 = lane & 3;
   const double i4p = 1.0 / (4.0 * QOL_PI);
   const double* pc = P.sx + (size_t)pan * hd * 3; /* the panel's first node */
   const double c0x = pc[0], c0y = pc[1], c0z = pc[2];
-  const int ntile = (n + DNT - 1) / DNT;
-  /* node value of this thread (field f, node nn of a tile), loaded early */
-  const int nf = threadIdx.x / DNT, nnn = threadIdx.x % DNT;
+  const int ntile = (n + UNT - 1) / UNT;
+  /* kernel values: target kr of the chunk, node quad kq of every tile */
+  const int kr = tid % UTT, kq = tid / UTT;
+  /* accumulators: tensor-memory lane quarter aq (rows 32 aq .. 32 aq + 31:
+   * single layer for aq < 2), column quarter ac; row ar of the chunk */
+  const int aq = warp & 3, ac = warp >> 2;
+  const int ar = 32 * (aq & 1) + lane;
+  const unsigned trow_t = tmem + ((unsigned)(32 * aq) << 16) + (unsigned)(ac * ACOL);
+  /* node staging: field nf, node nn of a tile */
+  const int nf = tid / UNT, nn = tid % UNT;
   auto node_load = [&](int t) -> double {
-    const int i = t * DNT + nnn;
+    const int i = t * UNT + nn;
     return (nf < 7 && i < n) ? node[(size_t)nf * n + i] : 0.0;
   };
   auto node_store = [&](int s, double v) {
     if (nf < 7) {
-      float* nd = reinterpret_cast<float*>(fsm + s * STG + 4 * KW + 2 * IW);
+      float* nd = reinterpret_cast<float*>(usm + s * STG + U::NDOFF);
       const double c = nf == 0 ? c0x : nf == 1 ? c0y : nf == 2 ? c0z : 0.0;
-      nd[nf * DNT + nnn] = (float)(nf == 6 ? v * i4p : v - c);
+      nd[nf * UNT + nn] = (float)(nf == 6 ? v * i4p : v - c);
     }
   };
-  auto fetch = [&](int t, int s) { /* TF32 parts of the tile's interpolation rows: one contiguous block each */
-    unsigned* Ih = fsm + s * STG + 4 * KW;
-    for (int e = threadIdx.x; e < IW / 2; e += blockDim.x) { /* 16-byte pieces of both parts */
-      const int part = e / (IW / 4), r = 4 * (e % (IW / 4));
-      cp_async16(Ih + part * IW + r, (part ? Ilg : Ihg) + (size_t)t * IW + r);
-    }
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  unsigned nfe = 0; /* thread 0: tiles whose interpolation rows were requested */
+  auto fetch = [&](unsigned u, int t) { /* thread 0: tile t (the CTA's tile u) into stage u % UNS, one bulk copy a part */
+    const unsigned s = u % UNS, bar = bf0 + 8 * s, dst = sbase + s * STG + 2 * ABYTES;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(2 * BBYTES) : "memory");
+    bulk_g2s(dst, Ihg + (size_t)t * (BBYTES / 4), BBYTES, bar);
+    bulk_g2s(dst + BBYTES, Ilg + (size_t)t * (BBYTES / 4), BBYTES, bar);
+    nfe = u + 1;
   };
-  /* FP32 kernel values of tile t as TF32 parts, written in A-fragment order:
-   * word q = ((mblock 4 + kslice) 32 + lane) 4 + i, i = rowhalf + 2 colhalf,
-   * holding K[16 mblock + g + 8 rowhalf][8 kslice + t + 4 colhalf] (lane = 4 g + t);
-   * consecutive threads write consecutive words */
-  auto kvals = [&](int t, int s, int nt) {
-    unsigned* KSh = fsm + s * STG;
-    unsigned* KSl = KSh + KW;
-    unsigned* KDh = KSl + KW;
-    unsigned* KDl = KDh + KW;
-    const float* nd = reinterpret_cast<const float*>(fsm + s * STG + 4 * KW + 2 * IW);
-    const int n0 = t * DNT;
-    for (int q = threadIdx.x; q < KW; q += blockDim.x) {
-      const int qb = q >> 7, ql = (q >> 2) & 31, qi = q & 3; /* (mblock, kslice), lane, element */
-      const int tt = 16 * (qb / (DNT / 8)) + (ql >> 2) + 8 * (qi & 1);
-      const int nn = 8 * (qb % (DNT / 8)) + (ql & 3) + 4 * (qi >> 1);
-      float sv = 0.0f, dv = 0.0f;
-      if (n0 + nn < n && tt < nt) {
-        const float dx = xt[3 * tt] - nd[nn], dy = xt[3 * tt + 1] - nd[DNT + nn], dz = xt[3 * tt + 2] - nd[2 * DNT + nn];
-        const float rr = dx * dx + dy * dy + dz * dz;
-        if (rr > 1.0e-28f) {
-          const float ri = rsqrtf(rr);
-          sv = nd[6 * DNT + nn] * ri;
-          dv = sv * ri * ri * (dx * nd[3 * DNT + nn] + dy * nd[4 * DNT + nn] + dz * nd[5 * DNT + nn]);
-        }
-      }
-      unsigned hi, lo;
-      tf32_split(sv, hi, lo);
-      KSh[q] = hi; KSl[q] = lo;
-      tf32_split(dv, hi, lo);
-      KDh[q] = hi; KDl[q] = lo;
-    }
-  };
-  for (int c0 = 0; c0 < cntl; c0 += DTT) {
-    const int nt = min(DTT, cntl - c0);
-    __syncthreads();
-    fetch(0, 0);
-    node_store(0, node_load(0));
-    if (threadIdx.x < DTT) {
-      const int tl = threadIdx.x < nt ? G.grp[p0 + offl + c0 + threadIdx.x] : -1;
-      tloc[threadIdx.x] = tl;
-      for (int d = 0; d < 3; ++d) tg[3 * threadIdx.x + d] = tl >= 0 ? Q.tcx[3 * (p0 + tl) + d] : 0.0;
-      xt[3 * threadIdx.x] = (float)(tg[3 * threadIdx.x] - c0x);
-      xt[3 * threadIdx.x + 1] = (float)(tg[3 * threadIdx.x + 1] - c0y);
-      xt[3 * threadIdx.x + 2] = (float)(tg[3 * threadIdx.x + 2] - c0z);
-    }
-    cp_async_wait_all();
-    __syncthreads();
-    kvals(0, 0, nt);
-    __syncthreads();
-    double aS[NB][4], aD[NB][4]; /* FP64 totals of this warp's fragments */
+  auto drain = [&](int buf, double* acc) {
 #pragma unroll
-    for (int b = 0; b < NB; ++b)
+    for (int j = 0; j < NB; ++j) tmem_add8(trow_t + (unsigned)(buf * NCW + 8 * j), acc + 8 * j);
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  };
+
+  /* branches depend only on values every thread agrees on (a wait's outcome
+   * is collected into to and made common at the next barrier), so every
+   * thread reaches the barriers and the warp-wide tensor-memory loads */
+  unsigned tc = 0; /* tiles committed by this CTA: tile u used stage u % UNS in its phase (u / UNS) & 1 */
+  int to = 0;      /* a wait timed out */
+  for (int c0 = 0; c0 < cntl && !to; c0 += UTT) {
+    const int nt = min(UTT, cntl - c0);
+    __syncthreads(); /* the previous chunk's epilogue is done with the stages and the target data */
+    if (tid < UTT) {
+      const int tl = tid < nt ? G.grp[p0 + offl + c0 + tid] : -1;
+      tloc[tid] = tl;
+      trow[tid] = tl >= 0 ? Q.tcxrow[p0 + tl] : 0;
+      for (int d = 0; d < 3; ++d) tg[3 * tid + d] = tl >= 0 ? Q.tcx[3 * (p0 + tl) + d] : 0.0;
+    }
+    if (tid == 0) fetch(tc, 0);
+    node_store(tc % UNS, node_load(0));
+    __syncthreads(); /* target data and tile 0's node values staged */
+    const bool kv = kr < nt;
+    const float xr = (float)(tg[3 * kr] - c0x), yr = (float)(tg[3 * kr + 1] - c0y), zr = (float)(tg[3 * kr + 2] - c0z);
+    double acc[ACOL];
 #pragma unroll
-      for (int c = 0; c < 4; ++c) { aS[b][c] = 0.0; aD[b][c] = 0.0; }
-    for (int t = 0; t < ntile; ++t) {
-      const int s = t & 1;
+    for (int j = 0; j < ACOL; ++j) acc[j] = 0.0;
+    for (int t = 0; t < ntile; ++t, ++tc) {
+      const int s = tc % UNS, s1 = (tc + 1) % UNS;
       double nv = 0.0;
-      if (t + 1 < ntile) { fetch(t + 1, s ^ 1); nv = node_load(t + 1); }
-      const uint4* KSh = reinterpret_cast<const uint4*>(fsm + s * STG);
-      const uint4* KSl = KSh + KW / 4;
-      const uint4* KDh = KSl + KW / 4;
-      const uint4* KDl = KDh + KW / 4;
-      const uint2* Ih = reinterpret_cast<const uint2*>(fsm + s * STG + 4 * KW);
-      const uint2* Il = Ih + IW / 2;
-      float fS[NB][4], fD[NB][4];
-#pragma unroll
-      for (int b = 0; b < NB; ++b)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) { fS[b][c] = 0.0f; fD[b][c] = 0.0f; }
-#pragma unroll
-      for (int ks = 0; ks < DNT / 8; ++ks) {
-        const int fa = (mb * (DNT / 8) + ks) * 32 + lane;
-        const uint4 vsh = KSh[fa], vsl = KSl[fa], vdh = KDh[fa], vdl = KDl[fa];
-        const unsigned sh[4] = {vsh.x, vsh.y, vsh.z, vsh.w}, sl[4] = {vsl.x, vsl.y, vsl.z, vsl.w};
-        const unsigned dh[4] = {vdh.x, vdh.y, vdh.z, vdh.w}, dl[4] = {vdl.x, vdl.y, vdl.z, vdl.w};
-#pragma unroll
-        for (int b = 0; b < NB; ++b) {
-          const int fb = (ks * NBT + nb0 + b) * 32 + lane;
-          const uint2 bh = Ih[fb], bl = Il[fb];
-          mma_tf32(fS[b], sl, bh.x, bh.y);
-          mma_tf32(fS[b], sh, bl.x, bl.y);
-          mma_tf32(fS[b], sh, bh.x, bh.y);
-          mma_tf32(fD[b], dl, bh.x, bh.y);
-          mma_tf32(fD[b], dh, bl.x, bl.y);
-          mma_tf32(fD[b], dh, bh.x, bh.y);
-        }
-      }
-#pragma unroll
-      for (int b = 0; b < NB; ++b)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) { aS[b][c] += (double)fS[b][c]; aD[b][c] += (double)fD[b][c]; }
       if (t + 1 < ntile) {
-        node_store(s ^ 1, nv);
-        cp_async_wait_all();
-        __syncthreads(); /* tile t+1's interpolation parts and nodes staged */
-        kvals(t + 1, s ^ 1, nt);
-      }
-      __syncthreads();
-    }
-    /* naive block (FP64) and the COO write; fragment element c: target
-     * tb0 + g + 8 (c >> 1), column cb0 + 8b + 2 t4 + (c & 1) */
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      const int tt = tb0 + g + 8 * (c >> 1);
-      if (tt >= nt) continue;
-      const int tl = tloc[tt];
-      const long long row = Q.tcxrow[p0 + tl];
-      const double x0 = tg[3 * tt], x1 = tg[3 * tt + 1], x2 = tg[3 * tt + 2];
-#pragma unroll
-      for (int b = 0; b < NB; ++b) {
-        const int k = cb0 + 8 * b + 2 * t4 + (c & 1);
-        if (k >= hd) continue;
-        double vs = aS[b][c], vd = aD[b][c];
-        if (O.subtract_naive) {
-          const size_t gj = (size_t)pan * hd + k;
-          double ns = 0.0, nd = 0.0;
-          if (row != (long long)gj + 1)
-            sdl_kernel(x0 - P.sx[3 * gj], x1 - P.sx[3 * gj + 1], x2 - P.sx[3 * gj + 2], P.snx[3 * gj],
-                       P.snx[3 * gj + 1], P.snx[3 * gj + 2], P.sw[gj] * i4p, ns, nd);
-          vs -= ns; vd -= nd;
+        /* stage s1 is free once tile tc + 1 - UNS's MMAs are done: thread 0
+         * waits for that before its copy into s1, and the barrier below
+         * orders every other thread's writes into s1 after its wait */
+        if (tid == 0) {
+          if (tc + 1 >= UNS) to |= !mbar_wait_bounded(md0 + 8 * s1, ((tc + 1 - UNS) / UNS) & 1);
+          fetch(tc + 1, t + 1);
         }
-        const size_t o = (size_t)p0 * hd + (size_t)k * m + tl;
-        O.vs[o] = vs;
-        O.vd[o] = vd;
+        nv = node_load(t + 1);
       }
+      { /* tile t's kernel values: target kr, nodes 4 kq .. 4 kq + 3, as TF32 parts */
+        const float* nd = reinterpret_cast<const float*>(usm + s * STG + U::NDOFF);
+        const float4 X = *reinterpret_cast<const float4*>(nd + 4 * kq);
+        const float4 Y = *reinterpret_cast<const float4*>(nd + UNT + 4 * kq);
+        const float4 Z = *reinterpret_cast<const float4*>(nd + 2 * UNT + 4 * kq);
+        const float4 NX = *reinterpret_cast<const float4*>(nd + 3 * UNT + 4 * kq);
+        const float4 NY = *reinterpret_cast<const float4*>(nd + 4 * UNT + 4 * kq);
+        const float4 NZ = *reinterpret_cast<const float4*>(nd + 5 * UNT + 4 * kq);
+        const float4 WW = *reinterpret_cast<const float4*>(nd + 6 * UNT + 4 * kq);
+        const float xs[4] = {X.x, X.y, X.z, X.w}, ys[4] = {Y.x, Y.y, Y.z, Y.w}, zs[4] = {Z.x, Z.y, Z.z, Z.w};
+        const float nxs[4] = {NX.x, NX.y, NX.z, NX.w}, nys[4] = {NY.x, NY.y, NY.z, NY.w};
+        const float nzs[4] = {NZ.x, NZ.y, NZ.z, NZ.w}, ws[4] = {WW.x, WW.y, WW.z, WW.w};
+        float sh[4], sl[4], dh[4], dl[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const float dx = xr - xs[i], dy = yr - ys[i], dz = zr - zs[i];
+          const float rr = dx * dx + dy * dy + dz * dz;
+          float sv = 0.0f, dv = 0.0f;
+          if (kv && rr > 1.0e-28f) {
+            const float ri = rsqrtf(rr);
+            sv = ws[i] * ri;
+            dv = sv * ri * ri * (dx * nxs[i] + dy * nys[i] + dz * nzs[i]);
+          }
+          tf32_split(sv, sh[i], sl[i]);
+          tf32_split(dv, dh[i], dl[i]);
+        }
+        unsigned char* A = usm + s * STG;
+        const int oS = (kq * 128 + kr) * 16, oD = (kq * 128 + UTT + kr) * 16;
+        *reinterpret_cast<float4*>(A + oS) = make_float4(sh[0], sh[1], sh[2], sh[3]);
+        *reinterpret_cast<float4*>(A + ABYTES + oS) = make_float4(sl[0], sl[1], sl[2], sl[3]);
+        *reinterpret_cast<float4*>(A + oD) = make_float4(dh[0], dh[1], dh[2], dh[3]);
+        *reinterpret_cast<float4*>(A + ABYTES + oD) = make_float4(dl[0], dl[1], dl[2], dl[3]);
+      }
+      if (t + 1 < ntile) node_store(s1, nv);
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); /* the A tile visible to the tensor cores */
+      to = __syncthreads_or(to);
+      if (to) break;
+      if (tid == 0) {
+        to |= !mbar_wait_bounded(bf0 + 8 * s, (tc / UNS) & 1); /* tile t's interpolation rows have landed */
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        /* descriptors of stage 0 advanced by (bytes >> 4): the start address is
+         * the low 14 bits and every shared address here is below 256 KB */
+        const unsigned long long a0 = umma_desc(sbase, 2048, 128) + (unsigned)(s * STG >> 4);
+        const unsigned long long b0 = umma_desc(sbase + 2 * ABYTES, 16 * NCW, 128) + (unsigned)(s * STG >> 4);
+        const unsigned d = tmem + (unsigned)(((t / UG) & 1) * NCW);
+#pragma unroll
+        for (int ks = 0; ks < UNT / 8; ++ks) {
+          const unsigned long long ah = a0 + 256 * ks, al = ah + (ABYTES >> 4);
+          const unsigned long long bh = b0 + 2 * NCW * ks, bl = bh + (BBYTES >> 4);
+          umma_tf32(d, al, bh, U::IDESC, (t % UG) | ks);
+          umma_tf32(d, ah, bl, U::IDESC, 1u);
+          umma_tf32(d, ah, bh, U::IDESC, 1u);
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(md0 + 8 * s)
+                     : "memory");
+      }
+      if (t % UG == 0 && t > 0) { /* group t / UG - 1 is complete with tile tc - 1: add it up */
+        to |= !mbar_wait_bounded(md0 + 8 * ((tc - 1) % UNS), ((tc - 1) / UNS) & 1);
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        drain((t / UG - 1) & 1, acc);
+      }
+    }
+    if (__syncthreads_or(to)) { to = 1; break; }
+    to |= !mbar_wait_bounded(md0 + 8 * ((tc - 1) % UNS), ((tc - 1) / UNS) & 1); /* the last group */
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    drain(((ntile - 1) / UG) & 1, acc);
+    to = __syncthreads_or(to); /* every MMA and copy of the chunk is complete: the stages are free */
+    if (to) break;
+#pragma unroll
+    for (int j = 0; j < ACOL; ++j) accs[((aq < 2 ? 0 : NCW) + ac * ACOL + j) * UTT + ar] = acc[j];
+    __syncthreads();
+    /* naive block (FP64) and the COO write, a thread per (column, target):
+     * consecutive threads take consecutive targets of a column */
+    for (int e = tid; e < hd * nt; e += UTHREADS) {
+      const int k = e / nt, r = e - k * nt;
+      double vs = accs[k * UTT + r], vd = accs[(NCW + k) * UTT + r];
+      if (O.subtract_naive) {
+        const size_t gj = (size_t)pan * hd + k;
+        double ns = 0.0, ndv = 0.0;
+        if (trow[r] != (long long)gj + 1)
+          sdl_kernel(tg[3 * r] - P.sx[3 * gj], tg[3 * r + 1] - P.sx[3 * gj + 1], tg[3 * r + 2] - P.sx[3 * gj + 2],
+                     P.snx[3 * gj], P.snx[3 * gj + 1], P.snx[3 * gj + 2], P.sw[gj] * i4p, ns, ndv);
+        vs -= ns; vd -= ndv;
+      }
+      const size_t o = (size_t)p0 * hd + (size_t)k * m + tloc[r];
+      O.vs[o] = vs;
+      O.vd[o] = vd;
     }
   }
-}
-template <int NB>
-constexpr size_t direct_tf32_smem() {
-  return sizeof(unsigned) * 2 * (4 * DNT * DTT + 2 * DNT * 32 * NB + 8 * DNT) + sizeof(double) * 3 * DTT +
-         sizeof(float) * 3 * DTT + sizeof(int) * DTT;
+  if (to) { /* a wait timed out: flag it, let the MMAs and copies in flight finish (bounded), free the tensor memory */
+    if (tid == 0) {
+      atomicOr(&g_qol_wait_err, 1u);
+      if (tc > 0) mbar_wait_bounded(md0 + 8 * ((tc - 1) % UNS), ((tc - 1) / UNS) & 1);
+      for (unsigned u = tc; u < nfe; ++u) mbar_wait_bounded(bf0 + 8 * (u % UNS), (u / UNS) & 1);
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(U::NCOL) : "memory");
+  }
 }
 
 /* ===================================================================== */
@@ -2285,13 +2410,17 @@ cudaError_t qol_launch_direct(const OrderTab& T, const PanelIn& P, const PairIn&
   };
   const int nb = T.ncw / 32; /* the padded interpolation rows fix the column blocks */
   if (nb < 1 || nb > 5 || T.ncw != 32 * ((T.hd + 31) / 32)) return cudaErrorInvalidValue;
-  if (T.sum_fp32) { /* the precision variant */
+  if (T.sum_fp32) { /* the precision variant: UTHREADS threads a CTA */
+    auto gu = [&](auto kern, size_t smem) {
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      kern<<<grid, UTHREADS, smem, st>>>(T, P, Q, W, G, O, pan0);
+    };
     switch (nb) {
-      case 1: go(k_direct_tf32<1>, direct_tf32_smem<1>()); break;
-      case 2: go(k_direct_tf32<2>, direct_tf32_smem<2>()); break;
-      case 3: go(k_direct_tf32<3>, direct_tf32_smem<3>()); break;
-      case 4: go(k_direct_tf32<4>, direct_tf32_smem<4>()); break;
-      case 5: go(k_direct_tf32<5>, direct_tf32_smem<5>()); break;
+      case 1: gu(k_direct_umma<1>, UmmaShape<1>::SMEM); break;
+      case 2: gu(k_direct_umma<2>, UmmaShape<2>::SMEM); break;
+      case 3: gu(k_direct_umma<3>, UmmaShape<3>::SMEM); break;
+      case 4: gu(k_direct_umma<4>, UmmaShape<4>::SMEM); break;
+      case 5: gu(k_direct_umma<5>, UmmaShape<5>::SMEM); break;
     }
     return cudaGetLastError();
   }
@@ -2303,6 +2432,16 @@ cudaError_t qol_launch_direct(const OrderTab& T, const PanelIn& P, const PairIn&
     case 5: go(k_direct<5>, direct_smem<5>()); break;
   }
   return cudaGetLastError();
+}
+cudaError_t qol_wait_error(unsigned* flag, cudaStream_t st) {
+  cudaError_t e = cudaMemcpyFromSymbolAsync(flag, g_qol_wait_err, sizeof(unsigned), 0, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess && *flag) {
+    const unsigned z = 0;
+    e = cudaMemcpyToSymbolAsync(g_qol_wait_err, &z, sizeof z, 0, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  }
+  return e;
 }
 cudaError_t qol_launch_direct_queue(const DirectJob* jobs, int nbmax, const int* items, int nitems, int* head,
                                     cudaStream_t st) {

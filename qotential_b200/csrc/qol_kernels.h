@@ -11,8 +11,8 @@ struct OrderTab {
   double dist;
   int n[4], nsub[4];
   const double* interp[4];    /* n_l x ncw, row-major; columns hd .. ncw-1 zero (16-byte rows) */
-  const unsigned* interp_hi[4], *interp_lo[4]; /* interp in FP32 as TF32 high and low parts (precision variant),
-                                                  in mma B-fragment order, rows zero-padded to tiles of 32 */
+  const unsigned* interp_hi[4], *interp_lo[4]; /* interp in FP32 as TF32 high and low parts (precision variant):
+                                                  tiles of 32 rows (zero-padded), each [row quad][ncw][4] */
   int ncw;                    /* 32 ceil(hd / 32) */
   int panel_cs, panel_nt;     /* k_rrq_panel's cluster size and CTA threads (0: the default choice) */
   const double* wt[4];        /* n_l */
@@ -27,7 +27,7 @@ struct OrderTab {
   const unsigned* xred;   /* per translation output: first partial slot, slot count */
   int xslots;
   const double* tginv;    /* nquad x nquad: 1/(tgl[i] - tgl[i-k-1]) at [k*nquad + i] */
-  int sum_fp32;           /* 1: level sums in FP32 on the 3xTF32 tensor path (precision variant) */
+  int sum_fp32;           /* 1: level sums in FP32, 3xTF32 on tcgen05 (precision variant) */
   int xsteps;
   const double* sk[4];    /* n_l x 4: the selector check's sketch vectors on the level nodes (I_l v, v = +-1) */
   int force_level;        /* 1..nlevel: every pair the walk resolves by a direct sum takes this level (labels) */
@@ -114,6 +114,9 @@ cudaError_t qol_launch_sel_update(const float* slot, int nslot, float inv_n, flo
 cudaError_t qol_launch_direct(const OrderTab& T, const PanelIn& P, const PairIn& Q, const LevelWS& W,
                               const PairWS& G, const OutCOO& O, int npan, cudaStream_t st,
                               int pan0 = 0 /* first panel of the launch */);
+/* reads (synchronising st) and clears the flag the FP32 level-sum kernel
+ * sets when one of its bounded waits times out; *flag nonzero: it did */
+cudaError_t qol_wait_error(unsigned* flag, cudaStream_t st);
 /* one pipeline job's level-sum inputs (the batched entry's persistent launch) */
 struct DirectJob {
   OrderTab T;
