@@ -872,8 +872,9 @@ def main():
         chosen["order10"] = forms_compare(W10, args.steps, 2)
         del W10
         torch.cuda.empty_cache()
-        chosen["note"] = ("chosen form = qol_set_sum_precision(1): level kernel sums in FP32 (3xTF32 tensor "
-                          "contraction, FP64 accumulation across tiles); RRQ moments, solves and fits FP64; "
+        chosen["note"] = ("chosen form = qol_set_sum_precision(1): level kernel sums in FP32 (3xTF32 "
+                          "contraction on tcgen05, compensated accumulation across 32-node tiles); RRQ "
+                          "moments, solves and fits FP64; "
                           "device step with inputs resident, CUDA events; row_error = per target row, "
                           "max |chosen - plain| / max |plain| over the row's entries")
     batched = None

@@ -259,9 +259,10 @@ int qol_interp_matrix(qol_int korder, qol_int n, const double* uv, double* M);
 #define QOL_NPHASE 10
 /* Precision of the level-resolved kernel sums for the calls that follow
  * (library-wide): 0 = FP64 (default; the drop-in), 1 = the precision variant:
- * kernel values in FP32, contraction with the interpolation rows on the TF32
- * tensor path with a 3xTF32 split, FP32 accumulation over 32-node tiles and
- * FP64 across them; the naive block, the RRQ moments, solves and quaternion
+ * kernel values in FP32, contraction with the interpolation rows on the
+ * tcgen05 tensor cores (kind::tf32) with a 3xTF32 split, FP32 accumulation
+ * over 32-node tiles and compensated FP32 sums across them, FP64 from the
+ * chunk's end on; the naive block, the RRQ moments, solves and quaternion
  * fits stay FP64.  qol_rrq_noalloc always uses FP64.  No counterpart in the
  * reference (all FP64). */
 int qol_set_sum_precision(int mode);

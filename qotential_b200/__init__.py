@@ -412,8 +412,9 @@ def qol_direct_farfield(sx, snx, sw, ub, ubn):
 
 
 def qol_set_sum_precision(mode):
-    """0: FP64 level sums (default, the drop-in); 1: FP32 level sums on the
-    3xTF32 tensor path with FP64 accumulation across tiles (precision variant)."""
+    """0: FP64 level sums (default, the drop-in); 1: FP32 level sums, a 3xTF32
+    contraction on the tcgen05 tensor cores, FP32 over 32-node tiles and
+    compensated sums across them (precision variant)."""
     _check(lib().qol_set_sum_precision(C.c_int(int(mode))))
 
 

@@ -612,8 +612,9 @@ constexpr size_t direct_smem() {
  * their relative accuracy), the contraction with the interpolation rows by
  * tcgen05.mma kind::tf32 with the 3xTF32 split (a b ~ a_lo b_hi + a_hi b_lo
  * + a_hi b_hi, a_hi = TF32 rounding of a, a_lo = TF32 rounding of the rest),
- * accumulated in FP32 in tensor memory over UG tiles of UNT nodes and in
- * FP64 registers across those groups; the naive block in FP64.
+ * accumulated in FP32 in tensor memory over UG tiles of UNT nodes and as
+ * compensated (Kahan) FP32 sums in registers across those groups, in FP64
+ * from there on; the naive block in FP64.
  *
  * One CTA of UTHREADS threads per (panel, level), the finest level first,
  * chunks of UTT = 64 targets.  The MMA's 128 rows are the single-layer rows
@@ -636,7 +637,7 @@ constexpr size_t direct_smem() {
 #define UTT 64        /* targets per chunk */
 #define UNT 32        /* level nodes per tile (4 MMA k-steps of 8) */
 #define UNS 3         /* pipeline stages */
-#define UG 2          /* tiles per FP32 accumulation group */
+#define UG 1          /* tiles per FP32 accumulation group */
 #define UTHREADS 512
 __device__ unsigned g_qol_wait_err; /* nonzero: a bounded wait of the FP32 level-sum kernel timed out */
 
@@ -689,23 +690,25 @@ __device__ __forceinline__ void umma_tf32(unsigned d, unsigned long long a, unsi
       : "memory");
 }
 /* 8 consecutive FP32 columns of this warp's 32 tensor-memory lanes, one lane
- * a thread, added into a[0..7] (the wait takes the registers, so nothing
- * reads them before the load has completed) */
-__device__ __forceinline__ void tmem_add8(unsigned taddr, double* a) {
-  unsigned v0, v1, v2, v3, v4, v5, v6, v7;
+ * a thread, added into the compensated sums (a, c)[0..7] (the wait takes the
+ * registers, so nothing reads them before the load has completed) */
+__device__ __forceinline__ void tmem_add8(unsigned taddr, float* a, float* c) {
+  unsigned v[8];
   asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
-               : "=r"(v0), "=r"(v1), "=r"(v2), "=r"(v3), "=r"(v4), "=r"(v5), "=r"(v6), "=r"(v7)
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
                : "r"(taddr));
   asm volatile("tcgen05.wait::ld.sync.aligned;\n"
-               : "+r"(v0), "+r"(v1), "+r"(v2), "+r"(v3), "+r"(v4), "+r"(v5), "+r"(v6), "+r"(v7)
+               : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7])
                :
                : "memory");
-  a[0] += (double)__uint_as_float(v0); a[1] += (double)__uint_as_float(v1);
-  a[2] += (double)__uint_as_float(v2); a[3] += (double)__uint_as_float(v3);
-  a[4] += (double)__uint_as_float(v4); a[5] += (double)__uint_as_float(v5);
-  a[6] += (double)__uint_as_float(v6); a[7] += (double)__uint_as_float(v7);
-}
-template <int NB>
+#pragma unroll
+  for (int e = 0; e < 8; ++e) { /* compensated (Kahan) FP32 sum: a + c carries about twice FP32's precision */
+    const float y = __uint_as_float(v[e]) - c[e];
+    const float t = a[e] + y;
+    c[e] = __fsub_rn(__fsub_rn(t, a[e]), y);
+    a[e] = t;
+  }
+}template <int NB>
 struct UmmaShape {
   static constexpr int NCW = 32 * NB;                 /* MMA N: padded interpolation columns */
   static constexpr int ABYTES = 128 * UNT * 4;        /* one TF32 part of the A tile */
@@ -803,9 +806,9 @@ __global__ void __launch_bounds__(UTHREADS, 1) k_direct_umma(OrderTab T, PanelIn
     bulk_g2s(dst + BBYTES, Ilg + (size_t)t * (BBYTES / 4), BBYTES, bar);
     nfe = u + 1;
   };
-  auto drain = [&](int buf, double* acc) {
+  auto drain = [&](int buf, float* acc, float* cmp) {
 #pragma unroll
-    for (int j = 0; j < NB; ++j) tmem_add8(trow_t + (unsigned)(buf * NCW + 8 * j), acc + 8 * j);
+    for (int j = 0; j < NB; ++j) tmem_add8(trow_t + (unsigned)(buf * NCW + 8 * j), acc + 8 * j, cmp + 8 * j);
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   };
 
@@ -828,9 +831,9 @@ __global__ void __launch_bounds__(UTHREADS, 1) k_direct_umma(OrderTab T, PanelIn
     __syncthreads(); /* target data and tile 0's node values staged */
     const bool kv = kr < nt;
     const float xr = (float)(tg[3 * kr] - c0x), yr = (float)(tg[3 * kr + 1] - c0y), zr = (float)(tg[3 * kr + 2] - c0z);
-    double acc[ACOL];
+    float acc[ACOL], cmp[ACOL]; /* compensated FP32 sums across the groups: acc - cmp */
 #pragma unroll
-    for (int j = 0; j < ACOL; ++j) acc[j] = 0.0;
+    for (int j = 0; j < ACOL; ++j) acc[j] = cmp[j] = 0.0f;
     for (int t = 0; t < ntile; ++t, ++tc) {
       const int s = tc % UNS, s1 = (tc + 1) % UNS;
       double nv = 0.0;
@@ -903,17 +906,17 @@ __global__ void __launch_bounds__(UTHREADS, 1) k_direct_umma(OrderTab T, PanelIn
       if (t % UG == 0 && t > 0) { /* group t / UG - 1 is complete with tile tc - 1: add it up */
         to |= !mbar_wait_bounded(md0 + 8 * ((tc - 1) % UNS), ((tc - 1) / UNS) & 1);
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-        drain((t / UG - 1) & 1, acc);
+        drain((t / UG - 1) & 1, acc, cmp);
       }
     }
     if (__syncthreads_or(to)) { to = 1; break; }
     to |= !mbar_wait_bounded(md0 + 8 * ((tc - 1) % UNS), ((tc - 1) / UNS) & 1); /* the last group */
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    drain(((ntile - 1) / UG) & 1, acc);
+    drain(((ntile - 1) / UG) & 1, acc, cmp);
     to = __syncthreads_or(to); /* every MMA and copy of the chunk is complete: the stages are free */
     if (to) break;
 #pragma unroll
-    for (int j = 0; j < ACOL; ++j) accs[((aq < 2 ? 0 : NCW) + ac * ACOL + j) * UTT + ar] = acc[j];
+    for (int j = 0; j < ACOL; ++j) accs[((aq < 2 ? 0 : NCW) + ac * ACOL + j) * UTT + ar] = (double)acc[j] - (double)cmp[j];
     __syncthreads();
     /* naive block (FP64) and the COO write, a thread per (column, target):
      * consecutive threads take consecutive targets of a column */

@@ -1,7 +1,8 @@
 """The precision variant of the level sums (qol_set_sum_precision(1): FP32
-kernel values, 3xTF32 tensor contraction, FP64 accumulation across tiles)
-against the FP64 drop-in: its error on the correction rows, stated here, and
-the GRF identity at matched error (the metric compares the two forms there)."""
+kernel values, 3xTF32 contraction on the tcgen05 tensor cores, compensated
+accumulation across 32-node tiles) against the FP64 drop-in and the oracle:
+its error on the correction rows, stated here, and the GRF identity at matched
+error (the metric compares the two forms there)."""
 import numpy as np
 import pytest
 
