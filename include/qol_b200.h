@@ -154,9 +154,8 @@ int qol_getnearquad_lap_rrq_batch_dev(qol_int njob, const qol_near_job* jobs, vo
  * every call waits once on the host for `stream` (it reads the number of RRQ
  * targets back before sizing the per-target launches).
  *  - The first call on a device sets up (takes the array's device address with
- *    cudaGetSymbolAddress, uploads constants); make that first call before
- *    any stream capture.  A call with a new (order, orderff, nquad) re-uploads
- *    the tables into the array.
+ *    cudaGetSymbolAddress, uploads constants).  A call with a new (order,
+ *    orderff, nquad) re-uploads the tables into the array.
  *  - Calls share the array: calls that overlap on the GPU (other streams, other
  *    host threads' work still running) race.  Serialize them.
  *  - Limit: the order's tables, the refined levels of the panel and the panel's
