@@ -30,7 +30,13 @@
 
 namespace {
 
+/* g_mu serialises the entry points, except qol_getnearquad_lap_rrq_dev,
+ * which holds it only to set up and then runs under its stream's lock (calls
+ * on different streams run concurrently); g_tab_mu guards the per-order
+ * tables (their creation and the autotuner's one write), which every call
+ * reads.  Lock order: g_mu, g_ctx_mu, a stream's lock, g_tab_mu. */
 std::recursive_mutex g_mu;
+std::recursive_mutex g_tab_mu;
 thread_local std::string g_err;
 
 int fail(int code, const char* fmt, ...) {
@@ -143,6 +149,7 @@ int ensure_device() {
 
 /* build (or fetch) the device tables for one (nterms, orderff, nquad) */
 int order_tables(int nterms, int orderff, int nquad, OrderCache** out, int refine = -1) {
+  std::lock_guard<std::recursive_mutex> tl(g_tab_mu);
   if (refine < 0) refine = g_refine;
   if (nterms < 2 || nterms > QOL_MAXL || orderff < 2 || orderff - 1 > 20 || nquad < 2 || nquad > QOL_MAXNQ ||
       nterms - 1 > 20)
@@ -368,9 +375,12 @@ struct PipeRun {
 
 int PipeRun::front() {
   C = nullptr;
-  int rc = order_tables(J.nterms, J.orderff, J.nquad, &C);
-  if (rc) return rc;
-  T = C->T;
+  int rc = 0;
+  {
+    std::lock_guard<std::recursive_mutex> tl(g_tab_mu);
+    if ((rc = order_tables(J.nterms, J.orderff, J.nquad, &C))) return rc;
+    T = C->T;
+  }
   T.dist = J.distff;
   T.sum_fp32 = g_sum_precision == 1;
   T.force_level = g_force_level;
@@ -454,6 +464,7 @@ int PipeRun::front() {
    * one warm-up and one timed launch; every shape gives the same results
    * (the same arithmetic split over more or fewer CTAs), the fastest is kept
    * with the order's tables */
+  std::lock_guard<std::recursive_mutex> tl(g_tab_mu); /* the tuner writes the order's tables */
   if (nrrq > 0 && g_autotune && !C->T.panel_cs && npan >= 256) {
     int cs[8], nt[8];
     const int ns = qol_panel_shapes(hd, nq, cs, nt, 8);
@@ -579,11 +590,28 @@ int PipeRun::back(long long* hist_out, std::vector<int>* grp_out, int* cnt_out, 
 }
 
 int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* hist_out, std::vector<int>* grp_out,
-                 int* cnt_out) {
-  PipeRun P(J, st, timeinfo);
+                 int* cnt_out, Arena* a1 = &g_arena, Arena* a2 = &g_arena2) {
+  PipeRun P(J, st, timeinfo, a1, a2);
   int rc = P.front();
   if (rc) return rc;
   return P.back(hist_out, grp_out, cnt_out, false);
+}
+
+/* the device entry's workspace per (device, stream): calls on one stream share
+ * it and are ordered by its lock; calls on different streams run concurrently */
+struct StreamCtx {
+  std::mutex mu;
+  Arena a1, a2;
+};
+std::mutex g_ctx_mu;
+std::map<std::pair<int, cudaStream_t>, std::unique_ptr<StreamCtx>> g_ctx;
+StreamCtx* stream_ctx(cudaStream_t st) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  std::lock_guard<std::mutex> g(g_ctx_mu);
+  std::unique_ptr<StreamCtx>& c = g_ctx[std::make_pair(dev, st)];
+  if (!c) c.reset(new StreamCtx());
+  return c.get();
 }
 
 /* ---------------- patch-level handles ---------------- */
@@ -852,6 +880,7 @@ int qol_set_autotune(int on) {
 
 int qol_panel_shape(qol_int nterms, qol_int orderff, qol_int nquad, int* cs, int* nt) {
   std::lock_guard<std::recursive_mutex> g(g_mu);
+  std::lock_guard<std::recursive_mutex> tl(g_tab_mu);
   if (!cs || !nt) return fail(QOL_ERR_ARG, "null argument");
   *cs = 0; *nt = 0;
   const long long key = nterms + 100LL * orderff + 10000LL * nquad;
@@ -1343,10 +1372,18 @@ int qol_getnearquad_lap_rrq_dev(qol_int npan, qol_int nterms, qol_int hdim, qol_
                                 const qol_int* tcxi, qol_int orderff, double distff, qol_int iside, qol_int nnz,
                                 qol_int* sparsei, qol_int* sparsej, double* sparsevs, double* sparsevd,
                                 void* stream, int sync, qol_int* level_hist) {
-  std::lock_guard<std::recursive_mutex> g(g_mu);
+  std::unique_lock<std::recursive_mutex> g(g_mu);
   int rc = ensure_device();
   if (rc) return rc;
   cudaStream_t st = (cudaStream_t)stream; /* 0 = the legacy default stream */
+  /* with the per-phase kernel timing on, the call stays under the global lock
+   * (the timings add into one set of totals); otherwise under its stream's */
+  StreamCtx* cx = g_ktime_on ? nullptr : stream_ctx(st);
+  std::unique_lock<std::mutex> sl;
+  if (cx) {
+    g.unlock();
+    sl = std::unique_lock<std::mutex>(cx->mu);
+  }
   std::vector<long long> xi(npan + 1);
   CK(cudaMemcpyAsync(xi.data(), tcxi, sizeof(long long) * (npan + 1), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
@@ -1358,7 +1395,8 @@ int qol_getnearquad_lap_rrq_dev(qol_int npan, qol_int nterms, qol_int hdim, qol_
   J.P = PanelIn{sx, snx, sw, rts, rps};
   J.Q = PairIn{tcx, (const long long*)tcxrow, (const long long*)tcxi};
   J.vs = sparsevs; J.vd = sparsevd; J.si = (long long*)sparsei; J.sj = (long long*)sparsej;
-  rc = run_pipeline(J, st, nullptr, level_hist, nullptr, nullptr);
+  rc = cx ? run_pipeline(J, st, nullptr, level_hist, nullptr, nullptr, &cx->a1, &cx->a2)
+          : run_pipeline(J, st, nullptr, level_hist, nullptr, nullptr);
   if (rc) return rc;
   if (sync) CK(cudaStreamSynchronize(st));
   return 0;
@@ -1369,6 +1407,12 @@ int qol_release_workspace(void) {
   if (cudaDeviceSynchronize() != cudaSuccess) return fail(QOL_ERR_CUDA, "qol_release_workspace: device sync");
   for (Arena* a : {&g_arena, &g_arena2, &g_arena_io, &g_arena_grf}) a->release();
   g_batch_arenas.clear();
+  std::lock_guard<std::mutex> cg(g_ctx_mu);
+  for (auto& kv : g_ctx) { /* a call still running on that stream finishes first */
+    std::lock_guard<std::mutex> sl(kv.second->mu);
+    kv.second->a1.release();
+    kv.second->a2.release();
+  }
   return 0;
 }
 
