@@ -11,7 +11,10 @@
  * Every entry point returns a status (0 = ok) and also writes the reference's
  * ier argument where the reference has one.  Status codes:
  *   0 QOL_OK, 1 QOL_ERR_NOSLOT / layout, 2 QOL_ERR_HANDLE / nnz too small,
- *   3 QOL_ERR_NPOLS, 5 QOL_ERR_CUDA, 6 QOL_ERR_ORDER (unsupported order),
+ *   3 QOL_ERR_NPOLS, 5 QOL_ERR_CUDA, 6 QOL_ERR_ORDER (unsupported order: the
+ *   getnearquad / GRF / rrq entries take nterms 2..15; at nterms 16, hdim 136,
+ *   no thread-block cluster of the per-panel RRQ precompute fits in shared
+ *   memory and the call is refused before any work),
  *   7 QOL_ERR_TABLES (precomputed tables differ from the library's),
  *   8 QOL_ERR_ARG (null pointer / negative size).
  * The library never falls back to a CPU path: without a usable GPU every

@@ -381,6 +381,12 @@ int PipeRun::front() {
     if ((rc = order_tables(J.nterms, J.orderff, J.nquad, &C))) return rc;
     T = C->T;
   }
+  {
+    int cs[8], nt[8];
+    if (qol_panel_shapes(T.hd, T.nquad, cs, nt, 8) == 0) /* hdim 136 (nterms 16): no cluster of the panel kernel fits */
+      return fail(QOL_ERR_ORDER, "nterms=%d (hdim %d): the per-panel RRQ precompute has no launch shape; nterms <= 15",
+                  J.nterms, T.hd);
+  }
   T.dist = J.distff;
   T.sum_fp32 = g_sum_precision == 1;
   T.force_level = g_force_level;
