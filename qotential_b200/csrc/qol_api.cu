@@ -450,6 +450,11 @@ int PipeRun::front() {
   CK(cudaMemcpyAsync(off_h.data(), J.chunk_pan ? rrq_off : rrq_off + npan, sizeof(long long) * off_h.size(),
                      cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
+  if (g_sel_mode && g_sel_w && !g_force_level && !g_refine) { /* the inference's waits on the tensor cores are bounded */
+    unsigned werr = 0;
+    CK(qol_sel_wait_error(&werr, st));
+    if (werr) return fail(QOL_ERR_CUDA, "selector inference: a wait on the tensor cores timed out");
+  }
   nrrq = off_h.back();
   R.nrrq = nrrq;
   /* per-pair RRQ moment storage (separate arena: its size is known only now) */

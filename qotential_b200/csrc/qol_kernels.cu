@@ -649,37 +649,6 @@ __device__ __forceinline__ void tf32_split(float x, float& hi, float& lo) {
   hi = __uint_as_float(tf32_rna_bits(__float_as_uint(x)));
   lo = __uint_as_float(tf32_rna_bits(__float_as_uint(x - hi)));
 }
-__device__ __forceinline__ unsigned long long gtimer_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
-  return t;
-}
-__device__ __forceinline__ bool mbar_test(unsigned a, unsigned parity) {
-  unsigned ok;
-  asm volatile("{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-               : "=r"(ok)
-               : "r"(a), "r"(parity)
-               : "memory");
-  return ok != 0;
-}
-/* wait until the phase of the given parity of the mbarrier at shared address
- * a has completed; false after about a second without it */
-__device__ bool mbar_wait_bounded(unsigned a, unsigned parity) {
-  if (mbar_test(a, parity)) return true;
-  const unsigned long long t0 = gtimer_ns();
-  do {
-    __nanosleep(64);
-    if (mbar_test(a, parity)) return true;
-  } while (gtimer_ns() - t0 < 1000000000ull);
-  return false;
-}
-/* shared-memory matrix descriptor of tcgen05.mma: K-major, no swizzle;
- * lbo: bytes between the two core matrices along K, sbo: bytes between
- * 8-row groups; bit 46: the descriptor version of sm_100 */
-__device__ __forceinline__ unsigned long long umma_desc(unsigned saddr, unsigned lbo, unsigned sbo) {
-  return (unsigned long long)((saddr >> 4) & 0x3FFFu) | ((unsigned long long)((lbo >> 4) & 0x3FFFu) << 16) |
-         ((unsigned long long)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
-}
 /* D[tmem] (+)= A B, TF32 operands from shared memory, FP32 accumulate;
  * acc = 0 overwrites D */
 __device__ __forceinline__ void umma_tf32(unsigned d, unsigned long long a, unsigned long long b, unsigned idesc,

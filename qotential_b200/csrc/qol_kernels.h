@@ -103,6 +103,9 @@ cudaError_t qol_launch_sel_features(int hd, const PanelIn& P, const PairIn& Q, i
 cudaError_t qol_launch_sel_infer(const OrderTab& T, const PanelIn& P, const PairIn& Q, const LevelWS& W,
                                  const PairWS& G, int npan, const float* wbf, float conf, unsigned long long* cnt,
                                  int mode, cudaStream_t st);
+/* reads (synchronising st) and clears the flag k_sel_infer sets when one of
+ * its bounded waits on the tensor cores times out; *flag nonzero: it did */
+cudaError_t qol_sel_wait_error(unsigned* flag, cudaStream_t st);
 #define QOL_SEL_BETA 10.0 /* safety factor of the two-level check */
 cudaError_t qol_launch_sel_check(const OrderTab& T, const PanelIn& P, const PairIn& Q, const LevelWS& W,
                                  const PairWS& G, int npan, double tol, unsigned long long* cnt, cudaStream_t st);

@@ -152,52 +152,193 @@ __global__ void __launch_bounds__(128) k_sel_features(int hd, PanelIn P, PairIn 
   }
 }
 
-/* logits of one feature vector with the weights in shared memory */
-__device__ __forceinline__ void sel_forward(const float* w, const float* xin, float* z) {
-  float x[F], h1[H];
-#pragma unroll
-  for (int c = 0; c < F; ++c) x[c] = bf(xin[c]);
-#pragma unroll
-  for (int i = 0; i < H; ++i) {
-    float a = w[OB1 + i];
-#pragma unroll
-    for (int c = 0; c < F; ++c) a = fmaf(w[OW1 + c * H + i], x[c], a);
-    h1[i] = bf(fmaxf(a, 0.0f));
-  }
-#pragma unroll
-  for (int k = 0; k < NC; ++k) z[k] = w[OB3 + k];
-  for (int j = 0; j < H; ++j) {
-    float a = w[OB2 + j];
-#pragma unroll
-    for (int i = 0; i < H; ++i) a = fmaf(w[OW2 + i * H + j], h1[i], a);
-    a = bf(fmaxf(a, 0.0f));
-#pragma unroll
-    for (int k = 0; k < NC; ++k) z[k] = fmaf(w[OW3 + j * NC + k], a, z[k]);
-  }
+/* ---------------------------------------------------------------------
+ * Inference on the fifth-generation tensor cores.  One CTA of SI_T = 128
+ * threads per panel, tiles of 128 pairs, a pair a thread: its row of every
+ * matrix and its lane of tensor memory.  The three layers are
+ * tcgen05.mma kind::f16 products with BF16 operands in shared memory
+ * (K-major, no swizzle: core matrices of 8 rows x 16 bytes) and FP32
+ * accumulators in SI_TMEM columns of tensor memory, which every layer
+ * reuses: X (128 x 16, the 8 features and zeros) times W1 (N 64), then H1
+ * (128 x 64) times W2 (N 64, four K steps of 16), then H2 times W3 (N 16: the
+ * 5 classes and zeros).  After each layer every thread reads its row back 8
+ * columns at a time, adds the bias, takes the ReLU and rounds to BF16 into
+ * the next layer's A row: BF16 features, weights and hidden activations with
+ * FP32 sums, as in training (k_sel_grad).  Thread 0 issues each layer's MMAs
+ * and waits for their commit (bounded, about a second); the outcome is agreed
+ * at a barrier, and after a timeout the CTA sets g_sel_wait_err, leaves the
+ * rest of the panel to the plain walk (level 0) and frees its tensor memory.
+ * --------------------------------------------------------------------- */
+#define SI_T 128   /* threads, pairs a tile, the MMAs' M */
+#define SI_TMEM 64u
+__device__ unsigned g_sel_wait_err; /* nonzero: a bounded wait of k_sel_infer timed out */
+
+/* byte offset of element (r, k) of a K-major BF16 operand of `rows` rows */
+__device__ __forceinline__ unsigned kmaj_off(int r, int k, int rows) {
+  return (unsigned)((k >> 3) * (rows >> 3) * 128 + (r >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2);
 }
+/* D[tmem] (+)= A B, BF16 operands from shared memory, FP32 accumulate; acc = 0 overwrites D */
+__device__ __forceinline__ void umma_bf16(unsigned d, unsigned long long a, unsigned long long b, unsigned idesc,
+                                          unsigned acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc)
+      : "memory");
+}
+/* instruction descriptor: FP32 accumulator, BF16 A and B, both K-major, N = n, M = 128 */
+__host__ __device__ constexpr unsigned si_idesc(int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(n >> 3) << 17) | (8u << 24);
+}
+/* 8 consecutive FP32 columns of this thread's tensor-memory lane (the wait
+ * takes the registers, so nothing reads them before the load has completed) */
+__device__ __forceinline__ void tmem_ld8(unsigned taddr, float* v) {
+  unsigned r0, r1, r2, r3, r4, r5, r6, r7;
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+               : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3), "=r"(r4), "=r"(r5), "=r"(r6), "=r"(r7)
+               : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n"
+               : "+r"(r0), "+r"(r1), "+r"(r2), "+r"(r3), "+r"(r4), "+r"(r5), "+r"(r6), "+r"(r7)
+               :
+               : "memory");
+  v[0] = __uint_as_float(r0); v[1] = __uint_as_float(r1); v[2] = __uint_as_float(r2); v[3] = __uint_as_float(r3);
+  v[4] = __uint_as_float(r4); v[5] = __uint_as_float(r5); v[6] = __uint_as_float(r6); v[7] = __uint_as_float(r7);
+}
+__device__ __forceinline__ unsigned pack_bf2(float lo, float hi) {
+  return (unsigned)__bfloat16_as_ushort(__float2bfloat16_rn(lo)) |
+         ((unsigned)__bfloat16_as_ushort(__float2bfloat16_rn(hi)) << 16);
+}
+/* dynamic shared memory of k_sel_infer: the descriptor and node coordinates,
+ * then (1024-aligned) the A tile (128 x 64), W1 (64 x 16), W2 (64 x 64), W3
+ * (16 x 64) as BF16, the biases (64 + 64 + 8 floats), the mbarrier and the
+ * tensor-memory address */
+__host__ __device__ constexpr size_t si_head(int hd) { return (sizeof(double) * (16 + 3 * (size_t)hd) + 1023) & ~(size_t)1023; }
+__host__ __device__ constexpr size_t si_smem(int hd) { return si_head(hd) + 16384 + 2048 + 8192 + 2048 + 4 * 136 + 16; }
 
 /* learned level decision of every pair of the panel: G.level = accepted level
- * (1..nlevel+1) or 0 (the plain walk decides); counters [accepted, low
- * confidence, check failed] */
-__global__ void __launch_bounds__(128) k_sel_infer(OrderTab T, PanelIn P, PairIn Q, LevelWS W, PairWS G,
-                                                   const float* wbf, float conf, unsigned long long* cnt, int mode) {
-  const int pan = blockIdx.x, hd = T.hd;
-  extern __shared__ double ssm[];
+ * (1..nlevel+1), a candidate -l for the two-level check (mode 2) or 0 (the
+ * plain walk decides); counters [accepted, low confidence, check failed] */
+__global__ void __launch_bounds__(SI_T) k_sel_infer(OrderTab T, PanelIn P, PairIn Q, LevelWS W, PairWS G,
+                                                    const float* wbf, float conf, unsigned long long* cnt, int mode) {
+  const int pan = blockIdx.x, hd = T.hd, tid = threadIdx.x, warp = tid >> 5;
+  extern __shared__ __align__(16) double ssm[];
   double* dsc = ssm;
   double* s_sx = ssm + 16;
-  float* w = reinterpret_cast<float*>(s_sx + 3 * hd);
-  for (int e = threadIdx.x; e < QOL_SEL_NW; e += blockDim.x) w[e] = wbf[e];
-  sel_stage(pan, hd, P, s_sx, dsc);
+  unsigned char* XA = reinterpret_cast<unsigned char*>(ssm) + si_head(hd);
+  unsigned char* B1 = XA + 16384;
+  unsigned char* B2 = B1 + 2048;
+  unsigned char* B3 = B2 + 8192;
+  float* bias = reinterpret_cast<float*>(B3 + 2048); /* b1 [0, 64), b2 [64, 128), b3 [128, 136) */
+  unsigned long long* mbar = reinterpret_cast<unsigned long long*>(bias + 136);
+  unsigned* tslot = reinterpret_cast<unsigned*>(mbar + 1);
   __shared__ unsigned long long sc[3];
-  if (threadIdx.x < 3) sc[threadIdx.x] = 0;
+  const unsigned mb = (unsigned)__cvta_generic_to_shared(mbar);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     (unsigned)__cvta_generic_to_shared(tslot)),
+                 "r"(SI_TMEM)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mb) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (tid < 3) sc[tid] = 0;
+  /* the weights as B operands (rows = outputs, K = inputs): W1[c][i] at (i, c),
+   * W2[i][j] at (j, i), W3[j][k] at (k, j); zero rows and columns pad K to 16
+   * and N to 16 */
+  for (int e = tid; e < 64 * 16; e += SI_T) {
+    const int i = e >> 4, c = e & 15;
+    *reinterpret_cast<__nv_bfloat16*>(B1 + kmaj_off(i, c, 64)) = __float2bfloat16_rn(c < F ? wbf[OW1 + c * H + i] : 0.0f);
+  }
+  for (int e = tid; e < 64 * 64; e += SI_T) {
+    const int j = e >> 6, i = e & 63;
+    *reinterpret_cast<__nv_bfloat16*>(B2 + kmaj_off(j, i, 64)) = __float2bfloat16_rn(wbf[OW2 + i * H + j]);
+  }
+  for (int e = tid; e < 16 * 64; e += SI_T) {
+    const int k = e >> 6, j = e & 63;
+    *reinterpret_cast<__nv_bfloat16*>(B3 + kmaj_off(k, j, 16)) = __float2bfloat16_rn(k < NC ? wbf[OW3 + j * NC + k] : 0.0f);
+  }
+  for (int e = tid; e < 136; e += SI_T)
+    bias[e] = e < 64 ? wbf[OB1 + e] : e < 128 ? wbf[OB2 + e - 64] : (e - 128 < NC ? wbf[OB3 + e - 128] : 0.0f);
+  sel_stage(pan, hd, P, s_sx, dsc); /* ends with a barrier */
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const unsigned tmem = *tslot;
+  const unsigned trow = tmem + ((unsigned)(32 * warp) << 16); /* this thread's lane: row tid */
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(XA), sb1 = sa + 16384, sb2 = sb1 + 2048, sb3 = sb2 + 8192;
   const long long p0 = Q.tcxi[pan] - 1, m = Q.tcxi[pan + 1] - Q.tcxi[pan];
-  unsigned a = 0, lo = 0, ck = 0;
-  for (long long t = threadIdx.x; t < m; t += blockDim.x) {
-    const double* x = Q.tcx + 3 * (p0 + t);
-    float f[F], z[NC];
-    sel_features(x, dsc, hd, s_sx, f);
-    sel_forward(w, f, z);
+  unsigned a = 0, lo = 0, ck = 0, ph = 0;
+  int to = 0;
+  /* the operands written (generic proxy) become visible to the tensor cores;
+   * thread 0 issues, all agree on the commit's arrival */
+  auto layer = [&](int which) -> bool {
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    int bad = 0;
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      if (which == 1) {
+        umma_bf16(tmem, umma_desc(sa, 2048, 128), umma_desc(sb1, 1024, 128), si_idesc(64), 0u);
+      } else {
+#pragma unroll
+        for (int ks = 0; ks < 4; ++ks) {
+          if (which == 2)
+            umma_bf16(tmem, umma_desc(sa + 4096 * ks, 2048, 128), umma_desc(sb2 + 2048 * ks, 1024, 128), si_idesc(64),
+                      (unsigned)ks);
+          else
+            umma_bf16(tmem, umma_desc(sa + 4096 * ks, 2048, 128), umma_desc(sb3 + 512 * ks, 256, 128), si_idesc(16),
+                      (unsigned)ks);
+        }
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(mb)
+                   : "memory");
+      bad = !mbar_wait_bounded(mb, ph & 1);
+    }
+    ++ph;
+    to = __syncthreads_or(bad);
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    return !to;
+  };
+  /* this thread's row of the layer's sums, biased, ReLU, BF16: the next A row */
+  auto hidden = [&](const float* b) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      float v[8];
+      tmem_ld8(trow + 8 * q, v);
+      uint4 o;
+      o.x = pack_bf2(fmaxf(v[0] + b[8 * q + 0], 0.0f), fmaxf(v[1] + b[8 * q + 1], 0.0f));
+      o.y = pack_bf2(fmaxf(v[2] + b[8 * q + 2], 0.0f), fmaxf(v[3] + b[8 * q + 3], 0.0f));
+      o.z = pack_bf2(fmaxf(v[4] + b[8 * q + 4], 0.0f), fmaxf(v[5] + b[8 * q + 5], 0.0f));
+      o.w = pack_bf2(fmaxf(v[6] + b[8 * q + 6], 0.0f), fmaxf(v[7] + b[8 * q + 7], 0.0f));
+      *reinterpret_cast<uint4*>(XA + kmaj_off(tid, 8 * q, SI_T)) = o;
+    }
+  };
+  for (long long t0 = 0; t0 < m && !to; t0 += SI_T) {
+    const long long t = t0 + tid;
+    const bool valid = t < m;
+    if (valid) G.level[p0 + t] = 0; /* the plain walk, unless decided below */
+    const double* x = Q.tcx + 3 * (p0 + (valid ? t : 0));
+    float f[F];
+    if (valid) sel_features(x, dsc, hd, s_sx, f);
+    else
+#pragma unroll
+      for (int c = 0; c < F; ++c) f[c] = 0.0f;
+    *reinterpret_cast<uint4*>(XA + kmaj_off(tid, 0, SI_T)) =
+        make_uint4(pack_bf2(f[0], f[1]), pack_bf2(f[2], f[3]), pack_bf2(f[4], f[5]), pack_bf2(f[6], f[7]));
+    *reinterpret_cast<uint4*>(XA + kmaj_off(tid, 8, SI_T)) = make_uint4(0u, 0u, 0u, 0u);
+    if (!layer(1)) break;
+    hidden(bias);
+    if (!layer(2)) break;
+    hidden(bias + 64);
+    if (!layer(3)) break;
+    float z[8];
+    tmem_ld8(trow, z);
+    if (!valid) continue;
+#pragma unroll
+    for (int k = 0; k < NC; ++k) z[k] += bias[128 + k];
     int best = 0;
 #pragma unroll
     for (int k = 1; k < NC; ++k) best = z[k] > z[best] ? k : best;
@@ -237,11 +378,20 @@ __global__ void __launch_bounds__(128) k_sel_infer(OrderTab T, PanelIn P, PairIn
     else ++ck;
     G.level[p0 + t] = (signed char)lv;
   }
+  if (to && tid == 0) {
+    atomicOr(&g_sel_wait_err, 1u);
+    mbar_wait_bounded(mb, (ph - 1) & 1); /* the MMAs in flight (bounded again) */
+  }
   atomicAdd(&sc[0], (unsigned long long)a);
   atomicAdd(&sc[1], (unsigned long long)lo);
   atomicAdd(&sc[2], (unsigned long long)ck);
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
-  if (threadIdx.x < 3) atomicAdd(&cnt[threadIdx.x], sc[threadIdx.x]);
+  if (tid < 3) atomicAdd(&cnt[tid], sc[tid]);
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(SI_TMEM) : "memory");
+  }
 }
 
 /* the two-level check of the direct-level candidates (G.level = -l, l =
@@ -543,9 +693,21 @@ cudaError_t qol_launch_sel_infer(const OrderTab& T, const PanelIn& P, const Pair
                                  const PairWS& G, int npan, const float* wbf, float conf, unsigned long long* cnt,
                                  int mode, cudaStream_t st) {
   if (npan <= 0) return cudaSuccess;
-  const size_t smem = sizeof(double) * (16 + 3 * T.hd) + sizeof(float) * QOL_SEL_NW;
-  k_sel_infer<<<npan, 128, smem, st>>>(T, P, Q, W, G, wbf, conf, cnt, mode);
+  const size_t smem = si_smem(T.hd);
+  cudaError_t e = cudaFuncSetAttribute(k_sel_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k_sel_infer<<<npan, SI_T, smem, st>>>(T, P, Q, W, G, wbf, conf, cnt, mode);
   return cudaGetLastError();
+}
+cudaError_t qol_sel_wait_error(unsigned* flag, cudaStream_t st) {
+  cudaError_t e = cudaMemcpyFromSymbolAsync(flag, g_sel_wait_err, sizeof(unsigned), 0, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess && *flag) {
+    const unsigned z = 0;
+    e = cudaMemcpyToSymbolAsync(g_sel_wait_err, &z, sizeof z, 0, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  }
+  return e;
 }
 
 cudaError_t qol_launch_sel_check(const OrderTab& T, const PanelIn& P, const PairIn& Q, const LevelWS& W,
