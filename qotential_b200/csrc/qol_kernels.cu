@@ -1906,17 +1906,13 @@ __host__ __device__ constexpr int mom_region(int L, int slots) {
  *     partial sums per piece, then their fixed-order sum per output.
  * (E) the moments of every h_{l,m}. */
 template <int LB>
-__global__ void __launch_bounds__(MOM_T) k_rrq_moments(OrderTab T, PairIn Q, PairWS G, RRQWS R) {
+__global__ void __launch_bounds__(MOM_T, 7) k_rrq_moments(OrderTab T, PairIn Q, PairWS G, RRQWS R) {
   constexpr int RPT = (LB * (LB + 1) + MOM_T - 1) / MOM_T; /* real rows of M per thread */
   extern __shared__ __align__(16) double mom_sm[];
-  __shared__ double s_rq[(QOL_MAXL + 2) * (QOL_MAXL + 2)];
-  __shared__ double s_rn[(QOL_MAXL + 2) * (QOL_MAXL + 2)];
+  /* c_rq and c_rn are read from constant memory (a warp reads at most two
+   * entries at a time), which leaves shared memory to more resident pairs */
   __shared__ double s_rd[QOL_MAXL + 2], s_ri[QOL_MAXL + 2];
   const int tid = threadIdx.x;
-  for (int e = tid; e < (QOL_MAXL + 2) * (QOL_MAXL + 2); e += MOM_T) {
-    s_rq[e] = c_rq[e / (QOL_MAXL + 2)][e % (QOL_MAXL + 2)];
-    s_rn[e] = c_rn[e / (QOL_MAXL + 2)][e % (QOL_MAXL + 2)];
-  }
   for (int e = tid; e < QOL_MAXL + 2; e += MOM_T) { s_rd[e] = c_rd[e]; s_ri[e] = c_rinv[e]; }
   const long long gidx = R.glo + blockIdx.x;
   if (gidx >= R.ghi) return; /* uniform over the CTA */
@@ -1984,7 +1980,7 @@ __global__ void __launch_bounds__(MOM_T) k_rrq_moments(OrderTab T, PairIn Q, Pai
       for (int e = 0; e < n1; ++e) {
         if (e > 0) {
           const int l = pa + e;
-          const double q = s_rq[l * (QOL_MAXL + 2) + pa], a = (2.0 * l - 1.0) * Z;
+          const double q = c_rq[l][pa], a = (2.0 * l - 1.0) * Z;
           const double nr = (a * ur - r2 * vr) * q, ni = (a * ui - r2 * vi) * q;
           vr = ur; vi = ui; ur = nr; ui = ni;
         }
@@ -1994,7 +1990,7 @@ __global__ void __launch_bounds__(MOM_T) k_rrq_moments(OrderTab T, PairIn Q, Pai
         if (e < n2) {
           if (e > 0) {
             const int l = qa + e;
-            const double q = s_rq[l * (QOL_MAXL + 2) + qa], a = (2.0 * l - 1.0) * Z;
+            const double q = c_rq[l][qa], a = (2.0 * l - 1.0) * Z;
             const double nr = (a * sr - r2 * tr) * q, ni = (a * si - r2 * ti) * q;
             tr = sr; ti = si; sr = nr; si = ni;
           }
@@ -2050,7 +2046,7 @@ __global__ void __launch_bounds__(MOM_T) k_rrq_moments(OrderTab T, PairIn Q, Pai
     double ar = dr, ai = di, br = 0.0, bi = 0.0;
     for (int l = m; l <= L; ++l) {
       if (l > m) {
-        const double q = s_rq[l * (QOL_MAXL + 2) + m], a = (2.0 * l - 1.0) * Z;
+        const double q = c_rq[l][m], a = (2.0 * l - 1.0) * Z;
         const double nr = (a * ar - r2 * br) * q, ni = (a * ai - r2 * bi) * q;
         br = ar; bi = ai; ar = nr; ai = ni;
       }
@@ -2117,7 +2113,7 @@ __global__ void __launch_bounds__(MOM_T) k_rrq_moments(OrderTab T, PairIn Q, Pai
     int l = 1;
     while ((l + 1) * l / 2 <= k) ++l;
     const int m = k - l * (l - 1) / 2 + 1, n = l - 1;
-    const double Nf = s_rn[l * (QOL_MAXL + 2) + m];
+    const double Nf = c_rn[l][m];
     /* P[d][c]: component c (x,y,z frame) of the d-weighted moment */
     double PD[3][3], PS[3][3];
     const double* t0 = Tt + (n * (n + 1) / 2 + (m - 1)) * 12; /* order m-1 (always <= n) */
