@@ -405,6 +405,8 @@ def config4(w, steps=2, warmup=1):
     forms = time_forms(P["ntri"], nterms, pairs, D, out, w, steps, warmup, fl)
     del out, D
     torch.cuda.empty_cache()
+    import qotential_b200 as qol
+    qol.qol_release_workspace()  # the device entry's workspace (its stream's) before the GRF calls' own
     grf = grf_forms(P, nterms, w, fl)
     for f in forms:
         forms[f]["grf_error"] = grf[f]

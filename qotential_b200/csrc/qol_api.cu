@@ -1387,14 +1387,13 @@ int qol_getnearquad_lap_rrq_dev(qol_int npan, qol_int nterms, qol_int hdim, qol_
   int rc = ensure_device();
   if (rc) return rc;
   cudaStream_t st = (cudaStream_t)stream; /* 0 = the legacy default stream */
-  /* with the per-phase kernel timing on, the call stays under the global lock
-   * (the timings add into one set of totals); otherwise under its stream's */
-  StreamCtx* cx = g_ktime_on ? nullptr : stream_ctx(st);
-  std::unique_lock<std::mutex> sl;
-  if (cx) {
-    g.unlock();
-    sl = std::unique_lock<std::mutex>(cx->mu);
-  }
+  /* the call runs on its stream's workspace under the stream's lock; with the
+   * per-phase kernel timing on it also keeps the global lock (the timings add
+   * into one set of totals) */
+  StreamCtx* cx = stream_ctx(st);
+  if (!cx) return fail(QOL_ERR_CUDA, "no current device");
+  if (!g_ktime_on) g.unlock();
+  std::unique_lock<std::mutex> sl(cx->mu);
   std::vector<long long> xi(npan + 1);
   CK(cudaMemcpyAsync(xi.data(), tcxi, sizeof(long long) * (npan + 1), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
@@ -1406,8 +1405,7 @@ int qol_getnearquad_lap_rrq_dev(qol_int npan, qol_int nterms, qol_int hdim, qol_
   J.P = PanelIn{sx, snx, sw, rts, rps};
   J.Q = PairIn{tcx, (const long long*)tcxrow, (const long long*)tcxi};
   J.vs = sparsevs; J.vd = sparsevd; J.si = (long long*)sparsei; J.sj = (long long*)sparsej;
-  rc = cx ? run_pipeline(J, st, nullptr, level_hist, nullptr, nullptr, &cx->a1, &cx->a2)
-          : run_pipeline(J, st, nullptr, level_hist, nullptr, nullptr);
+  rc = run_pipeline(J, st, nullptr, level_hist, nullptr, nullptr, &cx->a1, &cx->a2);
   if (rc) return rc;
   if (sync) CK(cudaStreamSynchronize(st));
   return 0;
