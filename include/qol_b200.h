@@ -130,6 +130,18 @@ int qol_getnearquad_lap_rrq_dev(qol_int npan, qol_int nterms, qol_int hdim, qol_
  * the largest call's needs and is reused; the batched entry keeps one per
  * job); the next call allocates again.  No counterpart in the reference. */
 int qol_release_workspace(void);
+/* CUDA graphs of qol_getnearquad_lap_rrq_dev (no counterpart in the reference):
+ * on a created stream (not the legacy default one), with the FP64 level sums
+ * and the per-phase timing off, the launches after the host's read of the RRQ
+ * count (level sums, RRQ phases, COO indices) are captured as a CUDA graph that
+ * the stream keeps and replays while every launch argument is unchanged (the
+ * same tables, workspace, buffers and sizes, as in a solver's repeated calls);
+ * any other call recaptures it.  Counts since load of the graphs captured and
+ * replayed (diagnostics). */
+int qol_graph_stats(qol_int* captures, qol_int* replays);
+/* 1 (default): the device entry captures and replays the graphs above; 0:
+ * it launches directly (a kept graph is freed with qol_release_workspace) */
+int qol_set_graphs(int enable);
 typedef struct {
   qol_int npan, nterms, hdim, nquad, nsrc;
   const double *sx, *snx, *sw, *rts, *rps;

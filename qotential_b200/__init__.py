@@ -15,7 +15,8 @@ import numpy as np
 __all__ = [
     "lib", "QolError", "qol_simplex_precomp", "qol_build_patch_levels", "qol_lap3dsdlpmat_levels",
     "qol_clear_patch_levels", "qol_clear_patch_levels_all", "qol_rrq", "qol_getnearquad_lap_rrq",
-    "qol_getnearquad_lap_rrq_dev", "qol_getnearquad_lap_rrq_batch_dev", "qol_release_workspace", "qol_grf_near", "qol_grf_near_multi", "qol_grf_near_range", "qol_direct_farfield",
+    "qol_getnearquad_lap_rrq_dev", "qol_getnearquad_lap_rrq_batch_dev", "qol_release_workspace", "qol_graph_stats", "qol_set_graphs",
+    "qol_grf_near", "qol_grf_near_multi", "qol_grf_near_range", "qol_direct_farfield",
     "qol_direct_farfield_range", "qol_surface_panels", "qol_surface_charts", "qol_surface_panels_charts",
     "qol_interp_matrix", "qol_set_sum_precision",
     "SELECTOR_NW", "qol_selector_features", "qol_selector_grad", "qol_selector_train", "qol_selector_set",
@@ -249,6 +250,18 @@ def qol_getnearquad_lap_rrq_batch_dev(jobs, stream=0):
 def qol_release_workspace():
     """free the device workspace the library keeps between calls"""
     _check(lib().qol_release_workspace())
+
+
+def qol_set_graphs(enable):
+    """1 (default): the device entry replays CUDA graphs of its back stage; 0: direct launches"""
+    _check(lib().qol_set_graphs(C.c_int(int(enable))))
+
+
+def qol_graph_stats():
+    """(captured, replayed): CUDA graphs of the device entry's back stage since load"""
+    c, r = C.c_longlong(0), C.c_longlong(0)
+    _check(lib().qol_graph_stats(C.byref(c), C.byref(r)))
+    return int(c.value), int(r.value)
 
 
 def qol_grf_near(npan, nterms, nquad, sx, snx, sw, rts, rps, ub, ubn, u=None, orderff=None, distff=1.4,

@@ -335,6 +335,33 @@ int aux_stream(cudaStream_t* out) {
   return 0;
 }
 
+/* the back stage's launches on one stream of the device entry, captured as a
+ * CUDA graph and replayed while every launch argument is unchanged (the same
+ * order tables, workspace, buffers and sizes: a solver's repeated calls) */
+struct BackKey {
+  OrderTab T;
+  PanelIn P;
+  PairIn Q;
+  LevelWS W;
+  PairWS G;
+  RRQWS R;
+  OutCOO O;
+  const double* chart;
+  long long *si, *sj;
+  long long nrrq;
+  int npan, exterior, direct_done;
+};
+struct BackGraph {
+  BackKey key;
+  cudaGraphExec_t exec = nullptr;
+  void drop() {
+    if (exec) cudaGraphExecDestroy(exec);
+    exec = nullptr;
+  }
+};
+std::atomic<long long> g_graph_captures{0}, g_graph_replays{0};
+std::atomic<int> g_graphs_on{1}; /* qol_set_graphs */
+
 /* one pipeline call, in two stages: front() sizes and lays out the
  * workspace, computes the refined levels, classifies the pairs and sizes the
  * per-pair RRQ storage (one host read of the RRQ count); back() runs the level
@@ -358,6 +385,7 @@ struct PipeRun {
   std::vector<long long> off_h;
   Timing tm;
   cudaStream_t st2 = nullptr;
+  BackGraph* graph = nullptr; /* the stream's cached back stage (device entry), or none */
   PipeRun(const Job& j, cudaStream_t s, double* ti, Arena* a1 = &g_arena, Arena* a2 = &g_arena2)
       : J(j), st(s), timeinfo(ti), A1(a1), A2(a2) {}
   void rec(int phase, int sidx = 0) {
@@ -371,6 +399,8 @@ struct PipeRun {
   }
   int front();
   int back(long long* hist_out, std::vector<int>* grp_out, int* cnt_out, bool direct_done);
+  int launches(bool direct_done);
+  bool back_graph(bool direct_done);
 };
 
 int PipeRun::front() {
@@ -517,7 +547,7 @@ int PipeRun::front() {
   return 0;
 }
 
-int PipeRun::back(long long* hist_out, std::vector<int>* grp_out, int* cnt_out, bool direct_done) {
+int PipeRun::launches(bool direct_done) {
   int rc = 0;
   /* one pass over all panels, or (host entry) panel chunks whose every phase
    * runs before the next chunk's, so that chunk c's values are final early
@@ -578,6 +608,63 @@ int PipeRun::back(long long* hist_out, std::vector<int>* grp_out, int* cnt_out, 
   rec(8);
   if (J.si) CK(qol_launch_coo_index(T, J.Q, J.si, J.sj, npan, st));
   rec(-1);
+  return 0;
+}
+
+/* the back stage as a CUDA graph (device entry, one pass, no per-phase
+ * timing, FP64 level sums, a created stream): replays the stream's graph when
+ * every launch argument is the one it was captured with, else captures the
+ * launches and keeps the graph; false when that is not possible here (the
+ * launches then run directly) */
+bool PipeRun::back_graph(bool direct_done) {
+  if (!graph || !g_graphs_on.load() || J.chunk_pan || tm.on || T.sum_fp32 || st == nullptr) return false;
+  R.plo = 0; R.phi = npan; R.glo = 0; R.ghi = nrrq; /* the one pass's ranges, as launches() sets them */
+  BackKey k;
+  std::memset(&k, 0, sizeof k);
+  std::memcpy(&k.T, &T, sizeof T);
+  std::memcpy(&k.P, &J.P, sizeof J.P);
+  std::memcpy(&k.Q, &J.Q, sizeof J.Q);
+  std::memcpy(&k.W, &W, sizeof W);
+  std::memcpy(&k.G, &G, sizeof G);
+  std::memcpy(&k.R, &R, sizeof R);
+  k.O.vs = O.vs; k.O.vd = O.vd; k.O.omega = O.omega; k.O.subtract_naive = O.subtract_naive;
+  k.chart = J.chart; k.si = J.si; k.sj = J.sj; k.nrrq = nrrq;
+  k.npan = npan; k.exterior = J.exterior; k.direct_done = direct_done;
+  if (graph->exec && std::memcmp(&graph->key, &k, sizeof k) == 0) {
+    if (cudaGraphLaunch(graph->exec, st) == cudaSuccess) {
+      ++g_graph_replays;
+      return true;
+    }
+    cudaGetLastError();
+    graph->drop();
+    return false;
+  }
+  graph->drop();
+  if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  const int lrc = launches(direct_done);
+  cudaGraph_t gr = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(st, &gr);
+  cudaGraphExec_t ex = nullptr;
+  bool ok = lrc == 0 && ce == cudaSuccess && gr && cudaGraphInstantiate(&ex, gr, 0) == cudaSuccess;
+  if (gr) cudaGraphDestroy(gr);
+  if (ok && cudaGraphLaunch(ex, st) != cudaSuccess) ok = false;
+  if (!ok) {
+    if (ex) cudaGraphExecDestroy(ex);
+    cudaGetLastError();
+    return false;
+  }
+  graph->exec = ex;
+  std::memcpy(&graph->key, &k, sizeof k);
+  ++g_graph_captures;
+  return true;
+}
+
+int PipeRun::back(long long* hist_out, std::vector<int>* grp_out, int* cnt_out, bool direct_done) {
+  int rc = 0;
+  if (!back_graph(direct_done) && (rc = launches(direct_done))) return rc;
   if (T.sum_fp32) { /* the FP32 level-sum kernel's waits are bounded: a timeout is reported here */
     unsigned werr = 0;
     CK(qol_wait_error(&werr, st));
@@ -607,8 +694,9 @@ int PipeRun::back(long long* hist_out, std::vector<int>* grp_out, int* cnt_out, 
 }
 
 int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* hist_out, std::vector<int>* grp_out,
-                 int* cnt_out, Arena* a1 = &g_arena, Arena* a2 = &g_arena2) {
+                 int* cnt_out, Arena* a1 = &g_arena, Arena* a2 = &g_arena2, BackGraph* graph = nullptr) {
   PipeRun P(J, st, timeinfo, a1, a2);
+  P.graph = graph;
   int rc = P.front();
   if (rc) return rc;
   return P.back(hist_out, grp_out, cnt_out, false);
@@ -619,6 +707,7 @@ int run_pipeline(const Job& J, cudaStream_t st, double* timeinfo, long long* his
 struct StreamCtx {
   std::mutex mu;
   Arena a1, a2;
+  BackGraph graph; /* its back stage, captured over a1 and a2 */
 };
 std::mutex g_ctx_mu;
 std::map<std::pair<int, cudaStream_t>, std::unique_ptr<StreamCtx>> g_ctx;
@@ -1411,9 +1500,22 @@ int qol_getnearquad_lap_rrq_dev(qol_int npan, qol_int nterms, qol_int hdim, qol_
   J.P = PanelIn{sx, snx, sw, rts, rps};
   J.Q = PairIn{tcx, (const long long*)tcxrow, (const long long*)tcxi};
   J.vs = sparsevs; J.vd = sparsevd; J.si = (long long*)sparsei; J.sj = (long long*)sparsej;
-  rc = run_pipeline(J, st, nullptr, level_hist, nullptr, nullptr, &cx->a1, &cx->a2);
+  rc = run_pipeline(J, st, nullptr, level_hist, nullptr, nullptr, &cx->a1, &cx->a2, &cx->graph);
   if (rc) return rc;
   if (sync) CK(cudaStreamSynchronize(st));
+  return 0;
+}
+
+int qol_set_graphs(int enable) {
+  if (enable != 0 && enable != 1) return fail(QOL_ERR_ARG, "qol_set_graphs: 0 or 1");
+  g_graphs_on.store(enable);
+  return 0;
+}
+
+int qol_graph_stats(qol_int* captures, qol_int* replays) {
+  if (!captures || !replays) return fail(QOL_ERR_ARG, "null argument");
+  *captures = g_graph_captures.load();
+  *replays = g_graph_replays.load();
   return 0;
 }
 
@@ -1425,6 +1527,7 @@ int qol_release_workspace(void) {
   std::lock_guard<std::mutex> cg(g_ctx_mu);
   for (auto& kv : g_ctx) { /* a call still running on that stream finishes first */
     std::lock_guard<std::mutex> sl(kv.second->mu);
+    kv.second->graph.drop(); /* it launches into the workspace freed here */
     kv.second->a1.release();
     kv.second->a2.release();
   }
